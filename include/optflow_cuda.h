@@ -1,0 +1,201 @@
+/*
+ * optflow_cuda.h -- C ABI of the B200 (sm_100a) engine for optflow-soil's dense local-phase
+ * flow + DIC pair path.
+ *
+ * The ABI is what a thin FFI crate (`optflow-cuda`, cargo feature `cuda`) binds to implement
+ * the reference's `FineEngine` trait and the two stages the trait does not cover yet (coarse POC
+ * and the finish). Every entry point is plain C: host pointers and sizes in, host pointers out,
+ * an int status (0 = ok, else an error whose text is written to `err`, at most `errlen` bytes,
+ * NUL-terminated). No call ever falls back to CPU code: a missing or failing device is an error,
+ * like `EngineError` -> `TrackError::Engine` -> exit status 2 in the reference
+ * (rust/crates/optflow-cli/src/run.rs:115-135).
+ *
+ * Images are row-major, `w` columns by `h` rows, pixel (x, y) at index y * w + x, values as the
+ * reference's `Image<f32>` (luminance in [0, 1]). Displacements are in pixels.
+ */
+#ifndef OPTFLOW_CUDA_H
+#define OPTFLOW_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OFC_ABI_VERSION 1
+#define OFC_MAX_SCALES 16
+
+/* Status codes. */
+#define OFC_OK 0
+#define OFC_ERR_ARG 1     /* invalid argument or configuration (Config::validate's messages) */
+#define OFC_ERR_DEVICE 2  /* CUDA error, no device, out of device memory */
+#define OFC_ERR_BUSY 3    /* more concurrent calls than lanes (GpuEngine refuses, never blocks) */
+#define OFC_ERR_WINDOW 4  /* window larger than the engine accepts (check_window) */
+
+/*
+ * Every `Config` field the pair path reads, with the reference's meaning and defaults
+ * (python/optflow_ref/config.py:22-120; rust/crates/optflow-core/src/config.rs:487-600).
+ * Fill with ofc_config_default() and override; the engine validates it like Config::validate
+ * (config.py:166-245) for the keys it holds.
+ */
+typedef struct ofc_config {
+    /* coarse stage (POC grid) */
+    int32_t grid_step;          /* 16 */
+    int32_t poc_win;            /* 64, power of two >= 16 */
+    double max_disp;            /* 32 px: sets the pyramid depth */
+    double poc_peak_min;        /* 0.1 */
+    double median_thresh;       /* 2.0 */
+    /* fine stage (local phase of the Gabor bank) */
+    double lam;                 /* 8 */
+    int32_t n_scales;           /* 3 */
+    double scales[OFC_MAX_SCALES]; /* 0.6, 1.0, 1.6 */
+    int32_t n_orient;           /* 4 */
+    double bandwidth;           /* 0.5 */
+    double dc_cut;              /* 2.0 */
+    double sigma_w;             /* 4 */
+    int32_t shape_order;        /* 1 (affine, 6 unknowns) or 2 (quadratic, 12) */
+    double sigma_s;             /* 4 */
+    int32_t outer_iters;        /* 8 */
+    int32_t inner_iters;        /* 2 */
+    /* validity and strain */
+    double conf_min;            /* 0.2 */
+    double edge_guard;          /* -1 = automatic */
+    double edge_guard_min_area; /* -1 = automatic */
+    double phase_tol;           /* 0.4 rad */
+    int32_t strain_win;         /* 15 */
+    int32_t prewarp_freeze_at;  /* 0 = off (Rust-only key, rust/crates/optflow-core/src/prewarp.rs:79-116) */
+} ofc_config;
+
+/* Outputs of one tracked pair (track::Result, python/optflow_ref/track.py:15-31; the CLI's
+ * `.npy` set, rust/crates/optflow-cli/src/io.rs:573-625). Every pointer holds w*h elements and may
+ * be NULL when the caller does not want that output. */
+typedef struct ofc_pair_out {
+    float* ux;      /* NaN where invalid */
+    float* uy;
+    float* conf;    /* confidence before masking */
+    float* exx;     /* Green-Lagrange strain */
+    float* eyy;
+    float* exy;
+    float* gmax;
+    float* vol;
+    uint8_t* valid; /* 1 where ux is finite */
+    float* raw_ux;  /* unmasked field (the init of a sequence's next frame) */
+    float* raw_uy;
+    double timing[3]; /* seconds: coarse, fine, strain (device time, CUDA events) */
+} ofc_pair_out;
+
+typedef struct ofc_engine ofc_engine;
+
+/* ABI version of the loaded library (OFC_ABI_VERSION). */
+int ofc_abi_version(void);
+
+/* Config::default() (config.py:24-120). */
+void ofc_config_default(ofc_config* cfg);
+
+/* Config::validate() for the keys above (config.py:166-245); message text as the reference's. */
+int ofc_config_validate(const ofc_config* cfg, char* err, size_t errlen);
+
+/* The resolved guard distances of the config (Config::edge_guard_px, auto_edge_guard_px,
+ * edge_guard_min_area_px; config.py:257-272). */
+double ofc_edge_guard_px(const ofc_config* cfg);
+double ofc_auto_edge_guard_px(const ofc_config* cfg);
+double ofc_edge_guard_min_area_px(const ofc_config* cfg);
+
+/* GpuEngine::new / with_lanes (rust/crates/optflow-gpu/src/engine.rs:94,103): an engine on CUDA
+ * device `device` that accepts up to `lanes` (1 or 2) concurrent calls. NULL on error. */
+ofc_engine* ofc_create(int device, int lanes, char* err, size_t errlen);
+void ofc_destroy(ofc_engine* eng);
+
+/* FineEngine::lanes (engine.rs:63-70). */
+int ofc_lanes(const ofc_engine* eng);
+
+/* FineEngine::check_window (engine.rs:42-46): refuse a window the engine cannot hold. */
+int ofc_check_window(ofc_engine* eng, size_t w, size_t h, const ofc_config* cfg, char* err, size_t errlen);
+
+/* FineEngine::release_caches (engine.rs:114-117): free plans and pooled device buffers. */
+void ofc_release_caches(ofc_engine* eng);
+
+/*
+ * FineEngine::refine_raw (rust/crates/optflow-core/src/engine.rs:32-40; contract of
+ * phaseflow.rs:1441-1459): the outer/inner iterations of the fine stage on one window.
+ * i1, ux, uy: w x h; i2: w2 x h2, pixel (x, y) of i1 sits at (x + shift_x, y + shift_y) in i2
+ * before it is displaced (positions outside i2 clamp to its border). Outputs: RawFlow planes
+ * (phaseflow.rs:1408-1414), w*h doubles each.
+ */
+int ofc_refine_raw(ofc_engine* eng, const float* i1, size_t w, size_t h,
+                   const float* i2, size_t w2, size_t h2, int64_t shift_x, int64_t shift_y,
+                   const float* ux, const float* uy, const ofc_config* cfg,
+                   double* out_ux, double* out_uy, double* out_energy, double* out_resid,
+                   char* err, size_t errlen);
+
+/*
+ * phaseflow::refine / refine_low (python/optflow_ref/phaseflow.py:427-511;
+ * rust/crates/optflow-core/src/phaseflow.rs:1684-1757): refine_raw on the whole image plus the
+ * confidence with its border rule. out_low (nullable) = the f64 confidence < conf_min.
+ */
+int ofc_refine(ofc_engine* eng, const float* i1, const float* i2, size_t w, size_t h,
+               const float* ux, const float* uy, const ofc_config* cfg,
+               float* out_ux, float* out_uy, float* out_conf, float* out_resid, uint8_t* out_low,
+               char* err, size_t errlen);
+
+/* Grid of the coarse stage for a w x h image (poc.grid_points, python/optflow_ref/poc.py:61-64). */
+int ofc_grid_shape(size_t w, size_t h, const ofc_config* cfg, size_t* nx, size_t* ny);
+
+/*
+ * poc::coarse_flow (python/optflow_ref/poc.py:216-239; rust/crates/optflow-core/src/poc.rs:694-767):
+ * grid displacement at full resolution. init_ux/init_uy (nullable, w x h): a dense guess.
+ * Outputs: xs (nx), ys (ny), gux/guy/gpeak (ny x nx).
+ */
+int ofc_coarse_flow(ofc_engine* eng, const float* a, const float* b, size_t w, size_t h,
+                    const float* init_ux, const float* init_uy, const ofc_config* cfg,
+                    int32_t* xs, int32_t* ys, float* gux, float* guy, float* gpeak,
+                    char* err, size_t errlen);
+
+/*
+ * strain::displacement_gradient + strain_fields (python/optflow_ref/strain.py:61-112;
+ * rust/crates/optflow-core/src/strain.rs:121-287): NaN-aware quadratic least-squares fit over
+ * win x win windows. Any output pointer may be NULL.
+ */
+int ofc_strain(ofc_engine* eng, const float* ux, const float* uy, size_t w, size_t h, int32_t win,
+               float* dudx, float* dudy, float* dvdx, float* dvdy,
+               float* exx, float* eyy, float* exy, float* gmax, float* vol,
+               char* err, size_t errlen);
+
+/*
+ * track::_finish (python/optflow_ref/track.py:56-108; rust/crates/optflow-core/src/track.rs:224-274,
+ * 330-420): low = conf < conf_min, guard band around large low components and the ROI exterior,
+ * border strip, NaN mask, strain. conf is the f64 confidence rounded to f32; roi nullable.
+ * out->raw_* and out->conf are copies of the inputs.
+ */
+int ofc_finish(ofc_engine* eng, const float* ux, const float* uy, const float* conf, const uint8_t* roi,
+               size_t w, size_t h, const ofc_config* cfg, ofc_pair_out* out, char* err, size_t errlen);
+
+/*
+ * track::track_pair (python/optflow_ref/track.py:115-146; rust/crates/optflow-core/src/track.rs:
+ * 567-623,765): coarse POC -> dense start -> fine stage -> finish, one pair, host buffers.
+ * roi (nullable): w*h bytes, nonzero = inside. init_ux/init_uy (nullable): a dense guess.
+ */
+int ofc_track_pair(ofc_engine* eng, const float* i1, const float* i2, size_t w, size_t h,
+                   const uint8_t* roi, const float* init_ux, const float* init_uy,
+                   const ofc_config* cfg, ofc_pair_out* out, char* err, size_t errlen);
+
+/*
+ * ofc_track_pair on device-resident buffers: every pointer (inputs and the out fields) is device
+ * memory of the engine's device; the work is queued on `stream` (a cudaStream_t, NULL = the
+ * engine's own stream) and the call returns once it is queued, with out->timing left zero.
+ * Inputs must stay untouched until the stream reaches the end of the work.
+ */
+int ofc_track_pair_device(ofc_engine* eng, const float* d_i1, const float* d_i2, size_t w, size_t h,
+                          const uint8_t* d_roi, const float* d_init_ux, const float* d_init_uy,
+                          const ofc_config* cfg, ofc_pair_out* d_out, void* stream,
+                          char* err, size_t errlen);
+
+/* Number of this library's kernels launched by this engine since it was created (the kernels
+ * are all hand-written; no library kernel runs on the path). */
+uint64_t ofc_kernel_launches(const ofc_engine* eng);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPTFLOW_CUDA_H */

@@ -1,0 +1,9 @@
+"""optflow_b200 -- B200 (sm_100a) engine for optflow-soil's dense local-phase flow + DIC pair path.
+
+The host side mirrors the reference's Python API (python/optflow_ref/track.py, phaseflow.py, poc.py,
+strain.py) over the C ABI of include/optflow_cuda.h; every computation runs in the CUDA library.
+"""
+from ._abi import EngineError, load  # noqa: F401
+from .config import Config  # noqa: F401
+from .api import (Engine, Flow, Grid, Result, coarse_flow, displacement_gradient, finish, refine,  # noqa: F401
+                  refine_raw, strain_fields, track_pair)

@@ -1,0 +1,136 @@
+"""ctypes mirror of include/optflow_cuda.h and the loader of the CUDA engine library.
+
+The library is built in-tree (``optflow-soil_b200/lib/liboptflow_cuda.so``, see ``build.py``).
+There is no fallback: if it is missing or fails to load, every call raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(HERE)
+LIB_DIR = os.path.join(PKG_ROOT, "lib")
+LIB_PATH = os.path.join(LIB_DIR, "liboptflow_cuda.so")
+
+OFC_ABI_VERSION = 1
+OFC_MAX_SCALES = 16
+
+c_float_p = ctypes.POINTER(ctypes.c_float)
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_u8_p = ctypes.POINTER(ctypes.c_uint8)
+c_i32_p = ctypes.POINTER(ctypes.c_int32)
+
+
+class OfcConfig(ctypes.Structure):
+    """struct ofc_config (include/optflow_cuda.h)."""
+    _fields_ = [
+        ("grid_step", ctypes.c_int32),
+        ("poc_win", ctypes.c_int32),
+        ("max_disp", ctypes.c_double),
+        ("poc_peak_min", ctypes.c_double),
+        ("median_thresh", ctypes.c_double),
+        ("lam", ctypes.c_double),
+        ("n_scales", ctypes.c_int32),
+        ("scales", ctypes.c_double * OFC_MAX_SCALES),
+        ("n_orient", ctypes.c_int32),
+        ("bandwidth", ctypes.c_double),
+        ("dc_cut", ctypes.c_double),
+        ("sigma_w", ctypes.c_double),
+        ("shape_order", ctypes.c_int32),
+        ("sigma_s", ctypes.c_double),
+        ("outer_iters", ctypes.c_int32),
+        ("inner_iters", ctypes.c_int32),
+        ("conf_min", ctypes.c_double),
+        ("edge_guard", ctypes.c_double),
+        ("edge_guard_min_area", ctypes.c_double),
+        ("phase_tol", ctypes.c_double),
+        ("strain_win", ctypes.c_int32),
+        ("prewarp_freeze_at", ctypes.c_int32),
+    ]
+
+
+class OfcPairOut(ctypes.Structure):
+    """struct ofc_pair_out (include/optflow_cuda.h)."""
+    _fields_ = [
+        ("ux", c_float_p),
+        ("uy", c_float_p),
+        ("conf", c_float_p),
+        ("exx", c_float_p),
+        ("eyy", c_float_p),
+        ("exy", c_float_p),
+        ("gmax", c_float_p),
+        ("vol", c_float_p),
+        ("valid", c_u8_p),
+        ("raw_ux", c_float_p),
+        ("raw_uy", c_float_p),
+        ("timing", ctypes.c_double * 3),
+    ]
+
+
+PAIR_FIELDS = ("ux", "uy", "conf", "exx", "eyy", "exy", "gmax", "vol", "valid", "raw_ux", "raw_uy")
+
+# every symbol the header declares, with its ctypes signature (restype, argtypes)
+_P = ctypes.c_void_p
+_S = ctypes.c_size_t
+_E = ctypes.c_char_p
+SIGNATURES = {
+    "ofc_abi_version": (ctypes.c_int, []),
+    "ofc_config_default": (None, [ctypes.POINTER(OfcConfig)]),
+    "ofc_config_validate": (ctypes.c_int, [ctypes.POINTER(OfcConfig), _E, _S]),
+    "ofc_edge_guard_px": (ctypes.c_double, [ctypes.POINTER(OfcConfig)]),
+    "ofc_auto_edge_guard_px": (ctypes.c_double, [ctypes.POINTER(OfcConfig)]),
+    "ofc_edge_guard_min_area_px": (ctypes.c_double, [ctypes.POINTER(OfcConfig)]),
+    "ofc_create": (_P, [ctypes.c_int, ctypes.c_int, _E, _S]),
+    "ofc_destroy": (None, [_P]),
+    "ofc_lanes": (ctypes.c_int, [_P]),
+    "ofc_check_window": (ctypes.c_int, [_P, _S, _S, ctypes.POINTER(OfcConfig), _E, _S]),
+    "ofc_release_caches": (None, [_P]),
+    "ofc_refine_raw": (ctypes.c_int, [_P, c_float_p, _S, _S, c_float_p, _S, _S, ctypes.c_int64, ctypes.c_int64,
+                                      c_float_p, c_float_p, ctypes.POINTER(OfcConfig),
+                                      c_double_p, c_double_p, c_double_p, c_double_p, _E, _S]),
+    "ofc_refine": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, c_float_p, c_float_p, ctypes.POINTER(OfcConfig),
+                                  c_float_p, c_float_p, c_float_p, c_float_p, c_u8_p, _E, _S]),
+    "ofc_grid_shape": (ctypes.c_int, [_S, _S, ctypes.POINTER(OfcConfig), ctypes.POINTER(_S), ctypes.POINTER(_S)]),
+    "ofc_coarse_flow": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, c_float_p, c_float_p,
+                                       ctypes.POINTER(OfcConfig), c_i32_p, c_i32_p, c_float_p, c_float_p, c_float_p,
+                                       _E, _S]),
+    "ofc_strain": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, ctypes.c_int32] + [c_float_p] * 9 + [_E, _S]),
+    "ofc_finish": (ctypes.c_int, [_P, c_float_p, c_float_p, c_float_p, c_u8_p, _S, _S, ctypes.POINTER(OfcConfig),
+                                  ctypes.POINTER(OfcPairOut), _E, _S]),
+    "ofc_track_pair": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, c_u8_p, c_float_p, c_float_p,
+                                      ctypes.POINTER(OfcConfig), ctypes.POINTER(OfcPairOut), _E, _S]),
+    "ofc_track_pair_device": (ctypes.c_int, [_P, _P, _P, _S, _S, _P, _P, _P, ctypes.POINTER(OfcConfig),
+                                             ctypes.POINTER(OfcPairOut), _P, _E, _S]),
+    "ofc_kernel_launches": (ctypes.c_uint64, [_P]),
+}
+
+
+class EngineError(RuntimeError):
+    """An error reported by the CUDA engine (the reference's EngineError, engine.rs:21-24)."""
+
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+_LIB = None
+
+
+def load(path=None):
+    """Load the engine library once and bind every declared symbol. Raises if it is missing."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = path or os.environ.get("OPTFLOW_CUDA_LIB", LIB_PATH)
+    if not os.path.exists(p):
+        raise EngineError(2, f"CUDA engine library not built: {p} (run __graft_entry__.build() or "
+                             f"python optflow-soil_b200/build.py)")
+    lib = ctypes.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.ofc_abi_version() != OFC_ABI_VERSION:
+        raise EngineError(2, f"ABI version mismatch: library {lib.ofc_abi_version()}, expected {OFC_ABI_VERSION}")
+    if path is None:
+        _LIB = lib
+    return lib

@@ -1,0 +1,264 @@
+"""The reference's Python API (python/optflow_ref) over the CUDA engine's C ABI.
+
+``track_pair``, ``refine``, ``coarse_flow``, ``displacement_gradient``, ``strain_fields`` and the
+``_finish`` step keep the reference's names, argument meaning and error behaviour (ValueError for bad
+input, as the reference raises), so tests written against the reference read the same here. Every
+call runs on the GPU through ``liboptflow_cuda.so``; there is no CPU path.
+"""
+import ctypes
+import threading
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import EngineError, OfcPairOut, c_double_p, c_float_p, c_i32_p, c_u8_p
+from .config import Config
+
+_ERRLEN = 1024
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None and a.shape != shape:
+        raise ValueError(f"expected shape {shape}, got {a.shape}")
+    return a
+
+
+def _ptr(a, typ):
+    return None if a is None else a.ctypes.data_as(typ)
+
+
+class Engine:
+    """An engine on one CUDA device (GpuEngine of rust/crates/optflow-gpu/src/engine.rs:94-103).
+
+    Holds the device context, plans and pooled buffers between calls until ``release_caches``.
+    """
+
+    def __init__(self, device=0, lanes=1):
+        self.lib = _abi.load()
+        err = ctypes.create_string_buffer(_ERRLEN)
+        h = self.lib.ofc_create(int(device), int(lanes), err, _ERRLEN)
+        if not h:
+            raise EngineError(_abi.OFC_ERR_DEVICE if hasattr(_abi, "OFC_ERR_DEVICE") else 2,
+                              err.value.decode() or "ofc_create failed")
+        self.handle = ctypes.c_void_p(h)
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.ofc_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _call(self, name, *args):
+        err = ctypes.create_string_buffer(_ERRLEN)
+        st = getattr(self.lib, name)(self.handle, *args, err, _ERRLEN)
+        if st != 0:
+            msg = err.value.decode()
+            if st == 1:
+                raise ValueError(msg)
+            raise EngineError(st, msg)
+
+    @property
+    def lanes(self):
+        return self.lib.ofc_lanes(self.handle)
+
+    def kernel_launches(self):
+        return int(self.lib.ofc_kernel_launches(self.handle))
+
+    def check_window(self, w, h, cfg=None):
+        c = (cfg or Config()).to_ofc()
+        self._call("ofc_check_window", ctypes.c_size_t(w), ctypes.c_size_t(h), ctypes.byref(c))
+
+    def release_caches(self):
+        self.lib.ofc_release_caches(self.handle)
+
+
+_default = {}
+_lock = threading.Lock()
+
+
+def default_engine(device=0):
+    with _lock:
+        if device not in _default:
+            _default[device] = Engine(device)
+        return _default[device]
+
+
+@dataclass
+class Flow:
+    """phaseflow.Flow (python/optflow_ref/phaseflow.py:53-60) without the crack bookkeeping."""
+    ux: np.ndarray
+    uy: np.ndarray
+    conf: np.ndarray
+    resid: np.ndarray
+    low: np.ndarray = None
+
+
+@dataclass
+class Grid:
+    """poc.Grid (python/optflow_ref/poc.py:9-15)."""
+    xs: np.ndarray
+    ys: np.ndarray
+    ux: np.ndarray
+    uy: np.ndarray
+    peak: np.ndarray
+
+
+@dataclass
+class Result:
+    """track.Result (python/optflow_ref/track.py:15-31) of one pair."""
+    ux: np.ndarray
+    uy: np.ndarray
+    conf: np.ndarray
+    strain: dict
+    raw_ux: np.ndarray
+    raw_uy: np.ndarray
+    timing: dict = field(default_factory=dict)
+    valid: np.ndarray = None
+
+
+def _prep_cfg(cfg):
+    cfg = cfg or Config()
+    cfg.validate()
+    return cfg, cfg.to_ofc()
+
+
+def refine_raw(I1, I2, ux, uy, cfg=None, shift=(0, 0), engine=None):
+    """FineEngine::refine_raw (rust/crates/optflow-core/src/engine.rs:32-40): dict of f64 planes
+    ux, uy, energy, resid of the window I1 (I2 any part of the second image placed at `shift`)."""
+    eng = engine or default_engine()
+    cfg, c = _prep_cfg(cfg)
+    a = _f32(I1)
+    h, w = a.shape
+    b = _f32(I2)
+    u, v = _f32(ux, (h, w)), _f32(uy, (h, w))
+    out = [np.empty((h, w), np.float64) for _ in range(4)]
+    eng._call("ofc_refine_raw", _ptr(a, c_float_p), w, h, _ptr(b, c_float_p), b.shape[1], b.shape[0],
+              ctypes.c_int64(shift[0]), ctypes.c_int64(shift[1]), _ptr(u, c_float_p), _ptr(v, c_float_p),
+              ctypes.byref(c), *[_ptr(o, c_double_p) for o in out])
+    return dict(zip(("ux", "uy", "energy", "resid"), out))
+
+
+def refine(I1, I2, ux, uy, cfg=None, engine=None) -> Flow:
+    """phaseflow.refine (python/optflow_ref/phaseflow.py:427-511)."""
+    eng = engine or default_engine()
+    cfg, c = _prep_cfg(cfg)
+    a = _f32(I1)
+    h, w = a.shape
+    b = _f32(I2, (h, w))
+    u, v = _f32(ux, (h, w)), _f32(uy, (h, w))
+    out = [np.empty((h, w), np.float32) for _ in range(4)]
+    low = np.empty((h, w), np.uint8)
+    eng._call("ofc_refine", _ptr(a, c_float_p), _ptr(b, c_float_p), w, h, _ptr(u, c_float_p), _ptr(v, c_float_p),
+              ctypes.byref(c), *[_ptr(o, c_float_p) for o in out], _ptr(low, c_u8_p))
+    return Flow(out[0], out[1], out[2], out[3], low.astype(bool))
+
+
+def coarse_flow(I1, I2, cfg=None, init_dense=None, engine=None) -> Grid:
+    """poc.coarse_flow (python/optflow_ref/poc.py:216-239)."""
+    eng = engine or default_engine()
+    cfg, c = _prep_cfg(cfg)
+    a = _f32(I1)
+    h, w = a.shape
+    b = _f32(I2, (h, w))
+    nx, ny = ctypes.c_size_t(), ctypes.c_size_t()
+    if eng.lib.ofc_grid_shape(w, h, ctypes.byref(c), ctypes.byref(nx), ctypes.byref(ny)) != 0:
+        raise ValueError(f"image {w}x{h} too small for poc_win {cfg.poc_win}")
+    nx, ny = nx.value, ny.value
+    xs, ys = np.empty(nx, np.int32), np.empty(ny, np.int32)
+    gu, gv, gp = (np.empty((ny, nx), np.float32) for _ in range(3))
+    iu = iv = None
+    if init_dense is not None:
+        iu, iv = _f32(init_dense[0], (h, w)), _f32(init_dense[1], (h, w))
+    eng._call("ofc_coarse_flow", _ptr(a, c_float_p), _ptr(b, c_float_p), w, h, _ptr(iu, c_float_p),
+              _ptr(iv, c_float_p), ctypes.byref(c), _ptr(xs, c_i32_p), _ptr(ys, c_i32_p), _ptr(gu, c_float_p),
+              _ptr(gv, c_float_p), _ptr(gp, c_float_p))
+    return Grid(xs, ys, gu, gv, gp)
+
+
+def displacement_gradient(ux, uy, win, engine=None):
+    """strain.displacement_gradient (python/optflow_ref/strain.py:61-97): (dudx, dudy, dvdx, dvdy)."""
+    return _strain(ux, uy, win, engine)[:4]
+
+
+def _strain(ux, uy, win, engine=None):
+    eng = engine or default_engine()
+    u = _f32(ux)
+    h, w = u.shape
+    v = _f32(uy, (h, w))
+    out = [np.empty((h, w), np.float32) for _ in range(9)]
+    eng._call("ofc_strain", _ptr(u, c_float_p), _ptr(v, c_float_p), w, h, int(win),
+              *[_ptr(o, c_float_p) for o in out])
+    return out
+
+
+def strain_fields(dudx, dudy, dvdx, dvdy):
+    """strain.strain_fields (python/optflow_ref/strain.py:100-112): host arithmetic on four maps."""
+    exx = dudx + 0.5 * (dudx**2 + dvdx**2)
+    eyy = dvdy + 0.5 * (dudy**2 + dvdy**2)
+    exy = 0.5 * (dudy + dvdx) + 0.5 * (dudx * dudy + dvdx * dvdy)
+    return {"Exx": exx, "Eyy": eyy, "Exy": exy, "exx": dudx, "eyy": dvdy, "exy": 0.5 * (dudy + dvdx),
+            "gmax": 2.0 * np.sqrt(((exx - eyy) / 2) ** 2 + exy**2),
+            "vol": (1 + dudx) * (1 + dvdy) - dudy * dvdx - 1.0}
+
+
+def _pair_out(h, w):
+    arrs = {k: np.empty((h, w), np.uint8 if k == "valid" else np.float32) for k in _abi.PAIR_FIELDS}
+    o = OfcPairOut()
+    for k, a in arrs.items():
+        setattr(o, k, _ptr(a, c_u8_p if k == "valid" else c_float_p))
+    return o, arrs
+
+
+def _result(o, arrs):
+    st = {"Exx": arrs["exx"], "Eyy": arrs["eyy"], "Exy": arrs["exy"], "gmax": arrs["gmax"], "vol": arrs["vol"]}
+    timing = dict(coarse=o.timing[0], fine=o.timing[1], strain=o.timing[2])
+    return Result(arrs["ux"], arrs["uy"], arrs["conf"], st, arrs["raw_ux"], arrs["raw_uy"], timing,
+                  arrs["valid"].astype(bool))
+
+
+def finish(ux, uy, conf, cfg=None, mask=None, engine=None) -> Result:
+    """track._finish (python/optflow_ref/track.py:56-108) without the crack options."""
+    eng = engine or default_engine()
+    cfg, c = _prep_cfg(cfg)
+    u = _f32(ux)
+    h, w = u.shape
+    v, cf = _f32(uy, (h, w)), _f32(conf, (h, w))
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    o, arrs = _pair_out(h, w)
+    eng._call("ofc_finish", _ptr(u, c_float_p), _ptr(v, c_float_p), _ptr(cf, c_float_p), _ptr(m, c_u8_p), w, h,
+              ctypes.byref(c), ctypes.byref(o))
+    return _result(o, arrs)
+
+
+def track_pair(I1, I2, cfg=None, mask=None, init=None, engine=None) -> Result:
+    """track.track_pair (python/optflow_ref/track.py:115-146): the displacement of I1's pixels into I2."""
+    I1 = np.asarray(I1)
+    I2 = np.asarray(I2)
+    if I1.shape != I2.shape:
+        raise ValueError(f"image sizes differ: {I1.shape} vs {I2.shape}")
+    if mask is not None and np.shape(mask) != I1.shape:
+        raise ValueError(f"ROI mask shape {np.shape(mask)} differs from the image shape {I1.shape}")
+    if mask is not None and not np.any(mask):
+        raise ValueError("ROI mask is empty")
+    cfg, c = _prep_cfg(cfg)
+    if min(I1.shape) < cfg.poc_win:
+        raise ValueError(f"image smaller than poc_win ({cfg.poc_win}): {I1.shape}")
+    eng = engine or default_engine()
+    a, b = _f32(I1), _f32(I2)
+    h, w = a.shape
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    iu = iv = None
+    if init is not None:
+        iu, iv = _f32(init[0], (h, w)), _f32(init[1], (h, w))
+    o, arrs = _pair_out(h, w)
+    eng._call("ofc_track_pair", _ptr(a, c_float_p), _ptr(b, c_float_p), w, h, _ptr(m, c_u8_p),
+              _ptr(iu, c_float_p), _ptr(iv, c_float_p), ctypes.byref(c), ctypes.byref(o))
+    return _result(o, arrs)

@@ -1,0 +1,224 @@
+"""numpy front end of the CPU oracle (oracle.cpp), for the tests and the benchmark's CPU baseline.
+
+TEST INFRASTRUCTURE: the checker of the CUDA engine, never part of it. Function names and
+conventions follow the reference's Python specification (python/optflow_ref/*.py): images are
+float64 arrays indexed [row, col], displacement fields (ux, uy) in pixels.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboptflow_oracle.so")
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+    return _lib
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _cfg(cfg):
+    from optflow_b200.config import Config
+    c = (cfg or Config()).to_ofc()
+    return ctypes.byref(c), c
+
+
+def threads(n=0):
+    return lib().oro_threads(int(n))
+
+
+def fft2(a, inverse=False):
+    z = np.ascontiguousarray(a, dtype=np.complex128).copy()
+    h, w = z.shape
+    lib().oro_fft2(_p(z), w, h, int(inverse))
+    return z
+
+
+def bspline_coeffs(img):
+    a = _d(img)
+    out = np.empty_like(a)
+    lib().oro_bspline_coeffs(_p(a), _p(out), a.shape[1], a.shape[0])
+    return out
+
+
+def sample(coeffs, x, y):
+    c = _d(coeffs)
+    x, y = np.broadcast_arrays(_d(x), _d(y))
+    x, y = _d(x), _d(y)
+    out = np.empty(x.shape)
+    lib().oro_sample(_p(c), c.shape[1], c.shape[0], _p(x), _p(y), ctypes.c_size_t(x.size), _p(out))
+    return out
+
+
+def gauss_blur(a, sigma):
+    a = _d(a)
+    out = np.empty_like(a)
+    lib().oro_gauss_blur(_p(a), _p(out), a.shape[1], a.shape[0], ctypes.c_double(sigma))
+    return out
+
+
+def edt(inp, return_indices=False):
+    """scipy.ndimage.distance_transform_edt(inp[, return_indices=True])."""
+    b = np.ascontiguousarray(inp != 0, dtype=np.uint8)
+    h, w = b.shape
+    dist = np.empty((h, w))
+    idx = np.empty((h, w), np.int64) if return_indices else None
+    lib().oro_edt(_p(b), w, h, _p(dist), _p(idx))
+    if not return_indices:
+        return dist
+    return dist, (idx // w, idx % w)
+
+
+def large_components(b, min_area):
+    a = np.ascontiguousarray(b, dtype=np.uint8)
+    out = np.empty_like(a)
+    lib().oro_large_components(_p(a), a.shape[1], a.shape[0], ctypes.c_double(min_area), _p(out))
+    return out.astype(bool)
+
+
+def reference_phase(I1, cfg=None):
+    """phaseflow.reference_phase: list of (r, gx, gy, amp) per filter."""
+    a = _d(I1)
+    h, w = a.shape
+    pc, c = _cfg(cfg)
+    F = c.n_orient * c.n_scales
+    planes = [np.empty((F, h, w)) for _ in range(5)]
+    lib().oro_reference_phase(_p(a), w, h, pc, *[_p(p) for p in planes])
+    re, im, gx, gy, amp = planes
+    return [(re[k] + 1j * im[k], gx[k], gy[k], amp[k]) for k in range(F)]
+
+
+def local_solve(sums, ux, uy, sigma, order):
+    """phaseflow.local_solve on the seven per-pixel sums: (ux, uy, energy, resid, slope)."""
+    s = _d(np.stack(sums))
+    ux, uy = _d(ux), _d(uy)
+    h, w = ux.shape
+    out = [np.empty((h, w)) for _ in range(4)]
+    slope = np.empty((h, w, 4))
+    lib().oro_local_solve(_p(s), _p(ux), _p(uy), w, h, ctypes.c_double(sigma), int(order),
+                          *[_p(o) for o in out], _p(slope))
+    return (*out, slope)
+
+
+def refine(I1, I2, ux, uy, cfg=None):
+    """phaseflow.refine: dict(ux, uy, conf, resid, energy)."""
+    a, b, ux, uy = _d(I1), _d(I2), _d(ux), _d(uy)
+    h, w = a.shape
+    pc, _ = _cfg(cfg)
+    out = [np.empty((h, w)) for _ in range(5)]
+    lib().oro_refine(_p(a), _p(b), w, h, _p(ux), _p(uy), pc, *[_p(o) for o in out])
+    return dict(zip(("ux", "uy", "conf", "resid", "energy"), out))
+
+
+def poc_shift(a, b):
+    a, b = _d(a), _d(b)
+    out = np.empty(3)
+    lib().oro_poc_shift(_p(a), _p(b), a.shape[1], a.shape[0], _p(out))
+    return float(out[0]), float(out[1]), float(out[2])
+
+
+def n_levels(max_disp, win, shape):
+    return lib().oro_n_levels(ctypes.c_double(max_disp), int(win), int(shape[0]), int(shape[1]))
+
+
+def level_window(shape, win):
+    wy, wx = ctypes.c_int(), ctypes.c_int()
+    ok = lib().oro_level_window(int(shape[0]), int(shape[1]), int(win), ctypes.byref(wy), ctypes.byref(wx))
+    return (wy.value, wx.value) if ok else None
+
+
+def poc_grid(I1, I2, xs, ys, win, init=None):
+    """poc.poc_grid (no clean): (ux, uy, peak) of shape (ny, nx)."""
+    a, b = _d(I1), _d(I2)
+    h, w = a.shape
+    wy, wx = (win, win) if np.isscalar(win) else win
+    xs = np.ascontiguousarray(xs, dtype=np.int32)
+    ys = np.ascontiguousarray(ys, dtype=np.int32)
+    ny, nx = len(ys), len(xs)
+    out = [np.empty((ny, nx)) for _ in range(3)]
+    iux = iuy = None
+    if init is not None:
+        iux, iuy = _d(init[0]), _d(init[1])
+    lib().oro_poc_grid(_p(a), _p(b), w, h, _p(xs), nx, _p(ys), ny, int(wy), int(wx), _p(iux), _p(iuy),
+                       *[_p(o) for o in out])
+    return out
+
+
+def grid_shape(shape, cfg=None):
+    pc, _ = _cfg(cfg)
+    nx, ny = ctypes.c_int(), ctypes.c_int()
+    lib().oro_grid_shape(int(shape[1]), int(shape[0]), pc, ctypes.byref(nx), ctypes.byref(ny))
+    return ny.value, nx.value
+
+
+def coarse_flow(I1, I2, cfg=None, init_dense=None):
+    """poc.coarse_flow: dict(xs, ys, ux, uy, peak)."""
+    a, b = _d(I1), _d(I2)
+    h, w = a.shape
+    ny, nx = grid_shape(a.shape, cfg)
+    pc, _ = _cfg(cfg)
+    xs, ys = np.empty(nx, np.int32), np.empty(ny, np.int32)
+    out = [np.empty((ny, nx)) for _ in range(3)]
+    iux = iuy = None
+    if init_dense is not None:
+        iux, iuy = _d(init_dense[0]), _d(init_dense[1])
+    lib().oro_coarse_flow(_p(a), _p(b), w, h, _p(iux), _p(iuy), pc, _p(xs), _p(ys), *[_p(o) for o in out])
+    return dict(xs=xs, ys=ys, ux=out[0], uy=out[1], peak=out[2])
+
+
+def displacement_gradient(ux, uy, win):
+    ux, uy = _d(ux), _d(uy)
+    h, w = ux.shape
+    out = [np.empty((h, w)) for _ in range(4)]
+    lib().oro_displacement_gradient(_p(ux), _p(uy), w, h, int(win), *[_p(o) for o in out])
+    return tuple(out)
+
+
+def finish(ux, uy, conf, cfg=None, mask=None):
+    """track._finish: (mx, my, strain dict)."""
+    ux, uy, conf = _d(ux), _d(uy), _d(conf)
+    h, w = ux.shape
+    pc, _ = _cfg(cfg)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    out = [np.empty((h, w)) for _ in range(7)]
+    lib().oro_finish(_p(ux), _p(uy), _p(conf), _p(m), w, h, pc, *[_p(o) for o in out])
+    return out[0], out[1], dict(zip(("Exx", "Eyy", "Exy", "gmax", "vol"), out[2:]))
+
+
+def track_pair(I1, I2, cfg=None, mask=None, init=None):
+    """track.track_pair: dict(ux, uy, conf, Exx, Eyy, Exy, gmax, vol, raw_ux, raw_uy, valid, timing)."""
+    a, b = _d(I1), _d(I2)
+    h, w = a.shape
+    pc, _ = _cfg(cfg)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    iux = iuy = None
+    if init is not None:
+        iux, iuy = _d(init[0]), _d(init[1])
+    out = np.empty((10, h, w))
+    timing = np.zeros(3)
+    lib().oro_track_pair(_p(a), _p(b), w, h, _p(m), _p(iux), _p(iuy), pc, _p(out), _p(timing))
+    names = ("ux", "uy", "conf", "Exx", "Eyy", "Exy", "gmax", "vol", "raw_ux", "raw_uy")
+    r = {k: out[i] for i, k in enumerate(names)}
+    r["valid"] = np.isfinite(r["ux"])
+    r["timing"] = dict(coarse=timing[0], fine=timing[1], strain=timing[2])
+    return r
