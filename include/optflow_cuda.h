@@ -19,6 +19,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define OFC_API __attribute__((visibility("default")))
+#else
+#define OFC_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -88,33 +94,33 @@ typedef struct ofc_pair_out {
 typedef struct ofc_engine ofc_engine;
 
 /* ABI version of the loaded library (OFC_ABI_VERSION). */
-int ofc_abi_version(void);
+OFC_API int ofc_abi_version(void);
 
 /* Config::default() (config.py:24-120). */
-void ofc_config_default(ofc_config* cfg);
+OFC_API void ofc_config_default(ofc_config* cfg);
 
 /* Config::validate() for the keys above (config.py:166-245); message text as the reference's. */
-int ofc_config_validate(const ofc_config* cfg, char* err, size_t errlen);
+OFC_API int ofc_config_validate(const ofc_config* cfg, char* err, size_t errlen);
 
 /* The resolved guard distances of the config (Config::edge_guard_px, auto_edge_guard_px,
  * edge_guard_min_area_px; config.py:257-272). */
-double ofc_edge_guard_px(const ofc_config* cfg);
-double ofc_auto_edge_guard_px(const ofc_config* cfg);
-double ofc_edge_guard_min_area_px(const ofc_config* cfg);
+OFC_API double ofc_edge_guard_px(const ofc_config* cfg);
+OFC_API double ofc_auto_edge_guard_px(const ofc_config* cfg);
+OFC_API double ofc_edge_guard_min_area_px(const ofc_config* cfg);
 
 /* GpuEngine::new / with_lanes (rust/crates/optflow-gpu/src/engine.rs:94,103): an engine on CUDA
  * device `device` that accepts up to `lanes` (1 or 2) concurrent calls. NULL on error. */
-ofc_engine* ofc_create(int device, int lanes, char* err, size_t errlen);
-void ofc_destroy(ofc_engine* eng);
+OFC_API ofc_engine* ofc_create(int device, int lanes, char* err, size_t errlen);
+OFC_API void ofc_destroy(ofc_engine* eng);
 
 /* FineEngine::lanes (engine.rs:63-70). */
-int ofc_lanes(const ofc_engine* eng);
+OFC_API int ofc_lanes(const ofc_engine* eng);
 
 /* FineEngine::check_window (engine.rs:42-46): refuse a window the engine cannot hold. */
-int ofc_check_window(ofc_engine* eng, size_t w, size_t h, const ofc_config* cfg, char* err, size_t errlen);
+OFC_API int ofc_check_window(ofc_engine* eng, size_t w, size_t h, const ofc_config* cfg, char* err, size_t errlen);
 
 /* FineEngine::release_caches (engine.rs:114-117): free plans and pooled device buffers. */
-void ofc_release_caches(ofc_engine* eng);
+OFC_API void ofc_release_caches(ofc_engine* eng);
 
 /*
  * FineEngine::refine_raw (rust/crates/optflow-core/src/engine.rs:32-40; contract of
@@ -123,7 +129,7 @@ void ofc_release_caches(ofc_engine* eng);
  * before it is displaced (positions outside i2 clamp to its border). Outputs: RawFlow planes
  * (phaseflow.rs:1408-1414), w*h doubles each.
  */
-int ofc_refine_raw(ofc_engine* eng, const float* i1, size_t w, size_t h,
+OFC_API int ofc_refine_raw(ofc_engine* eng, const float* i1, size_t w, size_t h,
                    const float* i2, size_t w2, size_t h2, int64_t shift_x, int64_t shift_y,
                    const float* ux, const float* uy, const ofc_config* cfg,
                    double* out_ux, double* out_uy, double* out_energy, double* out_resid,
@@ -134,20 +140,20 @@ int ofc_refine_raw(ofc_engine* eng, const float* i1, size_t w, size_t h,
  * rust/crates/optflow-core/src/phaseflow.rs:1684-1757): refine_raw on the whole image plus the
  * confidence with its border rule. out_low (nullable) = the f64 confidence < conf_min.
  */
-int ofc_refine(ofc_engine* eng, const float* i1, const float* i2, size_t w, size_t h,
+OFC_API int ofc_refine(ofc_engine* eng, const float* i1, const float* i2, size_t w, size_t h,
                const float* ux, const float* uy, const ofc_config* cfg,
                float* out_ux, float* out_uy, float* out_conf, float* out_resid, uint8_t* out_low,
                char* err, size_t errlen);
 
 /* Grid of the coarse stage for a w x h image (poc.grid_points, python/optflow_ref/poc.py:61-64). */
-int ofc_grid_shape(size_t w, size_t h, const ofc_config* cfg, size_t* nx, size_t* ny);
+OFC_API int ofc_grid_shape(size_t w, size_t h, const ofc_config* cfg, size_t* nx, size_t* ny);
 
 /*
  * poc::coarse_flow (python/optflow_ref/poc.py:216-239; rust/crates/optflow-core/src/poc.rs:694-767):
  * grid displacement at full resolution. init_ux/init_uy (nullable, w x h): a dense guess.
  * Outputs: xs (nx), ys (ny), gux/guy/gpeak (ny x nx).
  */
-int ofc_coarse_flow(ofc_engine* eng, const float* a, const float* b, size_t w, size_t h,
+OFC_API int ofc_coarse_flow(ofc_engine* eng, const float* a, const float* b, size_t w, size_t h,
                     const float* init_ux, const float* init_uy, const ofc_config* cfg,
                     int32_t* xs, int32_t* ys, float* gux, float* guy, float* gpeak,
                     char* err, size_t errlen);
@@ -157,7 +163,7 @@ int ofc_coarse_flow(ofc_engine* eng, const float* a, const float* b, size_t w, s
  * rust/crates/optflow-core/src/strain.rs:121-287): NaN-aware quadratic least-squares fit over
  * win x win windows. Any output pointer may be NULL.
  */
-int ofc_strain(ofc_engine* eng, const float* ux, const float* uy, size_t w, size_t h, int32_t win,
+OFC_API int ofc_strain(ofc_engine* eng, const float* ux, const float* uy, size_t w, size_t h, int32_t win,
                float* dudx, float* dudy, float* dvdx, float* dvdy,
                float* exx, float* eyy, float* exy, float* gmax, float* vol,
                char* err, size_t errlen);
@@ -168,7 +174,7 @@ int ofc_strain(ofc_engine* eng, const float* ux, const float* uy, size_t w, size
  * border strip, NaN mask, strain. conf is the f64 confidence rounded to f32; roi nullable.
  * out->raw_* and out->conf are copies of the inputs.
  */
-int ofc_finish(ofc_engine* eng, const float* ux, const float* uy, const float* conf, const uint8_t* roi,
+OFC_API int ofc_finish(ofc_engine* eng, const float* ux, const float* uy, const float* conf, const uint8_t* roi,
                size_t w, size_t h, const ofc_config* cfg, ofc_pair_out* out, char* err, size_t errlen);
 
 /*
@@ -176,7 +182,7 @@ int ofc_finish(ofc_engine* eng, const float* ux, const float* uy, const float* c
  * 567-623,765): coarse POC -> dense start -> fine stage -> finish, one pair, host buffers.
  * roi (nullable): w*h bytes, nonzero = inside. init_ux/init_uy (nullable): a dense guess.
  */
-int ofc_track_pair(ofc_engine* eng, const float* i1, const float* i2, size_t w, size_t h,
+OFC_API int ofc_track_pair(ofc_engine* eng, const float* i1, const float* i2, size_t w, size_t h,
                    const uint8_t* roi, const float* init_ux, const float* init_uy,
                    const ofc_config* cfg, ofc_pair_out* out, char* err, size_t errlen);
 
@@ -186,14 +192,14 @@ int ofc_track_pair(ofc_engine* eng, const float* i1, const float* i2, size_t w, 
  * engine's own stream) and the call returns once it is queued, with out->timing left zero.
  * Inputs must stay untouched until the stream reaches the end of the work.
  */
-int ofc_track_pair_device(ofc_engine* eng, const float* d_i1, const float* d_i2, size_t w, size_t h,
+OFC_API int ofc_track_pair_device(ofc_engine* eng, const float* d_i1, const float* d_i2, size_t w, size_t h,
                           const uint8_t* d_roi, const float* d_init_ux, const float* d_init_uy,
                           const ofc_config* cfg, ofc_pair_out* d_out, void* stream,
                           char* err, size_t errlen);
 
 /* Number of this library's kernels launched by this engine since it was created (the kernels
  * are all hand-written; no library kernel runs on the path). */
-uint64_t ofc_kernel_launches(const ofc_engine* eng);
+OFC_API uint64_t ofc_kernel_launches(const ofc_engine* eng);
 
 #ifdef __cplusplus
 }

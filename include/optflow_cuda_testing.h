@@ -1,0 +1,60 @@
+/*
+ * optflow_cuda_testing.h -- entry points into single stages of the CUDA engine, for the parity tests that
+ * pin each kernel against the reference's intermediate arrays. Same conventions as optflow_cuda.h (host
+ * buffers, int status, error text). None of these has a counterpart in the reference's engine interface;
+ * each cites the reference function whose output it reproduces.
+ */
+#ifndef OPTFLOW_CUDA_TESTING_H
+#define OPTFLOW_CUDA_TESTING_H
+
+#include "optflow_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* `lines` complex lines of length L (interleaved re, im float32), transformed in place: numpy fft
+ * (forward) or the unscaled inverse sum (inverse != 0), i.e. L * numpy ifft. */
+OFC_API int ofc_test_fft_lines(ofc_engine* eng, float* data, size_t lines, size_t L, int inverse, char* err,
+                               size_t errlen);
+
+/* phaseflow.reference_phase (python/optflow_ref/phaseflow.py:100-111): per filter k (F = n_scales *
+ * n_orient planes of w*h floats each) r.re, r.im, gx, gy, amp. */
+OFC_API int ofc_test_reference_phase(ofc_engine* eng, const float* i1, size_t w, size_t h, const ofc_config* cfg,
+                                     float* r_re, float* r_im, float* gx, float* gy, float* amp, char* err,
+                                     size_t errlen);
+
+/* bspline_coeffs(ifft2(fft2(pad(img)) * G_k)) of phaseflow.py:455-456 for every filter k: F planes of
+ * (h + 64) x (w + 64) complex values (interleaved float32). */
+OFC_API int ofc_test_responses(ofc_engine* eng, const float* img, size_t w, size_t h, const ofc_config* cfg,
+                               float* resp, char* err, size_t errlen);
+
+/* local_solve (phaseflow.py:177-188) on given per-pixel sums (7 planes of w*h doubles: gxx gxy gyy gxc
+ * gyc gcc gw): ux, uy, energy, resid (doubles), slope (4 planes). */
+OFC_API int ofc_test_local_solve(ofc_engine* eng, const double* sums, const double* ux, const double* uy, size_t w,
+                                 size_t h, const ofc_config* cfg, double* oux, double* ouy, double* energy,
+                                 double* resid, double* slope, char* err, size_t errlen);
+
+/* np.median of n doubles. */
+OFC_API int ofc_test_median(ofc_engine* eng, const double* v, size_t n, double* median, char* err, size_t errlen);
+
+/* track._large_components (python/optflow_ref/track.py:45-53) of a w x h mask. */
+OFC_API int ofc_test_large_components(ofc_engine* eng, const uint8_t* b, size_t w, size_t h, double min_area,
+                                      uint8_t* out, char* err, size_t errlen);
+
+/* The trusted pre-warp fill of phaseflow.prewarp (phaseflow.py:344-354) before the blur: ux, uy (doubles),
+ * slope (4 planes), low mask -> filled ux, uy. */
+OFC_API int ofc_test_prewarp_fill(ofc_engine* eng, const uint8_t* low, const double* ux, const double* uy,
+                                  const double* slope, size_t w, size_t h, double radius, double* oux, double* ouy,
+                                  char* err, size_t errlen);
+
+/* The seven per-pixel sums (gxx gxy gyy gxc gyc gcc gw, 7 planes of w*h doubles) of refine's first inner
+ * iteration from the start field (ux, uy): pre-warp = Gaussian blur of u, warp of i2, responses, accumulate
+ * (python/optflow_ref/phaseflow.py:451-483). */
+OFC_API int ofc_test_first_sums(ofc_engine* eng, const float* i1, const float* i2, size_t w, size_t h, const double* ux,
+                                const double* uy, const ofc_config* cfg, double* sums, char* err, size_t errlen);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPTFLOW_CUDA_TESTING_H */

@@ -1,0 +1,123 @@
+// common.cuh -- shared device helpers of the optflow B200 engine (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/optflow_cuda.h"
+
+namespace ofc {
+
+constexpr double PI = 3.14159265358979323846;
+constexpr int PAD = 32;                 // reflect padding of the Gabor responses (phaseflow.py:47)
+constexpr double APERTURE_TOL = 1e-3;   // phaseflow.py:50
+constexpr int HORIZON = 21;             // ceil(log(1e-12) / log|sqrt(3) - 2|) (interp.py:10)
+constexpr int IIR_WARM = 28;            // samples of warm-up of a segmented recursive filter: z^29 < 3e-17
+
+// An error that leaves the call with a status and a message (EngineError of the reference).
+struct Error : std::runtime_error {
+  int status;
+  Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define OFC_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      throw ::ofc::Error(OFC_ERR_DEVICE, std::string("CUDA error ") + cudaGetErrorString(e_) + \
+                                             " at " + __FILE__ + ":" + std::to_string(__LINE__)); \
+  } while (0)
+
+// kernel launch with error check and the engine's launch counter
+extern thread_local uint64_t* g_launch_counter;
+#define OFC_LAUNCH(kernel, grid, block, smem, stream, ...)                     \
+  do {                                                                         \
+    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                \
+    OFC_CUDA(cudaGetLastError());                                              \
+    if (::ofc::g_launch_counter) ++*::ofc::g_launch_counter;                   \
+  } while (0)
+
+inline unsigned div_up(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------- cubic B-spline (interp.py)
+__host__ __device__ inline long mirror_idx(long i, long n) {  // interp.py:38-43
+  if (n == 1) return 0;
+  long p = 2 * (n - 1);
+  i = i < 0 ? -i : i;
+  i %= p;
+  return i >= n ? p - i : i;
+}
+
+__host__ __device__ inline void bspline_weights(double t, double w[4]) {  // interp.py:46-49
+  double t2 = t * t, t3 = t2 * t;
+  double u = 1 - t;
+  w[0] = u * u * u / 6;
+  w[1] = (3 * t3 - 6 * t2 + 4) / 6;
+  w[2] = (-3 * t3 + 3 * t2 + 3 * t + 1) / 6;
+  w[3] = t3 / 6;
+}
+
+// taps of sample(): clamp to [0, n-1], floor, weights, mirrored indices (interp.py:52-69)
+struct Taps {
+  int xi[4], yi[4];
+  double wx[4], wy[4];
+};
+
+__device__ inline bool make_taps(double x, double y, int w, int h, Taps& t) {
+  if (!(x == x) || !(y == y)) return false;
+  x = fmin(fmax(x, 0.0), (double)(w - 1));
+  y = fmin(fmax(y, 0.0), (double)(h - 1));
+  double fx = floor(x), fy = floor(y);
+  long x0 = (long)fx, y0 = (long)fy;
+  bspline_weights(x - fx, t.wx);
+  bspline_weights(y - fy, t.wy);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    t.xi[k] = (int)mirror_idx(x0 + k - 1, w);
+    t.yi[k] = (int)mirror_idx(y0 + k - 1, h);
+  }
+  return true;
+}
+
+template <class T>
+__device__ inline double sample_real(const T* c, int w, const Taps& t) {
+  double out = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const T* row = c + (size_t)t.yi[j] * w;
+    double acc = t.wx[0] * (double)row[t.xi[0]];
+#pragma unroll
+    for (int k = 1; k < 4; k++) acc += t.wx[k] * (double)row[t.xi[k]];
+    out += t.wy[j] * acc;
+  }
+  return out;
+}
+
+// complex spline stored as float2; float accumulation of the 16 taps with f64-derived weights
+__device__ inline float2 sample_c32(const float2* __restrict__ c, int w, const Taps& t) {
+  float re = 0.f, im = 0.f;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const float2* row = c + (size_t)t.yi[j] * w;
+    float are = 0.f, aim = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      float2 v = __ldg(row + t.xi[k]);
+      float wk = (float)t.wx[k];
+      are = fmaf(wk, v.x, are);
+      aim = fmaf(wk, v.y, aim);
+    }
+    float wj = (float)t.wy[j];
+    re = fmaf(wj, are, re);
+    im = fmaf(wj, aim, im);
+  }
+  return make_float2(re, im);
+}
+
+// scalar bspline prefilter pole
+__host__ __device__ inline double bspline_z() { return sqrt(3.0) - 2.0; }  // interp.py:9
+
+}  // namespace ofc

@@ -1,0 +1,1109 @@
+// engine.cu -- the C ABI of include/optflow_cuda.h: engine state, device buffers, and the order of the
+// kernels of one pair (coarse POC -> dense start -> fine stage -> confidence -> finish).
+//
+// Everything between the upload of the inputs and the download of the outputs runs on one CUDA stream
+// with no host synchronisation: conditional steps of the reference (the energy-threshold reset, the
+// trusted pre-warp's "any low / not all trusted" cases) are decided on the device from counters that the
+// kernels read, so a whole pair can be captured and replayed as a CUDA graph.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+#include "fft.cuh"
+#include "kernels.cuh"
+#include "../../include/optflow_cuda_testing.h"
+
+namespace ofc {
+thread_local uint64_t* g_launch_counter = nullptr;
+}
+
+using namespace ofc;
+
+namespace {
+
+// ---------------------------------------------------------------- config helpers (config.py:247-272)
+double smax_of(const ofc_config& c) {
+  double m = 0;
+  for (int i = 0; i < c.n_scales; i++) m = std::max(m, c.scales[i]);
+  return m;
+}
+double auto_guard(const ofc_config& c) { return 3.0 * c.lam * smax_of(c) / (2 * PI * c.bandwidth); }
+double guard_px(const ofc_config& c) { return c.edge_guard >= 0 ? c.edge_guard : auto_guard(c); }
+double min_area_px(const ofc_config& c) {
+  if (c.edge_guard_min_area >= 0) return c.edge_guard_min_area;
+  double l = c.lam * smax_of(c);
+  return 2.0 * l * l;
+}
+
+std::string validate(const ofc_config& c) {  // Config.validate, config.py:166-245 (pair-path keys)
+  auto finite = [](double v) { return std::isfinite(v); };
+  if (c.n_scales < 1) return "scales must not be empty";
+  if (c.n_scales > OFC_MAX_SCALES) return "the CUDA engine holds at most 16 scales";
+  if (c.poc_win < 16 || (c.poc_win & (c.poc_win - 1))) return "poc_win must be a power of two >= 16";
+  if (c.grid_step < 1 || c.strain_win < 5 || c.strain_win % 2 == 0) return "grid_step >= 1 and strain_win odd >= 5 required";
+  if (c.dc_cut <= 0) return "dc_cut must be positive";
+  if (c.phase_tol <= 0) return "phase_tol must be positive";
+  if (c.shape_order != 1 && c.shape_order != 2) return "shape_order must be 1 or 2";
+  double smin = c.scales[0];
+  for (int i = 0; i < c.n_scales; i++) smin = std::min(smin, c.scales[i]);
+  if (c.lam * smin < 3 || c.sigma_w <= 0 || c.sigma_s <= 0)
+    return "shortest wavelength lam*min(scales) must be >= 3 px; sigmas must be positive";
+  const double* fl[] = {&c.max_disp, &c.poc_peak_min, &c.median_thresh, &c.lam, &c.bandwidth, &c.dc_cut, &c.sigma_w,
+                        &c.sigma_s, &c.conf_min, &c.edge_guard, &c.edge_guard_min_area, &c.phase_tol};
+  const char* nm[] = {"max_disp", "poc_peak_min", "median_thresh", "lam", "bandwidth", "dc_cut", "sigma_w",
+                      "sigma_s", "conf_min", "edge_guard", "edge_guard_min_area", "phase_tol"};
+  for (int i = 0; i < 12; i++)
+    if (!finite(*fl[i])) return std::string(nm[i]) + " must be a finite number";
+  for (int i = 0; i < c.n_scales; i++)
+    if (!finite(c.scales[i])) return "scales must be finite numbers";
+  if (c.bandwidth <= 0 || c.max_disp <= 0 || c.median_thresh <= 0) return "bandwidth, max_disp and median_thresh must be positive";
+  if (c.n_orient < 1 || c.outer_iters < 1 || c.inner_iters < 1) return "n_orient, outer_iters and inner_iters must be >= 1";
+  if (!(c.conf_min >= 0 && c.conf_min <= 1) || !(c.poc_peak_min >= 0 && c.poc_peak_min <= 1))
+    return "conf_min and poc_peak_min must lie in [0, 1]";
+  if (c.prewarp_freeze_at < 0) return "prewarp_freeze_at must be >= 0";
+  if (c.n_orient * c.n_scales > 64 || c.sigma_w > 256 || c.sigma_s > 256 || c.strain_win > 255 || c.poc_win > 1024)
+    return "at most 64 filters (n_orient * len(scales)); sigma_w, sigma_s <= 256, strain_win <= 255 and poc_win <= 1024 required";
+  if (c.grid_step > 4096 || guard_px(c) > 256)
+    return "grid_step <= 4096 and an edge guard (edge_guard, or the automatic one from lam, scales and bandwidth) <= 256 px required";
+  return "";
+}
+
+// ---------------------------------------------------------------- POC geometry (poc.py:61-64,168-195)
+int pow2_floor(long n) {
+  if (n < 1) return 0;
+  int b = 0;
+  while ((n >> (b + 1)) > 0) b++;
+  return 1 << b;
+}
+bool level_window(int h, int w, int win, int& wy, int& wx) {
+  int lim_h = pow2_floor(2 * h / 3), lim_w = pow2_floor(2 * w / 3);
+  if (win <= lim_h && win <= lim_w) { wy = wx = win; return true; }
+  if (h <= w) {
+    wy = std::min(win, lim_h);
+    wx = std::min(lim_w, std::max(win, win * win / std::max(wy, 1)));
+  } else {
+    wx = std::min(win, lim_w);
+    wy = std::min(lim_h, std::max(win, win * win / std::max(wx, 1)));
+  }
+  return std::min(wy, wx) >= 16;
+}
+int n_levels(double max_disp, int win, int h, int w) {
+  int L = (int)std::max(0.0, std::ceil(std::log2(std::max(max_disp, 1e-9) / (win / 4.0))));
+  int wy, wx;
+  while (L > 0 && !level_window(h >> L, w >> L, win, wy, wx)) L--;
+  return L;
+}
+std::vector<int> arange(int a, int b, int step) {
+  std::vector<int> v;
+  for (int i = a; i < b; i += step) v.push_back(i);
+  return v;
+}
+
+std::vector<double> gauss_kernel(double sigma) {  // interp.py:79-83
+  int r = (int)(4.0 * sigma + 0.5);
+  std::vector<double> k(2 * r + 1);
+  double s = 0;
+  for (int i = -r; i <= r; i++) {
+    double t = i / sigma;
+    k[i + r] = std::exp(-0.5 * t * t);
+  }
+  for (double v : k) s += v;
+  for (double& v : k) v /= s;
+  return k;
+}
+
+// ---------------------------------------------------------------- device buffers
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+struct Lane {
+  cudaStream_t stream = nullptr;
+  std::mutex busy;
+  std::unordered_map<std::string, std::unique_ptr<DevBuf>> pool;
+  std::map<int, std::pair<FftPlan, std::unique_ptr<DevBuf>>> plans;
+  cudaEvent_t ev[4] = {};
+
+  template <class T>
+  T* get(const std::string& name, size_t count) {
+    size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+    auto& b = pool[name];
+    if (!b) b.reset(new DevBuf());
+    if (b->bytes < bytes) {
+      if (b->p) OFC_CUDA(cudaFree(b->p));
+      b->p = nullptr;
+      b->bytes = 0;
+      OFC_CUDA(cudaMalloc(&b->p, bytes));
+      b->bytes = bytes;
+    }
+    return (T*)b->p;
+  }
+  template <class T>
+  T* upload(const std::string& name, const T* host, size_t count) {
+    T* d = get<T>(name, count);
+    OFC_CUDA(cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyHostToDevice, stream));
+    return d;
+  }
+  const FftPlan& plan(int L) {
+    auto it = plans.find(L);
+    if (it != plans.end()) return it->second.first;
+    FftPlan pl = fft_make_plan(L);
+    std::vector<float2> tw = fft_twiddles(L);
+    std::vector<double2> twd = fft_twiddles_f64(L);
+    std::unique_ptr<DevBuf> b(new DevBuf());
+    size_t b32 = tw.size() * sizeof(float2), b64 = twd.size() * sizeof(double2);
+    OFC_CUDA(cudaMalloc(&b->p, b64 + b32));
+    b->bytes = b64 + b32;
+    OFC_CUDA(cudaMemcpy(b->p, twd.data(), b64, cudaMemcpyHostToDevice));
+    OFC_CUDA(cudaMemcpy((char*)b->p + b64, tw.data(), b32, cudaMemcpyHostToDevice));
+    pl.twd = (const double2*)b->p;
+    pl.tw = (const float2*)((char*)b->p + b64);
+    auto& slot = plans[L];
+    slot.first = pl;
+    slot.second = std::move(b);
+    return slot.first;
+  }
+  void release() {
+    pool.clear();
+    plans.clear();
+  }
+};
+
+}  // namespace
+
+struct ofc_engine {
+  int device = 0;
+  int nlanes = 1;
+  uint64_t launches = 0;
+  std::vector<std::unique_ptr<Lane>> lanes;
+};
+
+namespace {
+
+void set_err(char* err, size_t len, const std::string& m) {
+  if (err && len) {
+    size_t n = std::min(len - 1, m.size());
+    std::memcpy(err, m.data(), n);
+    err[n] = 0;
+  }
+}
+
+// Runs f on a free lane of the engine (GpuEngine refuses instead of blocking, engine.rs:660-676).
+template <class F>
+int guarded(ofc_engine* e, char* err, size_t errlen, F&& f) {
+  if (!e) { set_err(err, errlen, "null engine"); return OFC_ERR_ARG; }
+  Lane* lane = nullptr;
+  std::unique_lock<std::mutex> lk;
+  for (auto& l : e->lanes) {
+    std::unique_lock<std::mutex> t(l->busy, std::try_to_lock);
+    if (t.owns_lock()) { lk = std::move(t); lane = l.get(); break; }
+  }
+  if (!lane) {
+    set_err(err, errlen, "the CUDA engine is busy: more concurrent calls than its " + std::to_string(e->nlanes) + " lane(s)");
+    return OFC_ERR_BUSY;
+  }
+  g_launch_counter = &e->launches;
+  try {
+    OFC_CUDA(cudaSetDevice(e->device));
+    f(*lane);
+    g_launch_counter = nullptr;
+    return OFC_OK;
+  } catch (const Error& x) {
+    g_launch_counter = nullptr;
+    set_err(err, errlen, x.what());
+    return x.status;
+  } catch (const std::exception& x) {
+    g_launch_counter = nullptr;
+    set_err(err, errlen, x.what());
+    return OFC_ERR_DEVICE;
+  }
+}
+
+// ---------------------------------------------------------------- the fine stage on one window
+struct FineOut {
+  double* ux;  // W*H each (ux and uy contiguous: uy = ux + W*H)
+  double* uy;
+  double* energy;
+  double* resid;
+  EnergyStats* stats;  // median of the final energy
+};
+
+// reference_phase (phaseflow.py:100-111) of i1 in float64 transforms, stored as float32 (r.re, r.im, gx, gy)
+// and amp per filter. The transforms run in float64 because the phase gradient divides by |r|^2: near a zero
+// of a response, the absolute error of a float32 transform (~1e-7 of the largest response) is a large
+// relative error of r, and the weighted gradient terms w g^2 ~ |r2| |r_y|^2 / |r| of the normal equations
+// amplify it. Filters are processed in groups to bound the scratch (3 planes of ph x pw float64 per filter).
+void reference_pack(Lane& L, const float* i1, int W, int H, const GaborTables& g, float4* ref4, float* amp) {
+  cudaStream_t st = L.stream;
+  const int ph = H + 2 * PAD, pw = W + 2 * PAD;
+  const size_t Np = (size_t)ph * pw;
+  const int G = std::min(g.F, 4);
+  double2* T64 = L.get<double2>("ref_T64", Np);
+  double2* U64 = L.get<double2>("ref_U64", Np * 3 * G);
+  const FftPlan& plw = L.plan(pw);
+  const FftPlan& plh = L.plan(ph);
+  launch_fft_rows_fwd_real_f64(i1, W, H, plw, ph, T64, st);
+  for (int k0 = 0; k0 < g.F; k0 += G) {
+    int k1 = std::min(g.F, k0 + G);
+    launch_fft_cols_ref_f64(T64, plh, pw, g, k0, k1, U64, st);
+    launch_fft_rows_inv_ref_f64(U64, plw, ph, k0, k1, W, H, ref4, amp, st);
+  }
+}
+
+// refine_raw (phaseflow.rs:1514-1613 / phaseflow.py:427-507) on the device. u2: 2 planes (ux | uy) holding
+// the start and receiving the result.
+FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int w2, int h2, long shx, long shy,
+                   double* u2, const ofc_config& c) {
+  cudaStream_t st = L.stream;
+  const size_t N = (size_t)W * H;
+  const int ph = H + 2 * PAD, pw = W + 2 * PAD;
+  const size_t Np = (size_t)ph * pw;
+  const int F = c.n_scales * c.n_orient;
+  const FftPlan& plw = L.plan(pw);
+  const FftPlan& plh = L.plan(ph);
+  // Gabor tables
+  std::vector<double> gt = gabor_tables_host(ph, pw, c);
+  double* dg = L.upload("gabor", gt.data(), gt.size());
+  GaborTables g;
+  g.F = F; g.ph = ph; g.pw = pw;
+  g.fx = dg; g.fy = dg + pw; g.hx = g.fy + ph; g.hy = g.hx + pw; g.ex = g.hy + ph; g.ey = g.ex + (size_t)F * pw;
+  // taps: smoothing Gaussian (sigma_s) and window moments k(t) t^p, p = 0..4 (sigma_w)
+  std::vector<double> ks = gauss_kernel(c.sigma_s);
+  int rs = (int)ks.size() / 2;
+  std::vector<double> kw = gauss_kernel(c.sigma_w);
+  int rw = (int)kw.size() / 2;
+  int K = 2 * rw + 1;
+  std::vector<double> mt((size_t)5 * K);
+  for (int p = 0; p < 5; p++)
+    for (int t = -rw; t <= rw; t++) mt[(size_t)p * K + t + rw] = kw[t + rw] * std::pow((double)t, p);
+  double* d_ks = L.upload("taps_s", ks.data(), ks.size());
+  double* d_mt = L.upload("taps_w", mt.data(), mt.size());
+
+  // reference pack (phaseflow.py:431, reference_phase)
+  float2* T = L.get<float2>("fft_T", Np);
+  float2* U = L.get<float2>("fft_U", Np * F);
+  float4* ref4 = L.get<float4>("ref4", N * F);
+  float* amp = L.get<float>("ref_amp", N * F);
+  reference_pack(L, i1, W, H, g, ref4, amp);
+  // spline of image 2 (kept for all iterations)
+  float* c2 = L.get<float>("spline2", (size_t)w2 * h2);
+  double* tmp2 = L.get<double>("spline2_tmp", (size_t)w2 * h2 * 2);
+  launch_bspline_f32(i2, c2, tmp2, w2, h2, st);
+
+  double* u2b = L.get<double>("u2b", 2 * N);
+  double* s2 = L.get<double>("s2", 2 * N);
+  double* cs2 = L.get<double>("cs2", 2 * N);
+  double* pre2 = L.get<double>("pre2", 2 * N);
+  double* tmpb = L.get<double>("blur_tmp", 2 * N);
+  double* energy = L.get<double>("energy", N);
+  double* resid = L.get<double>("resid", N);
+  double* slope = L.get<double>("slope", 4 * N);
+  double* sums = L.get<double>("sums", 7 * N);
+  double* yplanes = L.get<double>("yplanes", (size_t)moment_yplanes(c.shape_order) * N);
+  float* warped = L.get<float>("warped", N);
+  float2* R = L.get<float2>("resp", Np * F);
+  EnergyStats* stats = L.get<EnergyStats>("stats", 1);
+  unsigned long long* hist = L.get<unsigned long long>("hist", 4096);
+  uint8_t* low = L.get<uint8_t>("low", N);
+  uint8_t* frozen = L.get<uint8_t>("frozen", N);
+  uint8_t* okm = L.get<uint8_t>("okmask", N);
+  int* vdist = L.get<int>("vdist", N);
+  int* cold2 = L.get<int>("col_d2", N);
+  int* colrow = L.get<int>("col_row", N);
+  PrewarpCounts* counts = L.get<PrewarpCounts>("pw_counts", 2);
+  OFC_CUDA(cudaMemsetAsync(hist, 0, 4096 * sizeof(unsigned long long), st));
+  launch_fill_f64(resid, PI, N, st);
+  launch_fill_f64(energy, 1.0, N, st);
+  OFC_CUDA(cudaMemsetAsync(slope, 0, 4 * N * sizeof(double), st));
+
+  const double R_trust = auto_guard(c);
+  const int Kf = c.prewarp_freeze_at;
+  double* ucur = u2;
+  double* unext = u2b;
+  for (int it = 0; it < c.outer_iters; it++) {
+    const double* blur_in = ucur;
+    if (it > 0) {
+      uint8_t* lowp = low;
+      if (Kf >= 1 && it > Kf) {
+        lowp = frozen;  // the low pixels of iteration K (prewarp.rs:79-116)
+        OFC_CUDA(cudaMemcpyAsync(&counts[0].low, &counts[1].low, sizeof(int), cudaMemcpyDeviceToDevice, st));
+      } else {
+        OFC_CUDA(cudaMemsetAsync(&counts[0].low, 0, sizeof(int), st));
+        launch_confidence(energy, resid, ucur, ucur + N, W, H, stats, c.phase_tol, c.conf_min, false, 0.0, nullptr,
+                          nullptr, low, &counts[0].low, st);
+        if (Kf >= 1 && it == Kf) {
+          OFC_CUDA(cudaMemcpyAsync(frozen, low, N, cudaMemcpyDeviceToDevice, st));
+          OFC_CUDA(cudaMemcpyAsync(&counts[1].low, &counts[0].low, sizeof(int), cudaMemcpyDeviceToDevice, st));
+        }
+      }
+      launch_prewarp_fill(lowp, ucur, ucur + N, slope, W, H, R_trust, &counts[0], okm, vdist, cold2, colrow, pre2,
+                          pre2 + N, st);
+      blur_in = pre2;
+    }
+    launch_corr_y(blur_in, tmpb, 2, W, H, d_ks, rs, st);
+    launch_corr_x(tmpb, s2, 2, W, H, d_ks, rs, st);
+    launch_warp(c2, w2, h2, s2, s2 + N, shx, shy, W, H, warped, st);
+    launch_fft_rows_fwd_real(warped, W, H, plw, ph, T, st);
+    launch_fft_cols_filters(T, plh, pw, g, U, st);
+    launch_fft_rows_inv_resp(U, plw, ph, F, R, st);
+    launch_bspline_f64(s2, cs2, tmpb, 2, W, H, st);
+    for (int in = 0; in < c.inner_iters; in++) {
+      launch_accumulate(ref4, amp, R, F, ph, pw, ucur, ucur + N, s2, s2 + N, cs2, cs2 + N, W, H, sums, st);
+      launch_moments_solve(sums, ucur, ucur + N, W, H, c.shape_order, d_mt, rw, yplanes, unext, unext + N, energy,
+                           resid, slope, st);
+      const bool last_inner = in == c.inner_iters - 1;
+      launch_energy_stats(energy, N, stats, last_inner, st);
+      launch_median(energy, N, stats, hist, st);
+      launch_reset(energy, ucur, ucur + N, (int)N, stats, unext, unext + N, resid, slope, st);
+      std::swap(ucur, unext);
+    }
+  }
+  if (ucur != u2) OFC_CUDA(cudaMemcpyAsync(u2, ucur, 2 * N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return FineOut{u2, u2 + N, energy, resid, stats};
+}
+
+// ---------------------------------------------------------------- the coarse stage
+struct CoarseOut {
+  int nx, ny;
+  int* xs;  // device
+  int* ys;
+  double* ux;
+  double* uy;
+  double* peak;
+  std::vector<int> hxs, hys;
+};
+
+// coarse_flow (poc.py:216-239); a, b: float32 images W x H on the device; init: 2 planes or null
+CoarseOut coarse_dev(Lane& L, const float* a, const float* b, int W, int H, const double* init, const ofc_config& c) {
+  cudaStream_t st = L.stream;
+  if (c.poc_win > 64) throw Error(OFC_ERR_ARG, "the CUDA engine's POC windows are at most 64 x 64 (poc_win <= 64)");
+  const size_t N = (size_t)W * H;
+  int Lv = n_levels(c.max_disp, c.poc_win, H, W);
+  std::vector<double> k1 = gauss_kernel(1.0);
+  double* d_k1 = L.upload("taps_1", k1.data(), k1.size());
+  int r1 = (int)k1.size() / 2;
+  // pyramid (float64): level 0 is the input itself
+  std::vector<double*> pa(Lv + 1), pb(Lv + 1);
+  std::vector<int> pws(Lv + 1), phs(Lv + 1);
+  pa[0] = L.get<double>("pyr_a0", N);
+  pb[0] = L.get<double>("pyr_b0", N);
+  launch_f32_to_f64(a, pa[0], N, st);
+  launch_f32_to_f64(b, pb[0], N, st);
+  pws[0] = W;
+  phs[0] = H;
+  double* tmp = L.get<double>("pyr_tmp", N);
+  for (int l = 1; l <= Lv; l++) {
+    int w = (pws[l - 1] + 1) / 2, h = (phs[l - 1] + 1) / 2;
+    pa[l] = L.get<double>("pyr_a" + std::to_string(l), (size_t)w * h);
+    pb[l] = L.get<double>("pyr_b" + std::to_string(l), (size_t)w * h);
+    launch_downsample(pa[l - 1], pws[l - 1], phs[l - 1], pa[l], tmp, d_k1, r1, st);
+    launch_downsample(pb[l - 1], pws[l - 1], phs[l - 1], pb[l], tmp, d_k1, r1, st);
+    pws[l] = w;
+    phs[l] = h;
+  }
+  std::vector<int> xs0 = arange(c.poc_win / 2, W - c.poc_win / 2 + 1, c.grid_step);
+  std::vector<int> ys0 = arange(c.poc_win / 2, H - c.poc_win / 2 + 1, c.grid_step);
+  CoarseOut prev{};
+  bool have = false;
+  for (int lev = Lv; lev >= 0; lev--) {
+    int w = pws[lev], h = phs[lev];
+    int wy = c.poc_win, wx = c.poc_win;
+    std::vector<int> gx = xs0, gy = ys0;
+    if (lev != 0) {
+      level_window(h, w, c.poc_win, wy, wx);
+      gx = arange(wx / 2, w - wx / 2 + 1, c.grid_step);
+      gy = arange(wy / 2, h - wy / 2 + 1, c.grid_step);
+    }
+    if (gx.empty() || gy.empty()) throw Error(OFC_ERR_ARG, "image too small for the POC grid");
+    int nx = (int)gx.size(), ny = (int)gy.size();
+    std::string sfx = std::to_string(lev);
+    int* dxs = L.upload("poc_xs" + sfx, gx.data(), gx.size());
+    int* dys = L.upload("poc_ys" + sfx, gy.data(), gy.size());
+    double* iu = nullptr;
+    double* iv = nullptr;
+    if (have) {
+      iu = L.get<double>("poc_iu" + sfx, (size_t)nx * ny);
+      iv = L.get<double>("poc_iv" + sfx, (size_t)nx * ny);
+      launch_grid_sample(prev.ux, prev.uy, prev.xs, prev.ys, prev.nx, prev.ny, dxs, dys, nx, ny, 0.5, 2.0, iu, iv, st);
+    } else if (init) {
+      iu = L.get<double>("poc_iu" + sfx, (size_t)nx * ny);
+      iv = L.get<double>("poc_iv" + sfx, (size_t)nx * ny);
+      launch_init_from_dense(init, init + N, W, dxs, dys, nx, ny, 1 << lev, iu, iv, st);
+    }
+    double* gu = L.get<double>("poc_u" + sfx, (size_t)nx * ny);
+    double* gv = L.get<double>("poc_v" + sfx, (size_t)nx * ny);
+    double* gp = L.get<double>("poc_p" + sfx, (size_t)nx * ny);
+    PocLevel lv{w, h, nx, ny, wy, wx};
+    launch_poc_grid(pa[lev], pb[lev], lv, dxs, dys, iu, iv, gu, gv, gp, st);
+    uint8_t* scr = L.get<uint8_t>("poc_flags", (size_t)3 * nx * ny);
+    launch_poc_clean(gu, gv, gp, nx, ny, c.poc_peak_min, c.median_thresh, iu, iv, scr, st);
+    prev = CoarseOut{nx, ny, dxs, dys, gu, gv, gp, gx, gy};
+    have = true;
+  }
+  return prev;
+}
+
+// dense start of track_pair (track.py:131-137) into u2 (2 planes)
+void dense_start(Lane& L, const CoarseOut& g, int W, int H, const double* init, double* u2) {
+  cudaStream_t st = L.stream;
+  const size_t N = (size_t)W * H;
+  if (!init) {
+    launch_grid_sample(g.ux, g.uy, g.xs, g.ys, g.nx, g.ny, nullptr, nullptr, W, H, 1.0, 1.0, u2, u2 + N, st);
+    return;
+  }
+  double* cu = L.get<double>("corr_u", (size_t)g.nx * g.ny);
+  double* cv = L.get<double>("corr_v", (size_t)g.nx * g.ny);
+  launch_grid_minus_dense(g.ux, g.uy, init, init + N, W, g.xs, g.ys, g.nx, g.ny, cu, cv, st);
+  launch_grid_sample(cu, cv, g.xs, g.ys, g.nx, g.ny, nullptr, nullptr, W, H, 1.0, 1.0, u2, u2 + N, st);
+  launch_add(u2, init, 2 * N, st);
+}
+
+// _finish (track.py:56-108): low (u8), roi (u8 or null), ux/uy (raw, f64) -> outputs
+void finish_dev(Lane& L, const uint8_t* low, const uint8_t* roi, const double* ux, const double* uy,
+                const double* conf64, int W, int H, const ofc_config& c, const ofc_pair_out& o) {
+  cudaStream_t st = L.stream;
+  const size_t N = (size_t)W * H;
+  double guard = guard_px(c);
+  uint8_t* big = L.get<uint8_t>("fin_big", N);
+  uint8_t* src = L.get<uint8_t>("fin_src", N);
+  uint8_t* bad = L.get<uint8_t>("fin_bad", N);
+  int* parent = L.get<int>("fin_parent", N);
+  int* size = L.get<int>("fin_size", N);
+  int* vdist = L.get<int>("vdist", N);
+  double* mx = L.get<double>("fin_mx", 2 * N);
+  double* my = mx + N;
+  if (guard > 0) launch_large_components(low, W, H, min_area_px(c), parent, size, big, st);
+  launch_finish_mask(low, roi, big, W, H, guard, ux, uy, src, bad, vdist, mx, my, st);
+  double* yp = L.get<double>("strain_y", 11 * N);
+  launch_strain(mx, my, W, H, c.strain_win, yp, nullptr, nullptr, nullptr, nullptr, o.exx, o.eyy, o.exy, o.gmax, o.vol,
+                st);
+  launch_pair_outputs(mx, my, ux, uy, conf64, (int)N, o.ux, o.uy, o.conf, o.valid, o.raw_ux, o.raw_uy, st);
+}
+
+// the whole pair on device buffers; d_out fields are device pointers
+void track_pair_dev(Lane& L, const float* i1, const float* i2, int W, int H, const uint8_t* roi, const float* iux,
+                    const float* iuy, const ofc_config& c, const ofc_pair_out& o, bool timed, double* timing) {
+  cudaStream_t st = L.stream;
+  const size_t N = (size_t)W * H;
+  if (timed) OFC_CUDA(cudaEventRecord(L.ev[0], st));
+  double* init = nullptr;
+  if (iux) {
+    init = L.get<double>("init2", 2 * N);
+    launch_f32_to_f64(iux, init, N, st);
+    launch_f32_to_f64(iuy, init + N, N, st);
+  }
+  CoarseOut g = coarse_dev(L, i1, i2, W, H, init, c);
+  double* u2 = L.get<double>("u2", 2 * N);
+  dense_start(L, g, W, H, init, u2);
+  if (timed) OFC_CUDA(cudaEventRecord(L.ev[1], st));
+  FineOut f = refine_dev(L, i1, W, H, i2, W, H, 0, 0, u2, c);
+  double* conf64 = L.get<double>("conf64", N);
+  uint8_t* low = L.get<uint8_t>("low_final", N);
+  double B = guard_px(c) > 0 ? 4.0 * c.sigma_w : 0.0;
+  launch_confidence(f.energy, f.resid, f.ux, f.uy, W, H, f.stats, c.phase_tol, c.conf_min, true, B, nullptr, conf64,
+                    low, nullptr, st);
+  if (timed) OFC_CUDA(cudaEventRecord(L.ev[2], st));
+  finish_dev(L, low, roi, f.ux, f.uy, conf64, W, H, c, o);
+  if (timed) {
+    OFC_CUDA(cudaEventRecord(L.ev[3], st));
+    OFC_CUDA(cudaEventSynchronize(L.ev[3]));
+    float ms[3];
+    for (int i = 0; i < 3; i++) OFC_CUDA(cudaEventElapsedTime(&ms[i], L.ev[i], L.ev[i + 1]));
+    for (int i = 0; i < 3; i++) timing[i] = ms[i] * 1e-3;
+  }
+}
+
+void check_sizes(size_t w, size_t h) {
+  if (w < 1 || h < 1) throw Error(OFC_ERR_ARG, "empty image");
+  if (w > 32768 || h > 32768 || w * h > (size_t)1 << 30) throw Error(OFC_ERR_WINDOW, "image too large for the CUDA engine");
+}
+
+void check_fine_window(size_t w, size_t h, const ofc_config& c) {
+  check_sizes(w, h);
+  int pw = (int)w + 2 * PAD, ph = (int)h + 2 * PAD;
+  if (!fft_supported(pw) || !fft_supported(ph))
+    throw Error(OFC_ERR_WINDOW, "window " + std::to_string(w) + "x" + std::to_string(h) +
+                                    ": padded FFT size " + std::to_string(pw) + "x" + std::to_string(ph) +
+                                    " has a prime factor above 31, which the CUDA engine does not transform");
+  if (!fft_fits(ph, pw))
+    throw Error(OFC_ERR_WINDOW, "window " + std::to_string(w) + "x" + std::to_string(h) +
+                                    " exceeds the shared-memory FFT passes of the CUDA engine");
+}
+
+// low = conf < conf_min (track.py:66) for ofc_finish
+__global__ void k_threshold_low(const double* c64, double cm, uint8_t* low, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    low[i] = c64[i] < cm ? 1 : 0;
+}
+void ofc_threshold_low(const double* c64, double cm, uint8_t* low, size_t n, cudaStream_t st) {
+  OFC_LAUNCH(k_threshold_low, std::min<size_t>(div_up(n, 256), 4096), 256, 0, st, c64, cm, low, n);
+}
+
+void cfg_check(const ofc_config* c) {
+  if (!c) throw Error(OFC_ERR_ARG, "null config");
+  std::string m = validate(*c);
+  if (!m.empty()) throw Error(OFC_ERR_ARG, m);
+}
+
+}  // namespace
+
+// ================================================================= C ABI
+extern "C" {
+
+int ofc_abi_version(void) { return OFC_ABI_VERSION; }
+
+void ofc_config_default(ofc_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->grid_step = 16;
+  c->poc_win = 64;
+  c->max_disp = 32.0;
+  c->poc_peak_min = 0.1;
+  c->median_thresh = 2.0;
+  c->lam = 8.0;
+  c->n_scales = 3;
+  c->scales[0] = 0.6;
+  c->scales[1] = 1.0;
+  c->scales[2] = 1.6;
+  c->n_orient = 4;
+  c->bandwidth = 0.5;
+  c->dc_cut = 2.0;
+  c->sigma_w = 4.0;
+  c->shape_order = 1;
+  c->sigma_s = 4.0;
+  c->outer_iters = 8;
+  c->inner_iters = 2;
+  c->conf_min = 0.2;
+  c->edge_guard = -1.0;
+  c->edge_guard_min_area = -1.0;
+  c->phase_tol = 0.4;
+  c->strain_win = 15;
+  c->prewarp_freeze_at = 0;
+}
+
+int ofc_config_validate(const ofc_config* c, char* err, size_t errlen) {
+  if (!c) { set_err(err, errlen, "null config"); return OFC_ERR_ARG; }
+  std::string m = validate(*c);
+  if (m.empty()) return OFC_OK;
+  set_err(err, errlen, m);
+  return OFC_ERR_ARG;
+}
+
+double ofc_edge_guard_px(const ofc_config* c) { return guard_px(*c); }
+double ofc_auto_edge_guard_px(const ofc_config* c) { return auto_guard(*c); }
+double ofc_edge_guard_min_area_px(const ofc_config* c) { return min_area_px(*c); }
+
+ofc_engine* ofc_create(int device, int lanes, char* err, size_t errlen) {
+  try {
+    if (lanes < 1 || lanes > 2) throw Error(OFC_ERR_ARG, "lanes must be 1 or 2");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+      throw Error(OFC_ERR_DEVICE, std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "0 devices"));
+    if (device < 0 || device >= n) throw Error(OFC_ERR_DEVICE, "CUDA device " + std::to_string(device) + " does not exist");
+    OFC_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    OFC_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) throw Error(OFC_ERR_DEVICE, std::string("the engine is built for sm_100a; device is ") + prop.name);
+    std::unique_ptr<ofc_engine> eng(new ofc_engine());
+    eng->device = device;
+    eng->nlanes = lanes;
+    for (int i = 0; i < lanes; i++) {
+      std::unique_ptr<Lane> l(new Lane());
+      OFC_CUDA(cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking));
+      for (auto& ev : l->ev) OFC_CUDA(cudaEventCreate(&ev));
+      eng->lanes.push_back(std::move(l));
+    }
+    return eng.release();
+  } catch (const Error& x) {
+    set_err(err, errlen, x.what());
+    return nullptr;
+  }
+}
+
+void ofc_destroy(ofc_engine* e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  for (auto& l : e->lanes) {
+    std::lock_guard<std::mutex> lk(l->busy);
+    cudaStreamSynchronize(l->stream);
+    l->release();
+    for (auto& ev : l->ev) cudaEventDestroy(ev);
+    cudaStreamDestroy(l->stream);
+  }
+  delete e;
+}
+
+int ofc_lanes(const ofc_engine* e) { return e ? e->nlanes : 0; }
+
+uint64_t ofc_kernel_launches(const ofc_engine* e) { return e ? e->launches : 0; }
+
+int ofc_check_window(ofc_engine* e, size_t w, size_t h, const ofc_config* c, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane&) {
+    cfg_check(c);
+    check_fine_window(w, h, *c);
+    // device memory of the fine stage of one window (bytes per padded / window pixel, see the buffers of refine_dev)
+    size_t N = w * h, Np = (w + 2 * PAD) * (h + 2 * PAD);
+    int F = c->n_scales * c->n_orient;
+    size_t need = Np * 8 * (1 + 3 * F + F) + N * (20 * F + 8 * 60 + 4 * 8);
+    size_t fre = 0, tot = 0;
+    OFC_CUDA(cudaMemGetInfo(&fre, &tot));
+    if (need > tot * 9 / 10)
+      throw Error(OFC_ERR_WINDOW, "window " + std::to_string(w) + "x" + std::to_string(h) + " needs " +
+                                      std::to_string(need >> 20) + " MiB of device memory");
+  });
+}
+
+void ofc_release_caches(ofc_engine* e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  for (auto& l : e->lanes) {
+    std::lock_guard<std::mutex> lk(l->busy);
+    cudaStreamSynchronize(l->stream);
+    l->release();
+  }
+}
+
+int ofc_refine_raw(ofc_engine* e, const float* i1, size_t w, size_t h, const float* i2, size_t w2, size_t h2,
+                   int64_t shift_x, int64_t shift_y, const float* ux, const float* uy, const ofc_config* c,
+                   double* out_ux, double* out_uy, double* out_energy, double* out_resid, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_fine_window(w, h, *c);
+    check_sizes(w2, h2);
+    if (!i1 || !i2 || !ux || !uy) throw Error(OFC_ERR_ARG, "null input");
+    const size_t N = w * h;
+    cudaStream_t st = L.stream;
+    float* d1 = L.upload("in_i1", i1, N);
+    float* d2 = L.upload("in_i2", i2, w2 * h2);
+    float* du = L.upload("in_u", ux, N);
+    float* dv = L.upload("in_v", uy, N);
+    double* u2 = L.get<double>("u2", 2 * N);
+    launch_f32_to_f64(du, u2, N, st);
+    launch_f32_to_f64(dv, u2 + N, N, st);
+    FineOut f = refine_dev(L, d1, (int)w, (int)h, d2, (int)w2, (int)h2, (long)shift_x, (long)shift_y, u2, *c);
+    if (out_ux) OFC_CUDA(cudaMemcpyAsync(out_ux, f.ux, N * 8, cudaMemcpyDeviceToHost, st));
+    if (out_uy) OFC_CUDA(cudaMemcpyAsync(out_uy, f.uy, N * 8, cudaMemcpyDeviceToHost, st));
+    if (out_energy) OFC_CUDA(cudaMemcpyAsync(out_energy, f.energy, N * 8, cudaMemcpyDeviceToHost, st));
+    if (out_resid) OFC_CUDA(cudaMemcpyAsync(out_resid, f.resid, N * 8, cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int ofc_refine(ofc_engine* e, const float* i1, const float* i2, size_t w, size_t h, const float* ux, const float* uy,
+               const ofc_config* c, float* out_ux, float* out_uy, float* out_conf, float* out_resid, uint8_t* out_low,
+               char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_fine_window(w, h, *c);
+    if (!i1 || !i2 || !ux || !uy) throw Error(OFC_ERR_ARG, "null input");
+    const size_t N = w * h;
+    cudaStream_t st = L.stream;
+    float* d1 = L.upload("in_i1", i1, N);
+    float* d2 = L.upload("in_i2", i2, N);
+    float* du = L.upload("in_u", ux, N);
+    float* dv = L.upload("in_v", uy, N);
+    double* u2 = L.get<double>("u2", 2 * N);
+    launch_f32_to_f64(du, u2, N, st);
+    launch_f32_to_f64(dv, u2 + N, N, st);
+    FineOut f = refine_dev(L, d1, (int)w, (int)h, d2, (int)w, (int)h, 0, 0, u2, *c);
+    float* conf = L.get<float>("out_conf", N);
+    uint8_t* low = L.get<uint8_t>("low_final", N);
+    double B = guard_px(*c) > 0 ? 4.0 * c->sigma_w : 0.0;
+    launch_confidence(f.energy, f.resid, f.ux, f.uy, (int)w, (int)h, f.stats, c->phase_tol, c->conf_min, true, B, conf,
+                      nullptr, low, nullptr, st);
+    float* o32 = L.get<float>("out_f32", 3 * N);
+    launch_f64_to_f32(f.ux, o32, N, st);
+    launch_f64_to_f32(f.uy, o32 + N, N, st);
+    launch_f64_to_f32(f.resid, o32 + 2 * N, N, st);
+    if (out_ux) OFC_CUDA(cudaMemcpyAsync(out_ux, o32, N * 4, cudaMemcpyDeviceToHost, st));
+    if (out_uy) OFC_CUDA(cudaMemcpyAsync(out_uy, o32 + N, N * 4, cudaMemcpyDeviceToHost, st));
+    if (out_resid) OFC_CUDA(cudaMemcpyAsync(out_resid, o32 + 2 * N, N * 4, cudaMemcpyDeviceToHost, st));
+    if (out_conf) OFC_CUDA(cudaMemcpyAsync(out_conf, conf, N * 4, cudaMemcpyDeviceToHost, st));
+    if (out_low) OFC_CUDA(cudaMemcpyAsync(out_low, low, N, cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int ofc_grid_shape(size_t w, size_t h, const ofc_config* c, size_t* nx, size_t* ny) {
+  if (!c || !nx || !ny) return OFC_ERR_ARG;
+  std::vector<int> xs = arange(c->poc_win / 2, (int)w - c->poc_win / 2 + 1, c->grid_step);
+  std::vector<int> ys = arange(c->poc_win / 2, (int)h - c->poc_win / 2 + 1, c->grid_step);
+  *nx = xs.size();
+  *ny = ys.size();
+  return (xs.empty() || ys.empty()) ? OFC_ERR_ARG : OFC_OK;
+}
+
+int ofc_coarse_flow(ofc_engine* e, const float* a, const float* b, size_t w, size_t h, const float* init_ux,
+                    const float* init_uy, const ofc_config* c, int32_t* xs, int32_t* ys, float* gux, float* guy,
+                    float* gpeak, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_sizes(w, h);
+    if (!a || !b) throw Error(OFC_ERR_ARG, "null input");
+    if ((init_ux == nullptr) != (init_uy == nullptr)) throw Error(OFC_ERR_ARG, "init_ux and init_uy must both be given");
+    const size_t N = w * h;
+    cudaStream_t st = L.stream;
+    float* da = L.upload("in_i1", a, N);
+    float* db = L.upload("in_i2", b, N);
+    double* init = nullptr;
+    if (init_ux) {
+      float* du = L.upload("in_u", init_ux, N);
+      float* dv = L.upload("in_v", init_uy, N);
+      init = L.get<double>("init2", 2 * N);
+      launch_f32_to_f64(du, init, N, st);
+      launch_f32_to_f64(dv, init + N, N, st);
+    }
+    CoarseOut g = coarse_dev(L, da, db, (int)w, (int)h, init, *c);
+    size_t n = (size_t)g.nx * g.ny;
+    float* o = L.get<float>("out_f32", 3 * n);
+    launch_f64_to_f32(g.ux, o, n, st);
+    launch_f64_to_f32(g.uy, o + n, n, st);
+    launch_f64_to_f32(g.peak, o + 2 * n, n, st);
+    if (gux) OFC_CUDA(cudaMemcpyAsync(gux, o, n * 4, cudaMemcpyDeviceToHost, st));
+    if (guy) OFC_CUDA(cudaMemcpyAsync(guy, o + n, n * 4, cudaMemcpyDeviceToHost, st));
+    if (gpeak) OFC_CUDA(cudaMemcpyAsync(gpeak, o + 2 * n, n * 4, cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaStreamSynchronize(st));
+    if (xs) std::copy(g.hxs.begin(), g.hxs.end(), xs);
+    if (ys) std::copy(g.hys.begin(), g.hys.end(), ys);
+  });
+}
+
+int ofc_strain(ofc_engine* e, const float* ux, const float* uy, size_t w, size_t h, int32_t win, float* dudx,
+               float* dudy, float* dvdx, float* dvdy, float* exx, float* eyy, float* exy, float* gmax, float* vol,
+               char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    check_sizes(w, h);
+    if (win < 1 || win > 255) throw Error(OFC_ERR_ARG, "strain window must lie in [1, 255]");
+    const size_t N = w * h;
+    cudaStream_t st = L.stream;
+    float* du = L.upload("in_u", ux, N);
+    float* dv = L.upload("in_v", uy, N);
+    double* m2 = L.get<double>("fin_mx", 2 * N);
+    launch_f32_to_f64(du, m2, N, st);
+    launch_f32_to_f64(dv, m2 + N, N, st);
+    double* yp = L.get<double>("strain_y", 11 * N);
+    float* o = L.get<float>("out_f32", 9 * N);
+    launch_strain(m2, m2 + N, (int)w, (int)h, win, yp, o, o + N, o + 2 * N, o + 3 * N, o + 4 * N, o + 5 * N, o + 6 * N,
+                  o + 7 * N, o + 8 * N, st);
+    float* outs[9] = {dudx, dudy, dvdx, dvdy, exx, eyy, exy, gmax, vol};
+    for (int i = 0; i < 9; i++)
+      if (outs[i]) OFC_CUDA(cudaMemcpyAsync(outs[i], o + i * N, N * 4, cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+static void download_pair(Lane& L, const ofc_pair_out& d, ofc_pair_out* h, size_t N) {
+  cudaStream_t st = L.stream;
+  float* const* dsrc[10] = {&d.ux, &d.uy, &d.conf, &d.exx, &d.eyy, &d.exy, &d.gmax, &d.vol, &d.raw_ux, &d.raw_uy};
+  float** hdst[10] = {&h->ux, &h->uy, &h->conf, &h->exx, &h->eyy, &h->exy, &h->gmax, &h->vol, &h->raw_ux, &h->raw_uy};
+  for (int i = 0; i < 10; i++)
+    if (*hdst[i]) OFC_CUDA(cudaMemcpyAsync(*hdst[i], *dsrc[i], N * 4, cudaMemcpyDeviceToHost, st));
+  if (h->valid) OFC_CUDA(cudaMemcpyAsync(h->valid, d.valid, N, cudaMemcpyDeviceToHost, st));
+}
+
+static ofc_pair_out device_pair_out(Lane& L, size_t N) {
+  ofc_pair_out d{};
+  float* p = L.get<float>("out_pair", 10 * N);
+  float** f[10] = {&d.ux, &d.uy, &d.conf, &d.exx, &d.eyy, &d.exy, &d.gmax, &d.vol, &d.raw_ux, &d.raw_uy};
+  for (int i = 0; i < 10; i++) *f[i] = p + i * N;
+  d.valid = L.get<uint8_t>("out_valid", N);
+  return d;
+}
+
+int ofc_finish(ofc_engine* e, const float* ux, const float* uy, const float* conf, const uint8_t* roi, size_t w,
+               size_t h, const ofc_config* c, ofc_pair_out* out, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_sizes(w, h);
+    if (!ux || !uy || !conf || !out) throw Error(OFC_ERR_ARG, "null argument");
+    const size_t N = w * h;
+    cudaStream_t st = L.stream;
+    float* du = L.upload("in_u", ux, N);
+    float* dv = L.upload("in_v", uy, N);
+    float* dc = L.upload("in_conf", conf, N);
+    const uint8_t* droi = roi ? L.upload("in_roi", roi, N) : nullptr;
+    double* u2 = L.get<double>("u2", 2 * N);
+    double* c64 = L.get<double>("conf64", N);
+    launch_f32_to_f64(du, u2, N, st);
+    launch_f32_to_f64(dv, u2 + N, N, st);
+    launch_f32_to_f64(dc, c64, N, st);
+    // low = conf < conf_min on the given confidence (track.py:66)
+    uint8_t* low = L.get<uint8_t>("low_final", N);
+    ofc_threshold_low(c64, c->conf_min, low, N, st);
+    ofc_pair_out d = device_pair_out(L, N);
+    finish_dev(L, low, droi, u2, u2 + N, c64, (int)w, (int)h, *c, d);
+    download_pair(L, d, out, N);
+    OFC_CUDA(cudaStreamSynchronize(st));
+    std::memset(out->timing, 0, sizeof(out->timing));
+  });
+}
+
+int ofc_track_pair(ofc_engine* e, const float* i1, const float* i2, size_t w, size_t h, const uint8_t* roi,
+                   const float* init_ux, const float* init_uy, const ofc_config* c, ofc_pair_out* out, char* err,
+                   size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_fine_window(w, h, *c);
+    if (!i1 || !i2 || !out) throw Error(OFC_ERR_ARG, "null argument");
+    if ((init_ux == nullptr) != (init_uy == nullptr)) throw Error(OFC_ERR_ARG, "init_ux and init_uy must both be given");
+    if ((int)std::min(w, h) < c->poc_win)
+      throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
+    const size_t N = w * h;
+    float* d1 = L.upload("in_i1", i1, N);
+    float* d2 = L.upload("in_i2", i2, N);
+    const uint8_t* droi = roi ? L.upload("in_roi", roi, N) : nullptr;
+    const float* du = init_ux ? L.upload("in_u", init_ux, N) : nullptr;
+    const float* dv = init_uy ? L.upload("in_v", init_uy, N) : nullptr;
+    ofc_pair_out d = device_pair_out(L, N);
+    double timing[3] = {0, 0, 0};
+    track_pair_dev(L, d1, d2, (int)w, (int)h, droi, du, dv, *c, d, true, timing);
+    download_pair(L, d, out, N);
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+    for (int i = 0; i < 3; i++) out->timing[i] = timing[i];
+  });
+}
+
+int ofc_track_pair_device(ofc_engine* e, const float* d_i1, const float* d_i2, size_t w, size_t h, const uint8_t* d_roi,
+                          const float* d_init_ux, const float* d_init_uy, const ofc_config* c, ofc_pair_out* d_out,
+                          void* stream, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_fine_window(w, h, *c);
+    if (!d_i1 || !d_i2 || !d_out) throw Error(OFC_ERR_ARG, "null argument");
+    if ((int)std::min(w, h) < c->poc_win)
+      throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
+    cudaStream_t keep = L.stream;
+    if (stream) L.stream = (cudaStream_t)stream;
+    try {
+      track_pair_dev(L, d_i1, d_i2, (int)w, (int)h, d_roi, d_init_ux, d_init_uy, *c, *d_out, false, nullptr);
+    } catch (...) {
+      L.stream = keep;
+      throw;
+    }
+    L.stream = keep;
+    std::memset(d_out->timing, 0, sizeof(d_out->timing));
+  });
+}
+
+}  // extern "C"
+
+
+// ================================================================= single-stage entry points (testing header)
+extern "C" {
+
+int ofc_test_fft_lines(ofc_engine* e, float* data, size_t lines, size_t L, int inverse, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& Ln) {
+    if (!fft_supported((int)L)) throw Error(OFC_ERR_ARG, "unsupported FFT length");
+    const FftPlan& pl = Ln.plan((int)L);
+    float2* d = Ln.upload("t_fft", (const float2*)data, lines * L);
+    launch_fft_lines(d, (int)lines, pl, inverse != 0, Ln.stream);
+    OFC_CUDA(cudaMemcpyAsync(data, d, lines * L * sizeof(float2), cudaMemcpyDeviceToHost, Ln.stream));
+    OFC_CUDA(cudaStreamSynchronize(Ln.stream));
+  });
+}
+
+static GaborTables upload_gabor(Lane& L, int ph, int pw, const ofc_config& c) {
+  std::vector<double> gt = gabor_tables_host(ph, pw, c);
+  double* dg = L.upload("gabor", gt.data(), gt.size());
+  GaborTables g;
+  g.F = c.n_scales * c.n_orient;
+  g.ph = ph;
+  g.pw = pw;
+  g.fx = dg; g.fy = dg + pw; g.hx = g.fy + ph; g.hy = g.hx + pw; g.ex = g.hy + ph; g.ey = g.ex + (size_t)g.F * pw;
+  return g;
+}
+
+int ofc_test_reference_phase(ofc_engine* e, const float* i1, size_t w, size_t h, const ofc_config* c, float* r_re,
+                             float* r_im, float* gx, float* gy, float* amp, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_fine_window(w, h, *c);
+    const int W = (int)w, H = (int)h, ph = H + 2 * PAD, pw = W + 2 * PAD, F = c->n_scales * c->n_orient;
+    const size_t N = w * h, Np = (size_t)ph * pw;
+    GaborTables g = upload_gabor(L, ph, pw, *c);
+    float* d1 = L.upload("in_i1", i1, N);
+    float4* ref4 = L.get<float4>("ref4", N * F);
+    float* a = L.get<float>("ref_amp", N * F);
+    reference_pack(L, d1, W, H, g, ref4, a);
+    std::vector<float4> h4(N * F);
+    OFC_CUDA(cudaMemcpyAsync(h4.data(), ref4, N * F * sizeof(float4), cudaMemcpyDeviceToHost, L.stream));
+    if (amp) OFC_CUDA(cudaMemcpyAsync(amp, a, N * F * sizeof(float), cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+    for (size_t i = 0; i < N * F; i++) {
+      if (r_re) r_re[i] = h4[i].x;
+      if (r_im) r_im[i] = h4[i].y;
+      if (gx) gx[i] = h4[i].z;
+      if (gy) gy[i] = h4[i].w;
+    }
+  });
+}
+
+int ofc_test_responses(ofc_engine* e, const float* img, size_t w, size_t h, const ofc_config* c, float* resp, char* err,
+                       size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_fine_window(w, h, *c);
+    const int W = (int)w, H = (int)h, ph = H + 2 * PAD, pw = W + 2 * PAD, F = c->n_scales * c->n_orient;
+    const size_t N = w * h, Np = (size_t)ph * pw;
+    GaborTables g = upload_gabor(L, ph, pw, *c);
+    float* d1 = L.upload("in_i1", img, N);
+    float2* T = L.get<float2>("fft_T", Np);
+    float2* U = L.get<float2>("fft_U", Np * F);
+    float2* R = L.get<float2>("resp", Np * F);
+    launch_fft_rows_fwd_real(d1, W, H, L.plan(pw), ph, T, L.stream);
+    launch_fft_cols_filters(T, L.plan(ph), pw, g, U, L.stream);
+    launch_fft_rows_inv_resp(U, L.plan(pw), ph, F, R, L.stream);
+    OFC_CUDA(cudaMemcpyAsync(resp, R, Np * F * sizeof(float2), cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+  });
+}
+
+int ofc_test_local_solve(ofc_engine* e, const double* sums, const double* ux, const double* uy, size_t w, size_t h,
+                         const ofc_config* c, double* oux, double* ouy, double* energy, double* resid, double* slope,
+                         char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    const int W = (int)w, H = (int)h;
+    const size_t N = w * h;
+    std::vector<double> kw = gauss_kernel(c->sigma_w);
+    int rw = (int)kw.size() / 2, K = 2 * rw + 1;
+    std::vector<double> mt((size_t)5 * K);
+    for (int p = 0; p < 5; p++)
+      for (int t = -rw; t <= rw; t++) mt[(size_t)p * K + t + rw] = kw[t + rw] * std::pow((double)t, p);
+    double* d_mt = L.upload("taps_w", mt.data(), mt.size());
+    double* ds = L.upload("sums", sums, 7 * N);
+    double* u2 = L.get<double>("u2", 2 * N);
+    OFC_CUDA(cudaMemcpyAsync(u2, ux, N * 8, cudaMemcpyHostToDevice, L.stream));
+    OFC_CUDA(cudaMemcpyAsync(u2 + N, uy, N * 8, cudaMemcpyHostToDevice, L.stream));
+    double* o2 = L.get<double>("u2b", 2 * N);
+    double* en = L.get<double>("energy", N);
+    double* rs = L.get<double>("resid", N);
+    double* sl = L.get<double>("slope", 4 * N);
+    double* yp = L.get<double>("yplanes", (size_t)moment_yplanes(c->shape_order) * N);
+    EnergyStats* stats = L.get<EnergyStats>("stats", 1);
+    unsigned long long* hist = L.get<unsigned long long>("hist", 4096);
+    OFC_CUDA(cudaMemsetAsync(hist, 0, 4096 * sizeof(unsigned long long), L.stream));
+    launch_moments_solve(ds, u2, u2 + N, W, H, c->shape_order, d_mt, rw, yp, o2, o2 + N, en, rs, sl, L.stream);
+    launch_energy_stats(en, N, stats, false, L.stream);
+    launch_median(en, N, stats, hist, L.stream);
+    launch_reset(en, u2, u2 + N, (int)N, stats, o2, o2 + N, rs, sl, L.stream);
+    OFC_CUDA(cudaMemcpyAsync(oux, o2, N * 8, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaMemcpyAsync(ouy, o2 + N, N * 8, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaMemcpyAsync(energy, en, N * 8, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaMemcpyAsync(resid, rs, N * 8, cudaMemcpyDeviceToHost, L.stream));
+    if (slope) OFC_CUDA(cudaMemcpyAsync(slope, sl, 4 * N * 8, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+  });
+}
+
+int ofc_test_median(ofc_engine* e, const double* v, size_t n, double* median, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    if (n == 0) throw Error(OFC_ERR_ARG, "empty");
+    double* d = L.upload("t_med", v, n);
+    EnergyStats* stats = L.get<EnergyStats>("stats", 1);
+    unsigned long long* hist = L.get<unsigned long long>("hist", 4096);
+    OFC_CUDA(cudaMemsetAsync(hist, 0, 4096 * sizeof(unsigned long long), L.stream));
+    launch_energy_stats(d, n, stats, true, L.stream);
+    launch_median(d, n, stats, hist, L.stream);
+    EnergyStats hs;
+    OFC_CUDA(cudaMemcpyAsync(&hs, stats, sizeof(hs), cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+    *median = hs.median;
+  });
+}
+
+int ofc_test_large_components(ofc_engine* e, const uint8_t* b, size_t w, size_t h, double min_area, uint8_t* out,
+                              char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    const size_t N = w * h;
+    uint8_t* d = L.upload("t_cc", b, N);
+    uint8_t* o = L.get<uint8_t>("fin_big", N);
+    int* parent = L.get<int>("fin_parent", N);
+    int* size = L.get<int>("fin_size", N);
+    launch_large_components(d, (int)w, (int)h, min_area, parent, size, o, L.stream);
+    OFC_CUDA(cudaMemcpyAsync(out, o, N, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+  });
+}
+
+int ofc_test_prewarp_fill(ofc_engine* e, const uint8_t* low, const double* ux, const double* uy, const double* slope,
+                          size_t w, size_t h, double radius, double* oux, double* ouy, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    const size_t N = w * h;
+    const int W = (int)w, H = (int)h;
+    uint8_t* dl = L.upload("t_low", low, N);
+    double* u2 = L.get<double>("u2", 2 * N);
+    OFC_CUDA(cudaMemcpyAsync(u2, ux, N * 8, cudaMemcpyHostToDevice, L.stream));
+    OFC_CUDA(cudaMemcpyAsync(u2 + N, uy, N * 8, cudaMemcpyHostToDevice, L.stream));
+    double* sl = L.upload("slope", slope, 4 * N);
+    PrewarpCounts* counts = L.get<PrewarpCounts>("pw_counts", 2);
+    int nlow = 0;
+    for (size_t i = 0; i < N; i++) nlow += low[i] ? 1 : 0;
+    OFC_CUDA(cudaMemcpyAsync(&counts[0].low, &nlow, sizeof(int), cudaMemcpyHostToDevice, L.stream));
+    uint8_t* okm = L.get<uint8_t>("okmask", N);
+    int* vdist = L.get<int>("vdist", N);
+    int* cold2 = L.get<int>("col_d2", N);
+    int* colrow = L.get<int>("col_row", N);
+    double* pre2 = L.get<double>("pre2", 2 * N);
+    launch_prewarp_fill(dl, u2, u2 + N, sl, W, H, radius, &counts[0], okm, vdist, cold2, colrow, pre2, pre2 + N,
+                        L.stream);
+    OFC_CUDA(cudaMemcpyAsync(oux, pre2, N * 8, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaMemcpyAsync(ouy, pre2 + N, N * 8, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+  });
+}
+
+int ofc_test_first_sums(ofc_engine* e, const float* i1, const float* i2, size_t w, size_t h, const double* ux,
+                        const double* uy, const ofc_config* c, double* sums, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_fine_window(w, h, *c);
+    const int W = (int)w, H = (int)h, ph = H + 2 * PAD, pw = W + 2 * PAD, F = c->n_scales * c->n_orient;
+    const size_t N = w * h, Np = (size_t)ph * pw;
+    cudaStream_t st = L.stream;
+    GaborTables g = upload_gabor(L, ph, pw, *c);
+    float* d1 = L.upload("in_i1", i1, N);
+    float* d2 = L.upload("in_i2", i2, N);
+    double* u2 = L.get<double>("u2", 2 * N);
+    OFC_CUDA(cudaMemcpyAsync(u2, ux, N * 8, cudaMemcpyHostToDevice, st));
+    OFC_CUDA(cudaMemcpyAsync(u2 + N, uy, N * 8, cudaMemcpyHostToDevice, st));
+    float2* T = L.get<float2>("fft_T", Np);
+    float2* U = L.get<float2>("fft_U", Np * F);
+    float4* ref4 = L.get<float4>("ref4", N * F);
+    float* amp = L.get<float>("ref_amp", N * F);
+    reference_pack(L, d1, W, H, g, ref4, amp);
+    float* c2 = L.get<float>("spline2", N);
+    double* tmp2 = L.get<double>("spline2_tmp", 2 * N);
+    launch_bspline_f32(d2, c2, tmp2, W, H, st);
+    std::vector<double> ks = gauss_kernel(c->sigma_s);
+    double* d_ks = L.upload("taps_s", ks.data(), ks.size());
+    double* s2 = L.get<double>("s2", 2 * N);
+    double* cs2 = L.get<double>("cs2", 2 * N);
+    double* tmpb = L.get<double>("blur_tmp", 2 * N);
+    launch_corr_y(u2, tmpb, 2, W, H, d_ks, (int)ks.size() / 2, st);
+    launch_corr_x(tmpb, s2, 2, W, H, d_ks, (int)ks.size() / 2, st);
+    float* warped = L.get<float>("warped", N);
+    launch_warp(c2, W, H, s2, s2 + N, 0, 0, W, H, warped, st);
+    float2* R = L.get<float2>("resp", Np * F);
+    launch_fft_rows_fwd_real(warped, W, H, L.plan(pw), ph, T, st);
+    launch_fft_cols_filters(T, L.plan(ph), pw, g, U, st);
+    launch_fft_rows_inv_resp(U, L.plan(pw), ph, F, R, st);
+    launch_bspline_f64(s2, cs2, tmpb, 2, W, H, st);
+    double* ds = L.get<double>("sums", 7 * N);
+    launch_accumulate(ref4, amp, R, F, ph, pw, u2, u2 + N, s2, s2 + N, cs2, cs2 + N, W, H, ds, st);
+    OFC_CUDA(cudaMemcpyAsync(sums, ds, 7 * N * 8, cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,72 @@
+// fft.cuh -- arbitrary-length FP32 FFTs staged in shared memory, fused with the Gabor filter bank and the
+// cubic B-spline prefilter (the "responses" of the fine stage, python/optflow_ref/phaseflow.py:455-456).
+#pragma once
+#include "common.cuh"
+
+namespace ofc {
+
+constexpr int FFT_MAXST = 16;
+constexpr int FFT_E = 8;       // complex values per thread (sets the threads of a block)
+constexpr int FFT_TMAX = 512;  // threads per block at most
+
+// A 1-D plan of length L: mixed-radix Stockham stages (radix p[i], stride s[i] = product of the radices
+// before it) and the twiddle table W[t] = exp(-2 pi i t / L), t < L, rounded from float64.
+struct FftPlan {
+  int L = 0;
+  int nst = 0;
+  int p[FFT_MAXST] = {};
+  int s[FFT_MAXST] = {};
+  const float2* tw = nullptr;
+  const double2* twd = nullptr;  // the same table in float64
+};
+
+// radices with a register-resident butterfly; a length with any other prime factor is refused
+bool fft_supported(int L);
+// whether the column and row passes of a ph x pw padded window fit in shared memory
+bool fft_fits(int ph, int pw);
+// host: factor L and fill p/s; tw is set by the caller (device table of L values)
+FftPlan fft_make_plan(int L);
+std::vector<float2> fft_twiddles(int L);
+std::vector<double2> fft_twiddles_f64(int L);
+// threads of a block that transforms C interleaved lines of length L (multiple of C and of 32)
+int fft_threads(int L, int C);
+
+// Separable Gabor tables of one padded size (gabor_bank, phaseflow.py:73-89), float64 on the device:
+//   fx[pw], fy[ph]: the frequency grids (np.fft.fftfreq * 2 pi)
+//   hx[pw], hy[ph]: exp(-f^2 s_hp^2 / 2), so the DC high-pass is 1 - hx[x] hy[y]
+//   ex[F][pw], ey[F][ph]: the separable factors of filter k's Gaussian
+struct GaborTables {
+  int F = 0, ph = 0, pw = 0;
+  const double* fx = nullptr;
+  const double* fy = nullptr;
+  const double* hx = nullptr;
+  const double* hy = nullptr;
+  const double* ex = nullptr;
+  const double* ey = nullptr;
+};
+std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c);  // layout as above, contiguous
+
+// forward row transforms of the reflect-padded real image img (W x H) -> out (ph x pw), float32 or float64
+void launch_fft_rows_fwd_real(const float* img, int W, int H, const FftPlan& plw, int ph, float2* out,
+                              cudaStream_t st);
+void launch_fft_rows_fwd_real_f64(const float* img, int W, int H, const FftPlan& plw, int ph, double2* out,
+                                  cudaStream_t st);
+// column transforms of the responses: forward, then per filter multiply + inverse + B-spline prefilter along y
+// -> U: F planes (ph x pw)
+void launch_fft_cols_filters(const float2* T, const FftPlan& plh, int pw, const GaborTables& g, float2* U,
+                             cudaStream_t st);
+// column transforms of the reference pack in float64 for filters [k0, k1): 3 planes per filter
+// (S G, S G i fx, S G i fy), inverse along y
+void launch_fft_cols_ref_f64(const double2* T, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1,
+                             double2* U, cudaStream_t st);
+// inverse row transforms + B-spline prefilter along x + scale -> responses R (F planes of ph x pw)
+void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F, float2* R, cudaStream_t st);
+// inverse row transforms of the reference planes of filters [k0, k1), cropped to W x H: per filter
+// (r.re, r.im, gx, gy) and amp (reference_phase, phaseflow.py:100-111), formed in float64, stored float32
+void launch_fft_rows_inv_ref_f64(const double2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,
+                                 float4* ref4, float* amp, cudaStream_t st);
+
+// generic complex FFT of C-line batches held in global memory (tests and tools): data (lines x L)
+void launch_fft_lines(float2* data, int lines, const FftPlan& pl, bool inverse, cudaStream_t st);
+
+}  // namespace ofc

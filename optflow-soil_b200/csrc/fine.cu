@@ -1,0 +1,839 @@
+// fine.cu -- the per-pixel kernels of the fine stage (python/optflow_ref/phaseflow.py:427-511,
+// rust/crates/optflow-core/src/phaseflow.rs:1514-1613): smoothing, splines, warp, accumulate, window moments
+// and the local solve, the energy median, the confidence and the trusted pre-warp.
+#include <cfloat>
+
+#include "kernels.cuh"
+
+namespace ofc {
+
+// ---------------------------------------------------------------- separable correlation ("nearest")
+template <class Tin>
+__global__ void k_corr_y(const Tin* __restrict__ in, double* __restrict__ out, int W, int H,
+                         const double* __restrict__ taps, int r) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
+  int pl = blockIdx.z;
+  if (x >= W) return;
+  const Tin* a = in + (size_t)pl * W * H;
+  double s = 0;
+  for (int j = -r; j <= r; j++) {
+    int yy = min(max(y + j, 0), H - 1);
+    s += taps[j + r] * (double)a[(size_t)yy * W + x];
+  }
+  out[(size_t)pl * W * H + (size_t)y * W + x] = s;
+}
+
+__global__ void k_corr_x(const double* __restrict__ in, double* __restrict__ out, int W, int H,
+                         const double* __restrict__ taps, int r) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
+  int pl = blockIdx.z;
+  if (x >= W) return;
+  const double* a = in + (size_t)pl * W * H + (size_t)y * W;
+  double s = 0;
+  for (int j = -r; j <= r; j++) {
+    int xx = min(max(x + j, 0), W - 1);
+    s += taps[j + r] * a[xx];
+  }
+  out[(size_t)pl * W * H + (size_t)y * W + x] = s;
+}
+
+void launch_corr_y(const double* in, double* out, int n_planes, int W, int H, const double* taps, int r, cudaStream_t st) {
+  dim3 g(div_up(W, 128), H, n_planes);
+  OFC_LAUNCH(k_corr_y<double>, g, 128, 0, st, in, out, W, H, taps, r);
+}
+void launch_corr_x(const double* in, double* out, int n_planes, int W, int H, const double* taps, int r, cudaStream_t st) {
+  dim3 g(div_up(W, 128), H, n_planes);
+  OFC_LAUNCH(k_corr_x, g, 128, 0, st, in, out, W, H, taps, r);
+}
+void launch_corr_y_f32in(const float* in, double* out, int W, int H, const double* taps, int r, cudaStream_t st) {
+  dim3 g(div_up(W, 128), H, 1);
+  OFC_LAUNCH(k_corr_y<float>, g, 128, 0, st, in, out, W, H, taps, r);
+}
+
+// ---------------------------------------------------------------- B-spline prefilter in global memory
+// Segmented recursive filter along one axis (interp.py:13-27): a line of length n with element stride
+// `es`, lines `ls` apart. Each thread filters one segment of one line, entering it after a warm-up of
+// IIR_WARM samples (exact when the warm-up reaches the line's start/end). Causal: in -> y (times 6);
+// anticausal: y -> out.
+constexpr int SEG = 32;
+
+template <class Tin>
+__global__ void k_iir_causal(const Tin* __restrict__ in, double* __restrict__ y, int n, int nlines, long es, long ls,
+                             long plane) {
+  int line = blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= nlines) return;
+  const int s0 = blockIdx.y * SEG;
+  if (s0 >= n) return;
+  const int e0 = min(n, s0 + SEG);
+  const Tin* a = in + (size_t)blockIdx.z * plane + (size_t)line * ls;
+  double* o = y + (size_t)blockIdx.z * plane + (size_t)line * ls;
+  if (n == 1) { o[0] = (double)a[0]; return; }
+  const double z = bspline_z();
+  double acc;
+  int i0;
+  if (s0 - IIR_WARM <= 0) {
+    int hz = min(n, HORIZON);
+    acc = 0;
+    double zk = 1;
+    for (int k = 0; k < hz; k++) { acc += zk * (6.0 * (double)a[(size_t)k * es]); zk *= z; }
+    if (s0 == 0) o[0] = acc;
+    for (int i = 1; i < s0; i++) acc = 6.0 * (double)a[(size_t)i * es] + z * acc;
+    i0 = s0 == 0 ? 1 : s0;
+  } else {
+    acc = 0;
+    for (int i = s0 - IIR_WARM; i < s0; i++) acc = 6.0 * (double)a[(size_t)i * es] + z * acc;
+    i0 = s0;
+  }
+  for (int i = i0; i < e0; i++) {
+    acc = 6.0 * (double)a[(size_t)i * es] + z * acc;
+    o[(size_t)i * es] = acc;
+  }
+}
+
+template <class Tout>
+__global__ void k_iir_anticausal(const double* __restrict__ y, Tout* __restrict__ out, int n, int nlines, long es,
+                                 long ls, long plane) {
+  int line = blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= nlines) return;
+  const int s0 = blockIdx.y * SEG;
+  if (s0 >= n) return;
+  const int e0 = min(n, s0 + SEG);
+  const double* a = y + (size_t)blockIdx.z * plane + (size_t)line * ls;
+  Tout* o = out + (size_t)blockIdx.z * plane + (size_t)line * ls;
+  if (n == 1) { o[0] = (Tout)a[0]; return; }
+  const double z = bspline_z();
+  const double g = z / (z * z - 1.0);
+  double c;
+  if (e0 + IIR_WARM >= n - 1) {
+    c = g * (a[(size_t)(n - 1) * es] + z * a[(size_t)(n - 2) * es]);
+    if (e0 == n) o[(size_t)(n - 1) * es] = (Tout)c;
+    for (int i = n - 2; i >= e0; i--) c = z * (c - a[(size_t)i * es]);
+    if (e0 == n) {
+      for (int i = n - 2; i >= s0; i--) { c = z * (c - a[(size_t)i * es]); o[(size_t)i * es] = (Tout)c; }
+      return;
+    }
+  } else {
+    c = 0;
+    for (int i = e0 + IIR_WARM; i >= e0; i--) c = z * (c - a[(size_t)i * es]);
+  }
+  // c = c[e0]
+  for (int i = e0 - 1; i >= s0; i--) { c = z * (c - a[(size_t)i * es]); o[(size_t)i * es] = (Tout)c; }
+}
+
+template <class Tin, class Tout>
+static void bspline_axes(const Tin* in, Tout* out, double* tmp, double* tmp2, int n_planes, int W, int H, cudaStream_t st) {
+  long plane = (long)W * H;
+  // along y: lines = columns (stride 1 apart), element stride W
+  dim3 gy(div_up(W, 128), div_up(H, SEG), n_planes);
+  OFC_LAUNCH((k_iir_causal<Tin>), gy, 128, 0, st, in, tmp, H, W, (long)W, 1L, plane);
+  OFC_LAUNCH((k_iir_anticausal<double>), gy, 128, 0, st, tmp, tmp2, H, W, (long)W, 1L, plane);
+  // along x: lines = rows (W apart), element stride 1
+  dim3 gx(div_up(H, 128), div_up(W, SEG), n_planes);
+  OFC_LAUNCH((k_iir_causal<double>), gx, 128, 0, st, tmp2, tmp, W, H, 1L, (long)W, plane);
+  OFC_LAUNCH((k_iir_anticausal<Tout>), gx, 128, 0, st, tmp, out, W, H, 1L, (long)W, plane);
+}
+
+void launch_bspline_f64(const double* in, double* out, double* tmp, int n_planes, int W, int H, cudaStream_t st) {
+  // out doubles as the second scratch plane set (written last)
+  bspline_axes<double, double>(in, out, tmp, out, n_planes, W, H, st);
+}
+
+void launch_bspline_f32(const float* in, float* out, double* tmp, int W, int H, cudaStream_t st) {
+  // tmp holds 2 planes
+  bspline_axes<float, float>(in, out, tmp, tmp + (size_t)W * H, 1, W, H, st);
+}
+
+// ---------------------------------------------------------------- warp
+__global__ void k_warp(const float* __restrict__ c2, int w2, int h2, const double* __restrict__ sx,
+                       const double* __restrict__ sy, long shx, long shy, int W, int H, float* __restrict__ out) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
+  if (x >= W) return;
+  size_t p = (size_t)y * W + x;
+  Taps t;
+  double v;
+  if (make_taps(((double)x + (double)shx) + sx[p], ((double)y + (double)shy) + sy[p], w2, h2, t))
+    v = sample_real(c2, w2, t);
+  else
+    v = nan("");
+  out[p] = (float)v;
+}
+
+void launch_warp(const float* c2, int w2, int h2, const double* sx, const double* sy, long shx, long shy, int W, int H,
+                 float* out, cudaStream_t st) {
+  dim3 g(div_up(W, 128), H);
+  OFC_LAUNCH(k_warp, g, 128, 0, st, c2, w2, h2, sx, sy, shx, shy, W, H, out);
+}
+
+// ---------------------------------------------------------------- accumulate
+__global__ void __launch_bounds__(128) k_accumulate(const float4* __restrict__ ref4, const float* __restrict__ amp,
+                                                    const float2* __restrict__ R, int F, int ph, int pw,
+                                                    const double* __restrict__ ux, const double* __restrict__ uy,
+                                                    const double* __restrict__ sx, const double* __restrict__ sy,
+                                                    const double* __restrict__ csx, const double* __restrict__ csy,
+                                                    int W, int H, double* __restrict__ sums) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
+  if (x >= W) return;
+  const size_t N = (size_t)W * H;
+  const size_t p = (size_t)y * W + x;
+  const double u = ux[p], v = uy[p];
+  const double tx = x + u, ty = y + v;
+  double px = tx - sx[p], py = ty - sy[p];
+  // X' + s(X') = X + u(X): two fixed-point steps on the spline of s (phaseflow.py:469-472)
+  for (int it = 0; it < 2; it++) {
+    Taps t;
+    double nx, ny;
+    if (make_taps(px, py, W, H, t)) {
+      nx = tx - sample_real(csx, W, t);
+      ny = ty - sample_real(csy, W, t);
+    } else {
+      nx = ny = nan("");
+    }
+    px = nx;
+    py = ny;
+  }
+  double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
+  Taps t;
+  bool ok = make_taps(px + PAD, py + PAD, pw, ph, t);
+  const size_t plane = (size_t)ph * pw;
+  for (int k = 0; k < F; k++) {
+    float4 r1 = __ldg(ref4 + (size_t)k * N + p);
+    double a1k = (double)__ldg(amp + (size_t)k * N + p);
+    double br, bi;
+    if (ok) {
+      float2 r2 = sample_c32(R + (size_t)k * plane, pw, t);
+      br = r2.x;
+      bi = r2.y;
+    } else {
+      br = bi = nan("");
+    }
+    // r1 conj(r2)
+    double re = (double)r1.x * br + (double)r1.y * bi;
+    double im = (double)r1.y * br - (double)r1.x * bi;
+    double dphi = atan2(im, re);
+    double wk = a1k * sqrt(br * br + bi * bi);
+    double gx = r1.z, gy = r1.w;
+    double c = dphi + gx * u + gy * v;
+    a0 += wk * gx * gx;
+    a1 += wk * gx * gy;
+    a2 += wk * gy * gy;
+    a3 += wk * gx * c;
+    a4 += wk * gy * c;
+    a5 += wk * c * c;
+    a6 += wk;
+  }
+  sums[p] = a0;
+  sums[N + p] = a1;
+  sums[2 * N + p] = a2;
+  sums[3 * N + p] = a3;
+  sums[4 * N + p] = a4;
+  sums[5 * N + p] = a5;
+  sums[6 * N + p] = a6;
+}
+
+void launch_accumulate(const float4* ref4, const float* amp, const float2* R, int F, int ph, int pw, const double* ux,
+                       const double* uy, const double* sx, const double* sy, const double* csx, const double* csy,
+                       int W, int H, double* sums, cudaStream_t st) {
+  dim3 g(div_up(W, 128), H);
+  OFC_LAUNCH(k_accumulate, g, 128, 0, st, ref4, amp, R, F, ph, pw, ux, uy, sx, sy, csx, csy, W, H, sums);
+}
+
+// ---------------------------------------------------------------- window moments + solve
+// The moments a shape function of order 1 or 2 needs (phaseflow.py:123-161), resolved at compile time:
+// sources 0..6 = gxx gxy gyy gxc gyc gcc gw; a moment is (source, px, py); the y pass makes (source, py).
+struct MomTable {
+  int n = 0, ny = 0, nm = 0;
+  int ysrc[32] = {}, ypow[32] = {};
+  int mjob[64] = {}, mpx[64] = {};
+  int Midx[144] = {}, bidx[12] = {};
+  int gcc = 0, gw = 0;
+};
+
+__host__ __device__ constexpr MomTable build_table(int order) {
+  MomTable T{};
+  int uc[12] = {}, ux_[12] = {}, uy_[12] = {};
+  int pw1[6][2] = {{0, 0}, {1, 0}, {0, 1}, {2, 0}, {1, 1}, {0, 2}};
+  int npw = order == 1 ? 3 : 6;
+  int n = 0;
+  uc[n] = 0; ux_[n] = 0; uy_[n] = 0; n++;
+  uc[n] = 1; ux_[n] = 0; uy_[n] = 0; n++;
+  for (int i = 1; i < npw; i++)
+    for (int c = 0; c < 2; c++) { uc[n] = c; ux_[n] = pw1[i][0]; uy_[n] = pw1[i][1]; n++; }
+  T.n = n;
+  // moment list
+  int msrc[64] = {}, mx[64] = {}, my[64] = {};
+  int nm = 0;
+  auto find_or_add = [&](int s, int px, int py) {
+    for (int i = 0; i < nm; i++)
+      if (msrc[i] == s && mx[i] == px && my[i] == py) return i;
+    msrc[nm] = s; mx[nm] = px; my[nm] = py;
+    return nm++;
+  };
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) {
+      int a = uc[i] < uc[j] ? uc[i] : uc[j], b = uc[i] < uc[j] ? uc[j] : uc[i];
+      int key = a == 0 ? (b == 0 ? 0 : 1) : 2;
+      T.Midx[i * n + j] = find_or_add(key, ux_[i] + ux_[j], uy_[i] + uy_[j]);
+    }
+  for (int i = 0; i < n; i++) T.bidx[i] = find_or_add(3 + uc[i], ux_[i], uy_[i]);
+  T.gcc = find_or_add(5, 0, 0);
+  T.gw = find_or_add(6, 0, 0);
+  T.nm = nm;
+  int ny = 0;
+  for (int m = 0; m < nm; m++) {
+    int j = -1;
+    for (int q = 0; q < ny; q++)
+      if (T.ysrc[q] == msrc[m] && T.ypow[q] == my[m]) j = q;
+    if (j < 0) { T.ysrc[ny] = msrc[m]; T.ypow[ny] = my[m]; j = ny++; }
+    T.mjob[m] = j;
+    T.mpx[m] = mx[m];
+  }
+  T.ny = ny;
+  return T;
+}
+
+int moment_yplanes(int order) { return build_table(order).ny; }
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_moments_y(const double* __restrict__ sums, int W, int H,
+                                                   const double* __restrict__ mtaps, int r,
+                                                   double* __restrict__ yplanes) {
+  constexpr MomTable T = build_table(ORDER);
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
+  if (x >= W) return;
+  const size_t N = (size_t)W * H;
+  const int K = 2 * r + 1;
+  double acc[T.ny];
+#pragma unroll
+  for (int j = 0; j < T.ny; j++) acc[j] = 0;
+  for (int t = -r; t <= r; t++) {
+    int yy = min(max(y + t, 0), H - 1);
+    size_t q = (size_t)yy * W + x;
+    double s[7];
+#pragma unroll
+    for (int i = 0; i < 7; i++) s[i] = sums[i * N + q];
+#pragma unroll
+    for (int j = 0; j < T.ny; j++) acc[j] += mtaps[T.ypow[j] * K + t + r] * s[T.ysrc[j]];
+  }
+  size_t p = (size_t)y * W + x;
+#pragma unroll
+  for (int j = 0; j < T.ny; j++) yplanes[j * N + p] = acc[j];
+}
+
+template <int N>
+__device__ bool cholesky_solve_dev(double (&M)[N * N], double (&b)[N]) {
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    double d = M[j * N + j];
+#pragma unroll
+    for (int k = 0; k < j; k++) d -= M[j * N + k] * M[j * N + k];
+    if (!(d > 0.0 && d <= DBL_MAX)) return false;
+    double l = sqrt(d);
+    M[j * N + j] = l;
+#pragma unroll
+    for (int i = j + 1; i < N; i++) {
+      double s = M[i * N + j];
+#pragma unroll
+      for (int k = 0; k < j; k++) s -= M[i * N + k] * M[j * N + k];
+      M[i * N + j] = s / l;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    double s = b[i];
+#pragma unroll
+    for (int k = 0; k < i; k++) s -= M[i * N + k] * b[k];
+    b[i] = s / M[i * N + i];
+  }
+#pragma unroll
+  for (int i = N - 1; i >= 0; i--) {
+    double s = b[i];
+#pragma unroll
+    for (int k = i + 1; k < N; k++) s -= M[k * N + i] * b[k];
+    b[i] = s / M[i * N + i];
+  }
+  bool fin = true;
+#pragma unroll
+  for (int i = 0; i < N; i++) fin &= isfinite(b[i]);
+  return fin;
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_moments_x_solve(const double* __restrict__ yplanes,
+                                                         const double* __restrict__ uxin,
+                                                         const double* __restrict__ uyin, int W, int H,
+                                                         const double* __restrict__ mtaps, int r,
+                                                         double* __restrict__ oux, double* __restrict__ ouy,
+                                                         double* __restrict__ energy, double* __restrict__ resid,
+                                                         double* __restrict__ slope) {
+  constexpr MomTable T = build_table(ORDER);
+  constexpr int n = ORDER == 1 ? 6 : 12;
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
+  if (x >= W) return;
+  const size_t N = (size_t)W * H;
+  const int K = 2 * r + 1;
+  double m[T.nm];
+#pragma unroll
+  for (int i = 0; i < T.nm; i++) m[i] = 0;
+  const double* row = yplanes + (size_t)y * W;
+  for (int t = -r; t <= r; t++) {
+    int xx = min(max(x + t, 0), W - 1);
+    double yv[T.ny];
+#pragma unroll
+    for (int j = 0; j < T.ny; j++) yv[j] = row[j * N + xx];
+#pragma unroll
+    for (int i = 0; i < T.nm; i++) m[i] += mtaps[T.mpx[i] * K + t + r] * yv[T.mjob[i]];
+  }
+  const size_t p = (size_t)y * W + x;
+  double M[n * n], b[n], b0[n];
+#pragma unroll
+  for (int i = 0; i < n * n; i++) M[i] = m[T.Midx[i]];
+#pragma unroll
+  for (int i = 0; i < n; i++) b0[i] = b[i] = m[T.bidx[i]];
+  const double m00 = M[0], m11 = M[n + 1], m01 = M[1];
+  const double e = m00 + m11;
+  const double det2 = m00 * m11 - m01 * m01;
+  energy[p] = e;
+  bool ok = det2 > APERTURE_TOL * e * e;
+  if (ok) {
+    double tr = 0;
+#pragma unroll
+    for (int i = 0; i < n; i++) tr += M[i * n + i];
+    double ridge = 1e-12 * tr / n;
+#pragma unroll
+    for (int i = 0; i < n; i++) M[i * n + i] += ridge;
+    ok = cholesky_solve_dev<n>(M, b);
+  }
+  if (ok) {
+    double fit = 0;
+#pragma unroll
+    for (int i = 0; i < n; i++) fit += b[i] * b0[i];
+    double rr = m[T.gcc] - fit;
+    resid[p] = sqrt(fmax(rr, 0.0) / (m[T.gw] + 1e-30));
+    oux[p] = b[0];
+    ouy[p] = b[1];
+#pragma unroll
+    for (int i = 0; i < 4; i++) slope[i * N + p] = b[2 + i];
+  } else {
+    resid[p] = PI;
+    oux[p] = uxin[p];
+    ouy[p] = uyin[p];
+#pragma unroll
+    for (int i = 0; i < 4; i++) slope[i * N + p] = 0.0;
+  }
+}
+
+void launch_moments_solve(const double* sums, const double* ux, const double* uy, int W, int H, int order,
+                          const double* mtaps, int r, double* yplanes, double* oux, double* ouy, double* energy,
+                          double* resid, double* slope, cudaStream_t st) {
+  dim3 g(div_up(W, 128), H);
+  if (order == 1) {
+    OFC_LAUNCH(k_moments_y<1>, g, 128, 0, st, sums, W, H, mtaps, r, yplanes);
+    OFC_LAUNCH(k_moments_x_solve<1>, g, 128, 0, st, yplanes, ux, uy, W, H, mtaps, r, oux, ouy, energy, resid, slope);
+  } else {
+    OFC_LAUNCH(k_moments_y<2>, g, 128, 0, st, sums, W, H, mtaps, r, yplanes);
+    OFC_LAUNCH(k_moments_x_solve<2>, g, 128, 0, st, yplanes, ux, uy, W, H, mtaps, r, oux, ouy, energy, resid, slope);
+  }
+}
+
+// ---------------------------------------------------------------- energy statistics and median
+__device__ __forceinline__ unsigned long long okey(double v) {  // order-preserving key of a double
+  unsigned long long u = (unsigned long long)__double_as_longlong(v);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ULL);
+}
+__device__ __forceinline__ double okey_inv(unsigned long long k) {
+  unsigned long long u = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFULL) : ~k;
+  return __longlong_as_double((long long)u);
+}
+
+__device__ double atomic_min_d(double* a, double v) {
+  unsigned long long* p = (unsigned long long*)a;
+  unsigned long long old = *p, assumed;
+  while (v < __longlong_as_double(old)) {
+    assumed = old;
+    old = atomicCAS(p, assumed, __double_as_longlong(v));
+    if (old == assumed) break;
+  }
+  return __longlong_as_double(old);
+}
+__device__ double atomic_max_d(double* a, double v) {
+  unsigned long long* p = (unsigned long long*)a;
+  unsigned long long old = *p, assumed;
+  while (v > __longlong_as_double(old)) {
+    assumed = old;
+    old = atomicCAS(p, assumed, __double_as_longlong(v));
+    if (old == assumed) break;
+  }
+  return __longlong_as_double(old);
+}
+
+__global__ void k_stats_init(EnergyStats* s) {
+  s->lo = DBL_MAX;
+  s->hi = -DBL_MAX;
+  s->nan = 0;
+}
+
+__global__ void k_energy_stats(const double* __restrict__ e, size_t n, EnergyStats* s) {
+  double lo = DBL_MAX, hi = -DBL_MAX;
+  int nan = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double v = e[i];
+    if (v != v) nan = 1;
+    else { lo = fmin(lo, v); hi = fmax(hi, v); }
+  }
+  for (int o = 16; o; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffff, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffff, hi, o));
+    nan |= __shfl_xor_sync(0xffffffff, nan, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_min_d(&s->lo, lo);
+    atomic_max_d(&s->hi, hi);
+    if (nan) atomicOr(&s->nan, 1);
+  }
+}
+
+// the reset needs the median unless every energy is above 1e-9 max + 1e-30 (phaseflow.rs:846-854)
+__global__ void k_stats_decide(EnergyStats* s, int force, size_t n) {
+  bool skip = !s->nan && s->hi <= DBL_MAX / 2 && s->lo > 1e-9 * s->hi + 1e-30;
+  s->skip_reset = skip ? 1 : 0;
+  s->need_median = (force || !skip) ? 1 : 0;
+  s->median = s->nan ? nan("") : 0.0;
+  s->prefix = 0;
+  s->rank = (long long)(n / 2);
+  s->less = 0;
+}
+
+void launch_energy_stats(const double* energy, size_t n, EnergyStats* stats, bool force_median, cudaStream_t st) {
+  OFC_LAUNCH(k_stats_init, 1, 1, 0, st, stats);
+  OFC_LAUNCH(k_energy_stats, 296, 256, 0, st, energy, n, stats);
+  OFC_LAUNCH(k_stats_decide, 1, 1, 0, st, stats, force_median ? 1 : 0, n);
+}
+
+// radix select of the element of rank stats->rank: 12-bit digits from the top, pass `pass` covers bits
+// [64 - 12 (pass + 1), 64 - 12 pass) (the last pass has 4 bits)
+constexpr int RBITS = 12, RBINS = 1 << RBITS, RPASSES = 6;
+
+__device__ __forceinline__ void digit_of(int pass, int& shift, int& bits) {
+  int hi = 64 - RBITS * pass;
+  bits = hi >= RBITS ? RBITS : hi;
+  shift = hi - bits;
+}
+
+__global__ void k_radix_hist(const double* __restrict__ e, size_t n, const EnergyStats* s, int pass,
+                             unsigned long long* __restrict__ hist) {
+  if (!s->need_median || s->nan) return;
+  __shared__ unsigned int h[RBINS];
+  for (int i = threadIdx.x; i < RBINS; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  int shift, bits;
+  digit_of(pass, shift, bits);
+  const unsigned long long prefix = s->prefix;
+  const int hib = 64 - RBITS * pass;  // bits already fixed above `hib`
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long k = okey(e[i]);
+    bool match = hib == 64 ? true : ((k >> hib) == (prefix >> hib));
+    if (match) atomicAdd(&h[(k >> shift) & ((1ULL << bits) - 1)], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < RBINS; i += blockDim.x)
+    if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
+}
+
+__global__ void k_radix_pick(EnergyStats* s, int pass, unsigned long long* hist, size_t n) {
+  // one block of 1024 threads: find the bin holding rank, then clear the histogram
+  if (!s->need_median || s->nan) return;
+  __shared__ unsigned long long part[1024];
+  const int per = RBINS / 1024;
+  unsigned long long loc = 0;
+  for (int j = 0; j < per; j++) loc += hist[threadIdx.x * per + j];
+  part[threadIdx.x] = loc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long rank = s->rank;
+    long long acc = 0;
+    int bin = -1;
+    for (int t = 0; t < 1024 && bin < 0; t++) {
+      if (acc + (long long)part[t] > rank) {
+        for (int j = 0; j < per; j++) {
+          long long c = (long long)hist[t * per + j];
+          if (acc + c > rank) { bin = t * per + j; break; }
+          acc += c;
+        }
+      } else {
+        acc += (long long)part[t];
+      }
+    }
+    int shift, bits;
+    digit_of(pass, shift, bits);
+    s->prefix |= ((unsigned long long)bin) << shift;
+    s->rank = rank - acc;
+    s->less += acc;
+  }
+  __syncthreads();
+  for (int j = 0; j < per; j++) hist[threadIdx.x * per + j] = 0;
+}
+
+// after the passes: prefix = key of the element of rank n/2; for even n the one of rank n/2 - 1 is
+// the same value when `less` (elements below it) < n/2, else the largest element below it
+__global__ void k_median_lo(const double* __restrict__ e, size_t n, EnergyStats* s) {
+  if (!s->need_median || s->nan || (n % 2) || s->less < (long long)(n / 2)) return;
+  const unsigned long long hk = s->prefix;
+  unsigned long long best = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long k = okey(e[i]);
+    if (k < hk && k > best) best = k;
+  }
+  for (int o = 16; o; o >>= 1) {
+    unsigned long long v = __shfl_xor_sync(0xffffffff, best, o);
+    best = v > best ? v : best;
+  }
+  if ((threadIdx.x & 31) == 0 && best) atomicMax((unsigned long long*)&s->lo_val, best);
+}
+
+__global__ void k_median_init(EnergyStats* s) { s->lo_val = 0; }
+
+__global__ void k_median_final(EnergyStats* s, size_t n) {
+  if (!s->need_median) return;
+  if (s->nan) { s->median = nan(""); return; }
+  double hi = okey_inv(s->prefix);
+  if (n % 2) { s->median = hi; return; }
+  double lo = hi;
+  if (s->less >= (long long)(n / 2)) {
+    unsigned long long k = *(unsigned long long*)&s->lo_val;
+    lo = okey_inv(k);
+  }
+  s->median = (lo + hi) / 2.0;
+}
+
+void launch_median(const double* energy, size_t n, EnergyStats* stats, unsigned long long* hist, cudaStream_t st) {
+  for (int pass = 0; pass < RPASSES; pass++) {
+    OFC_LAUNCH(k_radix_hist, 296, 512, 0, st, energy, n, stats, pass, hist);
+    OFC_LAUNCH(k_radix_pick, 1, 1024, 0, st, stats, pass, hist, n);
+  }
+  OFC_LAUNCH(k_median_init, 1, 1, 0, st, stats);
+  OFC_LAUNCH(k_median_lo, 296, 256, 0, st, energy, n, stats);
+  OFC_LAUNCH(k_median_final, 1, 1, 0, st, stats, n);
+}
+
+__global__ void k_reset(const double* __restrict__ energy, const double* __restrict__ uxin,
+                        const double* __restrict__ uyin, int n, const EnergyStats* s, double* ux, double* uy,
+                        double* resid, double* slope) {
+  if (s->skip_reset) return;
+  const double thr = 1e-9 * s->median + 1e-30;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    if (!(energy[p] > thr)) {
+      ux[p] = uxin[p];
+      uy[p] = uyin[p];
+      resid[p] = PI;
+      for (int i = 0; i < 4; i++) slope[(size_t)i * n + p] = 0.0;
+    }
+  }
+}
+
+void launch_reset(const double* energy, const double* ux_in, const double* uy_in, int n, const EnergyStats* stats,
+                  double* ux, double* uy, double* resid, double* slope, cudaStream_t st) {
+  OFC_LAUNCH(k_reset, div_up(n, 256), 256, 0, st, energy, ux_in, uy_in, n, stats, ux, uy, resid, slope);
+}
+
+// ---------------------------------------------------------------- confidence
+__global__ void k_confidence(const double* __restrict__ energy, const double* __restrict__ resid,
+                             const double* __restrict__ ux, const double* __restrict__ uy, int W, int H,
+                             const EnergyStats* s, double tol, double conf_min, int border, double B,
+                             float* conf_out, double* conf64, uint8_t* low, int* count_low) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
+  if (x >= W) return;
+  size_t p = (size_t)y * W + x;
+  double scale = 0.25 * s->median + 1e-30;
+  double ratio = energy[p] / scale;
+  double tex = ratio != ratio ? ratio : fmin(1.0, ratio);
+  double q = resid[p] / tol;
+  double c = tex * exp(-(q * q));
+  if (border) {
+    double tx = x + ux[p], ty = y + uy[p];
+    double own = (double)min(min(x, y), min(W - 1 - x, H - 1 - y));
+    bool rep = own >= B && tx >= B && ty >= B && (W - 1) - tx >= B && (H - 1) - ty >= B;
+    c = rep ? (c != c ? c : fmin(fmax(c, 0.0), 1.0)) : 0.0;
+  }
+  bool lw = c < conf_min;
+  if (conf_out) conf_out[p] = (float)c;
+  if (conf64) conf64[p] = c;
+  if (low) low[p] = lw ? 1 : 0;
+  if (count_low) {
+    unsigned m = __ballot_sync(__activemask(), lw);
+    if ((threadIdx.x & 31) == __ffs(__activemask()) - 1 && m) atomicAdd(count_low, __popc(m));
+  }
+}
+
+void launch_confidence(const double* energy, const double* resid, const double* ux, const double* uy, int W, int H,
+                       const EnergyStats* stats, double phase_tol, double conf_min, bool border, double B,
+                       float* conf_out, double* conf64, uint8_t* low, int* count_low, cudaStream_t st) {
+  dim3 g(div_up(W, 128), H);
+  OFC_LAUNCH(k_confidence, g, 128, 0, st, energy, resid, ux, uy, W, H, stats, phase_tol, conf_min, border ? 1 : 0, B,
+             conf_out, conf64, low, count_low);
+}
+
+// ---------------------------------------------------------------- bounded distance tests
+// vertical distance (rows) to the nearest src pixel of the column within `cap`, else cap + 1
+__global__ void k_vdist(const uint8_t* __restrict__ src, int W, int H, int cap, int* __restrict__ vd,
+                        const int* gate) {
+  if (gate && *gate == 0) return;
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
+  if (x >= W) return;
+  int best = cap + 1;
+  for (int d = 0; d <= cap && d < best; d++) {
+    if ((y - d >= 0 && src[(size_t)(y - d) * W + x]) || (y + d < H && src[(size_t)(y + d) * W + x])) best = d;
+  }
+  vd[(size_t)y * W + x] = best;
+}
+
+// squared distance from vd within cap; mode 0: out |= (d <= limit); mode 1: out = (d > limit); counts ok
+__global__ void k_within(const int* __restrict__ vd, int W, int H, int cap, double limit, int mode, uint8_t* out,
+                         const int* gate, int* count) {
+  if (gate && *gate == 0) return;
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
+  if (x >= W) return;
+  long best = -1;
+  const int* row = vd + (size_t)y * W;
+  for (int dx = -cap; dx <= cap; dx++) {
+    int xx = x + dx;
+    if (xx < 0 || xx >= W) continue;
+    int v = row[xx];
+    if (v > cap) continue;
+    long d2 = (long)dx * dx + (long)v * v;
+    if (best < 0 || d2 < best) best = d2;
+  }
+  bool inside = best >= 0 && sqrt((double)best) <= limit;
+  size_t p = (size_t)y * W + x;
+  if (mode == 0) {
+    if (inside) out[p] = 1;
+  } else {
+    bool okp = !inside;
+    out[p] = okp ? 1 : 0;
+    if (count) {
+      unsigned m = __ballot_sync(__activemask(), okp);
+      if ((threadIdx.x & 31) == __ffs(__activemask()) - 1 && m) atomicAdd(count, __popc(m));
+    }
+  }
+}
+
+void launch_within(const uint8_t* src, int W, int H, double limit, int mode, uint8_t* out, int* vdist, cudaStream_t st) {
+  int cap = (int)floor(limit) + 1;
+  dim3 g(div_up(W, 128), H);
+  OFC_LAUNCH(k_vdist, g, 128, 0, st, src, W, H, cap, vdist, (const int*)nullptr);
+  OFC_LAUNCH(k_within, g, 128, 0, st, vdist, W, H, cap, limit, mode, out, (const int*)nullptr, (int*)nullptr);
+}
+
+// ---------------------------------------------------------------- trusted pre-warp
+// column sweeps: nearest ok pixel of the column (ties to the smaller row): col_d2 = dy^2 (or -1), col_row
+__global__ void k_col_nearest(const uint8_t* __restrict__ ok, int W, int H, const PrewarpCounts* c,
+                              int* __restrict__ col_d2, int* __restrict__ col_row) {
+  if (!(c->low > 0 && c->ok > 0 && c->ok < W * H)) return;
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= W) return;
+  int last = -1;
+  for (int y = 0; y < H; y++) {
+    size_t p = (size_t)y * W + x;
+    if (ok[p]) last = y;
+    col_row[p] = last;  // nearest above (or at)
+  }
+  int next = -1;
+  for (int y = H - 1; y >= 0; y--) {
+    size_t p = (size_t)y * W + x;
+    if (ok[p]) next = y;
+    int up = col_row[p];
+    int r = -1;
+    long d = -1;
+    if (up >= 0) { r = up; d = (long)(y - up); }
+    if (next >= 0 && (r < 0 || (long)(next - y) < d)) { r = next; d = next - y; }
+    col_row[p] = r;
+    col_d2[p] = r < 0 ? -1 : (int)(d * d);
+  }
+}
+
+// for every pixel that is not ok: the nearest ok pixel (smallest (d^2, column, row)), then the first-order
+// extrapolation u(N) + grad u(N) (X - N) (phaseflow.py:346-354); ok pixels keep u
+__global__ void k_extrapolate(const uint8_t* __restrict__ ok, const int* __restrict__ col_d2,
+                              const int* __restrict__ col_row, const double* __restrict__ ux,
+                              const double* __restrict__ uy, const double* __restrict__ slope, int W, int H,
+                              const PrewarpCounts* c, double* ux_pre, double* uy_pre) {
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
+  if (x >= W) return;
+  size_t p = (size_t)y * W + x;
+  const bool apply = c->low > 0 && c->ok > 0 && c->ok < W * H;
+  if (!apply || ok[p]) {
+    ux_pre[p] = ux[p];
+    uy_pre[p] = uy[p];
+    return;
+  }
+  const int* cd = col_d2 + (size_t)y * W;
+  const int* cr = col_row + (size_t)y * W;
+  long best = -1;
+  int bc = -1;
+  for (long D = 0; D < W; D++) {
+    if (best >= 0 && D * D > best) break;
+    long xl = x - D, xr = x + D;
+    if (xl >= 0 && cd[xl] >= 0) {
+      long d2 = D * D + cd[xl];
+      if (best < 0 || d2 < best || (d2 == best && xl < bc)) { best = d2; bc = (int)xl; }
+    }
+    if (D > 0 && xr < W && cd[xr] >= 0) {
+      long d2 = D * D + cd[xr];
+      if (best < 0 || d2 < best || (d2 == best && xr < bc)) { best = d2; bc = (int)xr; }
+    }
+  }
+  int br = cr[bc];
+  size_t q = (size_t)br * W + bc;
+  size_t N = (size_t)W * H;
+  double dx = (double)x - bc, dy = (double)y - br;
+  ux_pre[p] = ux[q] + slope[q] * dx + slope[2 * N + q] * dy;
+  uy_pre[p] = uy[q] + slope[N + q] * dx + slope[3 * N + q] * dy;
+}
+
+__global__ void k_zero_counts(PrewarpCounts* c) { c->ok = 0; }
+
+void launch_prewarp_fill(const uint8_t* low, const double* ux, const double* uy, const double* slope, int W, int H,
+                         double R, PrewarpCounts* counts, uint8_t* ok, int* vdist, int* col_d2, int* col_row,
+                         double* ux_pre, double* uy_pre, cudaStream_t st) {
+  int cap = (int)floor(R) + 1;
+  dim3 g(div_up(W, 128), H);
+  OFC_LAUNCH(k_zero_counts, 1, 1, 0, st, counts);
+  // ok = distance to the nearest low pixel > R (gated on any low pixel)
+  OFC_LAUNCH(k_vdist, g, 128, 0, st, low, W, H, cap, vdist, (const int*)&counts->low);
+  OFC_LAUNCH(k_within, g, 128, 0, st, vdist, W, H, cap, R, 1, ok, (const int*)&counts->low, &counts->ok);
+  OFC_LAUNCH(k_col_nearest, div_up(W, 128), 128, 0, st, ok, W, H, counts, col_d2, col_row);
+  OFC_LAUNCH(k_extrapolate, g, 128, 0, st, ok, col_d2, col_row, ux, uy, slope, W, H, counts, ux_pre, uy_pre);
+}
+
+// ---------------------------------------------------------------- conversions
+__global__ void k_d2f(const double* in, float* out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+__global__ void k_f2d(const float* in, double* out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+__global__ void k_fill(double* p, double v, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+void launch_f64_to_f32(const double* in, float* out, size_t n, cudaStream_t st) {
+  OFC_LAUNCH(k_d2f, std::min<size_t>(div_up(n, 256), 4096), 256, 0, st, in, out, n);
+}
+void launch_f32_to_f64(const float* in, double* out, size_t n, cudaStream_t st) {
+  OFC_LAUNCH(k_f2d, std::min<size_t>(div_up(n, 256), 4096), 256, 0, st, in, out, n);
+}
+void launch_fill_f64(double* p, double v, size_t n, cudaStream_t st) {
+  OFC_LAUNCH(k_fill, std::min<size_t>(div_up(n, 256), 4096), 256, 0, st, p, v, n);
+}
+
+}  // namespace ofc

@@ -1,0 +1,125 @@
+// kernels.cuh -- launchers of the non-FFT kernels of the engine (fine.cu, select.cu, poc.cu, finish.cu).
+#pragma once
+#include "common.cuh"
+
+namespace ofc {
+
+// ---------------------------------------------------------------- fine.cu
+// separable correlation with edge replication ("nearest", scipy correlate1d) of n_planes planes at once
+// (planes are contiguous W*H blocks); taps: 2r+1 doubles on the device
+void launch_corr_y(const double* in, double* out, int n_planes, int W, int H, const double* taps, int r, cudaStream_t st);
+void launch_corr_x(const double* in, double* out, int n_planes, int W, int H, const double* taps, int r, cudaStream_t st);
+void launch_corr_y_f32in(const float* in, double* out, int W, int H, const double* taps, int r, cudaStream_t st);
+
+// cubic B-spline coefficients (interp.py:30-35) of n_planes real planes: along y, then along x;
+// in -> out (float64 or float32 storage), tmp: W*H*n_planes float64 scratch
+void launch_bspline_f64(const double* in, double* out, double* tmp, int n_planes, int W, int H, cudaStream_t st);
+void launch_bspline_f32(const float* in, float* out, double* tmp, int W, int H, cudaStream_t st);
+
+// warp (interp.py:72-76 with the window shift of phaseflow.rs:1420-1439): out(x, y) = spline2 at
+// (x + shx + sx, y + shy + sy); spline2 is w2 x h2, out W x H
+void launch_warp(const float* c2, int w2, int h2, const double* sx, const double* sy, long shx, long shy, int W, int H,
+                 float* out, cudaStream_t st);
+
+// the seven per-pixel sums of an inner iteration (phaseflow.py:468-483); ref4/amp: F planes W x H;
+// R: F response planes (ph x pw); sums: 7 planes W x H
+void launch_accumulate(const float4* ref4, const float* amp, const float2* R, int F, int ph, int pw,
+                       const double* ux, const double* uy, const double* sx, const double* sy, const double* csx,
+                       const double* csy, int W, int H, double* sums, cudaStream_t st);
+
+// Gaussian window moments + the per-pixel shape-function solve (phaseflow.py:114-161): mtaps: the
+// window taps k(t) t^p for p = 0..4 (5 x (2r+1) doubles); yplanes: scratch of ny planes
+int moment_yplanes(int order);
+void launch_moments_solve(const double* sums, const double* ux, const double* uy, int W, int H, int order,
+                          const double* mtaps, int r, double* yplanes, double* oux, double* ouy, double* energy,
+                          double* resid, double* slope, cudaStream_t st);
+
+// min / max / NaN of the energy and whether its median is needed (stats: device struct, see fine.cu)
+struct EnergyStats {
+  double lo, hi;
+  int nan;
+  int need_median;  // set by the reduction: the reset needs it, or the caller forces it
+  int skip_reset;   // every energy is above 1e-9 max + 1e-30: no pixel is reset
+  double median;
+  // radix-select state
+  unsigned long long prefix;
+  long long rank;
+  long long less;
+  double lo_val;
+};
+void launch_energy_stats(const double* energy, size_t n, EnergyStats* stats, bool force_median, cudaStream_t st);
+// median of energy into stats->median (np.median), skipped when stats->need_median == 0;
+// hist: 4096 unsigned long long of scratch
+void launch_median(const double* energy, size_t n, EnergyStats* stats, unsigned long long* hist, cudaStream_t st);
+// reset below 1e-9 median + 1e-30 (phaseflow.py:149-151,158-161)
+void launch_reset(const double* energy, const double* ux_in, const double* uy_in, int n, const EnergyStats* stats,
+                  double* ux, double* uy, double* resid, double* slope, cudaStream_t st);
+
+// confidence before the border rule (phaseflow.py:320-323) and low = conf < conf_min; with border = true
+// also the border rule (phaseflow.py:297-317,508-510): conf_out (f32), low (u8), conf64 (nullable)
+void launch_confidence(const double* energy, const double* resid, const double* ux, const double* uy, int W, int H,
+                       const EnergyStats* stats, double phase_tol, double conf_min, bool border, double B,
+                       float* conf_out, double* conf64, uint8_t* low, int* count_low, cudaStream_t st);
+
+// trusted pre-warp (phaseflow.py:326-355): from low (u8) and the counters; writes ux_pre/uy_pre
+struct PrewarpCounts {
+  int low;
+  int ok;
+};
+void launch_prewarp_fill(const uint8_t* low, const double* ux, const double* uy, const double* slope, int W, int H,
+                         double R, PrewarpCounts* counts, uint8_t* ok, int* vdist, int* col_d2, int* col_row,
+                         double* ux_pre, double* uy_pre, cudaStream_t st);
+
+// bounded distance test: flag[p] |= (distance from p to the nearest src pixel <= limit) (mode 0) or
+// out[p] = (distance > limit) (mode 1); vdist: W*H ints of scratch
+void launch_within(const uint8_t* src, int W, int H, double limit, int mode, uint8_t* out, int* vdist, cudaStream_t st);
+
+void launch_f64_to_f32(const double* in, float* out, size_t n, cudaStream_t st);
+void launch_f32_to_f64(const float* in, double* out, size_t n, cudaStream_t st);
+void launch_fill_f64(double* p, double v, size_t n, cudaStream_t st);
+
+// ---------------------------------------------------------------- poc.cu
+struct PocLevel {
+  int W, H;       // level image size
+  int nx, ny;     // grid
+  int wy, wx;     // window
+};
+// downsample (poc.py:164-165) of a float64 (or float32 for level 0) image
+void launch_downsample(const double* in, int W, int H, double* out, double* tmp, const double* taps, int r,
+                       cudaStream_t st);
+// poc_grid (poc.py:67-92): one thread block per grid point; init (nullable) ny x nx
+void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const int* xs, const int* ys,
+                     const double* iux, const double* iuy, double* ux, double* uy, double* peak, cudaStream_t st);
+// clean (poc.py:95-140) in one thread block; fallback = init (nullable)
+void launch_poc_clean(double* ux, double* uy, double* peak, int nx, int ny, double peak_min, double thresh,
+                      const double* fbx, const double* fby, uint8_t* scratch, cudaStream_t st);
+// grid_sample (poc.py:143-161) of grid g (gnx x gny at nodes gxs, gys) at points (scale*X, scale*Y) of a
+// target grid (txs, tys: tnx x tny) times mult; or, with txs == nullptr, at every pixel of a tnx x tny image
+void launch_grid_sample(const double* gux, const double* guy, const int* gxs, const int* gys, int gnx, int gny,
+                        const int* txs, const int* tys, int tnx, int tny, double scale, double mult, double* oux,
+                        double* ouy, cudaStream_t st);
+// the init of the coarsest level from a dense guess: init_dense[Y sc, X sc] / sc
+void launch_init_from_dense(const double* dux, const double* duy, int W, const int* xs, const int* ys, int nx, int ny,
+                            int sc, double* iux, double* iuy, cudaStream_t st);
+// dense start with a guess (track.py:133-137): corr = g - init at the grid points
+void launch_grid_minus_dense(const double* gux, const double* guy, const double* dux, const double* duy, int W,
+                             const int* xs, const int* ys, int nx, int ny, double* cux, double* cuy, cudaStream_t st);
+void launch_add(double* a, const double* b, size_t n, cudaStream_t st);
+
+// ---------------------------------------------------------------- finish.cu
+// pixels of 4-connected components of b with at least min_area pixels (track.py:45-53)
+void launch_large_components(const uint8_t* b, int W, int H, double min_area, int* parent, int* size, uint8_t* out,
+                             cudaStream_t st);
+// finish masks: bad = low | ~roi | guard | border; mx/my = NaN where bad (track.py:66-98)
+void launch_finish_mask(const uint8_t* low, const uint8_t* roi, const uint8_t* big, int W, int H, double guard,
+                        const double* ux, const double* uy, uint8_t* src, uint8_t* bad, int* vdist, double* mx,
+                        double* my, cudaStream_t st);
+// displacement_gradient + strain_fields (strain.py:61-112): outputs nullable f32 planes
+void launch_strain(const double* mx, const double* my, int W, int H, int win, double* yplanes, float* dudx,
+                   float* dudy, float* dvdx, float* dvdy, float* exx, float* eyy, float* exy, float* gmax, float* vol,
+                   cudaStream_t st);
+void launch_pair_outputs(const double* mx, const double* my, const double* rux, const double* ruy,
+                         const double* conf64, int n, float* ux, float* uy, float* conf, uint8_t* valid, float* raw_ux,
+                         float* raw_uy, cudaStream_t st);
+
+}  // namespace ofc

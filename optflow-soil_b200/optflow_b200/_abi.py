@@ -104,6 +104,23 @@ SIGNATURES = {
 }
 
 
+# include/optflow_cuda_testing.h
+TEST_SIGNATURES = {
+    "ofc_test_fft_lines": (ctypes.c_int, [_P, c_float_p, _S, _S, ctypes.c_int, _E, _S]),
+    "ofc_test_reference_phase": (ctypes.c_int, [_P, c_float_p, _S, _S, ctypes.POINTER(OfcConfig)] + [c_float_p] * 5
+                                 + [_E, _S]),
+    "ofc_test_responses": (ctypes.c_int, [_P, c_float_p, _S, _S, ctypes.POINTER(OfcConfig), c_float_p, _E, _S]),
+    "ofc_test_local_solve": (ctypes.c_int, [_P, c_double_p, c_double_p, c_double_p, _S, _S, ctypes.POINTER(OfcConfig)]
+                             + [c_double_p] * 5 + [_E, _S]),
+    "ofc_test_median": (ctypes.c_int, [_P, c_double_p, _S, c_double_p, _E, _S]),
+    "ofc_test_large_components": (ctypes.c_int, [_P, c_u8_p, _S, _S, ctypes.c_double, c_u8_p, _E, _S]),
+    "ofc_test_first_sums": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, c_double_p, c_double_p,
+                                           ctypes.POINTER(OfcConfig), c_double_p, _E, _S]),
+    "ofc_test_prewarp_fill": (ctypes.c_int, [_P, c_u8_p, c_double_p, c_double_p, c_double_p, _S, _S, ctypes.c_double,
+                                             c_double_p, c_double_p, _E, _S]),
+}
+
+
 class EngineError(RuntimeError):
     """An error reported by the CUDA engine (the reference's EngineError, engine.rs:21-24)."""
 
@@ -125,7 +142,7 @@ def load(path=None):
         raise EngineError(2, f"CUDA engine library not built: {p} (run __graft_entry__.build() or "
                              f"python optflow-soil_b200/build.py)")
     lib = ctypes.CDLL(p)
-    for name, (res, args) in SIGNATURES.items():
+    for name, (res, args) in {**SIGNATURES, **TEST_SIGNATURES}.items():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args

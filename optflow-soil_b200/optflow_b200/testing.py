@@ -1,0 +1,104 @@
+"""Single-stage entry points of the CUDA engine (include/optflow_cuda_testing.h), for the parity tests."""
+import ctypes
+
+import numpy as np
+
+from ._abi import c_double_p, c_float_p, c_u8_p
+from .api import _f32, _ptr, default_engine
+from .config import Config
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def fft_lines(data, inverse=False, engine=None):
+    """Row-wise FFT of a 2-D complex array (numpy fft; inverse: L * numpy ifft)."""
+    eng = engine or default_engine()
+    a = np.ascontiguousarray(data, dtype=np.complex64).copy()
+    lines, L = a.shape
+    eng._call("ofc_test_fft_lines", a.ctypes.data_as(c_float_p), lines, L, int(inverse))
+    return a
+
+
+def reference_phase(I1, cfg=None, engine=None):
+    eng = engine or default_engine()
+    cfg = cfg or Config()
+    c = cfg.to_ofc()
+    a = _f32(I1)
+    h, w = a.shape
+    F = cfg.n_filters()
+    out = [np.empty((F, h, w), np.float32) for _ in range(5)]
+    eng._call("ofc_test_reference_phase", _ptr(a, c_float_p), w, h, ctypes.byref(c), *[_ptr(o, c_float_p) for o in out])
+    re, im, gx, gy, amp = out
+    return [(re[k] + 1j * im[k], gx[k], gy[k], amp[k]) for k in range(F)]
+
+
+def responses(img, cfg=None, engine=None):
+    eng = engine or default_engine()
+    cfg = cfg or Config()
+    c = cfg.to_ofc()
+    a = _f32(img)
+    h, w = a.shape
+    F = cfg.n_filters()
+    out = np.empty((F, h + 64, w + 64), np.complex64)
+    eng._call("ofc_test_responses", _ptr(a, c_float_p), w, h, ctypes.byref(c), out.ctypes.data_as(c_float_p))
+    return out
+
+
+def local_solve(sums, ux, uy, cfg=None, engine=None):
+    eng = engine or default_engine()
+    cfg = cfg or Config()
+    c = cfg.to_ofc()
+    s = _d(np.stack(sums))
+    ux, uy = _d(ux), _d(uy)
+    h, w = ux.shape
+    out = [np.empty((h, w)) for _ in range(4)]
+    slope = np.empty((4, h, w))
+    eng._call("ofc_test_local_solve", _ptr(s, c_double_p), _ptr(ux, c_double_p), _ptr(uy, c_double_p), w, h,
+              ctypes.byref(c), *[_ptr(o, c_double_p) for o in out], _ptr(slope, c_double_p))
+    return (*out, np.moveaxis(slope, 0, -1))
+
+
+def median(v, engine=None):
+    eng = engine or default_engine()
+    a = _d(v).ravel()
+    out = ctypes.c_double()
+    eng._call("ofc_test_median", _ptr(a, c_double_p), a.size, ctypes.byref(out))
+    return out.value
+
+
+def large_components(b, min_area, engine=None):
+    eng = engine or default_engine()
+    a = np.ascontiguousarray(b, dtype=np.uint8)
+    h, w = a.shape
+    out = np.empty_like(a)
+    eng._call("ofc_test_large_components", _ptr(a, c_u8_p), w, h, ctypes.c_double(min_area), _ptr(out, c_u8_p))
+    return out.astype(bool)
+
+
+def prewarp_fill(low, ux, uy, slope, radius, engine=None):
+    """slope: (h, w, 4) as in phaseflow.Flow.slope."""
+    eng = engine or default_engine()
+    lo = np.ascontiguousarray(low, dtype=np.uint8)
+    h, w = lo.shape
+    ux, uy = _d(ux), _d(uy)
+    sl = _d(np.moveaxis(np.asarray(slope), -1, 0))
+    ox, oy = np.empty((h, w)), np.empty((h, w))
+    eng._call("ofc_test_prewarp_fill", _ptr(lo, c_u8_p), _ptr(ux, c_double_p), _ptr(uy, c_double_p),
+              _ptr(sl, c_double_p), w, h, ctypes.c_double(radius), _ptr(ox, c_double_p), _ptr(oy, c_double_p))
+    return ox, oy
+
+
+def first_sums(I1, I2, ux, uy, cfg=None, engine=None):
+    """The seven per-pixel sums of refine's first inner iteration from the start field (ux, uy)."""
+    eng = engine or default_engine()
+    cfg = cfg or Config()
+    c = cfg.to_ofc()
+    a, b = _f32(I1), _f32(I2)
+    h, w = a.shape
+    ux, uy = _d(ux), _d(uy)
+    out = np.empty((7, h, w))
+    eng._call("ofc_test_first_sums", _ptr(a, c_float_p), _ptr(b, c_float_p), w, h, _ptr(ux, c_double_p),
+              _ptr(uy, c_double_p), ctypes.byref(c), _ptr(out, c_double_p))
+    return out

@@ -37,6 +37,9 @@ const double INF = std::numeric_limits<double>::infinity();
 const double NaN = std::numeric_limits<double>::quiet_NaN();
 const int PAD = 32;               // phaseflow.py:47
 const double APERTURE_TOL = 1e-3; // phaseflow.py:50
+// round the Gabor responses and the reference pack to float32 storage, as the Rust port stores them
+// (phaseflow.rs:988-1173: Complex32 responses, f32 RefPack); off by default (float64 like the Python)
+bool g_f32_storage = false;
 
 template <class T>
 struct Img {
@@ -489,6 +492,12 @@ vector<RefK> reference_phase(const ImgD& I1, const Bank& b) {
         o.gx(x, y) = std::imag(std::conj(r) * rx) / a2;
         o.gy(x, y) = std::imag(std::conj(r) * ry) / a2;
         o.amp(x, y) = std::sqrt(a2);
+        if (g_f32_storage) {
+          o.r(x, y) = cd((float)r.real(), (float)r.imag());
+          o.gx(x, y) = (float)o.gx(x, y);
+          o.gy(x, y) = (float)o.gy(x, y);
+          o.amp(x, y) = (float)o.amp(x, y);
+        }
       }
   }
   return out;
@@ -667,6 +676,38 @@ void prewarp(const ImgD& ux0, const ImgD& uy0, const vector<double>& slope, cons
   sy = gauss_blur(uy, c.sigma_s);
 }
 
+// the seven per-pixel sums of one inner iteration (phaseflow.py:468-483)
+void accumulate(const vector<RefK>& ref, const vector<ImgC>& resp, const ImgD& sx, const ImgD& sy, const ImgD& csx,
+                const ImgD& csy, const ImgD& ux, const ImgD& uy, ImgD sums[7]) {
+  int W = ux.w, H = ux.h, F = (int)ref.size();
+  for (int i = 0; i < 7; i++) sums[i] = ImgD(W, H, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < H; y++)
+    for (int x = 0; x < W; x++) {
+      size_t p = (size_t)y * W + x;
+      double u = ux.d[p], v = uy.d[p];
+      double tx = x + u, ty = y + v;
+      double px = tx - sx.d[p], py = ty - sy.d[p];
+      for (int s = 0; s < 2; s++) {
+        double nx = tx - sample(csx, px, py), ny = ty - sample(csy, px, py);
+        px = nx; py = ny;
+      }
+      double a[7] = {0, 0, 0, 0, 0, 0, 0};
+      for (int k = 0; k < F; k++) {
+        cd r1 = ref[k].r.d[p];
+        cd r2 = sample(resp[k], px + PAD, py + PAD);
+        double dphi = std::arg(r1 * std::conj(r2));
+        double wk = ref[k].amp.d[p] * std::abs(r2);
+        double gx = ref[k].gx.d[p], gy = ref[k].gy.d[p];
+        double cc = dphi + gx * u + gy * v;
+        a[0] += wk * gx * gx; a[1] += wk * gx * gy; a[2] += wk * gy * gy;
+        a[3] += wk * gx * cc; a[4] += wk * gy * cc; a[5] += wk * cc * cc;
+        a[6] += wk;
+      }
+      for (int i = 0; i < 7; i++) sums[i].d[p] = a[i];
+    }
+}
+
 struct RawFlow { ImgD ux, uy, energy, resid; };
 
 // refine (phaseflow.py:427-511) without the crack options, up to the confidence
@@ -713,6 +754,8 @@ RawFlow refine_raw(const ImgD& I1, const ImgD& I2, const ImgD& ux_in, const ImgD
       for (size_t p = 0; p < R.n(); p++) R.d[p] = F2.d[p] * bank.G[k].d[p];
       fft2(R, true);
       bspline_inplace(R);
+      if (g_f32_storage)
+        for (cd& v : R.d) v = cd((float)v.real(), (float)v.imag());
       resp[k] = std::move(R);
     }
     ImgD csx = sx, csy = sy;
@@ -720,32 +763,7 @@ RawFlow refine_raw(const ImgD& I1, const ImgD& I2, const ImgD& ux_in, const ImgD
     bspline_inplace(csy);
     for (int inner = 0; inner < c.inner_iters; inner++) {
       ImgD sums[7];
-      for (int i = 0; i < 7; i++) sums[i] = ImgD(W, H, 0.0);
-#pragma omp parallel for schedule(static)
-      for (int y = 0; y < H; y++)
-        for (int x = 0; x < W; x++) {
-          size_t p = (size_t)y * W + x;
-          double u = ux.d[p], v = uy.d[p];
-          double tx = x + u, ty = y + v;
-          double px = tx - sx.d[p], py = ty - sy.d[p];
-          for (int s = 0; s < 2; s++) {
-            double nx = tx - sample(csx, px, py), ny = ty - sample(csy, px, py);
-            px = nx; py = ny;
-          }
-          double a[7] = {0, 0, 0, 0, 0, 0, 0};
-          for (int k = 0; k < F; k++) {
-            cd r1 = ref[k].r.d[p];
-            cd r2 = sample(resp[k], px + PAD, py + PAD);
-            double dphi = std::arg(r1 * std::conj(r2));
-            double wk = ref[k].amp.d[p] * std::abs(r2);
-            double gx = ref[k].gx.d[p], gy = ref[k].gy.d[p];
-            double cc = dphi + gx * u + gy * v;
-            a[0] += wk * gx * gx; a[1] += wk * gx * gy; a[2] += wk * gy * gy;
-            a[3] += wk * gx * cc; a[4] += wk * gy * cc; a[5] += wk * cc * cc;
-            a[6] += wk;
-          }
-          for (int i = 0; i < 7; i++) sums[i].d[p] = a[i];
-        }
+      accumulate(ref, resp, sx, sy, csx, csy, ux, uy, sums);
       Solved s = local_solve(sums, ux, uy, c.sigma_w, c.shape_order);
       ux = std::move(s.ux); uy = std::move(s.uy);
       energy = std::move(s.energy); resid = std::move(s.resid);
@@ -1215,6 +1233,8 @@ void to_ptr(const ImgD& a, double* p) { if (p) std::memcpy(p, a.d.data(), sizeof
 // ------------------------------------------------------------------ C API (test infrastructure)
 extern "C" {
 
+void oro_set_f32_storage(int on) { g_f32_storage = on != 0; }
+
 int oro_threads(int n) { if (n > 0) omp_set_num_threads(n); return omp_get_max_threads(); }
 
 // numpy fft2 / ifft2 of an h x w complex array stored as interleaved (re, im) doubles
@@ -1298,6 +1318,40 @@ void oro_refine(const double* i1, const double* i2, int w, int h, const double* 
   ImgD cf;
   refine_conf(rf, *c, cf);
   to_ptr(rf.ux, ux); to_ptr(rf.uy, uy); to_ptr(cf, conf); to_ptr(rf.resid, resid); to_ptr(rf.energy, energy);
+}
+
+// the sums of the first inner iteration of refine from (ux, uy): pre-warp s = blur(u), warp, responses,
+// accumulate (7 planes of w*h)
+void oro_first_sums(const double* i1, const double* i2, int w, int h, const double* ux0, const double* uy0,
+                    const ofc_config* c, double* sums_out) {
+  ImgD I1 = from_ptr(i1, w, h), I2 = from_ptr(i2, w, h), ux = from_ptr(ux0, w, h), uy = from_ptr(uy0, w, h);
+  Bank bank = gabor_bank(h + 2 * PAD, w + 2 * PAD, *c);
+  vector<RefK> ref = reference_phase(I1, bank);
+  ImgD c2 = I2;
+  bspline_inplace(c2);
+  ImgD sx = gauss_blur(ux, c->sigma_s), sy = gauss_blur(uy, c->sigma_s);
+  ImgD warped(w, h);
+  for (int y = 0; y < h; y++)
+    for (int x = 0; x < w; x++) warped(x, y) = sample(c2, x + sx(x, y), y + sy(x, y));
+  ImgC F2 = pad_reflect(warped);
+  fft2(F2, false);
+  vector<ImgC> resp(bank.G.size());
+  for (size_t k = 0; k < bank.G.size(); k++) {
+    ImgC R(F2.w, F2.h);
+    for (size_t p = 0; p < R.n(); p++) R.d[p] = F2.d[p] * bank.G[k].d[p];
+    fft2(R, true);
+    bspline_inplace(R);
+    if (g_f32_storage)
+      for (cd& v : R.d) v = cd((float)v.real(), (float)v.imag());
+    resp[k] = std::move(R);
+  }
+  ImgD csx = sx, csy = sy;
+  bspline_inplace(csx);
+  bspline_inplace(csy);
+  ImgD sums[7];
+  accumulate(ref, resp, sx, sy, csx, csy, ux, uy, sums);
+  size_t N = (size_t)w * h;
+  for (int i = 0; i < 7; i++) std::memcpy(sums_out + i * N, sums[i].d.data(), N * sizeof(double));
 }
 
 void oro_poc_shift(const double* a, const double* b, int w, int h, double* out3) {

@@ -130,6 +130,21 @@ def refine(I1, I2, ux, uy, cfg=None):
     return dict(zip(("ux", "uy", "conf", "resid", "energy"), out))
 
 
+def first_sums(I1, I2, ux, uy, cfg=None):
+    """The seven per-pixel sums of refine's first inner iteration (pre-warp = blur of the start field)."""
+    a, b, ux, uy = _d(I1), _d(I2), _d(ux), _d(uy)
+    h, w = a.shape
+    pc, _ = _cfg(cfg)
+    out = np.empty((7, h, w))
+    lib().oro_first_sums(_p(a), _p(b), w, h, _p(ux), _p(uy), pc, _p(out))
+    return out
+
+
+def set_f32_storage(on):
+    """Round responses and reference pack to float32 (the Rust port's storage) in the oracle's refine."""
+    lib().oro_set_f32_storage(int(bool(on)))
+
+
 def poc_shift(a, b):
     a, b = _d(a), _d(b)
     out = np.empty(3)

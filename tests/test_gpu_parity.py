@@ -1,0 +1,159 @@
+"""The CUDA engine against the reference, through the C ABI: golden vectors written by the reference itself
+(tests/golden) and the CPU oracle on seeded inputs.
+
+Bars (the reference's own parity tests and the pair path's contract): ux, uy, conf, resid RMS < 1e-3
+(rust/crates/optflow-core/tests/parity_refine.rs:86-89); POC grid within 1e-3 px (parity_poc.rs:50-51);
+strain RMS < 1e-5 (parity_track.rs:70-72); validity masks identical except at pixels whose confidence is
+within a small distance of conf_min or whose guard decision follows from such a pixel.
+"""
+import numpy as np
+import pytest
+from conftest import golden, rms
+
+from optflow_b200 import Config, coarse_flow, displacement_gradient, refine, track_pair
+
+pytestmark = pytest.mark.gpu
+
+DISP_TOL = 1e-3
+STRAIN_TOL = 1e-5
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_refine_golden(order):
+    g = golden("refine")
+    f = refine(g["a"], g["b"], g["init_ux"], g["init_uy"], Config(shape_order=order))
+    for k in ("ux", "uy", "conf", "resid"):
+        assert rms(getattr(f, k), g[f"o{order}_{k}"]) < DISP_TOL, k
+    assert np.abs(f.ux - g[f"o{order}_ux"]).max() < 1e-2
+
+
+def test_refine_stripe_is_degenerate():
+    g = golden("stripe")
+    f = refine(g["a"], g["b"], g["init_ux"], g["init_uy"], Config())
+    assert f.conf.max() < Config().conf_min
+    assert np.isfinite(f.ux).all() and np.isfinite(f.uy).all()
+    assert rms(f.ux, g["ux"]) < DISP_TOL and rms(f.uy, g["uy"]) < DISP_TOL
+
+
+def test_refine_border_guard_off():
+    g = golden("border")
+    f = refine(g["a"], g["b"], g["init_ux"], g["init_uy"], Config(edge_guard=0.0))
+    assert (f.conf[:, :2] == 0).all() and (f.conf[-2:, :] == 0).all()
+    np.testing.assert_array_equal(f.conf == 0, g["conf"] == 0)
+    for k in ("ux", "uy", "conf"):
+        assert rms(getattr(f, k), g[k]) < DISP_TOL
+
+
+def test_coarse_flow_golden():
+    g = golden("poc")
+    r = coarse_flow(g["a"], g["b"], Config())
+    np.testing.assert_array_equal(r.xs, g["xs"])
+    np.testing.assert_array_equal(r.ys, g["ys"])
+    for k in ("ux", "uy", "peak"):
+        assert np.abs(getattr(r, k) - g[k]).max() < DISP_TOL, k
+    r = coarse_flow(g["a"], g["b"], Config(), init_dense=(g["init_ux"], g["init_uy"]))
+    assert np.abs(r.ux - g["iux"]).max() < DISP_TOL and np.abs(r.uy - g["iuy"]).max() < DISP_TOL
+    assert np.abs(r.peak - g["ipeak"]).max() < DISP_TOL
+    r = coarse_flow(g["a"], np.full(g["a"].shape, 0.5, np.float32), Config(), init_dense=(g["init_ux"], g["init_uy"]))
+    assert (r.peak == 0).all()
+    assert np.abs(r.ux - g["fux"]).max() < 1e-5 and np.abs(r.uy - g["fuy"]).max() < 1e-5
+
+
+def test_strain_golden():
+    g = golden("strain")
+    got = displacement_gradient(g["ux"], g["uy"], 15)
+    for a, k in zip(got, ("dudx", "dudy", "dvdx", "dvdy")):
+        np.testing.assert_array_equal(np.isnan(a), np.isnan(g[k]))
+        assert np.nanmax(np.abs(a - g[k])) < 1e-6
+
+
+def compare_pair(r, want, label, conf_band=0.02):
+    """Parity of a track_pair Result with the reference's outputs (want: dict of arrays)."""
+    valid_g = np.isfinite(r.ux)
+    valid_w = np.isfinite(want["ux"])
+    both = valid_g & valid_w
+    # validity: every disagreement must sit where the confidence is within conf_band of conf_min, or within
+    # the guard distance of such a pixel (a flipped low pixel moves the guard band around it)
+    cmin = Config().conf_min
+    near = np.abs(np.asarray(want["conf"], np.float64) - cmin) < conf_band
+    diff = valid_g != valid_w
+    if diff.any():
+        from scipy.ndimage import binary_dilation
+        zone = binary_dilation(near, iterations=int(np.ceil(Config().edge_guard_px())) + 1)
+        assert (diff & ~zone).sum() == 0, f"{label}: {int((diff & ~zone).sum())} validity differences away from threshold"
+    assert diff.mean() < 0.01, f"{label}: {diff.mean():.4f} of pixels change validity"
+    assert both.sum() > 0.5 * valid_w.sum()
+    assert rms(r.ux, want["ux"], both) < DISP_TOL, label
+    assert rms(r.uy, want["uy"], both) < DISP_TOL, label
+    assert rms(r.conf, want["conf"]) < DISP_TOL, label
+    # the unmasked field (the init of a sequence's next frame; not a CLI output) on the confident pixels
+    trusted = np.asarray(want["conf"]) >= cmin
+    assert rms(r.raw_ux, want["raw_ux"], trusted) < DISP_TOL and rms(r.raw_uy, want["raw_uy"], trusted) < DISP_TOL, label
+    for k in ("Exx", "Eyy", "Exy", "gmax", "vol"):
+        m = both & np.isfinite(r.strain[k]) & np.isfinite(want[k])
+        assert rms(r.strain[k], want[k], m) < STRAIN_TOL, (label, k)
+
+
+@pytest.mark.parametrize("name", ["pair_roi", "pair_affsin", "pair_init", "pair_seq256"])
+def test_track_pair_golden(name):
+    g = golden(name)
+    init = (g["init_ux"], g["init_uy"]) if "init_ux" in g else None
+    r = track_pair(g["a"], g["b"], Config(), mask=g.get("roi"), init=init)
+    compare_pair(r, g, name)
+    np.testing.assert_array_equal(r.valid, np.isfinite(r.ux))
+
+
+def _synthetic_pair(n, seed, t=(2.3, -1.4), exx=0.01, noise=0.01):
+    """A seeded speckle pair (Gaussian blobs, affine deformation) for the oracle comparisons."""
+    rng = np.random.default_rng(seed)
+    nb = int(0.6 * (n + 40) ** 2 / (np.pi * 4.0))
+    cx, cy = rng.uniform(-20, n + 20, (2, nb))
+    r = rng.uniform(1.5, 2.5, nb)
+    a = rng.uniform(0.3, 1.0, nb) * rng.choice([-1.0, 1.0], nb)
+    yy, xx = np.mgrid[0:n, 0:n].astype(np.float64)
+
+    def render(X, Y):
+        acc = np.zeros((n, n))
+        for k in range(nb):
+            x0, x1 = int(max(cx[k] - 12, 0)), int(min(cx[k] + 13, n))
+            y0, y1 = int(max(cy[k] - 12, 0)), int(min(cy[k] + 13, n))
+            if x0 >= x1 or y0 >= y1:
+                continue
+            dx = X[y0:y1, x0:x1] - cx[k]
+            dy = Y[y0:y1, x0:x1] - cy[k]
+            acc[y0:y1, x0:x1] += a[k] * np.exp(-(dx * dx + dy * dy) / (2 * r[k] ** 2))
+        return 0.5 + 0.25 * np.tanh(acc)
+
+    c = n / 2
+    X = c + (xx - c - t[0]) / (1 + exx)
+    Y = yy - t[1]
+    i1 = render(xx, yy) + rng.normal(0, noise, (n, n))
+    i2 = render(X, Y) + rng.normal(0, noise, (n, n))
+    q = lambda im: (np.round(np.clip(im, 0, 1) * 255) / 255).astype(np.float32)
+    return q(i1), q(i2)
+
+
+@pytest.mark.parametrize("n,seed", [(192, 1), (256, 2)])
+def test_track_pair_oracle(oracle, n, seed):
+    a, b = _synthetic_pair(n, seed)
+    roi = np.zeros((n, n), bool)
+    roi[n // 10:n - n // 10, n // 8:n - n // 8] = True
+    want = oracle.track_pair(a, b, Config(), mask=roi)
+    r = track_pair(a, b, Config(), mask=roi)
+    compare_pair(r, want, f"oracle{n}")
+
+
+def test_refine_raw_window_shift(oracle):
+    """refine_raw on a window of a larger pair (FineEngine::refine_raw with a shift) equals refine on the crop
+    when the second image's window covers the displaced positions."""
+    from optflow_b200 import refine_raw
+    a, b = _synthetic_pair(192, 7, t=(1.2, 0.7), exx=0.0)
+    x0, y0, w, h = 40, 32, 96, 112
+    u = np.full((h, w), 1.2, np.float32)
+    v = np.full((h, w), 0.7, np.float32)
+    sx, sy = x0 - 16, y0 - 16
+    i2 = b[sy:sy + h + 64, sx:sx + w + 64]
+    got = refine_raw(a[y0:y0 + h, x0:x0 + w], i2, u, v, Config(), shift=(x0 - sx, y0 - sy))
+    want = oracle.refine(a[y0:y0 + h, x0:x0 + w], b[y0:y0 + h, x0:x0 + w], u, v, Config())
+    inner = (slice(20, -20), slice(20, -20))
+    assert rms(got["ux"][inner], want["ux"][inner]) < 5e-3

@@ -1,0 +1,140 @@
+"""Each CUDA stage against the reference's intermediate arrays (through include/optflow_cuda_testing.h).
+
+The expected values come from the committed golden vectors (written by the reference itself) and from the
+CPU oracle, which tests/test_oracle.py pins to the reference.
+"""
+import numpy as np
+import pytest
+from conftest import golden
+
+from optflow_b200.config import Config
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def T():
+    from optflow_b200 import testing
+    return testing
+
+
+@pytest.mark.parametrize("L", [64, 128, 160, 192, 224, 320, 576, 832, 1088, 1152, 2112, 2*3*5*7*11, 3*17*19, 23*29, 31*8])
+def test_fft_lines_match_numpy(T, L):
+    rng = np.random.default_rng(L)
+    a = (rng.standard_normal((5, L)) + 1j * rng.standard_normal((5, L))).astype(np.complex64)
+    for inv in (False, True):
+        got = T.fft_lines(a, inverse=inv)
+        ref = np.fft.ifft(a.astype(np.complex128), axis=1) * L if inv else np.fft.fft(a.astype(np.complex128), axis=1)
+        err = np.abs(got - ref).max() / np.abs(ref).max()
+        assert err < 2e-6, (L, inv, err)
+
+
+def test_reference_phase(T):
+    """parity_gabor.rs:40-70: per filter, response error < 1e-4 of its largest |r|; phase gradient error
+    < 1e-3 rad/px on the pixels whose amplitude exceeds 5 % of the filter's largest."""
+    g = golden("gabor")
+    ref = T.reference_phase(g["img"])
+    for k, (r, gx, gy, amp) in enumerate(ref):
+        want = g["r_re"][k] + 1j * g["r_im"][k]
+        max_amp = np.abs(want).max()
+        assert np.abs(r - want).max() / max_amp < 1e-4
+        strong = g["amp"][k] > 0.05 * max_amp
+        assert strong.sum() > strong.size / 20
+        assert np.abs(gx - g["gx"][k])[strong].max() < 1e-3
+        assert np.abs(gy - g["gy"][k])[strong].max() < 1e-3
+        assert np.abs(amp - g["amp"][k])[strong].max() < 1e-4 * max_amp
+    # the float64 transforms keep the gradient accurate near the zeros of a response too
+    for k, (r, gx, gy, amp) in enumerate(ref):
+        weak = g["amp"][k] > 1e-4 * np.abs(g["r_re"][k] + 1j * g["r_im"][k]).max()
+        assert np.abs(gx - g["gx"][k])[weak].max() < 1e-2
+
+
+def _gabor_bank_np(shape, cfg):
+    """phaseflow.gabor_bank (python/optflow_ref/phaseflow.py:73-89), restated in numpy for the check."""
+    h, w = shape
+    fy = (np.fft.fftfreq(h) * 2 * np.pi)[:, None]
+    fx = (np.fft.fftfreq(w) * 2 * np.pi)[None, :]
+    s_hp = cfg.dc_cut * cfg.lam * max(cfg.scales) / (2 * np.pi)
+    hp = 1.0 - np.exp(-(fx ** 2 + fy ** 2) * s_hp ** 2 / 2)
+    bank = []
+    for sc in cfg.scales:
+        w0 = 2 * np.pi / (cfg.lam * sc)
+        s = cfg.bandwidth * w0
+        for k in range(cfg.n_orient):
+            th = np.pi * k / cfg.n_orient
+            bank.append(hp * np.exp(-((fx - w0 * np.cos(th)) ** 2 + (fy - w0 * np.sin(th)) ** 2) / (2 * s * s)))
+    return bank
+
+
+@pytest.mark.parametrize("shape", [(96, 128), (160, 224)])
+def test_responses(T, oracle, shape):
+    rng = np.random.default_rng(1)
+    img = rng.random(shape).astype(np.float32)
+    cfg = Config()
+    got = T.responses(img, cfg)
+    pad = np.pad(img.astype(np.float64), 32, mode="reflect")
+    F2 = np.fft.fft2(pad)
+    for k, G in enumerate(_gabor_bank_np(pad.shape, cfg)):
+        r = np.fft.ifft2(F2 * G)
+        want = oracle.bspline_coeffs(r.real) + 1j * oracle.bspline_coeffs(r.imag)
+        err = np.abs(got[k] - want).max() / np.abs(want).max()
+        assert err < 1e-4, (k, err)
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_local_solve(T, oracle, order):
+    rng = np.random.default_rng(order)
+    h, w = 70, 90
+    gx, gy = rng.normal(size=(2, 12, h, w))
+    wk = rng.uniform(0.1, 1.0, size=(12, h, w))
+    c = rng.normal(size=(12, h, w)) + 20.0  # large right-hand sides, as with |u| ~ 25 px
+    sums = [(wk * gx * gx).sum(0), (wk * gx * gy).sum(0), (wk * gy * gy).sum(0), (wk * gx * c).sum(0),
+            (wk * gy * c).sum(0), (wk * c * c).sum(0), wk.sum(0)]
+    sums[0][10:14, 10:14] = 0.0  # degenerate: no energy
+    sums[1][10:14, 10:14] = 0.0
+    sums[2][10:14, 10:14] = 0.0
+    ux, uy = rng.normal(size=(2, h, w))
+    got = T.local_solve(sums, ux, uy, Config(shape_order=order))
+    want = oracle.local_solve(sums, ux, uy, 4.0, order)
+    for a, b in zip(got, want):
+        np.testing.assert_allclose(a, b, rtol=1e-7, atol=1e-9)
+
+
+def test_median(T):
+    rng = np.random.default_rng(5)
+    for n in (1, 2, 3, 10, 1001, 4096, 100000):
+        v = rng.exponential(size=n) * 1e3
+        assert T.median(v) == np.median(v)
+    v = np.repeat(rng.random(50), 7)
+    assert T.median(v) == np.median(v)
+    assert T.median(np.array([3.0, 1.0, 2.0, 2.0])) == 2.0
+
+
+def test_large_components(T, oracle):
+    rng = np.random.default_rng(9)
+    for p in (0.3, 0.5, 0.6):
+        b = rng.random((123, 157)) < p
+        for area in (5, 50, 327.68):
+            np.testing.assert_array_equal(T.large_components(b, area), oracle.large_components(b, area))
+
+
+def test_prewarp_fill(T, oracle):
+    """phaseflow.prewarp's fill (phaseflow.py:344-354) with scipy's nearest-source tie rule."""
+    rng = np.random.default_rng(3)
+    h, w = 90, 120
+    low = np.zeros((h, w), bool)
+    low[30:60, 40:80] = True
+    low |= rng.random((h, w)) < 0.01
+    ux, uy = rng.normal(size=(2, h, w))
+    slope = rng.normal(size=(h, w, 4)) * 0.01
+    R = Config().auto_edge_guard_px()
+    gx, gy = T.prewarp_fill(low, ux, uy, slope, R)
+    ok = oracle.edt(~low) > R
+    _, (iy, ix) = oracle.edt(~ok, return_indices=True)
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    dx, dy = xx - ix, yy - iy
+    g = slope[iy, ix]
+    ex = np.where(ok, ux, ux[iy, ix] + g[..., 0] * dx + g[..., 2] * dy)
+    ey = np.where(ok, uy, uy[iy, ix] + g[..., 1] * dx + g[..., 3] * dy)
+    np.testing.assert_allclose(gx, ex, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(gy, ey, rtol=0, atol=1e-12)
