@@ -31,13 +31,22 @@ struct Error : std::runtime_error {
                                              " at " + __FILE__ + ":" + std::to_string(__LINE__)); \
   } while (0)
 
-// kernel launch with error check and the engine's launch counter
+// kernel launch with error check, the engine's launch counter and, in profile mode, CUDA events around the
+// launches whose kernel name matches the profile filter (the reference's per-kernel GPU timing,
+// OPTFLOW_GPU_KERNELS, rust/README.md:157-159)
+struct Profiler;
 extern thread_local uint64_t* g_launch_counter;
-#define OFC_LAUNCH(kernel, grid, block, smem, stream, ...)                     \
-  do {                                                                         \
-    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                \
-    OFC_CUDA(cudaGetLastError());                                              \
-    if (::ofc::g_launch_counter) ++*::ofc::g_launch_counter;                   \
+extern thread_local Profiler* g_profiler;
+void prof_before(const char* name, cudaStream_t st, void** token);
+void prof_after(void* token, cudaStream_t st);
+#define OFC_LAUNCH(kernel, grid, block, smem, stream, ...)                         \
+  do {                                                                             \
+    void* ofc_tok_ = nullptr;                                                      \
+    if (::ofc::g_profiler) ::ofc::prof_before(#kernel, (stream), &ofc_tok_);       \
+    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                    \
+    OFC_CUDA(cudaGetLastError());                                                  \
+    if (ofc_tok_) ::ofc::prof_after(ofc_tok_, (stream));                           \
+    if (::ofc::g_launch_counter) ++*::ofc::g_launch_counter;                       \
   } while (0)
 
 inline unsigned div_up(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }

@@ -18,9 +18,69 @@
 #include "fft.cuh"
 #include "kernels.cuh"
 #include "../../include/optflow_cuda_testing.h"
+#include "../../include/optflow_cuda_synth.h"
 
 namespace ofc {
 thread_local uint64_t* g_launch_counter = nullptr;
+thread_local Profiler* g_profiler = nullptr;
+
+// Events around the launches of the kernels whose name contains `filter`; resolved into per-kernel totals
+// when read (ofc_profile_read) or when the pool runs low.
+struct Profiler {
+  std::string filter;
+  struct Pending {
+    std::string name;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> pool;
+  std::map<std::string, std::pair<uint64_t, double>> totals;
+  std::mutex mu;
+  cudaEvent_t take() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      OFC_CUDA(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  void resolve() {
+    for (auto& p : pending) {
+      OFC_CUDA(cudaEventSynchronize(p.b));
+      float ms = 0;
+      OFC_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+      auto& t = totals[p.name];
+      t.first += 1;
+      t.second += ms;
+      pool.push_back(p.a);
+      pool.push_back(p.b);
+    }
+    pending.clear();
+  }
+  ~Profiler() {
+    for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
+
+void prof_before(const char* name, cudaStream_t st, void** token) {
+  Profiler* p = g_profiler;
+  std::string n(name);
+  if (!n.empty() && n.front() == '(') n = n.substr(1, n.size() - 2);
+  if (!p->filter.empty() && n.find(p->filter) == std::string::npos) return;
+  std::lock_guard<std::mutex> lk(p->mu);
+  if (p->pending.size() > 4096) p->resolve();
+  Profiler::Pending q{n, p->take(), p->take()};
+  OFC_CUDA(cudaEventRecord(q.a, st));
+  p->pending.push_back(q);
+  *token = &p->pending.back();
+}
+
+void prof_after(void* token, cudaStream_t st) {
+  OFC_CUDA(cudaEventRecord(((Profiler::Pending*)token)->b, st));
+}
 }
 
 using namespace ofc;
@@ -186,6 +246,7 @@ struct ofc_engine {
   int nlanes = 1;
   uint64_t launches = 0;
   std::vector<std::unique_ptr<Lane>> lanes;
+  std::unique_ptr<ofc::Profiler> prof;
 };
 
 namespace {
@@ -213,17 +274,21 @@ int guarded(ofc_engine* e, char* err, size_t errlen, F&& f) {
     return OFC_ERR_BUSY;
   }
   g_launch_counter = &e->launches;
+  g_profiler = e->prof.get();
   try {
     OFC_CUDA(cudaSetDevice(e->device));
     f(*lane);
     g_launch_counter = nullptr;
+    g_profiler = nullptr;
     return OFC_OK;
   } catch (const Error& x) {
     g_launch_counter = nullptr;
+    g_profiler = nullptr;
     set_err(err, errlen, x.what());
     return x.status;
   } catch (const std::exception& x) {
     g_launch_counter = nullptr;
+    g_profiler = nullptr;
     set_err(err, errlen, x.what());
     return OFC_ERR_DEVICE;
   }
@@ -555,6 +620,53 @@ void cfg_check(const ofc_config* c) {
   if (!m.empty()) throw Error(OFC_ERR_ARG, m);
 }
 
+}  // namespace
+
+// synth.cu
+namespace ofc {
+void synth_render_dev(const double* bx, const double* by, const double* br, const double* ba, const int* cell_start,
+                      int ncx, int ncy, double x0, double y0, double cell, int w, int h, int ss, const ofc_field* field,
+                      float* out, cudaStream_t st);
+}
+
+namespace {
+// bins the blobs by cell of the reference frame (host) and renders on the device
+void launch_synth_render(Lane& L, const double* bx, const double* by, const double* br, const double* ba, size_t n,
+                         int w, int h, int ss, const ofc_field* field, float* out) {
+  const double cell = 16.0;
+  double x0 = 0, y0 = 0, x1 = w, y1 = h;
+  for (size_t i = 0; i < n; i++) {
+    x0 = std::min(x0, bx[i]); y0 = std::min(y0, by[i]);
+    x1 = std::max(x1, bx[i]); y1 = std::max(y1, by[i]);
+  }
+  x0 -= cell; y0 -= cell;
+  int ncx = (int)((x1 - x0) / cell) + 2, ncy = (int)((y1 - y0) / cell) + 2;
+  std::vector<int> cnt((size_t)ncx * ncy + 1, 0);
+  std::vector<int> cid(n);
+  for (size_t i = 0; i < n; i++) {
+    int cx = (int)((bx[i] - x0) / cell), cy = (int)((by[i] - y0) / cell);
+    cid[i] = cy * ncx + cx;
+    cnt[cid[i] + 1]++;
+  }
+  for (size_t c = 1; c < cnt.size(); c++) cnt[c] += cnt[c - 1];
+  std::vector<double> sx(n), sy(n), sr(n), sa(n);
+  std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+  for (size_t i = 0; i < n; i++) {
+    int d = fill[cid[i]]++;
+    sx[d] = bx[i]; sy[d] = by[i]; sr[d] = br[i]; sa[d] = ba[i];
+  }
+  double* dx = L.upload("syn_x", sx.data(), n);
+  double* dy = L.upload("syn_y", sy.data(), n);
+  double* dr = L.upload("syn_r", sr.data(), n);
+  double* da = L.upload("syn_a", sa.data(), n);
+  int* dc = L.upload("syn_cells", cnt.data(), cnt.size());
+  float* dout = L.get<float>("syn_out", (size_t)w * h);
+  ofc_field* df = nullptr;
+  if (field) df = L.upload("syn_field", field, 1);
+  synth_render_dev(dx, dy, dr, da, dc, ncx, ncy, x0, y0, cell, w, h, ss, df, dout, L.stream);
+  OFC_CUDA(cudaMemcpyAsync(out, dout, (size_t)w * h * sizeof(float), cudaMemcpyDeviceToHost, L.stream));
+  OFC_CUDA(cudaStreamSynchronize(L.stream));
+}
 }  // namespace
 
 // ================================================================= C ABI
@@ -929,7 +1041,7 @@ int ofc_test_reference_phase(ofc_engine* e, const float* i1, size_t w, size_t h,
     cfg_check(c);
     check_fine_window(w, h, *c);
     const int W = (int)w, H = (int)h, ph = H + 2 * PAD, pw = W + 2 * PAD, F = c->n_scales * c->n_orient;
-    const size_t N = w * h, Np = (size_t)ph * pw;
+    const size_t N = w * h;
     GaborTables g = upload_gabor(L, ph, pw, *c);
     float* d1 = L.upload("in_i1", i1, N);
     float4* ref4 = L.get<float4>("ref4", N * F);
@@ -1103,6 +1215,58 @@ int ofc_test_first_sums(ofc_engine* e, const float* i1, const float* i2, size_t 
     launch_accumulate(ref4, amp, R, F, ph, pw, u2, u2 + N, s2, s2 + N, cs2, cs2 + N, W, H, ds, st);
     OFC_CUDA(cudaMemcpyAsync(sums, ds, 7 * N * 8, cudaMemcpyDeviceToHost, st));
     OFC_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int ofc_set_profile(ofc_engine* e, const char* filter) {
+  if (!e) return OFC_ERR_ARG;
+  try {
+    cudaSetDevice(e->device);
+    for (auto& l : e->lanes) OFC_CUDA(cudaStreamSynchronize(l->stream));
+    if (!filter) {
+      if (e->prof) e->prof->resolve();
+      e->prof.reset();
+      return OFC_OK;
+    }
+    if (!e->prof) e->prof.reset(new ofc::Profiler());
+    e->prof->filter = filter;
+    return OFC_OK;
+  } catch (const Error& x) {
+    return x.status;
+  }
+}
+
+int ofc_profile_read(ofc_engine* e, char* names, size_t stride, uint64_t* counts, double* ms, size_t cap) {
+  if (!e || !e->prof) return -1;
+  try {
+    cudaSetDevice(e->device);
+    std::lock_guard<std::mutex> lk(e->prof->mu);
+    e->prof->resolve();
+    size_t i = 0;
+    for (auto& kv : e->prof->totals) {
+      if (i >= cap) break;
+      if (names && stride) {
+        size_t n = std::min(stride - 1, kv.first.size());
+        std::memcpy(names + i * stride, kv.first.data(), n);
+        names[i * stride + n] = 0;
+      }
+      if (counts) counts[i] = kv.second.first;
+      if (ms) ms[i] = kv.second.second;
+      i++;
+    }
+    e->prof->totals.clear();
+    return (int)i;
+  } catch (const Error&) {
+    return -1;
+  }
+}
+
+int ofc_synth_render(ofc_engine* e, const double* bx, const double* by, const double* br, const double* ba, size_t n,
+                     size_t w, size_t h, int ss, const ofc_field* field, float* out, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    check_sizes(w, h);
+    if (ss < 1 || ss > 16) throw Error(OFC_ERR_ARG, "ss must lie in [1, 16]");
+    launch_synth_render(L, bx, by, br, ba, n, (int)w, (int)h, ss, field, out);
   });
 }
 

@@ -121,6 +121,21 @@ TEST_SIGNATURES = {
 }
 
 
+class OfcField(ctypes.Structure):
+    """struct ofc_field (include/optflow_cuda_synth.h)."""
+    _fields_ = [(n, ctypes.c_double) for n in ("a00", "a01", "a10", "a11", "cx", "cy", "tx", "ty", "amp",
+                                                "wavelength", "sx", "sy")]
+
+
+# include/optflow_cuda_synth.h
+SYNTH_SIGNATURES = {
+    "ofc_synth_render": (ctypes.c_int, [_P, c_double_p, c_double_p, c_double_p, c_double_p, _S, _S, _S, ctypes.c_int,
+                                        ctypes.POINTER(OfcField), c_float_p, _E, _S]),
+    "ofc_set_profile": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "ofc_profile_read": (ctypes.c_int, [_P, ctypes.c_char_p, _S, ctypes.POINTER(ctypes.c_uint64), c_double_p, _S]),
+}
+
+
 class EngineError(RuntimeError):
     """An error reported by the CUDA engine (the reference's EngineError, engine.rs:21-24)."""
 
@@ -142,7 +157,7 @@ def load(path=None):
         raise EngineError(2, f"CUDA engine library not built: {p} (run __graft_entry__.build() or "
                              f"python optflow-soil_b200/build.py)")
     lib = ctypes.CDLL(p)
-    for name, (res, args) in {**SIGNATURES, **TEST_SIGNATURES}.items():
+    for name, (res, args) in {**SIGNATURES, **TEST_SIGNATURES, **SYNTH_SIGNATURES}.items():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
