@@ -197,7 +197,9 @@ def main():
     dout = _abi.OfcPairOut()
     for k, t in outs.items():
         setattr(dout, k, ctypes.cast(t.data_ptr(), _abi.c_u8_p if k == "valid" else _abi.c_float_p))
-    stream = torch.cuda.current_stream(dev)
+    # a stream of its own: the engine reads a null stream handle as "the engine's stream", and torch's
+    # legacy default stream has the null handle
+    stream = torch.cuda.Stream(dev)
     err = ctypes.create_string_buffer(1024)
 
     def step():
@@ -223,7 +225,8 @@ def main():
     launches0 = eng.kernel_launches()
     ms = []
     for _ in range(args.steps):
-        flush.fill_(1.0)
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)

@@ -303,6 +303,17 @@ struct FineOut {
   EnergyStats* stats;  // median of the final energy
 };
 
+// the Gabor tables of a padded size on the device (float64 and float32 copies)
+GaborTables upload_gabor(Lane& L, int ph, int pw, const ofc_config& c) {
+  std::vector<double> gt = gabor_tables_host(ph, pw, c);
+  std::vector<float> g32(gt.begin(), gt.end());
+  double* d64 = L.upload("gabor", gt.data(), gt.size());
+  float* d32 = L.upload("gabor32", g32.data(), g32.size());
+  GaborTables g;
+  gabor_bind(g, d64, d32, ph, pw, c.n_scales * c.n_orient);
+  return g;
+}
+
 // reference_phase (phaseflow.py:100-111) of i1 in float64 transforms, stored as float32 (r.re, r.im, gx, gy)
 // and amp per filter. The transforms run in float64 because the phase gradient divides by |r|^2: near a zero
 // of a response, the absolute error of a float32 transform (~1e-7 of the largest response) is a large
@@ -336,12 +347,7 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
   const int F = c.n_scales * c.n_orient;
   const FftPlan& plw = L.plan(pw);
   const FftPlan& plh = L.plan(ph);
-  // Gabor tables
-  std::vector<double> gt = gabor_tables_host(ph, pw, c);
-  double* dg = L.upload("gabor", gt.data(), gt.size());
-  GaborTables g;
-  g.F = F; g.ph = ph; g.pw = pw;
-  g.fx = dg; g.fy = dg + pw; g.hx = g.fy + ph; g.hy = g.hx + pw; g.ex = g.hy + ph; g.ey = g.ex + (size_t)F * pw;
+  GaborTables g = upload_gabor(L, ph, pw, c);
   // taps: smoothing Gaussian (sigma_s) and window moments k(t) t^p, p = 0..4 (sigma_w)
   std::vector<double> ks = gauss_kernel(c.sigma_s);
   int rs = (int)ks.size() / 2;
@@ -1024,16 +1030,6 @@ int ofc_test_fft_lines(ofc_engine* e, float* data, size_t lines, size_t L, int i
   });
 }
 
-static GaborTables upload_gabor(Lane& L, int ph, int pw, const ofc_config& c) {
-  std::vector<double> gt = gabor_tables_host(ph, pw, c);
-  double* dg = L.upload("gabor", gt.data(), gt.size());
-  GaborTables g;
-  g.F = c.n_scales * c.n_orient;
-  g.ph = ph;
-  g.pw = pw;
-  g.fx = dg; g.fy = dg + pw; g.hx = g.fy + ph; g.hy = g.hx + pw; g.ex = g.hy + ph; g.ey = g.ex + (size_t)g.F * pw;
-  return g;
-}
 
 int ofc_test_reference_phase(ofc_engine* e, const float* i1, size_t w, size_t h, const ofc_config* c, float* r_re,
                              float* r_im, float* gx, float* gy, float* amp, char* err, size_t errlen) {

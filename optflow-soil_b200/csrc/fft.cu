@@ -45,6 +45,8 @@ FftPlan fft_make_plan(int L) {
   for (int i = 0; i < pl.nst; i++) {
     pl.p[i] = f[i];
     pl.s[i] = s;
+    // ceil(2^32 / s): q = umulhi(bi, magic) = floor(bi / s) for every bi < L * 4 here
+    pl.magic[i] = s == 1 ? 0u : (unsigned)((((unsigned long long)1 << 32) + s - 1) / s);
     s *= f[i];
   }
   return pl;
@@ -84,7 +86,9 @@ std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c) {
   double* fy = fx + pw;
   double* hx = fy + ph;
   double* hy = hx + pw;
-  double* ex = hy + ph;
+  double* omx = hy + ph;
+  double* omy = omx + pw;
+  double* ex = omy + ph;
   double* ey = ex + (size_t)F * pw;
   auto freq = [](int n, double* f) {  // np.fft.fftfreq(n) * 2 * pi
     double val = 1.0 / n;
@@ -96,8 +100,16 @@ std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c) {
   double smax = 0;
   for (int i = 0; i < c.n_scales; i++) smax = std::max(smax, c.scales[i]);
   double s_hp = c.dc_cut * c.lam * smax / (2 * PI);
-  for (int x = 0; x < pw; x++) hx[x] = std::exp(-(fx[x] * fx[x]) * (s_hp * s_hp) / 2);
-  for (int y = 0; y < ph; y++) hy[y] = std::exp(-(fy[y] * fy[y]) * (s_hp * s_hp) / 2);
+  for (int x = 0; x < pw; x++) {
+    double e = -(fx[x] * fx[x]) * (s_hp * s_hp) / 2;
+    hx[x] = std::exp(e);
+    omx[x] = -std::expm1(e);
+  }
+  for (int y = 0; y < ph; y++) {
+    double e = -(fy[y] * fy[y]) * (s_hp * s_hp) / 2;
+    hy[y] = std::exp(e);
+    omy[y] = -std::expm1(e);
+  }
   int k = 0;
   for (int si = 0; si < c.n_scales; si++) {
     double w0 = 2 * PI / (c.lam * c.scales[si]);
@@ -110,6 +122,25 @@ std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c) {
     }
   }
   return t;
+}
+
+void gabor_bind(GaborTables& g, const double* d64, const float* d32, int ph, int pw, int F) {
+  g.F = F;
+  g.ph = ph;
+  g.pw = pw;
+  g.fx = d64;
+  g.fy = g.fx + pw;
+  g.hx = g.fy + ph;
+  g.hy = g.hx + pw;
+  g.omx = g.hy + ph;
+  g.omy = g.omx + pw;
+  g.ex = g.omy + ph;
+  g.ey = g.ex + (size_t)F * pw;
+  g.hxf = d32 + pw + ph;
+  g.omxf = g.hxf + pw + ph;
+  g.omyf = g.omxf + pw;
+  g.exf = g.omyf + ph;
+  g.eyf = g.exf + (size_t)F * pw;
 }
 
 // ------------------------------------------------------------------------------------------ device
@@ -132,21 +163,63 @@ template <class C2> __device__ __forceinline__ C2 mkc(double re, double im);
 template <> __device__ __forceinline__ float2 mkc<float2>(double re, double im) { return make_float2((float)re, (float)im); }
 template <> __device__ __forceinline__ double2 mkc<double2>(double re, double im) { return make_double2(re, im); }
 
-// One Stockham stage of radix P from buffer A to buffer B (C interleaved lines of length L). Radices 2, 3,
-// 4, 5 and 8 have register butterflies; any other radix forms each output k as sum_j a_j w^{jk} with the
-// inputs read from shared memory and w^m = W[m L / P] from the twiddle table.
-template <class C2>
-__device__ __forceinline__ void fft_stage(const C2* __restrict__ A, C2* __restrict__ B, int C, int L, int P,
-                                          int s, const C2* __restrict__ tw, bool inv) {
-  const int m = L / (P * s);
-  const int nb = (L / P) * C;
-  const int LP = L / P;
+// Odd-radix butterfly with the symmetric form: for j = 1..(P-1)/2, a_j = v_j + v_{P-j}, b_j = v_j - v_{P-j};
+// o_0 = v_0 + sum a_j; o_k = v_0 + sum_j a_j cos_jk + i sum_j b_j sin_jk, o_{P-k} = the same with -i, where
+// w^{jk} = cos_jk + i sin_jk (w = exp(-2 pi i / P), conjugated for the inverse) is read from the twiddle table.
+template <int P, class C2, class Emit>
+__device__ __forceinline__ void odd_butterfly(const C2* in, size_t istep, const C2* __restrict__ tw, int LP, bool inv,
+                                              Emit emit) {
+  constexpr int Hh = (P - 1) / 2;
+  C2 v0 = in[0];
+  C2 av[Hh], bv[Hh];
+#pragma unroll
+  for (int j = 1; j <= Hh; j++) {
+    C2 x = in[j * istep], y = in[(P - j) * istep];
+    av[j - 1] = cadd(x, y);
+    bv[j - 1] = csub(x, y);
+  }
+  C2 s0 = v0;
+#pragma unroll
+  for (int j = 0; j < Hh; j++) s0 = cadd(s0, av[j]);
+  emit(0, s0);
+#pragma unroll
+  for (int k = 1; k <= Hh; k++) {
+    C2 t = v0, u = mkc<C2>(0.0, 0.0);
+#pragma unroll
+    for (int j = 1; j <= Hh; j++) {
+      C2 w = __ldg(tw + (size_t)((j * k) % P) * LP);
+      auto cs = w.x;
+      auto sn = inv ? -w.y : w.y;
+      t.x = fma(av[j - 1].x, cs, t.x);
+      t.y = fma(av[j - 1].y, cs, t.y);
+      u.x = fma(bv[j - 1].x, sn, u.x);
+      u.y = fma(bv[j - 1].y, sn, u.y);
+    }
+    // i u = (-u.y, u.x)
+    emit(k, mkc<C2>(t.x - u.y, t.y + u.x));
+    emit(P - k, mkc<C2>(t.x + u.y, t.y - u.x));
+  }
+}
+
+// One Stockham stage of radix P from buffer A to buffer B (C interleaved lines of length L, C = 1 << lc). q, r
+// of a butterfly come from multiplications by precomputed reciprocals (magic = ceil(2^32 / s), exact for the
+// sizes here). Radices 2, 4, 8 have hand-written butterflies, 3, 5, 7, 11 and 13 the symmetric odd form, and any
+// other radix (P = 0 here) a direct DFT with its inputs read from shared memory. Each radix is its own
+// non-inlined function, so that the registers of one radix's butterfly do not add to another's.
+template <int P, class C2>
+__device__ __noinline__ void stage_loop(const C2* __restrict__ A, C2* __restrict__ B, int lc, int L, int Pr, int s,
+                                        unsigned magic, const C2* __restrict__ tw, bool inv) {
+  const int RP = P ? P : Pr;
+  const int C = 1 << lc;
+  const int m = L / (RP * s);
+  const int nb = (L / RP) << lc;
+  const int LP = L / RP;
   const size_t istep = (size_t)s * m * C, ostep = (size_t)s * C;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-    int l = b % C, bi = b / C;
-    int q = bi / s, r = bi - q * s;
+    const int l = b & (C - 1), bi = b >> lc;
+    const int q = s == 1 ? bi : (int)__umulhi((unsigned)bi, magic), r = bi - q * s;
     const C2* in = A + (size_t)(r + s * q) * C + l;
-    C2* out = B + (size_t)(r + s * P * q) * C + l;
+    C2* out = B + (size_t)(r + s * RP * q) * C + l;
     auto emit = [&](int k, C2 val) {
       if (k > 0 && q > 0) {
         C2 w = __ldg(tw + (size_t)k * q * s);  // k q s < L
@@ -158,87 +231,72 @@ __device__ __forceinline__ void fft_stage(const C2* __restrict__ A, C2* __restri
       C2 w = __ldg(tw + (size_t)mm * LP);
       return inv ? conjf2(w) : w;
     };
-    switch (P) {
-      case 2: {
-        C2 a0 = in[0], a1 = in[istep];
-        emit(0, cadd(a0, a1));
-        emit(1, csub(a0, a1));
-        break;
-      }
-      case 4: {
-        C2 a0 = in[0], a1 = in[istep], a2 = in[2 * istep], a3 = in[3 * istep];
-        C2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
-        C2 t2 = cadd(a1, a3), t3 = rot(csub(a1, a3), inv);
-        emit(0, cadd(t0, t2));
-        emit(2, csub(t0, t2));
-        emit(1, cadd(t1, t3));
-        emit(3, csub(t1, t3));
-        break;
-      }
-      case 8: {
-        C2 v[8];
+    if constexpr (P == 2) {
+      C2 a0 = in[0], a1 = in[istep];
+      emit(0, cadd(a0, a1));
+      emit(1, csub(a0, a1));
+    } else if constexpr (P == 4) {
+      C2 a0 = in[0], a1 = in[istep], a2 = in[2 * istep], a3 = in[3 * istep];
+      C2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
+      C2 t2 = cadd(a1, a3), t3 = rot(csub(a1, a3), inv);
+      emit(0, cadd(t0, t2));
+      emit(2, csub(t0, t2));
+      emit(1, cadd(t1, t3));
+      emit(3, csub(t1, t3));
+    } else if constexpr (P == 8) {
+      C2 v[8];
 #pragma unroll
-        for (int j = 0; j < 8; j++) v[j] = in[j * istep];
-        C2 e[4], d[4];
-        {
-          C2 t0 = cadd(v[0], v[4]), t1 = csub(v[0], v[4]);
-          C2 t2 = cadd(v[2], v[6]), t3 = rot(csub(v[2], v[6]), inv);
-          e[0] = cadd(t0, t2); e[2] = csub(t0, t2); e[1] = cadd(t1, t3); e[3] = csub(t1, t3);
-        }
-        {
-          C2 t0 = cadd(v[1], v[5]), t1 = csub(v[1], v[5]);
-          C2 t2 = cadd(v[3], v[7]), t3 = rot(csub(v[3], v[7]), inv);
-          d[0] = cadd(t0, t2); d[2] = csub(t0, t2); d[1] = cadd(t1, t3); d[3] = csub(t1, t3);
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          C2 t = k == 0 ? d[0] : cmul(d[k], tw_m(k));
-          emit(k, cadd(e[k], t));
-          emit(k + 4, csub(e[k], t));
-        }
-        break;
+      for (int j = 0; j < 8; j++) v[j] = in[j * istep];
+      C2 e[4], d[4];
+      {
+        C2 t0 = cadd(v[0], v[4]), t1 = csub(v[0], v[4]);
+        C2 t2 = cadd(v[2], v[6]), t3 = rot(csub(v[2], v[6]), inv);
+        e[0] = cadd(t0, t2); e[2] = csub(t0, t2); e[1] = cadd(t1, t3); e[3] = csub(t1, t3);
       }
-      case 3: {
-        C2 a0 = in[0], a1 = in[istep], a2 = in[2 * istep];
-        C2 w1 = tw_m(1), w2 = tw_m(2);
-        emit(0, cadd(a0, cadd(a1, a2)));
-        emit(1, cadd(a0, cadd(cmul(a1, w1), cmul(a2, w2))));
-        emit(2, cadd(a0, cadd(cmul(a1, w2), cmul(a2, w1))));
-        break;
+      {
+        C2 t0 = cadd(v[1], v[5]), t1 = csub(v[1], v[5]);
+        C2 t2 = cadd(v[3], v[7]), t3 = rot(csub(v[3], v[7]), inv);
+        d[0] = cadd(t0, t2); d[2] = csub(t0, t2); d[1] = cadd(t1, t3); d[3] = csub(t1, t3);
       }
-      case 5: {
-        C2 a[5], w[5];
 #pragma unroll
-        for (int j = 0; j < 5; j++) {
-          a[j] = in[j * istep];
-          w[j] = tw_m(j);
-        }
-#pragma unroll
-        for (int k = 0; k < 5; k++) {
-          C2 acc = a[0];
-#pragma unroll
-          for (int j = 1; j < 5; j++) acc = cadd(acc, cmul(a[j], w[(j * k) % 5]));
-          emit(k, acc);
-        }
-        break;
+      for (int k = 0; k < 4; k++) {
+        C2 t = k == 0 ? d[0] : cmul(d[k], tw_m(k));
+        emit(k, cadd(e[k], t));
+        emit(k + 4, csub(e[k], t));
       }
-      default: {
-        for (int k = 0; k < P; k++) {
-          C2 acc = in[0];
-          int jk = 0;
-          for (int j = 1; j < P; j++) {
-            jk += k;
-            if (jk >= P) jk -= P;
-            C2 av = in[j * istep];
-            C2 w = tw_m(jk);
-            acc.x = fma(av.x, w.x, fma(-av.y, w.y, acc.x));
-            acc.y = fma(av.x, w.y, fma(av.y, w.x, acc.y));
-          }
-          emit(k, acc);
+    } else if constexpr (P == 3 || P == 5 || P == 7 || P == 11 || P == 13) {
+      odd_butterfly<P>(in, istep, tw, LP, inv, emit);
+    } else {
+      for (int k = 0; k < RP; k++) {
+        C2 acc = in[0];
+        int jk = 0;
+        for (int j = 1; j < RP; j++) {
+          jk += k;
+          if (jk >= RP) jk -= RP;
+          C2 av = in[j * istep];
+          C2 w = tw_m(jk);
+          acc.x = fma(av.x, w.x, fma(-av.y, w.y, acc.x));
+          acc.y = fma(av.x, w.y, fma(av.y, w.x, acc.y));
         }
-        break;
+        emit(k, acc);
       }
     }
+  }
+}
+
+template <class C2>
+__device__ __forceinline__ void fft_stage(const C2* __restrict__ A, C2* __restrict__ B, int lc, int L, int P, int s,
+                                          unsigned magic, const C2* __restrict__ tw, bool inv) {
+  switch (P) {
+    case 2: stage_loop<2, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
+    case 3: stage_loop<3, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
+    case 4: stage_loop<4, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
+    case 5: stage_loop<5, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
+    case 7: stage_loop<7, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
+    case 8: stage_loop<8, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
+    case 11: stage_loop<11, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
+    case 13: stage_loop<13, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
+    default: stage_loop<0, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
   }
   __syncthreads();
 }
@@ -251,8 +309,9 @@ __device__ C2* fft_run(C2* buf, C2* tmp, int C, const FftPlan& pl, bool inv) {
   const C2* tw;
   if constexpr (sizeof(C2) == sizeof(double2)) tw = (const C2*)pl.twd;
   else tw = (const C2*)pl.tw;
+  const int lc = C == 4 ? 2 : (C == 2 ? 1 : 0);
   for (int st = 0; st < pl.nst; st++) {
-    fft_stage<C2>(a, b, C, pl.L, pl.p[st], pl.s[st], tw, inv);
+    fft_stage<C2>(a, b, lc, pl.L, pl.p[st], pl.s[st], pl.magic[st], tw, inv);
     C2* t = a;
     a = b;
     b = t;
@@ -289,7 +348,7 @@ __device__ void prefilter_smem(float2* buf, int C, int n, double2* carry, double
       edge[l] = a;  // y[0]
     }
     // y[e0 - 1]
-    int start = e0 - 1 - IIR_WARM;
+    int start = e0 - 1 - IIR_WARM_F32;
     double2 y;
     if (start <= 0) {
       int hz = min(n, HORIZON);
@@ -340,7 +399,7 @@ __device__ void prefilter_smem(float2* buf, int C, int n, double2* carry, double
   const double g = z / (z * z - 1.0);
   if (live) {
     double2 c;
-    int stop = s0 + IIR_WARM;
+    int stop = s0 + IIR_WARM_F32;
     if (e0 == n) {
       double2 a = X(n - 1), b = X(n - 2);
       edge[C + l] = make_double2(g * (a.x + z * b.x), g * (a.y + z * b.y));
@@ -434,15 +493,22 @@ __global__ void __launch_bounds__(FFT_TMAX) k_fft_cols_filters(const C2* __restr
   for (int k = k0; k < k1; k++) {
     const double* exk = g.ex + (size_t)k * pw;
     const double* eyk = g.ey + (size_t)k * ph;
+    const float* exkf = g.exf + (size_t)k * pw;
+    const float* eykf = g.eyf + (size_t)k * ph;
     for (int v = 0; v < nvar; v++) {
       for (int i = threadIdx.x; i < ph * C; i += blockDim.x) {
         int y = i / C, l = i - y * C, x = min(x0 + l, pw - 1);
-        double G = (1.0 - g.hx[x] * g.hy[y]) * exk[x] * eyk[y];
         C2 sv = S[i];
-        double re = sv.x * G, im = sv.y * G;
-        if (v == 1) { double f = g.fx[x]; double t = re; re = -im * f; im = t * f; }        // x i fx
-        else if (v == 2) { double f = g.fy[y]; double t = re; re = -im * f; im = t * f; }   // x i fy
-        W1[i] = mkc<C2>(re, im);
+        if constexpr (sizeof(C2) == sizeof(float2)) {
+          float G = fmaf(g.hxf[x], g.omyf[y], g.omxf[x]) * (exkf[x] * eykf[y]);
+          W1[i] = mkc<C2>(sv.x * G, sv.y * G);
+        } else {
+          double G = fma(g.hx[x], g.omy[y], g.omx[x]) * exk[x] * eyk[y];
+          double re = sv.x * G, im = sv.y * G;
+          if (v == 1) { double f = g.fx[x]; double t = re; re = -im * f; im = t * f; }        // x i fx
+          else if (v == 2) { double f = g.fy[y]; double t = re; re = -im * f; im = t * f; }   // x i fy
+          W1[i] = mkc<C2>(re, im);
+        }
       }
       __syncthreads();
       C2* res = fft_run(W1, W2, C, plh, true);
@@ -459,7 +525,7 @@ __global__ void __launch_bounds__(FFT_TMAX) k_fft_cols_filters(const C2* __restr
   }
 }
 
-__global__ void __launch_bounds__(FFT_TMAX) k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int ph,
+__global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int ph,
                                                                 float scale, float2* __restrict__ R) {
   extern __shared__ float2 sm[];
   const int pw = plw.L;
@@ -489,15 +555,23 @@ __global__ void __launch_bounds__(FFT_TMAX) k_fft_rows_inv_ref(const C2* __restr
   const int y = blockIdx.x, kk = blockIdx.y, k = k0 + kk;  // y: row of the W x H crop
   const size_t plane = (size_t)ph * pw;
   for (int i = threadIdx.x; i < pw * 3; i += blockDim.x) {
-    int x = i / 3, v = i - 3 * x;
+    int v = i / pw, x = i - v * pw;
     sm[i] = U[(size_t)(3 * kk + v) * plane + (size_t)(y + PAD) * pw + x];
   }
   __syncthreads();
-  C2* r = fft_run(sm, t, 3, plw, true);
+  C2* rr[3];
+  for (int v = 0; v < 3; v++) {
+    C2* res = fft_run(sm + v * pw, t, 1, plw, true);
+    if (res != sm + v * pw) {
+      for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[v * pw + x] = res[x];
+      __syncthreads();
+    }
+    rr[v] = sm + v * pw;
+  }
   const double sc = 1.0 / ((double)ph * (double)pw);
   for (int x = threadIdx.x; x < W; x += blockDim.x) {
     int xp = x + PAD;
-    C2 a = r[xp * 3], b = r[xp * 3 + 1], c = r[xp * 3 + 2];
+    C2 a = rr[0][xp], b = rr[1][xp], c = rr[2][xp];
     double rre = a.x * sc, rim = a.y * sc;
     double xre = b.x * sc, xim = b.y * sc, yre = c.x * sc, yim = c.y * sc;
     double a2 = rre * rre + rim * rim + 1e-12;
@@ -510,7 +584,7 @@ __global__ void __launch_bounds__(FFT_TMAX) k_fft_rows_inv_ref(const C2* __restr
   }
 }
 
-__global__ void __launch_bounds__(FFT_TMAX) k_fft_lines(float2* data, FftPlan pl, int inv) {
+__global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_lines(float2* data, FftPlan pl, int inv) {
   extern __shared__ float2 sm[];
   float2* row = data + (size_t)blockIdx.x * pl.L;
   for (int x = threadIdx.x; x < pl.L; x += blockDim.x) sm[x] = row[x];
@@ -543,8 +617,7 @@ bool fft_fits(int ph, int pw) {
     size_t sm;
     cols_C(ph, sizeof(float2), true, T, sm);
     cols_C(ph, sizeof(double2), false, T, sm);
-    fft_threads(pw, 3);
-    return 6 * (size_t)pw * sizeof(double2) <= SMEM_MAX;
+    return 4 * (size_t)pw * sizeof(double2) <= SMEM_MAX;
   } catch (const Error&) {
     return false;
   }
@@ -594,8 +667,8 @@ void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F
 
 void launch_fft_rows_inv_ref_f64(const double2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,
                                  float4* ref4, float* amp, cudaStream_t st) {
-  int T = fft_threads(plw.L, 3);
-  size_t sm = (size_t)6 * plw.L * sizeof(double2);
+  int T = fft_threads(plw.L, 1);
+  size_t sm = (size_t)4 * plw.L * sizeof(double2);
   set_smem((const void*)k_fft_rows_inv_ref<double2>, sm);
   dim3 grid(H, k1 - k0);
   OFC_LAUNCH(k_fft_rows_inv_ref<double2>, grid, T, sm, st, U, plw, ph, W, H, k0, ref4, amp);

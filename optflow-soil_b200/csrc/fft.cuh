@@ -16,6 +16,7 @@ struct FftPlan {
   int nst = 0;
   int p[FFT_MAXST] = {};
   int s[FFT_MAXST] = {};
+  unsigned magic[FFT_MAXST] = {};
   const float2* tw = nullptr;
   const double2* twd = nullptr;  // the same table in float64
 };
@@ -31,20 +32,21 @@ std::vector<double2> fft_twiddles_f64(int L);
 // threads of a block that transforms C interleaved lines of length L (multiple of C and of 32)
 int fft_threads(int L, int C);
 
-// Separable Gabor tables of one padded size (gabor_bank, phaseflow.py:73-89), float64 on the device:
-//   fx[pw], fy[ph]: the frequency grids (np.fft.fftfreq * 2 pi)
-//   hx[pw], hy[ph]: exp(-f^2 s_hp^2 / 2), so the DC high-pass is 1 - hx[x] hy[y]
-//   ex[F][pw], ey[F][ph]: the separable factors of filter k's Gaussian
+// Separable Gabor tables of one padded size (gabor_bank, phaseflow.py:73-89). Filter k is
+//   G_k(x, y) = hp(x, y) ex_k[x] ey_k[y],  hp = 1 - hx[x] hy[y] = omx[x] + hx[x] omy[y]
+// with hx = exp(-f^2 s_hp^2 / 2) and omx = 1 - hx = -expm1(-f^2 s_hp^2 / 2) (no cancellation near DC), the
+// frequency grids fx, fy = np.fft.fftfreq * 2 pi, and the Gaussian factors ex_k, ey_k of filter k. float64 tables
+// (the reference pack) and float32 copies (the responses).
 struct GaborTables {
   int F = 0, ph = 0, pw = 0;
-  const double* fx = nullptr;
-  const double* fy = nullptr;
-  const double* hx = nullptr;
-  const double* hy = nullptr;
-  const double* ex = nullptr;
-  const double* ey = nullptr;
+  const double *fx = nullptr, *fy = nullptr, *hx = nullptr, *hy = nullptr, *omx = nullptr, *omy = nullptr;
+  const double *ex = nullptr, *ey = nullptr;
+  const float *hxf = nullptr, *omxf = nullptr, *omyf = nullptr, *exf = nullptr, *eyf = nullptr;
 };
-std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c);  // layout as above, contiguous
+// host tables: float64 [fx pw | fy ph | hx pw | hy ph | omx pw | omy ph | ex F*pw | ey F*ph]
+std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c);
+// binds g to a device copy of the tables: d64 (the host float64 vector) and d32 (its float32 image)
+void gabor_bind(GaborTables& g, const double* d64, const float* d32, int ph, int pw, int F);
 
 // forward row transforms of the reflect-padded real image img (W x H) -> out (ph x pw), float32 or float64
 void launch_fft_rows_fwd_real(const float* img, int W, int H, const FftPlan& plw, int ph, float2* out,

@@ -168,12 +168,17 @@ void launch_warp(const float* c2, int w2, int h2, const double* sx, const double
 }
 
 // ---------------------------------------------------------------- accumulate
-__global__ void __launch_bounds__(128) k_accumulate(const float4* __restrict__ ref4, const float* __restrict__ amp,
-                                                    const float2* __restrict__ R, int F, int ph, int pw,
-                                                    const double* __restrict__ ux, const double* __restrict__ uy,
-                                                    const double* __restrict__ sx, const double* __restrict__ sy,
-                                                    const double* __restrict__ csx, const double* __restrict__ csy,
-                                                    int W, int H, double* __restrict__ sums) {
+// One pixel per thread. The fixed point X' + s(X') = X + u(X) and the positions are float64; the twelve
+// responses are sampled with float32 weights and accumulation (they are stored as complex float32), and
+// the phase difference angle(r1 conj(r2)) is taken in float32 (the inputs carry float32 precision, the angle
+// is then exact to ~1e-7 rad); c = dphi + gx u + gy v and the seven sums are float64, since u reaches tens of
+// pixels and the residual sum gcc - theta . b cancels.
+__global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict__ ref4, const float* __restrict__ amp,
+                                                      const float2* __restrict__ R, int F, int ph, int pw,
+                                                      const double* __restrict__ ux, const double* __restrict__ uy,
+                                                      const double* __restrict__ sx, const double* __restrict__ sy,
+                                                      const double* __restrict__ csx, const double* __restrict__ csy,
+                                                      int W, int H, double* __restrict__ sums) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int y = blockIdx.y;
   if (x >= W) return;
@@ -197,32 +202,53 @@ __global__ void __launch_bounds__(128) k_accumulate(const float4* __restrict__ r
   }
   double a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
   Taps t;
-  bool ok = make_taps(px + PAD, py + PAD, pw, ph, t);
+  const bool ok = make_taps(px + PAD, py + PAD, pw, ph, t);
+  float fwx[4], fwy[4];
+  int off[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    fwx[k] = (float)t.wx[k];
+    fwy[k] = (float)t.wy[k];
+    off[k] = t.yi[k] * pw;
+  }
   const size_t plane = (size_t)ph * pw;
+  const float fnan = __int_as_float(0x7fc00000);
   for (int k = 0; k < F; k++) {
-    float4 r1 = __ldg(ref4 + (size_t)k * N + p);
-    double a1k = (double)__ldg(amp + (size_t)k * N + p);
-    double br, bi;
+    const float4 r1 = __ldg(ref4 + (size_t)k * N + p);
+    const float a1k = __ldg(amp + (size_t)k * N + p);
+    float br = fnan, bi = fnan;
     if (ok) {
-      float2 r2 = sample_c32(R + (size_t)k * plane, pw, t);
-      br = r2.x;
-      bi = r2.y;
-    } else {
-      br = bi = nan("");
+      const float2* Rk = R + (size_t)k * plane;
+      br = 0.f;
+      bi = 0.f;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const float2* row = Rk + off[j];
+        float are = 0.f, aim = 0.f;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          float2 c = __ldg(row + t.xi[q]);
+          are = fmaf(fwx[q], c.x, are);
+          aim = fmaf(fwx[q], c.y, aim);
+        }
+        br = fmaf(fwy[j], are, br);
+        bi = fmaf(fwy[j], aim, bi);
+      }
     }
     // r1 conj(r2)
-    double re = (double)r1.x * br + (double)r1.y * bi;
-    double im = (double)r1.y * br - (double)r1.x * bi;
-    double dphi = atan2(im, re);
-    double wk = a1k * sqrt(br * br + bi * bi);
-    double gx = r1.z, gy = r1.w;
-    double c = dphi + gx * u + gy * v;
-    a0 += wk * gx * gx;
-    a1 += wk * gx * gy;
-    a2 += wk * gy * gy;
-    a3 += wk * gx * c;
-    a4 += wk * gy * c;
-    a5 += wk * c * c;
+    const float re = fmaf(r1.x, br, r1.y * bi);
+    const float im = fmaf(r1.y, br, -r1.x * bi);
+    const double dphi = (double)atan2f(im, re);
+    const double wk = (double)(a1k * sqrtf(fmaf(br, br, bi * bi)));
+    const double gx = r1.z, gy = r1.w;
+    const double c = dphi + gx * u + gy * v;
+    const double wgx = wk * gx, wgy = wk * gy;
+    a0 = fma(wgx, gx, a0);
+    a1 = fma(wgx, gy, a1);
+    a2 = fma(wgy, gy, a2);
+    a3 = fma(wgx, c, a3);
+    a4 = fma(wgy, c, a4);
+    a5 = fma(wk * c, c, a5);
     a6 += wk;
   }
   sums[p] = a0;
@@ -297,6 +323,9 @@ __host__ __device__ constexpr MomTable build_table(int order) {
 
 int moment_yplanes(int order) { return build_table(order).ny; }
 
+// The window taps k(t) t^p are symmetric in t for even p and antisymmetric for odd p, so each pass pairs
+// the samples at +t and -t: sum_t k(t) t^p a(q + t) = [p == 0] k(0) a(q) + sum_{t >= 1} k(t) t^p (a(q + t) +- a(q - t)),
+// which halves the float64 multiply-adds (the passes are float64-throughput bound).
 template <int ORDER>
 __global__ void __launch_bounds__(128) k_moments_y(const double* __restrict__ sums, int W, int H,
                                                    const double* __restrict__ mtaps, int r,
@@ -310,14 +339,23 @@ __global__ void __launch_bounds__(128) k_moments_y(const double* __restrict__ su
   double acc[T.ny];
 #pragma unroll
   for (int j = 0; j < T.ny; j++) acc[j] = 0;
-  for (int t = -r; t <= r; t++) {
-    int yy = min(max(y + t, 0), H - 1);
-    size_t q = (size_t)yy * W + x;
-    double s[7];
 #pragma unroll
-    for (int i = 0; i < 7; i++) s[i] = sums[i * N + q];
+  for (int j = 0; j < T.ny; j++)
+    acc[j] = T.ypow[j] == 0 ? mtaps[r] * sums[(size_t)T.ysrc[j] * N + (size_t)y * W + x] : 0.0;
+  for (int t = 1; t <= r; t++) {
+    const size_t op = (size_t)min(y + t, H - 1) * W + x, om = (size_t)max(y - t, 0) * W + x;
 #pragma unroll
-    for (int j = 0; j < T.ny; j++) acc[j] += mtaps[T.ypow[j] * K + t + r] * s[T.ysrc[j]];
+    for (int src = 0; src < 7; src++) {
+      bool used = false;
+#pragma unroll
+      for (int j = 0; j < T.ny; j++) used |= T.ysrc[j] == src;
+      if (!used) continue;
+      const double ap = sums[(size_t)src * N + op], am = sums[(size_t)src * N + om];
+      const double sp = ap + am, dm = ap - am;
+#pragma unroll
+      for (int j = 0; j < T.ny; j++)
+        if (T.ysrc[j] == src) acc[j] = fma(mtaps[T.ypow[j] * K + r + t], (T.ypow[j] & 1) ? dm : sp, acc[j]);
+    }
   }
   size_t p = (size_t)y * W + x;
 #pragma unroll
@@ -325,13 +363,14 @@ __global__ void __launch_bounds__(128) k_moments_y(const double* __restrict__ su
 }
 
 template <int N>
-__device__ bool cholesky_solve_dev(double (&M)[N * N], double (&b)[N]) {
+__device__ __forceinline__ bool cholesky_solve_dev(double (&M)[N * N], double (&b)[N]) {
+  bool okp = true;
 #pragma unroll
   for (int j = 0; j < N; j++) {
     double d = M[j * N + j];
 #pragma unroll
     for (int k = 0; k < j; k++) d -= M[j * N + k] * M[j * N + k];
-    if (!(d > 0.0 && d <= DBL_MAX)) return false;
+    okp &= d > 0.0 && d <= DBL_MAX;  // a failed pivot goes on with meaningless values and reports false
     double l = sqrt(d);
     M[j * N + j] = l;
 #pragma unroll
@@ -356,7 +395,7 @@ __device__ bool cholesky_solve_dev(double (&M)[N * N], double (&b)[N]) {
     for (int k = i + 1; k < N; k++) s -= M[k * N + i] * b[k];
     b[i] = s / M[i * N + i];
   }
-  bool fin = true;
+  bool fin = okp;
 #pragma unroll
   for (int i = 0; i < N; i++) fin &= isfinite(b[i]);
   return fin;
@@ -377,17 +416,21 @@ __global__ void __launch_bounds__(128) k_moments_x_solve(const double* __restric
   if (x >= W) return;
   const size_t N = (size_t)W * H;
   const int K = 2 * r + 1;
+  // one pass over the tap pairs t = 1..r with every moment's accumulator live (independent chains)
   double m[T.nm];
-#pragma unroll
-  for (int i = 0; i < T.nm; i++) m[i] = 0;
   const double* row = yplanes + (size_t)y * W;
-  for (int t = -r; t <= r; t++) {
-    int xx = min(max(x + t, 0), W - 1);
-    double yv[T.ny];
 #pragma unroll
-    for (int j = 0; j < T.ny; j++) yv[j] = row[j * N + xx];
+  for (int i = 0; i < T.nm; i++) m[i] = T.mpx[i] == 0 ? mtaps[r] * row[(size_t)T.mjob[i] * N + x] : 0.0;
+  for (int t = 1; t <= r; t++) {
+    const int xp = min(x + t, W - 1), xm = max(x - t, 0);
 #pragma unroll
-    for (int i = 0; i < T.nm; i++) m[i] += mtaps[T.mpx[i] * K + t + r] * yv[T.mjob[i]];
+    for (int j = 0; j < T.ny; j++) {
+      const double ap = row[(size_t)j * N + xp], am = row[(size_t)j * N + xm];
+      const double sp = ap + am, dm = ap - am;
+#pragma unroll
+      for (int i = 0; i < T.nm; i++)
+        if (T.mjob[i] == j) m[i] = fma(mtaps[T.mpx[i] * K + r + t], (T.mpx[i] & 1) ? dm : sp, m[i]);
+    }
   }
   const size_t p = (size_t)y * W + x;
   double M[n * n], b[n], b0[n];
@@ -733,30 +776,59 @@ void launch_within(const uint8_t* src, int W, int H, double limit, int mode, uin
 }
 
 // ---------------------------------------------------------------- trusted pre-warp
-// column sweeps: nearest ok pixel of the column (ties to the smaller row): col_d2 = dy^2 (or -1), col_row
+// Nearest ok pixel of each pixel's column (ties to the smaller row): col_d2 = dy^2 (or -1 without one), col_row.
+// Two levels: k_col_segments records, per column and segment of CSEG rows, the first and last ok row; each pixel
+// then scans its own segment and, beyond it, the segments' summaries (at most H / CSEG of them).
+constexpr int CSEG = 64;
+
+__global__ void k_col_segments(const uint8_t* __restrict__ ok, int W, int H, const PrewarpCounts* c,
+                               int* __restrict__ seg_first, int* __restrict__ seg_last) {
+  if (!(c->low > 0 && c->ok > 0 && c->ok < W * H)) return;
+  int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int sg = blockIdx.y;
+  if (x >= W) return;
+  int y0 = sg * CSEG, y1 = min(H, y0 + CSEG);
+  int first = -1, last = -1;
+  for (int y = y0; y < y1; y++)
+    if (ok[(size_t)y * W + x]) {
+      if (first < 0) first = y;
+      last = y;
+    }
+  seg_first[(size_t)sg * W + x] = first;
+  seg_last[(size_t)sg * W + x] = last;
+}
+
 __global__ void k_col_nearest(const uint8_t* __restrict__ ok, int W, int H, const PrewarpCounts* c,
+                              const int* __restrict__ seg_first, const int* __restrict__ seg_last,
                               int* __restrict__ col_d2, int* __restrict__ col_row) {
   if (!(c->low > 0 && c->ok > 0 && c->ok < W * H)) return;
   int x = blockIdx.x * blockDim.x + threadIdx.x;
+  int y = blockIdx.y;
   if (x >= W) return;
-  int last = -1;
-  for (int y = 0; y < H; y++) {
-    size_t p = (size_t)y * W + x;
-    if (ok[p]) last = y;
-    col_row[p] = last;  // nearest above (or at)
+  const size_t p = (size_t)y * W + x;
+  const int sg = y / CSEG, y0 = sg * CSEG, y1 = min(H, y0 + CSEG);
+  int up = -1, dn = -1;
+  for (int yy = y; yy >= y0; yy--)
+    if (ok[(size_t)yy * W + x]) { up = yy; break; }
+  if (up < 0)
+    for (int s2 = sg - 1; s2 >= 0; s2--) {
+      int l = seg_last[(size_t)s2 * W + x];
+      if (l >= 0) { up = l; break; }
+    }
+  for (int yy = y; yy < y1; yy++)
+    if (ok[(size_t)yy * W + x]) { dn = yy; break; }
+  if (dn < 0) {
+    const int nseg = (H + CSEG - 1) / CSEG;
+    for (int s2 = sg + 1; s2 < nseg; s2++) {
+      int f = seg_first[(size_t)s2 * W + x];
+      if (f >= 0) { dn = f; break; }
+    }
   }
-  int next = -1;
-  for (int y = H - 1; y >= 0; y--) {
-    size_t p = (size_t)y * W + x;
-    if (ok[p]) next = y;
-    int up = col_row[p];
-    int r = -1;
-    long d = -1;
-    if (up >= 0) { r = up; d = (long)(y - up); }
-    if (next >= 0 && (r < 0 || (long)(next - y) < d)) { r = next; d = next - y; }
-    col_row[p] = r;
-    col_d2[p] = r < 0 ? -1 : (int)(d * d);
-  }
+  int r = up;
+  long d = up >= 0 ? (long)(y - up) : -1;
+  if (dn >= 0 && (r < 0 || (long)(dn - y) < d)) { r = dn; d = dn - y; }
+  col_row[p] = r;
+  col_d2[p] = r < 0 ? -1 : (int)(d * d);
 }
 
 // for every pixel that is not ok: the nearest ok pixel (smallest (d^2, column, row)), then the first-order
@@ -810,7 +882,10 @@ void launch_prewarp_fill(const uint8_t* low, const double* ux, const double* uy,
   // ok = distance to the nearest low pixel > R (gated on any low pixel)
   OFC_LAUNCH(k_vdist, g, 128, 0, st, low, W, H, cap, vdist, (const int*)&counts->low);
   OFC_LAUNCH(k_within, g, 128, 0, st, vdist, W, H, cap, R, 1, ok, (const int*)&counts->low, &counts->ok);
-  OFC_LAUNCH(k_col_nearest, div_up(W, 128), 128, 0, st, ok, W, H, counts, col_d2, col_row);
+  int* seg = vdist;  // the vertical distances are spent: 2 * ceil(H / CSEG) * W ints of segment summaries
+  const int nseg = (H + CSEG - 1) / CSEG;
+  OFC_LAUNCH(k_col_segments, dim3(div_up(W, 128), nseg), 128, 0, st, ok, W, H, counts, seg, seg + (size_t)nseg * W);
+  OFC_LAUNCH(k_col_nearest, g, 128, 0, st, ok, W, H, counts, seg, seg + (size_t)nseg * W, col_d2, col_row);
   OFC_LAUNCH(k_extrapolate, g, 128, 0, st, ok, col_d2, col_row, ux, uy, slope, W, H, counts, ux_pre, uy_pre);
 }
 

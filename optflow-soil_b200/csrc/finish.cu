@@ -7,11 +7,18 @@
 namespace ofc {
 
 // ---------------------------------------------------------------- 4-connected components (union-find)
-__device__ __forceinline__ int uf_find(const int* parent, int x) {
-  int p = __ldcg(parent + x);
+// find with path splitting: parent pointers only ever move to ancestors (smaller indices), so the plain stores
+// of the splitting keep every pointer an ancestor while other threads link roots by atomicCAS. Every access is
+// volatile: the compiler must neither keep a pointer in a register across another thread's update nor forward
+// this thread's own store to a later load.
+__device__ __forceinline__ int uf_find(int* parent, int x) {
+  volatile int* vp = parent;
+  int p = vp[x];
   while (p != x) {
+    int gp = vp[p];
+    if (gp != p) vp[x] = gp;
     x = p;
-    p = __ldcg(parent + x);
+    p = gp;
   }
   return x;
 }
@@ -45,19 +52,33 @@ __global__ void k_ccl_merge(const uint8_t* __restrict__ b, int W, int H, int* pa
   if (y + 1 < H && b[p + W]) uf_union(parent, p, p + W);
 }
 
-__global__ void k_ccl_count(const uint8_t* __restrict__ b, int n, int* parent, int* size) {
+// after the merge: every pixel points to its root. The walk only reads (a splitting write could put an
+// intermediate ancestor over another thread's root store), and every store is a root.
+__global__ void k_ccl_flatten(const uint8_t* __restrict__ b, int n, int* parent) {
+  volatile int* vp = parent;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     if (!b[p]) continue;
-    int r = uf_find(parent, p);
-    atomicAdd(size + r, 1);
+    int x = p, q = vp[x];
+    while (q != x) {
+      x = q;
+      q = vp[x];
+    }
+    vp[p] = x;
   }
 }
 
-__global__ void k_ccl_mark(const uint8_t* __restrict__ b, int n, const int* parent, const int* size, double min_area,
-                           uint8_t* out) {
+__global__ void k_ccl_count(const uint8_t* __restrict__ b, int n, const int* __restrict__ parent, int* size) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    if (!b[p]) continue;
+    atomicAdd(size + parent[p], 1);
+  }
+}
+
+__global__ void k_ccl_mark(const uint8_t* __restrict__ b, int n, const int* __restrict__ parent,
+                           const int* __restrict__ size, double min_area, uint8_t* out) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     uint8_t v = 0;
-    if (b[p]) v = (double)size[uf_find(parent, p)] >= min_area;
+    if (b[p]) v = (double)size[parent[p]] >= min_area;
     out[p] = v;
   }
 }
@@ -68,6 +89,7 @@ void launch_large_components(const uint8_t* b, int W, int H, double min_area, in
   unsigned g = std::min(div_up(n, 256), 8192u);
   OFC_LAUNCH(k_ccl_init, g, 256, 0, st, b, n, parent, size);
   OFC_LAUNCH(k_ccl_merge, dim3(div_up(W, 128), H), 128, 0, st, b, W, H, parent);
+  OFC_LAUNCH(k_ccl_flatten, g, 256, 0, st, b, n, parent);
   OFC_LAUNCH(k_ccl_count, g, 256, 0, st, b, n, parent, size);
   OFC_LAUNCH(k_ccl_mark, g, 256, 0, st, b, n, parent, size, min_area, out);
 }

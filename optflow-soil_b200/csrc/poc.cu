@@ -30,52 +30,74 @@ void launch_downsample(const double* in, int W, int H, double* out, double* tmp,
   OFC_LAUNCH(k_corr_x_decimate, g, 128, 0, st, tmp, W, H, taps, r, out);
 }
 
-// ---------------------------------------------------------------- float64 power-of-two FFT in smem
+// ---------------------------------------------------------------- float64 FFTs inside one warp
+// A line of n = 16, 32 or 64 complex values lives in a warp: n = 64 as (v0, v1) = (x[l], x[l + 32]) in lane l;
+// n = 32 as v0 = x[l]; n = 16 as v0 = x[l & 15] (lanes 16..31 hold a second line). Radix-2 butterflies
+// across lanes use shuffles; twiddles W_64^t come from a shared table (W_{2h}^j = W_64^{j 32 / h}).
+// dif: natural order in, bit-reversed out; dit: bit-reversed in, natural out.
 __device__ __forceinline__ double2 dmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-
-// one radix-2 Stockham stage over `nlines` lines of length n (element i of line l at l * ls + i * es);
-// tw64: W_64^t = exp(-2 pi i t / 64), t < 64 (n divides 64)
-__device__ void fft2_stage_d(double2* Z, int n, int nlines, int es, int ls, int s, const double2* tw64, bool inv) {
-  const int m = n / (2 * s);
-  const int nb = (n / 2) * nlines;
-  constexpr int MB = POC_MAXN / 2 / POC_T;  // 8 butterflies per thread at most
-  double2 v0[MB], v1[MB];
-#pragma unroll
-  for (int i = 0; i < MB; i++) {
-    int b = threadIdx.x + i * POC_T;
-    if (b < nb) {
-      int l = b % nlines, bi = b / nlines;
-      int q = bi / s, r = bi - q * s;
-      v0[i] = Z[l * ls + (r + s * q) * es];
-      v1[i] = Z[l * ls + (r + s * (q + m)) * es];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < MB; i++) {
-    int b = threadIdx.x + i * POC_T;
-    if (b < nb) {
-      int l = b % nlines, bi = b / nlines;
-      int q = bi / s, r = bi - q * s;
-      double2 o0 = make_double2(v0[i].x + v1[i].x, v0[i].y + v1[i].y);
-      double2 o1 = make_double2(v0[i].x - v1[i].x, v0[i].y - v1[i].y);
-      if (q > 0) {
-        double2 w = tw64[(q * s) * (64 / n)];
-        if (inv) w.y = -w.y;
-        o1 = dmul(o1, w);
-      }
-      Z[l * ls + (r + s * 2 * q) * es] = o0;
-      Z[l * ls + (r + s * (2 * q + 1)) * es] = o1;
-    }
-  }
-  __syncthreads();
+__device__ __forceinline__ double2 shfl_xor_d2(double2 v, int m) {
+  return make_double2(__shfl_xor_sync(0xffffffff, v.x, m), __shfl_xor_sync(0xffffffff, v.y, m));
+}
+__device__ __forceinline__ double2 twid(const double2* tw64, int t, bool inv) {
+  double2 w = tw64[t];
+  return inv ? make_double2(w.x, -w.y) : w;
 }
 
-__device__ void fft2d_d(double2* Z, int h, int w, const double2* tw64, bool inv) {
-  for (int s = 1; s < w; s *= 2) fft2_stage_d(Z, w, h, 1, w, s, tw64, inv);   // rows
-  for (int s = 1; s < h; s *= 2) fft2_stage_d(Z, h, w, w, 1, s, tw64, inv);   // columns
+__device__ __forceinline__ void warp_dif(double2& v0, double2& v1, int n, bool inv, const double2* tw64) {
+  const int l = threadIdx.x & 31;
+  int top = n / 2;
+  if (n == 64) {
+    double2 a = make_double2(v0.x + v1.x, v0.y + v1.y);
+    double2 b = dmul(make_double2(v0.x - v1.x, v0.y - v1.y), twid(tw64, l, inv));
+    v0 = a;
+    v1 = b;
+    top = 16;
+  }
+  for (int h = top; h >= 1; h >>= 1) {
+    const bool up = (l & h) != 0;
+    const double2 w = twid(tw64, (l & (h - 1)) * (32 / h), inv);
+    double2 p0 = shfl_xor_d2(v0, h);
+    v0 = up ? dmul(make_double2(p0.x - v0.x, p0.y - v0.y), w) : make_double2(v0.x + p0.x, v0.y + p0.y);
+    if (n == 64) {
+      double2 p1 = shfl_xor_d2(v1, h);
+      v1 = up ? dmul(make_double2(p1.x - v1.x, p1.y - v1.y), w) : make_double2(v1.x + p1.x, v1.y + p1.y);
+    }
+  }
+}
+
+__device__ __forceinline__ void warp_dit(double2& v0, double2& v1, int n, bool inv, const double2* tw64) {
+  const int l = threadIdx.x & 31;
+  const int top = n == 64 ? 16 : n / 2;
+  for (int h = 1; h <= top; h <<= 1) {
+    const bool up = (l & h) != 0;
+    const double2 w = twid(tw64, (l & (h - 1)) * (32 / h), inv);
+    double2 t0 = up ? dmul(v0, w) : v0;
+    double2 p0 = shfl_xor_d2(t0, h);
+    v0 = up ? make_double2(p0.x - t0.x, p0.y - t0.y) : make_double2(t0.x + p0.x, t0.y + p0.y);
+    if (n == 64) {
+      double2 t1 = up ? dmul(v1, w) : v1;
+      double2 p1 = shfl_xor_d2(t1, h);
+      v1 = up ? make_double2(p1.x - t1.x, p1.y - t1.y) : make_double2(t1.x + p1.x, t1.y + p1.y);
+    }
+  }
+  if (n == 64) {
+    double2 t = dmul(v1, twid(tw64, l, inv));
+    double2 a = make_double2(v0.x + t.x, v0.y + t.y), b = make_double2(v0.x - t.x, v0.y - t.y);
+    v0 = a;
+    v1 = b;
+  }
+}
+
+__device__ __forceinline__ int brev(int i, int bits) { return (int)(__brev((unsigned)i) >> (32 - bits)); }
+__device__ __forceinline__ int ilog2(int n) { return 31 - __clz(n); }
+
+// position -> natural index for the element held in register r of lane l of a length-n line
+__device__ __forceinline__ int pos_of(int r, int n) {
+  const int l = threadIdx.x & 31;
+  return n == 64 ? r * 32 + l : (n == 32 ? l : (l & 15));
 }
 
 __device__ double block_sum_d(double v, double* red) {
@@ -85,12 +107,8 @@ __device__ double block_sum_d(double v, double* red) {
   if (lane == 0) red[wid] = v;
   __syncthreads();
   double t = 0;
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < POC_T / 32; i++) t += red[i];
-    red[POC_T / 32] = t;
-  }
-  __syncthreads();
-  return red[POC_T / 32];
+  for (int i = 0; i < POC_T / 32; i++) t += red[i];
+  return t;
 }
 
 struct PocConst {
@@ -98,55 +116,113 @@ struct PocConst {
   double hy[64], hx[64];
 };
 
-// poc_shift (poc.py:39-54) of the window B at (x0, y0) of image b against the stored spectrum of A
-// (on the low-pass support only, alp); returns dx, dy, peak in res[0..2]
-__device__ void poc_shift_dev(const double* __restrict__ b, int W, int x0, int y0, int wy, int wx, const PocConst& pc,
-                              const double2* alp, int nly, int nlx, double lpm, double2* Z, double* red, double* res) {
-  const int n = wy * wx;
-  double s = 0;
-  for (int i = threadIdx.x; i < n; i += POC_T) {
-    int r = i / wx, q = i - r * wx;
-    double v = b[(size_t)(y0 + r) * W + x0 + q];
-    Z[i] = make_double2(v, 0);
-    s += v;
-  }
-  double mean = block_sum_d(s, red) / n;
-  for (int i = threadIdx.x; i < n; i += POC_T) {
-    int r = i / wx, q = i - r * wx;
-    Z[i] = make_double2((Z[i].x - mean) * (pc.hy[r * (64 / wy)] * pc.hx[q * (64 / wx)]), 0);
-  }
-  __syncthreads();
-  fft2d_d(Z, wy, wx, pc.tw64, false);
-  // C = B conj(A) / (|.| + 1e-12) on the low-pass support, zero elsewhere
-  const int qy = wy / 4, qx = wx / 4;
-  for (int i = threadIdx.x; i < n; i += POC_T) {
-    int ky = i / wx, kx = i - ky * wx;
-    int iy = ky <= qy ? ky : (ky >= wy - qy ? ky - (wy - 2 * qy - 1) : -1);
-    int ix = kx <= qx ? kx : (kx >= wx - qx ? kx - (wx - 2 * qx - 1) : -1);
-    double2 c = make_double2(0, 0);
-    if (iy >= 0 && ix >= 0) {
-      double2 B = Z[i], A = alp[iy * nlx + ix];
-      c = make_double2(B.x * A.x + B.y * A.y, B.y * A.x - B.x * A.y);
-      double mag = hypot(c.x, c.y) + 1e-12;
-      c.x /= mag;
-      c.y /= mag;
+// lines of a window handled by warp `wid` in a pass over `nlines` lines of length n: n = 16 packs two lines
+// per warp
+__device__ __forceinline__ int lines_per_warp(int n) { return n == 16 ? 2 : 1; }
+
+// Row transforms of a real window (values win(y, x), window mean removed, Hann weighted) into Z (natural
+// order, Z[y * wx + kx]).
+template <class Get>
+__device__ void rows_forward(Get get, double mean, int wy, int wx, const PocConst& pc, double2* Z) {
+  const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int lpw = lines_per_warp(wx), bits = ilog2(wx);
+  for (int y0 = wid * lpw; y0 < wy; y0 += (POC_T / 32) * lpw) {
+    int y = y0 + (lpw == 2 ? (l >> 4) : 0);
+    double2 v0 = make_double2(0, 0), v1 = make_double2(0, 0);
+    if (y < wy) {
+      int x = pos_of(0, wx);
+      v0 = make_double2((get(y, x) - mean) * (pc.hy[y * (64 / wy)] * pc.hx[x * (64 / wx)]), 0);
+      if (wx == 64) v1 = make_double2((get(y, x + 32) - mean) * (pc.hy[y * (64 / wy)] * pc.hx[x + 32]), 0);
     }
-    Z[i] = c;
+    warp_dif(v0, v1, wx, false, pc.tw64);
+    if (y < wy) {
+      Z[y * wx + brev(pos_of(0, wx), bits)] = v0;
+      if (wx == 64) Z[y * wx + brev(pos_of(1, wx), bits)] = v1;
+    }
+  }
+}
+
+// poc_shift (poc.py:39-54) of window B = b[y0 : y0 + wy, x0 : x0 + wx] against A's spectrum on the low-pass
+// support (alp, natural order); res = (dx, dy, peak)
+__device__ void poc_shift_dev(const double* __restrict__ b, int W, int x0, int y0, int wy, int wx, const PocConst& pc,
+                              const double2* alp, int nlx, double lpm, double2* Z, double* red, double* res) {
+  const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int n = wy * wx;
+  const int qy = wy / 4, qx = wx / 4;
+  double s = 0;
+  for (int i = threadIdx.x; i < n; i += POC_T) s += b[(size_t)(y0 + i / wx) * W + x0 + (i % wx)];
+  const double mean = block_sum_d(s, red) / n;
+  rows_forward([&](int y, int x) { return b[(size_t)(y0 + y) * W + x0 + x]; }, mean, wy, wx, pc, Z);
+  __syncthreads();
+  // columns on the low-pass support: forward (dif) -> C = B conj(A) / (|.| + 1e-12) on the support, 0 off it ->
+  // inverse (dit); the result goes back to the column of Z in natural order
+  {
+    const int lpw = lines_per_warp(wy), bits = ilog2(wy);
+    const int nlx2 = 2 * qx + 1;
+    for (int c0 = wid * lpw; c0 < nlx2; c0 += (POC_T / 32) * lpw) {
+      int ci = c0 + (lpw == 2 ? (l >> 4) : 0);
+      bool live = ci < nlx2;
+      int kx = ci <= qx ? ci : ci + (wx - 2 * qx - 1);
+      double2 v0 = make_double2(0, 0), v1 = make_double2(0, 0);
+      if (live) {
+        v0 = Z[pos_of(0, wy) * wx + kx];
+        if (wy == 64) v1 = Z[pos_of(1, wy) * wx + kx];
+      }
+      warp_dif(v0, v1, wy, false, pc.tw64);
+      for (int r = 0; r < (wy == 64 ? 2 : 1); r++) {
+        double2& v = r == 0 ? v0 : v1;
+        int ky = brev(pos_of(r, wy), bits);
+        int iy = ky <= qy ? ky : (ky >= wy - qy ? ky - (wy - 2 * qy - 1) : -1);
+        double2 cc = make_double2(0, 0);
+        if (live && iy >= 0) {
+          double2 A = alp[iy * nlx + ci];
+          cc = make_double2(v.x * A.x + v.y * A.y, v.y * A.x - v.x * A.y);
+          double mag = hypot(cc.x, cc.y) + 1e-12;
+          cc.x /= mag;
+          cc.y /= mag;
+        }
+        v = cc;
+      }
+      warp_dit(v0, v1, wy, true, pc.tw64);
+      if (live) {
+        Z[pos_of(0, wy) * wx + kx] = v0;
+        if (wy == 64) Z[pos_of(1, wy) * wx + kx] = v1;
+      }
+    }
   }
   __syncthreads();
-  fft2d_d(Z, wy, wx, pc.tw64, true);
-  // r = fftshift(real(ifft2)) / lpm; first maximum in row-major order, a NaN wins
+  // inverse rows (only the low-pass columns are non-zero); r = fftshift(real) / lpm; the surface is kept in
+  // natural order in the first half of each row of Z (each warp overwrites only rows it has read)
   const double sc = 1.0 / ((double)n) / lpm;
+  double* surf = (double*)Z;
   double best = -DBL_MAX;
   int bi = 0x7fffffff;
   bool bnan = false;
-  for (int i = threadIdx.x; i < n; i += POC_T) {
-    int y = i / wx, x = i - y * wx;
-    int sy = (y - wy / 2 + wy) % wy, sx = (x - wx / 2 + wx) % wx;
-    double v = Z[sy * wx + sx].x * sc;
-    bool vn = v != v;
-    bool take = bnan ? (vn && i < bi) : (vn || v > best || (v == best && i < bi));
-    if (take) { best = v; bi = i; bnan = vn; }
+  {
+    const int lpw = lines_per_warp(wx), bits = ilog2(wx);
+    for (int y0r = wid * lpw; y0r < wy; y0r += (POC_T / 32) * lpw) {
+      int y = y0r + (lpw == 2 ? (l >> 4) : 0);
+      bool live = y < wy;
+      double2 v0 = make_double2(0, 0), v1 = make_double2(0, 0);
+      int x0i = pos_of(0, wx), x1i = x0i + 32;
+      auto lp = [&](int x) { return x <= qx || x >= wx - qx; };
+      if (live && lp(x0i)) v0 = Z[y * wx + x0i];
+      if (live && wx == 64 && lp(x1i)) v1 = Z[y * wx + x1i];
+      __syncwarp();
+      warp_dif(v0, v1, wx, true, pc.tw64);
+      for (int r = 0; r < (wx == 64 ? 2 : 1); r++) {
+        double v = (r == 0 ? v0.x : v1.x) * sc;
+        int x = brev(pos_of(r, wx), bits);
+        if (live) {
+          surf[y * 2 * wx + x] = v;
+          int sy = (y + wy / 2) % wy, sxx = (x + wx / 2) % wx;
+          int idx = sy * wx + sxx;
+          bool vn = v != v;
+          bool take = bnan ? (vn && idx < bi) : (vn || v > best || (v == best && idx < bi));
+          if (take) { best = v; bi = idx; bnan = vn; }
+        }
+      }
+    }
   }
   for (int o = 16; o; o >>= 1) {
     double ov = __shfl_xor_sync(0xffffffff, best, o);
@@ -158,8 +234,7 @@ __device__ void poc_shift_dev(const double* __restrict__ b, int W, int x0, int y
   __shared__ double sv[POC_T / 32];
   __shared__ int si[POC_T / 32];
   __shared__ int sn[POC_T / 32];
-  int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) { sv[wid] = best; si[wid] = bi; sn[wid] = bnan; }
+  if (l == 0) { sv[wid] = best; si[wid] = bi; sn[wid] = bnan; }
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int k = 1; k < POC_T / 32; k++) {
@@ -170,9 +245,9 @@ __device__ void poc_shift_dev(const double* __restrict__ b, int W, int x0, int y
     int iy = bi / wx, ix = bi - iy * wx;
     iy = min(max(iy, 1), wy - 2);
     ix = min(max(ix, 1), wx - 2);
-    auto R = [&](int y, int x) {
-      int sy = (y - wy / 2 + wy) % wy, sx = (x - wx / 2 + wx) % wx;
-      return Z[sy * wx + sx].x * sc;
+    auto R = [&](int ys, int xs) {  // the shifted surface at (ys, xs)
+      int y = (ys - wy / 2 + wy) % wy, x = (xs - wx / 2 + wx) % wx;
+      return surf[y * 2 * wx + x];
     };
     auto parabola = [](double m, double c, double p) {  // poc.py:34-36
       double den = m - 2.0 * c + p;
@@ -188,17 +263,18 @@ __device__ void poc_shift_dev(const double* __restrict__ b, int W, int x0, int y
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(POC_T) k_poc_grid(const double* __restrict__ a, const double* __restrict__ b, int W,
-                                                     int H, int wy, int wx, const int* __restrict__ xs,
-                                                     const int* __restrict__ ys, int nx, const double* iux,
-                                                     const double* iuy, const PocConst* __restrict__ pcg, double lpm,
-                                                     double* oux, double* ouy, double* opeak) {
+__global__ void __launch_bounds__(POC_T, 2) k_poc_grid(const double* __restrict__ a, const double* __restrict__ b,
+                                                        int W, int H, int wy, int wx, const int* __restrict__ xs,
+                                                        const int* __restrict__ ys, int nx, const double* iux,
+                                                        const double* iuy, const PocConst* __restrict__ pcg,
+                                                        double lpm, double* oux, double* ouy, double* opeak) {
   extern __shared__ double2 dsm[];
   double2* Z = dsm;
-  const int nly = 2 * (wy / 4) + 1, nlx = 2 * (wx / 4) + 1;
+  const int qy = wy / 4, qx = wx / 4;
+  const int nlx = 2 * qx + 1;
   double2* alp = Z + wy * wx;
   __shared__ PocConst pc;
-  __shared__ double red[POC_T / 32 + 1];
+  __shared__ double red[POC_T / 32];
   __shared__ double res[3];
   for (int i = threadIdx.x; i < (int)(sizeof(PocConst) / sizeof(double)); i += POC_T)
     ((double*)&pc)[i] = ((const double*)pcg)[i];
@@ -207,28 +283,33 @@ __global__ void __launch_bounds__(POC_T) k_poc_grid(const double* __restrict__ a
   const int x = xs[j], y = ys[i];
   const int hy = wy / 2, hx = wx / 2;
   const int n = wy * wx;
+  const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
   __syncthreads();
-  // spectrum of A (poc.py:44), kept on the low-pass support
+  // spectrum of A (poc.py:44) on the low-pass support, natural order: alp[iy * nlx + ix]
+  const double* aw = a + (size_t)(y - hy) * W + (x - hx);
   double s = 0;
-  for (int t = threadIdx.x; t < n; t += POC_T) {
-    int r = t / wx, q = t - r * wx;
-    double v = a[(size_t)(y - hy + r) * W + (x - hx + q)];
-    Z[t] = make_double2(v, 0);
-    s += v;
-  }
-  double mean = block_sum_d(s, red) / n;
-  for (int t = threadIdx.x; t < n; t += POC_T) {
-    int r = t / wx, q = t - r * wx;
-    Z[t] = make_double2((Z[t].x - mean) * (pc.hy[r * (64 / wy)] * pc.hx[q * (64 / wx)]), 0);
-  }
+  for (int t = threadIdx.x; t < n; t += POC_T) s += aw[(size_t)(t / wx) * W + (t % wx)];
+  const double mean = block_sum_d(s, red) / n;
+  rows_forward([&](int yy, int xx) { return aw[(size_t)yy * W + xx]; }, mean, wy, wx, pc, Z);
   __syncthreads();
-  fft2d_d(Z, wy, wx, pc.tw64, false);
-  const int qy = wy / 4, qx = wx / 4;
-  for (int t = threadIdx.x; t < nly * nlx; t += POC_T) {
-    int iy = t / nlx, ix = t - iy * nlx;
-    int ky = iy <= qy ? iy : iy + (wy - 2 * qy - 1);
-    int kx = ix <= qx ? ix : ix + (wx - 2 * qx - 1);
-    alp[t] = Z[ky * wx + kx];
+  {
+    const int lpw = lines_per_warp(wy), bits = ilog2(wy);
+    for (int c0 = wid * lpw; c0 < nlx; c0 += (POC_T / 32) * lpw) {
+      int ci = c0 + (lpw == 2 ? (l >> 4) : 0);
+      bool live = ci < nlx;
+      int kx = ci <= qx ? ci : ci + (wx - 2 * qx - 1);
+      double2 v0 = make_double2(0, 0), v1 = make_double2(0, 0);
+      if (live) {
+        v0 = Z[pos_of(0, wy) * wx + kx];
+        if (wy == 64) v1 = Z[pos_of(1, wy) * wx + kx];
+      }
+      warp_dif(v0, v1, wy, false, pc.tw64);
+      for (int r = 0; r < (wy == 64 ? 2 : 1); r++) {
+        int ky = brev(pos_of(r, wy), bits);
+        int iy = ky <= qy ? ky : (ky >= wy - qy ? ky - (wy - 2 * qy - 1) : -1);
+        if (live && iy >= 0) alp[iy * nlx + ci] = r == 0 ? v0 : v1;
+      }
+    }
   }
   __syncthreads();
   double dx = iux ? iux[gi] : 0.0, dy = iuy ? iuy[gi] : 0.0;
@@ -237,7 +318,7 @@ __global__ void __launch_bounds__(POC_T) k_poc_grid(const double* __restrict__ a
     double ox = rint(dx), oy = rint(dy);  // Python round(): half to even
     long y0 = y - hy + (long)oy, x0 = x - hx + (long)ox;
     if (y0 < 0 || x0 < 0 || y0 + wy > H || x0 + wx > W) { pk = 0.0; break; }
-    poc_shift_dev(b, W, (int)x0, (int)y0, wy, wx, pc, alp, nly, nlx, lpm, Z, red, res);
+    poc_shift_dev(b, W, (int)x0, (int)y0, wy, wx, pc, alp, nlx, lpm, Z, red, res);
     double sx = res[0], sy = res[1];
     pk = res[2];
     dx = ox + sx;
@@ -253,15 +334,14 @@ __global__ void __launch_bounds__(POC_T) k_poc_grid(const double* __restrict__ a
 
 void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const int* xs, const int* ys,
                      const double* iux, const double* iuy, double* ux, double* uy, double* peak, cudaStream_t st) {
-  if (lv.wy * lv.wx > POC_MAXN || lv.wy > 64 || lv.wx > 64)
-    throw Error(OFC_ERR_ARG, "the CUDA engine's POC windows are at most 64 x 64 (poc_win <= 64)");
+  auto ok_len = [](int n) { return n == 16 || n == 32 || n == 64; };
+  if (!ok_len(lv.wy) || !ok_len(lv.wx))
+    throw Error(OFC_ERR_ARG, "the CUDA engine's POC windows are 16, 32 or 64 px a side (poc_win <= 64)");
   // constants: twiddles of length 64, Hann windows of the level's window, rounded from float64
   PocConst hc;
   for (int t = 0; t < 64; t++) {
     double ang = -2.0 * PI * t / 64.0;
     hc.tw64[t] = make_double2(std::cos(ang), std::sin(ang));
-  }
-  for (int t = 0; t < 64; t++) {
     hc.hy[t] = 0.0;
     hc.hx[t] = 0.0;
   }
