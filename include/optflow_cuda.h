@@ -197,6 +197,23 @@ OFC_API int ofc_track_pair_device(ofc_engine* eng, const float* d_i1, const floa
                           const ofc_config* cfg, ofc_pair_out* d_out, void* stream,
                           char* err, size_t errlen);
 
+/*
+ * The large-component mask of the guard (track._large_components, python/optflow_ref/track.py:45-53) for callers
+ * that cannot allocate device memory (no counterpart in the reference: it exists for hosts whose device memory
+ * is owned by someone else, such as a runtime whose pool allocator owns every device allocation, or an embedded
+ * host that may not grow device memory after start-up). No engine: d_mask (w*h bytes, nonzero = set) and d_out (w*h bytes) are the caller's
+ * device buffers on the current device, and the work is queued on `stream` (a cudaStream_t, NULL = the legacy
+ * default stream); the result is valid once the stream has reached the end of it. The call allocates nothing:
+ * its union-find scratch is a fixed device array of 2 * OFC_NOALLOC_MAX_PIXELS ints (8 MiB) that every device
+ * loading this library holds until exit, so w * h must not exceed OFC_NOALLOC_MAX_PIXELS (error OFC_ERR_WINDOW).
+ * The first call on a device looks the array's device address up and should come before any stream capture.
+ * Every call shares the one array: calls whose work overlaps on the GPU (two streams, or two host threads) race
+ * and give wrong masks; keep them ordered on one stream.
+ */
+#define OFC_NOALLOC_MAX_PIXELS (1u << 20)
+OFC_API int ofc_large_components_noalloc(const uint8_t* d_mask, size_t w, size_t h, double min_area, uint8_t* d_out,
+                                         void* stream, char* err, size_t errlen);
+
 /* Number of this library's kernels launched by this engine since it was created (the kernels
  * are all hand-written; no library kernel runs on the path). */
 OFC_API uint64_t ofc_kernel_launches(const ofc_engine* eng);

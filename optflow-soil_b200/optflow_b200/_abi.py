@@ -101,6 +101,7 @@ SIGNATURES = {
     "ofc_track_pair_device": (ctypes.c_int, [_P, _P, _P, _S, _S, _P, _P, _P, ctypes.POINTER(OfcConfig),
                                              ctypes.POINTER(OfcPairOut), _P, _E, _S]),
     "ofc_kernel_launches": (ctypes.c_uint64, [_P]),
+    "ofc_large_components_noalloc": (ctypes.c_int, [_P, _S, _S, ctypes.c_double, _P, _P, _E, _S]),
 }
 
 
