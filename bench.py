@@ -210,11 +210,12 @@ def main():
             raise RuntimeError(err.value.decode())
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
+    # the profile filter is part of the captured pair graphs' key: set it before the warm-up, which then
+    # captures the graphs the timed steps replay
+    lib.ofc_set_profile(eng.handle, b"" if args.profile_all else b"k_accumulate")
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
-
-    lib.ofc_set_profile(eng.handle, b"" if args.profile_all else b"k_accumulate")
     lib.ofc_profile_read(eng.handle, None, 0, None, None, 0)  # clear
     clocks = ClockSampler(local)
     clocks.start()

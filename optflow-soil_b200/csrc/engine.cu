@@ -28,6 +28,8 @@ thread_local Profiler* g_profiler = nullptr;
 // when read (ofc_profile_read) or when the pool runs low.
 struct Profiler {
   std::string filter;
+  // while a pair is captured as a graph, the event pairs go to the graph's list (recorded at every replay)
+  std::vector<std::tuple<std::string, cudaEvent_t, cudaEvent_t>>* capture = nullptr;
   struct Pending {
     std::string name;
     cudaEvent_t a, b;
@@ -71,6 +73,16 @@ void prof_before(const char* name, cudaStream_t st, void** token) {
   if (!n.empty() && n.front() == '(') n = n.substr(1, n.size() - 2);
   if (!p->filter.empty() && n.find(p->filter) == std::string::npos) return;
   std::lock_guard<std::mutex> lk(p->mu);
+  if (p->capture) {
+    cudaEvent_t a, b;
+    OFC_CUDA(cudaEventCreate(&a));
+    OFC_CUDA(cudaEventCreate(&b));
+    // External: a record node in the graph (a plain record inside a capture only orders streams)
+    OFC_CUDA(cudaEventRecordWithFlags(a, st, cudaEventRecordExternal));
+    p->capture->emplace_back(n, a, b);
+    *token = (void*)(uintptr_t)(1 + 2 * (p->capture->size() - 1));  // odd: an index into the capture list
+    return;
+  }
   if (p->pending.size() > 4096) p->resolve();
   Profiler::Pending q{n, p->take(), p->take()};
   OFC_CUDA(cudaEventRecord(q.a, st));
@@ -79,6 +91,11 @@ void prof_before(const char* name, cudaStream_t st, void** token) {
 }
 
 void prof_after(void* token, cudaStream_t st) {
+  uintptr_t t = (uintptr_t)token;
+  if (t & 1) {
+    OFC_CUDA(cudaEventRecordWithFlags(std::get<2>((*g_profiler->capture)[(t - 1) / 2]), st, cudaEventRecordExternal));
+    return;
+  }
   OFC_CUDA(cudaEventRecord(((Profiler::Pending*)token)->b, st));
 }
 }
@@ -200,7 +217,12 @@ struct Lane {
     auto& b = pool[name];
     if (!b) b.reset(new DevBuf());
     if (b->bytes < bytes) {
-      if (b->p) OFC_CUDA(cudaFree(b->p));
+      if (b->p) {
+        // captured graphs hold the old address: drop them (after the work in flight) before the buffer goes
+        OFC_CUDA(cudaStreamSynchronize(stream));
+        graphs.clear();
+        OFC_CUDA(cudaFree(b->p));
+      }
       b->p = nullptr;
       b->bytes = 0;
       OFC_CUDA(cudaMalloc(&b->p, bytes));
@@ -214,6 +236,40 @@ struct Lane {
     OFC_CUDA(cudaMemcpyAsync(d, host, count * sizeof(T), cudaMemcpyHostToDevice, stream));
     return d;
   }
+  // constant tables uploaded once per key (sizes and configuration in the key): the per-pair sequence then
+  // issues no host-to-device copy, so it can be captured as a CUDA graph
+  std::unordered_map<std::string, std::unique_ptr<DevBuf>> consts;
+  template <class T>
+  const T* cached(const std::string& key, const T* host, size_t count) {
+    auto& b = consts[key];
+    if (!b) {
+      b.reset(new DevBuf());
+      OFC_CUDA(cudaMalloc(&b->p, std::max<size_t>(count * sizeof(T), 256)));
+      b->bytes = count * sizeof(T);
+      OFC_CUDA(cudaMemcpy(b->p, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    return (const T*)b->p;
+  }
+  bool has_const(const std::string& key) const { return consts.count(key) != 0; }
+
+  // captured pair sequences, per (size, configuration, inputs present); events: the profile-mode event pairs
+  // recorded inside the graph (kernel name, start, end)
+  struct Graph {
+    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+    uint64_t launches[3] = {0, 0, 0};  // kernels per stage graph (the launch counter's share of a replay)
+    bool eager = false;                // the capture failed: this key runs eagerly
+    std::vector<std::tuple<std::string, cudaEvent_t, cudaEvent_t>> events;
+    ~Graph() {
+      for (auto g : exec)
+        if (g) cudaGraphExecDestroy(g);
+      for (auto& e : events) {
+        cudaEventDestroy(std::get<1>(e));
+        cudaEventDestroy(std::get<2>(e));
+      }
+    }
+  };
+  std::unordered_map<std::string, std::unique_ptr<Graph>> graphs;
+
   const FftPlan& plan(int L) {
     auto it = plans.find(L);
     if (it != plans.end()) return it->second.first;
@@ -234,10 +290,28 @@ struct Lane {
     return slot.first;
   }
   void release() {
+    graphs.clear();
+    consts.clear();
     pool.clear();
     plans.clear();
   }
 };
+
+// a key of the configuration fields the pair path reads
+std::string cfg_key(const ofc_config& c) {
+  char buf[512];
+  int n = std::snprintf(buf, sizeof buf, "%d,%d,%.17g,%.17g,%.17g,%.17g,%d,%d,%.17g,%.17g,%.17g,%d,%.17g,%d,%d,%.17g,%.17g,%.17g,%.17g,%d,%d",
+                        c.grid_step, c.poc_win, c.max_disp, c.poc_peak_min, c.median_thresh, c.lam, c.n_scales,
+                        c.n_orient, c.bandwidth, c.dc_cut, c.sigma_w, c.shape_order, c.sigma_s, c.outer_iters,
+                        c.inner_iters, c.conf_min, c.edge_guard, c.edge_guard_min_area, c.phase_tol, c.strain_win,
+                        c.prewarp_freeze_at);
+  std::string k(buf, n > 0 ? (size_t)n : 0);
+  for (int i = 0; i < c.n_scales; i++) {
+    std::snprintf(buf, sizeof buf, ",%.17g", c.scales[i]);
+    k += buf;
+  }
+  return k;
+}
 
 }  // namespace
 
@@ -305,13 +379,41 @@ struct FineOut {
 
 // the Gabor tables of a padded size on the device (float64 and float32 copies)
 GaborTables upload_gabor(Lane& L, int ph, int pw, const ofc_config& c) {
-  std::vector<double> gt = gabor_tables_host(ph, pw, c);
-  std::vector<float> g32(gt.begin(), gt.end());
-  double* d64 = L.upload("gabor", gt.data(), gt.size());
-  float* d32 = L.upload("gabor32", g32.data(), g32.size());
+  const std::string key = "gabor:" + std::to_string(ph) + "x" + std::to_string(pw) + ":" + cfg_key(c);
+  const double* d64;
+  const float* d32;
+  if (L.has_const(key)) {
+    d64 = L.cached<double>(key, nullptr, 0);
+    d32 = L.cached<float>(key + ":f32", nullptr, 0);
+  } else {
+    std::vector<double> gt = gabor_tables_host(ph, pw, c);
+    std::vector<float> g32(gt.begin(), gt.end());
+    d64 = L.cached(key, gt.data(), gt.size());
+    d32 = L.cached(key + ":f32", g32.data(), g32.size());
+  }
   GaborTables g;
   gabor_bind(g, d64, d32, ph, pw, c.n_scales * c.n_orient);
   return g;
+}
+
+// window taps: Gaussian (sigma) and, for the moments, k(t) t^p for p = 0..4
+const double* gauss_taps(Lane& L, double sigma, int& r) {
+  std::vector<double> k = gauss_kernel(sigma);
+  r = (int)k.size() / 2;
+  char key[64];
+  std::snprintf(key, sizeof key, "gauss:%.17g", sigma);
+  return L.cached(key, k.data(), k.size());
+}
+const double* moment_taps(Lane& L, double sigma, int& r) {
+  std::vector<double> kw = gauss_kernel(sigma);
+  r = (int)kw.size() / 2;
+  const int K = 2 * r + 1;
+  std::vector<double> mt((size_t)5 * K);
+  for (int p = 0; p < 5; p++)
+    for (int t = -r; t <= r; t++) mt[(size_t)p * K + t + r] = kw[t + r] * std::pow((double)t, p);
+  char key[64];
+  std::snprintf(key, sizeof key, "moments:%.17g", sigma);
+  return L.cached(key, mt.data(), mt.size());
 }
 
 // reference_phase (phaseflow.py:100-111) of i1 in float64 transforms, stored as float32 (r.re, r.im, gx, gy)
@@ -349,16 +451,9 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
   const FftPlan& plh = L.plan(ph);
   GaborTables g = upload_gabor(L, ph, pw, c);
   // taps: smoothing Gaussian (sigma_s) and window moments k(t) t^p, p = 0..4 (sigma_w)
-  std::vector<double> ks = gauss_kernel(c.sigma_s);
-  int rs = (int)ks.size() / 2;
-  std::vector<double> kw = gauss_kernel(c.sigma_w);
-  int rw = (int)kw.size() / 2;
-  int K = 2 * rw + 1;
-  std::vector<double> mt((size_t)5 * K);
-  for (int p = 0; p < 5; p++)
-    for (int t = -rw; t <= rw; t++) mt[(size_t)p * K + t + rw] = kw[t + rw] * std::pow((double)t, p);
-  double* d_ks = L.upload("taps_s", ks.data(), ks.size());
-  double* d_mt = L.upload("taps_w", mt.data(), mt.size());
+  int rs = 0, rw = 0;
+  const double* d_ks = gauss_taps(L, c.sigma_s, rs);
+  const double* d_mt = moment_taps(L, c.sigma_w, rw);
 
   // reference pack (phaseflow.py:431, reference_phase)
   float2* T = L.get<float2>("fft_T", Np);
@@ -446,8 +541,8 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
 // ---------------------------------------------------------------- the coarse stage
 struct CoarseOut {
   int nx, ny;
-  int* xs;  // device
-  int* ys;
+  const int* xs;  // device
+  const int* ys;
   double* ux;
   double* uy;
   double* peak;
@@ -460,9 +555,8 @@ CoarseOut coarse_dev(Lane& L, const float* a, const float* b, int W, int H, cons
   if (c.poc_win > 64) throw Error(OFC_ERR_ARG, "the CUDA engine's POC windows are at most 64 x 64 (poc_win <= 64)");
   const size_t N = (size_t)W * H;
   int Lv = n_levels(c.max_disp, c.poc_win, H, W);
-  std::vector<double> k1 = gauss_kernel(1.0);
-  double* d_k1 = L.upload("taps_1", k1.data(), k1.size());
-  int r1 = (int)k1.size() / 2;
+  int r1 = 0;
+  const double* d_k1 = gauss_taps(L, 1.0, r1);
   // pyramid (float64): level 0 is the input itself
   std::vector<double*> pa(Lv + 1), pb(Lv + 1);
   std::vector<int> pws(Lv + 1), phs(Lv + 1);
@@ -498,8 +592,13 @@ CoarseOut coarse_dev(Lane& L, const float* a, const float* b, int W, int H, cons
     if (gx.empty() || gy.empty()) throw Error(OFC_ERR_ARG, "image too small for the POC grid");
     int nx = (int)gx.size(), ny = (int)gy.size();
     std::string sfx = std::to_string(lev);
-    int* dxs = L.upload("poc_xs" + sfx, gx.data(), gx.size());
-    int* dys = L.upload("poc_ys" + sfx, gy.data(), gy.size());
+    const std::string gk = "pocgrid:" + std::to_string(W) + "x" + std::to_string(H) + ":" + sfx + ":" +
+                           std::to_string(c.poc_win) + ":" + std::to_string(c.grid_step);
+    const int* dxs = L.cached(gk + ":x", gx.data(), gx.size());
+    const int* dys = L.cached(gk + ":y", gy.data(), gy.size());
+    std::vector<unsigned char> pc(poc_const_bytes());
+    poc_const_host(wy, wx, pc.data());
+    const void* dconst = L.cached("pocconst:" + std::to_string(wy) + "x" + std::to_string(wx), pc.data(), pc.size());
     double* iu = nullptr;
     double* iv = nullptr;
     if (have) {
@@ -515,7 +614,7 @@ CoarseOut coarse_dev(Lane& L, const float* a, const float* b, int W, int H, cons
     double* gv = L.get<double>("poc_v" + sfx, (size_t)nx * ny);
     double* gp = L.get<double>("poc_p" + sfx, (size_t)nx * ny);
     PocLevel lv{w, h, nx, ny, wy, wx};
-    launch_poc_grid(pa[lev], pb[lev], lv, dxs, dys, iu, iv, gu, gv, gp, st);
+    launch_poc_grid(pa[lev], pb[lev], lv, dxs, dys, iu, iv, dconst, gu, gv, gp, st);
     uint8_t* scr = L.get<uint8_t>("poc_flags", (size_t)3 * nx * ny);
     launch_poc_clean(gu, gv, gp, nx, ny, c.poc_peak_min, c.median_thresh, iu, iv, scr, st);
     prev = CoarseOut{nx, ny, dxs, dys, gu, gv, gp, gx, gy};
@@ -562,31 +661,115 @@ void finish_dev(Lane& L, const uint8_t* low, const uint8_t* roi, const double* u
 }
 
 // the whole pair on device buffers; d_out fields are device pointers
-void track_pair_dev(Lane& L, const float* i1, const float* i2, int W, int H, const uint8_t* roi, const float* iux,
-                    const float* iuy, const ofc_config& c, const ofc_pair_out& o, bool timed, double* timing) {
+// One pair on the lane's own buffers, in three stages: 0 = coarse POC + dense start, 1 = fine stage + confidence,
+// 2 = guard + strain + outputs. Inputs: in_i1, in_i2 (float W*H), in_roi (bytes, when has_roi), in_u, in_v (float,
+// when has_init); outputs: out_pair (10 planes) and out_valid.
+void pair_stage(Lane& L, int stage, int W, int H, bool has_roi, bool has_init, const ofc_config& c) {
   cudaStream_t st = L.stream;
   const size_t N = (size_t)W * H;
-  if (timed) OFC_CUDA(cudaEventRecord(L.ev[0], st));
-  double* init = nullptr;
-  if (iux) {
-    init = L.get<double>("init2", 2 * N);
-    launch_f32_to_f64(iux, init, N, st);
-    launch_f32_to_f64(iuy, init + N, N, st);
-  }
-  CoarseOut g = coarse_dev(L, i1, i2, W, H, init, c);
+  const float* i1 = L.get<float>("in_i1", N);
+  const float* i2 = L.get<float>("in_i2", N);
   double* u2 = L.get<double>("u2", 2 * N);
-  dense_start(L, g, W, H, init, u2);
-  if (timed) OFC_CUDA(cudaEventRecord(L.ev[1], st));
-  FineOut f = refine_dev(L, i1, W, H, i2, W, H, 0, 0, u2, c);
   double* conf64 = L.get<double>("conf64", N);
   uint8_t* low = L.get<uint8_t>("low_final", N);
-  double B = guard_px(c) > 0 ? 4.0 * c.sigma_w : 0.0;
-  launch_confidence(f.energy, f.resid, f.ux, f.uy, W, H, f.stats, c.phase_tol, c.conf_min, true, B, nullptr, conf64,
-                    low, nullptr, st);
-  if (timed) OFC_CUDA(cudaEventRecord(L.ev[2], st));
-  finish_dev(L, low, roi, f.ux, f.uy, conf64, W, H, c, o);
-  if (timed) {
-    OFC_CUDA(cudaEventRecord(L.ev[3], st));
+  if (stage == 0) {
+    double* init = nullptr;
+    if (has_init) {
+      init = L.get<double>("init2", 2 * N);
+      launch_f32_to_f64(L.get<float>("in_u", N), init, N, st);
+      launch_f32_to_f64(L.get<float>("in_v", N), init + N, N, st);
+    }
+    CoarseOut g = coarse_dev(L, i1, i2, W, H, init, c);
+    dense_start(L, g, W, H, init, u2);
+  } else if (stage == 1) {
+    FineOut f = refine_dev(L, i1, W, H, i2, W, H, 0, 0, u2, c);
+    double B = guard_px(c) > 0 ? 4.0 * c.sigma_w : 0.0;
+    launch_confidence(f.energy, f.resid, f.ux, f.uy, W, H, f.stats, c.phase_tol, c.conf_min, true, B, nullptr,
+                      conf64, low, nullptr, st);
+  } else {
+    ofc_pair_out o{};
+    float* p = L.get<float>("out_pair", 10 * N);
+    float** f[10] = {&o.ux, &o.uy, &o.conf, &o.exx, &o.eyy, &o.exy, &o.gmax, &o.vol, &o.raw_ux, &o.raw_uy};
+    for (int i = 0; i < 10; i++) *f[i] = p + i * N;
+    o.valid = L.get<uint8_t>("out_valid", N);
+    const uint8_t* roi = has_roi ? L.get<uint8_t>("in_roi", N) : nullptr;
+    finish_dev(L, low, roi, u2, u2 + N, conf64, W, H, c, o);
+  }
+}
+
+// Runs the three stages on L.stream. The first call for a (size, configuration, inputs present, profile filter)
+// runs them eagerly, which allocates every buffer and uploads every constant, and then captures each stage as a
+// CUDA graph; later calls replay the graphs. timing (nullable): seconds per stage from events between the stages.
+void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_config& c, double* timing) {
+  cudaStream_t st = L.stream;
+  Profiler* prof = g_profiler;
+  const std::string key = std::to_string(W) + "x" + std::to_string(H) + ":" + cfg_key(c) + ":" +
+                          (has_roi ? "r" : "-") + (has_init ? "i" : "-") + ":" + (prof ? "P" + prof->filter : "");
+  auto it = L.graphs.find(key);
+  if (it == L.graphs.end() || it->second->eager) {
+    for (int sgi = 0; sgi < 3; sgi++) {
+      if (timing) OFC_CUDA(cudaEventRecord(L.ev[sgi], st));
+      pair_stage(L, sgi, W, H, has_roi, has_init, c);
+    }
+    if (timing) OFC_CUDA(cudaEventRecord(L.ev[3], st));
+  }
+  if (it == L.graphs.end()) {
+    std::unique_ptr<Lane::Graph> g(new Lane::Graph());
+    bool ok = true;
+    for (int sgi = 0; sgi < 3 && ok; sgi++) {
+      cudaGraph_t graph = nullptr;
+      const uint64_t before = g_launch_counter ? *g_launch_counter : 0;
+      OFC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+      if (prof) prof->capture = &g->events;
+      try {
+        pair_stage(L, sgi, W, H, has_roi, has_init, c);
+      } catch (...) {
+        if (prof) prof->capture = nullptr;
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+      }
+      if (prof) prof->capture = nullptr;
+      if (g_launch_counter) {
+        g->launches[sgi] = *g_launch_counter - before;  // captured, not launched
+        *g_launch_counter = before;
+      }
+      OFC_CUDA(cudaStreamEndCapture(st, &graph));
+      cudaError_t e = cudaGraphInstantiate(&g->exec[sgi], graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        ok = false;
+        (void)cudaGetLastError();
+      }
+    }
+    if (!ok) {
+      std::unique_ptr<Lane::Graph> bad(new Lane::Graph());
+      bad->eager = true;
+      g = std::move(bad);
+    }
+    L.graphs[key] = std::move(g);
+  } else if (!it->second->eager) {
+    Lane::Graph& g = *it->second;
+    for (int sgi = 0; sgi < 3; sgi++) {
+      if (timing) OFC_CUDA(cudaEventRecord(L.ev[sgi], st));
+      OFC_CUDA(cudaGraphLaunch(g.exec[sgi], st));
+      if (g_launch_counter) *g_launch_counter += g.launches[sgi];
+    }
+    if (timing) OFC_CUDA(cudaEventRecord(L.ev[3], st));
+    if (prof && !g.events.empty()) {
+      // the replay's kernel times: the graph records its event pairs anew at every launch
+      OFC_CUDA(cudaStreamSynchronize(st));
+      std::lock_guard<std::mutex> lk(prof->mu);
+      for (auto& ev : g.events) {
+        float ms = 0;
+        OFC_CUDA(cudaEventElapsedTime(&ms, std::get<1>(ev), std::get<2>(ev)));
+        auto& t = prof->totals[std::get<0>(ev)];
+        t.first += 1;
+        t.second += ms;
+      }
+    }
+  }
+  if (timing) {
     OFC_CUDA(cudaEventSynchronize(L.ev[3]));
     float ms[3];
     for (int i = 0; i < 3; i++) OFC_CUDA(cudaEventElapsedTime(&ms[i], L.ev[i], L.ev[i + 1]));
@@ -977,15 +1160,16 @@ int ofc_track_pair(ofc_engine* e, const float* i1, const float* i2, size_t w, si
     if ((int)std::min(w, h) < c->poc_win)
       throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
     const size_t N = w * h;
-    float* d1 = L.upload("in_i1", i1, N);
-    float* d2 = L.upload("in_i2", i2, N);
-    const uint8_t* droi = roi ? L.upload("in_roi", roi, N) : nullptr;
-    const float* du = init_ux ? L.upload("in_u", init_ux, N) : nullptr;
-    const float* dv = init_uy ? L.upload("in_v", init_uy, N) : nullptr;
-    ofc_pair_out d = device_pair_out(L, N);
+    L.upload("in_i1", i1, N);
+    L.upload("in_i2", i2, N);
+    if (roi) L.upload("in_roi", roi, N);
+    if (init_ux) {
+      L.upload("in_u", init_ux, N);
+      L.upload("in_v", init_uy, N);
+    }
     double timing[3] = {0, 0, 0};
-    track_pair_dev(L, d1, d2, (int)w, (int)h, droi, du, dv, *c, d, true, timing);
-    download_pair(L, d, out, N);
+    run_pair(L, (int)w, (int)h, roi != nullptr, init_ux != nullptr, *c, timing);
+    download_pair(L, device_pair_out(L, N), out, N);
     OFC_CUDA(cudaStreamSynchronize(L.stream));
     for (int i = 0; i < 3; i++) out->timing[i] = timing[i];
   });
@@ -998,12 +1182,31 @@ int ofc_track_pair_device(ofc_engine* e, const float* d_i1, const float* d_i2, s
     cfg_check(c);
     check_fine_window(w, h, *c);
     if (!d_i1 || !d_i2 || !d_out) throw Error(OFC_ERR_ARG, "null argument");
+    if ((d_init_ux == nullptr) != (d_init_uy == nullptr))
+      throw Error(OFC_ERR_ARG, "init_ux and init_uy must both be given");
     if ((int)std::min(w, h) < c->poc_win)
       throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
+    const size_t N = w * h;
     cudaStream_t keep = L.stream;
     if (stream) L.stream = (cudaStream_t)stream;
     try {
-      track_pair_dev(L, d_i1, d_i2, (int)w, (int)h, d_roi, d_init_ux, d_init_uy, *c, *d_out, false, nullptr);
+      // the caller's buffers are copied into the lane's (the captured graphs read and write fixed addresses)
+      cudaStream_t st = L.stream;
+      OFC_CUDA(cudaMemcpyAsync(L.get<float>("in_i1", N), d_i1, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(L.get<float>("in_i2", N), d_i2, N * 4, cudaMemcpyDeviceToDevice, st));
+      if (d_roi) OFC_CUDA(cudaMemcpyAsync(L.get<uint8_t>("in_roi", N), d_roi, N, cudaMemcpyDeviceToDevice, st));
+      if (d_init_ux) {
+        OFC_CUDA(cudaMemcpyAsync(L.get<float>("in_u", N), d_init_ux, N * 4, cudaMemcpyDeviceToDevice, st));
+        OFC_CUDA(cudaMemcpyAsync(L.get<float>("in_v", N), d_init_uy, N * 4, cudaMemcpyDeviceToDevice, st));
+      }
+      run_pair(L, (int)w, (int)h, d_roi != nullptr, d_init_ux != nullptr, *c, nullptr);
+      const ofc_pair_out d = device_pair_out(L, N);
+      float* const* dsrc[10] = {&d.ux, &d.uy, &d.conf, &d.exx, &d.eyy, &d.exy, &d.gmax, &d.vol, &d.raw_ux, &d.raw_uy};
+      float* const* udst[10] = {&d_out->ux,  &d_out->uy,  &d_out->conf, &d_out->exx,    &d_out->eyy,
+                                &d_out->exy, &d_out->gmax, &d_out->vol, &d_out->raw_ux, &d_out->raw_uy};
+      for (int i = 0; i < 10; i++)
+        if (*udst[i]) OFC_CUDA(cudaMemcpyAsync(*udst[i], *dsrc[i], N * 4, cudaMemcpyDeviceToDevice, st));
+      if (d_out->valid) OFC_CUDA(cudaMemcpyAsync(d_out->valid, d.valid, N, cudaMemcpyDeviceToDevice, st));
     } catch (...) {
       L.stream = keep;
       throw;

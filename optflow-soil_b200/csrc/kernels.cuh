@@ -87,9 +87,13 @@ struct PocLevel {
 // downsample (poc.py:164-165) of a float64 (or float32 for level 0) image
 void launch_downsample(const double* in, int W, int H, double* out, double* tmp, const double* taps, int r,
                        cudaStream_t st);
-// poc_grid (poc.py:67-92): one thread block per grid point; init (nullable) ny x nx
+// poc_grid (poc.py:67-92): one thread block per grid point; init (nullable) ny x nx; dconst: the window's
+// constants on the device (poc_const_host, poc_const_bytes() bytes)
+size_t poc_const_bytes();
+void poc_const_host(int wy, int wx, void* out);
 void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const int* xs, const int* ys,
-                     const double* iux, const double* iuy, double* ux, double* uy, double* peak, cudaStream_t st);
+                     const double* iux, const double* iuy, const void* dconst, double* ux, double* uy, double* peak,
+                     cudaStream_t st);
 // clean (poc.py:95-140) in one thread block; fallback = init (nullable)
 void launch_poc_clean(double* ux, double* uy, double* peak, int nx, int ny, double peak_min, double thresh,
                       const double* fbx, const double* fby, uint8_t* scratch, cudaStream_t st);

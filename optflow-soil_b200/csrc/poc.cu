@@ -2,12 +2,12 @@
 // windowed band-limited phase-only correlation on a grid, one thread block per grid point, with the
 // re-centring iterations, the outlier clean-up and the bilinear grid sampling.
 #include <cfloat>
+#include <cstring>
 
 #include "kernels.cuh"
 
 namespace ofc {
 
-constexpr int POC_MAXN = 4096;  // window pixels held in shared memory (64 x 64)
 constexpr int POC_T = 256;
 
 // ---------------------------------------------------------------- downsample (poc.py:164-165)
@@ -332,12 +332,10 @@ __global__ void __launch_bounds__(POC_T, 2) k_poc_grid(const double* __restrict_
   }
 }
 
-void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const int* xs, const int* ys,
-                     const double* iux, const double* iuy, double* ux, double* uy, double* peak, cudaStream_t st) {
-  auto ok_len = [](int n) { return n == 16 || n == 32 || n == 64; };
-  if (!ok_len(lv.wy) || !ok_len(lv.wx))
-    throw Error(OFC_ERR_ARG, "the CUDA engine's POC windows are 16, 32 or 64 px a side (poc_win <= 64)");
-  // constants: twiddles of length 64, Hann windows of the level's window, rounded from float64
+size_t poc_const_bytes() { return sizeof(PocConst); }
+
+// constants of a window: twiddles of length 64 and the Hann windows, rounded from float64 (poc.py:18-31)
+void poc_const_host(int wy, int wx, void* out) {
   PocConst hc;
   for (int t = 0; t < 64; t++) {
     double ang = -2.0 * PI * t / 64.0;
@@ -346,18 +344,23 @@ void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const
     hc.hx[t] = 0.0;
   }
   // hann(n)[k] = 0.5 - 0.5 cos(2 pi k / n), stored at k * (64 / n)
-  for (int k = 0; k < lv.wy; k++) hc.hy[k * (64 / lv.wy)] = 0.5 - 0.5 * std::cos(2 * PI * k / lv.wy);
-  for (int k = 0; k < lv.wx; k++) hc.hx[k * (64 / lv.wx)] = 0.5 - 0.5 * std::cos(2 * PI * k / lv.wx);
-  PocConst* dc = nullptr;
-  OFC_CUDA(cudaMallocAsync((void**)&dc, sizeof(PocConst), st));
-  OFC_CUDA(cudaMemcpyAsync(dc, &hc, sizeof(PocConst), cudaMemcpyHostToDevice, st));
+  for (int k = 0; k < wy; k++) hc.hy[k * (64 / wy)] = 0.5 - 0.5 * std::cos(2 * PI * k / wy);
+  for (int k = 0; k < wx; k++) hc.hx[k * (64 / wx)] = 0.5 - 0.5 * std::cos(2 * PI * k / wx);
+  std::memcpy(out, &hc, sizeof(hc));
+}
+
+void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const int* xs, const int* ys,
+                     const double* iux, const double* iuy, const void* dconst, double* ux, double* uy, double* peak,
+                     cudaStream_t st) {
+  auto ok_len = [](int n) { return n == 16 || n == 32 || n == 64; };
+  if (!ok_len(lv.wy) || !ok_len(lv.wx))
+    throw Error(OFC_ERR_ARG, "the CUDA engine's POC windows are 16, 32 or 64 px a side (poc_win <= 64)");
   // lp.mean(): the share of frequencies with |f| <= 0.25 on both axes
   double lpm = (double)(2 * (lv.wy / 4) + 1) * (double)(2 * (lv.wx / 4) + 1) / ((double)lv.wy * lv.wx);
   size_t smem = (size_t)(lv.wy * lv.wx + (2 * (lv.wy / 4) + 1) * (2 * (lv.wx / 4) + 1)) * sizeof(double2);
   OFC_CUDA(cudaFuncSetAttribute((const void*)k_poc_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  OFC_LAUNCH(k_poc_grid, lv.nx * lv.ny, POC_T, smem, st, a, b, lv.W, lv.H, lv.wy, lv.wx, xs, ys, lv.nx, iux, iuy, dc,
-             lpm, ux, uy, peak);
-  OFC_CUDA(cudaFreeAsync(dc, st));
+  OFC_LAUNCH(k_poc_grid, lv.nx * lv.ny, POC_T, smem, st, a, b, lv.W, lv.H, lv.wy, lv.wx, xs, ys, lv.nx, iux, iuy,
+             (const PocConst*)dconst, lpm, ux, uy, peak);
 }
 
 // ---------------------------------------------------------------- clean (poc.py:95-140)

@@ -262,3 +262,34 @@ def track_pair(I1, I2, cfg=None, mask=None, init=None, engine=None) -> Result:
     eng._call("ofc_track_pair", _ptr(a, c_float_p), _ptr(b, c_float_p), w, h, _ptr(m, c_u8_p),
               _ptr(iu, c_float_p), _ptr(iv, c_float_p), ctypes.byref(c), ctypes.byref(o))
     return _result(o, arrs)
+
+
+def track_pair_device(I1, I2, cfg=None, mask=None, init=None, stream=None, engine=None):
+    """track_pair on device-resident torch tensors (float32 images, optional uint8/bool ROI and init fields):
+    ofc_track_pair_device on ``stream`` (a torch.cuda.Stream; None = the engine's own stream, synchronised
+    before returning). Returns a dict of device tensors named as the pair outputs."""
+    import torch
+    if I1.shape != I2.shape or I1.dim() != 2:
+        raise ValueError(f"image sizes differ or are not 2-D: {tuple(I1.shape)} vs {tuple(I2.shape)}")
+    cfg, c = _prep_cfg(cfg)
+    h, w = I1.shape
+    dev = I1.device
+    a = I1.to(torch.float32).contiguous()
+    b = I2.to(dev, torch.float32).contiguous()
+    m = None if mask is None else mask.to(dev, torch.uint8).contiguous()
+    iu = iv = None
+    if init is not None:
+        iu = init[0].to(dev, torch.float32).contiguous()
+        iv = init[1].to(dev, torch.float32).contiguous()
+    outs = {k: torch.empty((h, w), dtype=torch.uint8 if k == "valid" else torch.float32, device=dev)
+            for k in _abi.PAIR_FIELDS}
+    o = OfcPairOut()
+    for k, t in outs.items():
+        setattr(o, k, ctypes.cast(t.data_ptr(), c_u8_p if k == "valid" else c_float_p))
+    eng = engine or default_engine(dev.index or 0)
+    p = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
+    eng._call("ofc_track_pair_device", p(a), p(b), w, h, p(m), p(iu), p(iv), ctypes.byref(c), ctypes.byref(o),
+              ctypes.c_void_p(stream.cuda_stream) if stream is not None else None)
+    if stream is None:
+        torch.cuda.synchronize(dev)
+    return outs

@@ -157,3 +157,67 @@ def test_refine_raw_window_shift(oracle):
     want = oracle.refine(a[y0:y0 + h, x0:x0 + w], b[y0:y0 + h, x0:x0 + w], u, v, Config())
     inner = (slice(20, -20), slice(20, -20))
     assert rms(got["ux"][inner], want["ux"][inner]) < 5e-3
+
+
+def test_track_pair_graph_replay_and_device_api():
+    """The first call of a (size, configuration) runs eagerly and captures the pair as CUDA graphs; later calls
+    replay them. Replays, a different size in between (which reallocates the pooled buffers and drops the
+    graphs) and the device-resident entry point on a caller's stream all give the eager call's outputs."""
+    import torch
+    from optflow_b200 import Engine, track_pair_device
+    a, b = _synthetic_pair(192, 11)
+    roi = np.zeros(a.shape, bool)
+    roi[10:-10, 12:-12] = True
+    eng = Engine(0)
+    try:
+        first = track_pair(a, b, Config(), mask=roi, engine=eng)
+        launches = eng.kernel_launches()
+        again = track_pair(a, b, Config(), mask=roi, engine=eng)
+        per_pair = eng.kernel_launches() - launches
+        assert per_pair > 0
+        big = _synthetic_pair(256, 12)
+        track_pair(big[0], big[1], Config(), engine=eng)
+        third = track_pair(a, b, Config(), mask=roi, engine=eng)
+        fourth = track_pair(a, b, Config(), mask=roi, engine=eng)
+        for r in (again, third, fourth):
+            for k in ("ux", "uy", "conf", "raw_ux", "raw_uy", "valid"):
+                np.testing.assert_array_equal(getattr(r, k), getattr(first, k), err_msg=k)
+            for k in ("Exx", "Eyy", "Exy", "gmax", "vol"):
+                np.testing.assert_array_equal(r.strain[k], first.strain[k], err_msg=k)
+        st = torch.cuda.Stream()
+        ta, tb, tr = (torch.from_numpy(x).cuda() for x in (a, b, roi))
+        for _ in range(2):
+            with torch.cuda.stream(st):
+                out = track_pair_device(ta, tb, Config(), mask=tr, stream=st, engine=eng)
+            st.synchronize()
+            np.testing.assert_array_equal(out["ux"].cpu().numpy(), first.ux)
+            np.testing.assert_array_equal(out["conf"].cpu().numpy(), first.conf)
+            np.testing.assert_array_equal(out["valid"].cpu().numpy().astype(bool), first.valid)
+            np.testing.assert_array_equal(out["exx"].cpu().numpy(), first.strain["Exx"])
+    finally:
+        eng.close()
+
+
+def test_profile_mode_counts_replayed_kernels():
+    """Profile mode (per-kernel device times, the reference's OPTFLOW_GPU_KERNELS) sees every launch of a
+    replayed pair graph: the accumulation runs outer_iters x inner_iters times per pair."""
+    import ctypes
+    from optflow_b200 import Engine
+    a, b = _synthetic_pair(192, 13)
+    eng = Engine(0)
+    try:
+        eng.lib.ofc_set_profile(eng.handle, b"k_accumulate")
+        for _ in range(3):
+            track_pair(a, b, Config(), engine=eng)
+        cap = 8
+        names = ctypes.create_string_buffer(cap * 64)
+        counts = (ctypes.c_uint64 * cap)()
+        ms = (ctypes.c_double * cap)()
+        n = eng.lib.ofc_profile_read(eng.handle, names, 64, counts, ms, cap)
+        eng.lib.ofc_set_profile(eng.handle, None)
+        got = {names.raw[i * 64:(i + 1) * 64].split(b"\0", 1)[0].decode(): (counts[i], ms[i]) for i in range(n)}
+        cfg = Config()
+        assert got["k_accumulate"][0] == 3 * cfg.outer_iters * cfg.inner_iters
+        assert got["k_accumulate"][1] > 0
+    finally:
+        eng.close()
