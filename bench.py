@@ -116,6 +116,13 @@ def accumulate_bytes(W, H, F=12):
     return N * (20 * F + 32 + 16 + 56) + Np * 8 * F
 
 
+# DRAM traffic of one k_accumulate launch over its algorithmic bytes, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum = 459.7 MB against 474.4 MB algorithmic on a 1024^2 pair,
+# profiles/k_accumulate_1024.txt); the traffic of a launch at another size is this ratio times its
+# algorithmic bytes (both grow with the pixel and padded-pixel counts)
+ACC_TRAFFIC_RATIO = 459.7 / 474.4
+
+
 def cpu_sample(a, b, roi, n=512):
     c0 = (a.shape[0] - n) // 2
     sl = (slice(c0, c0 + n), slice(c0, c0 + n))
@@ -308,7 +315,9 @@ def main():
             byts = accumulate_bytes(n, n, cfg.n_filters())
             achieved = byts / per_launch_s / 1e9
             roof = {"bound": "hbm", "kernel": "k_accumulate", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                    "frac": achieved / peak, "peak_source": peak_kind,
+                    "traffic": ACC_TRAFFIC_RATIO * byts,
+                    "traffic_source": "ncu capture at 1024^2 scaled by algorithmic bytes",
                     "algorithmic_bytes_per_launch": byts, "launch_ms": per_launch_s * 1e3,
                     "launches_per_step": acc[0] / args.steps}
         base = None
