@@ -190,7 +190,11 @@ OFC_API int ofc_track_pair(ofc_engine* eng, const float* i1, const float* i2, si
  * ofc_track_pair on device-resident buffers: every pointer (inputs and the out fields) is device
  * memory of the engine's device; the work is queued on `stream` (a cudaStream_t, NULL = the
  * engine's own stream) and the call returns once it is queued, with out->timing left zero.
- * Inputs must stay untouched until the stream reaches the end of the work.
+ * Inputs must stay untouched until the stream reaches the end of the work. The inputs are copied
+ * into the engine's own buffers and the outputs out of them on `stream`; the pair itself runs as
+ * three CUDA graphs, captured on the first call for a (size, configuration, ROI and init present)
+ * after one eager run, and replayed by later calls, so `stream` must not be under capture itself.
+ * ofc_track_pair runs the same graphs on the engine's stream.
  */
 OFC_API int ofc_track_pair_device(ofc_engine* eng, const float* d_i1, const float* d_i2, size_t w, size_t h,
                           const uint8_t* d_roi, const float* d_init_ux, const float* d_init_uy,

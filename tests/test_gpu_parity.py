@@ -221,3 +221,40 @@ def test_profile_mode_counts_replayed_kernels():
         assert got["k_accumulate"][1] > 0
     finally:
         eng.close()
+
+
+def test_busy_lane_refuses_instead_of_waiting():
+    """A call beyond the engine's lanes is refused with OFC_ERR_BUSY (3) at once, like the Metal engine's
+    per-lane try_lock (rust/crates/optflow-gpu/src/engine.rs:660-676); the lane is free again afterwards."""
+    import threading
+    from optflow_b200 import Engine, EngineError
+    a, b = _synthetic_pair(512, 14)
+    eng = Engine(0, lanes=1)
+    try:
+        track_pair(a, b, Config(), engine=eng)  # buffers and graphs exist: the next call is replay-only
+        done = threading.Event()
+
+        def work():
+            while True:  # the main thread's probes can hold the lane for a moment: retry those refusals
+                try:
+                    track_pair(a, b, Config(), engine=eng)
+                    break
+                except EngineError as e:
+                    if e.status != 3:
+                        raise
+            done.set()
+
+        worker = threading.Thread(target=work)
+        busy = 0
+        worker.start()
+        while not done.is_set() and worker.is_alive():
+            try:
+                eng.check_window(512, 512)
+            except EngineError as e:
+                assert e.status == 3 and "busy" in str(e)
+                busy += 1
+        worker.join()
+        assert busy > 0
+        eng.check_window(512, 512)
+    finally:
+        eng.close()
