@@ -275,15 +275,12 @@ struct Lane {
     if (it != plans.end()) return it->second.first;
     FftPlan pl = fft_make_plan(L);
     std::vector<float2> tw = fft_twiddles(L);
-    std::vector<double2> twd = fft_twiddles_f64(L);
     std::unique_ptr<DevBuf> b(new DevBuf());
-    size_t b32 = tw.size() * sizeof(float2), b64 = twd.size() * sizeof(double2);
-    OFC_CUDA(cudaMalloc(&b->p, b64 + b32));
-    b->bytes = b64 + b32;
-    OFC_CUDA(cudaMemcpy(b->p, twd.data(), b64, cudaMemcpyHostToDevice));
-    OFC_CUDA(cudaMemcpy((char*)b->p + b64, tw.data(), b32, cudaMemcpyHostToDevice));
-    pl.twd = (const double2*)b->p;
-    pl.tw = (const float2*)((char*)b->p + b64);
+    size_t b32 = tw.size() * sizeof(float2);
+    OFC_CUDA(cudaMalloc(&b->p, b32));
+    b->bytes = b32;
+    OFC_CUDA(cudaMemcpy(b->p, tw.data(), b32, cudaMemcpyHostToDevice));
+    pl.tw = (const float2*)b->p;
     auto& slot = plans[L];
     slot.first = pl;
     slot.second = std::move(b);
@@ -416,25 +413,23 @@ const double* moment_taps(Lane& L, double sigma, int& r) {
   return L.cached(key, mt.data(), mt.size());
 }
 
-// reference_phase (phaseflow.py:100-111) of i1 in float64 transforms, stored as float32 (r.re, r.im, gx, gy)
-// and amp per filter. The transforms run in float64 because the phase gradient divides by |r|^2: near a zero
-// of a response, the absolute error of a float32 transform (~1e-7 of the largest response) is a large
-// relative error of r, and the weighted gradient terms w g^2 ~ |r2| |r_y|^2 / |r| of the normal equations
-// amplify it. Filters are processed in groups to bound the scratch (3 planes of ph x pw float64 per filter).
+// reference_phase (phaseflow.py:100-111) of i1: float32 transforms, as the reference's Rust port computes them
+// (gabor.rs:230-270, rustfft f32), with (r.re, r.im, gx, gy) and amp formed per pixel in float64 and stored
+// float32 per filter. Filters are processed in groups to bound the scratch (3 planes of ph x pw per filter).
 void reference_pack(Lane& L, const float* i1, int W, int H, const GaborTables& g, float4* ref4, float* amp) {
   cudaStream_t st = L.stream;
   const int ph = H + 2 * PAD, pw = W + 2 * PAD;
   const size_t Np = (size_t)ph * pw;
   const int G = std::min(g.F, 4);
-  double2* T64 = L.get<double2>("ref_T64", Np);
-  double2* U64 = L.get<double2>("ref_U64", Np * 3 * G);
   const FftPlan& plw = L.plan(pw);
   const FftPlan& plh = L.plan(ph);
-  launch_fft_rows_fwd_real_f64(i1, W, H, plw, ph, T64, st);
+  float2* T32 = L.get<float2>("fft_T", Np);
+  float2* U32 = L.get<float2>("ref_U32", Np * 3 * G);
+  launch_fft_rows_fwd_real(i1, W, H, plw, ph, T32, st);
   for (int k0 = 0; k0 < g.F; k0 += G) {
     int k1 = std::min(g.F, k0 + G);
-    launch_fft_cols_ref_f64(T64, plh, pw, g, k0, k1, U64, st);
-    launch_fft_rows_inv_ref_f64(U64, plw, ph, k0, k1, W, H, ref4, amp, st);
+    launch_fft_cols_ref_f32(T32, plh, pw, g, k0, k1, U32, st);
+    launch_fft_rows_inv_ref_f32(U32, plw, ph, k0, k1, W, H, ref4, amp, st);
   }
 }
 

@@ -2,13 +2,14 @@
 //
 // One thread block transforms C interleaved lines held in shared memory (element i of line l at
 // buf[i * C + l]), ping-ponging between two buffers of L * C values: each Stockham stage reads a butterfly's
-// inputs from one and writes its outputs to the other. Radices 2, 3, 4, 5 and 8 have register butterflies;
-// other primes (up to 31) a direct DFT. Twiddles come from a table rounded from float64.
+// inputs from one and writes its outputs to the other. Radices 2, 4 and 8 have register butterflies, 3, 5, 7,
+// 11 and 13 the symmetric odd form, other primes (up to 31) a direct DFT. Twiddles come from a table rounded
+// from float64.
 //
 // The pass structure of one "responses" evaluation (per outer iteration of the fine stage):
 //   rows:    reflect pad + real->complex + forward row FFT                      (read 4 B/px, write 8 B/px)
-//   columns: forward column FFT, then per filter k: x G_k (separable, float64 tables), inverse column FFT,
-//            causal + anticausal B-spline prefilter along y                       (read 8, write 8F)
+//   columns: forward column FFT in place (read 8, write 8); then per (column pair, filter k): x G_k (separable
+//            tables), inverse column FFT, causal + anticausal B-spline prefilter along y  (read 8F, write 8F)
 //   rows:    inverse row FFT, prefilter along x, scale 36 / (ph pw)               (read 8F, write 8F)
 // The prefilter along y commutes with the inverse FFT along x (operators on different axes), so the
 // result is bspline_coeffs(ifft2(F2 * G)) of phaseflow.py:456 up to rounding.
@@ -57,15 +58,6 @@ std::vector<float2> fft_twiddles(int L) {
   for (int i = 0; i < L; i++) {
     double a = -2.0 * PI * (double)i / (double)L;
     t[i] = make_float2((float)std::cos(a), (float)std::sin(a));
-  }
-  return t;
-}
-
-std::vector<double2> fft_twiddles_f64(int L) {
-  std::vector<double2> t(L);
-  for (int i = 0; i < L; i++) {
-    double a = -2.0 * PI * (double)i / (double)L;
-    t[i] = make_double2(std::cos(a), std::sin(a));
   }
   return t;
 }
@@ -152,29 +144,64 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(
 __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
 // multiply by -i (forward) or +i (inverse)
 __device__ __forceinline__ float2 rot(float2 a, bool inv) { return inv ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 conjf2(double2 a) { return make_double2(a.x, -a.y); }
-__device__ __forceinline__ double2 rot(double2 a, bool inv) { return inv ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x); }
 template <class C2> __device__ __forceinline__ C2 mkc(double re, double im);
 template <> __device__ __forceinline__ float2 mkc<float2>(double re, double im) { return make_float2((float)re, (float)im); }
-template <> __device__ __forceinline__ double2 mkc<double2>(double re, double im) { return make_double2(re, im); }
+
+// cos and sin of 2 pi m / P at compile time (Taylor series after reduction to [-pi/8, pi/8] by octant; exact to
+// float64 rounding for the small P here), for the constant coefficients of the odd-radix butterflies
+constexpr double ct_poly_sin(double x) {
+  double t = x, s = x;
+  for (int n = 1; n < 14; n++) {
+    t *= -x * x / ((2 * n) * (2 * n + 1));
+    s += t;
+  }
+  return s;
+}
+constexpr double ct_poly_cos(double x) {
+  double t = 1, s = 1;
+  for (int n = 1; n < 14; n++) {
+    t *= -x * x / ((2 * n - 1) * (2 * n));
+    s += t;
+  }
+  return s;
+}
+// angle 2 pi m / P = q (pi / 4) + r with |r| <= pi / 8
+constexpr void ct_sincos(int m, int P, double& c, double& sn) {
+  double a = 2 * PI * (double)m / (double)P;
+  int q = (int)(a / (PI / 4) + 0.5);
+  double r = a - q * (PI / 4);
+  double cr = ct_poly_cos(r), sr = ct_poly_sin(r);
+  constexpr double h = 0.70710678118654752440;  // cos(pi / 4)
+  double cq[8] = {1, h, 0, -h, -1, -h, 0, h}, sq[8] = {0, h, 1, h, 0, -h, -1, -h};
+  c = cq[q & 7] * cr - sq[q & 7] * sr;
+  sn = sq[q & 7] * cr + cq[q & 7] * sr;
+}
+template <int P>
+struct OddCoef {  // cs[k][j] = cos(2 pi j k / P), sn[k][j] = -sin(2 pi j k / P) (the forward kernel exp(-2 pi i jk / P))
+  float cs[P][P] = {}, sn[P][P] = {};
+  constexpr OddCoef() {
+    for (int k = 0; k < P; k++)
+      for (int j = 0; j < P; j++) {
+        double c = 0, s = 0;
+        ct_sincos((j * k) % P, P, c, s);
+        cs[k][j] = (float)c;
+        sn[k][j] = (float)(-s);
+      }
+  }
+};
 
 // Odd-radix butterfly with the symmetric form: for j = 1..(P-1)/2, a_j = v_j + v_{P-j}, b_j = v_j - v_{P-j};
 // o_0 = v_0 + sum a_j; o_k = v_0 + sum_j a_j cos_jk + i sum_j b_j sin_jk, o_{P-k} = the same with -i, where
-// w^{jk} = cos_jk + i sin_jk (w = exp(-2 pi i / P), conjugated for the inverse) is read from the twiddle table.
-template <int P, class C2, class Emit>
-__device__ __forceinline__ void odd_butterfly(const C2* in, size_t istep, const C2* __restrict__ tw, int LP, bool inv,
-                                              Emit emit) {
+// w^{jk} = cos_jk + i sin_jk (w = exp(-2 pi i / P), conjugated for the inverse) are compile-time constants.
+template <int P, class C2, class Load, class Emit>
+__device__ __forceinline__ void odd_butterfly(Load in, bool inv, Emit emit) {
   constexpr int Hh = (P - 1) / 2;
-  C2 v0 = in[0];
+  constexpr OddCoef<P> K{};
+  C2 v0 = in(0);
   C2 av[Hh], bv[Hh];
 #pragma unroll
   for (int j = 1; j <= Hh; j++) {
-    C2 x = in[j * istep], y = in[(P - j) * istep];
+    C2 x = in(j), y = in(P - j);
     av[j - 1] = cadd(x, y);
     bv[j - 1] = csub(x, y);
   }
@@ -182,61 +209,75 @@ __device__ __forceinline__ void odd_butterfly(const C2* in, size_t istep, const 
 #pragma unroll
   for (int j = 0; j < Hh; j++) s0 = cadd(s0, av[j]);
   emit(0, s0);
+  const float sg = inv ? -1.f : 1.f;
 #pragma unroll
   for (int k = 1; k <= Hh; k++) {
     C2 t = v0, u = mkc<C2>(0.0, 0.0);
 #pragma unroll
     for (int j = 1; j <= Hh; j++) {
-      C2 w = __ldg(tw + (size_t)((j * k) % P) * LP);
-      auto cs = w.x;
-      auto sn = inv ? -w.y : w.y;
-      t.x = fma(av[j - 1].x, cs, t.x);
-      t.y = fma(av[j - 1].y, cs, t.y);
-      u.x = fma(bv[j - 1].x, sn, u.x);
-      u.y = fma(bv[j - 1].y, sn, u.y);
+      const float cs = K.cs[k][j], sn = K.sn[k][j];
+      t.x = fmaf(av[j - 1].x, cs, t.x);
+      t.y = fmaf(av[j - 1].y, cs, t.y);
+      u.x = fmaf(bv[j - 1].x, sn, u.x);
+      u.y = fmaf(bv[j - 1].y, sn, u.y);
     }
+    u.x *= sg;
+    u.y *= sg;
     // i u = (-u.y, u.x)
     emit(k, mkc<C2>(t.x - u.y, t.y + u.x));
     emit(P - k, mkc<C2>(t.x + u.y, t.y - u.x));
   }
 }
 
-// One Stockham stage of radix P from buffer A to buffer B (C interleaved lines of length L, C = 1 << lc). q, r
-// of a butterfly come from multiplications by precomputed reciprocals (magic = ceil(2^32 / s), exact for the
-// sizes here). Radices 2, 4, 8 have hand-written butterflies, 3, 5, 7, 11 and 13 the symmetric odd form, and any
-// other radix (P = 0 here) a direct DFT with its inputs read from shared memory. Each radix is its own
-// non-inlined function, so that the registers of one radix's butterfly do not add to another's.
+// Shared-memory layouts of the transform buffers: element i at i + (i >> sh), sh = FFT_PAD (one pad slot
+// per 16 values) or 31 (no padding; i < 2^31). A stage whose outputs lie s * C apart with s * C < 32 writes
+// padded, which spreads its stores over the banks; the other buffers, and always the final one, are
+// unpadded. Buffer capacity: fft_buf_len(L, C) values.
+constexpr int FFT_PAD = 4;
+__host__ __device__ constexpr int fft_buf_len(int L, int C) { return L * C + ((L * C) >> FFT_PAD) + 1; }
+
+// One Stockham stage of radix P from buffer A (layout shift ish) to buffer B (layout shift osh); C interleaved
+// lines of length L, C = 1 << lc. q, r of a butterfly come from multiplications by precomputed reciprocals
+// (magic = ceil(2^32 / s), exact for the sizes here). Radices 2, 4, 8 have hand-written butterflies, 3, 5, 7,
+// 11 and 13 the symmetric odd form, and any other radix (P = 0 here) a direct DFT with its inputs read from
+// shared memory. Each radix is its own non-inlined function, so that the registers of one radix's butterfly do
+// not add to another's.
 template <int P, class C2>
 __device__ __noinline__ void stage_loop(const C2* __restrict__ A, C2* __restrict__ B, int lc, int L, int Pr, int s,
-                                        unsigned magic, const C2* __restrict__ tw, bool inv) {
+                                        unsigned magic, const C2* __restrict__ tw, bool inv, int ish, int osh) {
   const int RP = P ? P : Pr;
   const int C = 1 << lc;
   const int m = L / (RP * s);
   const int nb = (L / RP) << lc;
   const int LP = L / RP;
-  const size_t istep = (size_t)s * m * C, ostep = (size_t)s * C;
+  const int istep = s * m * C, ostep = s * C;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     const int l = b & (C - 1), bi = b >> lc;
     const int q = s == 1 ? bi : (int)__umulhi((unsigned)bi, magic), r = bi - q * s;
-    const C2* in = A + (size_t)(r + s * q) * C + l;
-    C2* out = B + (size_t)(r + s * RP * q) * C + l;
+    const int ib = (r + s * q) * C + l;
+    const int ob = (r + s * RP * q) * C + l;
+    auto in = [&](int j) {
+      const int i = ib + j * istep;
+      return A[i + (i >> ish)];
+    };
     auto emit = [&](int k, C2 val) {
       if (k > 0 && q > 0) {
         C2 w = __ldg(tw + (size_t)k * q * s);  // k q s < L
         val = cmul(val, inv ? conjf2(w) : w);
       }
-      out[k * ostep] = val;
+      const int o = ob + k * ostep;
+      B[o + (o >> osh)] = val;
     };
     auto tw_m = [&](int mm) {  // w_P^mm
       C2 w = __ldg(tw + (size_t)mm * LP);
       return inv ? conjf2(w) : w;
     };
     if constexpr (P == 2) {
-      C2 a0 = in[0], a1 = in[istep];
+      C2 a0 = in(0), a1 = in(1);
       emit(0, cadd(a0, a1));
       emit(1, csub(a0, a1));
     } else if constexpr (P == 4) {
-      C2 a0 = in[0], a1 = in[istep], a2 = in[2 * istep], a3 = in[3 * istep];
+      C2 a0 = in(0), a1 = in(1), a2 = in(2), a3 = in(3);
       C2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
       C2 t2 = cadd(a1, a3), t3 = rot(csub(a1, a3), inv);
       emit(0, cadd(t0, t2));
@@ -246,7 +287,7 @@ __device__ __noinline__ void stage_loop(const C2* __restrict__ A, C2* __restrict
     } else if constexpr (P == 8) {
       C2 v[8];
 #pragma unroll
-      for (int j = 0; j < 8; j++) v[j] = in[j * istep];
+      for (int j = 0; j < 8; j++) v[j] = in(j);
       C2 e[4], d[4];
       {
         C2 t0 = cadd(v[0], v[4]), t1 = csub(v[0], v[4]);
@@ -258,22 +299,30 @@ __device__ __noinline__ void stage_loop(const C2* __restrict__ A, C2* __restrict
         C2 t2 = cadd(v[3], v[7]), t3 = rot(csub(v[3], v[7]), inv);
         d[0] = cadd(t0, t2); d[2] = csub(t0, t2); d[1] = cadd(t1, t3); d[3] = csub(t1, t3);
       }
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        C2 t = k == 0 ? d[0] : cmul(d[k], tw_m(k));
-        emit(k, cadd(e[k], t));
-        emit(k + 4, csub(e[k], t));
-      }
+      // w8^k, k = 1..3: (h, -h), (0, -1), (-h, -h) forward; conjugates inverse (h = cos(pi / 4))
+      constexpr float h = 0.70710678118654752440f;
+      const float sg = inv ? 1.f : -1.f;
+      C2 t1 = mkc<C2>(h * (d[1].x - sg * d[1].y), h * (d[1].y + sg * d[1].x));
+      C2 t2 = mkc<C2>(-sg * d[2].y, sg * d[2].x);
+      C2 t3 = mkc<C2>(h * (-d[3].x - sg * d[3].y), h * (-d[3].y + sg * d[3].x));
+      emit(0, cadd(e[0], d[0]));
+      emit(4, csub(e[0], d[0]));
+      emit(1, cadd(e[1], t1));
+      emit(5, csub(e[1], t1));
+      emit(2, cadd(e[2], t2));
+      emit(6, csub(e[2], t2));
+      emit(3, cadd(e[3], t3));
+      emit(7, csub(e[3], t3));
     } else if constexpr (P == 3 || P == 5 || P == 7 || P == 11 || P == 13) {
-      odd_butterfly<P>(in, istep, tw, LP, inv, emit);
+      odd_butterfly<P, C2>(in, inv, emit);
     } else {
       for (int k = 0; k < RP; k++) {
-        C2 acc = in[0];
+        C2 acc = in(0);
         int jk = 0;
         for (int j = 1; j < RP; j++) {
           jk += k;
           if (jk >= RP) jk -= RP;
-          C2 av = in[j * istep];
+          C2 av = in(j);
           C2 w = tw_m(jk);
           acc.x = fma(av.x, w.x, fma(-av.y, w.y, acc.x));
           acc.y = fma(av.x, w.y, fma(av.y, w.x, acc.y));
@@ -286,32 +335,36 @@ __device__ __noinline__ void stage_loop(const C2* __restrict__ A, C2* __restrict
 
 template <class C2>
 __device__ __forceinline__ void fft_stage(const C2* __restrict__ A, C2* __restrict__ B, int lc, int L, int P, int s,
-                                          unsigned magic, const C2* __restrict__ tw, bool inv) {
+                                          unsigned magic, const C2* __restrict__ tw, bool inv, int ish, int osh) {
   switch (P) {
-    case 2: stage_loop<2, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
-    case 3: stage_loop<3, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
-    case 4: stage_loop<4, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
-    case 5: stage_loop<5, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
-    case 7: stage_loop<7, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
-    case 8: stage_loop<8, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
-    case 11: stage_loop<11, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
-    case 13: stage_loop<13, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
-    default: stage_loop<0, C2>(A, B, lc, L, P, s, magic, tw, inv); break;
+    case 2: stage_loop<2, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
+    case 3: stage_loop<3, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
+    case 4: stage_loop<4, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
+    case 5: stage_loop<5, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
+    case 7: stage_loop<7, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
+    case 8: stage_loop<8, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
+    case 11: stage_loop<11, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
+    case 13: stage_loop<13, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
+    default: stage_loop<0, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
   }
   __syncthreads();
 }
 
-// runs the plan on buf (tmp: scratch of the same size); returns the buffer that holds the result
-template <class C2>
-__device__ C2* fft_run(C2* buf, C2* tmp, int C, const FftPlan& pl, bool inv) {
+// runs the plan on buf (tmp: scratch of the same capacity, fft_buf_len(L, C)); buf holds the input unpadded
+// and the returned buffer the result unpadded
+template <int C, class C2>
+__device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
+  static_assert(C == 1 || C == 2 || C == 4, "C: a power of two up to 4");
+  static_assert(sizeof(C2) == sizeof(float2), "float32 transforms");
   C2* a = buf;
   C2* b = tmp;
-  const C2* tw;
-  if constexpr (sizeof(C2) == sizeof(double2)) tw = (const C2*)pl.twd;
-  else tw = (const C2*)pl.tw;
-  const int lc = C == 4 ? 2 : (C == 2 ? 1 : 0);
+  const C2* tw = (const C2*)pl.tw;
+  constexpr int lc = C == 4 ? 2 : (C == 2 ? 1 : 0);
+  int ish = 31;
   for (int st = 0; st < pl.nst; st++) {
-    fft_stage<C2>(a, b, lc, pl.L, pl.p[st], pl.s[st], pl.magic[st], tw, inv);
+    const int osh = (st + 1 < pl.nst && pl.s[st] * C < 32) ? FFT_PAD : 31;
+    fft_stage<C2>(a, b, lc, pl.L, pl.p[st], pl.s[st], pl.magic[st], tw, inv, ish, osh);
+    ish = osh;
     C2* t = a;
     a = b;
     b = t;
@@ -320,204 +373,195 @@ __device__ C2* fft_run(C2* buf, C2* tmp, int C, const FftPlan& pl, bool inv) {
 }
 
 // Cubic B-spline prefilter (interp.py:13-27, without the factor 6, which the caller folds into its
-// scale) of C interleaved complex lines of length n in buf, in float64 arithmetic. The line is cut into
-// T / C segments; each recursive pass computes every segment's entry value from a warm-up of IIR_WARM
-// samples (z^29 < 3e-17, below float64 rounding), then runs its segment. carry: 2 * T double2 of scratch.
-__device__ void prefilter_smem(float2* buf, int C, int n, double2* carry, double2* edge) {
+// scale) of C interleaved complex lines of length n in buf, in float32 arithmetic (the filter is stable,
+// |z| < 1, so its rounding errors decay geometrically and stay at the level of the float32 storage). The
+// line is cut into at most T / C segments; each recursive pass computes every segment's entry value from a
+// warm-up of IIR_WARM_F32 samples (z^17 < 6e-10, below float32 rounding), then runs its segment.
+// carry: 2 * T float2 of scratch; edge: 2 * C float2 (both may lie in the transform's idle buffer).
+template <int C>
+__device__ void prefilter_smem(float2* buf, int n, float2* carry, float2* edge) {
   if (n == 1) return;
-  const double z = bspline_z();
+  const float z = (float)bspline_z();
   const int tid = threadIdx.x, T = blockDim.x;
-  const int S = T / C;  // segments per line
+  // segments per line: at most T / C, with an odd length, so that the threads of a warp, which walk their
+  // segments in step, fall on distinct banks
+  int S = T / C;
+  while (S > 1 && (((n + S - 1) / S) & 1) == 0) S--;
   const int l = tid % C, sg = tid / C;
   const int len = (n + S - 1) / S;
   const int s0 = sg * len, e0 = min(n, s0 + len);
   const bool live = sg < S && s0 < e0;
-  auto X = [&](int i) { float2 v = buf[(size_t)i * C + l]; return make_double2(v.x, v.y); };
-  // ---- causal: y[0] = sum_{k < min(n, 21)} z^k x[k]; y[i] = x[i] + z y[i-1]
+  auto X = [&](int i) { return buf[i * C + l]; };
+  auto init_causal = [&]() {  // y[0] = sum_{k < min(n, 21)} z^k x[k]
+    int hz = min(n, HORIZON);
+    float2 a = make_float2(0.f, 0.f);
+    float zk = 1.f;
+    for (int k = 0; k < hz; k++) {
+      float2 v = X(k);
+      a.x = fmaf(zk, v.x, a.x);
+      a.y = fmaf(zk, v.y, a.y);
+      zk *= z;
+    }
+    return a;
+  };
+  // ---- causal: y[i] = x[i] + z y[i-1]
   if (live) {
-    if (sg == 0) {
-      int hz = min(n, HORIZON);
-      double2 a = make_double2(0, 0);
-      double zk = 1.0;
-      for (int k = 0; k < hz; k++) {
-        double2 v = X(k);
-        a.x += zk * v.x;
-        a.y += zk * v.y;
-        zk *= z;
-      }
-      edge[l] = a;  // y[0]
-    }
-    // y[e0 - 1]
+    if (sg == 0) edge[l] = init_causal();
     int start = e0 - 1 - IIR_WARM_F32;
-    double2 y;
+    float2 y;
+    int i = start;
     if (start <= 0) {
-      int hz = min(n, HORIZON);
-      y = make_double2(0, 0);
-      double zk = 1.0;
-      for (int k = 0; k < hz; k++) {
-        double2 v = X(k);
-        y.x += zk * v.x;
-        y.y += zk * v.y;
-        zk *= z;
-      }
-      for (int i = 1; i < e0; i++) {
-        double2 v = X(i);
-        y.x = v.x + z * y.x;
-        y.y = v.y + z * y.y;
-      }
+      y = init_causal();
+      i = 1;
     } else {
-      y = make_double2(0, 0);
-      for (int i = start; i < e0; i++) {
-        double2 v = X(i);
-        y.x = v.x + z * y.x;
-        y.y = v.y + z * y.y;
-      }
+      y = make_float2(0.f, 0.f);
     }
-    carry[tid] = y;
+    for (; i < e0; i++) {
+      float2 v = X(i);
+      y.x = fmaf(z, y.x, v.x);
+      y.y = fmaf(z, y.y, v.y);
+    }
+    carry[tid] = y;  // y[e0 - 1]
   }
   __syncthreads();
   if (live) {
-    double2 y;
+    float2 y;
     int i0;
     if (sg == 0) {
       y = edge[l];
-      buf[l] = make_float2((float)y.x, (float)y.y);
+      buf[l] = y;
       i0 = 1;
     } else {
       y = carry[tid - C];
       i0 = s0;
     }
     for (int i = i0; i < e0; i++) {
-      double2 v = X(i);
-      y.x = v.x + z * y.x;
-      y.y = v.y + z * y.y;
-      buf[(size_t)i * C + l] = make_float2((float)y.x, (float)y.y);
+      float2 v = X(i);
+      y.x = fmaf(z, y.x, v.x);
+      y.y = fmaf(z, y.y, v.y);
+      buf[i * C + l] = y;
     }
   }
   __syncthreads();
   // ---- anticausal: c[n-1] = z / (z^2 - 1) (y[n-1] + z y[n-2]); c[i] = z (c[i+1] - y[i])
-  const double g = z / (z * z - 1.0);
+  const float g = (float)(bspline_z() / (bspline_z() * bspline_z() - 1.0));
+  auto init_anti = [&]() {
+    float2 a = X(n - 1), b = X(n - 2);
+    return make_float2(g * fmaf(z, b.x, a.x), g * fmaf(z, b.y, a.y));
+  };
   if (live) {
-    double2 c;
+    if (e0 == n) edge[C + l] = init_anti();
     int stop = s0 + IIR_WARM_F32;
-    if (e0 == n) {
-      double2 a = X(n - 1), b = X(n - 2);
-      edge[C + l] = make_double2(g * (a.x + z * b.x), g * (a.y + z * b.y));
-    }
+    float2 c;
+    int i = stop;
     if (stop >= n - 1) {
-      double2 a = X(n - 1), b = X(n - 2);
-      c = make_double2(g * (a.x + z * b.x), g * (a.y + z * b.y));
-      for (int i = n - 2; i >= s0; i--) {
-        double2 v = X(i);
-        c.x = z * (c.x - v.x);
-        c.y = z * (c.y - v.y);
-      }
+      c = init_anti();
+      i = n - 2;
     } else {
-      c = make_double2(0, 0);
-      for (int i = stop; i >= s0; i--) {
-        double2 v = X(i);
-        c.x = z * (c.x - v.x);
-        c.y = z * (c.y - v.y);
-      }
+      c = make_float2(0.f, 0.f);
+    }
+    for (; i >= s0; i--) {
+      float2 v = X(i);
+      c.x = z * (c.x - v.x);
+      c.y = z * (c.y - v.y);
     }
     carry[T + tid] = c;  // c[s0]
   }
   __syncthreads();
   if (live) {
-    double2 c;
+    float2 c;
     int i0;
     if (e0 == n) {
       c = edge[C + l];
-      buf[(size_t)(n - 1) * C + l] = make_float2((float)c.x, (float)c.y);
+      buf[(n - 1) * C + l] = c;
       i0 = n - 2;
     } else {
       c = carry[T + tid + C];  // c[e0] of the next segment
       i0 = e0 - 1;
     }
     for (int i = i0; i >= s0; i--) {
-      double2 v = X(i);
+      float2 v = X(i);
       c.x = z * (c.x - v.x);
       c.y = z * (c.y - v.y);
-      buf[(size_t)i * C + l] = make_float2((float)c.x, (float)c.y);
+      buf[i * C + l] = c;
     }
   }
   __syncthreads();
 }
 
+// reflect (mirror without repeating the edge, interp.py:38-43) of an index at most one period outside [0, n)
+__device__ __forceinline__ int reflect_near(int i, int n) {
+  int m = i < 0 ? -i : i;
+  if (m >= n) m = 2 * (n - 1) - m;
+  if (m < 0 || m >= n) m = (int)mirror_idx(i, n);  // far outside (n tiny): the general rule
+  return m;
+}
+
 // ---------------------------------------------------------------- kernels
-template <class C2>
-__global__ void __launch_bounds__(FFT_TMAX) k_fft_rows_fwd_real(const float* __restrict__ img, int W, int H, FftPlan plw,
-                                                                int ph, C2* __restrict__ out) {
+// Every kernel stages its lines in buffers of fft_buf_len(L, C) values (the transforms' padded layouts); the
+// prefilter's carries live in the buffer the transform left idle.
+
+__global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_fwd_real(const float* __restrict__ img, int W, int H,
+                                                                  FftPlan plw, int ph, float2* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  C2* sm = (C2*)smraw;
+  float2* sm = (float2*)smraw;
   const int pw = plw.L;
-  C2* t = sm + pw;
+  float2* t = sm + fft_buf_len(pw, 1);
   const int yp = blockIdx.x;
-  const int ys = (int)mirror_idx(yp - PAD, H);
+  const int ys = reflect_near(yp - PAD, H);
   const float* row = img + (size_t)ys * W;
-  for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[x] = mkc<C2>(__ldg(row + mirror_idx(x - PAD, W)), 0.0);
+  for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[x] = make_float2(__ldg(row + reflect_near(x - PAD, W)), 0.f);
   __syncthreads();
-  C2* r = fft_run(sm, t, 1, plw, false);
-  C2* o = out + (size_t)yp * pw;
+  float2* r = fft_run<1>(sm, t, plw, false);
+  float2* o = out + (size_t)yp * pw;
   for (int x = threadIdx.x; x < pw; x += blockDim.x) o[x] = r[x];
 }
 
-// Tin: ph x pw row-transformed; per block C adjacent columns. Shared memory: S (spectrum), W1, W2 (ping-pong),
-// prefilter carries.
-template <class C2>
-__global__ void __launch_bounds__(FFT_TMAX) k_fft_cols_filters(const C2* __restrict__ Tin, FftPlan plh, int pw,
-                                                               GaborTables g, int C, int refpack, int k0,
-                                                               int k1, C2* __restrict__ U) {
+// The reference pack's column pass: per block C adjacent columns of Tin (ph x pw, row-transformed; element i of
+// the block's tile is row i >> LC, column i & (C - 1)); forward transform, then for filters [k0, k1) the three
+// planes S G, S G i fx, S G i fy (factors formed in float64), each inverted along y into U (3 planes per filter).
+// Shared memory: S (spectrum) and W1, W2 (ping-pong).
+template <int C>
+__global__ void __launch_bounds__(FFT_TMAX) k_fft_cols_refpack(const float2* __restrict__ Tin, FftPlan plh, int pw,
+                                                               GaborTables g, int k0, int k1, float2* __restrict__ U) {
+  constexpr int LC = C == 4 ? 2 : (C == 2 ? 1 : 0);
   extern __shared__ __align__(16) unsigned char smraw[];
-  C2* sm = (C2*)smraw;
+  float2* sm = (float2*)smraw;
   const int ph = plh.L;
-  const size_t LC = (size_t)ph * C;
-  C2* S = sm;
-  C2* W1 = sm + LC;
-  C2* W2 = sm + 2 * LC;
-  double2* carry = (double2*)(((uintptr_t)(sm + 3 * LC) + 15) & ~(uintptr_t)15);  // 16-byte aligned
-  double2* edge = carry + 2 * blockDim.x;
+  const int n = ph * C, nb = fft_buf_len(ph, C);
+  float2* S = sm;
+  float2* W1 = sm + nb;
+  float2* W2 = sm + 2 * nb;
   const int x0 = blockIdx.x * C;
-  for (int i = threadIdx.x; i < ph * C; i += blockDim.x) {
-    int y = i / C, l = i - y * C, x = x0 + l;
-    S[i] = x < pw ? Tin[(size_t)y * pw + x] : mkc<C2>(0.0, 0.0);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int y = i >> LC, x = x0 + (i & (C - 1));
+    S[i] = x < pw ? Tin[(size_t)y * pw + x] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  C2* spec = fft_run(S, W1, C, plh, false);
+  float2* spec = fft_run<C>(S, W1, plh, false);
   if (spec != S) {
-    for (int i = threadIdx.x; i < ph * C; i += blockDim.x) S[i] = spec[i];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) S[i] = spec[i];
     __syncthreads();
   }
   const size_t plane = (size_t)ph * pw;
-  const int nvar = refpack ? 3 : 1;
   for (int k = k0; k < k1; k++) {
     const double* exk = g.ex + (size_t)k * pw;
     const double* eyk = g.ey + (size_t)k * ph;
-    const float* exkf = g.exf + (size_t)k * pw;
-    const float* eykf = g.eyf + (size_t)k * ph;
-    for (int v = 0; v < nvar; v++) {
-      for (int i = threadIdx.x; i < ph * C; i += blockDim.x) {
-        int y = i / C, l = i - y * C, x = min(x0 + l, pw - 1);
-        C2 sv = S[i];
-        if constexpr (sizeof(C2) == sizeof(float2)) {
-          float G = fmaf(g.hxf[x], g.omyf[y], g.omxf[x]) * (exkf[x] * eykf[y]);
-          W1[i] = mkc<C2>(sv.x * G, sv.y * G);
-        } else {
-          double G = fma(g.hx[x], g.omy[y], g.omx[x]) * exk[x] * eyk[y];
-          double re = sv.x * G, im = sv.y * G;
-          if (v == 1) { double f = g.fx[x]; double t = re; re = -im * f; im = t * f; }        // x i fx
-          else if (v == 2) { double f = g.fy[y]; double t = re; re = -im * f; im = t * f; }   // x i fy
-          W1[i] = mkc<C2>(re, im);
-        }
+    for (int v = 0; v < 3; v++) {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        int y = i >> LC, x = min(x0 + (i & (C - 1)), pw - 1);
+        float2 sv = S[i];
+        double G = fma(g.hx[x], g.omy[y], g.omx[x]) * exk[x] * eyk[y];
+        double re = sv.x * G, im = sv.y * G;
+        if (v == 1) { double f = g.fx[x]; double t = re; re = -im * f; im = t * f; }        // x i fx
+        else if (v == 2) { double f = g.fy[y]; double t = re; re = -im * f; im = t * f; }   // x i fy
+        W1[i] = make_float2((float)re, (float)im);
       }
       __syncthreads();
-      C2* res = fft_run(W1, W2, C, plh, true);
-      if constexpr (sizeof(C2) == sizeof(float2)) {
-        if (!refpack) prefilter_smem((float2*)res, C, ph, carry, edge);
-      }
-      C2* dst = U + (size_t)((k - k0) * nvar + v) * plane;
-      for (int i = threadIdx.x; i < ph * C; i += blockDim.x) {
-        int y = i / C, l = i - y * C, x = x0 + l;
+      float2* res = fft_run<C>(W1, W2, plh, true);
+      float2* dst = U + (size_t)((k - k0) * 3 + v) * plane;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        int y = i >> LC, x = x0 + (i & (C - 1));
         if (x < pw) dst[(size_t)y * pw + x] = res[i];
       }
       __syncthreads();
@@ -525,53 +569,105 @@ __global__ void __launch_bounds__(FFT_TMAX) k_fft_cols_filters(const C2* __restr
   }
 }
 
+// The column pass of the responses in two kernels, so that a block holds only two buffers of C columns
+// (several blocks per SM instead of one): k_fft_cols_fwd writes the column spectrum S (ph x pw, row-major,
+// small enough to stay in L2), then k_fft_cols_inv_filter, one block per (C columns, filter k), multiplies S by
+// G_k, inverts along y and prefilters along y into plane k of U.
+constexpr int COLS_TMAX = 320;  // threads per block of the split column pass (3 blocks per SM: <= 64 registers)
+
+template <int C>
+__global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_fwd(const float2* Tin, FftPlan plh, int pw, float2* S) {
+  constexpr int LC = C == 4 ? 2 : (C == 2 ? 1 : 0);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2* A = (float2*)smraw;
+  const int ph = plh.L, n = ph * C;
+  float2* B = A + fft_buf_len(ph, C);
+  const int x0 = blockIdx.x * C;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int y = i >> LC, x = x0 + (i & (C - 1));
+    A[i] = x < pw ? Tin[(size_t)y * pw + x] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  float2* r = fft_run<C>(A, B, plh, false);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int y = i >> LC, x = x0 + (i & (C - 1));
+    if (x < pw) S[(size_t)y * pw + x] = r[i];
+  }
+}
+
+template <int C>
+__global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const float2* __restrict__ S, FftPlan plh, int pw,
+                                                                      GaborTables g, float2* __restrict__ U) {
+  constexpr int LC = C == 4 ? 2 : (C == 2 ? 1 : 0);
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2* A = (float2*)smraw;
+  const int ph = plh.L, n = ph * C;
+  float2* B = A + fft_buf_len(ph, C);
+  const int x0 = blockIdx.x * C, k = blockIdx.y;
+  const float* exkf = g.exf + (size_t)k * pw;
+  const float* eykf = g.eyf + (size_t)k * ph;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int y = i >> LC, xr = x0 + (i & (C - 1)), x = min(xr, pw - 1);
+    float2 sv = xr < pw ? S[(size_t)y * pw + x] : make_float2(0.f, 0.f);
+    float G = fmaf(__ldg(g.hxf + x), __ldg(g.omyf + y), __ldg(g.omxf + x)) * (__ldg(exkf + x) * __ldg(eykf + y));
+    A[i] = make_float2(sv.x * G, sv.y * G);
+  }
+  __syncthreads();
+  float2* r = fft_run<C>(A, B, plh, true);
+  float2* carry = r == A ? B : A;
+  prefilter_smem<C>(r, ph, carry, carry + 2 * blockDim.x);
+  float2* dst = U + (size_t)k * ph * pw;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int y = i >> LC, x = x0 + (i & (C - 1));
+    if (x < pw) dst[(size_t)y * pw + x] = r[i];
+  }
+}
+
 __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int ph,
-                                                                float scale, float2* __restrict__ R) {
+                                                                  float scale, float2* __restrict__ R) {
   extern __shared__ float2 sm[];
   const int pw = plw.L;
-  float2* t = sm + pw;
-  double2* carry = (double2*)(sm + 2 * pw);
-  double2* edge = carry + 2 * blockDim.x;
+  float2* t = sm + fft_buf_len(pw, 1);
   const int y = blockIdx.x, k = blockIdx.y;
   const size_t off = (size_t)k * ph * pw + (size_t)y * pw;
   for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[x] = U[off + x];
   __syncthreads();
-  float2* r = fft_run(sm, t, 1, plw, true);
-  prefilter_smem(r, 1, pw, carry, edge);
+  float2* r = fft_run<1>(sm, t, plw, true);
+  float2* carry = r == sm ? t : sm;
+  prefilter_smem<1>(r, pw, carry, carry + 2 * blockDim.x);
   for (int x = threadIdx.x; x < pw; x += blockDim.x) {
     float2 v = r[x];
     R[off + x] = make_float2(v.x * scale, v.y * scale);
   }
 }
 
-template <class C2>
-__global__ void __launch_bounds__(FFT_TMAX) k_fft_rows_inv_ref(const C2* __restrict__ U, FftPlan plw, int ph, int W,
+__global__ void __launch_bounds__(FFT_TMAX) k_fft_rows_inv_ref(const float2* __restrict__ U, FftPlan plw, int ph, int W,
                                                                int H, int k0, float4* __restrict__ ref4,
                                                                float* __restrict__ amp) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  C2* sm = (C2*)smraw;
-  const int pw = plw.L;
-  C2* t = sm + 3 * pw;
+  float2* sm = (float2*)smraw;
+  const int pw = plw.L, nb = fft_buf_len(pw, 1);
+  float2* t = sm + 3 * nb;
   const int y = blockIdx.x, kk = blockIdx.y, k = k0 + kk;  // y: row of the W x H crop
   const size_t plane = (size_t)ph * pw;
   for (int i = threadIdx.x; i < pw * 3; i += blockDim.x) {
     int v = i / pw, x = i - v * pw;
-    sm[i] = U[(size_t)(3 * kk + v) * plane + (size_t)(y + PAD) * pw + x];
+    sm[v * nb + x] = U[(size_t)(3 * kk + v) * plane + (size_t)(y + PAD) * pw + x];
   }
   __syncthreads();
-  C2* rr[3];
+  float2* rr[3];
   for (int v = 0; v < 3; v++) {
-    C2* res = fft_run(sm + v * pw, t, 1, plw, true);
-    if (res != sm + v * pw) {
-      for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[v * pw + x] = res[x];
+    float2* res = fft_run<1>(sm + v * nb, t, plw, true);
+    if (res != sm + v * nb) {
+      for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[v * nb + x] = res[x];
       __syncthreads();
     }
-    rr[v] = sm + v * pw;
+    rr[v] = sm + v * nb;
   }
   const double sc = 1.0 / ((double)ph * (double)pw);
   for (int x = threadIdx.x; x < W; x += blockDim.x) {
     int xp = x + PAD;
-    C2 a = rr[0][xp], b = rr[1][xp], c = rr[2][xp];
+    float2 a = rr[0][xp], b = rr[1][xp], c = rr[2][xp];
     double rre = a.x * sc, rim = a.y * sc;
     double xre = b.x * sc, xim = b.y * sc, yre = c.x * sc, yim = c.y * sc;
     double a2 = rre * rre + rim * rim + 1e-12;
@@ -589,7 +685,7 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_lines(float2* data, FftPlan
   float2* row = data + (size_t)blockIdx.x * pl.L;
   for (int x = threadIdx.x; x < pl.L; x += blockDim.x) sm[x] = row[x];
   __syncthreads();
-  float2* r = fft_run(sm, sm + pl.L, 1, pl, inv != 0);
+  float2* r = fft_run<1>(sm, sm + fft_buf_len(pl.L, 1), pl, inv != 0);
   for (int x = threadIdx.x; x < pl.L; x += blockDim.x) row[x] = r[x];
 }
 
@@ -600,12 +696,18 @@ static void set_smem(const void* fn, size_t bytes) {
   OFC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
-// columns per block of the column pass: C adjacent columns make 32-byte row segments; elem: bytes per value
-static int cols_C(int ph, size_t elem, bool carries, int& T, size_t& sm) {
-  for (int C : {int(32 / elem), int(16 / elem), 1}) {
-    if (C < 1) continue;
+static size_t fbytes(int L, int C) { return (size_t)fft_buf_len(L, C) * sizeof(float2); }
+
+// shared memory of a transform with a prefilter: two buffers, the idle one holding 2 T + 2 C carries
+static size_t smem_prefilter(int L, int C, int T) {
+  return std::max<size_t>(2 * fbytes(L, C), fbytes(L, C) + (size_t)(2 * T + 2 * C) * sizeof(float2));
+}
+
+// columns per block of the reference pack's column pass: C adjacent columns make 32-byte row segments
+static int cols_C(int ph, int& T, size_t& sm) {
+  for (int C : {4, 2, 1}) {
     T = fft_threads(ph, C);
-    sm = (size_t)3 * ph * C * elem + 16 + (carries ? (size_t)(2 * T + 2 * C) * sizeof(double2) : 0);
+    sm = 3 * fbytes(ph, C);
     if (sm <= SMEM_MAX) return C;
   }
   throw Error(OFC_ERR_WINDOW, "padded height " + std::to_string(ph) + " too large for the column pass");
@@ -615,9 +717,10 @@ bool fft_fits(int ph, int pw) {
   try {
     int T;
     size_t sm;
-    cols_C(ph, sizeof(float2), true, T, sm);
-    cols_C(ph, sizeof(double2), false, T, sm);
-    return 4 * (size_t)pw * sizeof(double2) <= SMEM_MAX;
+    int Tc = std::min(fft_threads(ph, 2), COLS_TMAX);
+    if (smem_prefilter(ph, 2, Tc) > SMEM_MAX) return false;
+    cols_C(ph, T, sm);
+    return 4 * fbytes(pw, 1) <= SMEM_MAX && smem_prefilter(pw, 1, fft_threads(pw, 1)) <= SMEM_MAX;
   } catch (const Error&) {
     return false;
   }
@@ -625,58 +728,67 @@ bool fft_fits(int ph, int pw) {
 
 void launch_fft_rows_fwd_real(const float* img, int W, int H, const FftPlan& plw, int ph, float2* out, cudaStream_t st) {
   int T = fft_threads(plw.L, 1);
-  size_t sm = (size_t)2 * plw.L * sizeof(float2);
-  set_smem((const void*)k_fft_rows_fwd_real<float2>, sm);
-  OFC_LAUNCH(k_fft_rows_fwd_real<float2>, ph, T, sm, st, img, W, H, plw, ph, out);
+  size_t sm = 2 * fbytes(plw.L, 1);
+  set_smem((const void*)k_fft_rows_fwd_real, sm);
+  OFC_LAUNCH(k_fft_rows_fwd_real, ph, T, sm, st, img, W, H, plw, ph, out);
 }
 
-void launch_fft_rows_fwd_real_f64(const float* img, int W, int H, const FftPlan& plw, int ph, double2* out,
-                                  cudaStream_t st) {
-  int T = fft_threads(plw.L, 1);
-  size_t sm = (size_t)2 * plw.L * sizeof(double2);
-  set_smem((const void*)k_fft_rows_fwd_real<double2>, sm);
-  OFC_LAUNCH(k_fft_rows_fwd_real<double2>, ph, T, sm, st, img, W, H, plw, ph, out);
-}
-
-void launch_fft_cols_filters(const float2* Tin, const FftPlan& plh, int pw, const GaborTables& g, float2* U,
-                             cudaStream_t st) {
-  int T;
-  size_t sm;
-  int C = cols_C(plh.L, sizeof(float2), true, T, sm);
-  set_smem((const void*)k_fft_cols_filters<float2>, sm);
-  OFC_LAUNCH(k_fft_cols_filters<float2>, div_up(pw, C), T, sm, st, Tin, plh, pw, g, C, 0, 0, g.F, U);
-}
-
-void launch_fft_cols_ref_f64(const double2* Tin, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1,
-                             double2* U, cudaStream_t st) {
-  int T;
-  size_t sm;
-  int C = cols_C(plh.L, sizeof(double2), false, T, sm);
-  set_smem((const void*)k_fft_cols_filters<double2>, sm);
-  OFC_LAUNCH(k_fft_cols_filters<double2>, div_up(pw, C), T, sm, st, Tin, plh, pw, g, C, 1, k0, k1, U);
+void launch_fft_cols_filters(float2* T, const FftPlan& plh, int pw, const GaborTables& g, float2* U, cudaStream_t st) {
+  constexpr int C = 2;
+  const int ph = plh.L;
+  int nt = std::min(fft_threads(ph, C), COLS_TMAX);
+  size_t sm_f = 2 * fbytes(ph, C);
+  size_t sm_i = smem_prefilter(ph, C, nt);
+  if (sm_i > SMEM_MAX) throw Error(OFC_ERR_WINDOW, "padded height " + std::to_string(ph) + " too large for the column pass");
+  set_smem((const void*)k_fft_cols_fwd<C>, sm_f);
+  set_smem((const void*)k_fft_cols_inv_filter<C>, sm_i);
+  // in place: a block reads its C columns whole before it writes their spectrum back
+  OFC_LAUNCH(k_fft_cols_fwd<C>, div_up(pw, C), nt, sm_f, st, T, plh, pw, T);
+  dim3 grid(div_up(pw, C), g.F);
+  OFC_LAUNCH(k_fft_cols_inv_filter<C>, grid, nt, sm_i, st, T, plh, pw, g, U);
 }
 
 void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F, float2* R, cudaStream_t st) {
   int T = fft_threads(plw.L, 1);
-  size_t sm = (size_t)2 * plw.L * sizeof(float2) + (size_t)(2 * T + 2) * sizeof(double2);
+  size_t sm = smem_prefilter(plw.L, 1, T);
   set_smem((const void*)k_fft_rows_inv_resp, sm);
   float scale = (float)(36.0 / ((double)ph * (double)plw.L));
   dim3 grid(ph, F);
   OFC_LAUNCH(k_fft_rows_inv_resp, grid, T, sm, st, U, plw, ph, scale, R);
 }
 
-void launch_fft_rows_inv_ref_f64(const double2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,
+void launch_fft_cols_ref_f32(const float2* Tin, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1,
+                             float2* U, cudaStream_t st) {
+  int T;
+  size_t sm;
+  int C = cols_C(plh.L, T, sm);
+  switch (C) {
+    case 4:
+      set_smem((const void*)k_fft_cols_refpack<4>, sm);
+      OFC_LAUNCH(k_fft_cols_refpack<4>, div_up(pw, C), T, sm, st, Tin, plh, pw, g, k0, k1, U);
+      break;
+    case 2:
+      set_smem((const void*)k_fft_cols_refpack<2>, sm);
+      OFC_LAUNCH(k_fft_cols_refpack<2>, div_up(pw, C), T, sm, st, Tin, plh, pw, g, k0, k1, U);
+      break;
+    default:
+      set_smem((const void*)k_fft_cols_refpack<1>, sm);
+      OFC_LAUNCH(k_fft_cols_refpack<1>, div_up(pw, C), T, sm, st, Tin, plh, pw, g, k0, k1, U);
+  }
+}
+
+void launch_fft_rows_inv_ref_f32(const float2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,
                                  float4* ref4, float* amp, cudaStream_t st) {
   int T = fft_threads(plw.L, 1);
-  size_t sm = (size_t)4 * plw.L * sizeof(double2);
-  set_smem((const void*)k_fft_rows_inv_ref<double2>, sm);
+  size_t sm = 4 * fbytes(plw.L, 1);
+  set_smem((const void*)k_fft_rows_inv_ref, sm);
   dim3 grid(H, k1 - k0);
-  OFC_LAUNCH(k_fft_rows_inv_ref<double2>, grid, T, sm, st, U, plw, ph, W, H, k0, ref4, amp);
+  OFC_LAUNCH(k_fft_rows_inv_ref, grid, T, sm, st, U, plw, ph, W, H, k0, ref4, amp);
 }
 
 void launch_fft_lines(float2* data, int lines, const FftPlan& pl, bool inverse, cudaStream_t st) {
   int T = fft_threads(pl.L, 1);
-  size_t sm = (size_t)2 * pl.L * sizeof(float2);
+  size_t sm = 2 * fbytes(pl.L, 1);
   set_smem((const void*)k_fft_lines, sm);
   OFC_LAUNCH(k_fft_lines, lines, T, sm, st, data, pl, inverse ? 1 : 0);
 }

@@ -18,7 +18,6 @@ struct FftPlan {
   int s[FFT_MAXST] = {};
   unsigned magic[FFT_MAXST] = {};
   const float2* tw = nullptr;
-  const double2* twd = nullptr;  // the same table in float64
 };
 
 // radices with a register-resident butterfly; a length with any other prime factor is refused
@@ -28,7 +27,6 @@ bool fft_fits(int ph, int pw);
 // host: factor L and fill p/s; tw is set by the caller (device table of L values)
 FftPlan fft_make_plan(int L);
 std::vector<float2> fft_twiddles(int L);
-std::vector<double2> fft_twiddles_f64(int L);
 // threads of a block that transforms C interleaved lines of length L (multiple of C and of 32)
 int fft_threads(int L, int C);
 
@@ -48,24 +46,22 @@ std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c);
 // binds g to a device copy of the tables: d64 (the host float64 vector) and d32 (its float32 image)
 void gabor_bind(GaborTables& g, const double* d64, const float* d32, int ph, int pw, int F);
 
-// forward row transforms of the reflect-padded real image img (W x H) -> out (ph x pw), float32 or float64
+// forward row transforms of the reflect-padded real image img (W x H) -> out (ph x pw)
 void launch_fft_rows_fwd_real(const float* img, int W, int H, const FftPlan& plw, int ph, float2* out,
                               cudaStream_t st);
-void launch_fft_rows_fwd_real_f64(const float* img, int W, int H, const FftPlan& plw, int ph, double2* out,
-                                  cudaStream_t st);
-// column transforms of the responses: forward, then per filter multiply + inverse + B-spline prefilter along y
-// -> U: F planes (ph x pw)
-void launch_fft_cols_filters(const float2* T, const FftPlan& plh, int pw, const GaborTables& g, float2* U,
-                             cudaStream_t st);
-// column transforms of the reference pack in float64 for filters [k0, k1): 3 planes per filter
-// (S G, S G i fx, S G i fy), inverse along y
-void launch_fft_cols_ref_f64(const double2* T, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1,
-                             double2* U, cudaStream_t st);
+// column transforms of the responses: forward (in place in T, which then holds the 2-D spectrum), then per
+// filter multiply + inverse + B-spline prefilter along y -> U: F planes (ph x pw)
+void launch_fft_cols_filters(float2* T, const FftPlan& plh, int pw, const GaborTables& g, float2* U, cudaStream_t st);
 // inverse row transforms + B-spline prefilter along x + scale -> responses R (F planes of ph x pw)
 void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F, float2* R, cudaStream_t st);
-// inverse row transforms of the reference planes of filters [k0, k1), cropped to W x H: per filter
-// (r.re, r.im, gx, gy) and amp (reference_phase, phaseflow.py:100-111), formed in float64, stored float32
-void launch_fft_rows_inv_ref_f64(const double2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,
+
+// the reference pack (reference_phase, phaseflow.py:92-112): column transforms of filters [k0, k1), 3 planes per
+// filter (S G, S G i fx, S G i fy; the factors formed in float64), inverse along y; then the inverse row transforms
+// cropped to W x H with, per pixel, (r.re, r.im, gx, gy) and amp formed in float64 and stored float32. The
+// transforms are float32, as the reference's Rust port computes them (rustfft f32, gabor.rs:230-270).
+void launch_fft_cols_ref_f32(const float2* T, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1,
+                             float2* U, cudaStream_t st);
+void launch_fft_rows_inv_ref_f32(const float2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,
                                  float4* ref4, float* amp, cudaStream_t st);
 
 // generic complex FFT of C-line batches held in global memory (tests and tools): data (lines x L)

@@ -43,10 +43,14 @@ def test_reference_phase(T):
         assert np.abs(gx - g["gx"][k])[strong].max() < 1e-3
         assert np.abs(gy - g["gy"][k])[strong].max() < 1e-3
         assert np.abs(amp - g["amp"][k])[strong].max() < 1e-4 * max_amp
-    # the float64 transforms keep the gradient accurate near the zeros of a response too
+    # near the zeros of a response the gradient Im(conj r rx) / |r|^2 amplifies the float32 transforms' absolute
+    # error e max|r| (e ~ 1e-6; the reference's Rust port has the same float32 transforms) by max|r|^2 / amp^2:
+    # scaled by (amp / max)^2 the error stays below e times (the filter's frequency + 1) < 1e-5
     for k, (r, gx, gy, amp) in enumerate(ref):
-        weak = g["amp"][k] > 1e-4 * np.abs(g["r_re"][k] + 1j * g["r_im"][k]).max()
-        assert np.abs(gx - g["gx"][k])[weak].max() < 1e-2
+        max_amp = np.abs(g["r_re"][k] + 1j * g["r_im"][k]).max()
+        weak = g["amp"][k] > 1e-4 * max_amp
+        err = np.maximum(np.abs(gx - g["gx"][k]), np.abs(gy - g["gy"][k]))
+        assert (err * (g["amp"][k] / max_amp) ** 2)[weak].max() < 1e-5
 
 
 def _gabor_bank_np(shape, cfg):
