@@ -401,13 +401,19 @@ const double* gauss_taps(Lane& L, double sigma, int& r) {
   std::snprintf(key, sizeof key, "gauss:%.17g", sigma);
   return L.cached(key, k.data(), k.size());
 }
-const double* moment_taps(Lane& L, double sigma, int& r) {
+// the window taps k(t) t^p, p = 0..4, on the device (5 x (2r + 1)) and, for the default radius, as the kernel
+// parameter tp (t = 0..r)
+const double* moment_taps(Lane& L, double sigma, int& r, MomTaps& tp) {
   std::vector<double> kw = gauss_kernel(sigma);
   r = (int)kw.size() / 2;
   const int K = 2 * r + 1;
   std::vector<double> mt((size_t)5 * K);
   for (int p = 0; p < 5; p++)
     for (int t = -r; t <= r; t++) mt[(size_t)p * K + t + r] = kw[t + r] * std::pow((double)t, p);
+  tp = MomTaps{};
+  if (r == MOM_R)
+    for (int p = 0; p < 5; p++)
+      for (int t = 0; t <= r; t++) tp.k[p][t] = mt[(size_t)p * K + t + r];
   char key[64];
   std::snprintf(key, sizeof key, "moments:%.17g", sigma);
   return L.cached(key, mt.data(), mt.size());
@@ -448,7 +454,8 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
   // taps: smoothing Gaussian (sigma_s) and window moments k(t) t^p, p = 0..4 (sigma_w)
   int rs = 0, rw = 0;
   const double* d_ks = gauss_taps(L, c.sigma_s, rs);
-  const double* d_mt = moment_taps(L, c.sigma_w, rw);
+  MomTaps mtp;
+  const double* d_mt = moment_taps(L, c.sigma_w, rw, mtp);
 
   // reference pack (phaseflow.py:431, reference_phase)
   float2* T = L.get<float2>("fft_T", Np);
@@ -520,7 +527,7 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
     launch_bspline_f64(s2, cs2, tmpb, 2, W, H, st);
     for (int in = 0; in < c.inner_iters; in++) {
       launch_accumulate(ref4, amp, R, F, ph, pw, ucur, ucur + N, s2, s2 + N, cs2, cs2 + N, W, H, sums, st);
-      launch_moments_solve(sums, ucur, ucur + N, W, H, c.shape_order, d_mt, rw, yplanes, unext, unext + N, energy,
+      launch_moments_solve(sums, ucur, ucur + N, W, H, c.shape_order, d_mt, rw, mtp, yplanes, unext, unext + N, energy,
                            resid, slope, st);
       const bool last_inner = in == c.inner_iters - 1;
       launch_energy_stats(energy, N, stats, last_inner, st);
@@ -1281,12 +1288,9 @@ int ofc_test_local_solve(ofc_engine* e, const double* sums, const double* ux, co
     cfg_check(c);
     const int W = (int)w, H = (int)h;
     const size_t N = w * h;
-    std::vector<double> kw = gauss_kernel(c->sigma_w);
-    int rw = (int)kw.size() / 2, K = 2 * rw + 1;
-    std::vector<double> mt((size_t)5 * K);
-    for (int p = 0; p < 5; p++)
-      for (int t = -rw; t <= rw; t++) mt[(size_t)p * K + t + rw] = kw[t + rw] * std::pow((double)t, p);
-    double* d_mt = L.upload("taps_w", mt.data(), mt.size());
+    int rw = 0;
+    MomTaps mtp;
+    const double* d_mt = moment_taps(L, c->sigma_w, rw, mtp);
     double* ds = L.upload("sums", sums, 7 * N);
     double* u2 = L.get<double>("u2", 2 * N);
     OFC_CUDA(cudaMemcpyAsync(u2, ux, N * 8, cudaMemcpyHostToDevice, L.stream));
@@ -1299,7 +1303,7 @@ int ofc_test_local_solve(ofc_engine* e, const double* sums, const double* ux, co
     EnergyStats* stats = L.get<EnergyStats>("stats", 1);
     unsigned long long* hist = L.get<unsigned long long>("hist", 4096);
     OFC_CUDA(cudaMemsetAsync(hist, 0, 4096 * sizeof(unsigned long long), L.stream));
-    launch_moments_solve(ds, u2, u2 + N, W, H, c->shape_order, d_mt, rw, yp, o2, o2 + N, en, rs, sl, L.stream);
+    launch_moments_solve(ds, u2, u2 + N, W, H, c->shape_order, d_mt, rw, mtp, yp, o2, o2 + N, en, rs, sl, L.stream);
     launch_energy_stats(en, N, stats, false, L.stream);
     launch_median(en, N, stats, hist, L.stream);
     launch_reset(en, u2, u2 + N, (int)N, stats, o2, o2 + N, rs, sl, L.stream);

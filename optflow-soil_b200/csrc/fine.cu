@@ -362,6 +362,8 @@ __global__ void __launch_bounds__(128) k_moments_y(const double* __restrict__ su
   for (int j = 0; j < T.ny; j++) yplanes[j * N + p] = acc[j];
 }
 
+// Every inner loop below runs over a constant trip count with a guard (k < j rather than a bound of j): a bound
+// that depends on the outer index can leave the inner loop rolled, and the matrix then lives in local memory.
 template <int N>
 __device__ __forceinline__ bool cholesky_solve_dev(double (&M)[N * N], double (&b)[N]) {
   bool okp = true;
@@ -369,15 +371,18 @@ __device__ __forceinline__ bool cholesky_solve_dev(double (&M)[N * N], double (&
   for (int j = 0; j < N; j++) {
     double d = M[j * N + j];
 #pragma unroll
-    for (int k = 0; k < j; k++) d -= M[j * N + k] * M[j * N + k];
+    for (int k = 0; k < N; k++)
+      if (k < j) d -= M[j * N + k] * M[j * N + k];
     okp &= d > 0.0 && d <= DBL_MAX;  // a failed pivot goes on with meaningless values and reports false
     double l = sqrt(d);
     M[j * N + j] = l;
 #pragma unroll
-    for (int i = j + 1; i < N; i++) {
+    for (int i = 0; i < N; i++) {
+      if (i <= j) continue;
       double s = M[i * N + j];
 #pragma unroll
-      for (int k = 0; k < j; k++) s -= M[i * N + k] * M[j * N + k];
+      for (int k = 0; k < N; k++)
+        if (k < j) s -= M[i * N + k] * M[j * N + k];
       M[i * N + j] = s / l;
     }
   }
@@ -385,14 +390,16 @@ __device__ __forceinline__ bool cholesky_solve_dev(double (&M)[N * N], double (&
   for (int i = 0; i < N; i++) {
     double s = b[i];
 #pragma unroll
-    for (int k = 0; k < i; k++) s -= M[i * N + k] * b[k];
+    for (int k = 0; k < N; k++)
+      if (k < i) s -= M[i * N + k] * b[k];
     b[i] = s / M[i * N + i];
   }
 #pragma unroll
   for (int i = N - 1; i >= 0; i--) {
     double s = b[i];
 #pragma unroll
-    for (int k = i + 1; k < N; k++) s -= M[k * N + i] * b[k];
+    for (int k = 0; k < N; k++)
+      if (k > i) s -= M[k * N + i] * b[k];
     b[i] = s / M[i * N + i];
   }
   bool fin = okp;
@@ -471,9 +478,231 @@ __global__ void __launch_bounds__(128) k_moments_x_solve(const double* __restric
   }
 }
 
+// ---- register-blocked window moments for the default window (r = MOM_R = 16, 33 taps)
+// y pass: a thread owns RY consecutive rows of one column; it loads the RY + 2r rows of a source plane once
+// (instead of 2r + 1 loads per output row, most of them L2 traffic) and forms every y-plane of that source,
+// with the tap loop outermost so that the RY x (powers) accumulators advance side by side (independent
+// float64 chains: the pass is bound by float64 latency otherwise).
+constexpr int MOM_RY = 4;
+
+template <int ORDER>
+__global__ void __launch_bounds__(128, 4) k_moments_y_rb(const double* __restrict__ sums, int W, int H, MomTaps tp,
+                                                         double* __restrict__ yplanes) {
+  constexpr MomTable T = build_table(ORDER);
+  constexpr int R = MOM_R, RY = MOM_RY, NV = RY + 2 * R;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y0 = blockIdx.y * RY;
+  if (x >= W) return;
+  const size_t N = (size_t)W * H;
+#pragma unroll
+  for (int src = 0; src < 7; src++) {
+    bool used = false;
+    bool pw[5] = {false, false, false, false, false};
+#pragma unroll
+    for (int j = 0; j < T.ny; j++)
+      if (T.ysrc[j] == src) {
+        used = true;
+        pw[T.ypow[j]] = true;
+      }
+    if (!used) continue;
+    const double* plane = sums + (size_t)src * N + x;
+    double v[NV];
+#pragma unroll
+    for (int i = 0; i < NV; i++) v[i] = plane[(size_t)min(max(y0 - R + i, 0), H - 1) * W];
+    double acc[RY][5];
+#pragma unroll
+    for (int j = 0; j < RY; j++)
+#pragma unroll
+      for (int p = 0; p < 5; p++) acc[j][p] = p == 0 ? tp.k[0][0] * v[j + R] : 0.0;
+#pragma unroll
+    for (int t = 1; t <= R; t++)
+#pragma unroll
+      for (int j = 0; j < RY; j++) {
+        const double sp = v[j + R + t] + v[j + R - t], dm = v[j + R + t] - v[j + R - t];
+#pragma unroll
+        for (int p = 0; p < 5; p++)
+          if (pw[p]) acc[j][p] = fma(tp.k[p][t], (p & 1) ? dm : sp, acc[j][p]);
+      }
+#pragma unroll
+    for (int j = 0; j < RY; j++) {
+      if (y0 + j >= H) break;
+      const size_t o = (size_t)(y0 + j) * W + x;
+#pragma unroll
+      for (int q = 0; q < T.ny; q++)
+        if (T.ysrc[q] == src) yplanes[(size_t)q * N + o] = acc[j][T.ypow[q]];
+    }
+  }
+}
+
+// x pass + solve: a block of 128 threads owns a row segment of SEG = 128 RX pixels. For each y-plane it stages
+// the segment and its 2r halo in shared memory (double-buffered, the next plane's loads in flight meanwhile); a
+// thread takes the RX + 2r values around its RX consecutive pixels into registers (an odd RX keeps the warp's
+// reads on distinct banks) and writes their moments into a shared tile of nm x SEG (tap loop outermost, RX x
+// powers accumulators side by side); then each thread solves the pixels tid + 128 i from the tile.
+template <int ORDER>
+struct MomX {
+  static constexpr int RX = ORDER == 1 ? 3 : 1;
+  static constexpr int NT = 128, SEG = NT * RX, WIN = SEG + 2 * MOM_R;
+  static constexpr size_t smem() { return (size_t)(2 * WIN + build_table(ORDER).nm * SEG) * sizeof(double); }
+};
+
+// the NPF values of a row segment (with its halo) that thread tid stages: i = tid + NT j
+template <int ORDER>
+struct MomPf {
+  static constexpr int NPF = (MomX<ORDER>::WIN + MomX<ORDER>::NT - 1) / MomX<ORDER>::NT;
+  double v[NPF];
+};
+
+template <int ORDER>
+__device__ __forceinline__ void mom_x_fetch(const double* __restrict__ row, int x0, int W, MomPf<ORDER>& pf) {
+  constexpr int R = MOM_R, NT = MomX<ORDER>::NT, WIN = MomX<ORDER>::WIN;
+#pragma unroll
+  for (int j = 0; j < MomPf<ORDER>::NPF; j++) {
+    const int i = threadIdx.x + NT * j;
+    if (i < WIN) pf.v[j] = row[min(max(x0 - R + i, 0), W - 1)];
+  }
+}
+
+template <int ORDER>
+__device__ __forceinline__ void mom_x_stage(double* wb, const MomPf<ORDER>& pf) {
+  constexpr int NT = MomX<ORDER>::NT, WIN = MomX<ORDER>::WIN;
+#pragma unroll
+  for (int j = 0; j < MomPf<ORDER>::NPF; j++) {
+    const int i = threadIdx.x + NT * j;
+    if (i < WIN) wb[i] = pf.v[j];
+  }
+}
+
+// plane Q: its segment is in shared buffer Q & 1; while it is processed, the loads of plane Q + 1 are in flight
+// (registers pf), which are then staged into the other buffer. The barrier at the end orders both buffers.
+template <int ORDER, int Q>
+__device__ __forceinline__ void mom_x_planes(const double* __restrict__ yplanes, size_t N, int y, int x0, int W,
+                                             double* smd, double* mom, const MomTaps& tp, MomPf<ORDER>& pf) {
+  constexpr MomTable T = build_table(ORDER);
+  if constexpr (Q < T.ny) {
+    constexpr int R = MOM_R, RX = MomX<ORDER>::RX, SEG = MomX<ORDER>::SEG, WIN = MomX<ORDER>::WIN, NV = RX + 2 * R;
+    const int tid = threadIdx.x;
+    if constexpr (Q + 1 < T.ny) mom_x_fetch<ORDER>(yplanes + (size_t)(Q + 1) * N + (size_t)y * W, x0, W, pf);
+    const double* wb = smd + (Q & 1) * WIN;
+    double v[NV];
+#pragma unroll
+    for (int i = 0; i < NV; i++) v[i] = wb[tid * RX + i];
+    int mi[5] = {-1, -1, -1, -1, -1};  // moment index of (Q, px)
+#pragma unroll
+    for (int m = 0; m < T.nm; m++)
+      if (T.mjob[m] == Q) mi[T.mpx[m]] = m;
+    double acc[RX][5];
+#pragma unroll
+    for (int i = 0; i < RX; i++)
+#pragma unroll
+      for (int p = 0; p < 5; p++) acc[i][p] = p == 0 ? tp.k[0][0] * v[i + R] : 0.0;
+#pragma unroll
+    for (int t = 1; t <= R; t++)
+#pragma unroll
+      for (int i = 0; i < RX; i++) {
+        const double sp = v[i + R + t] + v[i + R - t], dm = v[i + R + t] - v[i + R - t];
+#pragma unroll
+        for (int p = 0; p < 5; p++)
+          if (mi[p] >= 0) acc[i][p] = fma(tp.k[p][t], (p & 1) ? dm : sp, acc[i][p]);
+      }
+#pragma unroll
+    for (int p = 0; p < 5; p++)
+      if (mi[p] >= 0)
+#pragma unroll
+        for (int i = 0; i < RX; i++) mom[mi[p] * SEG + tid * RX + i] = acc[i][p];
+    if constexpr (Q + 1 < T.ny) mom_x_stage<ORDER>(smd + ((Q + 1) & 1) * WIN, pf);
+    __syncthreads();
+    mom_x_planes<ORDER, Q + 1>(yplanes, N, y, x0, W, smd, mom, tp, pf);
+  }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128, 2) k_moments_x_solve_rb(const double* __restrict__ yplanes,
+                                                               const double* __restrict__ uxin,
+                                                               const double* __restrict__ uyin, int W, int H,
+                                                               MomTaps tp, double* __restrict__ oux,
+                                                               double* __restrict__ ouy, double* __restrict__ energy,
+                                                               double* __restrict__ resid, double* __restrict__ slope) {
+  constexpr MomTable T = build_table(ORDER);
+  constexpr int n = ORDER == 1 ? 6 : 12;
+  constexpr int RX = MomX<ORDER>::RX, NT = MomX<ORDER>::NT, SEG = MomX<ORDER>::SEG, WIN = MomX<ORDER>::WIN;
+  extern __shared__ double smd[];
+  double* mom = smd + 2 * WIN;
+  const int tid = threadIdx.x, y = blockIdx.y, x0 = blockIdx.x * SEG;
+  const size_t N = (size_t)W * H;
+  MomPf<ORDER> pf;
+  mom_x_fetch<ORDER>(yplanes + (size_t)y * W, x0, W, pf);
+  mom_x_stage<ORDER>(smd, pf);
+  __syncthreads();
+  mom_x_planes<ORDER, 0>(yplanes, N, y, x0, W, smd, mom, tp, pf);
+#pragma unroll 1
+  for (int i = 0; i < RX; i++) {
+    const int s = tid + NT * i, x = x0 + s;
+    if (x >= W) continue;
+    double m[T.nm];
+#pragma unroll
+    for (int k = 0; k < T.nm; k++) m[k] = mom[k * SEG + s];
+    const size_t p = (size_t)y * W + x;
+    double M[n * n], b[n], b0[n];
+#pragma unroll
+    for (int k = 0; k < n * n; k++) M[k] = m[T.Midx[k]];
+#pragma unroll
+    for (int k = 0; k < n; k++) b0[k] = b[k] = m[T.bidx[k]];
+    const double m00 = M[0], m11 = M[n + 1], m01 = M[1];
+    const double e = m00 + m11;
+    const double det2 = m00 * m11 - m01 * m01;
+    energy[p] = e;
+    bool ok = det2 > APERTURE_TOL * e * e;
+    if (ok) {
+      double tr = 0;
+#pragma unroll
+      for (int k = 0; k < n; k++) tr += M[k * n + k];
+      double ridge = 1e-12 * tr / n;
+#pragma unroll
+      for (int k = 0; k < n; k++) M[k * n + k] += ridge;
+      ok = cholesky_solve_dev<n>(M, b);
+    }
+    if (ok) {
+      double fit = 0;
+#pragma unroll
+      for (int k = 0; k < n; k++) fit += b[k] * b0[k];
+      double rr = m[T.gcc] - fit;
+      resid[p] = sqrt(fmax(rr, 0.0) / (m[T.gw] + 1e-30));
+      oux[p] = b[0];
+      ouy[p] = b[1];
+#pragma unroll
+      for (int k = 0; k < 4; k++) slope[k * N + p] = b[2 + k];
+    } else {
+      resid[p] = PI;
+      oux[p] = uxin[p];
+      ouy[p] = uyin[p];
+#pragma unroll
+      for (int k = 0; k < 4; k++) slope[k * N + p] = 0.0;
+    }
+  }
+}
+
+template <int ORDER>
+static void launch_moments_rb(const double* sums, const double* ux, const double* uy, int W, int H, const MomTaps& tp,
+                              double* yplanes, double* oux, double* ouy, double* energy, double* resid, double* slope,
+                              cudaStream_t st) {
+  dim3 gy(div_up(W, 128), div_up(H, MOM_RY));
+  OFC_LAUNCH(k_moments_y_rb<ORDER>, gy, 128, 0, st, sums, W, H, tp, yplanes);
+  const size_t sm = MomX<ORDER>::smem();
+  OFC_CUDA(cudaFuncSetAttribute((const void*)k_moments_x_solve_rb<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sm));
+  dim3 gx(div_up(W, MomX<ORDER>::SEG), H);
+  OFC_LAUNCH(k_moments_x_solve_rb<ORDER>, gx, 128, sm, st, yplanes, ux, uy, W, H, tp, oux, ouy, energy, resid, slope);
+}
+
 void launch_moments_solve(const double* sums, const double* ux, const double* uy, int W, int H, int order,
-                          const double* mtaps, int r, double* yplanes, double* oux, double* ouy, double* energy,
-                          double* resid, double* slope, cudaStream_t st) {
+                          const double* mtaps, int r, const MomTaps& tp, double* yplanes, double* oux, double* ouy,
+                          double* energy, double* resid, double* slope, cudaStream_t st) {
+  if (r == MOM_R) {
+    if (order == 1) launch_moments_rb<1>(sums, ux, uy, W, H, tp, yplanes, oux, ouy, energy, resid, slope, st);
+    else launch_moments_rb<2>(sums, ux, uy, W, H, tp, yplanes, oux, ouy, energy, resid, slope, st);
+    return;
+  }
   dim3 g(div_up(W, 128), H);
   if (order == 1) {
     OFC_LAUNCH(k_moments_y<1>, g, 128, 0, st, sums, W, H, mtaps, r, yplanes);

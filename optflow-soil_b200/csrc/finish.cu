@@ -225,15 +225,18 @@ __global__ void k_strain_x(const double* __restrict__ yp, int W, int H, int h, i
     for (int j = 0; j < 6; j++) {
       double d = L[j * 6 + j];
 #pragma unroll
-      for (int k = 0; k < j; k++) d -= L[j * 6 + k] * L[j * 6 + k];
+      for (int k = 0; k < 6; k++)  // constant trip counts with guards keep L in registers
+        if (k < j) d -= L[j * 6 + k] * L[j * 6 + k];
       if (!(d > 0.0 && d <= DBL_MAX)) ok = false;
       double l = sqrt(d);
       L[j * 6 + j] = l;
 #pragma unroll
-      for (int i = j + 1; i < 6; i++) {
+      for (int i = 0; i < 6; i++) {
+        if (i <= j) continue;
         double s = L[i * 6 + j];
 #pragma unroll
-        for (int k = 0; k < j; k++) s -= L[i * 6 + k] * L[j * 6 + k];
+        for (int k = 0; k < 6; k++)
+          if (k < j) s -= L[i * 6 + k] * L[j * 6 + k];
         L[i * 6 + j] = s / l;
       }
     }
@@ -242,7 +245,8 @@ __global__ void k_strain_x(const double* __restrict__ yp, int W, int H, int h, i
       for (int i = 0; i < 6; i++) {
         double su = bu[i], sv = bv[i];
 #pragma unroll
-        for (int k = 0; k < i; k++) { su -= L[i * 6 + k] * bu[k]; sv -= L[i * 6 + k] * bv[k]; }
+        for (int k = 0; k < 6; k++)
+          if (k < i) { su -= L[i * 6 + k] * bu[k]; sv -= L[i * 6 + k] * bv[k]; }
         bu[i] = su / L[i * 6 + i];
         bv[i] = sv / L[i * 6 + i];
       }
@@ -250,7 +254,8 @@ __global__ void k_strain_x(const double* __restrict__ yp, int W, int H, int h, i
       for (int i = 5; i >= 0; i--) {
         double su = bu[i], sv = bv[i];
 #pragma unroll
-        for (int k = i + 1; k < 6; k++) { su -= L[k * 6 + i] * bu[k]; sv -= L[k * 6 + i] * bv[k]; }
+        for (int k = 0; k < 6; k++)
+          if (k > i) { su -= L[k * 6 + i] * bu[k]; sv -= L[k * 6 + i] * bv[k]; }
         bu[i] = su / L[i * 6 + i];
         bv[i] = sv / L[i * 6 + i];
       }

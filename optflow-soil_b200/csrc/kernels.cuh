@@ -28,11 +28,16 @@ void launch_accumulate(const float4* ref4, const float* amp, const float2* R, in
                        const double* csy, int W, int H, double* sums, cudaStream_t st);
 
 // Gaussian window moments + the per-pixel shape-function solve (phaseflow.py:114-161): mtaps: the
-// window taps k(t) t^p for p = 0..4 (5 x (2r+1) doubles); yplanes: scratch of ny planes
+// window taps k(t) t^p for p = 0..4 (5 x (2r+1) doubles, device); tp: the same taps for t = 0..r as a kernel
+// parameter (used by the register-blocked kernels of the default window, r = MOM_R); yplanes: scratch of ny planes
+constexpr int MOM_R = 16;
+struct MomTaps {
+  double k[5][MOM_R + 1];  // k[p][t] = k(t) t^p
+};
 int moment_yplanes(int order);
 void launch_moments_solve(const double* sums, const double* ux, const double* uy, int W, int H, int order,
-                          const double* mtaps, int r, double* yplanes, double* oux, double* ouy, double* energy,
-                          double* resid, double* slope, cudaStream_t st);
+                          const double* mtaps, int r, const MomTaps& tp, double* yplanes, double* oux, double* ouy,
+                          double* energy, double* resid, double* slope, cudaStream_t st);
 
 // min / max / NaN of the energy and whether its median is needed (stats: device struct, see fine.cu)
 struct EnergyStats {
