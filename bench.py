@@ -108,12 +108,12 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-# algorithmic bytes of one k_accumulate launch: per pixel the reference pack (float4 + amp per filter), the
-# field (ux, uy, sx, sy: float64), its spline (csx, csy), the seven sums written (float64); per padded pixel the
+# algorithmic bytes of one k_accumulate launch: per pixel the reference pack (float4 per filter), the field
+# (ux, uy, sx, sy: float64), its spline (csx, csy), the seven sums written (float64); per padded pixel the
 # twelve response planes (complex float32), each read once
 def accumulate_bytes(W, H, F=12):
     N, Np = W * H, (W + 64) * (H + 64)
-    return N * (20 * F + 32 + 16 + 56) + Np * 8 * F
+    return N * (16 * F + 32 + 16 + 56) + Np * 8 * F
 
 
 # DRAM traffic of one k_accumulate launch over its algorithmic bytes, from one ncu capture

@@ -76,18 +76,27 @@ struct Taps {
   double wx[4], wy[4];
 };
 
+// mirror_idx for an index at most one reflection outside [0, n) (the taps of a clamped position lie in
+// [-1, n + 1]): two compares instead of a division; the general rule where one reflection is not enough (n < 3)
+__device__ __forceinline__ int mirror_near(int i, int n) {
+  int m = i < 0 ? -i : i;
+  if (m >= n) m = 2 * (n - 1) - m;
+  if (m < 0 || m >= n) m = (int)mirror_idx(i, n);
+  return m;
+}
+
 __device__ inline bool make_taps(double x, double y, int w, int h, Taps& t) {
   if (!(x == x) || !(y == y)) return false;
   x = fmin(fmax(x, 0.0), (double)(w - 1));
   y = fmin(fmax(y, 0.0), (double)(h - 1));
   double fx = floor(x), fy = floor(y);
-  long x0 = (long)fx, y0 = (long)fy;
+  int x0 = (int)fx, y0 = (int)fy;
   bspline_weights(x - fx, t.wx);
   bspline_weights(y - fy, t.wy);
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    t.xi[k] = (int)mirror_idx(x0 + k - 1, w);
-    t.yi[k] = (int)mirror_idx(y0 + k - 1, h);
+    t.xi[k] = mirror_near(x0 + k - 1, w);
+    t.yi[k] = mirror_near(y0 + k - 1, h);
   }
   return true;
 }
@@ -104,6 +113,30 @@ __device__ inline double sample_real(const T* c, int w, const Taps& t) {
     out += t.wy[j] * acc;
   }
   return out;
+}
+
+// two real splines sampled at the same taps (one set of 32-bit offsets for both)
+template <class T>
+__device__ __forceinline__ void sample2_real(const T* __restrict__ c1, const T* __restrict__ c2, int w, const Taps& t,
+                                             double& o1, double& o2) {
+  int o[16];
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int k = 0; k < 4; k++) o[j * 4 + k] = t.yi[j] * w + t.xi[k];
+  o1 = 0;
+  o2 = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    double a1 = t.wx[0] * (double)c1[o[j * 4]], a2 = t.wx[0] * (double)c2[o[j * 4]];
+#pragma unroll
+    for (int k = 1; k < 4; k++) {
+      a1 += t.wx[k] * (double)c1[o[j * 4 + k]];
+      a2 += t.wx[k] * (double)c2[o[j * 4 + k]];
+    }
+    o1 += t.wy[j] * a1;
+    o2 += t.wy[j] * a2;
+  }
 }
 
 // complex spline stored as float2; float accumulation of the 16 taps with f64-derived weights

@@ -5,6 +5,8 @@
 
 #include "kernels.cuh"
 
+#include <cuda_pipeline.h>
+
 namespace ofc {
 
 // ---------------------------------------------------------------- separable correlation ("nearest")
@@ -168,22 +170,27 @@ void launch_warp(const float* c2, int w2, int h2, const double* sx, const double
 }
 
 // ---------------------------------------------------------------- accumulate
-// One pixel per thread. The fixed point X' + s(X') = X + u(X) and the positions are float64; the twelve
-// responses are sampled with float32 weights and accumulation (they are stored as complex float32), and
-// the phase difference angle(r1 conj(r2)) is taken in float32 (the inputs carry float32 precision, the angle
-// is then exact to ~1e-7 rad); c = dphi + gx u + gy v and the seven sums are float64, since u reaches tens of
-// pixels and the residual sum gcc - theta . b cancels.
-__global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict__ ref4, const float* __restrict__ amp,
-                                                      const float2* __restrict__ R, int F, int ph, int pw,
-                                                      const double* __restrict__ ux, const double* __restrict__ uy,
-                                                      const double* __restrict__ sx, const double* __restrict__ sy,
-                                                      const double* __restrict__ csx, const double* __restrict__ csy,
-                                                      int W, int H, double* __restrict__ sums) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y;
+// One pixel per thread. The fixed point X' + s(X') = X + u(X) and the positions are float64; the responses are
+// sampled with float32 weights and accumulation (they are stored as complex float32), and the phase difference
+// angle(r1 conj(r2)) is taken in float32 (the inputs carry float32 precision, the angle is then exact to ~1e-7
+// rad); c = dphi + gx u + gy v and the seven sums are float64, since u reaches tens of pixels and the residual
+// sum gcc - theta . b cancels. The kernel is latency-bound, so: the F reference-pack values of the pixel are
+// copied to shared memory asynchronously at the start (in flight during the fixed point); |r1| is formed from
+// the pack instead of a second load; the 16 tap offsets are computed once and reused by every filter.
+__global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict__ ref4, const float2* __restrict__ R,
+                                                      int F, int ph, int pw, const double* __restrict__ ux,
+                                                      const double* __restrict__ uy, const double* __restrict__ sx,
+                                                      const double* __restrict__ sy, const double* __restrict__ csx,
+                                                      const double* __restrict__ csy, int W, int H,
+                                                      double* __restrict__ sums) {
+  extern __shared__ float4 pk[];  // F x 128
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
   if (x >= W) return;
   const size_t N = (size_t)W * H;
   const size_t p = (size_t)y * W + x;
+  for (int k = 0; k < F; k++) __pipeline_memcpy_async(&pk[k * 128 + threadIdx.x], ref4 + (size_t)k * N + p, 16);
+  __pipeline_commit();
   const double u = ux[p], v = uy[p];
   const double tx = x + u, ty = y + v;
   double px = tx - sx[p], py = ty - sy[p];
@@ -192,8 +199,10 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
     Taps t;
     double nx, ny;
     if (make_taps(px, py, W, H, t)) {
-      nx = tx - sample_real(csx, W, t);
-      ny = ty - sample_real(csy, W, t);
+      double s1, s2;
+      sample2_real(csx, csy, W, t, s1, s2);
+      nx = tx - s1;
+      ny = ty - s2;
     } else {
       nx = ny = nan("");
     }
@@ -204,18 +213,23 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
   Taps t;
   const bool ok = make_taps(px + PAD, py + PAD, pw, ph, t);
   float fwx[4], fwy[4];
-  int off[4];
+  int o16[16];
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     fwx[k] = (float)t.wx[k];
     fwy[k] = (float)t.wy[k];
-    off[k] = t.yi[k] * pw;
   }
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) o16[j * 4 + q] = t.yi[j] * pw + t.xi[q];
   const size_t plane = (size_t)ph * pw;
   const float fnan = __int_as_float(0x7fc00000);
+  __pipeline_wait_prior(0);
   for (int k = 0; k < F; k++) {
-    const float4 r1 = __ldg(ref4 + (size_t)k * N + p);
-    const float a1k = __ldg(amp + (size_t)k * N + p);
+    const float4 r1 = pk[k * 128 + threadIdx.x];
+    // |r1| as the reference pack's amplitude (phaseflow.py:111), from the stored float32 response
+    const float a1k = sqrtf(fmaf(r1.x, r1.x, fmaf(r1.y, r1.y, 1e-12f)));
     float br = fnan, bi = fnan;
     if (ok) {
       const float2* Rk = R + (size_t)k * plane;
@@ -223,11 +237,10 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
       bi = 0.f;
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        const float2* row = Rk + off[j];
         float are = 0.f, aim = 0.f;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          float2 c = __ldg(row + t.xi[q]);
+          const float2 c = __ldg(Rk + o16[j * 4 + q]);
           are = fmaf(fwx[q], c.x, are);
           aim = fmaf(fwx[q], c.y, aim);
         }
@@ -260,11 +273,14 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
   sums[6 * N + p] = a6;
 }
 
-void launch_accumulate(const float4* ref4, const float* amp, const float2* R, int F, int ph, int pw, const double* ux,
-                       const double* uy, const double* sx, const double* sy, const double* csx, const double* csy,
-                       int W, int H, double* sums, cudaStream_t st) {
+void launch_accumulate(const float4* ref4, const float2* R, int F, int ph, int pw, const double* ux, const double* uy,
+                       const double* sx, const double* sy, const double* csx, const double* csy, int W, int H,
+                       double* sums, cudaStream_t st) {
   dim3 g(div_up(W, 128), H);
-  OFC_LAUNCH(k_accumulate, g, 128, 0, st, ref4, amp, R, F, ph, pw, ux, uy, sx, sy, csx, csy, W, H, sums);
+  const size_t sm = (size_t)F * 128 * sizeof(float4);
+  if (sm > 227 * 1024) throw Error(OFC_ERR_WINDOW, "too many Gabor filters (" + std::to_string(F) + ") for the CUDA engine");
+  OFC_CUDA(cudaFuncSetAttribute((const void*)k_accumulate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  OFC_LAUNCH(k_accumulate, g, 128, sm, st, ref4, R, F, ph, pw, ux, uy, sx, sy, csx, csy, W, H, sums);
 }
 
 // ---------------------------------------------------------------- window moments + solve

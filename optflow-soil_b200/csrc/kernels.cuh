@@ -21,11 +21,11 @@ void launch_bspline_f32(const float* in, float* out, double* tmp, int W, int H, 
 void launch_warp(const float* c2, int w2, int h2, const double* sx, const double* sy, long shx, long shy, int W, int H,
                  float* out, cudaStream_t st);
 
-// the seven per-pixel sums of an inner iteration (phaseflow.py:468-483); ref4/amp: F planes W x H;
-// R: F response planes (ph x pw); sums: 7 planes W x H
-void launch_accumulate(const float4* ref4, const float* amp, const float2* R, int F, int ph, int pw,
-                       const double* ux, const double* uy, const double* sx, const double* sy, const double* csx,
-                       const double* csy, int W, int H, double* sums, cudaStream_t st);
+// the seven per-pixel sums of an inner iteration (phaseflow.py:468-483); ref4: F planes W x H of the reference
+// pack (r.re, r.im, gx, gy); R: F response planes (ph x pw); sums: 7 planes W x H
+void launch_accumulate(const float4* ref4, const float2* R, int F, int ph, int pw, const double* ux, const double* uy,
+                       const double* sx, const double* sy, const double* csx, const double* csy, int W, int H,
+                       double* sums, cudaStream_t st);
 
 // Gaussian window moments + the per-pixel shape-function solve (phaseflow.py:114-161): mtaps: the
 // window taps k(t) t^p for p = 0..4 (5 x (2r+1) doubles, device); tp: the same taps for t = 0..r as a kernel
