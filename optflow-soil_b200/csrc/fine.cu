@@ -380,9 +380,11 @@ __global__ void __launch_bounds__(128) k_moments_y(const double* __restrict__ su
 
 // Every inner loop below runs over a constant trip count with a guard (k < j rather than a bound of j): a bound
 // that depends on the outer index can leave the inner loop rolled, and the matrix then lives in local memory.
+// One division per pivot: the factor's column and both substitutions multiply by the pivot's reciprocal.
 template <int N>
 __device__ __forceinline__ bool cholesky_solve_dev(double (&M)[N * N], double (&b)[N]) {
   bool okp = true;
+  double il[N];
 #pragma unroll
   for (int j = 0; j < N; j++) {
     double d = M[j * N + j];
@@ -390,7 +392,8 @@ __device__ __forceinline__ bool cholesky_solve_dev(double (&M)[N * N], double (&
     for (int k = 0; k < N; k++)
       if (k < j) d -= M[j * N + k] * M[j * N + k];
     okp &= d > 0.0 && d <= DBL_MAX;  // a failed pivot goes on with meaningless values and reports false
-    double l = sqrt(d);
+    const double l = sqrt(d);
+    il[j] = 1.0 / l;
     M[j * N + j] = l;
 #pragma unroll
     for (int i = 0; i < N; i++) {
@@ -399,7 +402,7 @@ __device__ __forceinline__ bool cholesky_solve_dev(double (&M)[N * N], double (&
 #pragma unroll
       for (int k = 0; k < N; k++)
         if (k < j) s -= M[i * N + k] * M[j * N + k];
-      M[i * N + j] = s / l;
+      M[i * N + j] = s * il[j];
     }
   }
 #pragma unroll
@@ -408,7 +411,7 @@ __device__ __forceinline__ bool cholesky_solve_dev(double (&M)[N * N], double (&
 #pragma unroll
     for (int k = 0; k < N; k++)
       if (k < i) s -= M[i * N + k] * b[k];
-    b[i] = s / M[i * N + i];
+    b[i] = s * il[i];
   }
 #pragma unroll
   for (int i = N - 1; i >= 0; i--) {
@@ -416,7 +419,7 @@ __device__ __forceinline__ bool cholesky_solve_dev(double (&M)[N * N], double (&
 #pragma unroll
     for (int k = 0; k < N; k++)
       if (k > i) s -= M[k * N + i] * b[k];
-    b[i] = s / M[i * N + i];
+    b[i] = s * il[i];
   }
   bool fin = okp;
 #pragma unroll
@@ -833,29 +836,50 @@ __global__ void k_radix_hist(const double* __restrict__ e, size_t n, const Energ
     if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
 }
 
-__global__ void k_radix_pick(EnergyStats* s, int pass, unsigned long long* hist, size_t n) {
-  // one block of 1024 threads: find the bin holding rank, then clear the histogram
+__global__ void __launch_bounds__(1024) k_radix_pick(EnergyStats* s, int pass, unsigned long long* hist, size_t n) {
+  // one block of 1024 threads: a block scan of the bin counts (4 bins per thread); the thread whose range
+  // holds rank finds the bin; then the histogram is cleared for the next pass
   if (!s->need_median || s->nan) return;
-  __shared__ unsigned long long part[1024];
-  const int per = RBINS / 1024;
-  unsigned long long loc = 0;
-  for (int j = 0; j < per; j++) loc += hist[threadIdx.x * per + j];
-  part[threadIdx.x] = loc;
+  __shared__ long long wsum[32];
+  constexpr int per = RBINS / 1024;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  long long c[per];
+  long long loc = 0;
+#pragma unroll
+  for (int j = 0; j < per; j++) {
+    c[j] = (long long)hist[tid * per + j];
+    loc += c[j];
+  }
+  long long inc = loc;  // inclusive scan within the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    long long v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
+  }
+  if (lane == 31) wsum[wid] = inc;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    long long rank = s->rank;
-    long long acc = 0;
-    int bin = -1;
-    for (int t = 0; t < 1024 && bin < 0; t++) {
-      if (acc + (long long)part[t] > rank) {
-        for (int j = 0; j < per; j++) {
-          long long c = (long long)hist[t * per + j];
-          if (acc + c > rank) { bin = t * per + j; break; }
-          acc += c;
-        }
-      } else {
-        acc += (long long)part[t];
+  if (wid == 0) {
+    long long w = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      long long v = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += v;
+    }
+    wsum[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  const long long excl = inc - loc + (wid ? wsum[wid - 1] : 0);
+  const long long rank = s->rank;
+  if (excl <= rank && rank < excl + loc) {  // exactly one thread
+    long long acc = excl;
+    int bin = tid * per;
+#pragma unroll
+    for (int j = 0; j < per; j++) {
+      if (acc + c[j] > rank) {
+        bin = tid * per + j;
+        break;
       }
+      acc += c[j];
     }
     int shift, bits;
     digit_of(pass, shift, bits);
@@ -863,8 +887,8 @@ __global__ void k_radix_pick(EnergyStats* s, int pass, unsigned long long* hist,
     s->rank = rank - acc;
     s->less += acc;
   }
-  __syncthreads();
-  for (int j = 0; j < per; j++) hist[threadIdx.x * per + j] = 0;
+#pragma unroll
+  for (int j = 0; j < per; j++) hist[tid * per + j] = 0;
 }
 
 // after the passes: prefix = key of the element of rank n/2; for even n the one of rank n/2 - 1 is

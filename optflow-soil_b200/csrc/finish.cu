@@ -211,7 +211,7 @@ __global__ void k_strain_x(const double* __restrict__ yp, int W, int H, int h, i
   const double nanv = nan("");
   r[0] = r[1] = r[2] = r[3] = nanv;
   if (mm[0][0] >= 0.5 * win * win) {
-    double L[36], bu[6], bv[6];
+    double L[36], bu[6], bv[6], il[6];
     bool ok = true;
 #pragma unroll
     for (int i = 0; i < 6; i++) {
@@ -229,6 +229,7 @@ __global__ void k_strain_x(const double* __restrict__ yp, int W, int H, int h, i
         if (k < j) d -= L[j * 6 + k] * L[j * 6 + k];
       if (!(d > 0.0 && d <= DBL_MAX)) ok = false;
       double l = sqrt(d);
+      il[j] = 1.0 / l;  // one division per pivot; the rest multiply by it
       L[j * 6 + j] = l;
 #pragma unroll
       for (int i = 0; i < 6; i++) {
@@ -237,7 +238,7 @@ __global__ void k_strain_x(const double* __restrict__ yp, int W, int H, int h, i
 #pragma unroll
         for (int k = 0; k < 6; k++)
           if (k < j) s -= L[i * 6 + k] * L[j * 6 + k];
-        L[i * 6 + j] = s / l;
+        L[i * 6 + j] = s * il[j];
       }
     }
     if (ok) {
@@ -247,8 +248,8 @@ __global__ void k_strain_x(const double* __restrict__ yp, int W, int H, int h, i
 #pragma unroll
         for (int k = 0; k < 6; k++)
           if (k < i) { su -= L[i * 6 + k] * bu[k]; sv -= L[i * 6 + k] * bv[k]; }
-        bu[i] = su / L[i * 6 + i];
-        bv[i] = sv / L[i * 6 + i];
+        bu[i] = su * il[i];
+        bv[i] = sv * il[i];
       }
 #pragma unroll
       for (int i = 5; i >= 0; i--) {
@@ -256,8 +257,8 @@ __global__ void k_strain_x(const double* __restrict__ yp, int W, int H, int h, i
 #pragma unroll
         for (int k = 0; k < 6; k++)
           if (k > i) { su -= L[k * 6 + i] * bu[k]; sv -= L[k * 6 + i] * bv[k]; }
-        bu[i] = su / L[i * 6 + i];
-        bv[i] = sv / L[i * 6 + i];
+        bu[i] = su * il[i];
+        bv[i] = sv * il[i];
       }
       bool fin = true;
 #pragma unroll

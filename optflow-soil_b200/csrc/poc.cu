@@ -121,7 +121,8 @@ struct PocConst {
 __device__ __forceinline__ int lines_per_warp(int n) { return n == 16 ? 2 : 1; }
 
 // Row transforms of a real window (values win(y, x), window mean removed, Hann weighted) into Z (natural
-// order, Z[y * wx + kx]).
+// order, Z[y * (wx + 1) + kx]: rows padded by one entry, so that a warp reading a column, one row per lane,
+// spreads over the banks instead of hitting one).
 template <class Get>
 __device__ void rows_forward(Get get, double mean, int wy, int wx, const PocConst& pc, double2* Z) {
   const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -136,8 +137,8 @@ __device__ void rows_forward(Get get, double mean, int wy, int wx, const PocCons
     }
     warp_dif(v0, v1, wx, false, pc.tw64);
     if (y < wy) {
-      Z[y * wx + brev(pos_of(0, wx), bits)] = v0;
-      if (wx == 64) Z[y * wx + brev(pos_of(1, wx), bits)] = v1;
+      Z[y * (wx + 1) + brev(pos_of(0, wx), bits)] = v0;
+      if (wx == 64) Z[y * (wx + 1) + brev(pos_of(1, wx), bits)] = v1;
     }
   }
 }
@@ -165,8 +166,8 @@ __device__ void poc_shift_dev(const double* __restrict__ b, int W, int x0, int y
       int kx = ci <= qx ? ci : ci + (wx - 2 * qx - 1);
       double2 v0 = make_double2(0, 0), v1 = make_double2(0, 0);
       if (live) {
-        v0 = Z[pos_of(0, wy) * wx + kx];
-        if (wy == 64) v1 = Z[pos_of(1, wy) * wx + kx];
+        v0 = Z[pos_of(0, wy) * (wx + 1) + kx];
+        if (wy == 64) v1 = Z[pos_of(1, wy) * (wx + 1) + kx];
       }
       warp_dif(v0, v1, wy, false, pc.tw64);
       for (int r = 0; r < (wy == 64 ? 2 : 1); r++) {
@@ -185,8 +186,8 @@ __device__ void poc_shift_dev(const double* __restrict__ b, int W, int x0, int y
       }
       warp_dit(v0, v1, wy, true, pc.tw64);
       if (live) {
-        Z[pos_of(0, wy) * wx + kx] = v0;
-        if (wy == 64) Z[pos_of(1, wy) * wx + kx] = v1;
+        Z[pos_of(0, wy) * (wx + 1) + kx] = v0;
+        if (wy == 64) Z[pos_of(1, wy) * (wx + 1) + kx] = v1;
       }
     }
   }
@@ -206,15 +207,15 @@ __device__ void poc_shift_dev(const double* __restrict__ b, int W, int x0, int y
       double2 v0 = make_double2(0, 0), v1 = make_double2(0, 0);
       int x0i = pos_of(0, wx), x1i = x0i + 32;
       auto lp = [&](int x) { return x <= qx || x >= wx - qx; };
-      if (live && lp(x0i)) v0 = Z[y * wx + x0i];
-      if (live && wx == 64 && lp(x1i)) v1 = Z[y * wx + x1i];
+      if (live && lp(x0i)) v0 = Z[y * (wx + 1) + x0i];
+      if (live && wx == 64 && lp(x1i)) v1 = Z[y * (wx + 1) + x1i];
       __syncwarp();
       warp_dif(v0, v1, wx, true, pc.tw64);
       for (int r = 0; r < (wx == 64 ? 2 : 1); r++) {
         double v = (r == 0 ? v0.x : v1.x) * sc;
         int x = brev(pos_of(r, wx), bits);
         if (live) {
-          surf[y * 2 * wx + x] = v;
+          surf[y * 2 * (wx + 1) + x] = v;
           int sy = (y + wy / 2) % wy, sxx = (x + wx / 2) % wx;
           int idx = sy * wx + sxx;
           bool vn = v != v;
@@ -247,7 +248,7 @@ __device__ void poc_shift_dev(const double* __restrict__ b, int W, int x0, int y
     ix = min(max(ix, 1), wx - 2);
     auto R = [&](int ys, int xs) {  // the shifted surface at (ys, xs)
       int y = (ys - wy / 2 + wy) % wy, x = (xs - wx / 2 + wx) % wx;
-      return surf[y * 2 * wx + x];
+      return surf[y * 2 * (wx + 1) + x];
     };
     auto parabola = [](double m, double c, double p) {  // poc.py:34-36
       double den = m - 2.0 * c + p;
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(POC_T, 2) k_poc_grid(const double* __restrict_
   double2* Z = dsm;
   const int qy = wy / 4, qx = wx / 4;
   const int nlx = 2 * qx + 1;
-  double2* alp = Z + wy * wx;
+  double2* alp = Z + wy * (wx + 1);
   __shared__ PocConst pc;
   __shared__ double red[POC_T / 32];
   __shared__ double res[3];
@@ -300,8 +301,8 @@ __global__ void __launch_bounds__(POC_T, 2) k_poc_grid(const double* __restrict_
       int kx = ci <= qx ? ci : ci + (wx - 2 * qx - 1);
       double2 v0 = make_double2(0, 0), v1 = make_double2(0, 0);
       if (live) {
-        v0 = Z[pos_of(0, wy) * wx + kx];
-        if (wy == 64) v1 = Z[pos_of(1, wy) * wx + kx];
+        v0 = Z[pos_of(0, wy) * (wx + 1) + kx];
+        if (wy == 64) v1 = Z[pos_of(1, wy) * (wx + 1) + kx];
       }
       warp_dif(v0, v1, wy, false, pc.tw64);
       for (int r = 0; r < (wy == 64 ? 2 : 1); r++) {
@@ -357,7 +358,7 @@ void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const
     throw Error(OFC_ERR_ARG, "the CUDA engine's POC windows are 16, 32 or 64 px a side (poc_win <= 64)");
   // lp.mean(): the share of frequencies with |f| <= 0.25 on both axes
   double lpm = (double)(2 * (lv.wy / 4) + 1) * (double)(2 * (lv.wx / 4) + 1) / ((double)lv.wy * lv.wx);
-  size_t smem = (size_t)(lv.wy * lv.wx + (2 * (lv.wy / 4) + 1) * (2 * (lv.wx / 4) + 1)) * sizeof(double2);
+  size_t smem = (size_t)(lv.wy * (lv.wx + 1) + (2 * (lv.wy / 4) + 1) * (2 * (lv.wx / 4) + 1)) * sizeof(double2);
   OFC_CUDA(cudaFuncSetAttribute((const void*)k_poc_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   OFC_LAUNCH(k_poc_grid, lv.nx * lv.ny, POC_T, smem, st, a, b, lv.W, lv.H, lv.wy, lv.wx, xs, ys, lv.nx, iux, iuy,
              (const PocConst*)dconst, lpm, ux, uy, peak);
