@@ -117,10 +117,10 @@ def accumulate_bytes(W, H, F=12):
 
 
 # DRAM traffic of one k_accumulate launch over its algorithmic bytes, from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum = 459.7 MB against 474.4 MB algorithmic on a 1024^2 pair,
+# (dram__bytes_read.sum + dram__bytes_write.sum = 404.4 MB against 424.0 MB algorithmic on a 1024^2 pair,
 # profiles/k_accumulate_1024.txt); the traffic of a launch at another size is this ratio times its
 # algorithmic bytes (both grow with the pixel and padded-pixel counts)
-ACC_TRAFFIC_RATIO = 459.7 / 474.4
+ACC_TRAFFIC_RATIO = 404.4 / 424.0
 
 
 def cpu_sample(a, b, roi, n=512):

@@ -432,6 +432,7 @@ void reference_pack(Lane& L, const float* i1, int W, int H, const GaborTables& g
   float2* T32 = L.get<float2>("fft_T", Np);
   float2* U32 = L.get<float2>("ref_U32", Np * 3 * G);
   launch_fft_rows_fwd_real(i1, W, H, plw, ph, T32, st);
+  launch_fft_cols_fwd(T32, plh, pw, st);
   for (int k0 = 0; k0 < g.F; k0 += G) {
     int k1 = std::min(g.F, k0 + G);
     launch_fft_cols_ref_f32(T32, plh, pw, g, k0, k1, U32, st);

@@ -517,58 +517,6 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_fwd_real(const float* 
   for (int x = threadIdx.x; x < pw; x += blockDim.x) o[x] = r[x];
 }
 
-// The reference pack's column pass: per block C adjacent columns of Tin (ph x pw, row-transformed; element i of
-// the block's tile is row i >> LC, column i & (C - 1)); forward transform, then for filters [k0, k1) the three
-// planes S G, S G i fx, S G i fy (factors formed in float64), each inverted along y into U (3 planes per filter).
-// Shared memory: S (spectrum) and W1, W2 (ping-pong).
-template <int C>
-__global__ void __launch_bounds__(FFT_TMAX) k_fft_cols_refpack(const float2* __restrict__ Tin, FftPlan plh, int pw,
-                                                               GaborTables g, int k0, int k1, float2* __restrict__ U) {
-  constexpr int LC = C == 4 ? 2 : (C == 2 ? 1 : 0);
-  extern __shared__ __align__(16) unsigned char smraw[];
-  float2* sm = (float2*)smraw;
-  const int ph = plh.L;
-  const int n = ph * C, nb = fft_buf_len(ph, C);
-  float2* S = sm;
-  float2* W1 = sm + nb;
-  float2* W2 = sm + 2 * nb;
-  const int x0 = blockIdx.x * C;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    int y = i >> LC, x = x0 + (i & (C - 1));
-    S[i] = x < pw ? Tin[(size_t)y * pw + x] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  float2* spec = fft_run<C>(S, W1, plh, false);
-  if (spec != S) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) S[i] = spec[i];
-    __syncthreads();
-  }
-  const size_t plane = (size_t)ph * pw;
-  for (int k = k0; k < k1; k++) {
-    const double* exk = g.ex + (size_t)k * pw;
-    const double* eyk = g.ey + (size_t)k * ph;
-    for (int v = 0; v < 3; v++) {
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        int y = i >> LC, x = min(x0 + (i & (C - 1)), pw - 1);
-        float2 sv = S[i];
-        double G = fma(g.hx[x], g.omy[y], g.omx[x]) * exk[x] * eyk[y];
-        double re = sv.x * G, im = sv.y * G;
-        if (v == 1) { double f = g.fx[x]; double t = re; re = -im * f; im = t * f; }        // x i fx
-        else if (v == 2) { double f = g.fy[y]; double t = re; re = -im * f; im = t * f; }   // x i fy
-        W1[i] = make_float2((float)re, (float)im);
-      }
-      __syncthreads();
-      float2* res = fft_run<C>(W1, W2, plh, true);
-      float2* dst = U + (size_t)((k - k0) * 3 + v) * plane;
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        int y = i >> LC, x = x0 + (i & (C - 1));
-        if (x < pw) dst[(size_t)y * pw + x] = res[i];
-      }
-      __syncthreads();
-    }
-  }
-}
-
 // The column pass of the responses in two kernels, so that a block holds only two buffers of C columns
 // (several blocks per SM instead of one): k_fft_cols_fwd writes the column spectrum S (ph x pw, row-major,
 // small enough to stay in L2), then k_fft_cols_inv_filter, one block per (C columns, filter k), multiplies S by
@@ -595,28 +543,45 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_fwd(const float2* Tin
   }
 }
 
-template <int C>
+// REFPACK = false: the responses (filter k = blockIdx.y: S G_k, inverse, prefilter along y) into plane k of U.
+// REFPACK = true: the reference pack of filters [k0, k0 + gridDim.y / 3): blockIdx.y = 3 (k - k0) + v with the
+// planes S G, S G i fx, S G i fy for v = 0, 1, 2 (factors formed in float64), inverse, no prefilter, into plane
+// blockIdx.y of U.
+template <int C, bool REFPACK>
 __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const float2* __restrict__ S, FftPlan plh, int pw,
-                                                                      GaborTables g, float2* __restrict__ U) {
+                                                                      GaborTables g, int k0, float2* __restrict__ U) {
   constexpr int LC = C == 4 ? 2 : (C == 2 ? 1 : 0);
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* A = (float2*)smraw;
   const int ph = plh.L, n = ph * C;
   float2* B = A + fft_buf_len(ph, C);
-  const int x0 = blockIdx.x * C, k = blockIdx.y;
+  const int x0 = blockIdx.x * C;
+  const int k = REFPACK ? k0 + blockIdx.y / 3 : blockIdx.y, var = REFPACK ? blockIdx.y % 3 : 0;
   const float* exkf = g.exf + (size_t)k * pw;
   const float* eykf = g.eyf + (size_t)k * ph;
+  const double* exk = g.ex + (size_t)k * pw;
+  const double* eyk = g.ey + (size_t)k * ph;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     int y = i >> LC, xr = x0 + (i & (C - 1)), x = min(xr, pw - 1);
     float2 sv = xr < pw ? S[(size_t)y * pw + x] : make_float2(0.f, 0.f);
-    float G = fmaf(__ldg(g.hxf + x), __ldg(g.omyf + y), __ldg(g.omxf + x)) * (__ldg(exkf + x) * __ldg(eykf + y));
-    A[i] = make_float2(sv.x * G, sv.y * G);
+    if (!REFPACK) {
+      float G = fmaf(__ldg(g.hxf + x), __ldg(g.omyf + y), __ldg(g.omxf + x)) * (__ldg(exkf + x) * __ldg(eykf + y));
+      A[i] = make_float2(sv.x * G, sv.y * G);
+    } else {
+      double G = fma(g.hx[x], g.omy[y], g.omx[x]) * exk[x] * eyk[y];
+      double re = sv.x * G, im = sv.y * G;
+      if (var == 1) { double f = g.fx[x]; double t = re; re = -im * f; im = t * f; }        // x i fx
+      else if (var == 2) { double f = g.fy[y]; double t = re; re = -im * f; im = t * f; }   // x i fy
+      A[i] = make_float2((float)re, (float)im);
+    }
   }
   __syncthreads();
   float2* r = fft_run<C>(A, B, plh, true);
-  float2* carry = r == A ? B : A;
-  prefilter_smem<C>(r, ph, carry, carry + 2 * blockDim.x);
-  float2* dst = U + (size_t)k * ph * pw;
+  if (!REFPACK) {
+    float2* carry = r == A ? B : A;
+    prefilter_smem<C>(r, ph, carry, carry + 2 * blockDim.x);
+  }
+  float2* dst = U + (size_t)blockIdx.y * ph * pw;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     int y = i >> LC, x = x0 + (i & (C - 1));
     if (x < pw) dst[(size_t)y * pw + x] = r[i];
@@ -641,7 +606,7 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_resp(const float2*
   }
 }
 
-__global__ void __launch_bounds__(FFT_TMAX) k_fft_rows_inv_ref(const float2* __restrict__ U, FftPlan plw, int ph, int W,
+__global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_ref(const float2* __restrict__ U, FftPlan plw, int ph, int W,
                                                                int H, int k0, float4* __restrict__ ref4,
                                                                float* __restrict__ amp) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -703,23 +668,10 @@ static size_t smem_prefilter(int L, int C, int T) {
   return std::max<size_t>(2 * fbytes(L, C), fbytes(L, C) + (size_t)(2 * T + 2 * C) * sizeof(float2));
 }
 
-// columns per block of the reference pack's column pass: C adjacent columns make 32-byte row segments
-static int cols_C(int ph, int& T, size_t& sm) {
-  for (int C : {4, 2, 1}) {
-    T = fft_threads(ph, C);
-    sm = 3 * fbytes(ph, C);
-    if (sm <= SMEM_MAX) return C;
-  }
-  throw Error(OFC_ERR_WINDOW, "padded height " + std::to_string(ph) + " too large for the column pass");
-}
-
 bool fft_fits(int ph, int pw) {
   try {
-    int T;
-    size_t sm;
     int Tc = std::min(fft_threads(ph, 2), COLS_TMAX);
     if (smem_prefilter(ph, 2, Tc) > SMEM_MAX) return false;
-    cols_C(ph, T, sm);
     return 4 * fbytes(pw, 1) <= SMEM_MAX && smem_prefilter(pw, 1, fft_threads(pw, 1)) <= SMEM_MAX;
   } catch (const Error&) {
     return false;
@@ -741,11 +693,11 @@ void launch_fft_cols_filters(float2* T, const FftPlan& plh, int pw, const GaborT
   size_t sm_i = smem_prefilter(ph, C, nt);
   if (sm_i > SMEM_MAX) throw Error(OFC_ERR_WINDOW, "padded height " + std::to_string(ph) + " too large for the column pass");
   set_smem((const void*)k_fft_cols_fwd<C>, sm_f);
-  set_smem((const void*)k_fft_cols_inv_filter<C>, sm_i);
+  set_smem((const void*)k_fft_cols_inv_filter<C, false>, sm_i);
   // in place: a block reads its C columns whole before it writes their spectrum back
   OFC_LAUNCH(k_fft_cols_fwd<C>, div_up(pw, C), nt, sm_f, st, T, plh, pw, T);
   dim3 grid(div_up(pw, C), g.F);
-  OFC_LAUNCH(k_fft_cols_inv_filter<C>, grid, nt, sm_i, st, T, plh, pw, g, U);
+  OFC_LAUNCH((k_fft_cols_inv_filter<C, false>), grid, nt, sm_i, st, T, plh, pw, g, 0, U);
 }
 
 void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F, float2* R, cudaStream_t st) {
@@ -757,24 +709,24 @@ void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F
   OFC_LAUNCH(k_fft_rows_inv_resp, grid, T, sm, st, U, plw, ph, scale, R);
 }
 
-void launch_fft_cols_ref_f32(const float2* Tin, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1,
+void launch_fft_cols_fwd(float2* T, const FftPlan& plh, int pw, cudaStream_t st) {
+  constexpr int C = 2;
+  const int ph = plh.L;
+  int nt = std::min(fft_threads(ph, C), COLS_TMAX);
+  size_t sm_f = 2 * fbytes(ph, C);
+  set_smem((const void*)k_fft_cols_fwd<C>, sm_f);
+  OFC_LAUNCH(k_fft_cols_fwd<C>, div_up(pw, C), nt, sm_f, st, T, plh, pw, T);
+}
+
+void launch_fft_cols_ref_f32(const float2* S, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1,
                              float2* U, cudaStream_t st) {
-  int T;
-  size_t sm;
-  int C = cols_C(plh.L, T, sm);
-  switch (C) {
-    case 4:
-      set_smem((const void*)k_fft_cols_refpack<4>, sm);
-      OFC_LAUNCH(k_fft_cols_refpack<4>, div_up(pw, C), T, sm, st, Tin, plh, pw, g, k0, k1, U);
-      break;
-    case 2:
-      set_smem((const void*)k_fft_cols_refpack<2>, sm);
-      OFC_LAUNCH(k_fft_cols_refpack<2>, div_up(pw, C), T, sm, st, Tin, plh, pw, g, k0, k1, U);
-      break;
-    default:
-      set_smem((const void*)k_fft_cols_refpack<1>, sm);
-      OFC_LAUNCH(k_fft_cols_refpack<1>, div_up(pw, C), T, sm, st, Tin, plh, pw, g, k0, k1, U);
-  }
+  constexpr int C = 2;
+  const int ph = plh.L;
+  int nt = std::min(fft_threads(ph, C), COLS_TMAX);
+  size_t sm = 2 * fbytes(ph, C);
+  set_smem((const void*)k_fft_cols_inv_filter<C, true>, sm);
+  dim3 grid(div_up(pw, C), 3 * (k1 - k0));
+  OFC_LAUNCH((k_fft_cols_inv_filter<C, true>), grid, nt, sm, st, S, plh, pw, g, k0, U);
 }
 
 void launch_fft_rows_inv_ref_f32(const float2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,

@@ -55,11 +55,14 @@ void launch_fft_cols_filters(float2* T, const FftPlan& plh, int pw, const GaborT
 // inverse row transforms + B-spline prefilter along x + scale -> responses R (F planes of ph x pw)
 void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F, float2* R, cudaStream_t st);
 
-// the reference pack (reference_phase, phaseflow.py:92-112): column transforms of filters [k0, k1), 3 planes per
-// filter (S G, S G i fx, S G i fy; the factors formed in float64), inverse along y; then the inverse row transforms
-// cropped to W x H with, per pixel, (r.re, r.im, gx, gy) and amp formed in float64 and stored float32. The
-// transforms are float32, as the reference's Rust port computes them (rustfft f32, gabor.rs:230-270).
-void launch_fft_cols_ref_f32(const float2* T, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1,
+// the reference pack (reference_phase, phaseflow.py:92-112). launch_fft_cols_fwd: forward column transforms of the
+// row-transformed T, in place (T then holds the 2-D spectrum S); launch_fft_cols_ref_f32: for filters [k0, k1) the
+// 3 planes per filter S G, S G i fx, S G i fy (the factors formed in float64), inverse along y, into U; then the
+// inverse row transforms cropped to W x H with, per pixel, (r.re, r.im, gx, gy) and amp formed in float64 and
+// stored float32. The transforms are float32, as the reference's Rust port computes them (rustfft f32,
+// gabor.rs:230-270).
+void launch_fft_cols_fwd(float2* T, const FftPlan& plh, int pw, cudaStream_t st);
+void launch_fft_cols_ref_f32(const float2* S, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1,
                              float2* U, cudaStream_t st);
 void launch_fft_rows_inv_ref_f32(const float2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,
                                  float4* ref4, float* amp, cudaStream_t st);
