@@ -41,11 +41,86 @@ __global__ void k_corr_x(const double* __restrict__ in, double* __restrict__ out
   out[(size_t)pl * W * H + (size_t)y * W + x] = s;
 }
 
+// The same correlations for the default smoothing window (r = 16, sigma_s = 4). y: a thread owns CY_RY
+// consecutive rows of a column and loads their 2r + CY_RY input rows once (instead of 2r + 1 loads per output,
+// most of them L2 traffic); x: a block stages a row segment and its halo in shared memory and a thread forms
+// CX_RX consecutive outputs from one register window (odd CX_RX: the warp's reads fall on distinct banks).
+// Symmetric taps are paired (k(t) = k(-t)).
+constexpr int CORR_R = 16, CY_RY = 4, CX_RX = 3;
+
+__global__ void __launch_bounds__(128, 4) k_corr_y_rb(const double* __restrict__ in, double* __restrict__ out, int W,
+                                                     int H, const double* __restrict__ taps) {
+  constexpr int R = CORR_R, RY = CY_RY, NV = RY + 2 * R;
+  __shared__ double tk[R + 1];
+  if (threadIdx.x <= R) tk[threadIdx.x] = taps[R + threadIdx.x];
+  __syncthreads();
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y0 = blockIdx.y * RY;
+  if (x >= W) return;
+  const double* a = in + (size_t)blockIdx.z * W * H + x;
+  double v[NV];
+#pragma unroll
+  for (int i = 0; i < NV; i++) v[i] = a[(size_t)min(max(y0 - R + i, 0), H - 1) * W];
+  double acc[RY];
+#pragma unroll
+  for (int j = 0; j < RY; j++) acc[j] = tk[0] * v[j + R];
+#pragma unroll
+  for (int t = 1; t <= R; t++) {
+    const double k = tk[t];
+#pragma unroll
+    for (int j = 0; j < RY; j++) acc[j] = fma(k, v[j + R + t] + v[j + R - t], acc[j]);
+  }
+  double* o = out + (size_t)blockIdx.z * W * H + x;
+#pragma unroll
+  for (int j = 0; j < RY; j++)
+    if (y0 + j < H) o[(size_t)(y0 + j) * W] = acc[j];
+}
+
+__global__ void __launch_bounds__(128) k_corr_x_rb(const double* __restrict__ in, double* __restrict__ out, int W, int H,
+                                                  const double* __restrict__ taps) {
+  constexpr int R = CORR_R, RX = CX_RX, NT = 128, SEG = NT * RX, WIN = SEG + 2 * R, NV = RX + 2 * R;
+  __shared__ double tk[R + 1];
+  __shared__ double wb[WIN];
+  __shared__ double ob[SEG];
+  const int tid = threadIdx.x, x0 = blockIdx.x * SEG;
+  const double* row = in + (size_t)blockIdx.z * W * H + (size_t)blockIdx.y * W;
+  if (tid <= R) tk[tid] = taps[R + tid];
+  for (int i = tid; i < WIN; i += NT) wb[i] = row[min(max(x0 - R + i, 0), W - 1)];
+  __syncthreads();
+  double v[NV];
+#pragma unroll
+  for (int i = 0; i < NV; i++) v[i] = wb[tid * RX + i];
+  double acc[RX];
+#pragma unroll
+  for (int j = 0; j < RX; j++) acc[j] = tk[0] * v[j + R];
+#pragma unroll
+  for (int t = 1; t <= R; t++) {
+    const double k = tk[t];
+#pragma unroll
+    for (int j = 0; j < RX; j++) acc[j] = fma(k, v[j + R + t] + v[j + R - t], acc[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < RX; j++) ob[tid * RX + j] = acc[j];
+  __syncthreads();
+  double* o = out + (size_t)blockIdx.z * W * H + (size_t)blockIdx.y * W;
+  for (int i = tid; i < SEG; i += NT)
+    if (x0 + i < W) o[x0 + i] = ob[i];
+}
+
 void launch_corr_y(const double* in, double* out, int n_planes, int W, int H, const double* taps, int r, cudaStream_t st) {
+  if (r == CORR_R) {
+    dim3 g(div_up(W, 128), div_up(H, CY_RY), n_planes);
+    OFC_LAUNCH(k_corr_y_rb, g, 128, 0, st, in, out, W, H, taps);
+    return;
+  }
   dim3 g(div_up(W, 128), H, n_planes);
   OFC_LAUNCH(k_corr_y<double>, g, 128, 0, st, in, out, W, H, taps, r);
 }
 void launch_corr_x(const double* in, double* out, int n_planes, int W, int H, const double* taps, int r, cudaStream_t st) {
+  if (r == CORR_R) {
+    dim3 g(div_up(W, 128 * CX_RX), H, n_planes);
+    OFC_LAUNCH(k_corr_x_rb, g, 128, 0, st, in, out, W, H, taps);
+    return;
+  }
   dim3 g(div_up(W, 128), H, n_planes);
   OFC_LAUNCH(k_corr_x, g, 128, 0, st, in, out, W, H, taps, r);
 }
@@ -124,6 +199,90 @@ __global__ void k_iir_anticausal(const double* __restrict__ y, Tout* __restrict_
   for (int i = e0 - 1; i >= s0; i--) { c = z * (c - a[(size_t)i * es]); o[(size_t)i * es] = (Tout)c; }
 }
 
+// Both recursions along x (rows) in one pass through a shared-memory tile: a block of XR_ROWS threads owns
+// XR_ROWS rows and the column segment [s0, s0 + XR_SEG); it loads columns [s0 - IIR_WARM, e0 + IIR_WARM]
+// (clamped to the row) with coalesced row reads, each thread runs the causal recursion over its tile row (warm-up
+// from the tile's start, or the exact start at column 0) and then the anticausal one down to s0 (warm-up from the
+// tile's end, or the exact start at the row's end), and the block stores the segment with coalesced row writes.
+// One thread per row makes the recursion sequential in a row; an odd row stride keeps the threads' column
+// accesses on distinct banks.
+constexpr int XR_ROWS = 64, XR_SEG = 64, XR_TW = XR_SEG + 2 * IIR_WARM + 1;  // 121 doubles per tile row (odd)
+
+template <class Tout>
+__global__ void __launch_bounds__(XR_ROWS) k_iir_x(const double* __restrict__ in, Tout* __restrict__ out, int n, int nrows,
+                                                  long plane) {
+  extern __shared__ double tile[];  // XR_ROWS x XR_TW
+  const int r0 = blockIdx.y * XR_ROWS, s0 = blockIdx.x * XR_SEG;
+  const int e0 = min(n, s0 + XR_SEG), c0 = max(0, s0 - IIR_WARM), c1 = min(n, e0 + IIR_WARM + 1), cw = c1 - c0;
+  const double* a = in + (size_t)blockIdx.z * plane;
+  Tout* o = out + (size_t)blockIdx.z * plane;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  // asynchronous copies: the whole tile is in flight at once (a load-then-store loop waits a DRAM latency per row)
+  for (int rr = wid; rr < XR_ROWS; rr += nw) {
+    if (r0 + rr >= nrows) break;
+    const double* src = a + (size_t)(r0 + rr) * n + c0;
+    for (int c = lane; c < cw; c += 32) __pipeline_memcpy_async(&tile[rr * XR_TW + c], src + c, sizeof(double));
+  }
+  __pipeline_commit();
+  __pipeline_wait_prior(0);
+  __syncthreads();
+  const int row = threadIdx.x;
+  if (r0 + row < nrows) {
+    double* t = tile + row * XR_TW;  // t[i - c0] = value at column i
+    if (n == 1) {
+      // a single column: the coefficient is the value (as the separate passes give)
+    } else {
+      const double z = bspline_z();
+      double acc;
+      int i0;
+      if (c0 == 0) {  // exact start: y[0] = sum_{k < min(n, 21)} z^k 6 x[k]
+        const int hz = min(n, HORIZON);
+        acc = 0;
+        double zk = 1;
+        for (int k = 0; k < hz; k++) {
+          acc += zk * (6.0 * t[k]);
+          zk *= z;
+        }
+        t[0] = acc;
+        i0 = 1;
+      } else {
+        acc = 0;
+        i0 = 0;
+      }
+#pragma unroll 4
+      for (int i = i0; i < cw; i++) {
+        acc = 6.0 * t[i] + z * acc;
+        t[i] = acc;
+      }
+      const double g = z / (z * z - 1.0);
+      double c;
+      int i1;
+      if (c1 == n) {  // exact start: c[n-1] = z / (z^2 - 1) (y[n-1] + z y[n-2])
+        c = g * (t[cw - 1] + z * t[cw - 2]);
+        t[cw - 1] = c;
+        i1 = cw - 2;
+      } else {
+        c = 0;
+        i1 = cw - 1;
+      }
+#pragma unroll 4
+      for (int i = i1; i >= s0 - c0; i--) {
+        c = z * (c - t[i]);
+        t[i] = c;
+      }
+    }
+  }
+  __syncthreads();
+  for (int rr = wid; rr < XR_ROWS; rr += nw) {
+    if (r0 + rr >= nrows) break;
+    Tout* dst = o + (size_t)(r0 + rr) * n + s0;
+    const double* t = tile + rr * XR_TW + (s0 - c0);
+    for (int c = lane; c < e0 - s0; c += 32) dst[c] = (Tout)t[c];
+  }
+}
+
+// y pass: in -> tmp (causal) -> tmp2 (anticausal); x pass: tmp2 -> out. tmp may alias out (it is dead once the
+// x pass starts); tmp2 must not, since the x pass's tiles overlap.
 template <class Tin, class Tout>
 static void bspline_axes(const Tin* in, Tout* out, double* tmp, double* tmp2, int n_planes, int W, int H, cudaStream_t st) {
   long plane = (long)W * H;
@@ -131,15 +290,16 @@ static void bspline_axes(const Tin* in, Tout* out, double* tmp, double* tmp2, in
   dim3 gy(div_up(W, 128), div_up(H, SEG), n_planes);
   OFC_LAUNCH((k_iir_causal<Tin>), gy, 128, 0, st, in, tmp, H, W, (long)W, 1L, plane);
   OFC_LAUNCH((k_iir_anticausal<double>), gy, 128, 0, st, tmp, tmp2, H, W, (long)W, 1L, plane);
-  // along x: lines = rows (W apart), element stride 1
-  dim3 gx(div_up(H, 128), div_up(W, SEG), n_planes);
-  OFC_LAUNCH((k_iir_causal<double>), gx, 128, 0, st, tmp2, tmp, W, H, 1L, (long)W, plane);
-  OFC_LAUNCH((k_iir_anticausal<Tout>), gx, 128, 0, st, tmp, out, W, H, 1L, (long)W, plane);
+  // along x: both recursions in one pass through shared-memory tiles
+  const size_t sm = (size_t)XR_ROWS * XR_TW * sizeof(double);
+  OFC_CUDA(cudaFuncSetAttribute((const void*)k_iir_x<Tout>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  dim3 gx(div_up(W, XR_SEG), div_up(H, XR_ROWS), n_planes);
+  OFC_LAUNCH(k_iir_x<Tout>, gx, XR_ROWS, sm, st, tmp2, out, W, H, plane);
 }
 
 void launch_bspline_f64(const double* in, double* out, double* tmp, int n_planes, int W, int H, cudaStream_t st) {
-  // out doubles as the second scratch plane set (written last)
-  bspline_axes<double, double>(in, out, tmp, out, n_planes, W, H, st);
+  // out doubles as the causal scratch of the y pass; tmp holds the y pass's result for the x pass
+  bspline_axes<double, double>(in, out, (double*)out, tmp, n_planes, W, H, st);
 }
 
 void launch_bspline_f32(const float* in, float* out, double* tmp, int W, int H, cudaStream_t st) {
