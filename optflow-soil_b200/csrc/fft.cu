@@ -236,12 +236,76 @@ __device__ __forceinline__ void odd_butterfly(Load in, bool inv, Emit emit) {
 constexpr int FFT_PAD = 4;
 __host__ __device__ constexpr int fft_buf_len(int L, int C) { return L * C + ((L * C) >> FFT_PAD) + 1; }
 
+// The butterfly of radix P (P = 0: a direct DFT of runtime radix RP) on inputs in(j), j < P, with outputs
+// through emit(k, value) (which applies the inter-stage twiddle); tw_m(m) = w_P^m for the direct DFT.
+template <int P, class C2, class In, class Emit, class TwM>
+__device__ __forceinline__ void butterfly(In in, Emit emit, TwM tw_m, int RP, bool inv) {
+  if constexpr (P == 2) {
+    C2 a0 = in(0), a1 = in(1);
+    emit(0, cadd(a0, a1));
+    emit(1, csub(a0, a1));
+  } else if constexpr (P == 4) {
+    C2 a0 = in(0), a1 = in(1), a2 = in(2), a3 = in(3);
+    C2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
+    C2 t2 = cadd(a1, a3), t3 = rot(csub(a1, a3), inv);
+    emit(0, cadd(t0, t2));
+    emit(2, csub(t0, t2));
+    emit(1, cadd(t1, t3));
+    emit(3, csub(t1, t3));
+  } else if constexpr (P == 8) {
+    C2 v[8];
+#pragma unroll
+    for (int j = 0; j < 8; j++) v[j] = in(j);
+    C2 e[4], d[4];
+    {
+      C2 t0 = cadd(v[0], v[4]), t1 = csub(v[0], v[4]);
+      C2 t2 = cadd(v[2], v[6]), t3 = rot(csub(v[2], v[6]), inv);
+      e[0] = cadd(t0, t2); e[2] = csub(t0, t2); e[1] = cadd(t1, t3); e[3] = csub(t1, t3);
+    }
+    {
+      C2 t0 = cadd(v[1], v[5]), t1 = csub(v[1], v[5]);
+      C2 t2 = cadd(v[3], v[7]), t3 = rot(csub(v[3], v[7]), inv);
+      d[0] = cadd(t0, t2); d[2] = csub(t0, t2); d[1] = cadd(t1, t3); d[3] = csub(t1, t3);
+    }
+    // w8^k, k = 1..3: (h, -h), (0, -1), (-h, -h) forward; conjugates inverse (h = cos(pi / 4))
+    constexpr float h = 0.70710678118654752440f;
+    const float sg = inv ? 1.f : -1.f;
+    C2 t1 = mkc<C2>(h * (d[1].x - sg * d[1].y), h * (d[1].y + sg * d[1].x));
+    C2 t2 = mkc<C2>(-sg * d[2].y, sg * d[2].x);
+    C2 t3 = mkc<C2>(h * (-d[3].x - sg * d[3].y), h * (-d[3].y + sg * d[3].x));
+    emit(0, cadd(e[0], d[0]));
+    emit(4, csub(e[0], d[0]));
+    emit(1, cadd(e[1], t1));
+    emit(5, csub(e[1], t1));
+    emit(2, cadd(e[2], t2));
+    emit(6, csub(e[2], t2));
+    emit(3, cadd(e[3], t3));
+    emit(7, csub(e[3], t3));
+  } else if constexpr (P == 3 || P == 5 || P == 7 || P == 11 || P == 13) {
+    odd_butterfly<P, C2>(in, inv, emit);
+  } else {
+    for (int k = 0; k < RP; k++) {
+      C2 acc = in(0);
+      int jk = 0;
+      for (int j = 1; j < RP; j++) {
+        jk += k;
+        if (jk >= RP) jk -= RP;
+        C2 av = in(j);
+        C2 w = tw_m(jk);
+        acc.x = fma(av.x, w.x, fma(-av.y, w.y, acc.x));
+        acc.y = fma(av.x, w.y, fma(av.y, w.x, acc.y));
+      }
+      emit(k, acc);
+    }
+  }
+}
+
 // One Stockham stage of radix P from buffer A (layout shift ish) to buffer B (layout shift osh); C interleaved
 // lines of length L, C = 1 << lc. q, r of a butterfly come from multiplications by precomputed reciprocals
 // (magic = ceil(2^32 / s), exact for the sizes here). Radices 2, 4, 8 have hand-written butterflies, 3, 5, 7,
 // 11 and 13 the symmetric odd form, and any other radix (P = 0 here) a direct DFT with its inputs read from
 // shared memory. Each radix is its own non-inlined function, so that the registers of one radix's butterfly do
-// not add to another's.
+// not add to another's. Butterfly b reads elements b + j istep (b = bi C + l with bi = q s + r).
 template <int P, class C2>
 __device__ __noinline__ void stage_loop(const C2* __restrict__ A, C2* __restrict__ B, int lc, int L, int Pr, int s,
                                         unsigned magic, const C2* __restrict__ tw, bool inv, int ish, int osh) {
@@ -254,10 +318,9 @@ __device__ __noinline__ void stage_loop(const C2* __restrict__ A, C2* __restrict
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     const int l = b & (C - 1), bi = b >> lc;
     const int q = s == 1 ? bi : (int)__umulhi((unsigned)bi, magic), r = bi - q * s;
-    const int ib = (r + s * q) * C + l;
     const int ob = (r + s * RP * q) * C + l;
     auto in = [&](int j) {
-      const int i = ib + j * istep;
+      const int i = b + j * istep;
       return A[i + (i >> ish)];
     };
     auto emit = [&](int k, C2 val) {
@@ -272,64 +335,78 @@ __device__ __noinline__ void stage_loop(const C2* __restrict__ A, C2* __restrict
       C2 w = __ldg(tw + (size_t)mm * LP);
       return inv ? conjf2(w) : w;
     };
-    if constexpr (P == 2) {
-      C2 a0 = in(0), a1 = in(1);
-      emit(0, cadd(a0, a1));
-      emit(1, csub(a0, a1));
-    } else if constexpr (P == 4) {
-      C2 a0 = in(0), a1 = in(1), a2 = in(2), a3 = in(3);
-      C2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
-      C2 t2 = cadd(a1, a3), t3 = rot(csub(a1, a3), inv);
-      emit(0, cadd(t0, t2));
-      emit(2, csub(t0, t2));
-      emit(1, cadd(t1, t3));
-      emit(3, csub(t1, t3));
-    } else if constexpr (P == 8) {
-      C2 v[8];
-#pragma unroll
-      for (int j = 0; j < 8; j++) v[j] = in(j);
-      C2 e[4], d[4];
-      {
-        C2 t0 = cadd(v[0], v[4]), t1 = csub(v[0], v[4]);
-        C2 t2 = cadd(v[2], v[6]), t3 = rot(csub(v[2], v[6]), inv);
-        e[0] = cadd(t0, t2); e[2] = csub(t0, t2); e[1] = cadd(t1, t3); e[3] = csub(t1, t3);
+    butterfly<P, C2>(in, emit, tw_m, RP, inv);
+  }
+}
+
+// The same stage with every size known at compile time (radix P, stride S, length L, lines C, layout shifts):
+// the quotients, strides and padded offsets fold into constants.
+template <int P, int S, int L, int C, int ISH, int OSH, class C2>
+__device__ __noinline__ void stage_fixed(const C2* __restrict__ A, C2* __restrict__ B, const C2* __restrict__ tw,
+                                         bool inv) {
+  constexpr int PB = (P == 2 || P == 3 || P == 4 || P == 5 || P == 7 || P == 8 || P == 11 || P == 13) ? P : 0;
+  constexpr int M = L / (P * S), NB = (L / P) * C, ISTEP = S * M * C, OSTEP = S * C, LP = L / P;
+  for (int b = threadIdx.x; b < NB; b += blockDim.x) {
+    const int l = b % C, bi = b / C;
+    const int q = bi / S, r = bi - q * S;
+    const int ob = (r + S * P * q) * C + l;
+    auto in = [&](int j) {
+      const int i = b + j * ISTEP;
+      if constexpr (ISH < 31) return A[i + (i >> ISH)];
+      else return A[i];
+    };
+    auto emit = [&](int k, C2 val) {
+      if (k > 0 && q > 0) {
+        C2 w = __ldg(tw + k * S * q);  // k q S < L
+        val = cmul(val, inv ? conjf2(w) : w);
       }
-      {
-        C2 t0 = cadd(v[1], v[5]), t1 = csub(v[1], v[5]);
-        C2 t2 = cadd(v[3], v[7]), t3 = rot(csub(v[3], v[7]), inv);
-        d[0] = cadd(t0, t2); d[2] = csub(t0, t2); d[1] = cadd(t1, t3); d[3] = csub(t1, t3);
-      }
-      // w8^k, k = 1..3: (h, -h), (0, -1), (-h, -h) forward; conjugates inverse (h = cos(pi / 4))
-      constexpr float h = 0.70710678118654752440f;
-      const float sg = inv ? 1.f : -1.f;
-      C2 t1 = mkc<C2>(h * (d[1].x - sg * d[1].y), h * (d[1].y + sg * d[1].x));
-      C2 t2 = mkc<C2>(-sg * d[2].y, sg * d[2].x);
-      C2 t3 = mkc<C2>(h * (-d[3].x - sg * d[3].y), h * (-d[3].y + sg * d[3].x));
-      emit(0, cadd(e[0], d[0]));
-      emit(4, csub(e[0], d[0]));
-      emit(1, cadd(e[1], t1));
-      emit(5, csub(e[1], t1));
-      emit(2, cadd(e[2], t2));
-      emit(6, csub(e[2], t2));
-      emit(3, cadd(e[3], t3));
-      emit(7, csub(e[3], t3));
-    } else if constexpr (P == 3 || P == 5 || P == 7 || P == 11 || P == 13) {
-      odd_butterfly<P, C2>(in, inv, emit);
-    } else {
-      for (int k = 0; k < RP; k++) {
-        C2 acc = in(0);
-        int jk = 0;
-        for (int j = 1; j < RP; j++) {
-          jk += k;
-          if (jk >= RP) jk -= RP;
-          C2 av = in(j);
-          C2 w = tw_m(jk);
-          acc.x = fma(av.x, w.x, fma(-av.y, w.y, acc.x));
-          acc.y = fma(av.x, w.y, fma(av.y, w.x, acc.y));
-        }
-        emit(k, acc);
-      }
-    }
+      const int o = ob + k * OSTEP;
+      if constexpr (OSH < 31) B[o + (o >> OSH)] = val;
+      else B[o] = val;
+    };
+    auto tw_m = [&](int mm) {  // w_P^mm
+      C2 w = __ldg(tw + mm * LP);
+      return inv ? conjf2(w) : w;
+    };
+    butterfly<PB, C2>(in, emit, tw_m, P, inv);
+  }
+}
+
+// compile-time plan: the factorisation of fft_make_plan (8s, 4s, 2s, then odd primes up to 31)
+struct CPlan {
+  int nst = 0;
+  int p[FFT_MAXST] = {}, s[FFT_MAXST] = {};
+};
+constexpr CPlan cplan(int L) {
+  CPlan c{};
+  int m = L, f[FFT_MAXST] = {}, n = 0;
+  while (m % 8 == 0) { f[n++] = 8; m /= 8; }
+  while (m % 4 == 0) { f[n++] = 4; m /= 4; }
+  while (m % 2 == 0) { f[n++] = 2; m /= 2; }
+  const int primes[10] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31};
+  for (int i = 0; i < 10; i++)
+    while (m % primes[i] == 0) { f[n++] = primes[i]; m /= primes[i]; }
+  int st = 1;
+  for (int i = 0; i < n; i++) {
+    c.p[i] = f[i];
+    c.s[i] = st;
+    st *= f[i];
+  }
+  c.nst = n;
+  return c;
+}
+
+template <int L, int C, int ST, class C2>
+__device__ __forceinline__ C2* fft_run_fixed(C2* a, C2* b, const C2* tw, bool inv) {
+  constexpr CPlan P = cplan(L);
+  if constexpr (ST == P.nst) {
+    return a;
+  } else {
+    constexpr int OSH = (ST + 1 < P.nst && P.s[ST] * C < 32) ? FFT_PAD : 31;
+    constexpr int ISH = ST == 0 ? 31 : (P.s[ST - 1] * C < 32 ? FFT_PAD : 31);
+    stage_fixed<P.p[ST], P.s[ST], L, C, ISH, OSH, C2>(a, b, tw, inv);
+    __syncthreads();
+    return fft_run_fixed<L, C, ST + 1, C2>(b, a, tw, inv);
   }
 }
 
@@ -360,6 +437,8 @@ __device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
   C2* b = tmp;
   const C2* tw = (const C2*)pl.tw;
   constexpr int lc = C == 4 ? 2 : (C == 2 ? 1 : 0);
+  // the padded length of 2048-wide images (2112 = 8 8 3 11) runs with its plan fixed at compile time
+  if (pl.L == 2112) return fft_run_fixed<2112, C, 0, C2>(buf, tmp, tw, inv);
   int ish = 31;
   for (int st = 0; st < pl.nst; st++) {
     const int osh = (st + 1 < pl.nst && pl.s[st] * C < 32) ? FFT_PAD : 31;
