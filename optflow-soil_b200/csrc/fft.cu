@@ -495,6 +495,7 @@ __device__ void prefilter_smem(float2* buf, int n, float2* carry, float2* edge) 
     } else {
       y = make_float2(0.f, 0.f);
     }
+#pragma unroll 4
     for (; i < e0; i++) {
       float2 v = X(i);
       y.x = fmaf(z, y.x, v.x);
@@ -514,6 +515,7 @@ __device__ void prefilter_smem(float2* buf, int n, float2* carry, float2* edge) 
       y = carry[tid - C];
       i0 = s0;
     }
+#pragma unroll 4
     for (int i = i0; i < e0; i++) {
       float2 v = X(i);
       y.x = fmaf(z, y.x, v.x);
@@ -539,6 +541,7 @@ __device__ void prefilter_smem(float2* buf, int n, float2* carry, float2* edge) 
     } else {
       c = make_float2(0.f, 0.f);
     }
+#pragma unroll 4
     for (; i >= s0; i--) {
       float2 v = X(i);
       c.x = z * (c.x - v.x);
@@ -558,6 +561,7 @@ __device__ void prefilter_smem(float2* buf, int n, float2* carry, float2* edge) 
       c = carry[T + tid + C];  // c[e0] of the next segment
       i0 = e0 - 1;
     }
+#pragma unroll 4
     for (int i = i0; i >= s0; i--) {
       float2 v = X(i);
       c.x = z * (c.x - v.x);
