@@ -16,7 +16,6 @@ constexpr int PAD = 32;                 // reflect padding of the Gabor response
 constexpr double APERTURE_TOL = 1e-3;   // phaseflow.py:50
 constexpr int HORIZON = 21;             // ceil(log(1e-12) / log|sqrt(3) - 2|) (interp.py:10)
 constexpr int IIR_WARM = 28;            // samples of warm-up of a segmented recursive filter: z^29 < 3e-17
-constexpr int IIR_WARM_F32 = 16;        // the same for float32 data: z^17 < 6e-10
 
 // An error that leaves the call with a status and a message (EngineError of the reference).
 struct Error : std::runtime_error {

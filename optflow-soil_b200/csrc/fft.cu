@@ -8,11 +8,12 @@
 //
 // The pass structure of one "responses" evaluation (per outer iteration of the fine stage):
 //   rows:    reflect pad + real->complex + forward row FFT                      (read 4 B/px, write 8 B/px)
-//   columns: forward column FFT in place (read 8, write 8); then per (column pair, filter k): x G_k (separable
-//            tables), inverse column FFT, causal + anticausal B-spline prefilter along y  (read 8F, write 8F)
-//   rows:    inverse row FFT, prefilter along x, scale 36 / (ph pw)               (read 8F, write 8F)
-// The prefilter along y commutes with the inverse FFT along x (operators on different axes), so the
-// result is bspline_coeffs(ifft2(F2 * G)) of phaseflow.py:456 up to rounding.
+//   columns: forward column FFT in place (read 8, write 8); then per (column pair, filter k): x G_k and the
+//            B-spline prefilter's periodic factor 1 / ((4 + 2 cos wx)(4 + 2 cos wy)) (separable tables), inverse
+//            column FFT, the prefilter's edge terms along y                        (read 8F, write 8F)
+//   rows:    inverse row FFT, the prefilter's edge terms along x, scale 36 / (ph pw)  (read 8F, write 8F)
+// The prefilter is separable and linear, so its factors and edge terms along one axis commute with the
+// transforms along the other, and the result is bspline_coeffs(ifft2(F2 * G)) of phaseflow.py:456 up to rounding.
 #include "fft.cuh"
 
 #include <cmath>
@@ -73,7 +74,7 @@ int fft_threads(int L, int C) {
 
 std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c) {
   int F = c.n_scales * c.n_orient;
-  std::vector<double> t((size_t)3 * (pw + ph) + (size_t)F * (pw + ph));
+  std::vector<double> t((size_t)4 * (pw + ph) + (size_t)F * (pw + ph));
   double* fx = t.data();
   double* fy = fx + pw;
   double* hx = fy + ph;
@@ -113,6 +114,11 @@ std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c) {
       for (int y = 0; y < ph; y++) { double d = fy[y] - cy; ey[(size_t)k * ph + y] = std::exp(-(d * d) / (2 * s * s)); }
     }
   }
+  // the B-spline prefilter on the periodic grid, per axis: 1 / (4 + 2 cos w)
+  double* bx = ey + (size_t)F * ph;
+  double* by = bx + pw;
+  for (int x = 0; x < pw; x++) bx[x] = 1.0 / (4.0 + 2.0 * std::cos(2 * PI * (double)x / pw));
+  for (int y = 0; y < ph; y++) by[y] = 1.0 / (4.0 + 2.0 * std::cos(2 * PI * (double)y / ph));
   return t;
 }
 
@@ -133,6 +139,8 @@ void gabor_bind(GaborTables& g, const double* d64, const float* d32, int ph, int
   g.omyf = g.omxf + pw;
   g.exf = g.omyf + ph;
   g.eyf = g.exf + (size_t)F * pw;
+  g.bxf = g.eyf + (size_t)F * ph;
+  g.byf = g.bxf + pw;
 }
 
 // ------------------------------------------------------------------------------------------ device
@@ -451,122 +459,72 @@ __device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
   return a;
 }
 
-// Cubic B-spline prefilter (interp.py:13-27, without the factor 6, which the caller folds into its
-// scale) of C interleaved complex lines of length n in buf, in float32 arithmetic (the filter is stable,
-// |z| < 1, so its rounding errors decay geometrically and stay at the level of the float32 storage). The
-// line is cut into at most T / C segments; each recursive pass computes every segment's entry value from a
-// warm-up of IIR_WARM_F32 samples (z^17 < 6e-10, below float32 rounding), then runs its segment.
-// carry: 2 * T float2 of scratch; edge: 2 * C float2 (both may lie in the transform's idle buffer).
+// Cubic B-spline prefilter (interp.py:13-27, without the factor 6, which the caller folds into its scale) of C
+// interleaved complex lines of length n in buf, given the lines already divided by 4 + 2 cos w on the periodic
+// grid (the response multiply folds that factor into the filter). Per axis the recursion's transfer function is
+// -z / (1 - 2 z cos w + z^2) = 1 / (4 + 2 cos w), so the periodic division is the recursion on the periodic
+// extension; the reference's recursion on the line (causal start sum_{k < 21} z^k x[k], anticausal start
+// z / (z^2 - 1) (y[n-1] + z y[n-2])) differs from it by two closed-form edge terms:
+//   c[i] = c_per[i] - D0 z^(i+1) / (1 - z^2) + E z^(n-1-i),
+//   D0 = y[0] - y_per[0] = sum_{k < 21} z^k x[k] - sum_{k >= 0} z^k x[-k],  E = c[n-1] - c_per[n-1],
+// with x recovered locally as x[i] = c_per[i-1] + 4 c_per[i] + c_per[i+1] (circular) and the sums cut at
+// z^32 < 1e-18 (lines here are at least 65 long, so the terms of the two ends never meet). scratch: 2 C float4.
 template <int C>
-__device__ void prefilter_smem(float2* buf, int n, float2* carry, float2* edge) {
-  if (n == 1) return;
+__device__ void bspline_edges(float2* buf, int n, float4* scratch) {
   const float z = (float)bspline_z();
-  const int tid = threadIdx.x, T = blockDim.x;
-  // segments per line: at most T / C, with an odd length, so that the threads of a warp, which walk their
-  // segments in step, fall on distinct banks
-  int S = T / C;
-  while (S > 1 && (((n + S - 1) / S) & 1) == 0) S--;
-  const int l = tid % C, sg = tid / C;
-  const int len = (n + S - 1) / S;
-  const int s0 = sg * len, e0 = min(n, s0 + len);
-  const bool live = sg < S && s0 < e0;
-  auto X = [&](int i) { return buf[i * C + l]; };
-  auto init_causal = [&]() {  // y[0] = sum_{k < min(n, 21)} z^k x[k]
-    int hz = min(n, HORIZON);
-    float2 a = make_float2(0.f, 0.f);
-    float zk = 1.f;
-    for (int k = 0; k < hz; k++) {
-      float2 v = X(k);
-      a.x = fmaf(zk, v.x, a.x);
-      a.y = fmaf(zk, v.y, a.y);
-      zk *= z;
-    }
-    return a;
-  };
-  // ---- causal: y[i] = x[i] + z y[i-1]
-  if (live) {
-    if (sg == 0) edge[l] = init_causal();
-    int start = e0 - 1 - IIR_WARM_F32;
-    float2 y;
-    int i = start;
-    if (start <= 0) {
-      y = init_causal();
-      i = 1;
-    } else {
-      y = make_float2(0.f, 0.f);
-    }
-#pragma unroll 4
-    for (; i < e0; i++) {
-      float2 v = X(i);
-      y.x = fmaf(z, y.x, v.x);
-      y.y = fmaf(z, y.y, v.y);
-    }
-    carry[tid] = y;  // y[e0 - 1]
-  }
-  __syncthreads();
-  if (live) {
-    float2 y;
-    int i0;
-    if (sg == 0) {
-      y = edge[l];
-      buf[l] = y;
-      i0 = 1;
-    } else {
-      y = carry[tid - C];
-      i0 = s0;
-    }
-#pragma unroll 4
-    for (int i = i0; i < e0; i++) {
-      float2 v = X(i);
-      y.x = fmaf(z, y.x, v.x);
-      y.y = fmaf(z, y.y, v.y);
-      buf[i * C + l] = y;
-    }
-  }
-  __syncthreads();
-  // ---- anticausal: c[n-1] = z / (z^2 - 1) (y[n-1] + z y[n-2]); c[i] = z (c[i+1] - y[i])
   const float g = (float)(bspline_z() / (bspline_z() * bspline_z() - 1.0));
-  auto init_anti = [&]() {
-    float2 a = X(n - 1), b = X(n - 2);
-    return make_float2(g * fmaf(z, b.x, a.x), g * fmaf(z, b.y, a.y));
+  const float q = (float)(1.0 / (1.0 - bspline_z() * bspline_z()));
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  auto c = [&](int i, int l) { return buf[(i < 0 ? i + n : (i >= n ? i - n : i)) * C + l]; };
+  auto xr = [&](int i, int l) {
+    const float2 a = c(i - 1, l), b = c(i, l), d = c(i + 1, l);
+    return make_float2(fmaf(4.f, b.x, a.x + d.x), fmaf(4.f, b.y, a.y + d.y));
   };
-  if (live) {
-    if (e0 == n) edge[C + l] = init_anti();
-    int stop = s0 + IIR_WARM_F32;
-    float2 c;
-    int i = stop;
-    if (stop >= n - 1) {
-      c = init_anti();
-      i = n - 2;
-    } else {
-      c = make_float2(0.f, 0.f);
+  for (int l = wid; l < C; l += (int)(blockDim.x >> 5)) {  // a warp per line: its two edge constants, lane k
+    const int k = lane;                                       // taking the terms of z^k
+    float zk = 1.f;
+    for (int j = 0; j < k; j++) zk *= z;
+    const int hz = min(n, HORIZON);
+    float2 d0 = make_float2(0.f, 0.f);
+    if (k < hz) {
+      const float2 v = xr(k, l);
+      d0 = make_float2(zk * v.x, zk * v.y);
     }
-#pragma unroll 4
-    for (; i >= s0; i--) {
-      float2 v = X(i);
-      c.x = z * (c.x - v.x);
-      c.y = z * (c.y - v.y);
+    const float2 w = xr(k == 0 ? 0 : n - k, l);
+    d0.x = fmaf(-zk, w.x, d0.x);
+    d0.y = fmaf(-zk, w.y, d0.y);
+    const float2 ya = xr(n - 1 - k, l), yb = xr(n - 2 - k, l);
+    float ax = zk * ya.x, ay = zk * ya.y, bx = zk * yb.x, by = zk * yb.y;
+    for (int o = 16; o; o >>= 1) {
+      d0.x += __shfl_xor_sync(0xffffffffu, d0.x, o);
+      d0.y += __shfl_xor_sync(0xffffffffu, d0.y, o);
+      ax += __shfl_xor_sync(0xffffffffu, ax, o);
+      ay += __shfl_xor_sync(0xffffffffu, ay, o);
+      bx += __shfl_xor_sync(0xffffffffu, bx, o);
+      by += __shfl_xor_sync(0xffffffffu, by, o);
     }
-    carry[T + tid] = c;  // c[s0]
+    if (lane == 0) {
+      const float2 cl = c(n - 1, l);
+      scratch[l] = make_float4(d0.x, d0.y, g * fmaf(z, bx, ax) - cl.x, g * fmaf(z, by, ay) - cl.y);
+    }
   }
   __syncthreads();
-  if (live) {
-    float2 c;
-    int i0;
-    if (e0 == n) {
-      c = edge[C + l];
-      buf[(n - 1) * C + l] = c;
-      i0 = n - 2;
+  for (int t = tid; t < 64 * C; t += blockDim.x) {
+    const int l = t % C, j = t / C;  // j < 32: the start of the line; j >= 32: its end
+    const float4 k = scratch[l];
+    if (j < 32) {
+      float zp = z;  // z^(i+1), i = j
+      for (int m = 0; m < j; m++) zp *= z;
+      float2& v = buf[j * C + l];
+      v.x = fmaf(-k.x * q, zp, v.x);
+      v.y = fmaf(-k.y * q, zp, v.y);
     } else {
-      c = carry[T + tid + C];  // c[e0] of the next segment
-      i0 = e0 - 1;
-    }
-#pragma unroll 4
-    for (int i = i0; i >= s0; i--) {
-      float2 v = X(i);
-      c.x = z * (c.x - v.x);
-      c.y = z * (c.y - v.y);
-      buf[i * C + l] = c;
+      const int i = n - 64 + j;  // j = 32..63 -> i = n-32..n-1
+      float zp = 1.f;            // z^(n-1-i)
+      for (int m = 0; m < n - 1 - i; m++) zp *= z;
+      float2& v = buf[i * C + l];
+      v.x = fmaf(k.z, zp, v.x);
+      v.y = fmaf(k.w, zp, v.y);
     }
   }
   __syncthreads();
@@ -648,7 +606,9 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const floa
     int y = i >> LC, xr = x0 + (i & (C - 1)), x = min(xr, pw - 1);
     float2 sv = xr < pw ? S[(size_t)y * pw + x] : make_float2(0.f, 0.f);
     if (!REFPACK) {
-      float G = fmaf(__ldg(g.hxf + x), __ldg(g.omyf + y), __ldg(g.omxf + x)) * (__ldg(exkf + x) * __ldg(eykf + y));
+      // the Gabor factor and the B-spline prefilter on the periodic grid along both axes
+      float G = fmaf(__ldg(g.hxf + x), __ldg(g.omyf + y), __ldg(g.omxf + x)) * (__ldg(exkf + x) * __ldg(eykf + y)) *
+                (__ldg(g.bxf + x) * __ldg(g.byf + y));
       A[i] = make_float2(sv.x * G, sv.y * G);
     } else {
       double G = fma(g.hx[x], g.omy[y], g.omx[x]) * exk[x] * eyk[y];
@@ -661,8 +621,8 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const floa
   __syncthreads();
   float2* r = fft_run<C>(A, B, plh, true);
   if (!REFPACK) {
-    float2* carry = r == A ? B : A;
-    prefilter_smem<C>(r, ph, carry, carry + 2 * blockDim.x);
+    float2* idle = r == A ? B : A;
+    bspline_edges<C>(r, ph, (float4*)(((uintptr_t)idle + 15) & ~(uintptr_t)15));  // the prefilter's edge terms along y
   }
   float2* dst = U + (size_t)blockIdx.y * ph * pw;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -681,8 +641,8 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_resp(const float2*
   for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[x] = U[off + x];
   __syncthreads();
   float2* r = fft_run<1>(sm, t, plw, true);
-  float2* carry = r == sm ? t : sm;
-  prefilter_smem<1>(r, pw, carry, carry + 2 * blockDim.x);
+  float2* idle = r == sm ? t : sm;
+  bspline_edges<1>(r, pw, (float4*)(((uintptr_t)idle + 15) & ~(uintptr_t)15));  // the prefilter's edge terms along x
   for (int x = threadIdx.x; x < pw; x += blockDim.x) {
     float2 v = r[x];
     R[off + x] = make_float2(v.x * scale, v.y * scale);
@@ -746,9 +706,11 @@ static void set_smem(const void* fn, size_t bytes) {
 
 static size_t fbytes(int L, int C) { return (size_t)fft_buf_len(L, C) * sizeof(float2); }
 
-// shared memory of a transform with a prefilter: two buffers, the idle one holding 2 T + 2 C carries
+// shared memory of a transform with the prefilter's edge terms: two buffers, the idle one holding C float4
+// from its first 16-byte boundary
 static size_t smem_prefilter(int L, int C, int T) {
-  return std::max<size_t>(2 * fbytes(L, C), fbytes(L, C) + (size_t)(2 * T + 2 * C) * sizeof(float2));
+  (void)T;
+  return std::max<size_t>(2 * fbytes(L, C), fbytes(L, C) + 16 + (size_t)C * sizeof(float4));
 }
 
 bool fft_fits(int ph, int pw) {
