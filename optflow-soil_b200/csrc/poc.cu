@@ -333,6 +333,208 @@ __global__ void __launch_bounds__(POC_T, 2) k_poc_grid(const double* __restrict_
   }
 }
 
+// ---------------------------------------------------------------- 64 x 64 windows: real transforms, half spectrum
+// The windows are real, so (1) the forward row transforms run two rows per complex transform, z = a1 + i a2,
+// unpacked as A1[k] = (Z[k] + conj Z[-k]) / 2, A2[k] = (Z[k] - conj Z[-k]) / (2 i); (2) only the columns
+// kx = 0..16 of the low-pass support are transformed along y: the columns 48..63 are their conjugate mirror
+// (the cross-power spectrum of real windows is Hermitian, C(-k) = conj C(k)); (3) after the inverse column
+// transforms every row is Hermitian in kx, so its inverse is real and two rows share one complex inverse,
+// r1 + i r2 = ifft(D1 + i D2). Per re-centring 98 line transforms instead of 194. Hz[y * ZS + kx]: the half
+// spectrum (kx = 0..16; row stride 17 entries = 4 banks, so a warp reading a column spreads over the banks).
+constexpr int ZS = 17;
+
+__device__ __forceinline__ double2 shfl_d2(double2 v, int src) {
+  return make_double2(__shfl_sync(0xffffffff, v.x, src), __shfl_sync(0xffffffff, v.y, src));
+}
+__device__ __forceinline__ int brev5(int i) { return (int)(__brev((unsigned)i) >> 27); }
+
+// forward rows of a real 64 x 64 window (get(y, x) minus mean, Hann weighted) into the half spectrum Hz
+template <class Get>
+__device__ void rows_forward64(Get get, double mean, const PocConst& pc, double2* Hz) {
+  const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
+  // lane l holds Z[k0] (register 0) and Z[k0 + 1] (register 1), k0 = 2 brev5(l) (the bit-reversed output);
+  // Z[-k0] lies in register 0 of lane pl0, Z[-(k0 + 1)] in register 1 of lane 31 - l
+  const int k0 = 2 * brev5(l), pl0 = brev5((32 - brev5(l)) & 31);
+  for (int j = wid; j < 32; j += POC_T / 32) {
+    const int y1 = 2 * j, y2 = 2 * j + 1;
+    double2 v0 = make_double2((get(y1, l) - mean) * (pc.hy[y1] * pc.hx[l]), (get(y2, l) - mean) * (pc.hy[y2] * pc.hx[l]));
+    double2 v1 = make_double2((get(y1, l + 32) - mean) * (pc.hy[y1] * pc.hx[l + 32]),
+                              (get(y2, l + 32) - mean) * (pc.hy[y2] * pc.hx[l + 32]));
+    warp_dif(v0, v1, 64, false, pc.tw64);
+    const double2 p0 = shfl_d2(v0, pl0), p1 = shfl_d2(v1, 31 - l);
+    auto unpack = [&](double2 z, double2 q, int k) {
+      if (k <= 16) {
+        Hz[y1 * ZS + k] = make_double2(0.5 * (z.x + q.x), 0.5 * (z.y - q.y));
+        Hz[y2 * ZS + k] = make_double2(0.5 * (z.y + q.y), -0.5 * (z.x - q.x));
+      }
+    };
+    unpack(v0, p0, k0);
+    unpack(v1, p1, k0 + 1);
+  }
+}
+
+// row index of the low-pass support for a transformed row ky (ky <= 16 or ky >= 48), or -1
+__device__ __forceinline__ int lp_row64(int ky) { return ky <= 16 ? ky : (ky >= 48 ? ky - 31 : -1); }
+
+// poc_shift (poc.py:39-54) of window B = b[y0 : y0 + 64, x0 : x0 + 64] against A's half spectrum on the low-pass
+// support (alp[iy * 17 + kx], iy = 0..32); res = (dx, dy, peak)
+__device__ void poc_shift64(const double* __restrict__ b, int W, int x0, int y0, const PocConst& pc,
+                            const double2* alp, double lpm, double2* Hz, double* surf, double* red, double* res) {
+  const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
+  double s = 0;
+  for (int i = threadIdx.x; i < 4096; i += POC_T) s += b[(size_t)(y0 + (i >> 6)) * W + x0 + (i & 63)];
+  const double mean = block_sum_d(s, red) / 4096.0;
+  const double* bw = b + (size_t)y0 * W + x0;
+  rows_forward64([&](int y, int x) { return bw[(size_t)y * W + x]; }, mean, pc, Hz);
+  __syncthreads();
+  // columns kx = 0..16: forward (dif) -> C = B conj(A) / (|.| + 1e-12) on the low-pass rows, 0 elsewhere ->
+  // inverse (dit) back to natural order
+  for (int ci = wid; ci < ZS; ci += POC_T / 32) {
+    double2 v0 = Hz[l * ZS + ci], v1 = Hz[(l + 32) * ZS + ci];
+    warp_dif(v0, v1, 64, false, pc.tw64);
+    for (int r = 0; r < 2; r++) {
+      double2& v = r == 0 ? v0 : v1;
+      const int iy = lp_row64(brev(32 * r + l, 6));
+      double2 cc = make_double2(0, 0);
+      if (iy >= 0) {
+        const double2 A = alp[iy * ZS + ci];
+        cc = make_double2(v.x * A.x + v.y * A.y, v.y * A.x - v.x * A.y);
+        const double mag = hypot(cc.x, cc.y) + 1e-12;
+        cc.x /= mag;
+        cc.y /= mag;
+      }
+      v = cc;
+    }
+    warp_dit(v0, v1, 64, true, pc.tw64);
+    Hz[l * ZS + ci] = v0;
+    Hz[(l + 32) * ZS + ci] = v1;
+  }
+  __syncthreads();
+  // inverse rows, two per transform: E = D1 + i D2 with D[kx] = Hz[kx] (kx <= 16), conj Hz[64 - kx] (kx >= 48);
+  // the real surface r = fftshift(ifft2(C)) / lpm in natural order, and the first maximum (NaN wins)
+  const double sc = 1.0 / 4096.0 / lpm;
+  double best = -DBL_MAX;
+  int bi = 0x7fffffff;
+  bool bnan = false;
+  for (int j = wid; j < 32; j += POC_T / 32) {
+    const int y1 = 2 * j, y2 = 2 * j + 1;
+    double2 v0 = make_double2(0, 0), v1 = make_double2(0, 0);
+    if (l <= 16) {
+      const double2 d1 = Hz[y1 * ZS + l], d2 = Hz[y2 * ZS + l];
+      v0 = make_double2(d1.x - d2.y, d1.y + d2.x);
+    }
+    if (l >= 16) {
+      const int m = 32 - l;  // kx = 32 + l, 64 - kx = 32 - l
+      const double2 d1 = Hz[y1 * ZS + m], d2 = Hz[y2 * ZS + m];  // conj d1 + i conj d2
+      v1 = make_double2(d1.x + d2.y, -d1.y + d2.x);
+    }
+    warp_dif(v0, v1, 64, true, pc.tw64);
+    for (int r = 0; r < 2; r++) {
+      const double2 v = r == 0 ? v0 : v1;
+      const int x = brev(32 * r + l, 6);
+      const int sxx = (x + 32) & 63;
+      for (int h = 0; h < 2; h++) {
+        const int y = h == 0 ? y1 : y2;
+        const double val = (h == 0 ? v.x : v.y) * sc;
+        surf[y * 64 + x] = val;
+        const int idx = ((y + 32) & 63) * 64 + sxx;
+        const bool vn = val != val;
+        const bool take = bnan ? (vn && idx < bi) : (vn || val > best || (val == best && idx < bi));
+        if (take) { best = val; bi = idx; bnan = vn; }
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    double ov = __shfl_xor_sync(0xffffffff, best, o);
+    int oi = __shfl_xor_sync(0xffffffff, bi, o);
+    bool on = __shfl_xor_sync(0xffffffff, (int)bnan, o) != 0;
+    bool take = bnan ? (on && oi < bi) : (on || ov > best || (ov == best && oi < bi));
+    if (take) { best = ov; bi = oi; bnan = on; }
+  }
+  __shared__ double sv[POC_T / 32];
+  __shared__ int si[POC_T / 32];
+  __shared__ int sn[POC_T / 32];
+  if (l == 0) { sv[wid] = best; si[wid] = bi; sn[wid] = bnan; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < POC_T / 32; k++) {
+      bool on = sn[k] != 0;
+      bool take = bnan ? (on && si[k] < bi) : (on || sv[k] > best || (sv[k] == best && si[k] < bi));
+      if (take) { best = sv[k]; bi = si[k]; bnan = on; }
+    }
+    int iy = bi >> 6, ix = bi & 63;
+    iy = min(max(iy, 1), 62);
+    ix = min(max(ix, 1), 62);
+    auto R = [&](int ys, int xs) { return surf[((ys + 32) & 63) * 64 + ((xs + 32) & 63)]; };  // the shifted surface
+    auto parabola = [](double m, double c, double p) {  // poc.py:34-36
+      double den = m - 2.0 * c + p;
+      return den == 0 ? 0.0 : 0.5 * (m - p) / den;
+    };
+    double c = R(iy, ix);
+    double sxp = parabola(R(iy, ix - 1), c, R(iy, ix + 1));
+    double syp = parabola(R(iy - 1, ix), c, R(iy + 1, ix));
+    res[0] = ix - 32 + sxp;
+    res[1] = iy - 32 + syp;
+    res[2] = c;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(POC_T, 2) k_poc_grid64(const double* __restrict__ a, const double* __restrict__ b,
+                                                          int W, int H, const int* __restrict__ xs,
+                                                          const int* __restrict__ ys, int nx, const double* iux,
+                                                          const double* iuy, const PocConst* __restrict__ pcg,
+                                                          double lpm, double* oux, double* ouy, double* opeak) {
+  extern __shared__ double2 dsm[];
+  double2* Hz = dsm;                    // 64 x 17
+  double2* alp = Hz + 64 * ZS;          // 33 x 17
+  double* surf = (double*)(alp + 33 * ZS);  // 64 x 64
+  __shared__ PocConst pc;
+  __shared__ double red[POC_T / 32];
+  __shared__ double res[3];
+  for (int i = threadIdx.x; i < (int)(sizeof(PocConst) / sizeof(double)); i += POC_T)
+    ((double*)&pc)[i] = ((const double*)pcg)[i];
+  const int gi = blockIdx.x;
+  const int j = gi % nx, i = gi / nx;
+  const int x = xs[j], y = ys[i];
+  const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  // half spectrum of A (poc.py:44) on the low-pass support: alp[iy * 17 + kx]
+  const double* aw = a + (size_t)(y - 32) * W + (x - 32);
+  double s = 0;
+  for (int t = threadIdx.x; t < 4096; t += POC_T) s += aw[(size_t)(t >> 6) * W + (t & 63)];
+  const double mean = block_sum_d(s, red) / 4096.0;
+  rows_forward64([&](int yy, int xx) { return aw[(size_t)yy * W + xx]; }, mean, pc, Hz);
+  __syncthreads();
+  for (int ci = wid; ci < ZS; ci += POC_T / 32) {
+    double2 v0 = Hz[l * ZS + ci], v1 = Hz[(l + 32) * ZS + ci];
+    warp_dif(v0, v1, 64, false, pc.tw64);
+    for (int r = 0; r < 2; r++) {
+      const int iy = lp_row64(brev(32 * r + l, 6));
+      if (iy >= 0) alp[iy * ZS + ci] = r == 0 ? v0 : v1;
+    }
+  }
+  __syncthreads();
+  double dx = iux ? iux[gi] : 0.0, dy = iuy ? iuy[gi] : 0.0;
+  double pk = 0.0;
+  for (int it = 0; it < 3; it++) {
+    double ox = rint(dx), oy = rint(dy);  // Python round(): half to even
+    long y0 = y - 32 + (long)oy, x0 = x - 32 + (long)ox;
+    if (y0 < 0 || x0 < 0 || y0 + 64 > H || x0 + 64 > W) { pk = 0.0; break; }
+    poc_shift64(b, W, (int)x0, (int)y0, pc, alp, lpm, Hz, surf, red, res);
+    double sx = res[0], sy = res[1];
+    pk = res[2];
+    dx = ox + sx;
+    dy = oy + sy;
+    if (fabs(sx) < 0.5 && fabs(sy) < 0.5) break;
+  }
+  if (threadIdx.x == 0) {
+    oux[gi] = dx;
+    ouy[gi] = dy;
+    opeak[gi] = pk;
+  }
+}
+
 size_t poc_const_bytes() { return sizeof(PocConst); }
 
 // constants of a window: twiddles of length 64 and the Hann windows, rounded from float64 (poc.py:18-31)
@@ -358,6 +560,13 @@ void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const
     throw Error(OFC_ERR_ARG, "the CUDA engine's POC windows are 16, 32 or 64 px a side (poc_win <= 64)");
   // lp.mean(): the share of frequencies with |f| <= 0.25 on both axes
   double lpm = (double)(2 * (lv.wy / 4) + 1) * (double)(2 * (lv.wx / 4) + 1) / ((double)lv.wy * lv.wx);
+  if (lv.wy == 64 && lv.wx == 64) {
+    const size_t sm64 = (size_t)(64 * ZS + 33 * ZS) * sizeof(double2) + 64 * 64 * sizeof(double);
+    OFC_CUDA(cudaFuncSetAttribute((const void*)k_poc_grid64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64));
+    OFC_LAUNCH(k_poc_grid64, lv.nx * lv.ny, POC_T, sm64, st, a, b, lv.W, lv.H, xs, ys, lv.nx, iux, iuy,
+               (const PocConst*)dconst, lpm, ux, uy, peak);
+    return;
+  }
   size_t smem = (size_t)(lv.wy * (lv.wx + 1) + (2 * (lv.wy / 4) + 1) * (2 * (lv.wx / 4) + 1)) * sizeof(double2);
   OFC_CUDA(cudaFuncSetAttribute((const void*)k_poc_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   OFC_LAUNCH(k_poc_grid, lv.nx * lv.ny, POC_T, smem, st, a, b, lv.W, lv.H, lv.wy, lv.wx, xs, ys, lv.nx, iux, iuy,
