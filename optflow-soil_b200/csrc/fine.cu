@@ -713,15 +713,15 @@ __global__ void __launch_bounds__(128, 4) k_moments_y_rb(const double* __restric
   }
 }
 
-// x pass + solve: a block of 128 threads owns a row segment of SEG = 128 RX pixels. For each y-plane it stages
+// x pass + solve: a block of NT threads owns a row segment of SEG = NT RX pixels. For each y-plane it stages
 // the segment and its 2r halo in shared memory (double-buffered, the next plane's loads in flight meanwhile); a
 // thread takes the RX + 2r values around its RX consecutive pixels into registers (an odd RX keeps the warp's
 // reads on distinct banks) and writes their moments into a shared tile of nm x SEG (tap loop outermost, RX x
-// powers accumulators side by side); then each thread solves the pixels tid + 128 i from the tile.
+// powers accumulators side by side); then each thread solves the pixels tid + NT i from the tile.
 template <int ORDER>
 struct MomX {
   static constexpr int RX = ORDER == 1 ? 3 : 1;
-  static constexpr int NT = 128, SEG = NT * RX, WIN = SEG + 2 * MOM_R;
+  static constexpr int NT = 64, SEG = NT * RX, WIN = SEG + 2 * MOM_R;
   static constexpr size_t smem() { return (size_t)(2 * WIN + build_table(ORDER).nm * SEG) * sizeof(double); }
 };
 
@@ -796,7 +796,7 @@ __device__ __forceinline__ void mom_x_planes(const double* __restrict__ yplanes,
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(128, 2) k_moments_x_solve_rb(const double* __restrict__ yplanes,
+__global__ void __launch_bounds__(MomX<ORDER>::NT, 4) k_moments_x_solve_rb(const double* __restrict__ yplanes,
                                                                const double* __restrict__ uxin,
                                                                const double* __restrict__ uyin, int W, int H,
                                                                MomTaps tp, double* __restrict__ oux,
@@ -871,7 +871,8 @@ static void launch_moments_rb(const double* sums, const double* ux, const double
   OFC_CUDA(cudaFuncSetAttribute((const void*)k_moments_x_solve_rb<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sm));
   dim3 gx(div_up(W, MomX<ORDER>::SEG), H);
-  OFC_LAUNCH(k_moments_x_solve_rb<ORDER>, gx, 128, sm, st, yplanes, ux, uy, W, H, tp, oux, ouy, energy, resid, slope);
+  OFC_LAUNCH(k_moments_x_solve_rb<ORDER>, gx, MomX<ORDER>::NT, sm, st, yplanes, ux, uy, W, H, tp, oux, ouy, energy, resid,
+             slope);
 }
 
 void launch_moments_solve(const double* sums, const double* ux, const double* uy, int W, int H, int order,
