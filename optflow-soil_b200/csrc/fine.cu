@@ -959,6 +959,7 @@ __global__ void k_stats_decide(EnergyStats* s, int force, size_t n) {
   s->prefix = 0;
   s->rank = (long long)(n / 2);
   s->less = 0;
+  s->ticket = 0;
 }
 
 void launch_energy_stats(const double* energy, size_t n, EnergyStats* stats, bool force_median, cudaStream_t st) {
@@ -977,10 +978,17 @@ __device__ __forceinline__ void digit_of(int pass, int& shift, int& bits) {
   shift = hi - bits;
 }
 
-__global__ void k_radix_hist(const double* __restrict__ e, size_t n, const EnergyStats* s, int pass,
-                             unsigned long long* __restrict__ hist) {
+// One pass: a block histogram of the digit over the elements that match the prefix, added to hist; the last block
+// to finish (a ticket taken after a fence) scans hist, finds the bin holding rank, extends the prefix and clears
+// hist for the next pass.
+constexpr int RH_T = 512;
+
+__global__ void __launch_bounds__(RH_T) k_radix_hist(const double* __restrict__ e, size_t n, EnergyStats* s, int pass,
+                                                    unsigned long long* hist) {
   if (!s->need_median || s->nan) return;
   __shared__ unsigned int h[RBINS];
+  __shared__ long long wsum[RH_T / 32];
+  __shared__ bool last;
   for (int i = threadIdx.x; i < RBINS; i += blockDim.x) h[i] = 0;
   __syncthreads();
   int shift, bits;
@@ -995,23 +1003,23 @@ __global__ void k_radix_hist(const double* __restrict__ e, size_t n, const Energ
   __syncthreads();
   for (int i = threadIdx.x; i < RBINS; i += blockDim.x)
     if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
-}
-
-__global__ void __launch_bounds__(1024) k_radix_pick(EnergyStats* s, int pass, unsigned long long* hist, size_t n) {
-  // one block of 1024 threads: a block scan of the bin counts (4 bins per thread); the thread whose range
-  // holds rank finds the bin; then the histogram is cleared for the next pass
-  if (!s->need_median || s->nan) return;
-  __shared__ long long wsum[32];
-  constexpr int per = RBINS / 1024;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&s->ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // the pick: a block scan of the bin counts (RBINS / RH_T bins per thread)
+  constexpr int per = RBINS / RH_T;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   long long c[per];
   long long loc = 0;
 #pragma unroll
   for (int j = 0; j < per; j++) {
-    c[j] = (long long)hist[tid * per + j];
+    c[j] = (long long)__ldcg(hist + tid * per + j);
     loc += c[j];
   }
-  long long inc = loc;  // inclusive scan within the warp
+  long long inc = loc;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     long long v = __shfl_up_sync(0xffffffffu, inc, o);
@@ -1020,13 +1028,13 @@ __global__ void __launch_bounds__(1024) k_radix_pick(EnergyStats* s, int pass, u
   if (lane == 31) wsum[wid] = inc;
   __syncthreads();
   if (wid == 0) {
-    long long w = wsum[lane];
+    long long w = lane < RH_T / 32 ? wsum[lane] : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       long long v = __shfl_up_sync(0xffffffffu, w, o);
       if (lane >= o) w += v;
     }
-    wsum[lane] = w;  // inclusive over warps
+    if (lane < RH_T / 32) wsum[lane] = w;
   }
   __syncthreads();
   const long long excl = inc - loc + (wid ? wsum[wid - 1] : 0);
@@ -1042,14 +1050,13 @@ __global__ void __launch_bounds__(1024) k_radix_pick(EnergyStats* s, int pass, u
       }
       acc += c[j];
     }
-    int shift, bits;
-    digit_of(pass, shift, bits);
     s->prefix |= ((unsigned long long)bin) << shift;
     s->rank = rank - acc;
     s->less += acc;
   }
 #pragma unroll
   for (int j = 0; j < per; j++) hist[tid * per + j] = 0;
+  if (tid == 0) s->ticket = 0;
 }
 
 // after the passes: prefix = key of the element of rank n/2; for even n the one of rank n/2 - 1 is
@@ -1086,8 +1093,7 @@ __global__ void k_median_final(EnergyStats* s, size_t n) {
 
 void launch_median(const double* energy, size_t n, EnergyStats* stats, unsigned long long* hist, cudaStream_t st) {
   for (int pass = 0; pass < RPASSES; pass++) {
-    OFC_LAUNCH(k_radix_hist, 296, 512, 0, st, energy, n, stats, pass, hist);
-    OFC_LAUNCH(k_radix_pick, 1, 1024, 0, st, stats, pass, hist, n);
+    OFC_LAUNCH(k_radix_hist, 296, RH_T, 0, st, energy, n, stats, pass, hist);
   }
   OFC_LAUNCH(k_median_init, 1, 1, 0, st, stats);
   OFC_LAUNCH(k_median_lo, 296, 256, 0, st, energy, n, stats);

@@ -51,6 +51,7 @@ struct EnergyStats {
   long long rank;
   long long less;
   double lo_val;
+  unsigned int ticket;  // blocks of the current histogram pass that are done (the last one picks)
 };
 void launch_energy_stats(const double* energy, size_t n, EnergyStats* stats, bool force_median, cudaStream_t st);
 // median of energy into stats->median (np.median), skipped when stats->need_median == 0;

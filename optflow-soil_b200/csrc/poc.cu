@@ -587,44 +587,51 @@ __device__ double median_small(double* v, int n) {  // np.median of n <= 8 value
   return n % 2 ? v[n / 2] : (v[n / 2 - 1] + v[n / 2]) / 2.0;
 }
 
-__global__ void k_poc_clean(double* ux, double* uy, double* peak, int nx, int ny, double peak_min, double thresh,
-                            const double* fbx, const double* fby, uint8_t* flags) {
+// valid = peak >= peak_min; out = valid and not a normalised-median outlier among its valid 8-neighbours
+// (poc.py:101-121); one thread per grid point
+__global__ void k_poc_outliers(const double* __restrict__ ux, const double* __restrict__ uy,
+                               const double* __restrict__ peak, int nx, int ny, double peak_min, double thresh,
+                               uint8_t* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nx * ny) return;
+  const int di[8] = {-1, -1, -1, 0, 0, 1, 1, 1}, dj[8] = {-1, 0, 1, -1, 1, -1, 0, 1};
+  const int i = p / nx, j = p - i * nx;
+  uint8_t o = peak[p] >= peak_min;
+  if (o) {
+    double vx[8], vy[8];
+    int c = 0;
+    for (int k = 0; k < 8; k++) {
+      int a = i + di[k], b = j + dj[k];
+      if (a >= 0 && a < ny && b >= 0 && b < nx && peak[a * nx + b] >= peak_min) {
+        vx[c] = ux[a * nx + b];
+        vy[c] = uy[a * nx + b];
+        c++;
+      }
+    }
+    if (c >= 3) {
+      for (int comp = 0; comp < 2; comp++) {
+        double* vals = comp == 0 ? vx : vy;
+        double self = comp == 0 ? ux[p] : uy[p];
+        double med = median_small(vals, c);
+        double dev[8];
+        for (int k = 0; k < c; k++) dev[k] = fabs(vals[k] - med);
+        double res = median_small(dev, c);
+        if (fabs(self - med) / (res + 0.1) > thresh) o = 0;
+      }
+    }
+  }
+  out[p] = o;
+}
+
+// the rest of clean (poc.py:122-140) in one thread block: no point left -> the fallback; else fill passes from
+// the 8-neighbour medians until every point is set; invalid peaks -> 0
+__global__ void k_poc_fill(double* ux, double* uy, double* peak, int nx, int ny, double peak_min, const double* fbx,
+                           const double* fby, uint8_t* flags) {
   const int n = nx * ny;
-  uint8_t* valid = flags;
   uint8_t* out = flags + n;
   uint8_t* nw = flags + 2 * n;
   __shared__ int any, all;
   const int di[8] = {-1, -1, -1, 0, 0, 1, 1, 1}, dj[8] = {-1, 0, 1, -1, 1, -1, 0, 1};
-  for (int p = threadIdx.x; p < n; p += blockDim.x) valid[p] = peak[p] >= peak_min;
-  __syncthreads();
-  for (int p = threadIdx.x; p < n; p += blockDim.x) {
-    int i = p / nx, j = p - i * nx;
-    uint8_t o = valid[p];
-    if (o) {
-      double vx[8], vy[8];
-      int c = 0;
-      for (int k = 0; k < 8; k++) {
-        int a = i + di[k], b = j + dj[k];
-        if (a >= 0 && a < ny && b >= 0 && b < nx && valid[a * nx + b]) {
-          vx[c] = ux[a * nx + b];
-          vy[c] = uy[a * nx + b];
-          c++;
-        }
-      }
-      if (c >= 3) {
-        for (int comp = 0; comp < 2; comp++) {
-          double* vals = comp == 0 ? vx : vy;
-          double self = comp == 0 ? ux[p] : uy[p];
-          double med = median_small(vals, c);
-          double dev[8];
-          for (int k = 0; k < c; k++) dev[k] = fabs(vals[k] - med);
-          double res = median_small(dev, c);
-          if (fabs(self - med) / (res + 0.1) > thresh) o = 0;
-        }
-      }
-    }
-    out[p] = o;
-  }
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
   for (int p = threadIdx.x; p < n; p += blockDim.x)
@@ -670,12 +677,14 @@ __global__ void k_poc_clean(double* ux, double* uy, double* peak, int nx, int ny
     __syncthreads();
   }
   for (int p = threadIdx.x; p < n; p += blockDim.x)
-    if (!valid[p]) peak[p] = 0.0;
+    if (!(peak[p] >= peak_min)) peak[p] = 0.0;
 }
 
 void launch_poc_clean(double* ux, double* uy, double* peak, int nx, int ny, double peak_min, double thresh,
                       const double* fbx, const double* fby, uint8_t* scratch, cudaStream_t st) {
-  OFC_LAUNCH(k_poc_clean, 1, 1024, 0, st, ux, uy, peak, nx, ny, peak_min, thresh, fbx, fby, scratch);
+  const int n = nx * ny;
+  OFC_LAUNCH(k_poc_outliers, div_up(n, 128), 128, 0, st, ux, uy, peak, nx, ny, peak_min, thresh, scratch + n);
+  OFC_LAUNCH(k_poc_fill, 1, 1024, 0, st, ux, uy, peak, nx, ny, peak_min, fbx, fby, scratch);
 }
 
 // ---------------------------------------------------------------- grid sampling (poc.py:143-161)
