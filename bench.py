@@ -116,11 +116,11 @@ def accumulate_bytes(W, H, F=12):
     return N * (16 * F + 32 + 16 + 56) + Np * 8 * F
 
 
-# DRAM traffic of one k_accumulate launch over its algorithmic bytes, from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum = 404.4 MB against 424.0 MB algorithmic on a 1024^2 pair,
-# profiles/k_accumulate_1024.txt); the traffic of a launch at another size is this ratio times its
-# algorithmic bytes (both grow with the pixel and padded-pixel counts)
-ACC_TRAFFIC_RATIO = 404.4 / 424.0
+# DRAM traffic of one k_accumulate launch over its algorithmic bytes, from one ncu capture on the 2048^2 pair
+# (dram__bytes_read.sum + dram__bytes_write.sum = 1640.1 MB against 1669.7 MB algorithmic,
+# profiles/k_accumulate_2048.txt); at another size the traffic is this ratio times its algorithmic bytes (both
+# grow with the pixel and padded-pixel counts)
+ACC_TRAFFIC_RATIO = 1640.1 / 1669.7
 
 
 def cpu_sample(a, b, roi, n=512):
@@ -317,7 +317,7 @@ def main():
             roof = {"bound": "hbm", "kernel": "k_accumulate", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": peak_kind,
                     "traffic": ACC_TRAFFIC_RATIO * byts,
-                    "traffic_source": "ncu capture at 1024^2 scaled by algorithmic bytes",
+                    "traffic_source": "ncu capture of this kernel on the 2048^2 pair (ratio to algorithmic bytes)",
                     "algorithmic_bytes_per_launch": byts, "launch_ms": per_launch_s * 1e3,
                     "launches_per_step": acc[0] / args.steps}
         base = None
