@@ -17,6 +17,9 @@
 #include "fft.cuh"
 
 #include <cmath>
+#include <type_traits>
+
+#include <cuda_pipeline.h>
 
 namespace ofc {
 
@@ -436,8 +439,9 @@ __device__ __forceinline__ void fft_stage(const C2* __restrict__ A, C2* __restri
 }
 
 // runs the plan on buf (tmp: scratch of the same capacity, fft_buf_len(L, C)); buf holds the input unpadded
-// and the returned buffer the result unpadded
-template <int C, class C2>
+// and the returned buffer the result unpadded. FIXL > 0: the length is FIXL and the plan is fixed at compile time
+// (kernels are instantiated per FIXL, so that a fixed-length kernel carries no runtime-plan code and its registers).
+template <int FIXL, int C, class C2>
 __device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
   static_assert(C == 1 || C == 2 || C == 4, "C: a power of two up to 4");
   static_assert(sizeof(C2) == sizeof(float2), "float32 transforms");
@@ -445,8 +449,7 @@ __device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
   C2* b = tmp;
   const C2* tw = (const C2*)pl.tw;
   constexpr int lc = C == 4 ? 2 : (C == 2 ? 1 : 0);
-  // the padded length of 2048-wide images (2112 = 8 8 3 11) runs with its plan fixed at compile time
-  if (pl.L == 2112) return fft_run_fixed<2112, C, 0, C2>(buf, tmp, tw, inv);
+  if constexpr (FIXL > 0) return fft_run_fixed<FIXL, C, 0, C2>(buf, tmp, tw, inv);
   int ish = 31;
   for (int st = 0; st < pl.nst; st++) {
     const int osh = (st + 1 < pl.nst && pl.s[st] * C < 32) ? FFT_PAD : 31;
@@ -457,6 +460,20 @@ __device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
     b = t;
   }
   return a;
+}
+
+// z^e, 0 <= e < 64, of the B-spline pole z = sqrt(3) - 2 (interp.py:9): the product of its binary powers z^(2^b),
+// formed in float64 at compile time and rounded once
+constexpr double BZ1 = -0.26794919243112270, BZ2 = BZ1 * BZ1, BZ4 = BZ2 * BZ2, BZ8 = BZ4 * BZ4, BZ16 = BZ8 * BZ8,
+                 BZ32 = BZ16 * BZ16;
+__device__ __forceinline__ float zpow(int e) {
+  float r = (e & 1) ? (float)BZ1 : 1.f;
+  r *= (e & 2) ? (float)BZ2 : 1.f;
+  r *= (e & 4) ? (float)BZ4 : 1.f;
+  r *= (e & 8) ? (float)BZ8 : 1.f;
+  r *= (e & 16) ? (float)BZ16 : 1.f;
+  r *= (e & 32) ? (float)BZ32 : 1.f;
+  return r;
 }
 
 // Cubic B-spline prefilter (interp.py:13-27, without the factor 6, which the caller folds into its scale) of C
@@ -471,9 +488,9 @@ __device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
 // z^32 < 1e-18 (lines here are at least 65 long, so the terms of the two ends never meet). scratch: 2 C float4.
 template <int C>
 __device__ void bspline_edges(float2* buf, int n, float4* scratch) {
-  const float z = (float)bspline_z();
-  const float g = (float)(bspline_z() / (bspline_z() * bspline_z() - 1.0));
-  const float q = (float)(1.0 / (1.0 - bspline_z() * bspline_z()));
+  const float z = (float)BZ1;
+  const float g = (float)(BZ1 / (BZ2 - 1.0));
+  const float q = (float)(1.0 / (1.0 - BZ2));
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   auto c = [&](int i, int l) { return buf[(i < 0 ? i + n : (i >= n ? i - n : i)) * C + l]; };
   auto xr = [&](int i, int l) {
@@ -482,8 +499,7 @@ __device__ void bspline_edges(float2* buf, int n, float4* scratch) {
   };
   for (int l = wid; l < C; l += (int)(blockDim.x >> 5)) {  // a warp per line: its two edge constants, lane k
     const int k = lane;                                       // taking the terms of z^k
-    float zk = 1.f;
-    for (int j = 0; j < k; j++) zk *= z;
+    const float zk = zpow(k);
     const int hz = min(n, HORIZON);
     float2 d0 = make_float2(0.f, 0.f);
     if (k < hz) {
@@ -513,15 +529,13 @@ __device__ void bspline_edges(float2* buf, int n, float4* scratch) {
     const int l = t % C, j = t / C;  // j < 32: the start of the line; j >= 32: its end
     const float4 k = scratch[l];
     if (j < 32) {
-      float zp = z;  // z^(i+1), i = j
-      for (int m = 0; m < j; m++) zp *= z;
+      const float zp = zpow(j + 1);  // z^(i+1), i = j
       float2& v = buf[j * C + l];
       v.x = fmaf(-k.x * q, zp, v.x);
       v.y = fmaf(-k.y * q, zp, v.y);
     } else {
       const int i = n - 64 + j;  // j = 32..63 -> i = n-32..n-1
-      float zp = 1.f;            // z^(n-1-i)
-      for (int m = 0; m < n - 1 - i; m++) zp *= z;
+      const float zp = zpow(n - 1 - i);
       float2& v = buf[i * C + l];
       v.x = fmaf(k.z, zp, v.x);
       v.y = fmaf(k.w, zp, v.y);
@@ -540,36 +554,43 @@ __device__ __forceinline__ int reflect_near(int i, int n) {
 
 // ---------------------------------------------------------------- kernels
 // Every kernel stages its lines in buffers of fft_buf_len(L, C) values (the transforms' padded layouts); the
-// prefilter's carries live in the buffer the transform left idle.
+// prefilter's carries live in the buffer the transform left idle. The kernels are instantiated for FIXL = 0 (any
+// supported length, the plan read at run time) and FIXL = FFT_FIXED_L (2112 = 8 8 3 11, the padded length of
+// 2048-wide images, the plan fixed at compile time); the launchers pick by the plan's length.
+constexpr int FFT_FIXED_L = 2112;
 
+// buffer stride of the kernels that stage several lines: fft_buf_len rounded up to an even count (16-byte aligned)
+__host__ __device__ constexpr int fft_buf_stride(int L, int C) { return (fft_buf_len(L, C) + 1) & ~1; }
+
+template <int FIXL>
 __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_fwd_real(const float* __restrict__ img, int W, int H,
                                                                   FftPlan plw, int ph, float2* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* sm = (float2*)smraw;
-  const int pw = plw.L;
+  const int pw = FIXL ? FIXL : plw.L;
   float2* t = sm + fft_buf_len(pw, 1);
   const int yp = blockIdx.x;
   const int ys = reflect_near(yp - PAD, H);
   const float* row = img + (size_t)ys * W;
   for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[x] = make_float2(__ldg(row + reflect_near(x - PAD, W)), 0.f);
   __syncthreads();
-  float2* r = fft_run<1>(sm, t, plw, false);
+  float2* r = fft_run<FIXL, 1>(sm, t, plw, false);
   float2* o = out + (size_t)yp * pw;
   for (int x = threadIdx.x; x < pw; x += blockDim.x) o[x] = r[x];
 }
 
 // The column pass of the responses in two kernels, so that a block holds only two buffers of C columns
 // (several blocks per SM instead of one): k_fft_cols_fwd writes the column spectrum S (ph x pw, row-major,
-// small enough to stay in L2), then k_fft_cols_inv_filter, one block per (C columns, filter k), multiplies S by
-// G_k, inverts along y and prefilters along y into plane k of U.
-constexpr int COLS_TMAX = 320;  // threads per block of the split column pass (3 blocks per SM: <= 64 registers)
+// small enough to stay in L2), then the inverse pass (k_fft_cols_pair, or k_fft_cols_inv_filter where the column
+// pair does not fit beside the two buffers) multiplies S by the factors of each plane, inverts along y and stores.
+constexpr int COLS_TMAX = 320;  // threads per block of the split column pass
 
-template <int C>
+template <int C, int FIXL>
 __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_fwd(const float2* Tin, FftPlan plh, int pw, float2* S) {
   constexpr int LC = C == 4 ? 2 : (C == 2 ? 1 : 0);
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* A = (float2*)smraw;
-  const int ph = plh.L, n = ph * C;
+  const int ph = FIXL ? FIXL : plh.L, n = ph * C;
   float2* B = A + fft_buf_len(ph, C);
   const int x0 = blockIdx.x * C;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -577,17 +598,97 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_fwd(const float2* Tin
     A[i] = x < pw ? Tin[(size_t)y * pw + x] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  float2* r = fft_run<C>(A, B, plh, false);
+  float2* r = fft_run<FIXL, C>(A, B, plh, false);
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     int y = i >> LC, x = x0 + (i & (C - 1));
     if (x < pw) S[(size_t)y * pw + x] = r[i];
   }
 }
 
-// REFPACK = false: the responses (filter k = blockIdx.y: S G_k, inverse, prefilter along y) into plane k of U.
-// REFPACK = true: the reference pack of filters [k0, k0 + gridDim.y / 3): blockIdx.y = 3 (k - k0) + v with the
-// planes S G, S G i fx, S G i fy for v = 0, 1, 2 (factors formed in float64), inverse, no prefilter, into plane
-// blockIdx.y of U.
+// The inverse column pass with the spectrum of a column pair staged once per block: the block copies its two
+// columns of S (ph x 2) into shared memory, then for each of its planes multiplies them by the plane's factor into
+// A, inverts along y (A, B) and stores the pair. REFPACK = false: the responses of the filters
+// [RESP_G blockIdx.y, RESP_G (blockIdx.y + 1)) (x G_k and the B-spline prefilter's periodic factors, inverse,
+// the prefilter's edge terms along y) into plane k of U. REFPACK = true: variant v = blockIdx.y of the reference
+// pack (S G, S G i fx, S G i fy; factors in float64) of the filters [k0, k1) into plane 3 (k - k0) + v of U.
+// A thread's column is fixed (blockDim is even), so the x factors are read once.
+constexpr int RESP_G = 4;
+template <bool REFPACK, int FIXL>
+__global__ void __launch_bounds__(COLS_TMAX, 2) k_fft_cols_pair(const float2* __restrict__ S, FftPlan plh, int pw,
+                                                                GaborTables g, int k0, int k1, float2* __restrict__ U) {
+  constexpr int C = 2;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int ph = FIXL ? FIXL : plh.L, n = ph * C, tid = threadIdx.x, nt = blockDim.x;
+  float2* raw = (float2*)smraw;
+  float2* A = raw + n;
+  float2* B = A + fft_buf_stride(ph, C);
+  const int x0 = blockIdx.x * C;
+  const bool rows16 = x0 + 1 < pw && pw % 2 == 0;  // each row of the pair is 16 bytes on a 16-byte boundary
+  if (rows16) {
+    for (int y = tid; y < ph; y += nt) __pipeline_memcpy_async(raw + 2 * y, S + (size_t)y * pw + x0, 16);
+    __pipeline_commit();
+    __pipeline_wait_prior(0);
+  } else {
+    for (int i = tid; i < n; i += nt) {
+      const int y = i >> 1, x = x0 + (i & 1);
+      raw[i] = x < pw ? S[(size_t)y * pw + x] : make_float2(0.f, 0.f);
+    }
+  }
+  __syncthreads();
+  const int x = min(x0 + (tid & 1), pw - 1);
+  auto store = [&](const float2* r, int plane) {
+    float2* dst = U + (size_t)plane * ph * pw + x0;
+    if (rows16) {
+      for (int y = tid; y < ph; y += nt) *(float4*)(dst + (size_t)y * pw) = *(const float4*)(r + 2 * y);
+    } else {
+      for (int i = tid; i < n; i += nt)
+        if (x0 + (i & 1) < pw) dst[(size_t)(i >> 1) * pw + (i & 1)] = r[i];
+    }
+  };
+  if (!REFPACK) {
+    const float hx = __ldg(g.hxf + x), omx = __ldg(g.omxf + x), bx = __ldg(g.bxf + x);
+    const int kend = min(g.F, (int)(blockIdx.y + 1) * RESP_G);
+    for (int k = blockIdx.y * RESP_G; k < kend; k++) {
+      const float ex = __ldg(g.exf + (size_t)k * pw + x);
+      const float* eyk = g.eyf + (size_t)k * ph;
+      for (int i = tid; i < n; i += nt) {
+        const int y = i >> 1;
+        const float2 sv = raw[i];
+        const float G = fmaf(hx, __ldg(g.omyf + y), omx) * (ex * __ldg(eyk + y)) * (bx * __ldg(g.byf + y));
+        A[i] = make_float2(sv.x * G, sv.y * G);
+      }
+      __syncthreads();
+      float2* r = fft_run<FIXL, C>(A, B, plh, true);
+      float2* idle = r == A ? B : A;
+      bspline_edges<C>(r, ph, (float4*)idle);  // the prefilter's edge terms along y
+      store(r, k);
+      __syncthreads();
+    }
+  } else {
+    const int v = blockIdx.y;
+    const double hx = g.hx[x], omx = g.omx[x], fx = g.fx[x];
+    for (int k = k0; k < k1; k++) {
+      const double ex = g.ex[(size_t)k * pw + x];
+      const double* eyk = g.ey + (size_t)k * ph;
+      for (int i = tid; i < n; i += nt) {
+        const int y = i >> 1;
+        const float2 sv = raw[i];
+        const double G = fma(hx, g.omy[y], omx) * ex * eyk[y];
+        double re = sv.x * G, im = sv.y * G;
+        if (v == 1) { const double t = re; re = -im * fx; im = t * fx; }                 // x i fx
+        else if (v == 2) { const double f = g.fy[y]; const double t = re; re = -im * f; im = t * f; }  // x i fy
+        A[i] = make_float2((float)re, (float)im);
+      }
+      __syncthreads();
+      float2* r = fft_run<FIXL, C>(A, B, plh, true);
+      store(r, 3 * (k - k0) + v);
+      __syncthreads();
+    }
+  }
+}
+
+// The same inverse column pass with one block per (C columns, plane) and no staged spectrum: the form for padded
+// heights whose column pair does not fit in shared memory beside the two transform buffers.
 template <int C, bool REFPACK>
 __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const float2* __restrict__ S, FftPlan plh, int pw,
                                                                       GaborTables g, int k0, float2* __restrict__ U) {
@@ -619,7 +720,7 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const floa
     }
   }
   __syncthreads();
-  float2* r = fft_run<C>(A, B, plh, true);
+  float2* r = fft_run<0, C>(A, B, plh, true);
   if (!REFPACK) {
     float2* idle = r == A ? B : A;
     bspline_edges<C>(r, ph, (float4*)(((uintptr_t)idle + 15) & ~(uintptr_t)15));  // the prefilter's edge terms along y
@@ -631,30 +732,60 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const floa
   }
 }
 
-__global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int ph,
-                                                                  float scale, float2* __restrict__ R) {
-  extern __shared__ float2 sm[];
-  const int pw = plw.L;
-  float2* t = sm + fft_buf_len(pw, 1);
-  const int y = blockIdx.x, k = blockIdx.y;
-  const size_t off = (size_t)k * ph * pw + (size_t)y * pw;
-  for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[x] = U[off + x];
-  __syncthreads();
-  float2* r = fft_run<1>(sm, t, plw, true);
-  float2* idle = r == sm ? t : sm;
-  bspline_edges<1>(r, pw, (float4*)(((uintptr_t)idle + 15) & ~(uintptr_t)15));  // the prefilter's edge terms along x
-  for (int x = threadIdx.x; x < pw; x += blockDim.x) {
-    float2 v = r[x];
-    R[off + x] = make_float2(v.x * scale, v.y * scale);
+// Inverse row transforms of the filtered spectra, persistent: a block walks the lines blockIdx.x, + gridDim.x, ...
+// (line = k ph + y of the F planes) and copies the next line into a third buffer (cp.async) while it transforms the
+// current one; then the prefilter's edge terms along x and the scale 36 / (ph pw).
+template <int FIXL>
+__global__ void __launch_bounds__(FIXL ? 288 : FFT_TMAX, FIXL ? 3 : 2)
+    k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int nlines, float scale, float2* __restrict__ R) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int L = FIXL ? FIXL : plw.L, nb = fft_buf_stride(L, 1);
+  float2* in = (float2*)smraw;
+  float2* tmp = in + nb;
+  float2* pre = tmp + nb;
+  auto prefetch = [&](int line, float2* dst) {
+    const float2* src = U + (size_t)line * L;
+    if (L % 2 == 0) {  // 16-byte chunks: the line starts on a 16-byte boundary
+      for (int i = threadIdx.x; i < L / 2; i += blockDim.x) __pipeline_memcpy_async(dst + 2 * i, src + 2 * i, 16);
+    } else {
+      for (int i = threadIdx.x; i < L; i += blockDim.x) __pipeline_memcpy_async(dst + i, src + i, 8);
+    }
+    __pipeline_commit();
+  };
+  int line = blockIdx.x;
+  if (line < nlines) prefetch(line, in);
+  for (; line < nlines; line += gridDim.x) {
+    const int nxt = line + gridDim.x;
+    if (nxt < nlines) {
+      prefetch(nxt, pre);
+      __pipeline_wait_prior(1);
+    } else {
+      __pipeline_wait_prior(0);
+    }
+    __syncthreads();
+    float2* r = fft_run<FIXL, 1>(in, tmp, plw, true);
+    float2* idle = r == in ? tmp : in;
+    bspline_edges<1>(r, L, (float4*)idle);  // the prefilter's edge terms along x
+    float2* o = R + (size_t)line * L;
+    for (int x = threadIdx.x; x < L; x += blockDim.x) {
+      const float2 v = r[x];
+      o[x] = make_float2(v.x * scale, v.y * scale);
+    }
+    __syncthreads();
+    float2* done = in;
+    in = pre;
+    pre = tmp;
+    tmp = done;
   }
 }
 
+template <int FIXL>
 __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_ref(const float2* __restrict__ U, FftPlan plw, int ph, int W,
                                                                int H, int k0, float4* __restrict__ ref4,
                                                                float* __restrict__ amp) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* sm = (float2*)smraw;
-  const int pw = plw.L, nb = fft_buf_len(pw, 1);
+  const int pw = FIXL ? FIXL : plw.L, nb = fft_buf_len(pw, 1);
   float2* t = sm + 3 * nb;
   const int y = blockIdx.x, kk = blockIdx.y, k = k0 + kk;  // y: row of the W x H crop
   const size_t plane = (size_t)ph * pw;
@@ -665,7 +796,7 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_ref(const float2* 
   __syncthreads();
   float2* rr[3];
   for (int v = 0; v < 3; v++) {
-    float2* res = fft_run<1>(sm + v * nb, t, plw, true);
+    float2* res = fft_run<FIXL, 1>(sm + v * nb, t, plw, true);
     if (res != sm + v * nb) {
       for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[v * nb + x] = res[x];
       __syncthreads();
@@ -688,13 +819,15 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_ref(const float2* 
   }
 }
 
+template <int FIXL>
 __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_lines(float2* data, FftPlan pl, int inv) {
   extern __shared__ float2 sm[];
-  float2* row = data + (size_t)blockIdx.x * pl.L;
-  for (int x = threadIdx.x; x < pl.L; x += blockDim.x) sm[x] = row[x];
+  const int L = FIXL ? FIXL : pl.L;
+  float2* row = data + (size_t)blockIdx.x * L;
+  for (int x = threadIdx.x; x < L; x += blockDim.x) sm[x] = row[x];
   __syncthreads();
-  float2* r = fft_run<1>(sm, sm + fft_buf_len(pl.L, 1), pl, inv != 0);
-  for (int x = threadIdx.x; x < pl.L; x += blockDim.x) row[x] = r[x];
+  float2* r = fft_run<FIXL, 1>(sm, sm + fft_buf_len(L, 1), pl, inv != 0);
+  for (int x = threadIdx.x; x < L; x += blockDim.x) row[x] = r[x];
 }
 
 // ---------------------------------------------------------------- launchers
@@ -712,12 +845,32 @@ static size_t smem_prefilter(int L, int C, int T) {
   (void)T;
   return std::max<size_t>(2 * fbytes(L, C), fbytes(L, C) + 16 + (size_t)C * sizeof(float4));
 }
+// k_fft_cols_pair: the column pair and two buffers at the even stride
+static size_t smem_cols_pair(int L) { return ((size_t)2 * L + 2 * (size_t)fft_buf_stride(L, 2)) * sizeof(float2); }
+// k_fft_rows_inv_resp: three buffers at the even stride
+static size_t smem_rows_resp(int L) { return 3 * (size_t)fft_buf_stride(L, 1) * sizeof(float2); }
+
+// calls f with std::integral_constant<int, FIXL> for the kernels' instantiation of length L
+template <class Fn>
+static void by_length(int L, Fn f) {
+  if (L == FFT_FIXED_L) f(std::integral_constant<int, FFT_FIXED_L>{});
+  else f(std::integral_constant<int, 0>{});
+}
+
+// blocks of a persistent launch: as many as are resident at once, at most one per unit of work
+static int persistent_blocks(const void* fn, int threads, size_t smem, int work) {
+  int dev = 0, sms = 0, per = 0;
+  OFC_CUDA(cudaGetDevice(&dev));
+  OFC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  OFC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem));
+  return std::max(1, std::min(work, std::max(per, 1) * sms));
+}
 
 bool fft_fits(int ph, int pw) {
   try {
     int Tc = std::min(fft_threads(ph, 2), COLS_TMAX);
     if (smem_prefilter(ph, 2, Tc) > SMEM_MAX) return false;
-    return 4 * fbytes(pw, 1) <= SMEM_MAX && smem_prefilter(pw, 1, fft_threads(pw, 1)) <= SMEM_MAX;
+    return 4 * fbytes(pw, 1) <= SMEM_MAX && smem_rows_resp(pw) <= SMEM_MAX;
   } catch (const Error&) {
     return false;
   }
@@ -726,68 +879,98 @@ bool fft_fits(int ph, int pw) {
 void launch_fft_rows_fwd_real(const float* img, int W, int H, const FftPlan& plw, int ph, float2* out, cudaStream_t st) {
   int T = fft_threads(plw.L, 1);
   size_t sm = 2 * fbytes(plw.L, 1);
-  set_smem((const void*)k_fft_rows_fwd_real, sm);
-  OFC_LAUNCH(k_fft_rows_fwd_real, ph, T, sm, st, img, W, H, plw, ph, out);
+  by_length(plw.L, [&](auto fl) {
+    constexpr int FL = decltype(fl)::value;
+    set_smem((const void*)k_fft_rows_fwd_real<FL>, sm);
+    OFC_LAUNCH(k_fft_rows_fwd_real<FL>, ph, T, sm, st, img, W, H, plw, ph, out);
+  });
 }
 
-void launch_fft_cols_filters(float2* T, const FftPlan& plh, int pw, const GaborTables& g, float2* U, cudaStream_t st) {
+static void cols_fwd(float2* T, const FftPlan& plh, int pw, cudaStream_t st) {
   constexpr int C = 2;
   const int ph = plh.L;
   int nt = std::min(fft_threads(ph, C), COLS_TMAX);
   size_t sm_f = 2 * fbytes(ph, C);
-  size_t sm_i = smem_prefilter(ph, C, nt);
-  if (sm_i > SMEM_MAX) throw Error(OFC_ERR_WINDOW, "padded height " + std::to_string(ph) + " too large for the column pass");
-  set_smem((const void*)k_fft_cols_fwd<C>, sm_f);
-  set_smem((const void*)k_fft_cols_inv_filter<C, false>, sm_i);
   // in place: a block reads its C columns whole before it writes their spectrum back
-  OFC_LAUNCH(k_fft_cols_fwd<C>, div_up(pw, C), nt, sm_f, st, T, plh, pw, T);
-  dim3 grid(div_up(pw, C), g.F);
-  OFC_LAUNCH((k_fft_cols_inv_filter<C, false>), grid, nt, sm_i, st, T, plh, pw, g, 0, U);
+  by_length(ph, [&](auto fl) {
+    constexpr int FL = decltype(fl)::value;
+    set_smem((const void*)k_fft_cols_fwd<C, FL>, sm_f);
+    OFC_LAUNCH((k_fft_cols_fwd<C, FL>), div_up(pw, C), nt, sm_f, st, T, plh, pw, T);
+  });
+}
+
+// the inverse column pass of the responses (REFPACK false, planes = filters) or of the reference pack's filters
+// [k0, k1) (planes = 3 (k1 - k0))
+template <bool REFPACK>
+static void cols_inverse(const float2* S, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1, float2* U,
+                         cudaStream_t st) {
+  constexpr int C = 2;
+  const int ph = plh.L;
+  int nt = std::min(fft_threads(ph, C), COLS_TMAX);
+  const size_t sm_p = smem_cols_pair(ph);
+  if (sm_p <= SMEM_MAX) {
+    dim3 grid(div_up(pw, C), REFPACK ? 3 : div_up(g.F, RESP_G));
+    by_length(ph, [&](auto fl) {
+      constexpr int FL = decltype(fl)::value;
+      set_smem((const void*)k_fft_cols_pair<REFPACK, FL>, sm_p);
+      if constexpr (REFPACK) OFC_LAUNCH((k_fft_cols_pair<true, FL>), grid, nt, sm_p, st, S, plh, pw, g, k0, k1, U);
+      else OFC_LAUNCH((k_fft_cols_pair<false, FL>), grid, nt, sm_p, st, S, plh, pw, g, k0, k1, U);
+    });
+    return;
+  }
+  size_t sm_i = REFPACK ? 2 * fbytes(ph, C) : smem_prefilter(ph, C, nt);
+  if (sm_i > SMEM_MAX) throw Error(OFC_ERR_WINDOW, "padded height " + std::to_string(ph) + " too large for the column pass");
+  set_smem((const void*)k_fft_cols_inv_filter<C, REFPACK>, sm_i);
+  dim3 grid(div_up(pw, C), REFPACK ? 3 * (k1 - k0) : g.F);
+  if constexpr (REFPACK) OFC_LAUNCH((k_fft_cols_inv_filter<C, true>), grid, nt, sm_i, st, S, plh, pw, g, k0, U);
+  else OFC_LAUNCH((k_fft_cols_inv_filter<C, false>), grid, nt, sm_i, st, S, plh, pw, g, k0, U);
+}
+
+void launch_fft_cols_filters(float2* T, const FftPlan& plh, int pw, const GaborTables& g, float2* U, cudaStream_t st) {
+  cols_fwd(T, plh, pw, st);
+  cols_inverse<false>(T, plh, pw, g, 0, g.F, U, st);
 }
 
 void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F, float2* R, cudaStream_t st) {
   int T = fft_threads(plw.L, 1);
-  size_t sm = smem_prefilter(plw.L, 1, T);
-  set_smem((const void*)k_fft_rows_inv_resp, sm);
+  size_t sm = smem_rows_resp(plw.L);
   float scale = (float)(36.0 / ((double)ph * (double)plw.L));
-  dim3 grid(ph, F);
-  OFC_LAUNCH(k_fft_rows_inv_resp, grid, T, sm, st, U, plw, ph, scale, R);
+  const int nlines = F * ph;
+  by_length(plw.L, [&](auto fl) {
+    constexpr int FL = decltype(fl)::value;
+    const void* fn = (const void*)k_fft_rows_inv_resp<FL>;
+    set_smem(fn, sm);
+    OFC_LAUNCH(k_fft_rows_inv_resp<FL>, persistent_blocks(fn, T, sm, nlines), T, sm, st, U, plw, nlines, scale, R);
+  });
 }
 
-void launch_fft_cols_fwd(float2* T, const FftPlan& plh, int pw, cudaStream_t st) {
-  constexpr int C = 2;
-  const int ph = plh.L;
-  int nt = std::min(fft_threads(ph, C), COLS_TMAX);
-  size_t sm_f = 2 * fbytes(ph, C);
-  set_smem((const void*)k_fft_cols_fwd<C>, sm_f);
-  OFC_LAUNCH(k_fft_cols_fwd<C>, div_up(pw, C), nt, sm_f, st, T, plh, pw, T);
-}
+void launch_fft_cols_fwd(float2* T, const FftPlan& plh, int pw, cudaStream_t st) { cols_fwd(T, plh, pw, st); }
 
 void launch_fft_cols_ref_f32(const float2* S, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1,
                              float2* U, cudaStream_t st) {
-  constexpr int C = 2;
-  const int ph = plh.L;
-  int nt = std::min(fft_threads(ph, C), COLS_TMAX);
-  size_t sm = 2 * fbytes(ph, C);
-  set_smem((const void*)k_fft_cols_inv_filter<C, true>, sm);
-  dim3 grid(div_up(pw, C), 3 * (k1 - k0));
-  OFC_LAUNCH((k_fft_cols_inv_filter<C, true>), grid, nt, sm, st, S, plh, pw, g, k0, U);
+  cols_inverse<true>(S, plh, pw, g, k0, k1, U, st);
 }
 
 void launch_fft_rows_inv_ref_f32(const float2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,
                                  float4* ref4, float* amp, cudaStream_t st) {
   int T = fft_threads(plw.L, 1);
   size_t sm = 4 * fbytes(plw.L, 1);
-  set_smem((const void*)k_fft_rows_inv_ref, sm);
   dim3 grid(H, k1 - k0);
-  OFC_LAUNCH(k_fft_rows_inv_ref, grid, T, sm, st, U, plw, ph, W, H, k0, ref4, amp);
+  by_length(plw.L, [&](auto fl) {
+    constexpr int FL = decltype(fl)::value;
+    set_smem((const void*)k_fft_rows_inv_ref<FL>, sm);
+    OFC_LAUNCH(k_fft_rows_inv_ref<FL>, grid, T, sm, st, U, plw, ph, W, H, k0, ref4, amp);
+  });
 }
 
 void launch_fft_lines(float2* data, int lines, const FftPlan& pl, bool inverse, cudaStream_t st) {
   int T = fft_threads(pl.L, 1);
   size_t sm = 2 * fbytes(pl.L, 1);
-  set_smem((const void*)k_fft_lines, sm);
-  OFC_LAUNCH(k_fft_lines, lines, T, sm, st, data, pl, inverse ? 1 : 0);
+  by_length(pl.L, [&](auto fl) {
+    constexpr int FL = decltype(fl)::value;
+    set_smem((const void*)k_fft_lines<FL>, sm);
+    OFC_LAUNCH(k_fft_lines<FL>, lines, T, sm, st, data, pl, inverse ? 1 : 0);
+  });
 }
 
 }  // namespace ofc

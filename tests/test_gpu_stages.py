@@ -85,6 +85,57 @@ def test_responses(T, oracle, shape):
         assert err < 1e-4, (k, err)
 
 
+@pytest.mark.parametrize("shape", [(2048, 2048), (2048, 136), (136, 2048)])
+def test_responses_fixed_length(T, oracle, shape):
+    """Padded length 2112 (2048-pixel sides, the benchmark's size) runs the transforms' compile-time plan and the
+    staged column-pair / persistent row kernels; the mixed shapes pair it with a runtime plan on the other axis."""
+    rng = np.random.default_rng(7)
+    img = rng.random(shape).astype(np.float32)
+    cfg = Config()
+    got = T.responses(img, cfg)
+    pad = np.pad(img.astype(np.float64), 32, mode="reflect")
+    F2 = np.fft.fft2(pad)
+    bank = _gabor_bank_np(pad.shape, cfg)
+    for k in (0, 5, 11):
+        r = np.fft.ifft2(F2 * bank[k])
+        want = oracle.bspline_coeffs(r.real) + 1j * oracle.bspline_coeffs(r.imag)
+        err = np.abs(got[k] - want).max() / np.abs(want).max()
+        assert err < 1e-4, (shape, k, err)
+
+
+@pytest.mark.parametrize("shape", [(2048, 2048), (136, 2048)])
+def test_reference_phase_fixed_length(T, shape):
+    """reference_phase (phaseflow.py:92-112) at padded length 2112 against a float64 numpy restatement: the
+    response within 1e-4 of its largest |r|, the phase gradient within 1e-3 rad/px where the amplitude exceeds 5 %
+    of the largest (the tolerances of parity_gabor.rs:40-70)."""
+    rng = np.random.default_rng(8)
+    img = rng.random(shape).astype(np.float32)
+    cfg = Config()
+    got = T.reference_phase(img, cfg)
+    h, w = shape
+    pad = np.pad(img.astype(np.float64), 32, mode="reflect")
+    F2 = np.fft.fft2(pad)
+    fy = (np.fft.fftfreq(pad.shape[0]) * 2 * np.pi)[:, None]
+    fx = (np.fft.fftfreq(pad.shape[1]) * 2 * np.pi)[None, :]
+    bank = _gabor_bank_np(pad.shape, cfg)
+    crop = (slice(32, 32 + h), slice(32, 32 + w))
+    for k in (0, 7):
+        Z = F2 * bank[k]
+        r = np.fft.ifft2(Z)[crop]
+        rx = np.fft.ifft2(Z * 1j * fx)[crop]
+        ry = np.fft.ifft2(Z * 1j * fy)[crop]
+        a2 = np.abs(r) ** 2 + 1e-12
+        gx, gy = (np.conj(r) * rx).imag / a2, (np.conj(r) * ry).imag / a2
+        g_r, g_gx, g_gy, g_amp = got[k]
+        max_amp = np.abs(r).max()
+        assert np.abs(g_r - r).max() / max_amp < 1e-4
+        strong = np.sqrt(a2) > 0.05 * max_amp
+        assert strong.sum() > strong.size / 20
+        assert np.abs(g_gx - gx)[strong].max() < 1e-3
+        assert np.abs(g_gy - gy)[strong].max() < 1e-3
+        assert np.abs(g_amp - np.sqrt(a2))[strong].max() < 1e-4 * max_amp
+
+
 @pytest.mark.parametrize("order", [1, 2])
 def test_local_solve(T, oracle, order):
     rng = np.random.default_rng(order)
