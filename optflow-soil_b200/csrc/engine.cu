@@ -482,7 +482,7 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
   float* warped = L.get<float>("warped", N);
   float2* R = L.get<float2>("resp", Np * F);
   EnergyStats* stats = L.get<EnergyStats>("stats", 1);
-  unsigned long long* hist = L.get<unsigned long long>("hist", 4096);
+  unsigned long long* hist = L.get<unsigned long long>("hist", MEDIAN_SCRATCH);
   uint8_t* low = L.get<uint8_t>("low", N);
   uint8_t* frozen = L.get<uint8_t>("frozen", N);
   uint8_t* okm = L.get<uint8_t>("okmask", N);
@@ -531,8 +531,7 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
       launch_moments_solve(sums, ucur, ucur + N, W, H, c.shape_order, d_mt, rw, mtp, yplanes, unext, unext + N, energy,
                            resid, slope, st);
       const bool last_inner = in == c.inner_iters - 1;
-      launch_energy_stats(energy, N, stats, last_inner, st);
-      launch_median(energy, N, stats, hist, st);
+      launch_energy_median(energy, N, stats, last_inner, hist, st);
       launch_reset(energy, ucur, ucur + N, (int)N, stats, unext, unext + N, resid, slope, st);
       std::swap(ucur, unext);
     }
@@ -1302,11 +1301,10 @@ int ofc_test_local_solve(ofc_engine* e, const double* sums, const double* ux, co
     double* sl = L.get<double>("slope", 4 * N);
     double* yp = L.get<double>("yplanes", (size_t)moment_yplanes(c->shape_order) * N);
     EnergyStats* stats = L.get<EnergyStats>("stats", 1);
-    unsigned long long* hist = L.get<unsigned long long>("hist", 4096);
+    unsigned long long* hist = L.get<unsigned long long>("hist", MEDIAN_SCRATCH);
     OFC_CUDA(cudaMemsetAsync(hist, 0, 4096 * sizeof(unsigned long long), L.stream));
     launch_moments_solve(ds, u2, u2 + N, W, H, c->shape_order, d_mt, rw, mtp, yp, o2, o2 + N, en, rs, sl, L.stream);
-    launch_energy_stats(en, N, stats, false, L.stream);
-    launch_median(en, N, stats, hist, L.stream);
+    launch_energy_median(en, N, stats, false, hist, L.stream);
     launch_reset(en, u2, u2 + N, (int)N, stats, o2, o2 + N, rs, sl, L.stream);
     OFC_CUDA(cudaMemcpyAsync(oux, o2, N * 8, cudaMemcpyDeviceToHost, L.stream));
     OFC_CUDA(cudaMemcpyAsync(ouy, o2 + N, N * 8, cudaMemcpyDeviceToHost, L.stream));
@@ -1322,10 +1320,9 @@ int ofc_test_median(ofc_engine* e, const double* v, size_t n, double* median, ch
     if (n == 0) throw Error(OFC_ERR_ARG, "empty");
     double* d = L.upload("t_med", v, n);
     EnergyStats* stats = L.get<EnergyStats>("stats", 1);
-    unsigned long long* hist = L.get<unsigned long long>("hist", 4096);
+    unsigned long long* hist = L.get<unsigned long long>("hist", MEDIAN_SCRATCH);
     OFC_CUDA(cudaMemsetAsync(hist, 0, 4096 * sizeof(unsigned long long), L.stream));
-    launch_energy_stats(d, n, stats, true, L.stream);
-    launch_median(d, n, stats, hist, L.stream);
+    launch_energy_median(d, n, stats, true, hist, L.stream);
     EnergyStats hs;
     OFC_CUDA(cudaMemcpyAsync(&hs, stats, sizeof(hs), cudaMemcpyDeviceToHost, L.stream));
     OFC_CUDA(cudaStreamSynchronize(L.stream));

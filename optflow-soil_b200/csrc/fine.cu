@@ -924,53 +924,30 @@ __device__ double atomic_max_d(double* a, double v) {
   return __longlong_as_double(old);
 }
 
-__global__ void k_stats_init(EnergyStats* s) {
+// ---- median of the energy (np.median, phaseflow.py:149-151): an exact radix select over order-preserving keys.
+// 1. k_stats_hist0: min / max / NaN (the reset rule, phaseflow.rs:846-854) and the histogram of the top 12 key bits
+//    in one scan; the last block decides whether the median is needed and picks the first digit.
+// 2. k_radix_hist pass 1: the next 12 bits among the elements of that bucket.
+// 3. k_radix_compact: the elements of the 24-bit bucket into a candidate list (at most CAND_CAP), and the largest
+//    key below the bucket.
+// 4. k_radix_final (one block): the remaining 40 bits over the candidates, and the largest key below the median's.
+// A bucket above CAND_CAP (heavy ties) sets `fallback`: passes 2..5 and k_median_lo then run over all elements.
+constexpr int RBITS = 12, RBINS = 1 << RBITS, RPASSES = 6;
+constexpr int RH_T = 512;
+
+__global__ void k_stats_init(EnergyStats* s, size_t n) {
   s->lo = DBL_MAX;
   s->hi = -DBL_MAX;
   s->nan = 0;
-}
-
-__global__ void k_energy_stats(const double* __restrict__ e, size_t n, EnergyStats* s) {
-  double lo = DBL_MAX, hi = -DBL_MAX;
-  int nan = 0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    double v = e[i];
-    if (v != v) nan = 1;
-    else { lo = fmin(lo, v); hi = fmax(hi, v); }
-  }
-  for (int o = 16; o; o >>= 1) {
-    lo = fmin(lo, __shfl_xor_sync(0xffffffff, lo, o));
-    hi = fmax(hi, __shfl_xor_sync(0xffffffff, hi, o));
-    nan |= __shfl_xor_sync(0xffffffff, nan, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomic_min_d(&s->lo, lo);
-    atomic_max_d(&s->hi, hi);
-    if (nan) atomicOr(&s->nan, 1);
-  }
-}
-
-// the reset needs the median unless every energy is above 1e-9 max + 1e-30 (phaseflow.rs:846-854)
-__global__ void k_stats_decide(EnergyStats* s, int force, size_t n) {
-  bool skip = !s->nan && s->hi <= DBL_MAX / 2 && s->lo > 1e-9 * s->hi + 1e-30;
-  s->skip_reset = skip ? 1 : 0;
-  s->need_median = (force || !skip) ? 1 : 0;
-  s->median = s->nan ? nan("") : 0.0;
   s->prefix = 0;
   s->rank = (long long)(n / 2);
   s->less = 0;
   s->ticket = 0;
+  s->lo_val = 0;
+  s->ncand = 0;
+  s->fallback = 0;
+  s->below_max = 0;
 }
-
-void launch_energy_stats(const double* energy, size_t n, EnergyStats* stats, bool force_median, cudaStream_t st) {
-  OFC_LAUNCH(k_stats_init, 1, 1, 0, st, stats);
-  OFC_LAUNCH(k_energy_stats, 296, 256, 0, st, energy, n, stats);
-  OFC_LAUNCH(k_stats_decide, 1, 1, 0, st, stats, force_median ? 1 : 0, n);
-}
-
-// radix select of the element of rank stats->rank: 12-bit digits from the top, pass `pass` covers bits
-// [64 - 12 (pass + 1), 64 - 12 pass) (the last pass has 4 bits)
-constexpr int RBITS = 12, RBINS = 1 << RBITS, RPASSES = 6;
 
 __device__ __forceinline__ void digit_of(int pass, int& shift, int& bits) {
   int hi = 64 - RBITS * pass;
@@ -978,38 +955,9 @@ __device__ __forceinline__ void digit_of(int pass, int& shift, int& bits) {
   shift = hi - bits;
 }
 
-// One pass: a block histogram of the digit over the elements that match the prefix, added to hist; the last block
-// to finish (a ticket taken after a fence) scans hist, finds the bin holding rank, extends the prefix and clears
-// hist for the next pass.
-constexpr int RH_T = 512;
-
-__global__ void __launch_bounds__(RH_T) k_radix_hist(const double* __restrict__ e, size_t n, EnergyStats* s, int pass,
-                                                    unsigned long long* hist) {
-  if (!s->need_median || s->nan) return;
-  __shared__ unsigned int h[RBINS];
-  __shared__ long long wsum[RH_T / 32];
-  __shared__ bool last;
-  for (int i = threadIdx.x; i < RBINS; i += blockDim.x) h[i] = 0;
-  __syncthreads();
-  int shift, bits;
-  digit_of(pass, shift, bits);
-  const unsigned long long prefix = s->prefix;
-  const int hib = 64 - RBITS * pass;  // bits already fixed above `hib`
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    unsigned long long k = okey(e[i]);
-    bool match = hib == 64 ? true : ((k >> hib) == (prefix >> hib));
-    if (match) atomicAdd(&h[(k >> shift) & ((1ULL << bits) - 1)], 1u);
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < RBINS; i += blockDim.x)
-    if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&s->ticket, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // the pick: a block scan of the bin counts (RBINS / RH_T bins per thread)
+// run by every thread of the last block of a histogram pass: scans the RBINS counts of hist, finds the bin that
+// holds rank, extends the prefix by it, and clears hist and the ticket for the next pass
+__device__ void radix_pick(unsigned long long* hist, EnergyStats* s, int shift, long long* wsum) {
   constexpr int per = RBINS / RH_T;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   long long c[per];
@@ -1059,10 +1007,203 @@ __global__ void __launch_bounds__(RH_T) k_radix_hist(const double* __restrict__ 
   if (tid == 0) s->ticket = 0;
 }
 
+// adds the block histogram h to hist; returns true in every thread of the block that finished last
+__device__ bool radix_flush(const unsigned int* h, unsigned long long* hist, EnergyStats* s, bool* last) {
+  for (int i = threadIdx.x; i < RBINS; i += blockDim.x)
+    if (h[i]) atomicAdd(&hist[i], (unsigned long long)h[i]);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) *last = atomicAdd(&s->ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (*last) __threadfence();
+  return *last;
+}
+
+__global__ void __launch_bounds__(RH_T) k_stats_hist0(const double* __restrict__ e, size_t n, EnergyStats* s, int force,
+                                                     unsigned long long* hist) {
+  __shared__ unsigned int h[RBINS];
+  __shared__ long long wsum[RH_T / 32];
+  __shared__ double rlo[RH_T / 32], rhi[RH_T / 32];
+  __shared__ int rnan[RH_T / 32];
+  __shared__ bool last;
+  for (int i = threadIdx.x; i < RBINS; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  double lo = DBL_MAX, hi = -DBL_MAX;
+  int anynan = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double v = e[i];
+    if (v != v) anynan = 1;
+    else { lo = fmin(lo, v); hi = fmax(hi, v); }
+    atomicAdd(&h[okey(v) >> (64 - RBITS)], 1u);
+  }
+  for (int o = 16; o; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffff, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffff, hi, o));
+    anynan |= __shfl_xor_sync(0xffffffff, anynan, o);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { rlo[wid] = lo; rhi[wid] = hi; rnan[wid] = anynan; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < RH_T / 32; w++) { lo = fmin(lo, rlo[w]); hi = fmax(hi, rhi[w]); anynan |= rnan[w]; }
+    atomic_min_d(&s->lo, lo);
+    atomic_max_d(&s->hi, hi);
+    if (anynan) atomicOr(&s->nan, 1);
+  }
+  if (!radix_flush(h, hist, s, &last)) return;
+  // the reset needs the median unless every energy is above 1e-9 max + 1e-30 (phaseflow.rs:846-854)
+  const int snan = __ldcg(&s->nan);
+  const double slo = __ldcg(&s->lo), shi = __ldcg(&s->hi);
+  const bool skip = !snan && shi <= DBL_MAX / 2 && slo > 1e-9 * shi + 1e-30;
+  const bool need = force || !skip;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s->skip_reset = skip ? 1 : 0;
+    s->need_median = need ? 1 : 0;
+    s->median = snan ? nan("") : 0.0;
+  }
+  if (need && !snan) {
+    radix_pick(hist, s, 64 - RBITS, wsum);
+  } else {
+    for (int i = threadIdx.x; i < RBINS; i += blockDim.x) hist[i] = 0;
+    if (threadIdx.x == 0) s->ticket = 0;
+  }
+}
+
+// One pass over the elements that match the prefix: a block histogram of the digit, added to hist; the last block
+// picks. Passes >= 2 run only on the fallback.
+__global__ void __launch_bounds__(RH_T) k_radix_hist(const double* __restrict__ e, size_t n, EnergyStats* s, int pass,
+                                                    unsigned long long* hist) {
+  if (!s->need_median || s->nan) return;
+  if (pass >= 2 && !s->fallback) return;
+  __shared__ unsigned int h[RBINS];
+  __shared__ long long wsum[RH_T / 32];
+  __shared__ bool last;
+  for (int i = threadIdx.x; i < RBINS; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  int shift, bits;
+  digit_of(pass, shift, bits);
+  const unsigned long long prefix = s->prefix;
+  const int hib = 64 - RBITS * pass;  // bits already fixed above `hib`
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long k = okey(e[i]);
+    bool match = hib == 64 ? true : ((k >> hib) == (prefix >> hib));
+    if (match) atomicAdd(&h[(k >> shift) & ((1ULL << bits) - 1)], 1u);
+  }
+  __syncthreads();
+  if (!radix_flush(h, hist, s, &last)) return;
+  radix_pick(hist, s, shift, wsum);
+}
+
+constexpr int CBITS = 64 - 2 * RBITS;  // key bits below the bucket of the first two passes
+
+__global__ void k_radix_compact(const double* __restrict__ e, size_t n, EnergyStats* s, unsigned long long* cand) {
+  if (!s->need_median || s->nan) return;
+  const unsigned long long pre = s->prefix >> CBITS;
+  unsigned long long below = 0;
+  const int lane = threadIdx.x & 31;
+  for (size_t i0 = blockIdx.x * (size_t)blockDim.x; i0 < n; i0 += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = i0 + threadIdx.x;
+    unsigned long long k = 0;
+    bool in = false;
+    if (i < n) {
+      k = okey(e[i]);
+      const unsigned long long kk = k >> CBITS;
+      in = kk == pre;
+      if (kk < pre && k > below) below = k;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, in);
+    if (m) {  // one atomic per warp: the warp's matches take consecutive slots
+      unsigned base = 0;
+      if (lane == __ffs(m) - 1) base = atomicAdd(&s->ncand, (unsigned)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+      const unsigned slot = base + __popc(m & ((1u << lane) - 1));
+      if (in && slot < CAND_CAP) cand[slot] = k;
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    const unsigned long long v = __shfl_xor_sync(0xffffffffu, below, o);
+    below = v > below ? v : below;
+  }
+  if (lane == 0 && below) atomicMax(&s->below_max, below);
+}
+
+// the remaining CBITS bits of the median's key over the candidates (10-bit digits), and the largest key below it
+__global__ void __launch_bounds__(1024) k_radix_final(EnergyStats* s, const unsigned long long* __restrict__ cand) {
+  if (!s->need_median || s->nan) return;
+  const unsigned nc = s->ncand;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (nc > (unsigned)CAND_CAP) {
+    if (tid == 0) s->fallback = 1;
+    return;
+  }
+  __shared__ unsigned int h[1024];
+  __shared__ unsigned int wtot[32];
+  __shared__ unsigned long long sh_prefix, wmax[32];
+  __shared__ long long sh_rank, sh_less;
+  unsigned long long prefix = s->prefix;
+  long long rank = s->rank, less = s->less;
+  for (int shift = CBITS - 10; shift >= 0; shift -= 10) {
+    h[tid] = 0;
+    __syncthreads();
+    for (unsigned i = tid; i < nc; i += 1024) {
+      const unsigned long long k = cand[i];
+      if ((k >> (shift + 10)) == (prefix >> (shift + 10))) atomicAdd(&h[(k >> shift) & 1023], 1u);
+    }
+    __syncthreads();
+    const unsigned c = h[tid];
+    unsigned inc = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += v;
+    }
+    if (lane == 31) wtot[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+      unsigned w = wtot[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += v;
+      }
+      wtot[lane] = w;
+    }
+    __syncthreads();
+    const long long excl = (long long)(inc - c) + (wid ? wtot[wid - 1] : 0);
+    if (excl <= rank && rank < excl + (long long)c) {  // exactly one thread
+      sh_prefix = prefix | ((unsigned long long)tid << shift);
+      sh_rank = rank - excl;
+      sh_less = less + excl;
+    }
+    __syncthreads();
+    prefix = sh_prefix;
+    rank = sh_rank;
+    less = sh_less;
+  }
+  unsigned long long best = 0;
+  for (unsigned i = tid; i < nc; i += 1024) {
+    const unsigned long long k = cand[i];
+    if (k < prefix && k > best) best = k;
+  }
+  for (int o = 16; o; o >>= 1) {
+    const unsigned long long v = __shfl_xor_sync(0xffffffffu, best, o);
+    best = v > best ? v : best;
+  }
+  if (lane == 0) wmax[wid] = best;
+  __syncthreads();
+  if (tid == 0) {
+    best = s->below_max;
+    for (int w = 0; w < 32; w++) best = wmax[w] > best ? wmax[w] : best;
+    s->prefix = prefix;
+    s->rank = rank;
+    s->less = less;
+    *(unsigned long long*)&s->lo_val = best;
+  }
+}
+
 // after the passes: prefix = key of the element of rank n/2; for even n the one of rank n/2 - 1 is
-// the same value when `less` (elements below it) < n/2, else the largest element below it
+// the same value when `less` (elements below it) < n/2, else the largest element below it (fallback path)
 __global__ void k_median_lo(const double* __restrict__ e, size_t n, EnergyStats* s) {
-  if (!s->need_median || s->nan || (n % 2) || s->less < (long long)(n / 2)) return;
+  if (!s->need_median || s->nan || !s->fallback || (n % 2) || s->less < (long long)(n / 2)) return;
   const unsigned long long hk = s->prefix;
   unsigned long long best = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -1075,8 +1216,6 @@ __global__ void k_median_lo(const double* __restrict__ e, size_t n, EnergyStats*
   }
   if ((threadIdx.x & 31) == 0 && best) atomicMax((unsigned long long*)&s->lo_val, best);
 }
-
-__global__ void k_median_init(EnergyStats* s) { s->lo_val = 0; }
 
 __global__ void k_median_final(EnergyStats* s, size_t n) {
   if (!s->need_median) return;
@@ -1091,11 +1230,16 @@ __global__ void k_median_final(EnergyStats* s, size_t n) {
   s->median = (lo + hi) / 2.0;
 }
 
-void launch_median(const double* energy, size_t n, EnergyStats* stats, unsigned long long* hist, cudaStream_t st) {
-  for (int pass = 0; pass < RPASSES; pass++) {
-    OFC_LAUNCH(k_radix_hist, 296, RH_T, 0, st, energy, n, stats, pass, hist);
-  }
-  OFC_LAUNCH(k_median_init, 1, 1, 0, st, stats);
+void launch_energy_median(const double* energy, size_t n, EnergyStats* stats, bool force_median,
+                          unsigned long long* scratch, cudaStream_t st) {
+  unsigned long long* hist = scratch;
+  unsigned long long* cand = scratch + RBINS;
+  OFC_LAUNCH(k_stats_init, 1, 1, 0, st, stats, n);
+  OFC_LAUNCH(k_stats_hist0, 296, RH_T, 0, st, energy, n, stats, force_median ? 1 : 0, hist);
+  OFC_LAUNCH(k_radix_hist, 296, RH_T, 0, st, energy, n, stats, 1, hist);
+  OFC_LAUNCH(k_radix_compact, 296, 256, 0, st, energy, n, stats, cand);
+  OFC_LAUNCH(k_radix_final, 1, 1024, 0, st, stats, cand);
+  for (int pass = 2; pass < RPASSES; pass++) OFC_LAUNCH(k_radix_hist, 296, RH_T, 0, st, energy, n, stats, pass, hist);
   OFC_LAUNCH(k_median_lo, 296, 256, 0, st, energy, n, stats);
   OFC_LAUNCH(k_median_final, 1, 1, 0, st, stats, n);
 }
@@ -1204,11 +1348,93 @@ __global__ void k_within(const int* __restrict__ vd, int W, int H, int cap, doub
   }
 }
 
-void launch_within(const uint8_t* src, int W, int H, double limit, int mode, uint8_t* out, int* vdist, cudaStream_t st) {
-  int cap = (int)floor(limit) + 1;
+// The same test in one pass through a shared-memory tile of WT_X x WT_Y pixels with a halo of cap (<= WT_CAPMAX)
+// on every side: the vertical distances of the tile's columns come from two running scans per column (the last
+// src row at or above, the next at or below), then each pixel takes the smallest dx^2 + v^2 over |dx| <= cap.
+// Results equal k_vdist + k_within's; count (mode 1) is summed per block.
+constexpr int WT_X = 128, WT_Y = 32, WT_CAPMAX = 32, WT_T = 256;
+
+__global__ void __launch_bounds__(WT_T) k_within_tile(const uint8_t* __restrict__ src, int W, int H, int cap,
+                                                      double limit, int mode, uint8_t* out, const int* gate,
+                                                      int* count) {
+  if (gate && *gate == 0) return;
+  __shared__ uint8_t s[(WT_Y + 2 * WT_CAPMAX) * (WT_X + 2 * WT_CAPMAX)];
+  __shared__ uint8_t vd[WT_Y * (WT_X + 2 * WT_CAPMAX)];
+  __shared__ int wsum[WT_T / 32];
+  const int TW = WT_X + 2 * cap, TH = WT_Y + 2 * cap, tid = threadIdx.x;
+  const int bx = blockIdx.x * WT_X, by = blockIdx.y * WT_Y;
+  for (int i = tid; i < TW * TH; i += WT_T) {
+    const int ty = i / TW, tx = i - ty * TW, gx = bx - cap + tx, gy = by - cap + ty;
+    s[i] = (gx >= 0 && gx < W && gy >= 0 && gy < H) ? src[(size_t)gy * W + gx] : 0;
+  }
+  __syncthreads();
+  for (int tx = tid; tx < TW; tx += WT_T) {
+    int last = -(1 << 20);
+    for (int ty = 0; ty < cap + WT_Y; ty++) {
+      if (s[ty * TW + tx]) last = ty;
+      if (ty >= cap) vd[(ty - cap) * TW + tx] = (uint8_t)min(ty - last, cap + 1);
+    }
+    int next = 1 << 20;
+    for (int ty = TH - 1; ty >= cap; ty--) {
+      if (s[ty * TW + tx]) next = ty;
+      if (ty < cap + WT_Y) {
+        uint8_t& v = vd[(ty - cap) * TW + tx];
+        v = (uint8_t)min((int)v, min(next - ty, cap + 1));
+      }
+    }
+  }
+  __syncthreads();
+  int cnt = 0;
+  for (int i = tid; i < WT_X * WT_Y; i += WT_T) {  // the same trip count for every thread
+    const int r = i / WT_X, c = i - r * WT_X, gx = bx + c, gy = by + r;
+    const uint8_t* row = vd + r * TW + c + cap;
+    int best = -1;
+    for (int dx = -cap; dx <= cap; dx++) {
+      const int v = row[dx];
+      if (v > cap) continue;
+      const int d2 = dx * dx + v * v;
+      if (best < 0 || d2 < best) best = d2;
+    }
+    const bool inside = best >= 0 && sqrt((double)best) <= limit;
+    if (gx < W && gy < H) {
+      const size_t p = (size_t)gy * W + gx;
+      if (mode == 0) {
+        if (inside) out[p] = 1;
+      } else {
+        out[p] = inside ? 0 : 1;
+        cnt += inside ? 0 : 1;
+      }
+    }
+  }
+  if (count) {
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if ((tid & 31) == 0) wsum[tid >> 5] = cnt;
+    __syncthreads();
+    if (tid == 0) {
+      int t = 0;
+      for (int w = 0; w < WT_T / 32; w++) t += wsum[w];
+      if (t) atomicAdd(count, t);
+    }
+  }
+}
+
+// out |= (distance to src <= limit) (mode 0), or out = (distance > limit) with the count of such pixels (mode 1),
+// gated on *gate != 0 when gate is given
+static void within(const uint8_t* src, int W, int H, double limit, int mode, uint8_t* out, int* vdist, const int* gate,
+                   int* count, cudaStream_t st) {
+  const int cap = (int)floor(limit) + 1;
+  if (cap <= WT_CAPMAX) {
+    dim3 g(div_up(W, WT_X), div_up(H, WT_Y));
+    OFC_LAUNCH(k_within_tile, g, WT_T, 0, st, src, W, H, cap, limit, mode, out, gate, count);
+    return;
+  }
   dim3 g(div_up(W, 128), H);
-  OFC_LAUNCH(k_vdist, g, 128, 0, st, src, W, H, cap, vdist, (const int*)nullptr);
-  OFC_LAUNCH(k_within, g, 128, 0, st, vdist, W, H, cap, limit, mode, out, (const int*)nullptr, (int*)nullptr);
+  OFC_LAUNCH(k_vdist, g, 128, 0, st, src, W, H, cap, vdist, gate);
+  OFC_LAUNCH(k_within, g, 128, 0, st, vdist, W, H, cap, limit, mode, out, gate, count);
+}
+
+void launch_within(const uint8_t* src, int W, int H, double limit, int mode, uint8_t* out, int* vdist, cudaStream_t st) {
+  within(src, W, H, limit, mode, out, vdist, nullptr, nullptr, st);
 }
 
 // ---------------------------------------------------------------- trusted pre-warp
@@ -1312,12 +1538,10 @@ __global__ void k_zero_counts(PrewarpCounts* c) { c->ok = 0; }
 void launch_prewarp_fill(const uint8_t* low, const double* ux, const double* uy, const double* slope, int W, int H,
                          double R, PrewarpCounts* counts, uint8_t* ok, int* vdist, int* col_d2, int* col_row,
                          double* ux_pre, double* uy_pre, cudaStream_t st) {
-  int cap = (int)floor(R) + 1;
   dim3 g(div_up(W, 128), H);
   OFC_LAUNCH(k_zero_counts, 1, 1, 0, st, counts);
   // ok = distance to the nearest low pixel > R (gated on any low pixel)
-  OFC_LAUNCH(k_vdist, g, 128, 0, st, low, W, H, cap, vdist, (const int*)&counts->low);
-  OFC_LAUNCH(k_within, g, 128, 0, st, vdist, W, H, cap, R, 1, ok, (const int*)&counts->low, &counts->ok);
+  within(low, W, H, R, 1, ok, vdist, (const int*)&counts->low, &counts->ok, st);
   int* seg = vdist;  // the vertical distances are spent: 2 * ceil(H / CSEG) * W ints of segment summaries
   const int nseg = (H + CSEG - 1) / CSEG;
   OFC_LAUNCH(k_col_segments, dim3(div_up(W, 128), nseg), 128, 0, st, ok, W, H, counts, seg, seg + (size_t)nseg * W);

@@ -52,11 +52,16 @@ struct EnergyStats {
   long long less;
   double lo_val;
   unsigned int ticket;  // blocks of the current histogram pass that are done (the last one picks)
+  unsigned int ncand;   // elements in the bucket of the first two digits (candidates of the final select)
+  int fallback;         // more than CAND_CAP candidates: the remaining digits take full passes
+  unsigned long long below_max;  // the largest key below that bucket
 };
-void launch_energy_stats(const double* energy, size_t n, EnergyStats* stats, bool force_median, cudaStream_t st);
-// median of energy into stats->median (np.median), skipped when stats->need_median == 0;
-// hist: 4096 unsigned long long of scratch
-void launch_median(const double* energy, size_t n, EnergyStats* stats, unsigned long long* hist, cudaStream_t st);
+constexpr int CAND_CAP = 1 << 16;
+constexpr size_t MEDIAN_SCRATCH = 4096 + (size_t)CAND_CAP;  // unsigned long long: the histogram, then the candidates
+// stats->lo/hi/nan/skip_reset of energy, and its median into stats->median (np.median) when the reset needs it
+// or force_median; scratch: MEDIAN_SCRATCH unsigned long long whose first 4096 are zero (they are left zero)
+void launch_energy_median(const double* energy, size_t n, EnergyStats* stats, bool force_median,
+                          unsigned long long* scratch, cudaStream_t st);
 // reset below 1e-9 median + 1e-30 (phaseflow.py:149-151,158-161)
 void launch_reset(const double* energy, const double* ux_in, const double* uy_in, int n, const EnergyStats* stats,
                   double* ux, double* uy, double* resid, double* slope, cudaStream_t st);

@@ -163,6 +163,18 @@ def test_median(T):
     v = np.repeat(rng.random(50), 7)
     assert T.median(v) == np.median(v)
     assert T.median(np.array([3.0, 1.0, 2.0, 2.0])) == 2.0
+    # both signs; values clustered in one binade (a large bucket after two digits)
+    for v in (rng.standard_normal(100001), 1.0 + rng.random(200000) * 1e-6):
+        assert T.median(v) == np.median(v)
+    # ties: a bucket within the candidate list, and beyond it (the remaining digits then take full passes), with
+    # odd and even counts and the lower middle element inside or below the tied value
+    for n_tie, n in ((30000, 100000), (150000, 200001), (150000, 200000), (60000, 120000)):
+        v = rng.exponential(size=n)
+        v[:n_tie] = np.median(v)
+        rng.shuffle(v)
+        assert T.median(v) == np.median(v), (n_tie, n)
+    v = np.concatenate([np.zeros(60000), rng.random(60000)])
+    assert T.median(v) == np.median(v)
 
 
 def test_large_components(T, oracle):
