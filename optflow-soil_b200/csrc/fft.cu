@@ -75,6 +75,11 @@ int fft_threads(int L, int C) {
   return std::max(unit, std::min(T, cap));
 }
 
+size_t gabor_yt2_offset(int ph, int pw, int F) {
+  const size_t base = (size_t)4 * (pw + ph) + (size_t)F * (pw + ph);
+  return (base + 1) & ~(size_t)1;
+}
+
 std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c) {
   int F = c.n_scales * c.n_orient;
   std::vector<double> t((size_t)4 * (pw + ph) + (size_t)F * (pw + ph));
@@ -122,6 +127,16 @@ std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c) {
   double* by = bx + pw;
   for (int x = 0; x < pw; x++) bx[x] = 1.0 / (4.0 + 2.0 * std::cos(2 * PI * (double)x / pw));
   for (int y = 0; y < ph; y++) by[y] = 1.0 / (4.0 + 2.0 * std::cos(2 * PI * (double)y / ph));
+  // per filter and row: (omy[y], ey_k[y] by[y]), from an even offset (a float2 table in the float32 image)
+  std::vector<double> yt((size_t)2 * F * ph);
+  for (int k2 = 0; k2 < F; k2++)
+    for (int y = 0; y < ph; y++) {
+      yt[2 * ((size_t)k2 * ph + y)] = omy[y];
+      yt[2 * ((size_t)k2 * ph + y) + 1] = ey[(size_t)k2 * ph + y] * by[y];
+    }
+  const size_t o = gabor_yt2_offset(ph, pw, F);
+  t.resize(o + yt.size(), 0.0);
+  std::copy(yt.begin(), yt.end(), t.begin() + o);
   return t;
 }
 
@@ -144,6 +159,7 @@ void gabor_bind(GaborTables& g, const double* d64, const float* d32, int ph, int
   g.eyf = g.exf + (size_t)F * pw;
   g.bxf = g.eyf + (size_t)F * ph;
   g.byf = g.bxf + pw;
+  g.yt2 = (const float2*)(d32 + gabor_yt2_offset(ph, pw, F));
 }
 
 // ------------------------------------------------------------------------------------------ device
@@ -591,17 +607,29 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_fwd(const float2* Tin
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* A = (float2*)smraw;
   const int ph = FIXL ? FIXL : plh.L, n = ph * C;
-  float2* B = A + fft_buf_len(ph, C);
+  float2* B = A + fft_buf_stride(ph, C);  // 16-byte aligned: the result may be either buffer
   const int x0 = blockIdx.x * C;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    int y = i >> LC, x = x0 + (i & (C - 1));
-    A[i] = x < pw ? Tin[(size_t)y * pw + x] : make_float2(0.f, 0.f);
+  // C = 2 with an even row pitch: each row of the pair is 16 bytes on a 16-byte boundary, copied asynchronously
+  const bool rows16 = C == 2 && pw % 2 == 0;
+  if (rows16) {
+    for (int y = threadIdx.x; y < ph; y += blockDim.x) __pipeline_memcpy_async(A + 2 * y, Tin + (size_t)y * pw + x0, 16);
+    __pipeline_commit();
+    __pipeline_wait_prior(0);
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      int y = i >> LC, x = x0 + (i & (C - 1));
+      A[i] = x < pw ? Tin[(size_t)y * pw + x] : make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
   float2* r = fft_run<FIXL, C>(A, B, plh, false);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    int y = i >> LC, x = x0 + (i & (C - 1));
-    if (x < pw) S[(size_t)y * pw + x] = r[i];
+  if (rows16) {
+    for (int y = threadIdx.x; y < ph; y += blockDim.x) *(float4*)(S + (size_t)y * pw + x0) = *(const float4*)(r + 2 * y);
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      int y = i >> LC, x = x0 + (i & (C - 1));
+      if (x < pw) S[(size_t)y * pw + x] = r[i];
+    }
   }
 }
 
@@ -613,6 +641,33 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_fwd(const float2* Tin
 // pack (S G, S G i fx, S G i fy; factors in float64) of the filters [k0, k1) into plane 3 (k - k0) + v of U.
 // A thread's column is fixed (blockDim is even), so the x factors are read once.
 constexpr int RESP_G = 4;
+
+// A[i] = raw[i] f(i, t_i) for the n values of a column pair, t_i the row table entry of element i (row i / 2). With
+// the length fixed (FIXL, blockDim = COLS_TMAX) the table loads of UN elements are issued together before their
+// multiplies, so that their latencies overlap.
+template <int FIXL, int UN, class T, class Fn>
+__device__ __forceinline__ void cols_multiply(int n, const T* __restrict__ tab, Fn f) {
+  if constexpr (FIXL > 0) {
+    constexpr int NI = (2 * FIXL + COLS_TMAX - 1) / COLS_TMAX;
+#pragma unroll
+    for (int m0 = 0; m0 < NI; m0 += UN) {
+      T tv[UN];
+#pragma unroll
+      for (int u = 0; u < UN; u++) {
+        const int i = threadIdx.x + COLS_TMAX * (m0 + u);
+        if (m0 + u < NI && i < 2 * FIXL) tv[u] = __ldg(tab + (i >> 1));
+      }
+#pragma unroll
+      for (int u = 0; u < UN; u++) {
+        const int i = threadIdx.x + COLS_TMAX * (m0 + u);
+        if (m0 + u < NI && i < 2 * FIXL) f(i, tv[u]);
+      }
+    }
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) f(i, __ldg(tab + (i >> 1)));
+  }
+}
+
 template <bool REFPACK, int FIXL>
 __global__ void __launch_bounds__(COLS_TMAX, 2) k_fft_cols_pair(const float2* __restrict__ S, FftPlan plh, int pw,
                                                                 GaborTables g, int k0, int k1, float2* __restrict__ U) {
@@ -649,14 +704,13 @@ __global__ void __launch_bounds__(COLS_TMAX, 2) k_fft_cols_pair(const float2* __
     const float hx = __ldg(g.hxf + x), omx = __ldg(g.omxf + x), bx = __ldg(g.bxf + x);
     const int kend = min(g.F, (int)(blockIdx.y + 1) * RESP_G);
     for (int k = blockIdx.y * RESP_G; k < kend; k++) {
-      const float ex = __ldg(g.exf + (size_t)k * pw + x);
-      const float* eyk = g.eyf + (size_t)k * ph;
-      for (int i = tid; i < n; i += nt) {
-        const int y = i >> 1;
+      // G = (hx + omx omy) ex ey (bx by): the x factors of the thread's column, (omy, ey by) from the row table
+      const float exb = __ldg(g.exf + (size_t)k * pw + x) * bx;
+      cols_multiply<FIXL, 14>(n, g.yt2 + (size_t)k * ph, [&](int i, float2 t) {
         const float2 sv = raw[i];
-        const float G = fmaf(hx, __ldg(g.omyf + y), omx) * (ex * __ldg(eyk + y)) * (bx * __ldg(g.byf + y));
+        const float G = fmaf(hx, t.x, omx) * exb * t.y;
         A[i] = make_float2(sv.x * G, sv.y * G);
-      }
+      });
       __syncthreads();
       float2* r = fft_run<FIXL, C>(A, B, plh, true);
       float2* idle = r == A ? B : A;
@@ -670,15 +724,16 @@ __global__ void __launch_bounds__(COLS_TMAX, 2) k_fft_cols_pair(const float2* __
     for (int k = k0; k < k1; k++) {
       const double ex = g.ex[(size_t)k * pw + x];
       const double* eyk = g.ey + (size_t)k * ph;
-      for (int i = tid; i < n; i += nt) {
+      // the row factors omy[y] ey_k[y] (and fy[y]) gathered per element, their loads batched
+      cols_multiply<FIXL, 7>(n, g.omy, [&](int i, double omy) {
         const int y = i >> 1;
         const float2 sv = raw[i];
-        const double G = fma(hx, g.omy[y], omx) * ex * eyk[y];
+        const double G = fma(hx, omy, omx) * ex * __ldg(eyk + y);
         double re = sv.x * G, im = sv.y * G;
         if (v == 1) { const double t = re; re = -im * fx; im = t * fx; }                 // x i fx
-        else if (v == 2) { const double f = g.fy[y]; const double t = re; re = -im * f; im = t * f; }  // x i fy
+        else if (v == 2) { const double f = __ldg(g.fy + y); const double t = re; re = -im * f; im = t * f; }  // x i fy
         A[i] = make_float2((float)re, (float)im);
-      }
+      });
       __syncthreads();
       float2* r = fft_run<FIXL, C>(A, B, plh, true);
       store(r, 3 * (k - k0) + v);
@@ -869,7 +924,7 @@ static int persistent_blocks(const void* fn, int threads, size_t smem, int work)
 bool fft_fits(int ph, int pw) {
   try {
     int Tc = std::min(fft_threads(ph, 2), COLS_TMAX);
-    if (smem_prefilter(ph, 2, Tc) > SMEM_MAX) return false;
+    if (smem_prefilter(ph, 2, Tc) > SMEM_MAX || 2 * (size_t)fft_buf_stride(ph, 2) * sizeof(float2) > SMEM_MAX) return false;
     return 4 * fbytes(pw, 1) <= SMEM_MAX && smem_rows_resp(pw) <= SMEM_MAX;
   } catch (const Error&) {
     return false;
@@ -890,7 +945,7 @@ static void cols_fwd(float2* T, const FftPlan& plh, int pw, cudaStream_t st) {
   constexpr int C = 2;
   const int ph = plh.L;
   int nt = std::min(fft_threads(ph, C), COLS_TMAX);
-  size_t sm_f = 2 * fbytes(ph, C);
+  size_t sm_f = 2 * (size_t)fft_buf_stride(ph, C) * sizeof(float2);
   // in place: a block reads its C columns whole before it writes their spectrum back
   by_length(ph, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
@@ -909,6 +964,7 @@ static void cols_inverse(const float2* S, const FftPlan& plh, int pw, const Gabo
   int nt = std::min(fft_threads(ph, C), COLS_TMAX);
   const size_t sm_p = smem_cols_pair(ph);
   if (sm_p <= SMEM_MAX) {
+    if (ph == FFT_FIXED_L && nt != COLS_TMAX) throw Error(OFC_ERR_DEVICE, "column pass: unexpected block size");
     dim3 grid(div_up(pw, C), REFPACK ? 3 : div_up(g.F, RESP_G));
     by_length(ph, [&](auto fl) {
       constexpr int FL = decltype(fl)::value;

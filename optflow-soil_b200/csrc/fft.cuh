@@ -41,9 +41,12 @@ struct GaborTables {
   const double *ex = nullptr, *ey = nullptr;
   const float *hxf = nullptr, *omxf = nullptr, *omyf = nullptr, *exf = nullptr, *eyf = nullptr;
   const float *bxf = nullptr, *byf = nullptr;  // 1 / (4 + 2 cos w) per axis: the B-spline prefilter on the periodic grid
+  const float2* yt2 = nullptr;  // per filter k and row y: (omy[y], ey_k[y] by[y]) (float32)
 };
-// host tables: float64 [fx pw | fy ph | hx pw | hy ph | omx pw | omy ph | ex F*pw | ey F*ph | bx pw | by ph]
+// host tables: float64 [fx pw | fy ph | hx pw | hy ph | omx pw | omy ph | ex F*pw | ey F*ph | bx pw | by ph], then
+// from gabor_yt2_offset (even) the pairs (omy[y], ey_k[y] by[y]) per filter and row
 std::vector<double> gabor_tables_host(int ph, int pw, const ofc_config& c);
+size_t gabor_yt2_offset(int ph, int pw, int F);
 // binds g to a device copy of the tables: d64 (the host float64 vector) and d32 (its float32 image)
 void gabor_bind(GaborTables& g, const double* d64, const float* d32, int ph, int pw, int F);
 
