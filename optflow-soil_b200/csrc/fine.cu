@@ -1354,18 +1354,31 @@ __global__ void k_within(const int* __restrict__ vd, int W, int H, int cap, doub
 // Results equal k_vdist + k_within's; count (mode 1) is summed per block.
 constexpr int WT_X = 128, WT_Y = 32, WT_CAPMAX = 32, WT_T = 256;
 
-__global__ void __launch_bounds__(WT_T) k_within_tile(const uint8_t* __restrict__ src, int W, int H, int cap,
+template <int CAPT>
+__global__ void __launch_bounds__(WT_T) k_within_tile(const uint8_t* __restrict__ src, int W, int H, int cap_rt,
                                                       double limit, int mode, uint8_t* out, const int* gate,
                                                       int* count) {
   if (gate && *gate == 0) return;
+  const int cap = CAPT ? CAPT : cap_rt;
   __shared__ uint8_t s[(WT_Y + 2 * WT_CAPMAX) * (WT_X + 2 * WT_CAPMAX)];
   __shared__ uint8_t vd[WT_Y * (WT_X + 2 * WT_CAPMAX)];
   __shared__ int wsum[WT_T / 32];
   const int TW = WT_X + 2 * cap, TH = WT_Y + 2 * cap, tid = threadIdx.x;
   const int bx = blockIdx.x * WT_X, by = blockIdx.y * WT_Y;
-  for (int i = tid; i < TW * TH; i += WT_T) {
-    const int ty = i / TW, tx = i - ty * TW, gx = bx - cap + tx, gy = by - cap + ty;
-    s[i] = (gx >= 0 && gx < W && gy >= 0 && gy < H) ? src[(size_t)gy * W + gx] : 0;
+  // the tile, 8 loads in flight per thread
+  for (int i0 = 0; i0 < TW * TH; i0 += 8 * WT_T) {
+    uint8_t v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int i = i0 + u * WT_T + tid;
+      const int ty = i / TW, tx = i - ty * TW, gx = bx - cap + tx, gy = by - cap + ty;
+      v[u] = (i < TW * TH && gx >= 0 && gx < W && gy >= 0 && gy < H) ? __ldg(src + (size_t)gy * W + gx) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int i = i0 + u * WT_T + tid;
+      if (i < TW * TH) s[i] = v[u];
+    }
   }
   __syncthreads();
   for (int tx = tid; tx < TW; tx += WT_T) {
@@ -1388,14 +1401,14 @@ __global__ void __launch_bounds__(WT_T) k_within_tile(const uint8_t* __restrict_
   for (int i = tid; i < WT_X * WT_Y; i += WT_T) {  // the same trip count for every thread
     const int r = i / WT_X, c = i - r * WT_X, gx = bx + c, gy = by + r;
     const uint8_t* row = vd + r * TW + c + cap;
-    int best = -1;
+    int best = 1 << 30;  // no vertical distance within cap: d2 stays above every limit^2 with limit < cap
+#pragma unroll
     for (int dx = -cap; dx <= cap; dx++) {
       const int v = row[dx];
-      if (v > cap) continue;
-      const int d2 = dx * dx + v * v;
-      if (best < 0 || d2 < best) best = d2;
+      const int d2 = v > cap ? (1 << 30) : dx * dx + v * v;
+      best = min(best, d2);
     }
-    const bool inside = best >= 0 && sqrt((double)best) <= limit;
+    const bool inside = best < (1 << 30) && sqrt((double)best) <= limit;
     if (gx < W && gy < H) {
       const size_t p = (size_t)gy * W + gx;
       if (mode == 0) {
@@ -1425,7 +1438,10 @@ static void within(const uint8_t* src, int W, int H, double limit, int mode, uin
   const int cap = (int)floor(limit) + 1;
   if (cap <= WT_CAPMAX) {
     dim3 g(div_up(W, WT_X), div_up(H, WT_Y));
-    OFC_LAUNCH(k_within_tile, g, WT_T, 0, st, src, W, H, cap, limit, mode, out, gate, count);
+    if (cap == 13)  // the default radii (12.22 px)
+      OFC_LAUNCH(k_within_tile<13>, g, WT_T, 0, st, src, W, H, cap, limit, mode, out, gate, count);
+    else
+      OFC_LAUNCH(k_within_tile<0>, g, WT_T, 0, st, src, W, H, cap, limit, mode, out, gate, count);
     return;
   }
   dim3 g(div_up(W, 128), H);
