@@ -138,6 +138,26 @@ __device__ __forceinline__ void sample2_real(const T* __restrict__ c1, const T* 
   }
 }
 
+// two real splines stored interleaved (double2 per pixel), sampled at the same taps
+__device__ __forceinline__ double2 sample_pair(const double2* __restrict__ c, int w, const Taps& t) {
+  double o1 = 0, o2 = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const double2* row = c + (size_t)t.yi[j] * w;
+    const double2 c0 = __ldg(row + t.xi[0]);
+    double a1 = t.wx[0] * c0.x, a2 = t.wx[0] * c0.y;
+#pragma unroll
+    for (int k = 1; k < 4; k++) {
+      const double2 v = __ldg(row + t.xi[k]);
+      a1 += t.wx[k] * v.x;
+      a2 += t.wx[k] * v.y;
+    }
+    o1 += t.wy[j] * a1;
+    o2 += t.wy[j] * a2;
+  }
+  return make_double2(o1, o2);
+}
+
 // complex spline stored as float2; float accumulation of the 16 taps with f64-derived weights
 __device__ inline float2 sample_c32(const float2* __restrict__ c, int w, const Taps& t) {
   float re = 0.f, im = 0.f;

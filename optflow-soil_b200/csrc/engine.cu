@@ -525,9 +525,9 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
     launch_fft_rows_fwd_real(warped, W, H, plw, ph, T, st);
     launch_fft_cols_filters(T, plh, pw, g, U, st);
     launch_fft_rows_inv_resp(U, plw, ph, F, R, st);
-    launch_bspline_f64(s2, cs2, tmpb, 2, W, H, st);
+    launch_bspline_f64_pair(s2, (double2*)cs2, tmpb, W, H, st);
     for (int in = 0; in < c.inner_iters; in++) {
-      launch_accumulate(ref4, R, F, ph, pw, ucur, ucur + N, s2, s2 + N, cs2, cs2 + N, W, H, sums, st);
+      launch_accumulate(ref4, R, F, ph, pw, ucur, ucur + N, s2, s2 + N, (const double2*)cs2, W, H, sums, st);
       launch_moments_solve(sums, ucur, ucur + N, W, H, c.shape_order, d_mt, rw, mtp, yplanes, unext, unext + N, energy,
                            resid, slope, st);
       const bool last_inner = in == c.inner_iters - 1;
@@ -1406,9 +1406,9 @@ int ofc_test_first_sums(ofc_engine* e, const float* i1, const float* i2, size_t 
     launch_fft_rows_fwd_real(warped, W, H, L.plan(pw), ph, T, st);
     launch_fft_cols_filters(T, L.plan(ph), pw, g, U, st);
     launch_fft_rows_inv_resp(U, L.plan(pw), ph, F, R, st);
-    launch_bspline_f64(s2, cs2, tmpb, 2, W, H, st);
+    launch_bspline_f64_pair(s2, (double2*)cs2, tmpb, W, H, st);
     double* ds = L.get<double>("sums", 7 * N);
-    launch_accumulate(ref4, R, F, ph, pw, u2, u2 + N, s2, s2 + N, cs2, cs2 + N, W, H, ds, st);
+    launch_accumulate(ref4, R, F, ph, pw, u2, u2 + N, s2, s2 + N, (const double2*)cs2, W, H, ds, st);
     OFC_CUDA(cudaMemcpyAsync(sums, ds, 7 * N * 8, cudaMemcpyDeviceToHost, st));
     OFC_CUDA(cudaStreamSynchronize(st));
   });

@@ -208,7 +208,8 @@ __global__ void k_iir_anticausal(const double* __restrict__ y, Tout* __restrict_
 // accesses on distinct banks.
 constexpr int XR_ROWS = 64, XR_SEG = 64, XR_TW = XR_SEG + 2 * IIR_WARM + 1;  // 121 doubles per tile row (odd)
 
-template <class Tout>
+// ILV: the planes (two) are written interleaved, out[2 p + plane]
+template <class Tout, bool ILV>
 __global__ void __launch_bounds__(XR_ROWS) k_iir_x(const double* __restrict__ in, Tout* __restrict__ out, int n, int nrows,
                                                   long plane) {
   extern __shared__ double tile[];  // XR_ROWS x XR_TW
@@ -275,15 +276,20 @@ __global__ void __launch_bounds__(XR_ROWS) k_iir_x(const double* __restrict__ in
   __syncthreads();
   for (int rr = wid; rr < XR_ROWS; rr += nw) {
     if (r0 + rr >= nrows) break;
-    Tout* dst = o + (size_t)(r0 + rr) * n + s0;
     const double* t = tile + rr * XR_TW + (s0 - c0);
-    for (int c = lane; c < e0 - s0; c += 32) dst[c] = (Tout)t[c];
+    if (ILV) {
+      Tout* dst = out + ((size_t)(r0 + rr) * n + s0) * 2 + blockIdx.z;
+      for (int c = lane; c < e0 - s0; c += 32) dst[2 * c] = (Tout)t[c];
+    } else {
+      Tout* dst = o + (size_t)(r0 + rr) * n + s0;
+      for (int c = lane; c < e0 - s0; c += 32) dst[c] = (Tout)t[c];
+    }
   }
 }
 
-// y pass: in -> tmp (causal) -> tmp2 (anticausal); x pass: tmp2 -> out. tmp may alias out (it is dead once the
-// x pass starts); tmp2 must not, since the x pass's tiles overlap.
-template <class Tin, class Tout>
+// y pass: in -> tmp (causal) -> tmp2 (anticausal); x pass: tmp2 -> out (ILV: two planes interleaved). tmp may alias
+// out (it is dead once the x pass starts); tmp2 must not, since the x pass's tiles overlap.
+template <class Tin, class Tout, bool ILV = false>
 static void bspline_axes(const Tin* in, Tout* out, double* tmp, double* tmp2, int n_planes, int W, int H, cudaStream_t st) {
   long plane = (long)W * H;
   // along y: lines = columns (stride 1 apart), element stride W
@@ -292,14 +298,19 @@ static void bspline_axes(const Tin* in, Tout* out, double* tmp, double* tmp2, in
   OFC_LAUNCH((k_iir_anticausal<double>), gy, 128, 0, st, tmp, tmp2, H, W, (long)W, 1L, plane);
   // along x: both recursions in one pass through shared-memory tiles
   const size_t sm = (size_t)XR_ROWS * XR_TW * sizeof(double);
-  OFC_CUDA(cudaFuncSetAttribute((const void*)k_iir_x<Tout>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  OFC_CUDA(cudaFuncSetAttribute((const void*)k_iir_x<Tout, ILV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   dim3 gx(div_up(W, XR_SEG), div_up(H, XR_ROWS), n_planes);
-  OFC_LAUNCH(k_iir_x<Tout>, gx, XR_ROWS, sm, st, tmp2, out, W, H, plane);
+  OFC_LAUNCH((k_iir_x<Tout, ILV>), gx, XR_ROWS, sm, st, tmp2, out, W, H, plane);
 }
 
 void launch_bspline_f64(const double* in, double* out, double* tmp, int n_planes, int W, int H, cudaStream_t st) {
   // out doubles as the causal scratch of the y pass; tmp holds the y pass's result for the x pass
   bspline_axes<double, double>(in, out, (double*)out, tmp, n_planes, W, H, st);
+}
+
+void launch_bspline_f64_pair(const double* in, double2* out, double* tmp, int W, int H, cudaStream_t st) {
+  // out (2 W H doubles) doubles as the causal scratch of the y pass; tmp holds the y pass's result
+  bspline_axes<double, double, true>(in, (double*)out, (double*)out, tmp, 2, W, H, st);
 }
 
 void launch_bspline_f32(const float* in, float* out, double* tmp, int W, int H, cudaStream_t st) {
@@ -335,14 +346,14 @@ void launch_warp(const float* c2, int w2, int h2, const double* sx, const double
 // angle(r1 conj(r2)) is taken in float32 (the inputs carry float32 precision, the angle is then exact to ~1e-7
 // rad); c = dphi + gx u + gy v and the seven sums are float64, since u reaches tens of pixels and the residual
 // sum gcc - theta . b cancels. The kernel is latency-bound, so: the F reference-pack values of the pixel are
-// copied to shared memory asynchronously at the start (in flight during the fixed point); |r1| is formed from
-// the pack instead of a second load; the 16 tap offsets are computed once and reused by every filter.
+// copied to shared memory asynchronously at the start (in flight during the fixed point); |r1| |r2| is one square
+// root of |r1|^2 |r2|^2, with |r1|^2 formed from the pack; the 16 tap offsets are computed once and reused by every
+// filter; the field spline is stored interleaved (one 16-byte load per tap for both components).
 __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict__ ref4, const float2* __restrict__ R,
                                                       int F, int ph, int pw, const double* __restrict__ ux,
                                                       const double* __restrict__ uy, const double* __restrict__ sx,
-                                                      const double* __restrict__ sy, const double* __restrict__ csx,
-                                                      const double* __restrict__ csy, int W, int H,
-                                                      double* __restrict__ sums) {
+                                                      const double* __restrict__ sy, const double2* __restrict__ cs,
+                                                      int W, int H, double* __restrict__ sums) {
   extern __shared__ float4 pk[];  // F x 128
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y;
@@ -359,10 +370,9 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
     Taps t;
     double nx, ny;
     if (make_taps(px, py, W, H, t)) {
-      double s1, s2;
-      sample2_real(csx, csy, W, t, s1, s2);
-      nx = tx - s1;
-      ny = ty - s2;
+      const double2 sv = sample_pair(cs, W, t);
+      nx = tx - sv.x;
+      ny = ty - sv.y;
     } else {
       nx = ny = nan("");
     }
@@ -388,8 +398,8 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
   __pipeline_wait_prior(0);
   for (int k = 0; k < F; k++) {
     const float4 r1 = pk[k * 128 + threadIdx.x];
-    // |r1| as the reference pack's amplitude (phaseflow.py:111), from the stored float32 response
-    const float a1k = sqrtf(fmaf(r1.x, r1.x, fmaf(r1.y, r1.y, 1e-12f)));
+    // |r1|^2 as the reference pack's amplitude squared (phaseflow.py:111), from the stored float32 response
+    const float q1 = fmaf(r1.x, r1.x, fmaf(r1.y, r1.y, 1e-12f));
     float br = fnan, bi = fnan;
     if (ok) {
       const float2* Rk = R + (size_t)k * plane;
@@ -412,7 +422,7 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
     const float re = fmaf(r1.x, br, r1.y * bi);
     const float im = fmaf(r1.y, br, -r1.x * bi);
     const double dphi = (double)atan2f(im, re);
-    const double wk = (double)(a1k * sqrtf(fmaf(br, br, bi * bi)));
+    const double wk = (double)sqrtf(q1 * fmaf(br, br, bi * bi));  // |r1| |r2|
     const double gx = r1.z, gy = r1.w;
     const double c = dphi + gx * u + gy * v;
     const double wgx = wk * gx, wgy = wk * gy;
@@ -434,13 +444,13 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
 }
 
 void launch_accumulate(const float4* ref4, const float2* R, int F, int ph, int pw, const double* ux, const double* uy,
-                       const double* sx, const double* sy, const double* csx, const double* csy, int W, int H,
-                       double* sums, cudaStream_t st) {
+                       const double* sx, const double* sy, const double2* cs, int W, int H, double* sums,
+                       cudaStream_t st) {
   dim3 g(div_up(W, 128), H);
   const size_t sm = (size_t)F * 128 * sizeof(float4);
   if (sm > 227 * 1024) throw Error(OFC_ERR_WINDOW, "too many Gabor filters (" + std::to_string(F) + ") for the CUDA engine");
   OFC_CUDA(cudaFuncSetAttribute((const void*)k_accumulate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  OFC_LAUNCH(k_accumulate, g, 128, sm, st, ref4, R, F, ph, pw, ux, uy, sx, sy, csx, csy, W, H, sums);
+  OFC_LAUNCH(k_accumulate, g, 128, sm, st, ref4, R, F, ph, pw, ux, uy, sx, sy, cs, W, H, sums);
 }
 
 // ---------------------------------------------------------------- window moments + solve

@@ -15,6 +15,8 @@ void launch_corr_y_f32in(const float* in, double* out, int W, int H, const doubl
 // in -> out (float64 or float32 storage), tmp: W*H*n_planes float64 scratch
 void launch_bspline_f64(const double* in, double* out, double* tmp, int n_planes, int W, int H, cudaStream_t st);
 void launch_bspline_f32(const float* in, float* out, double* tmp, int W, int H, cudaStream_t st);
+// the same for the two planes of in, written interleaved (out: W H double2); tmp: 2 W H doubles
+void launch_bspline_f64_pair(const double* in, double2* out, double* tmp, int W, int H, cudaStream_t st);
 
 // warp (interp.py:72-76 with the window shift of phaseflow.rs:1420-1439): out(x, y) = spline2 at
 // (x + shx + sx, y + shy + sy); spline2 is w2 x h2, out W x H
@@ -24,8 +26,8 @@ void launch_warp(const float* c2, int w2, int h2, const double* sx, const double
 // the seven per-pixel sums of an inner iteration (phaseflow.py:468-483); ref4: F planes W x H of the reference
 // pack (r.re, r.im, gx, gy); R: F response planes (ph x pw); sums: 7 planes W x H
 void launch_accumulate(const float4* ref4, const float2* R, int F, int ph, int pw, const double* ux, const double* uy,
-                       const double* sx, const double* sy, const double* csx, const double* csy, int W, int H,
-                       double* sums, cudaStream_t st);
+                       const double* sx, const double* sy, const double2* cs, int W, int H, double* sums,
+                       cudaStream_t st);
 
 // Gaussian window moments + the per-pixel shape-function solve (phaseflow.py:114-161): mtaps: the
 // window taps k(t) t^p for p = 0..4 (5 x (2r+1) doubles, device); tp: the same taps for t = 0..r as a kernel
