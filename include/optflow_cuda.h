@@ -136,6 +136,30 @@ OFC_API int ofc_refine_raw(ofc_engine* eng, const float* i1, size_t w, size_t h,
                    char* err, size_t errlen);
 
 /*
+ * The refine_raw calls of a tiling driver's windows (the tile loop of rust/crates/optflow-core/src/tile.rs:420-472
+ * calls FineEngine::refine_prepared once per tile; the batch replaces that loop): window k has the arguments of
+ * ofc_refine_raw. The results equal n calls of ofc_refine_raw, bit for bit. Window k + 1's inputs upload and
+ * window k - 1's outputs download on a second stream while window k computes; with pinned host buffers
+ * (cudaHostAlloc or cudaHostRegister) the copies overlap the compute. Any output pointer may be NULL. All
+ * windows are checked before any work; the error text names the failing window.
+ */
+typedef struct ofc_window {
+  const float* i1;     /* w x h */
+  size_t w, h;
+  const float* i2;     /* w2 x h2 */
+  size_t w2, h2;
+  int64_t shift_x, shift_y;
+  const float* ux;     /* w x h */
+  const float* uy;
+  double* out_ux;      /* w x h each */
+  double* out_uy;
+  double* out_energy;
+  double* out_resid;
+} ofc_window;
+OFC_API int ofc_refine_batch(ofc_engine* eng, const ofc_window* wins, size_t n, const ofc_config* cfg,
+                     char* err, size_t errlen);
+
+/*
  * phaseflow::refine / refine_low (python/optflow_ref/phaseflow.py:427-511;
  * rust/crates/optflow-core/src/phaseflow.rs:1684-1757): refine_raw on the whole image plus the
  * confidence with its border rule. out_low (nullable) = the f64 confidence < conf_min.

@@ -210,6 +210,14 @@ struct Lane {
   std::unordered_map<std::string, std::unique_ptr<DevBuf>> pool;
   std::map<int, std::pair<FftPlan, std::unique_ptr<DevBuf>>> plans;
   cudaEvent_t ev[4] = {};
+  // the copy stream of batched calls and its ordering events (created on first use)
+  cudaStream_t copy = nullptr;
+  cudaEvent_t bev[8] = {};
+  void ensure_copy_stream() {
+    if (copy) return;
+    OFC_CUDA(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
+    for (auto& e : bev) OFC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
 
   template <class T>
   T* get(const std::string& name, size_t count) {
@@ -939,8 +947,13 @@ void ofc_destroy(ofc_engine* e) {
   for (auto& l : e->lanes) {
     std::lock_guard<std::mutex> lk(l->busy);
     cudaStreamSynchronize(l->stream);
+    if (l->copy) cudaStreamSynchronize(l->copy);
     l->release();
     for (auto& ev : l->ev) cudaEventDestroy(ev);
+    if (l->copy) {
+      for (auto& ev : l->bev) cudaEventDestroy(ev);
+      cudaStreamDestroy(l->copy);
+    }
     cudaStreamDestroy(l->stream);
   }
   delete e;
@@ -998,6 +1011,99 @@ int ofc_refine_raw(ofc_engine* e, const float* i1, size_t w, size_t h, const flo
     if (out_uy) OFC_CUDA(cudaMemcpyAsync(out_uy, f.uy, N * 8, cudaMemcpyDeviceToHost, st));
     if (out_energy) OFC_CUDA(cudaMemcpyAsync(out_energy, f.energy, N * 8, cudaMemcpyDeviceToHost, st));
     if (out_resid) OFC_CUDA(cudaMemcpyAsync(out_resid, f.resid, N * 8, cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int ofc_refine_batch(ofc_engine* e, const ofc_window* wins, size_t n, const ofc_config* c, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    if (n == 0) return;
+    if (!wins) throw Error(OFC_ERR_ARG, "null window list");
+    size_t maxN = 0, max2 = 0;
+    for (size_t k = 0; k < n; k++) {
+      const ofc_window& w = wins[k];
+      try {
+        check_fine_window(w.w, w.h, *c);
+        check_sizes(w.w2, w.h2);
+        if (!w.i1 || !w.i2 || !w.ux || !w.uy) throw Error(OFC_ERR_ARG, "null input");
+      } catch (const Error& x) {
+        throw Error(x.status, "window " + std::to_string(k) + ": " + x.what());
+      }
+      maxN = std::max(maxN, w.w * w.h);
+      max2 = std::max(max2, w.w2 * w.h2);
+    }
+    L.ensure_copy_stream();
+    cudaStream_t st = L.stream, cs = L.copy;
+    cudaEvent_t* in_ready = L.bev;       // inputs of set s uploaded
+    cudaEvent_t* in_free = L.bev + 2;    // the refine that read set s is done
+    cudaEvent_t* out_ready = L.bev + 4;  // outputs staged in staging set s
+    cudaEvent_t* out_done = L.bev + 6;   // staging set s downloaded
+    // two input sets and two output staging sets, sized for the largest window before any work is queued
+    float *in1[2], *in2[2], *inu[2], *inv[2];
+    double* stage[2];
+    for (int s2 = 0; s2 < 2; s2++) {
+      const std::string t = std::to_string(s2);
+      in1[s2] = L.get<float>("batch_i1_" + t, maxN);
+      in2[s2] = L.get<float>("batch_i2_" + t, max2);
+      inu[s2] = L.get<float>("batch_u_" + t, maxN);
+      inv[s2] = L.get<float>("batch_v_" + t, maxN);
+      stage[s2] = L.get<double>("batch_out_" + t, 4 * maxN);
+    }
+    double* u2 = L.get<double>("u2", 2 * maxN);
+    auto upload = [&](size_t k, int s2) {
+      const ofc_window& w = wins[k];
+      const size_t N = w.w * w.h;
+      OFC_CUDA(cudaMemcpyAsync(in1[s2], w.i1, N * 4, cudaMemcpyHostToDevice, cs));
+      OFC_CUDA(cudaMemcpyAsync(in2[s2], w.i2, w.w2 * w.h2 * 4, cudaMemcpyHostToDevice, cs));
+      OFC_CUDA(cudaMemcpyAsync(inu[s2], w.ux, N * 4, cudaMemcpyHostToDevice, cs));
+      OFC_CUDA(cudaMemcpyAsync(inv[s2], w.uy, N * 4, cudaMemcpyHostToDevice, cs));
+      OFC_CUDA(cudaEventRecord(in_ready[s2], cs));
+    };
+    auto download = [&](size_t k) {
+      const int s2 = (int)(k & 1);
+      const ofc_window& w = wins[k];
+      const size_t N = w.w * w.h;
+      OFC_CUDA(cudaStreamWaitEvent(cs, out_ready[s2], 0));
+      double* outs[4] = {w.out_ux, w.out_uy, w.out_energy, w.out_resid};
+      for (int q = 0; q < 4; q++)
+        if (outs[q]) OFC_CUDA(cudaMemcpyAsync(outs[q], stage[s2] + q * N, N * 8, cudaMemcpyDeviceToHost, cs));
+      OFC_CUDA(cudaEventRecord(out_done[s2], cs));
+    };
+    // copy stream: upload k + 1 while k computes, download k - 1 after k is queued (so that a pageable download,
+    // which holds the host until it is done, leaves the compute stream with work). On an error both streams are
+    // drained before the call returns, so no copy into the caller's buffers outlives it.
+    struct Drain {
+      cudaStream_t a, b;
+      ~Drain() {
+        cudaStreamSynchronize(a);
+        cudaStreamSynchronize(b);
+      }
+    } drain{cs, st};
+    upload(0, 0);
+    for (size_t k = 0; k < n; k++) {
+      const int s2 = (int)(k & 1);
+      const ofc_window& w = wins[k];
+      const size_t N = w.w * w.h;
+      OFC_CUDA(cudaStreamWaitEvent(st, in_ready[s2], 0));
+      launch_f32_to_f64(inu[s2], u2, N, st);
+      launch_f32_to_f64(inv[s2], u2 + N, N, st);
+      FineOut f = refine_dev(L, in1[s2], (int)w.w, (int)w.h, in2[s2], (int)w.w2, (int)w.h2, (long)w.shift_x,
+                             (long)w.shift_y, u2, *c);
+      OFC_CUDA(cudaEventRecord(in_free[s2], st));
+      if (k >= 2) OFC_CUDA(cudaStreamWaitEvent(st, out_done[s2], 0));  // staging set s2 held window k - 2
+      const double* res[4] = {f.ux, f.uy, f.energy, f.resid};
+      for (int q = 0; q < 4; q++)
+        OFC_CUDA(cudaMemcpyAsync(stage[s2] + q * N, res[q], N * 8, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaEventRecord(out_ready[s2], st));
+      if (k + 1 < n) {
+        if (k >= 1) OFC_CUDA(cudaStreamWaitEvent(cs, in_free[s2 ^ 1], 0));  // window k - 1 read set s2 ^ 1
+        upload(k + 1, s2 ^ 1);
+      }
+      if (k >= 1) download(k - 1);
+    }
+    download(n - 1);
+    OFC_CUDA(cudaStreamSynchronize(cs));
     OFC_CUDA(cudaStreamSynchronize(st));
   });
 }

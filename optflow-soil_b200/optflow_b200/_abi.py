@@ -66,6 +66,26 @@ class OfcPairOut(ctypes.Structure):
     ]
 
 
+class OfcWindow(ctypes.Structure):
+    """ofc_window of include/optflow_cuda.h: the arguments of one refine_raw call of a batch."""
+    _fields_ = [
+        ("i1", c_float_p),
+        ("w", ctypes.c_size_t),
+        ("h", ctypes.c_size_t),
+        ("i2", c_float_p),
+        ("w2", ctypes.c_size_t),
+        ("h2", ctypes.c_size_t),
+        ("shift_x", ctypes.c_int64),
+        ("shift_y", ctypes.c_int64),
+        ("ux", c_float_p),
+        ("uy", c_float_p),
+        ("out_ux", c_double_p),
+        ("out_uy", c_double_p),
+        ("out_energy", c_double_p),
+        ("out_resid", c_double_p),
+    ]
+
+
 PAIR_FIELDS = ("ux", "uy", "conf", "exx", "eyy", "exy", "gmax", "vol", "valid", "raw_ux", "raw_uy")
 
 # every symbol the header declares, with its ctypes signature (restype, argtypes)
@@ -87,6 +107,7 @@ SIGNATURES = {
     "ofc_refine_raw": (ctypes.c_int, [_P, c_float_p, _S, _S, c_float_p, _S, _S, ctypes.c_int64, ctypes.c_int64,
                                       c_float_p, c_float_p, ctypes.POINTER(OfcConfig),
                                       c_double_p, c_double_p, c_double_p, c_double_p, _E, _S]),
+    "ofc_refine_batch": (ctypes.c_int, [_P, ctypes.c_void_p, _S, ctypes.POINTER(OfcConfig), _E, _S]),
     "ofc_refine": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, c_float_p, c_float_p, ctypes.POINTER(OfcConfig),
                                   c_float_p, c_float_p, c_float_p, c_float_p, c_u8_p, _E, _S]),
     "ofc_grid_shape": (ctypes.c_int, [_S, _S, ctypes.POINTER(OfcConfig), ctypes.POINTER(_S), ctypes.POINTER(_S)]),

@@ -146,6 +146,29 @@ def refine_raw(I1, I2, ux, uy, cfg=None, shift=(0, 0), engine=None):
     return dict(zip(("ux", "uy", "energy", "resid"), out))
 
 
+def refine_batch(windows, cfg=None, engine=None):
+    """The refine_raw calls of a tiling driver's windows in one call (the tile loop of
+    rust/crates/optflow-core/src/tile.rs:420-472): windows is a sequence of (I1, I2, ux, uy, shift);
+    returns one refine_raw result dict per window, bit-identical to separate refine_raw calls."""
+    eng = engine or default_engine()
+    cfg, c = _prep_cfg(cfg)
+    keep, outs = [], []
+    arr = (_abi.OfcWindow * max(1, len(windows)))()
+    for k, (I1, I2, ux, uy, shift) in enumerate(windows):
+        a = _f32(I1)
+        h, w = a.shape
+        b = _f32(I2)
+        u, v = _f32(ux, (h, w)), _f32(uy, (h, w))
+        out = [np.empty((h, w), np.float64) for _ in range(4)]
+        keep += [a, b, u, v]
+        outs.append(out)
+        arr[k] = _abi.OfcWindow(_ptr(a, c_float_p), w, h, _ptr(b, c_float_p), b.shape[1], b.shape[0], int(shift[0]),
+                                int(shift[1]), _ptr(u, c_float_p), _ptr(v, c_float_p),
+                                *[_ptr(o, c_double_p) for o in out])
+    eng._call("ofc_refine_batch", ctypes.cast(arr, ctypes.c_void_p), len(windows), ctypes.byref(c))
+    return [dict(zip(("ux", "uy", "energy", "resid"), out)) for out in outs]
+
+
 def refine(I1, I2, ux, uy, cfg=None, engine=None) -> Flow:
     """phaseflow.refine (python/optflow_ref/phaseflow.py:427-511)."""
     eng = engine or default_engine()

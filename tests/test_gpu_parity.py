@@ -159,6 +159,34 @@ def test_refine_raw_window_shift(oracle):
     assert rms(got["ux"][inner], want["ux"][inner]) < 5e-3
 
 
+def test_refine_batch_equals_refine_raw():
+    """ofc_refine_batch (the tile loop's refine_raw calls in one call, copies on a second stream) gives each
+    window's refine_raw result bit for bit, for windows of different sizes and shifts; a bad window is refused
+    by index before any work."""
+    from optflow_b200 import EngineError, refine_batch, refine_raw
+    a, b = _synthetic_pair(192, 11, t=(0.9, -0.6), exx=0.004)
+    wins = []
+    for (x0, y0, w, h) in ((40, 32, 96, 112), (0, 0, 128, 96), (24, 40, 160, 128), (40, 32, 96, 112)):
+        u = np.full((h, w), 0.9, np.float32)
+        v = np.full((h, w), -0.6, np.float32)
+        sx, sy = max(x0 - 16, 0), max(y0 - 16, 0)
+        i2 = b[sy:sy + h + 32, sx:sx + w + 32]
+        wins.append((a[y0:y0 + h, x0:x0 + w], i2, u, v, (x0 - sx, y0 - sy)))
+    got = refine_batch(wins, Config())
+    assert len(got) == len(wins)
+    for k, (i1, i2, u, v, sh) in enumerate(wins):
+        want = refine_raw(i1, i2, u, v, Config(), shift=sh)
+        for q in ("ux", "uy", "energy", "resid"):
+            assert np.array_equal(got[k][q], want[q], equal_nan=True), (k, q)
+    assert refine_batch([], Config()) == []
+    z = np.zeros((0, 0), np.float32)
+    with pytest.raises(ValueError, match="window 1: empty"):
+        refine_batch(wins[:1] + [(z, z, z, z, (0, 0))], Config())
+    p45 = np.zeros((45, 45), np.float32)  # padded 109: a prime above 31
+    with pytest.raises(EngineError, match="window 2"):
+        refine_batch(wins[:2] + [(p45, p45, p45, p45, (0, 0))], Config())
+
+
 def test_track_pair_graph_replay_and_device_api():
     """The first call of a (size, configuration) runs eagerly and captures the pair as CUDA graphs; later calls
     replay them. Replays, a different size in between (which reallocates the pooled buffers and drops the
