@@ -840,17 +840,26 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_ref(const float2* 
                                                                float* __restrict__ amp) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* sm = (float2*)smraw;
-  const int pw = FIXL ? FIXL : plw.L, nb = fft_buf_len(pw, 1);
+  const int pw = FIXL ? FIXL : plw.L, nb = fft_buf_stride(pw, 1);
   float2* t = sm + 3 * nb;
   const int y = blockIdx.x, kk = blockIdx.y, k = k0 + kk;  // y: row of the W x H crop
   const size_t plane = (size_t)ph * pw;
-  for (int i = threadIdx.x; i < pw * 3; i += blockDim.x) {
-    int v = i / pw, x = i - v * pw;
-    sm[v * nb + x] = U[(size_t)(3 * kk + v) * plane + (size_t)(y + PAD) * pw + x];
+  // the three rows in three groups of asynchronous copies: rows 1 and 2 land while row 0 is transformed
+  for (int v = 0; v < 3; v++) {
+    const float2* src = U + (size_t)(3 * kk + v) * plane + (size_t)(y + PAD) * pw;
+    if (pw % 2 == 0) {  // 16-byte chunks: the row starts on a 16-byte boundary
+      for (int i = threadIdx.x; i < pw / 2; i += blockDim.x) __pipeline_memcpy_async(sm + v * nb + 2 * i, src + 2 * i, 16);
+    } else {
+      for (int i = threadIdx.x; i < pw; i += blockDim.x) __pipeline_memcpy_async(sm + v * nb + i, src + i, 8);
+    }
+    __pipeline_commit();
   }
-  __syncthreads();
   float2* rr[3];
   for (int v = 0; v < 3; v++) {
+    if (v == 0) __pipeline_wait_prior(2);
+    else if (v == 1) __pipeline_wait_prior(1);
+    else __pipeline_wait_prior(0);
+    __syncthreads();
     float2* res = fft_run<FIXL, 1>(sm + v * nb, t, plw, true);
     if (res != sm + v * nb) {
       for (int x = threadIdx.x; x < pw; x += blockDim.x) sm[v * nb + x] = res[x];
@@ -865,9 +874,10 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_ref(const float2* 
     double rre = a.x * sc, rim = a.y * sc;
     double xre = b.x * sc, xim = b.y * sc, yre = c.x * sc, yim = c.y * sc;
     double a2 = rre * rre + rim * rim + 1e-12;
-    // Im(conj(r) rx) / a2 (phaseflow.py:109-110)
-    double gx = (rre * xim - rim * xre) / a2;
-    double gy = (rre * yim - rim * yre) / a2;
+    // Im(conj(r) rx) / a2 (phaseflow.py:109-110), one reciprocal for both (stored as float32)
+    const double ia2 = 1.0 / a2;
+    double gx = (rre * xim - rim * xre) * ia2;
+    double gy = (rre * yim - rim * yre) * ia2;
     size_t o = (size_t)k * W * H + (size_t)y * W + x;
     ref4[o] = make_float4((float)rre, (float)rim, (float)gx, (float)gy);
     amp[o] = (float)sqrt(a2);
@@ -925,7 +935,7 @@ bool fft_fits(int ph, int pw) {
   try {
     int Tc = std::min(fft_threads(ph, 2), COLS_TMAX);
     if (smem_prefilter(ph, 2, Tc) > SMEM_MAX || 2 * (size_t)fft_buf_stride(ph, 2) * sizeof(float2) > SMEM_MAX) return false;
-    return 4 * fbytes(pw, 1) <= SMEM_MAX && smem_rows_resp(pw) <= SMEM_MAX;
+    return 4 * (size_t)fft_buf_stride(pw, 1) * sizeof(float2) <= SMEM_MAX && smem_rows_resp(pw) <= SMEM_MAX;
   } catch (const Error&) {
     return false;
   }
@@ -1010,7 +1020,7 @@ void launch_fft_cols_ref_f32(const float2* S, const FftPlan& plh, int pw, const 
 void launch_fft_rows_inv_ref_f32(const float2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,
                                  float4* ref4, float* amp, cudaStream_t st) {
   int T = fft_threads(plw.L, 1);
-  size_t sm = 4 * fbytes(plw.L, 1);
+  size_t sm = 4 * (size_t)fft_buf_stride(plw.L, 1) * sizeof(float2);
   dim3 grid(H, k1 - k0);
   by_length(plw.L, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
