@@ -643,23 +643,23 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_fwd(const float2* Tin
 constexpr int RESP_G = 4;
 
 // A[i] = raw[i] f(i, t_i) for the n values of a column pair, t_i the row table entry of element i (row i / 2). With
-// the length fixed (FIXL, blockDim = COLS_TMAX) the table loads of UN elements are issued together before their
+// the length fixed (FIXL, blockDim = NT) the table loads of UN elements are issued together before their
 // multiplies, so that their latencies overlap.
-template <int FIXL, int UN, class T, class Fn>
+template <int FIXL, int NT, int UN, class T, class Fn>
 __device__ __forceinline__ void cols_multiply(int n, const T* __restrict__ tab, Fn f) {
   if constexpr (FIXL > 0) {
-    constexpr int NI = (2 * FIXL + COLS_TMAX - 1) / COLS_TMAX;
+    constexpr int NI = (2 * FIXL + NT - 1) / NT;
 #pragma unroll
     for (int m0 = 0; m0 < NI; m0 += UN) {
       T tv[UN];
 #pragma unroll
       for (int u = 0; u < UN; u++) {
-        const int i = threadIdx.x + COLS_TMAX * (m0 + u);
+        const int i = threadIdx.x + NT * (m0 + u);
         if (m0 + u < NI && i < 2 * FIXL) tv[u] = __ldg(tab + (i >> 1));
       }
 #pragma unroll
       for (int u = 0; u < UN; u++) {
-        const int i = threadIdx.x + COLS_TMAX * (m0 + u);
+        const int i = threadIdx.x + NT * (m0 + u);
         if (m0 + u < NI && i < 2 * FIXL) f(i, tv[u]);
       }
     }
@@ -668,8 +668,13 @@ __device__ __forceinline__ void cols_multiply(int n, const T* __restrict__ tab, 
   }
 }
 
+// threads of the fixed-length column-pair kernel: the responses COLS_TMAX; the reference pack, whose float64 factors
+// take more time per element, one per radix-8 butterfly of the two columns (2 x 2112 / 8)
+constexpr int PAIR_T_REF = 544;
+template <bool REFPACK>
+constexpr int pair_threads(int fixl) { return fixl && REFPACK ? PAIR_T_REF : COLS_TMAX; }
 template <bool REFPACK, int FIXL>
-__global__ void __launch_bounds__(COLS_TMAX, 2) k_fft_cols_pair(const float2* __restrict__ S, FftPlan plh, int pw,
+__global__ void __launch_bounds__(pair_threads<REFPACK>(FIXL), 2) k_fft_cols_pair(const float2* __restrict__ S, FftPlan plh, int pw,
                                                                 GaborTables g, int k0, int k1, float2* __restrict__ U) {
   constexpr int C = 2;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -706,7 +711,7 @@ __global__ void __launch_bounds__(COLS_TMAX, 2) k_fft_cols_pair(const float2* __
     for (int k = blockIdx.y * RESP_G; k < kend; k++) {
       // G = (hx + omx omy) ex ey (bx by): the x factors of the thread's column, (omy, ey by) from the row table
       const float exb = __ldg(g.exf + (size_t)k * pw + x) * bx;
-      cols_multiply<FIXL, 14>(n, g.yt2 + (size_t)k * ph, [&](int i, float2 t) {
+      cols_multiply<FIXL, COLS_TMAX, 14>(n, g.yt2 + (size_t)k * ph, [&](int i, float2 t) {
         const float2 sv = raw[i];
         const float G = fmaf(hx, t.x, omx) * exb * t.y;
         A[i] = make_float2(sv.x * G, sv.y * G);
@@ -725,7 +730,7 @@ __global__ void __launch_bounds__(COLS_TMAX, 2) k_fft_cols_pair(const float2* __
       const double ex = g.ex[(size_t)k * pw + x];
       const double* eyk = g.ey + (size_t)k * ph;
       // the row factors omy[y] ey_k[y] (and fy[y]) gathered per element, their loads batched
-      cols_multiply<FIXL, 7>(n, g.omy, [&](int i, double omy) {
+      cols_multiply<FIXL, PAIR_T_REF, 4>(n, g.omy, [&](int i, double omy) {
         const int y = i >> 1;
         const float2 sv = raw[i];
         const double G = fma(hx, omy, omx) * ex * __ldg(eyk + y);
@@ -974,7 +979,7 @@ static void cols_inverse(const float2* S, const FftPlan& plh, int pw, const Gabo
   int nt = std::min(fft_threads(ph, C), COLS_TMAX);
   const size_t sm_p = smem_cols_pair(ph);
   if (sm_p <= SMEM_MAX) {
-    if (ph == FFT_FIXED_L && nt != COLS_TMAX) throw Error(OFC_ERR_DEVICE, "column pass: unexpected block size");
+    if (ph == FFT_FIXED_L) nt = pair_threads<REFPACK>(ph);  // the block size the fixed-length kernel assumes
     dim3 grid(div_up(pw, C), REFPACK ? 3 : div_up(g.F, RESP_G));
     by_length(ph, [&](auto fl) {
       constexpr int FL = decltype(fl)::value;

@@ -91,6 +91,63 @@ __device__ __forceinline__ void warp_dit(double2& v0, double2& v1, int n, bool i
   }
 }
 
+// The twiddles a lane of the 64-point transforms uses, held in registers (a shared table read by the lanes of a
+// warp at the strides (l & (h - 1)) 32 / h falls on few banks): w[0] = W_64^l for the outer radix-2 step, then
+// w[s] = W_64^((l & (h - 1)) 32 / h) for the steps h = 16, 8, 4, 2, 1 (s = 1..5).
+struct Tw64 {
+  double2 w[6];
+};
+__device__ __forceinline__ Tw64 lane_tw64(const double2* tw64) {
+  const int l = threadIdx.x & 31;
+  Tw64 t;
+  t.w[0] = tw64[l];
+  int s = 1;
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1, s++) t.w[s] = tw64[(l & (h - 1)) * (32 / h)];
+  return t;
+}
+__device__ __forceinline__ double2 cjif(double2 w, bool inv) { return inv ? make_double2(w.x, -w.y) : w; }
+
+// warp_dif / warp_dit for n = 64 with the lane's twiddles in registers (the same arithmetic)
+__device__ __forceinline__ void warp_dif64(double2& v0, double2& v1, bool inv, const Tw64& T) {
+  const int l = threadIdx.x & 31;
+  {
+    double2 a = make_double2(v0.x + v1.x, v0.y + v1.y);
+    double2 b = dmul(make_double2(v0.x - v1.x, v0.y - v1.y), cjif(T.w[0], inv));
+    v0 = a;
+    v1 = b;
+  }
+  int s = 1;
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1, s++) {
+    const bool up = (l & h) != 0;
+    const double2 w = cjif(T.w[s], inv);
+    double2 p0 = shfl_xor_d2(v0, h);
+    v0 = up ? dmul(make_double2(p0.x - v0.x, p0.y - v0.y), w) : make_double2(v0.x + p0.x, v0.y + p0.y);
+    double2 p1 = shfl_xor_d2(v1, h);
+    v1 = up ? dmul(make_double2(p1.x - v1.x, p1.y - v1.y), w) : make_double2(v1.x + p1.x, v1.y + p1.y);
+  }
+}
+__device__ __forceinline__ void warp_dit64(double2& v0, double2& v1, bool inv, const Tw64& T) {
+  const int l = threadIdx.x & 31;
+  int s = 5;
+#pragma unroll
+  for (int h = 1; h <= 16; h <<= 1, s--) {
+    const bool up = (l & h) != 0;
+    const double2 w = cjif(T.w[s], inv);
+    double2 t0 = up ? dmul(v0, w) : v0;
+    double2 p0 = shfl_xor_d2(t0, h);
+    v0 = up ? make_double2(p0.x - t0.x, p0.y - t0.y) : make_double2(t0.x + p0.x, t0.y + p0.y);
+    double2 t1 = up ? dmul(v1, w) : v1;
+    double2 p1 = shfl_xor_d2(t1, h);
+    v1 = up ? make_double2(p1.x - t1.x, p1.y - t1.y) : make_double2(t1.x + p1.x, t1.y + p1.y);
+  }
+  double2 t = dmul(v1, cjif(T.w[0], inv));
+  double2 a = make_double2(v0.x + t.x, v0.y + t.y), b = make_double2(v0.x - t.x, v0.y - t.y);
+  v0 = a;
+  v1 = b;
+}
+
 __device__ __forceinline__ int brev(int i, int bits) { return (int)(__brev((unsigned)i) >> (32 - bits)); }
 __device__ __forceinline__ int ilog2(int n) { return 31 - __clz(n); }
 
@@ -350,7 +407,7 @@ __device__ __forceinline__ int brev5(int i) { return (int)(__brev((unsigned)i) >
 
 // forward rows of a real 64 x 64 window (get(y, x) minus mean, Hann weighted) into the half spectrum Hz
 template <class Get>
-__device__ void rows_forward64(Get get, double mean, const PocConst& pc, double2* Hz) {
+__device__ void rows_forward64(Get get, double mean, const PocConst& pc, const Tw64& tw, double2* Hz) {
   const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
   // lane l holds Z[k0] (register 0) and Z[k0 + 1] (register 1), k0 = 2 brev5(l) (the bit-reversed output);
   // Z[-k0] lies in register 0 of lane pl0, Z[-(k0 + 1)] in register 1 of lane 31 - l
@@ -360,7 +417,7 @@ __device__ void rows_forward64(Get get, double mean, const PocConst& pc, double2
     double2 v0 = make_double2((get(y1, l) - mean) * (pc.hy[y1] * pc.hx[l]), (get(y2, l) - mean) * (pc.hy[y2] * pc.hx[l]));
     double2 v1 = make_double2((get(y1, l + 32) - mean) * (pc.hy[y1] * pc.hx[l + 32]),
                               (get(y2, l + 32) - mean) * (pc.hy[y2] * pc.hx[l + 32]));
-    warp_dif(v0, v1, 64, false, pc.tw64);
+    warp_dif64(v0, v1, false, tw);
     const double2 p0 = shfl_d2(v0, pl0), p1 = shfl_d2(v1, 31 - l);
     auto unpack = [&](double2 z, double2 q, int k) {
       if (k <= 16) {
@@ -378,20 +435,20 @@ __device__ __forceinline__ int lp_row64(int ky) { return ky <= 16 ? ky : (ky >= 
 
 // poc_shift (poc.py:39-54) of window B = b[y0 : y0 + 64, x0 : x0 + 64] against A's half spectrum on the low-pass
 // support (alp[iy * 17 + kx], iy = 0..32); res = (dx, dy, peak)
-__device__ void poc_shift64(const double* __restrict__ b, int W, int x0, int y0, const PocConst& pc,
+__device__ void poc_shift64(const double* __restrict__ b, int W, int x0, int y0, const PocConst& pc, const Tw64& tw,
                             const double2* alp, double lpm, double2* Hz, double* surf, double* red, double* res) {
   const int wid = threadIdx.x >> 5, l = threadIdx.x & 31;
   double s = 0;
   for (int i = threadIdx.x; i < 4096; i += POC_T) s += b[(size_t)(y0 + (i >> 6)) * W + x0 + (i & 63)];
   const double mean = block_sum_d(s, red) / 4096.0;
   const double* bw = b + (size_t)y0 * W + x0;
-  rows_forward64([&](int y, int x) { return bw[(size_t)y * W + x]; }, mean, pc, Hz);
+  rows_forward64([&](int y, int x) { return bw[(size_t)y * W + x]; }, mean, pc, tw, Hz);
   __syncthreads();
   // columns kx = 0..16: forward (dif) -> C = B conj(A) / (|.| + 1e-12) on the low-pass rows, 0 elsewhere ->
   // inverse (dit) back to natural order
   for (int ci = wid; ci < ZS; ci += POC_T / 32) {
     double2 v0 = Hz[l * ZS + ci], v1 = Hz[(l + 32) * ZS + ci];
-    warp_dif(v0, v1, 64, false, pc.tw64);
+    warp_dif64(v0, v1, false, tw);
     for (int r = 0; r < 2; r++) {
       double2& v = r == 0 ? v0 : v1;
       const int iy = lp_row64(brev(32 * r + l, 6));
@@ -405,7 +462,7 @@ __device__ void poc_shift64(const double* __restrict__ b, int W, int x0, int y0,
       }
       v = cc;
     }
-    warp_dit(v0, v1, 64, true, pc.tw64);
+    warp_dit64(v0, v1, true, tw);
     Hz[l * ZS + ci] = v0;
     Hz[(l + 32) * ZS + ci] = v1;
   }
@@ -428,7 +485,7 @@ __device__ void poc_shift64(const double* __restrict__ b, int W, int x0, int y0,
       const double2 d1 = Hz[y1 * ZS + m], d2 = Hz[y2 * ZS + m];  // conj d1 + i conj d2
       v1 = make_double2(d1.x + d2.y, -d1.y + d2.x);
     }
-    warp_dif(v0, v1, 64, true, pc.tw64);
+    warp_dif64(v0, v1, true, tw);
     for (int r = 0; r < 2; r++) {
       const double2 v = r == 0 ? v0 : v1;
       const int x = brev(32 * r + l, 6);
@@ -436,7 +493,7 @@ __device__ void poc_shift64(const double* __restrict__ b, int W, int x0, int y0,
       for (int h = 0; h < 2; h++) {
         const int y = h == 0 ? y1 : y2;
         const double val = (h == 0 ? v.x : v.y) * sc;
-        surf[y * 64 + x] = val;
+        surf[y * 64 + 32 * r + l] = val;  // stored in the transform's (bit-reversed) column order
         const int idx = ((y + 32) & 63) * 64 + sxx;
         const bool vn = val != val;
         const bool take = bnan ? (vn && idx < bi) : (vn || val > best || (val == best && idx < bi));
@@ -465,7 +522,8 @@ __device__ void poc_shift64(const double* __restrict__ b, int W, int x0, int y0,
     int iy = bi >> 6, ix = bi & 63;
     iy = min(max(iy, 1), 62);
     ix = min(max(ix, 1), 62);
-    auto R = [&](int ys, int xs) { return surf[((ys + 32) & 63) * 64 + ((xs + 32) & 63)]; };  // the shifted surface
+    // the shifted surface; column x of the unshifted surface sits at position brev6(x) of its row
+    auto R = [&](int ys, int xs) { return surf[((ys + 32) & 63) * 64 + brev((xs + 32) & 63, 6)]; };
     auto parabola = [](double m, double c, double p) {  // poc.py:34-36
       double den = m - 2.0 * c + p;
       return den == 0 ? 0.0 : 0.5 * (m - p) / den;
@@ -501,14 +559,15 @@ __global__ void __launch_bounds__(POC_T, 2) k_poc_grid64(const double* __restric
   __syncthreads();
   // half spectrum of A (poc.py:44) on the low-pass support: alp[iy * 17 + kx]
   const double* aw = a + (size_t)(y - 32) * W + (x - 32);
+  const Tw64 tw = lane_tw64(pc.tw64);
   double s = 0;
   for (int t = threadIdx.x; t < 4096; t += POC_T) s += aw[(size_t)(t >> 6) * W + (t & 63)];
   const double mean = block_sum_d(s, red) / 4096.0;
-  rows_forward64([&](int yy, int xx) { return aw[(size_t)yy * W + xx]; }, mean, pc, Hz);
+  rows_forward64([&](int yy, int xx) { return aw[(size_t)yy * W + xx]; }, mean, pc, tw, Hz);
   __syncthreads();
   for (int ci = wid; ci < ZS; ci += POC_T / 32) {
     double2 v0 = Hz[l * ZS + ci], v1 = Hz[(l + 32) * ZS + ci];
-    warp_dif(v0, v1, 64, false, pc.tw64);
+    warp_dif64(v0, v1, false, tw);
     for (int r = 0; r < 2; r++) {
       const int iy = lp_row64(brev(32 * r + l, 6));
       if (iy >= 0) alp[iy * ZS + ci] = r == 0 ? v0 : v1;
@@ -521,7 +580,7 @@ __global__ void __launch_bounds__(POC_T, 2) k_poc_grid64(const double* __restric
     double ox = rint(dx), oy = rint(dy);  // Python round(): half to even
     long y0 = y - 32 + (long)oy, x0 = x - 32 + (long)ox;
     if (y0 < 0 || x0 < 0 || y0 + 64 > H || x0 + 64 > W) { pk = 0.0; break; }
-    poc_shift64(b, W, (int)x0, (int)y0, pc, alp, lpm, Hz, surf, red, res);
+    poc_shift64(b, W, (int)x0, (int)y0, pc, tw, alp, lpm, Hz, surf, red, res);
     double sx = res[0], sy = res[1];
     pk = res[2];
     dx = ox + sx;
