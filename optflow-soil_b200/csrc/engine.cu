@@ -210,6 +210,10 @@ struct Lane {
   std::unordered_map<std::string, std::unique_ptr<DevBuf>> pool;
   std::map<int, std::pair<FftPlan, std::unique_ptr<DevBuf>>> plans;
   cudaEvent_t ev[4] = {};
+  // a second compute stream for work that overlaps the main one inside a pair (the reference pack beside the
+  // coarse stage) and its fork / join events
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   // the copy stream of batched calls and its ordering events (created on first use)
   cudaStream_t copy = nullptr;
   cudaEvent_t bev[8] = {};
@@ -430,8 +434,8 @@ const double* moment_taps(Lane& L, double sigma, int& r, MomTaps& tp) {
 // reference_phase (phaseflow.py:100-111) of i1: float32 transforms, as the reference's Rust port computes them
 // (gabor.rs:230-270, rustfft f32), with (r.re, r.im, gx, gy) and amp formed per pixel in float64 and stored
 // float32 per filter. Filters are processed in groups to bound the scratch (3 planes of ph x pw per filter).
-void reference_pack(Lane& L, const float* i1, int W, int H, const GaborTables& g, float4* ref4, float* amp) {
-  cudaStream_t st = L.stream;
+void reference_pack(Lane& L, const float* i1, int W, int H, const GaborTables& g, float4* ref4, float* amp,
+                    cudaStream_t st) {
   const int ph = H + 2 * PAD, pw = W + 2 * PAD;
   const size_t Np = (size_t)ph * pw;
   const int G = std::min(g.F, 4);
@@ -448,10 +452,26 @@ void reference_pack(Lane& L, const float* i1, int W, int H, const GaborTables& g
   }
 }
 
+// The parts of refine_dev that depend on the images only: the reference pack of i1 and the spline of i2, on
+// stream st (the pair path runs them on the lane's side stream beside the coarse stage).
+void fine_prep(Lane& L, const float* i1, int W, int H, const float* i2, int w2, int h2, const ofc_config& c,
+               cudaStream_t st) {
+  const size_t N = (size_t)W * H;
+  const int ph = H + 2 * PAD, pw = W + 2 * PAD;
+  const int F = c.n_scales * c.n_orient;
+  GaborTables g = upload_gabor(L, ph, pw, c);
+  float4* ref4 = L.get<float4>("ref4", N * F);
+  float* amp = L.get<float>("ref_amp", N * F);
+  reference_pack(L, i1, W, H, g, ref4, amp, st);
+  float* c2 = L.get<float>("spline2", (size_t)w2 * h2);
+  double* tmp2 = L.get<double>("spline2_tmp", (size_t)w2 * h2 * 2);
+  launch_bspline_f32(i2, c2, tmp2, w2, h2, st);
+}
+
 // refine_raw (phaseflow.rs:1514-1613 / phaseflow.py:427-507) on the device. u2: 2 planes (ux | uy) holding
-// the start and receiving the result.
+// the start and receiving the result. prepared: fine_prep already ran for these images (ordered before this call).
 FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int w2, int h2, long shx, long shy,
-                   double* u2, const ofc_config& c) {
+                   double* u2, const ofc_config& c, bool prepared) {
   cudaStream_t st = L.stream;
   const size_t N = (size_t)W * H;
   const int ph = H + 2 * PAD, pw = W + 2 * PAD;
@@ -471,11 +491,9 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
   float2* U = L.get<float2>("fft_U", Np * F);
   float4* ref4 = L.get<float4>("ref4", N * F);
   float* amp = L.get<float>("ref_amp", N * F);
-  reference_pack(L, i1, W, H, g, ref4, amp);
   // spline of image 2 (kept for all iterations)
   float* c2 = L.get<float>("spline2", (size_t)w2 * h2);
-  double* tmp2 = L.get<double>("spline2_tmp", (size_t)w2 * h2 * 2);
-  launch_bspline_f32(i2, c2, tmp2, w2, h2, st);
+  if (!prepared) fine_prep(L, i1, W, H, i2, w2, h2, c, st);
 
   double* u2b = L.get<double>("u2b", 2 * N);
   double* s2 = L.get<double>("s2", 2 * N);
@@ -683,6 +701,11 @@ void pair_stage(Lane& L, int stage, int W, int H, bool has_roi, bool has_init, c
   double* conf64 = L.get<double>("conf64", N);
   uint8_t* low = L.get<uint8_t>("low_final", N);
   if (stage == 0) {
+    // the reference pack of i1 and the spline of i2 on the side stream, beside the coarse stage (joined below)
+    OFC_CUDA(cudaEventRecord(L.fork, st));
+    OFC_CUDA(cudaStreamWaitEvent(L.side, L.fork, 0));
+    fine_prep(L, i1, W, H, i2, W, H, c, L.side);
+    OFC_CUDA(cudaEventRecord(L.join, L.side));
     double* init = nullptr;
     if (has_init) {
       init = L.get<double>("init2", 2 * N);
@@ -691,8 +714,9 @@ void pair_stage(Lane& L, int stage, int W, int H, bool has_roi, bool has_init, c
     }
     CoarseOut g = coarse_dev(L, i1, i2, W, H, init, c);
     dense_start(L, g, W, H, init, u2);
+    OFC_CUDA(cudaStreamWaitEvent(st, L.join, 0));
   } else if (stage == 1) {
-    FineOut f = refine_dev(L, i1, W, H, i2, W, H, 0, 0, u2, c);
+    FineOut f = refine_dev(L, i1, W, H, i2, W, H, 0, 0, u2, c, true);
     double B = guard_px(c) > 0 ? 4.0 * c.sigma_w : 0.0;
     launch_confidence(f.energy, f.resid, f.ux, f.uy, W, H, f.stats, c.phase_tol, c.conf_min, true, B, nullptr,
                       conf64, low, nullptr, st);
@@ -931,6 +955,9 @@ ofc_engine* ofc_create(int device, int lanes, char* err, size_t errlen) {
     for (int i = 0; i < lanes; i++) {
       std::unique_ptr<Lane> l(new Lane());
       OFC_CUDA(cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking));
+      OFC_CUDA(cudaStreamCreateWithFlags(&l->side, cudaStreamNonBlocking));
+      OFC_CUDA(cudaEventCreateWithFlags(&l->fork, cudaEventDisableTiming));
+      OFC_CUDA(cudaEventCreateWithFlags(&l->join, cudaEventDisableTiming));
       for (auto& ev : l->ev) OFC_CUDA(cudaEventCreate(&ev));
       eng->lanes.push_back(std::move(l));
     }
@@ -948,8 +975,12 @@ void ofc_destroy(ofc_engine* e) {
     std::lock_guard<std::mutex> lk(l->busy);
     cudaStreamSynchronize(l->stream);
     if (l->copy) cudaStreamSynchronize(l->copy);
+    cudaStreamSynchronize(l->side);
     l->release();
     for (auto& ev : l->ev) cudaEventDestroy(ev);
+    cudaEventDestroy(l->fork);
+    cudaEventDestroy(l->join);
+    cudaStreamDestroy(l->side);
     if (l->copy) {
       for (auto& ev : l->bev) cudaEventDestroy(ev);
       cudaStreamDestroy(l->copy);
@@ -1006,7 +1037,7 @@ int ofc_refine_raw(ofc_engine* e, const float* i1, size_t w, size_t h, const flo
     double* u2 = L.get<double>("u2", 2 * N);
     launch_f32_to_f64(du, u2, N, st);
     launch_f32_to_f64(dv, u2 + N, N, st);
-    FineOut f = refine_dev(L, d1, (int)w, (int)h, d2, (int)w2, (int)h2, (long)shift_x, (long)shift_y, u2, *c);
+    FineOut f = refine_dev(L, d1, (int)w, (int)h, d2, (int)w2, (int)h2, (long)shift_x, (long)shift_y, u2, *c, false);
     if (out_ux) OFC_CUDA(cudaMemcpyAsync(out_ux, f.ux, N * 8, cudaMemcpyDeviceToHost, st));
     if (out_uy) OFC_CUDA(cudaMemcpyAsync(out_uy, f.uy, N * 8, cudaMemcpyDeviceToHost, st));
     if (out_energy) OFC_CUDA(cudaMemcpyAsync(out_energy, f.energy, N * 8, cudaMemcpyDeviceToHost, st));
@@ -1089,7 +1120,7 @@ int ofc_refine_batch(ofc_engine* e, const ofc_window* wins, size_t n, const ofc_
       launch_f32_to_f64(inu[s2], u2, N, st);
       launch_f32_to_f64(inv[s2], u2 + N, N, st);
       FineOut f = refine_dev(L, in1[s2], (int)w.w, (int)w.h, in2[s2], (int)w.w2, (int)w.h2, (long)w.shift_x,
-                             (long)w.shift_y, u2, *c);
+                             (long)w.shift_y, u2, *c, false);
       OFC_CUDA(cudaEventRecord(in_free[s2], st));
       if (k >= 2) OFC_CUDA(cudaStreamWaitEvent(st, out_done[s2], 0));  // staging set s2 held window k - 2
       const double* res[4] = {f.ux, f.uy, f.energy, f.resid};
@@ -1124,7 +1155,7 @@ int ofc_refine(ofc_engine* e, const float* i1, const float* i2, size_t w, size_t
     double* u2 = L.get<double>("u2", 2 * N);
     launch_f32_to_f64(du, u2, N, st);
     launch_f32_to_f64(dv, u2 + N, N, st);
-    FineOut f = refine_dev(L, d1, (int)w, (int)h, d2, (int)w, (int)h, 0, 0, u2, *c);
+    FineOut f = refine_dev(L, d1, (int)w, (int)h, d2, (int)w, (int)h, 0, 0, u2, *c, false);
     float* conf = L.get<float>("out_conf", N);
     uint8_t* low = L.get<uint8_t>("low_final", N);
     double B = guard_px(*c) > 0 ? 4.0 * c->sigma_w : 0.0;
@@ -1353,7 +1384,7 @@ int ofc_test_reference_phase(ofc_engine* e, const float* i1, size_t w, size_t h,
     float* d1 = L.upload("in_i1", i1, N);
     float4* ref4 = L.get<float4>("ref4", N * F);
     float* a = L.get<float>("ref_amp", N * F);
-    reference_pack(L, d1, W, H, g, ref4, a);
+    reference_pack(L, d1, W, H, g, ref4, a, L.stream);
     std::vector<float4> h4(N * F);
     OFC_CUDA(cudaMemcpyAsync(h4.data(), ref4, N * F * sizeof(float4), cudaMemcpyDeviceToHost, L.stream));
     if (amp) OFC_CUDA(cudaMemcpyAsync(amp, a, N * F * sizeof(float), cudaMemcpyDeviceToHost, L.stream));
@@ -1495,7 +1526,7 @@ int ofc_test_first_sums(ofc_engine* e, const float* i1, const float* i2, size_t 
     float2* U = L.get<float2>("fft_U", Np * F);
     float4* ref4 = L.get<float4>("ref4", N * F);
     float* amp = L.get<float>("ref_amp", N * F);
-    reference_pack(L, d1, W, H, g, ref4, amp);
+    reference_pack(L, d1, W, H, g, ref4, amp, L.stream);
     float* c2 = L.get<float>("spline2", N);
     double* tmp2 = L.get<double>("spline2_tmp", 2 * N);
     launch_bspline_f32(d2, c2, tmp2, W, H, st);
