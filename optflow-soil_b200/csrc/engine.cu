@@ -667,8 +667,10 @@ void dense_start(Lane& L, const CoarseOut& g, int W, int H, const double* init, 
 }
 
 // _finish (track.py:56-108): low (u8), roi (u8 or null), ux/uy (raw, f64) -> outputs
+// fine_planes: o.conf, o.raw_ux and o.raw_uy were written already (the pair path writes them at the end of the fine
+// stage, so that a host download of them overlaps this stage)
 void finish_dev(Lane& L, const uint8_t* low, const uint8_t* roi, const double* ux, const double* uy,
-                const double* conf64, int W, int H, const ofc_config& c, const ofc_pair_out& o) {
+                const double* conf64, int W, int H, const ofc_config& c, const ofc_pair_out& o, bool fine_planes) {
   cudaStream_t st = L.stream;
   const size_t N = (size_t)W * H;
   double guard = guard_px(c);
@@ -685,7 +687,10 @@ void finish_dev(Lane& L, const uint8_t* low, const uint8_t* roi, const double* u
   double* yp = L.get<double>("strain_y", 11 * N);
   launch_strain(mx, my, W, H, c.strain_win, yp, nullptr, nullptr, nullptr, nullptr, o.exx, o.eyy, o.exy, o.gmax, o.vol,
                 st);
-  launch_pair_outputs(mx, my, ux, uy, conf64, (int)N, o.ux, o.uy, o.conf, o.valid, o.raw_ux, o.raw_uy, st);
+  if (fine_planes)
+    launch_pair_outputs(mx, my, ux, uy, conf64, (int)N, o.ux, o.uy, nullptr, o.valid, nullptr, nullptr, st);
+  else
+    launch_pair_outputs(mx, my, ux, uy, conf64, (int)N, o.ux, o.uy, o.conf, o.valid, o.raw_ux, o.raw_uy, st);
 }
 
 // the whole pair on device buffers; d_out fields are device pointers
@@ -718,8 +723,12 @@ void pair_stage(Lane& L, int stage, int W, int H, bool has_roi, bool has_init, c
   } else if (stage == 1) {
     FineOut f = refine_dev(L, i1, W, H, i2, W, H, 0, 0, u2, c, true);
     double B = guard_px(c) > 0 ? 4.0 * c.sigma_w : 0.0;
-    launch_confidence(f.energy, f.resid, f.ux, f.uy, W, H, f.stats, c.phase_tol, c.conf_min, true, B, nullptr,
+    // the output planes that depend on the fine stage only: conf, raw_ux, raw_uy (device_pair_out's layout)
+    float* op = L.get<float>("out_pair", 10 * N);
+    launch_confidence(f.energy, f.resid, f.ux, f.uy, W, H, f.stats, c.phase_tol, c.conf_min, true, B, op + 2 * N,
                       conf64, low, nullptr, st);
+    launch_f64_to_f32(u2, op + 8 * N, N, st);
+    launch_f64_to_f32(u2 + N, op + 9 * N, N, st);
   } else {
     ofc_pair_out o{};
     float* p = L.get<float>("out_pair", 10 * N);
@@ -727,14 +736,15 @@ void pair_stage(Lane& L, int stage, int W, int H, bool has_roi, bool has_init, c
     for (int i = 0; i < 10; i++) *f[i] = p + i * N;
     o.valid = L.get<uint8_t>("out_valid", N);
     const uint8_t* roi = has_roi ? L.get<uint8_t>("in_roi", N) : nullptr;
-    finish_dev(L, low, roi, u2, u2 + N, conf64, W, H, c, o);
+    finish_dev(L, low, roi, u2, u2 + N, conf64, W, H, c, o, true);
   }
 }
 
 // Runs the three stages on L.stream. The first call for a (size, configuration, inputs present, profile filter)
 // runs them eagerly, which allocates every buffer and uploads every constant, and then captures each stage as a
-// CUDA graph; later calls replay the graphs. timing (nullable): seconds per stage from events between the stages.
-void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_config& c, double* timing) {
+// CUDA graph; later calls replay the graphs. timing: record the stage events L.ev[0..3] (the start of each stage
+// and the end), which pair_timing reads.
+void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_config& c, bool timing) {
   cudaStream_t st = L.stream;
   Profiler* prof = g_profiler;
   const std::string key = std::to_string(W) + "x" + std::to_string(H) + ":" + cfg_key(c) + ":" +
@@ -803,12 +813,14 @@ void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_conf
       }
     }
   }
-  if (timing) {
-    OFC_CUDA(cudaEventSynchronize(L.ev[3]));
-    float ms[3];
-    for (int i = 0; i < 3; i++) OFC_CUDA(cudaEventElapsedTime(&ms[i], L.ev[i], L.ev[i + 1]));
-    for (int i = 0; i < 3; i++) timing[i] = ms[i] * 1e-3;
-  }
+}
+
+// seconds per stage of the last run_pair that recorded its stage events (waits for its end)
+void pair_timing(Lane& L, double* timing) {
+  OFC_CUDA(cudaEventSynchronize(L.ev[3]));
+  float ms[3];
+  for (int i = 0; i < 3; i++) OFC_CUDA(cudaEventElapsedTime(&ms[i], L.ev[i], L.ev[i + 1]));
+  for (int i = 0; i < 3; i++) timing[i] = ms[i] * 1e-3;
 }
 
 void check_sizes(size_t w, size_t h) {
@@ -1281,7 +1293,7 @@ int ofc_finish(ofc_engine* e, const float* ux, const float* uy, const float* con
     uint8_t* low = L.get<uint8_t>("low_final", N);
     ofc_threshold_low(c64, c->conf_min, low, N, st);
     ofc_pair_out d = device_pair_out(L, N);
-    finish_dev(L, low, droi, u2, u2 + N, c64, (int)w, (int)h, *c, d);
+    finish_dev(L, low, droi, u2, u2 + N, c64, (int)w, (int)h, *c, d, false);
     download_pair(L, d, out, N);
     OFC_CUDA(cudaStreamSynchronize(st));
     std::memset(out->timing, 0, sizeof(out->timing));
@@ -1306,10 +1318,33 @@ int ofc_track_pair(ofc_engine* e, const float* i1, const float* i2, size_t w, si
       L.upload("in_u", init_ux, N);
       L.upload("in_v", init_uy, N);
     }
-    double timing[3] = {0, 0, 0};
-    run_pair(L, (int)w, (int)h, roi != nullptr, init_ux != nullptr, *c, timing);
-    download_pair(L, device_pair_out(L, N), out, N);
+    run_pair(L, (int)w, (int)h, roi != nullptr, init_ux != nullptr, *c, true);
+    // conf, raw_ux and raw_uy are final when the fine stage ends (event ev[2]): their download runs on the copy
+    // stream during the finish stage; the other planes follow it on the lane's stream
+    const ofc_pair_out d = device_pair_out(L, N);
+    L.ensure_copy_stream();
+    struct Drain {
+      cudaStream_t a, b;
+      ~Drain() {
+        cudaStreamSynchronize(a);
+        cudaStreamSynchronize(b);
+      }
+    } drain{L.copy, L.stream};
+    OFC_CUDA(cudaStreamWaitEvent(L.copy, L.ev[2], 0));
+    ofc_pair_out early{}, late = *out;
+    early.conf = out->conf;
+    early.raw_ux = out->raw_ux;
+    early.raw_uy = out->raw_uy;
+    late.conf = late.raw_ux = late.raw_uy = nullptr;
+    cudaStream_t keep = L.stream;
+    L.stream = L.copy;
+    download_pair(L, d, &early, N);
+    L.stream = keep;
+    download_pair(L, d, &late, N);
+    OFC_CUDA(cudaStreamSynchronize(L.copy));
     OFC_CUDA(cudaStreamSynchronize(L.stream));
+    double timing[3];
+    pair_timing(L, timing);
     for (int i = 0; i < 3; i++) out->timing[i] = timing[i];
   });
 }
@@ -1338,7 +1373,7 @@ int ofc_track_pair_device(ofc_engine* e, const float* d_i1, const float* d_i2, s
         OFC_CUDA(cudaMemcpyAsync(L.get<float>("in_u", N), d_init_ux, N * 4, cudaMemcpyDeviceToDevice, st));
         OFC_CUDA(cudaMemcpyAsync(L.get<float>("in_v", N), d_init_uy, N * 4, cudaMemcpyDeviceToDevice, st));
       }
-      run_pair(L, (int)w, (int)h, d_roi != nullptr, d_init_ux != nullptr, *c, nullptr);
+      run_pair(L, (int)w, (int)h, d_roi != nullptr, d_init_ux != nullptr, *c, false);
       const ofc_pair_out d = device_pair_out(L, N);
       float* const* dsrc[10] = {&d.ux, &d.uy, &d.conf, &d.exx, &d.eyy, &d.exy, &d.gmax, &d.vol, &d.raw_ux, &d.raw_uy};
       float* const* udst[10] = {&d_out->ux,  &d_out->uy,  &d_out->conf, &d_out->exx,    &d_out->eyy,
