@@ -214,6 +214,7 @@ struct Lane {
   // coarse stage) and its fork / join events
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  cudaEvent_t masked = nullptr;  // the pair's masked field and valid mask are written (recorded inside its finish stage)
   // the copy stream of batched calls and its ordering events (created on first use)
   cudaStream_t copy = nullptr;
   cudaEvent_t bev[8] = {};
@@ -684,13 +685,20 @@ void finish_dev(Lane& L, const uint8_t* low, const uint8_t* roi, const double* u
   double* my = mx + N;
   if (guard > 0) launch_large_components(low, W, H, min_area_px(c), parent, size, big, st);
   launch_finish_mask(low, roi, big, W, H, guard, ux, uy, src, bad, vdist, mx, my, st);
+  // the masked field and the valid mask first; then the event L.masked (a host download of those planes may start
+  // there, during the strain)
+  if (fine_planes) {
+    launch_pair_outputs(mx, my, ux, uy, conf64, (int)N, o.ux, o.uy, nullptr, o.valid, nullptr, nullptr, st);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    OFC_CUDA(cudaStreamIsCapturing(st, &cap));
+    if (cap == cudaStreamCaptureStatusActive) OFC_CUDA(cudaEventRecordWithFlags(L.masked, st, cudaEventRecordExternal));
+    else OFC_CUDA(cudaEventRecord(L.masked, st));
+  } else {
+    launch_pair_outputs(mx, my, ux, uy, conf64, (int)N, o.ux, o.uy, o.conf, o.valid, o.raw_ux, o.raw_uy, st);
+  }
   double* yp = L.get<double>("strain_y", 11 * N);
   launch_strain(mx, my, W, H, c.strain_win, yp, nullptr, nullptr, nullptr, nullptr, o.exx, o.eyy, o.exy, o.gmax, o.vol,
                 st);
-  if (fine_planes)
-    launch_pair_outputs(mx, my, ux, uy, conf64, (int)N, o.ux, o.uy, nullptr, o.valid, nullptr, nullptr, st);
-  else
-    launch_pair_outputs(mx, my, ux, uy, conf64, (int)N, o.ux, o.uy, o.conf, o.valid, o.raw_ux, o.raw_uy, st);
 }
 
 // the whole pair on device buffers; d_out fields are device pointers
@@ -970,6 +978,7 @@ ofc_engine* ofc_create(int device, int lanes, char* err, size_t errlen) {
       OFC_CUDA(cudaStreamCreateWithFlags(&l->side, cudaStreamNonBlocking));
       OFC_CUDA(cudaEventCreateWithFlags(&l->fork, cudaEventDisableTiming));
       OFC_CUDA(cudaEventCreateWithFlags(&l->join, cudaEventDisableTiming));
+      OFC_CUDA(cudaEventCreateWithFlags(&l->masked, cudaEventDisableTiming));
       for (auto& ev : l->ev) OFC_CUDA(cudaEventCreate(&ev));
       eng->lanes.push_back(std::move(l));
     }
@@ -992,6 +1001,7 @@ void ofc_destroy(ofc_engine* e) {
     for (auto& ev : l->ev) cudaEventDestroy(ev);
     cudaEventDestroy(l->fork);
     cudaEventDestroy(l->join);
+    cudaEventDestroy(l->masked);
     cudaStreamDestroy(l->side);
     if (l->copy) {
       for (auto& ev : l->bev) cudaEventDestroy(ev);
@@ -1319,8 +1329,9 @@ int ofc_track_pair(ofc_engine* e, const float* i1, const float* i2, size_t w, si
       L.upload("in_v", init_uy, N);
     }
     run_pair(L, (int)w, (int)h, roi != nullptr, init_ux != nullptr, *c, true);
-    // conf, raw_ux and raw_uy are final when the fine stage ends (event ev[2]): their download runs on the copy
-    // stream during the finish stage; the other planes follow it on the lane's stream
+    // conf, raw_ux and raw_uy are final when the fine stage ends (event ev[2]), ux, uy and valid when the finish
+    // stage has masked the field (event L.masked): their downloads run on the copy stream during the rest of the
+    // pair; the strain planes follow on the lane's stream
     const ofc_pair_out d = device_pair_out(L, N);
     L.ensure_copy_stream();
     struct Drain {
@@ -1331,14 +1342,20 @@ int ofc_track_pair(ofc_engine* e, const float* i1, const float* i2, size_t w, si
       }
     } drain{L.copy, L.stream};
     OFC_CUDA(cudaStreamWaitEvent(L.copy, L.ev[2], 0));
-    ofc_pair_out early{}, late = *out;
+    ofc_pair_out early{}, masked{}, late = *out;
     early.conf = out->conf;
     early.raw_ux = out->raw_ux;
     early.raw_uy = out->raw_uy;
-    late.conf = late.raw_ux = late.raw_uy = nullptr;
+    masked.ux = out->ux;
+    masked.uy = out->uy;
+    masked.valid = out->valid;
+    late.conf = late.raw_ux = late.raw_uy = late.ux = late.uy = nullptr;
+    late.valid = nullptr;
     cudaStream_t keep = L.stream;
     L.stream = L.copy;
     download_pair(L, d, &early, N);
+    OFC_CUDA(cudaStreamWaitEvent(L.copy, L.masked, 0));  // ux, uy, valid during the strain
+    download_pair(L, d, &masked, N);
     L.stream = keep;
     download_pair(L, d, &late, N);
     OFC_CUDA(cudaStreamSynchronize(L.copy));

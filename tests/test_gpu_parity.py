@@ -212,6 +212,22 @@ def test_track_pair_graph_replay_and_device_api():
                 np.testing.assert_array_equal(getattr(r, k), getattr(first, k), err_msg=k)
             for k in ("Exx", "Eyy", "Exy", "gmax", "vol"):
                 np.testing.assert_array_equal(r.strain[k], first.strain[k], err_msg=k)
+        # another pair of the same size between replays: each call downloads its own outputs (the host call
+        # downloads some planes on a second stream while the pair's last stages run)
+        c, d = _synthetic_pair(192, 13, t=(0.4, -1.1))
+        other = track_pair(c, d, Config(), mask=roi, engine=eng)
+        fifth = track_pair(a, b, Config(), mask=roi, engine=eng)
+        eng2 = Engine(0)
+        try:
+            other_eager = track_pair(c, d, Config(), mask=roi, engine=eng2)
+        finally:
+            eng2.close()
+        for k in ("ux", "uy", "conf", "raw_ux", "raw_uy", "valid"):
+            np.testing.assert_array_equal(getattr(other, k), getattr(other_eager, k), err_msg=k)
+            np.testing.assert_array_equal(getattr(fifth, k), getattr(first, k), err_msg=k)
+        for k in ("Exx", "Eyy", "Exy", "gmax", "vol"):
+            np.testing.assert_array_equal(other.strain[k], other_eager.strain[k], err_msg=k)
+        assert not np.array_equal(other.raw_ux, first.raw_ux)
         st = torch.cuda.Stream()
         ta, tb, tr = (torch.from_numpy(x).cuda() for x in (a, b, roi))
         for _ in range(2):
