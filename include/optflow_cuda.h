@@ -160,6 +160,29 @@ OFC_API int ofc_refine_batch(ofc_engine* eng, const ofc_window* wins, size_t n, 
                      char* err, size_t errlen);
 
 /*
+ * tavg::align_to (rust/crates/optflow-cli/src/tavg.rs:116-161; python/optflow_ref/tavg.py:30-58): `other`
+ * resampled onto the pixel grid of `centre` (both w x h) by the motion of the coarse POC flow centre -> other:
+ * model 0, the robust affine fit (tavg.rs:81-114) to the grid points with a peak and, when mask (w x h, nullable)
+ * is given, inside it; model 1 ("dense"), the coarse flow interpolated bilinearly. out = other(x + u(x)) by
+ * the cubic B-spline of `other` (interp::warp). *aligned = 0 (out untouched) when no motion could be estimated
+ * (fewer than 6 grid points, or a degenerate fit).
+ */
+OFC_API int ofc_align_to(ofc_engine* eng, const float* centre, const float* other, size_t w, size_t h,
+                 const uint8_t* mask, int model, const ofc_config* cfg, float* out, int* aligned,
+                 char* err, size_t errlen);
+
+/*
+ * tavg::average_window_with (rust/crates/optflow-cli/src/tavg.rs:163-210; python/optflow_ref/tavg.py:61-74):
+ * the mean of frames[0..n) (each w x h) around frames[centre], summed in float64 (the others in order, then the
+ * centre). align 0: plain mean; 1: every other frame aligned to the centre first (affine model, mask as in
+ * ofc_align_to); 2: the same with the dense model. A frame whose alignment fails is left out, or with
+ * keep_unaligned enters unaligned. *used (nullable): the frames in the mean, the centre included.
+ */
+OFC_API int ofc_average_window(ofc_engine* eng, const float* const* frames, size_t n, size_t centre, size_t w,
+                       size_t h, int align, const uint8_t* mask, int keep_unaligned, const ofc_config* cfg,
+                       float* out, int* used, char* err, size_t errlen);
+
+/*
  * phaseflow::refine / refine_low (python/optflow_ref/phaseflow.py:427-511;
  * rust/crates/optflow-core/src/phaseflow.rs:1684-1757): refine_raw on the whole image plus the
  * confidence with its border rule. out_low (nullable) = the f64 confidence < conf_min.

@@ -848,6 +848,146 @@ void check_fine_window(size_t w, size_t h, const ofc_config& c) {
                                     " exceeds the shared-memory FFT passes of the CUDA engine");
 }
 
+// ---------------------------------------------------------------- temporal averaging front-end (tavg)
+// rust/crates/optflow-cli/src/tavg.rs (the CLI's implementation; python/optflow_ref/tavg.py is its specification,
+// whose scipy map_coordinates warp differs from the CLI's B-spline warp only near the image border).
+
+// least squares v = c0 + c1 x + c2 y through the selected points in centred coordinates, by Gaussian elimination
+// with partial pivoting (the last of equal pivots) on the 3 x 3 normal equations (tavg.rs:34-79); false on a pivot
+// below 1e-12
+static bool tavg_lstsq(const std::vector<double>& xs, const std::vector<double>& ys, const std::vector<double>& v,
+                       const std::vector<char>& sel, double out[3]) {
+  double n = 0, mx = 0, my = 0;
+  for (size_t i = 0; i < xs.size(); i++)
+    if (sel[i]) { n += 1; mx += xs[i]; my += ys[i]; }
+  mx /= n;
+  my /= n;
+  double a[3][4] = {};
+  for (size_t i = 0; i < xs.size(); i++) {
+    if (!sel[i]) continue;
+    const double row[3] = {1.0, xs[i] - mx, ys[i] - my};
+    for (int r = 0; r < 3; r++) {
+      for (int c = 0; c < 3; c++) a[r][c] += row[r] * row[c];
+      a[r][3] += row[r] * v[i];
+    }
+  }
+  for (int c = 0; c < 3; c++) {
+    int p = c;
+    for (int i = c + 1; i < 3; i++)
+      if (std::fabs(a[i][c]) >= std::fabs(a[p][c])) p = i;
+    if (std::fabs(a[p][c]) < 1e-12) return false;
+    for (int k = 0; k < 4; k++) std::swap(a[c][k], a[p][k]);
+    for (int i = c + 1; i < 3; i++) {
+      const double f = a[i][c] / a[c][c];
+      for (int k = c; k < 4; k++) a[i][k] -= f * a[c][k];
+    }
+  }
+  double x[3];
+  for (int i = 2; i >= 0; i--) {
+    double t = a[i][3];
+    for (int j = i + 1; j < 3; j++) t -= a[i][j] * x[j];
+    x[i] = t / a[i][i];
+  }
+  out[0] = x[0] - x[1] * mx - x[2] * my;
+  out[1] = x[1];
+  out[2] = x[2];
+  return true;
+}
+
+// robust affine through scattered displacements (tavg.rs:81-114): four fits, each keeping the points whose
+// residual is at most max(3 x 1.4826 MAD, 0.05 px) of the previous one; false below 6 points or on a failed solve
+static bool tavg_fit_affine(const std::vector<double>& xs, const std::vector<double>& ys, const std::vector<double>& ux,
+                            const std::vector<double>& uy, double cx[3], double cy[3]) {
+  const size_t n = xs.size();
+  std::vector<char> sel(n, 1);
+  std::vector<double> r(n);
+  for (int pass = 0; pass < 4; pass++) {
+    size_t cnt = 0;
+    for (char s2 : sel) cnt += s2 ? 1 : 0;
+    if (cnt < 6) return false;
+    if (!tavg_lstsq(xs, ys, ux, sel, cx) || !tavg_lstsq(xs, ys, uy, sel, cy)) return false;
+    std::vector<double> rs;
+    for (size_t i = 0; i < n; i++) {
+      r[i] = std::hypot(cx[0] + cx[1] * xs[i] + cx[2] * ys[i] - ux[i], cy[0] + cy[1] * xs[i] + cy[2] * ys[i] - uy[i]);
+      if (sel[i]) rs.push_back(r[i]);
+    }
+    std::sort(rs.begin(), rs.end());
+    const size_t m = rs.size();
+    const double med = m % 2 ? rs[m / 2] : 0.5 * (rs[m / 2 - 1] + rs[m / 2]);
+    const double lim = std::max(3.0 * 1.4826 * med, 0.05);
+    for (size_t i = 0; i < n; i++) sel[i] = r[i] <= lim ? 1 : 0;
+  }
+  return true;
+}
+
+// the affine field c0 + c1 x + c2 y per axis, rounded to float32 (the CLI's Image<f32> field, tavg.rs:152-157)
+__global__ void k_affine_field(double ax, double bx, double cx, double ay, double by, double cy, int W, int H,
+                               double* __restrict__ ux, double* __restrict__ uy) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  const size_t p = (size_t)y * W + x;
+  ux[p] = (double)(float)(ax + bx * (double)x + cx * (double)y);
+  uy[p] = (double)(float)(ay + by * (double)x + cy * (double)y);
+}
+
+// align_to (tavg.rs:116-161) on device images c, o (W x H f32) into out: false when no motion could be estimated
+// (no output written). model 0: the robust affine fit to the POC grid points with a peak and (hmask, host, nullable)
+// inside the mask; 1: the coarse flow interpolated bilinearly. out = o(x + u(x)) by the cubic B-spline of o.
+static bool tavg_align_dev(Lane& L, const float* c, const float* o, int W, int H, const uint8_t* hmask, int model,
+                           const ofc_config& cfg, float* out) {
+  cudaStream_t st = L.stream;
+  const size_t N = (size_t)W * H;
+  CoarseOut g = coarse_dev(L, c, o, W, H, nullptr, cfg);
+  double* u2 = L.get<double>("tavg_u2", 2 * N);
+  if (model == 1) {
+    launch_grid_sample(g.ux, g.uy, g.xs, g.ys, g.nx, g.ny, nullptr, nullptr, W, H, 1.0, 1.0, u2, u2 + N, st);
+    float* f = L.get<float>("tavg_f32", 2 * N);  // the field as float32 (tavg.rs:127-133)
+    launch_f64_to_f32(u2, f, 2 * N, st);
+    launch_f32_to_f64(f, u2, 2 * N, st);
+  } else {
+    const size_t ng = (size_t)g.nx * g.ny;
+    std::vector<double> gu(ng), gv(ng), gp(ng);
+    OFC_CUDA(cudaMemcpyAsync(gu.data(), g.ux, ng * 8, cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaMemcpyAsync(gv.data(), g.uy, ng * 8, cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaMemcpyAsync(gp.data(), g.peak, ng * 8, cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaStreamSynchronize(st));
+    std::vector<double> xs, ys, vx, vy;
+    for (int iy = 0; iy < g.ny; iy++)
+      for (int ix = 0; ix < g.nx; ix++) {
+        const size_t j = (size_t)iy * g.nx + ix;
+        const int x = g.hxs[ix], y = g.hys[iy];
+        if (!((float)gp[j] > 0.0f)) continue;
+        if (hmask && !hmask[(size_t)y * W + x]) continue;
+        xs.push_back(x);
+        ys.push_back(y);
+        vx.push_back((double)(float)gu[j]);  // the grid is float32 (poc.rs Grid)
+        vy.push_back((double)(float)gv[j]);
+      }
+    if (xs.size() < 6) return false;
+    double cx[3], cy[3];
+    if (!tavg_fit_affine(xs, ys, vx, vy, cx, cy)) return false;
+    OFC_LAUNCH(k_affine_field, dim3(div_up(W, 128), H), 128, 0, st, cx[0], cx[1], cx[2], cy[0], cy[1], cy[2], W, H, u2,
+               u2 + N);
+  }
+  float* c2 = L.get<float>("tavg_spline", N);
+  double* tmp = L.get<double>("tavg_spline_tmp", 2 * N);
+  launch_bspline_f32(o, c2, tmp, W, H, st);
+  launch_warp(c2, W, H, u2, u2 + N, 0, 0, W, H, out, st);
+  return true;
+}
+
+// the mean of the frames of a window in float64: the sum of the others (in order) added to the centre, over their
+// count (tavg.rs:195-206)
+__global__ void k_tavg_add(const float* __restrict__ f, size_t n, double* __restrict__ acc, int first) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    acc[i] = first ? (double)f[i] : acc[i] + (double)f[i];
+}
+__global__ void k_tavg_mean(const float* __restrict__ c, const double* __restrict__ acc, size_t n, double cnt,
+                            float* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (float)(((double)c[i] + acc[i]) / cnt);
+}
+
 // low = conf < conf_min (track.py:66) for ofc_finish
 __global__ void k_threshold_low(const double* c64, double cm, uint8_t* low, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -1363,6 +1503,70 @@ int ofc_track_pair(ofc_engine* e, const float* i1, const float* i2, size_t w, si
     double timing[3];
     pair_timing(L, timing);
     for (int i = 0; i < 3; i++) out->timing[i] = timing[i];
+  });
+}
+
+int ofc_align_to(ofc_engine* e, const float* centre, const float* other, size_t w, size_t h, const uint8_t* mask,
+                 int model, const ofc_config* c, float* out, int* aligned, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_sizes(w, h);
+    if (!centre || !other || !out || !aligned) throw Error(OFC_ERR_ARG, "null argument");
+    if (model != 0 && model != 1) throw Error(OFC_ERR_ARG, "tavg model must be 0 (affine) or 1 (dense)");
+    if ((int)std::min(w, h) < c->poc_win)
+      throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
+    const size_t N = w * h;
+    const float* dc = L.upload("tavg_c", centre, N);
+    const float* d_o = L.upload("tavg_o", other, N);
+    float* d_out = L.get<float>("tavg_out", N);
+    const bool ok = tavg_align_dev(L, dc, d_o, (int)w, (int)h, model == 0 ? mask : nullptr, model, *c, d_out);
+    if (ok) OFC_CUDA(cudaMemcpyAsync(out, d_out, N * 4, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+    *aligned = ok ? 1 : 0;
+  });
+}
+
+int ofc_average_window(ofc_engine* e, const float* const* frames, size_t n, size_t centre, size_t w, size_t h,
+                       int align, const uint8_t* mask, int keep_unaligned, const ofc_config* c, float* out,
+                       int* used_count, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_sizes(w, h);
+    if (!frames || !out || n == 0) throw Error(OFC_ERR_ARG, "no frames");
+    if (centre >= n) throw Error(OFC_ERR_ARG, "centre index beyond the frames");
+    for (size_t i = 0; i < n; i++)
+      if (!frames[i]) throw Error(OFC_ERR_ARG, "null frame " + std::to_string(i));
+    if (align < 0 || align > 2) throw Error(OFC_ERR_ARG, "align must be 0 (none), 1 (affine) or 2 (dense)");
+    if (align && (int)std::min(w, h) < c->poc_win)
+      throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
+    const size_t N = w * h;
+    cudaStream_t st = L.stream;
+    const float* dc = L.upload("tavg_c", frames[centre], N);
+    float* dframe = L.get<float>("tavg_o", N);
+    float* dal = L.get<float>("tavg_out", N);
+    double* acc = L.get<double>("tavg_acc", N);
+    const unsigned blocks = std::min(div_up(N, 256), 8192u);
+    int used = 0;
+    for (size_t i = 0; i < n; i++) {
+      if (i == centre) continue;
+      OFC_CUDA(cudaMemcpyAsync(dframe, frames[i], N * 4, cudaMemcpyHostToDevice, st));
+      const float* add = dframe;
+      if (align) {
+        if (tavg_align_dev(L, dc, dframe, (int)w, (int)h, align == 1 ? mask : nullptr, align - 1, *c, dal)) add = dal;
+        else if (!keep_unaligned) continue;
+      }
+      OFC_LAUNCH(k_tavg_add, blocks, 256, 0, st, add, N, acc, used == 0 ? 1 : 0);
+      used++;
+    }
+    if (used == 0) {
+      OFC_CUDA(cudaMemcpyAsync(out, dc, N * 4, cudaMemcpyDeviceToHost, st));
+    } else {
+      float* dout = L.get<float>("tavg_mean", N);
+      OFC_LAUNCH(k_tavg_mean, blocks, 256, 0, st, dc, acc, N, (double)(used + 1), dout);
+      OFC_CUDA(cudaMemcpyAsync(out, dout, N * 4, cudaMemcpyDeviceToHost, st));
+    }
+    OFC_CUDA(cudaStreamSynchronize(st));
+    if (used_count) *used_count = used + 1;
   });
 }
 

@@ -237,3 +237,126 @@ def track_pair(I1, I2, cfg=None, mask=None, init=None):
     r["valid"] = np.isfinite(r["ux"])
     r["timing"] = dict(coarse=timing[0], fine=timing[1], strain=timing[2])
     return r
+
+
+# ---- temporal averaging front-end: the reference CLI's arithmetic (rust/crates/optflow-cli/src/tavg.rs), which
+# follows python/optflow_ref/tavg.py except for its warp (the B-spline of interp::warp instead of scipy's
+# map_coordinates; they agree away from the image border)
+
+def _tavg_lstsq(xs, ys, v, sel):
+    """v = c0 + c1 x + c2 y through the selected points, centred coordinates, Gaussian elimination with partial
+    pivoting on the normal equations (tavg.rs:34-79); None on a pivot below 1e-12."""
+    mx, my = xs[sel].mean(), ys[sel].mean()
+    rows = np.stack([np.ones(sel.sum()), xs[sel] - mx, ys[sel] - my], axis=1)
+    a = np.zeros((3, 4))
+    for row, val in zip(rows, v[sel]):
+        a[:, :3] += np.outer(row, row)
+        a[:, 3] += row * val
+    for c in range(3):
+        p = c
+        for i in range(c + 1, 3):
+            if abs(a[i, c]) >= abs(a[p, c]):
+                p = i
+        if abs(a[p, c]) < 1e-12:
+            return None
+        a[[c, p]] = a[[p, c]]
+        for i in range(c + 1, 3):
+            f = a[i, c] / a[c, c]
+            a[i, c:] -= f * a[c, c:]
+    x = np.zeros(3)
+    for i in (2, 1, 0):
+        x[i] = (a[i, 3] - sum(a[i, j] * x[j] for j in range(i + 1, 3))) / a[i, i]
+    return np.array([x[0] - x[1] * mx - x[2] * my, x[1], x[2]])
+
+
+def tavg_fit_affine(xs, ys, ux, uy):
+    """Robust affine through scattered displacements (tavg.rs:81-114): (cx, cy) or None."""
+    xs, ys, ux, uy = (np.asarray(a, np.float64) for a in (xs, ys, ux, uy))
+    sel = np.ones(len(xs), bool)
+    coef = None
+    for _ in range(4):
+        if sel.sum() < 6:
+            return None
+        cx, cy = _tavg_lstsq(xs, ys, ux, sel), _tavg_lstsq(xs, ys, uy, sel)
+        if cx is None or cy is None:
+            return None
+        coef = (cx, cy)
+        r = np.hypot(cx[0] + cx[1] * xs + cx[2] * ys - ux, cy[0] + cy[1] * xs + cy[2] * ys - uy)
+        mad = 1.4826 * np.median(r[sel])
+        sel = r <= max(3.0 * mad, 0.05)
+    return coef
+
+
+def grid_sample(grid, x, y):
+    """Bilinear interpolation of the grid field clamped to the grid (poc.rs:546-572)."""
+    def frac(q, nodes):
+        n = len(nodes)
+        if n == 1:
+            return np.zeros_like(q), np.zeros(q.shape, int), np.zeros(q.shape, int)
+        step = float(nodes[1] - nodes[0])
+        f = np.clip((q - nodes[0]) / step, 0.0, n - 1.0)
+        i0 = np.minimum(np.floor(f).astype(int), n - 2)
+        return f - i0, i0, np.minimum(i0 + 1, n - 1)
+    tx, x0, x1 = frac(np.asarray(x, np.float64), grid["xs"])
+    ty, y0, y1 = frac(np.asarray(y, np.float64), grid["ys"])
+    out = []
+    for a in (np.asarray(grid["ux"], np.float32).astype(np.float64), np.asarray(grid["uy"], np.float32).astype(np.float64)):
+        out.append((1 - ty) * ((1 - tx) * a[y0, x0] + tx * a[y0, x1]) + ty * ((1 - tx) * a[y1, x0] + tx * a[y1, x1]))
+    return out
+
+
+def warp(img, ux, uy):
+    """interp::warp (rust/crates/optflow-core/src/interp.rs:390-414): img at (x + ux, y + uy) by its cubic B-spline."""
+    h, w = img.shape
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    c = bspline_coeffs(np.asarray(img, np.float32).astype(np.float64))
+    return sample(c, xx + np.asarray(ux, np.float64), yy + np.asarray(uy, np.float64))
+
+
+def align_to(centre, other, cfg=None, mask=None, model="affine"):
+    """tavg::align_to (tavg.rs:116-161): `other` on the pixel grid of `centre`, or None."""
+    h, w = centre.shape
+    g = coarse_flow(centre, other, cfg)
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    if model == "dense":
+        ux, uy = grid_sample(g, xx, yy)
+    else:
+        Y, X = np.meshgrid(g["ys"], g["xs"], indexing="ij")
+        ok = np.asarray(g["peak"], np.float32) > 0
+        if mask is not None:
+            ok &= np.asarray(mask, bool)[Y, X]
+        if ok.sum() < 6:
+            return None
+        coef = tavg_fit_affine(X[ok], Y[ok], np.asarray(g["ux"], np.float32)[ok], np.asarray(g["uy"], np.float32)[ok])
+        if coef is None:
+            return None
+        cx, cy = coef
+        ux = cx[0] + cx[1] * xx + cx[2] * yy
+        uy = cy[0] + cy[1] * xx + cy[2] * yy
+    ux, uy = np.float32(ux).astype(np.float64), np.float32(uy).astype(np.float64)  # the CLI's float32 fields
+    return np.float32(warp(other, ux, uy))
+
+
+def average_window(frames, centre, align=False, cfg=None, mask=None, keep_unaligned=False, model="affine"):
+    """tavg::average_window_with (tavg.rs:163-210): float32 mean (float64 sums: the others in order, then the
+    centre) of the window."""
+    c = np.asarray(frames[centre], np.float32)
+    used = []
+    for i, f in enumerate(frames):
+        if i == centre:
+            continue
+        f = np.asarray(f, np.float32)
+        if align:
+            a = align_to(c, f, cfg, mask, model)
+            if a is None:
+                if not keep_unaligned:
+                    continue
+                a = f
+            f = a
+        used.append(f.astype(np.float64))
+    if not used:
+        return c.copy()
+    s = used[0].copy()
+    for u in used[1:]:
+        s += u
+    return np.float32((c.astype(np.float64) + s) / (len(used) + 1))

@@ -141,6 +141,24 @@ def _meta():
         return json.load(fh)
 
 
+def test_tavg(oracle):
+    """The temporal-averaging restatement against the reference's tavg.py (tests/golden/tavg.npz): aligned frames
+    agree away from the border (the reference warps with scipy's map_coordinates, the CLI with the B-spline of
+    interp::warp), the plain mean exactly; the mask keeps the motion of the masked part only."""
+    g = golden("tavg")
+    cfg = Config(max_disp=8.0)
+    fr = [f.astype(np.float64) for f in g["frames"]]
+    m = (slice(20, -20), slice(20, -20))
+    for got, want in ((oracle.align_to(fr[2], fr[0], cfg), g["aff0"]), (oracle.align_to(fr[2], fr[4], cfg), g["aff4"]),
+                      (oracle.align_to(fr[0], g["split"], cfg, model="dense"), g["dense"]),
+                      (oracle.align_to(g["m_static"], g["m_half"], cfg, mask=g["mask"].astype(bool)), g["masked"]),
+                      (oracle.align_to(g["m_static"], g["m_half"], cfg), g["unmasked"]),
+                      (oracle.average_window(fr, 2, align=True, cfg=cfg), g["aligned"])):
+        assert np.abs(got[m] - want[m]).max() < 1e-6
+    np.testing.assert_array_equal(oracle.average_window(fr, 2), g["plain"])
+    assert oracle.align_to(np.full((128, 128), 0.5), np.full((128, 128), 0.5), cfg) is None
+
+
 def test_ref_fixture_interp(oracle):
     img = ref_fixture("interp_img").astype(np.float64)
     x, y = ref_fixture("interp_x"), ref_fixture("interp_y")
