@@ -160,6 +160,21 @@ OFC_API int ofc_refine_batch(ofc_engine* eng, const ofc_window* wins, size_t n, 
                      char* err, size_t errlen);
 
 /*
+ * track::track_sequence, chain mode (rust/crates/optflow-core/src/track.rs:1030-1245; python/optflow_ref/track.py:
+ * 260-315): frames[0..n) (each w x h) against a moving reference. Frame k is tracked directly against the current
+ * reference (coarse + fine, the previous leg's raw field as the dense start); the reference moves to frame k - 1
+ * when the leg's mean confidence over the reportable ROI pixels falls below ref_update_conf (the previous leg then
+ * extends the frame-0 link: its displacement is composed and its confidence min-accumulated). outs[k - 1] gets
+ * frame k's result on the frame-0 grid (composed raw field, link confidence, guard and strain of the finish; timing
+ * coarse / fine of the leg, strain of the finish); reference[k - 1] and mean_conf[k - 1] (nullable) the reference
+ * index and the mean confidence. roi (nullable): the frame-0 ROI of the finish and of the mean. The hybrid mode is
+ * not part of this entry point.
+ */
+OFC_API int ofc_track_sequence(ofc_engine* eng, const float* const* frames, size_t n, size_t w, size_t h,
+                       const uint8_t* roi, const ofc_config* cfg, double ref_update_conf, ofc_pair_out* outs,
+                       int32_t* reference, double* mean_conf, char* err, size_t errlen);
+
+/*
  * tavg::align_to (rust/crates/optflow-cli/src/tavg.rs:116-161; python/optflow_ref/tavg.py:30-58): `other`
  * resampled onto the pixel grid of `centre` (both w x h) by the motion of the coarse POC flow centre -> other:
  * model 0, the robust affine fit (tavg.rs:81-114) to the grid points with a peak and, when mask (w x h, nullable)

@@ -751,15 +751,17 @@ void pair_stage(Lane& L, int stage, int W, int H, bool has_roi, bool has_init, c
 // Runs the three stages on L.stream. The first call for a (size, configuration, inputs present, profile filter)
 // runs them eagerly, which allocates every buffer and uploads every constant, and then captures each stage as a
 // CUDA graph; later calls replay the graphs. timing: record the stage events L.ev[0..3] (the start of each stage
-// and the end), which pair_timing reads.
-void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_config& c, bool timing) {
+// and the end), which pair_timing reads. nstages: 3 (the pair) or 2 (a sequence leg: coarse and fine, whose
+// conf, raw_ux and raw_uy planes of "out_pair" are its result).
+void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_config& c, bool timing, int nstages) {
   cudaStream_t st = L.stream;
   Profiler* prof = g_profiler;
   const std::string key = std::to_string(W) + "x" + std::to_string(H) + ":" + cfg_key(c) + ":" +
-                          (has_roi ? "r" : "-") + (has_init ? "i" : "-") + ":" + (prof ? "P" + prof->filter : "");
+                          (has_roi ? "r" : "-") + (has_init ? "i" : "-") + ":" + std::to_string(nstages) + ":" +
+                          (prof ? "P" + prof->filter : "");
   auto it = L.graphs.find(key);
   if (it == L.graphs.end() || it->second->eager) {
-    for (int sgi = 0; sgi < 3; sgi++) {
+    for (int sgi = 0; sgi < nstages; sgi++) {
       if (timing) OFC_CUDA(cudaEventRecord(L.ev[sgi], st));
       pair_stage(L, sgi, W, H, has_roi, has_init, c);
     }
@@ -768,7 +770,7 @@ void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_conf
   if (it == L.graphs.end()) {
     std::unique_ptr<Lane::Graph> g(new Lane::Graph());
     bool ok = true;
-    for (int sgi = 0; sgi < 3 && ok; sgi++) {
+    for (int sgi = 0; sgi < nstages && ok; sgi++) {
       cudaGraph_t graph = nullptr;
       const uint64_t before = g_launch_counter ? *g_launch_counter : 0;
       OFC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
@@ -802,7 +804,7 @@ void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_conf
     L.graphs[key] = std::move(g);
   } else if (!it->second->eager) {
     Lane::Graph& g = *it->second;
-    for (int sgi = 0; sgi < 3; sgi++) {
+    for (int sgi = 0; sgi < nstages; sgi++) {
       if (timing) OFC_CUDA(cudaEventRecord(L.ev[sgi], st));
       OFC_CUDA(cudaGraphLaunch(g.exec[sgi], st));
       if (g_launch_counter) *g_launch_counter += g.launches[sgi];
@@ -986,6 +988,84 @@ __global__ void k_tavg_mean(const float* __restrict__ c, const double* __restric
                             float* __restrict__ out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     out[i] = (float)(((double)c[i] + acc[i]) / cnt);
+}
+
+// ---------------------------------------------------------------- sequence chain (track_sequence)
+// rust/crates/optflow-core/src/track.rs:863-1245 (python/optflow_ref/track.py:231-315)
+
+// bilinear sample in float64 with the reference's rules (track.rs:866-896): NaN outside [0, w-1] x [0, h-1], for a
+// non-finite coordinate, and where a NaN of the image enters the cell
+__device__ __forceinline__ double bilinear64(const float* __restrict__ a, int w, int h, double x, double y) {
+  if (!(isfinite(x) && isfinite(y)) || x < 0.0 || y < 0.0 || x > (double)(w - 1) || y > (double)(h - 1)) return nan("");
+  int x0 = 0, x1 = 0, y0 = 0, y1 = 0;
+  double tx = 0.0, ty = 0.0;
+  if (w > 1) { x0 = min((int)floor(x), w - 2); x1 = x0 + 1; tx = x - x0; }
+  if (h > 1) { y0 = min((int)floor(y), h - 2); y1 = y0 + 1; ty = y - y0; }
+  auto at = [&](int yy, int xx) { return (double)a[(size_t)yy * w + xx]; };
+  return (1.0 - ty) * ((1.0 - tx) * at(y0, x0) + tx * at(y0, x1)) + ty * ((1.0 - tx) * at(y1, x0) + tx * at(y1, x1));
+}
+
+// compose (track.rs:904-930): c = a + b(X + a), float64, stored float32
+__global__ void k_compose(const float* __restrict__ ax, const float* __restrict__ ay, const float* __restrict__ bx,
+                          const float* __restrict__ by, int W, int H, float* __restrict__ cx, float* __restrict__ cy) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  const size_t i = (size_t)y * W + x;
+  const double u = ax[i], v = ay[i], px = x + u, py = y + v;
+  cx[i] = (float)(u + bilinear64(bx, W, H, px, py));
+  cy[i] = (float)(v + bilinear64(by, W, H, px, py));
+}
+
+// link_conf (track.rs:935-955): min(c0r, conf(X + u0r)), a NaN sample counting as 0; out may be c0r
+__global__ void k_link_conf(const double* c0r, const float* __restrict__ conf, const float* __restrict__ ux,
+                            const float* __restrict__ uy, int W, int H, double* out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  const size_t i = (size_t)y * W + x;
+  const double c = bilinear64(conf, W, H, x + (double)ux[i], y + (double)uy[i]);
+  out[i] = fmin(c0r[i], isfinite(c) ? c : 0.0);
+}
+
+// mean_conf (track.rs:957-1023): the reportable image of the leg (the border rule on its raw field), then per pixel
+// the sampled confidence where it counts; the rows summed in order by one thread each, the rows folded in order
+__global__ void k_reportable(const float* __restrict__ rx, const float* __restrict__ ry, int W, int H, double B,
+                             float* __restrict__ rep) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  const size_t i = (size_t)y * W + x;
+  const double tx = x + (double)rx[i], ty = y + (double)ry[i];
+  const double own = (double)min(min(x, y), min(W - 1 - x, H - 1 - y));
+  rep[i] = (own >= B && tx >= B && ty >= B && (W - 1) - tx >= B && (H - 1) - ty >= B) ? 1.f : 0.f;
+}
+__global__ void k_mean_conf_rows(const float* __restrict__ conf, const float* __restrict__ rep,
+                                 const float* __restrict__ ux, const float* __restrict__ uy,
+                                 const uint8_t* __restrict__ mask, int W, int H, double* __restrict__ rsum,
+                                 long long* __restrict__ rcnt) {
+  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= H) return;
+  double sum = 0.0;
+  long long n = 0;
+  for (int x = 0; x < W; x++) {
+    const size_t i = (size_t)y * W + x;
+    const double px = x + (double)ux[i], py = y + (double)uy[i];
+    const double c = bilinear64(conf, W, H, px, py);
+    if (isfinite(c) && bilinear64(rep, W, H, px, py) > 0.5 && (!mask || mask[i])) {
+      sum += c;
+      n++;
+    }
+  }
+  rsum[y] = sum;
+  rcnt[y] = n;
+}
+__global__ void k_mean_conf_fold(const double* __restrict__ rsum, const long long* __restrict__ rcnt, int H,
+                                 double* out) {
+  double s = 0.0;
+  long long n = 0;
+  for (int y = 0; y < H; y++) {
+    s += rsum[y];
+    n += rcnt[y];
+  }
+  *out = n == 0 ? 0.0 : s / (double)n;
 }
 
 // low = conf < conf_min (track.py:66) for ofc_finish
@@ -1468,7 +1548,7 @@ int ofc_track_pair(ofc_engine* e, const float* i1, const float* i2, size_t w, si
       L.upload("in_u", init_ux, N);
       L.upload("in_v", init_uy, N);
     }
-    run_pair(L, (int)w, (int)h, roi != nullptr, init_ux != nullptr, *c, true);
+    run_pair(L, (int)w, (int)h, roi != nullptr, init_ux != nullptr, *c, true, 3);
     // conf, raw_ux and raw_uy are final when the fine stage ends (event ev[2]), ux, uy and valid when the finish
     // stage has masked the field (event L.masked): their downloads run on the copy stream during the rest of the
     // pair; the strain planes follow on the lane's stream
@@ -1503,6 +1583,127 @@ int ofc_track_pair(ofc_engine* e, const float* i1, const float* i2, size_t w, si
     double timing[3];
     pair_timing(L, timing);
     for (int i = 0; i < 3; i++) out->timing[i] = timing[i];
+  });
+}
+
+int ofc_track_sequence(ofc_engine* e, const float* const* frames, size_t n, size_t w, size_t h, const uint8_t* roi,
+                       const ofc_config* c, double ref_update_conf, ofc_pair_out* outs, int32_t* reference,
+                       double* mean_conf, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    if (!frames || n == 0) throw Error(OFC_ERR_ARG, "no frames");
+    check_sizes(w, h);
+    for (size_t k = 0; k < n; k++)
+      if (!frames[k]) throw Error(OFC_ERR_ARG, "null frame " + std::to_string(k));
+    if (n > 1 && !outs) throw Error(OFC_ERR_ARG, "null outputs");
+    if (!(ref_update_conf >= 0.0 && ref_update_conf <= 1.0)) throw Error(OFC_ERR_ARG, "ref_update_conf must be in [0, 1]");
+    const size_t N = w * h;
+    if (roi) {
+      bool any = false;
+      for (size_t i = 0; i < N && !any; i++) any = roi[i] != 0;
+      if (!any) throw Error(OFC_ERR_ARG, "ROI mask is empty");
+    }
+    if (n == 1) return;
+    if ((int)std::min(w, h) < c->poc_win)
+      throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
+    check_fine_window(w, h, *c);
+    const int W = (int)w, H = (int)h;
+    cudaStream_t st = L.stream;
+    const dim3 g2(div_up(W, 128), H);
+    // the run's state on the device (track.rs:1030-1043)
+    float* ref = L.get<float>("seq_ref", N);
+    float* prev = L.get<float>("seq_prev", N);
+    float* fk = L.get<float>("seq_fk", N);
+    float* u0r = L.get<float>("seq_u0r", 2 * N);
+    float* u0n = L.get<float>("seq_u0n", 2 * N);
+    double* c0r = L.get<double>("seq_c0r", N);
+    double* conf0 = L.get<double>("seq_conf0", N);
+    float* praw = L.get<float>("seq_praw", 2 * N);
+    float* pconf = L.get<float>("seq_pconf", N);
+    float* cxy = L.get<float>("seq_cxy", 2 * N);
+    double* c64 = L.get<double>("seq_c64", 2 * N);
+    float* rep = L.get<float>("seq_rep", N);
+    double* rsum = L.get<double>("seq_rsum", (size_t)H);
+    long long* rcnt = L.get<long long>("seq_rcnt", (size_t)H);
+    double* dmean = L.get<double>("seq_mean", 1);
+    uint8_t* low = L.get<uint8_t>("seq_low", N);
+    const uint8_t* droi = roi ? L.upload("seq_roi", roi, N) : nullptr;
+    float* in1 = L.get<float>("in_i1", N);
+    float* in2 = L.get<float>("in_i2", N);
+    float* inu = L.get<float>("in_u", N);
+    float* inv = L.get<float>("in_v", N);
+    const ofc_pair_out d = device_pair_out(L, N);  // the leg's conf, raw_ux, raw_uy (planes 2, 8, 9)
+    const double B = guard_px(*c) > 0 ? 4.0 * c->sigma_w : 0.0;
+    OFC_CUDA(cudaMemcpyAsync(ref, frames[0], N * 4, cudaMemcpyHostToDevice, st));
+    OFC_CUDA(cudaMemcpyAsync(prev, ref, N * 4, cudaMemcpyDeviceToDevice, st));
+    OFC_CUDA(cudaMemsetAsync(u0r, 0, 2 * N * 4, st));
+    launch_fill_f64(c0r, 1.0, N, st);
+    bool have_prev = false;
+    int ref_idx = 0;
+    double t_coarse = 0, t_fine = 0;
+    // one leg reference -> frame k (pair_flow_on, track.rs:558-623): the coarse and fine stages on the lane's pair
+    // buffers, with the previous leg's raw field as the dense start when given
+    auto leg = [&](bool with_init) {
+      OFC_CUDA(cudaMemcpyAsync(in1, ref, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(in2, fk, N * 4, cudaMemcpyDeviceToDevice, st));
+      if (with_init) {
+        OFC_CUDA(cudaMemcpyAsync(inu, praw, N * 4, cudaMemcpyDeviceToDevice, st));
+        OFC_CUDA(cudaMemcpyAsync(inv, praw + N, N * 4, cudaMemcpyDeviceToDevice, st));
+      }
+      run_pair(L, W, H, false, with_init, *c, true, 2);
+      float ms0 = 0, ms1 = 0;
+      OFC_CUDA(cudaEventSynchronize(L.ev[3]));
+      OFC_CUDA(cudaEventElapsedTime(&ms0, L.ev[0], L.ev[1]));
+      OFC_CUDA(cudaEventElapsedTime(&ms1, L.ev[1], L.ev[3]));
+      t_coarse = ms0 * 1e-3;
+      t_fine = ms1 * 1e-3;
+    };
+    auto leg_mean = [&]() {
+      OFC_LAUNCH(k_reportable, g2, 128, 0, st, d.raw_ux, d.raw_uy, W, H, B, rep);
+      OFC_LAUNCH(k_mean_conf_rows, div_up(H, 128), 128, 0, st, d.conf, rep, u0r, u0r + N, droi, W, H, rsum, rcnt);
+      OFC_LAUNCH(k_mean_conf_fold, 1, 1, 0, st, rsum, rcnt, H, dmean);
+      double m = 0;
+      OFC_CUDA(cudaMemcpyAsync(&m, dmean, 8, cudaMemcpyDeviceToHost, st));
+      OFC_CUDA(cudaStreamSynchronize(st));
+      return m;
+    };
+    for (size_t k = 1; k < n; k++) {
+      OFC_CUDA(cudaMemcpyAsync(fk, frames[k], N * 4, cudaMemcpyHostToDevice, st));
+      leg(have_prev);
+      double cmean = leg_mean();
+      if (cmean < ref_update_conf && ref_idx != (int)k - 1) {
+        // the reference moves to frame k - 1: the previous leg extends the link of frame 0 (track.rs:1135-1155)
+        OFC_LAUNCH(k_link_conf, g2, 128, 0, st, c0r, pconf, u0r, u0r + N, W, H, c0r);
+        OFC_LAUNCH(k_compose, g2, 128, 0, st, u0r, u0r + N, praw, praw + N, W, H, u0n, u0n + N);
+        OFC_CUDA(cudaMemcpyAsync(u0r, u0n, 2 * N * 4, cudaMemcpyDeviceToDevice, st));
+        OFC_CUDA(cudaMemcpyAsync(ref, prev, N * 4, cudaMemcpyDeviceToDevice, st));
+        ref_idx = (int)k - 1;
+        leg(false);
+        cmean = leg_mean();
+      }
+      // frame 0 -> k and its link confidence, then the finish on the frame-0 grid (track.rs:1157-1200)
+      OFC_LAUNCH(k_compose, g2, 128, 0, st, u0r, u0r + N, d.raw_ux, d.raw_uy, W, H, cxy, cxy + N);
+      OFC_LAUNCH(k_link_conf, g2, 128, 0, st, c0r, d.conf, u0r, u0r + N, W, H, conf0);
+      OFC_CUDA(cudaMemcpyAsync(praw, d.raw_ux, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(praw + N, d.raw_uy, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(pconf, d.conf, N * 4, cudaMemcpyDeviceToDevice, st));
+      launch_f32_to_f64(cxy, c64, 2 * N, st);
+      ofc_threshold_low(conf0, c->conf_min, low, N, st);
+      OFC_CUDA(cudaEventRecord(L.ev[0], st));
+      finish_dev(L, low, droi, c64, c64 + N, conf0, W, H, *c, d, false);
+      OFC_CUDA(cudaEventRecord(L.ev[1], st));
+      download_pair(L, d, &outs[k - 1], N);
+      OFC_CUDA(cudaMemcpyAsync(prev, fk, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaStreamSynchronize(st));
+      float ms = 0;
+      OFC_CUDA(cudaEventElapsedTime(&ms, L.ev[0], L.ev[1]));
+      outs[k - 1].timing[0] = t_coarse;
+      outs[k - 1].timing[1] = t_fine;
+      outs[k - 1].timing[2] = ms * 1e-3;
+      if (reference) reference[k - 1] = ref_idx;
+      if (mean_conf) mean_conf[k - 1] = cmean;
+      have_prev = true;
+    }
   });
 }
 
@@ -1594,7 +1795,7 @@ int ofc_track_pair_device(ofc_engine* e, const float* d_i1, const float* d_i2, s
         OFC_CUDA(cudaMemcpyAsync(L.get<float>("in_u", N), d_init_ux, N * 4, cudaMemcpyDeviceToDevice, st));
         OFC_CUDA(cudaMemcpyAsync(L.get<float>("in_v", N), d_init_uy, N * 4, cudaMemcpyDeviceToDevice, st));
       }
-      run_pair(L, (int)w, (int)h, d_roi != nullptr, d_init_ux != nullptr, *c, false);
+      run_pair(L, (int)w, (int)h, d_roi != nullptr, d_init_ux != nullptr, *c, false, 3);
       const ofc_pair_out d = device_pair_out(L, N);
       float* const* dsrc[10] = {&d.ux, &d.uy, &d.conf, &d.exx, &d.eyy, &d.exy, &d.gmax, &d.vol, &d.raw_ux, &d.raw_uy};
       float* const* udst[10] = {&d_out->ux,  &d_out->uy,  &d_out->conf, &d_out->exx,    &d_out->eyy,

@@ -108,6 +108,8 @@ SIGNATURES = {
                                       c_float_p, c_float_p, ctypes.POINTER(OfcConfig),
                                       c_double_p, c_double_p, c_double_p, c_double_p, _E, _S]),
     "ofc_refine_batch": (ctypes.c_int, [_P, ctypes.c_void_p, _S, ctypes.POINTER(OfcConfig), _E, _S]),
+    "ofc_track_sequence": (ctypes.c_int, [_P, ctypes.POINTER(c_float_p), _S, _S, _S, c_u8_p, ctypes.POINTER(OfcConfig),
+                                          ctypes.c_double, ctypes.POINTER(OfcPairOut), c_i32_p, c_double_p, _E, _S]),
     "ofc_align_to": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, c_u8_p, ctypes.c_int, ctypes.POINTER(OfcConfig),
                                     c_float_p, ctypes.POINTER(ctypes.c_int), _E, _S]),
     "ofc_average_window": (ctypes.c_int, [_P, ctypes.POINTER(c_float_p), _S, _S, _S, _S, ctypes.c_int, c_u8_p,

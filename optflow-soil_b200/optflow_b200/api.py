@@ -287,6 +287,48 @@ def track_pair(I1, I2, cfg=None, mask=None, init=None, engine=None) -> Result:
     return _result(o, arrs)
 
 
+def track_sequence(frames, cfg=None, mask=None, engine=None):
+    """track.track_sequence in chain mode (python/optflow_ref/track.py:260-315; rust/crates/optflow-core/src/track.rs:
+    1030-1245): yields (k, Result) with the displacement from frame 0 to frame k, k = 1, 2, ...; Result.timing adds
+    the reference index and the leg's mean confidence. The frames are tracked in one ofc_track_sequence call (all of
+    them are read first). seq_mode "hybrid" is not on the GPU engine (NotImplementedError)."""
+    cfg, c = _prep_cfg(cfg)
+    fr = [np.asarray(f) for f in frames]
+    if not fr:
+        raise ValueError("no frames")
+    if cfg.seq_mode == "hybrid":
+        raise NotImplementedError("seq_mode 'hybrid' is not part of the GPU engine's sequence entry point")
+    h, w = fr[0].shape
+    for k, f in enumerate(fr):
+        if f.shape != fr[0].shape:
+            raise ValueError(f"frame {k} has shape {f.shape}, expected {fr[0].shape}")
+    if mask is not None and np.shape(mask) != fr[0].shape:
+        raise ValueError(f"ROI mask shape {np.shape(mask)} differs from the frame shape {fr[0].shape}")
+    if mask is not None and not np.any(mask):
+        raise ValueError("ROI mask is empty")
+    if len(fr) > 1 and min(h, w) < cfg.poc_win:
+        raise ValueError(f"image smaller than poc_win ({cfg.poc_win}): {fr[0].shape}")
+    eng = engine or default_engine()
+    f32 = [_f32(f) for f in fr]
+    ptrs = (c_float_p * len(f32))(*[_ptr(f, c_float_p) for f in f32])
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    nk = max(len(fr) - 1, 1)
+    outs = (OfcPairOut * nk)()
+    arrs = []
+    for k in range(len(fr) - 1):
+        o, a = _pair_out(h, w)
+        outs[k] = o
+        arrs.append(a)
+    ref = np.zeros(nk, np.int32)
+    mean = np.zeros(nk)
+    eng._call("ofc_track_sequence", ptrs, len(fr), w, h, _ptr(m, c_u8_p), ctypes.byref(c), float(cfg.ref_update_conf),
+              outs, _ptr(ref, _abi.c_i32_p), _ptr(mean, c_double_p))
+    for k in range(1, len(fr)):
+        r = _result(outs[k - 1], arrs[k - 1])
+        r.timing.update(reference=int(ref[k - 1]), mean_conf=float(mean[k - 1]))
+        yield k, r
+
+
 def track_pair_device(I1, I2, cfg=None, mask=None, init=None, stream=None, engine=None):
     """track_pair on device-resident torch tensors (float32 images, optional uint8/bool ROI and init fields):
     ofc_track_pair_device on ``stream`` (a torch.cuda.Stream; None = the engine's own stream, synchronised
