@@ -174,6 +174,61 @@ OFC_API int ofc_track_sequence(ofc_engine* eng, const float* const* frames, size
                        const uint8_t* roi, const ofc_config* cfg, double ref_update_conf, ofc_pair_out* outs,
                        int32_t* reference, double* mean_conf, char* err, size_t errlen);
 
+/* The hybrid keys of Config (config.py:69-78; rust/crates/optflow-core/src/config.rs): fb_max >= 0 frames a pixel
+ * may be carried by the adjacent leg, fb_radius (px, > 0; <= 0 means 4 sigma_w: Config.fb_radius_px), fb_min_support
+ * >= 0 direct-good pixels the gate's window must hold (0 switches the gate off), fb_tol > 0 px. */
+typedef struct ofc_hybrid {
+    int32_t fb_max;         /* 10 */
+    double fb_radius;       /* -1 */
+    int32_t fb_min_support; /* 20 */
+    double fb_tol;          /* 0.5 */
+} ofc_hybrid;
+
+/* Per-frame record of a hybrid run (Result.timing of track.py:498-501): the reference index, the direct leg's mean
+ * confidence, the largest fallback counter, and the shares of ROI pixels valid by fallback, rejected by the
+ * spatial gate, and re-acquired. */
+typedef struct ofc_hybrid_frame {
+    int32_t reference;
+    int32_t n_fb_max;
+    double mean_conf;
+    double fallback_frac;
+    double fb_gate_rejected;
+    double reacquired;
+} ofc_hybrid_frame;
+
+/* A leg source that replaces the engine's own pair tracking (the reference's tests script legs the same way by
+ * replacing track_pair, python/tests/test_hybrid.py:38-52): called on the host for the leg frames[i] -> frames[j]
+ * with the dense start (init_ux/init_uy, w x h, NULL when the leg has none); writes the leg's raw field and its
+ * confidence (w x h each) and returns 0, or non-zero to stop the run with OFC_ERR_ARG. */
+typedef int (*ofc_leg_fn)(void* user, int32_t i, int32_t j, const float* init_ux, const float* init_uy,
+                          float* raw_ux, float* raw_uy, float* conf);
+
+/*
+ * track::track_sequence with seq_mode "hybrid" (python/optflow_ref/track.py:385-503; rust/crates/optflow-core/src/
+ * track/hybrid.rs:252-566): the chain's direct leg per pixel where its link confidence reaches conf_min, else the
+ * adjacent leg k - 1 -> k carries the pixel for at most fb_max frames, valid only where it agrees with the local
+ * affine model of the direct-good pixels (ofc_local_affine_agreement; fb_min_support > 0); pixels in fallback when
+ * the reference moves are unanchored until a leg from an older reference agrees with them. ref_update_conf[k - 1]
+ * is the threshold at frame k (the reference reads cfg.ref_update_conf anew at every frame). outs[k - 1] as in
+ * ofc_track_sequence (conf: the link confidence, or the decayed adjacent one of a fallback pixel); fb (nullable,
+ * (n - 1) x w x h) the fallback counters; info (nullable, n - 1). leg (nullable): a scripted leg source.
+ */
+OFC_API int ofc_track_sequence_hybrid(ofc_engine* eng, const float* const* frames, size_t n, size_t w, size_t h,
+                              const uint8_t* roi, const ofc_config* cfg, const double* ref_update_conf,
+                              const ofc_hybrid* hy, ofc_pair_out* outs, int32_t* fb, ofc_hybrid_frame* info,
+                              ofc_leg_fn leg, void* leg_user, char* err, size_t errlen);
+
+/*
+ * _local_affine_agreement (python/optflow_ref/track.py:331-382; rust/crates/optflow-core/src/track/hybrid.rs:
+ * 146-250): per pixel an affine model u(q) = a + B (q - p), ridge 1e-3 r^2 on B, fitted to (ux, uy) of the support
+ * pixels in the window of half-size r = max(1, round(radius)), in two passes (the second drops support pixels
+ * whose residual against their own first-pass model exceeds 3 tol). ok = the last pass held >= min_support pixels,
+ * at least 3, and |(tx, ty) - a| <= tol; n (nullable) = the number of them. All planes w x h.
+ */
+OFC_API int ofc_local_affine_agreement(ofc_engine* eng, size_t w, size_t h, const double* ux, const double* uy,
+                               const uint8_t* support, const double* tx, const double* ty, double radius,
+                               int64_t min_support, double tol, uint8_t* ok, int32_t* n, char* err, size_t errlen);
+
 /*
  * tavg::align_to (rust/crates/optflow-cli/src/tavg.rs:116-161; python/optflow_ref/tavg.py:30-58): `other`
  * resampled onto the pixel grid of `centre` (both w x h) by the motion of the coarse POC flow centre -> other:

@@ -1068,6 +1068,296 @@ __global__ void k_mean_conf_fold(const double* __restrict__ rsum, const long lon
   *out = n == 0 ? 0.0 : s / (double)n;
 }
 
+// ---------------------------------------------------------------- hybrid sequence mode
+// python/optflow_ref/track.py:331-503 (rust/crates/optflow-core/src/track/hybrid.rs)
+
+// pixel classes of one hybrid frame, one uint16 per pixel (the boolean planes of track.py:441-487)
+enum : uint16_t {
+  HY_GOOD = 1,     // direct-good (after the re-acquisition: good | re)
+  HY_CANDRE = 2,   // re-acquisition candidate: direct_ok, unanchored, in the ROI, the reference older than k - 1
+  HY_NEED = 4,     // needs the adjacent leg: not good, in the ROI, u_{k-1} finite, n_fb + 1 <= fb_max
+  HY_HASFB = 8,    // a fallback value exists (need and adjacent confidence >= conf_min)
+  HY_AGREE = 16,   // |u_direct - u_fallback| <= fb_tol
+  HY_RENOFB = 32,  // candidate without a fallback value (after the spatial gate when it ran)
+  HY_RE = 64,      // re-acquired
+  HY_FBCAND = 128, // fallback candidate
+  HY_FBOK = 256    // fallback candidate that passed the spatial gate
+};
+
+__device__ __forceinline__ double conf_at64(const float* __restrict__ conf, int W, int H, double px, double py) {
+  const double c = bilinear64(conf, W, H, px, py);
+  return isfinite(c) ? c : 0.0;
+}
+
+// the reference moves to k - 1 (track.py:433-437): c0K = the old leg's confidence at X + u0K where the pixel was
+// direct-good at k - 1, else 0 (unanchored); anch = good_prev
+__global__ void k_hyb_move(const float* __restrict__ pconf, const float* __restrict__ u0x,
+                           const float* __restrict__ u0y, const uint8_t* __restrict__ good_prev, int W, int H,
+                           double* __restrict__ c0r, uint8_t* __restrict__ anch) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  const size_t i = (size_t)y * W + x;
+  const bool g = good_prev[i] != 0;
+  c0r[i] = g ? conf_at64(pconf, W, H, x + (double)u0x[i], y + (double)u0y[i]) : 0.0;
+  anch[i] = g ? 1 : 0;
+}
+
+// the direct leg on the frame-0 grid (track.py:441-451): c = compose(u0K, leg), leg_c = conf_at(leg, u0K), link,
+// and the classes good, cand_re, need; any[0] = some pixel needs the adjacent leg
+__global__ void k_hyb_classify(const float* __restrict__ rx, const float* __restrict__ ry,
+                               const float* __restrict__ conf, const float* __restrict__ u0x,
+                               const float* __restrict__ u0y, const double* __restrict__ c0r,
+                               const uint8_t* __restrict__ anch, const float* __restrict__ upx,
+                               const float* __restrict__ upy, const int* __restrict__ nfb,
+                               const uint8_t* __restrict__ roi, int W, int H, double conf_min, int fb_max,
+                               int reacq_ok, float* __restrict__ cx, float* __restrict__ cy,
+                               double* __restrict__ legc, double* __restrict__ link, uint16_t* __restrict__ fl,
+                               int* any) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  const size_t i = (size_t)y * W + x;
+  const double u = u0x[i], v = u0y[i], px = x + u, py = y + v;
+  const float vx = (float)(u + bilinear64(rx, W, H, px, py)), vy = (float)(v + bilinear64(ry, W, H, px, py));
+  const double lc = conf_at64(conf, W, H, px, py);
+  const bool an = anch[i] != 0, in = !roi || roi[i];
+  const double lk = an ? fmin(c0r[i], lc) : lc;
+  const bool dok = isfinite(vx) && isfinite(vy) && lk >= conf_min;
+  const bool good = dok && an;
+  const bool cre = dok && !an && in && reacq_ok;
+  const bool need = !good && in && isfinite(upx[i]) && isfinite(upy[i]) && nfb[i] < fb_max;
+  cx[i] = vx;
+  cy[i] = vy;
+  legc[i] = lc;
+  link[i] = lk;
+  fl[i] = (good ? HY_GOOD : 0) | (cre ? HY_CANDRE : 0) | (need ? HY_NEED : 0);
+  if (need) *any = 1;
+}
+
+// the adjacent leg carried from u_{k-1} (track.py:453-464): a = compose(u_{k-1}, adj), u_{k-1} where that leaves the
+// image, ca = conf_at(adj, u_{k-1}); without the leg (rx null) a = u_{k-1}, ca = 0
+__global__ void k_hyb_adjacent(const float* __restrict__ rx, const float* __restrict__ ry,
+                               const float* __restrict__ conf, const float* __restrict__ upx,
+                               const float* __restrict__ upy, int W, int H, float* __restrict__ ax,
+                               float* __restrict__ ay, double* __restrict__ ca) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  const size_t i = (size_t)y * W + x;
+  if (!rx) {
+    ax[i] = upx[i];
+    ay[i] = upy[i];
+    ca[i] = 0.0;
+    return;
+  }
+  const double u = upx[i], v = upy[i], px = x + u, py = y + v;
+  const float vx = (float)(u + bilinear64(rx, W, H, px, py)), vy = (float)(v + bilinear64(ry, W, H, px, py));
+  const bool ok = isfinite(vx) && isfinite(vy);
+  ax[i] = ok ? vx : upx[i];
+  ay[i] = ok ? vy : upy[i];
+  ca[i] = conf_at64(conf, W, H, px, py);
+}
+
+// has_fb, agree, re_nofb (track.py:465-470); support = good & roi for the gate of re_nofb; any[1] = some ROI pixel
+// is a candidate without a fallback value
+__global__ void k_hyb_pre(uint16_t* __restrict__ fl, const float* __restrict__ cx, const float* __restrict__ cy,
+                          const float* __restrict__ ax, const float* __restrict__ ay, const double* __restrict__ ca,
+                          const uint8_t* __restrict__ roi, size_t N, double conf_min, double fb_tol,
+                          uint8_t* __restrict__ support, int* any) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    uint16_t f = fl[i];
+    const bool in = !roi || roi[i];
+    const bool hasfb = (f & HY_NEED) && ca[i] >= conf_min;
+    const bool agree = hypot((double)cx[i] - (double)ax[i], (double)cy[i] - (double)ay[i]) <= fb_tol;
+    const bool renofb = (f & HY_CANDRE) && !hasfb;
+    f |= (hasfb ? HY_HASFB : 0) | (agree ? HY_AGREE : 0) | (renofb ? HY_RENOFB : 0);
+    fl[i] = f;
+    support[i] = ((f & HY_GOOD) && in) ? 1 : 0;
+    if (renofb && in) any[1] = 1;
+  }
+}
+
+// re-acquisition and the counters (track.py:476-481): re = (cand_re & has_fb & agree) | re_nofb (gated by gate0
+// when given), c0K = leg_c and anchored where re, good |= re, n_fb = 0 where good else min(n_fb + 1, fb_max + 1),
+// fb_cand; support = good & roi for the fallback gate; any[2] = some ROI pixel is a fallback candidate
+__global__ void k_hyb_re(uint16_t* __restrict__ fl, const uint8_t* __restrict__ gate0,
+                         const double* __restrict__ legc, double* __restrict__ c0r, uint8_t* __restrict__ anch,
+                         int* __restrict__ nfb, const double* __restrict__ ca, const uint8_t* __restrict__ roi,
+                         size_t N, int fb_max, double conf_min, uint8_t* __restrict__ support, int* any) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    uint16_t f = fl[i];
+    const bool in = !roi || roi[i];
+    const bool renofb = (f & HY_RENOFB) && (!gate0 || gate0[i]);
+    const bool re = ((f & HY_CANDRE) && (f & HY_HASFB) && (f & HY_AGREE)) || renofb;
+    bool good = (f & HY_GOOD) != 0;
+    if (re) {
+      c0r[i] = legc[i];
+      anch[i] = 1;
+      good = true;
+    }
+    const int nf = good ? 0 : (int)min((long long)nfb[i] + 1, (long long)fb_max + 1);
+    nfb[i] = nf;
+    const bool fbc = !good && (f & HY_NEED) && nf <= fb_max && ca[i] >= conf_min;
+    f = (uint16_t)((f & ~(HY_GOOD | HY_RENOFB)) | (good ? HY_GOOD : 0) | (renofb ? HY_RENOFB : 0) |
+                   (re ? HY_RE : 0) | (fbc ? HY_FBCAND : 0));
+    fl[i] = f;
+    support[i] = (good && in) ? 1 : 0;
+    if (fbc && in) any[2] = 1;
+  }
+}
+
+// the frame's output (track.py:486-501): u = c where good else a (u_{k} of the next frame, and its float64 copy
+// for the finish), conf = link or ca (1 - n_fb / (fb_max + 1))^+, low = !(good | fb_ok), good_prev = good;
+// cnt[0..2] += fb_ok, fb_cand & !fb_ok, re over the ROI; cnt[3] = max n_fb over the image
+__global__ void k_hyb_out(uint16_t* __restrict__ fl, const uint8_t* __restrict__ gate, const float* __restrict__ cx,
+                          const float* __restrict__ cy, const float* __restrict__ ax, const float* __restrict__ ay,
+                          const double* __restrict__ link, const double* __restrict__ ca, const int* __restrict__ nfb,
+                          const uint8_t* __restrict__ roi, size_t N, int fb_max, float* __restrict__ ux,
+                          float* __restrict__ uy, double* __restrict__ u64x, double* __restrict__ u64y,
+                          double* __restrict__ conf, uint8_t* __restrict__ low, uint8_t* __restrict__ good_prev,
+                          unsigned long long* cnt) {
+  unsigned long long c0 = 0, c1 = 0, c2 = 0, mx = 0;
+  const double cap = (double)fb_max + 1.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+    uint16_t f = fl[i];
+    const bool in = !roi || roi[i];
+    const bool good = (f & HY_GOOD) != 0;
+    const bool fbok = (f & HY_FBCAND) && (!gate || gate[i]);
+    const float vx = good ? cx[i] : ax[i], vy = good ? cy[i] : ay[i];
+    ux[i] = vx;
+    uy[i] = vy;
+    u64x[i] = vx;
+    u64y[i] = vy;
+    const int nf = nfb[i];
+    conf[i] = good ? link[i] : ca[i] * fmax(0.0, 1.0 - (double)nf / cap);
+    low[i] = (good || fbok) ? 0 : 1;
+    good_prev[i] = good ? 1 : 0;
+    fl[i] = (uint16_t)(f | (fbok ? HY_FBOK : 0));
+    c0 += (fbok && in);
+    c1 += ((f & HY_FBCAND) && !fbok && in);
+    c2 += ((f & HY_RE) && in);
+    mx = max(mx, (unsigned long long)nf);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    c0 += __shfl_down_sync(0xffffffffu, c0, o);
+    c1 += __shfl_down_sync(0xffffffffu, c1, o);
+    c2 += __shfl_down_sync(0xffffffffu, c2, o);
+    mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (c0) atomicAdd(&cnt[0], c0);
+    if (c1) atomicAdd(&cnt[1], c1);
+    if (c2) atomicAdd(&cnt[2], c2);
+    atomicMax(&cnt[3], mx);
+  }
+}
+
+// _local_affine_agreement (track.py:331-382): window sums of the 12 moments of the selected pixels, rows first
+// (zero outside the image), then the columns and the 3 x 3 ridge solve per pixel. Moments, in order: 1, x, y, xx,
+// xy, yy, u, xu, yu, v, xv, yv, each a product of the pixel's own float64 values (the reference's box(w * xx * comp)).
+constexpr int LAA_M = 12;
+
+template <typename T>
+__global__ void k_laa_rows(const uint8_t* __restrict__ sel, const T* __restrict__ ux, const T* __restrict__ uy, int W,
+                           int H, int r, double* __restrict__ rows) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  const size_t row = (size_t)y * W, N = (size_t)W * H;
+  double s[LAA_M];
+#pragma unroll
+  for (int m = 0; m < LAA_M; m++) s[m] = 0.0;
+  const double yd = y;
+  const int q0 = max(0, x - r), q1 = min(W - 1, x + r);
+  for (int q = q0; q <= q1; q++) {
+    if (!sel[row + q]) continue;
+    const double xd = q, u = (double)ux[row + q], v = (double)uy[row + q];
+    s[0] += 1.0;
+    s[1] += xd;
+    s[2] += yd;
+    s[3] += xd * xd;
+    s[4] += xd * yd;
+    s[5] += yd * yd;
+    s[6] += u;
+    s[7] += xd * u;
+    s[8] += yd * u;
+    s[9] += v;
+    s[10] += xd * v;
+    s[11] += yd * v;
+  }
+#pragma unroll
+  for (int m = 0; m < LAA_M; m++) rows[m * N + row + x] = s[m];
+}
+
+// m c = b for two right-hand sides by Gaussian elimination with partial pivoting (the first of equal pivots, as
+// LAPACK's getrf); false for a zero or non-finite pivot (hybrid.rs:112-144)
+__device__ bool solve3x2(double a[3][5], double out[3][2]) {
+  for (int c = 0; c < 3; c++) {
+    int p = c;
+    for (int i = c + 1; i < 3; i++)
+      if (fabs(a[i][c]) > fabs(a[p][c])) p = i;
+    if (a[p][c] == 0.0 || !isfinite(a[p][c])) return false;
+    if (p != c)
+      for (int j = 0; j < 5; j++) {
+        const double t = a[c][j];
+        a[c][j] = a[p][j];
+        a[p][j] = t;
+      }
+    for (int i = c + 1; i < 3; i++) {
+      const double f = a[i][c] / a[c][c];
+      for (int j = c; j < 5; j++) a[i][j] -= f * a[c][j];
+    }
+  }
+  for (int k = 0; k < 2; k++)
+    for (int i = 2; i >= 0; i--) {
+      double s = a[i][3 + k];
+      for (int j = i + 1; j < 3; j++) s -= a[i][j] * out[j][k];
+      out[i][k] = s / a[i][i];
+    }
+  return true;
+}
+
+// the column sums and the fit at every pixel; pass 0 writes the robust selection of the next pass (support pixels
+// within 3 tol of their own model), pass 1 the test ok = n + 0.5 >= min_support, n >= 3, |(tx, ty) - a| <= tol
+template <typename T>
+__global__ void k_laa_solve(const double* __restrict__ rows, int W, int H, int r, double ridge, int pass,
+                            const uint8_t* __restrict__ support, const T* __restrict__ ux, const T* __restrict__ uy,
+                            const T* __restrict__ tx, const T* __restrict__ ty, double tol, double min_support,
+                            uint8_t* __restrict__ out, int* __restrict__ nout) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  const size_t N = (size_t)W * H, i = (size_t)y * W + x;
+  double S[LAA_M];
+#pragma unroll
+  for (int m = 0; m < LAA_M; m++) S[m] = 0.0;
+  const int q0 = max(0, y - r), q1 = min(H - 1, y + r);
+  for (int q = q0; q <= q1; q++) {
+    const size_t j = (size_t)q * W + x;
+#pragma unroll
+    for (int m = 0; m < LAA_M; m++) S[m] += rows[m * N + j];
+  }
+  const double xd = x, yd = y, s1 = S[0];
+  const bool okfit = s1 >= 3.0;
+  double a0 = nan(""), a1 = nan("");
+  if (okfit) {
+    const double sxc = S[1] - xd * s1, syc = S[2] - yd * s1;
+    const double sxxc = S[3] - 2.0 * xd * S[1] + xd * xd * s1;
+    const double sxyc = S[4] - xd * S[2] - yd * S[1] + xd * yd * s1;
+    const double syyc = S[5] - 2.0 * yd * S[2] + yd * yd * s1;
+    double a[3][5] = {{s1, sxc, syc, S[6], S[9]},
+                      {sxc, sxxc + ridge * s1, sxyc, S[7] - xd * S[6], S[10] - xd * S[9]},
+                      {syc, sxyc, syyc + ridge * s1, S[8] - yd * S[6], S[11] - yd * S[9]}};
+    double c[3][2];
+    if (solve3x2(a, c)) {
+      a0 = c[0][0];
+      a1 = c[0][1];
+    }
+  }
+  if (pass == 0) {
+    out[i] = (support[i] && hypot((double)ux[i] - a0, (double)uy[i] - a1) <= 3.0 * tol) ? 1 : 0;
+  } else {
+    out[i] = (s1 + 0.5 >= min_support && okfit && hypot((double)tx[i] - a0, (double)ty[i] - a1) <= tol) ? 1 : 0;
+    if (nout) nout[i] = (int)rint(s1);
+  }
+}
+
 // low = conf < conf_min (track.py:66) for ofc_finish
 __global__ void k_threshold_low(const double* c64, double cm, uint8_t* low, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -1081,6 +1371,35 @@ void cfg_check(const ofc_config* c) {
   if (!c) throw Error(OFC_ERR_ARG, "null config");
   std::string m = validate(*c);
   if (!m.empty()) throw Error(OFC_ERR_ARG, m);
+}
+
+// Config.validate for the hybrid keys (config.py:195-200), the reference's messages
+void hybrid_check(const ofc_hybrid* hy) {
+  if (!hy) throw Error(OFC_ERR_ARG, "null hybrid keys");
+  if (hy->fb_max < 0) throw Error(OFC_ERR_ARG, "fb_max must be >= 0");
+  if (!std::isfinite(hy->fb_radius) || !std::isfinite(hy->fb_tol) || hy->fb_tol <= 0 || hy->fb_radius == 0)
+    throw Error(OFC_ERR_ARG, "fb_radius must be finite and nonzero (negative: 4 sigma_w), fb_tol finite and positive");
+  if (hy->fb_min_support < 0) throw Error(OFC_ERR_ARG, "fb_min_support must be >= 0 and tavg in [0, 64]");
+}
+
+// _local_affine_agreement on device planes (track.py:331-382): two passes of row sums and column sums + solve; the
+// half-size r = max(1, round(radius)) (ties to even), the ridge 1e-3 r^2 on B
+template <typename T>
+void laa_dev(Lane& L, int W, int H, const uint8_t* support, const T* ux, const T* uy, const T* tx, const T* ty,
+             double radius, long long min_support, double tol, uint8_t* ok, int* nout) {
+  cudaStream_t st = L.stream;
+  const size_t N = (size_t)W * H;
+  const double rd = std::max(1.0, std::nearbyint(radius));
+  const double ridge = 1e-3 * rd * rd;
+  const int r = (int)std::min(rd, (double)std::max(W, H));  // a wider window clips to the same sums
+  double* rows = L.get<double>("laa_rows", LAA_M * N);
+  uint8_t* sel = L.get<uint8_t>("laa_sel", N);
+  const dim3 g(div_up(W, 128), H);
+  const double ms = (double)min_support;
+  OFC_LAUNCH(k_laa_rows<T>, g, 128, 0, st, support, ux, uy, W, H, r, rows);
+  OFC_LAUNCH(k_laa_solve<T>, g, 128, 0, st, rows, W, H, r, ridge, 0, support, ux, uy, tx, ty, tol, ms, sel, nullptr);
+  OFC_LAUNCH(k_laa_rows<T>, g, 128, 0, st, sel, ux, uy, W, H, r, rows);
+  OFC_LAUNCH(k_laa_solve<T>, g, 128, 0, st, rows, W, H, r, ridge, 1, sel, ux, uy, tx, ty, tol, ms, ok, nout);
 }
 
 }  // namespace
@@ -1596,7 +1915,7 @@ int ofc_track_sequence(ofc_engine* e, const float* const* frames, size_t n, size
     for (size_t k = 0; k < n; k++)
       if (!frames[k]) throw Error(OFC_ERR_ARG, "null frame " + std::to_string(k));
     if (n > 1 && !outs) throw Error(OFC_ERR_ARG, "null outputs");
-    if (!(ref_update_conf >= 0.0 && ref_update_conf <= 1.0)) throw Error(OFC_ERR_ARG, "ref_update_conf must be in [0, 1]");
+    if (!std::isfinite(ref_update_conf)) throw Error(OFC_ERR_ARG, "ref_update_conf must be a finite number");
     const size_t N = w * h;
     if (roi) {
       bool any = false;
@@ -1704,6 +2023,243 @@ int ofc_track_sequence(ofc_engine* e, const float* const* frames, size_t n, size
       if (mean_conf) mean_conf[k - 1] = cmean;
       have_prev = true;
     }
+  });
+}
+
+int ofc_track_sequence_hybrid(ofc_engine* e, const float* const* frames, size_t n, size_t w, size_t h,
+                              const uint8_t* roi, const ofc_config* c, const double* ruc, const ofc_hybrid* hy,
+                              ofc_pair_out* outs, int32_t* fb, ofc_hybrid_frame* info, ofc_leg_fn legfn,
+                              void* leg_user, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    hybrid_check(hy);
+    if (!frames || n == 0) throw Error(OFC_ERR_ARG, "no frames");
+    check_sizes(w, h);
+    for (size_t k = 0; k < n; k++)
+      if (!frames[k]) throw Error(OFC_ERR_ARG, "null frame " + std::to_string(k));
+    if (n > 1 && !outs) throw Error(OFC_ERR_ARG, "null outputs");
+    if (n > 1 && !ruc) throw Error(OFC_ERR_ARG, "null ref_update_conf");
+    for (size_t k = 0; k + 1 < n; k++)
+      if (!std::isfinite(ruc[k])) throw Error(OFC_ERR_ARG, "ref_update_conf must be a finite number");
+    const size_t N = w * h;
+    size_t n_roi = N;
+    if (roi) {
+      n_roi = 0;
+      for (size_t i = 0; i < N; i++) n_roi += roi[i] != 0;
+      if (n_roi == 0) throw Error(OFC_ERR_ARG, "ROI mask is empty");
+    }
+    if (n == 1) return;
+    if ((int)std::min(w, h) < c->poc_win)
+      throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
+    if (!legfn) check_fine_window(w, h, *c);
+    const int W = (int)w, H = (int)h;
+    cudaStream_t st = L.stream;
+    const dim3 g2(div_up(W, 128), H);
+    const unsigned gN = std::min<unsigned>(div_up(N, 256), 148 * 8);
+    const double cm = c->conf_min, radius = hy->fb_radius > 0 ? hy->fb_radius : 4.0 * c->sigma_w;
+    const bool gate_on = hy->fb_min_support > 0;
+    // the chain's state (track.py:423-427) and the hybrid's (track.py:428-431)
+    float* ref = L.get<float>("seq_ref", N);
+    float* prev = L.get<float>("seq_prev", N);
+    float* fk = L.get<float>("seq_fk", N);
+    float* u0r = L.get<float>("seq_u0r", 2 * N);
+    double* c0r = L.get<double>("seq_c0r", N);
+    float* praw = L.get<float>("seq_praw", 2 * N);  // the direct leg of the last frame: its raw field and conf
+    float* pconf = L.get<float>("seq_pconf", N);
+    float* rep = L.get<float>("seq_rep", N);
+    double* rsum = L.get<double>("seq_rsum", (size_t)H);
+    long long* rcnt = L.get<long long>("seq_rcnt", (size_t)H);
+    double* dmean = L.get<double>("seq_mean", 1);
+    uint8_t* low = L.get<uint8_t>("seq_low", N);
+    uint8_t* anch = L.get<uint8_t>("hy_anch", N);
+    uint8_t* goodp = L.get<uint8_t>("hy_goodp", N);
+    int* nfb = L.get<int>("hy_nfb", N);
+    float* uprev = L.get<float>("hy_uprev", 2 * N);
+    float* padj = L.get<float>("hy_padj", 2 * N);
+    float* cxy = L.get<float>("hy_cxy", 2 * N);
+    float* axy = L.get<float>("hy_axy", 2 * N);
+    double* legc = L.get<double>("hy_legc", N);
+    double* link = L.get<double>("hy_link", N);
+    double* ca = L.get<double>("hy_ca", N);
+    double* conf64 = L.get<double>("hy_conf", N);
+    double* u64 = L.get<double>("hy_u64", 2 * N);
+    uint16_t* fl = L.get<uint16_t>("hy_flags", N);
+    uint8_t* support = L.get<uint8_t>("hy_support", N);
+    uint8_t* gate0 = L.get<uint8_t>("hy_gate0", N);
+    uint8_t* gate = L.get<uint8_t>("hy_gate", N);
+    int* dany = L.get<int>("hy_any", 4);
+    unsigned long long* dcnt = L.get<unsigned long long>("hy_cnt", 4);
+    const uint8_t* droi = roi ? L.upload("seq_roi", roi, N) : nullptr;
+    float* in1 = L.get<float>("in_i1", N);
+    float* in2 = L.get<float>("in_i2", N);
+    float* inu = L.get<float>("in_u", N);
+    float* inv = L.get<float>("in_v", N);
+    const ofc_pair_out d = device_pair_out(L, N);  // a leg's conf, raw_ux, raw_uy; the frame's outputs
+    const double B = guard_px(*c) > 0 ? 4.0 * c->sigma_w : 0.0;
+    OFC_CUDA(cudaMemcpyAsync(ref, frames[0], N * 4, cudaMemcpyHostToDevice, st));
+    OFC_CUDA(cudaMemcpyAsync(prev, ref, N * 4, cudaMemcpyDeviceToDevice, st));
+    OFC_CUDA(cudaMemsetAsync(u0r, 0, 2 * N * 4, st));
+    launch_fill_f64(c0r, 1.0, N, st);
+    OFC_CUDA(cudaMemsetAsync(anch, 1, N, st));
+    OFC_CUDA(cudaMemsetAsync(goodp, 1, N, st));
+    OFC_CUDA(cudaMemsetAsync(nfb, 0, N * 4, st));
+    OFC_CUDA(cudaMemsetAsync(uprev, 0, 2 * N * 4, st));
+    bool have_prev = false, have_padj = false;
+    int ref_idx = 0;
+    std::vector<float> hbuf;
+    // one leg frames[ia] -> frames[ib] (track.py:200-206) into d's conf / raw planes: the engine's coarse and fine
+    // stages with the dense start `init` (2 planes, nullable), or the caller's leg source; returns coarse, fine (s)
+    auto leg = [&](const float* a, int ia, const float* b, int ib, const float* init) -> std::pair<double, double> {
+      if (legfn) {
+        hbuf.resize(5 * N);
+        float* hi = hbuf.data();
+        float* ho = hi + 2 * N;
+        if (init) OFC_CUDA(cudaMemcpyAsync(hi, init, 2 * N * 4, cudaMemcpyDeviceToHost, st));
+        OFC_CUDA(cudaStreamSynchronize(st));
+        if (legfn(leg_user, ia, ib, init ? hi : nullptr, init ? hi + N : nullptr, ho, ho + N, ho + 2 * N) != 0)
+          throw Error(OFC_ERR_ARG, "the leg source failed on the leg " + std::to_string(ia) + " -> " + std::to_string(ib));
+        OFC_CUDA(cudaMemcpyAsync(d.raw_ux, ho, N * 4, cudaMemcpyHostToDevice, st));
+        OFC_CUDA(cudaMemcpyAsync(d.raw_uy, ho + N, N * 4, cudaMemcpyHostToDevice, st));
+        OFC_CUDA(cudaMemcpyAsync(d.conf, ho + 2 * N, N * 4, cudaMemcpyHostToDevice, st));
+        OFC_CUDA(cudaStreamSynchronize(st));
+        return {0.0, 0.0};
+      }
+      OFC_CUDA(cudaMemcpyAsync(in1, a, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(in2, b, N * 4, cudaMemcpyDeviceToDevice, st));
+      if (init) {
+        OFC_CUDA(cudaMemcpyAsync(inu, init, N * 4, cudaMemcpyDeviceToDevice, st));
+        OFC_CUDA(cudaMemcpyAsync(inv, init + N, N * 4, cudaMemcpyDeviceToDevice, st));
+      }
+      run_pair(L, W, H, false, init != nullptr, *c, true, 2);
+      float ms0 = 0, ms1 = 0;
+      OFC_CUDA(cudaEventSynchronize(L.ev[3]));
+      OFC_CUDA(cudaEventElapsedTime(&ms0, L.ev[0], L.ev[1]));
+      OFC_CUDA(cudaEventElapsedTime(&ms1, L.ev[1], L.ev[3]));
+      return {ms0 * 1e-3, ms1 * 1e-3};
+    };
+    auto leg_mean = [&]() {
+      OFC_LAUNCH(k_reportable, g2, 128, 0, st, d.raw_ux, d.raw_uy, W, H, B, rep);
+      OFC_LAUNCH(k_mean_conf_rows, div_up(H, 128), 128, 0, st, d.conf, rep, u0r, u0r + N, droi, W, H, rsum, rcnt);
+      OFC_LAUNCH(k_mean_conf_fold, 1, 1, 0, st, rsum, rcnt, H, dmean);
+      double m = 0;
+      OFC_CUDA(cudaMemcpyAsync(&m, dmean, 8, cudaMemcpyDeviceToHost, st));
+      OFC_CUDA(cudaStreamSynchronize(st));
+      return m;
+    };
+    int any[4];
+    auto read_any = [&]() {
+      OFC_CUDA(cudaMemcpyAsync(any, dany, sizeof(any), cudaMemcpyDeviceToHost, st));
+      OFC_CUDA(cudaStreamSynchronize(st));
+    };
+    for (size_t k = 1; k < n; k++) {
+      const int K = (int)k;
+      OFC_CUDA(cudaMemcpyAsync(fk, frames[k], N * 4, cudaMemcpyHostToDevice, st));
+      std::pair<double, double> t = leg(ref, ref_idx, fk, K, have_prev ? praw : nullptr);
+      double cmean = leg_mean();
+      if (cmean < ruc[k - 1] && ref_idx != K - 1) {
+        // the reference moves to k - 1 (track.py:433-440): c0K replaced, anchors = good_prev, u0K = u_{k-1}
+        OFC_LAUNCH(k_hyb_move, g2, 128, 0, st, pconf, u0r, u0r + N, goodp, W, H, c0r, anch);
+        OFC_CUDA(cudaMemcpyAsync(u0r, uprev, 2 * N * 4, cudaMemcpyDeviceToDevice, st));
+        OFC_CUDA(cudaMemcpyAsync(ref, prev, N * 4, cudaMemcpyDeviceToDevice, st));
+        ref_idx = K - 1;
+        t = leg(ref, ref_idx, fk, K, nullptr);
+        cmean = leg_mean();
+      }
+      OFC_CUDA(cudaMemcpyAsync(praw, d.raw_ux, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(praw + N, d.raw_uy, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(pconf, d.conf, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaMemsetAsync(dany, 0, 4 * sizeof(int), st));
+      OFC_CUDA(cudaMemsetAsync(dcnt, 0, 4 * sizeof(unsigned long long), st));
+      OFC_LAUNCH(k_hyb_classify, g2, 128, 0, st, praw, praw + N, pconf, u0r, u0r + N, c0r, anch, uprev, uprev + N,
+                 nfb, droi, W, H, cm, hy->fb_max, ref_idx + 1 < K ? 1 : 0, cxy, cxy + N, legc, link, fl, dany);
+      read_any();
+      const float *arx = nullptr, *ary = nullptr, *acf = nullptr;
+      if (any[0]) {
+        if (ref_idx == K - 1) {  // the direct leg is the adjacent leg
+          arx = praw;
+          ary = praw + N;
+          acf = pconf;
+        } else {
+          const std::pair<double, double> ta = leg(prev, K - 1, fk, K, have_padj ? padj : nullptr);
+          t.first += ta.first;
+          t.second += ta.second;
+          arx = d.raw_ux;
+          ary = d.raw_uy;
+          acf = d.conf;
+        }
+      }
+      OFC_LAUNCH(k_hyb_adjacent, g2, 128, 0, st, arx, ary, acf, uprev, uprev + N, W, H, axy, axy + N, ca);
+      if (any[0]) {
+        OFC_CUDA(cudaMemcpyAsync(padj, arx, N * 4, cudaMemcpyDeviceToDevice, st));
+        OFC_CUDA(cudaMemcpyAsync(padj + N, ary, N * 4, cudaMemcpyDeviceToDevice, st));
+      }
+      have_padj = any[0] != 0;
+      OFC_LAUNCH(k_hyb_pre, gN, 256, 0, st, fl, cxy, cxy + N, axy, axy + N, ca, droi, N, cm, hy->fb_tol, support,
+                 dany);
+      read_any();
+      const uint8_t* g0 = nullptr;
+      if (gate_on && any[1]) {
+        laa_dev<float>(L, W, H, support, cxy, cxy + N, cxy, cxy + N, radius, hy->fb_min_support, hy->fb_tol, gate0,
+                       nullptr);
+        g0 = gate0;
+      }
+      OFC_LAUNCH(k_hyb_re, gN, 256, 0, st, fl, g0, legc, c0r, anch, nfb, ca, droi, N, hy->fb_max, cm, support, dany);
+      read_any();
+      const uint8_t* g1 = nullptr;
+      if (gate_on && any[2]) {
+        laa_dev<float>(L, W, H, support, cxy, cxy + N, axy, axy + N, radius, hy->fb_min_support, hy->fb_tol, gate,
+                       nullptr);
+        g1 = gate;
+      }
+      OFC_LAUNCH(k_hyb_out, gN, 256, 0, st, fl, g1, cxy, cxy + N, axy, axy + N, link, ca, nfb, droi, N, hy->fb_max,
+                 uprev, uprev + N, u64, u64 + N, conf64, low, goodp, dcnt);
+      OFC_CUDA(cudaEventRecord(L.ev[0], st));
+      finish_dev(L, low, droi, u64, u64 + N, conf64, W, H, *c, d, false);
+      OFC_CUDA(cudaEventRecord(L.ev[1], st));
+      download_pair(L, d, &outs[k - 1], N);
+      if (fb) OFC_CUDA(cudaMemcpyAsync(fb + (k - 1) * N, nfb, N * 4, cudaMemcpyDeviceToHost, st));
+      unsigned long long cnt[4];
+      OFC_CUDA(cudaMemcpyAsync(cnt, dcnt, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+      OFC_CUDA(cudaMemcpyAsync(prev, fk, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaStreamSynchronize(st));
+      float ms = 0;
+      OFC_CUDA(cudaEventElapsedTime(&ms, L.ev[0], L.ev[1]));
+      outs[k - 1].timing[0] = t.first;
+      outs[k - 1].timing[1] = t.second;
+      outs[k - 1].timing[2] = ms * 1e-3;
+      if (info) {
+        ofc_hybrid_frame& f = info[k - 1];
+        f.reference = ref_idx;
+        f.n_fb_max = (int32_t)cnt[3];
+        f.mean_conf = cmean;
+        f.fallback_frac = (double)cnt[0] / (double)n_roi;
+        f.fb_gate_rejected = (double)cnt[1] / (double)n_roi;
+        f.reacquired = (double)cnt[2] / (double)n_roi;
+      }
+      have_prev = true;
+    }
+  });
+}
+
+int ofc_local_affine_agreement(ofc_engine* e, size_t w, size_t h, const double* ux, const double* uy,
+                               const uint8_t* support, const double* tx, const double* ty, double radius,
+                               int64_t min_support, double tol, uint8_t* ok, int32_t* n, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    check_sizes(w, h);
+    if (!ux || !uy || !support || !tx || !ty || !ok) throw Error(OFC_ERR_ARG, "null argument");
+    if (!std::isfinite(radius) || !std::isfinite(tol)) throw Error(OFC_ERR_ARG, "radius and tol must be finite");
+    const size_t N = w * h;
+    const double* dux = L.upload("laa_ux", ux, N);
+    const double* duy = L.upload("laa_uy", uy, N);
+    const double* dtx = L.upload("laa_tx", tx, N);
+    const double* dty = L.upload("laa_ty", ty, N);
+    const uint8_t* dsup = L.upload("laa_support", support, N);
+    uint8_t* dok = L.get<uint8_t>("laa_ok", N);
+    int* dn = L.get<int>("laa_n", N);
+    laa_dev<double>(L, (int)w, (int)h, dsup, dux, duy, dtx, dty, radius, (long long)min_support, tol, dok, dn);
+    OFC_CUDA(cudaMemcpyAsync(ok, dok, N, cudaMemcpyDeviceToHost, L.stream));
+    if (n) OFC_CUDA(cudaMemcpyAsync(n, dn, N * 4, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
   });
 }
 

@@ -7,4 +7,4 @@ from ._abi import EngineError, load  # noqa: F401
 from .config import Config  # noqa: F401
 from .api import (Engine, Flow, Grid, Result, coarse_flow, displacement_gradient, finish, refine,  # noqa: F401
                   refine_raw, refine_batch, strain_fields, track_pair, track_pair_device,
-                  track_sequence)
+                  track_sequence, track_sequence_hybrid, local_affine_agreement)

@@ -86,6 +86,32 @@ class OfcWindow(ctypes.Structure):
     ]
 
 
+class OfcHybrid(ctypes.Structure):
+    """ofc_hybrid of include/optflow_cuda.h: the hybrid keys of Config."""
+    _fields_ = [
+        ("fb_max", ctypes.c_int32),
+        ("fb_radius", ctypes.c_double),
+        ("fb_min_support", ctypes.c_int32),
+        ("fb_tol", ctypes.c_double),
+    ]
+
+
+class OfcHybridFrame(ctypes.Structure):
+    """ofc_hybrid_frame of include/optflow_cuda.h: the per-frame record of a hybrid run."""
+    _fields_ = [
+        ("reference", ctypes.c_int32),
+        ("n_fb_max", ctypes.c_int32),
+        ("mean_conf", ctypes.c_double),
+        ("fallback_frac", ctypes.c_double),
+        ("fb_gate_rejected", ctypes.c_double),
+        ("reacquired", ctypes.c_double),
+    ]
+
+
+# ofc_leg_fn: (user, i, j, init_ux, init_uy, raw_ux, raw_uy, conf) -> 0 on success
+LEG_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, c_float_p, c_float_p,
+                          c_float_p, c_float_p, c_float_p)
+
 PAIR_FIELDS = ("ux", "uy", "conf", "exx", "eyy", "exy", "gmax", "vol", "valid", "raw_ux", "raw_uy")
 
 # every symbol the header declares, with its ctypes signature (restype, argtypes)
@@ -110,6 +136,13 @@ SIGNATURES = {
     "ofc_refine_batch": (ctypes.c_int, [_P, ctypes.c_void_p, _S, ctypes.POINTER(OfcConfig), _E, _S]),
     "ofc_track_sequence": (ctypes.c_int, [_P, ctypes.POINTER(c_float_p), _S, _S, _S, c_u8_p, ctypes.POINTER(OfcConfig),
                                           ctypes.c_double, ctypes.POINTER(OfcPairOut), c_i32_p, c_double_p, _E, _S]),
+    "ofc_track_sequence_hybrid": (ctypes.c_int, [_P, ctypes.POINTER(c_float_p), _S, _S, _S, c_u8_p,
+                                                 ctypes.POINTER(OfcConfig), c_double_p, ctypes.POINTER(OfcHybrid),
+                                                 ctypes.POINTER(OfcPairOut), c_i32_p, ctypes.POINTER(OfcHybridFrame),
+                                                 LEG_FN, _P, _E, _S]),
+    "ofc_local_affine_agreement": (ctypes.c_int, [_P, _S, _S, c_double_p, c_double_p, c_u8_p, c_double_p, c_double_p,
+                                                  ctypes.c_double, ctypes.c_int64, ctypes.c_double, c_u8_p, c_i32_p,
+                                                  _E, _S]),
     "ofc_align_to": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, c_u8_p, ctypes.c_int, ctypes.POINTER(OfcConfig),
                                     c_float_p, ctypes.POINTER(ctypes.c_int), _E, _S]),
     "ofc_average_window": (ctypes.c_int, [_P, ctypes.POINTER(c_float_p), _S, _S, _S, _S, ctypes.c_int, c_u8_p,

@@ -122,6 +122,7 @@ class Result:
     raw_uy: np.ndarray
     timing: dict = field(default_factory=dict)
     valid: np.ndarray = None
+    fb: np.ndarray = None  # hybrid sequences only: frames each pixel has been carried by the adjacent leg
 
 
 def _prep_cfg(cfg):
@@ -287,17 +288,9 @@ def track_pair(I1, I2, cfg=None, mask=None, init=None, engine=None) -> Result:
     return _result(o, arrs)
 
 
-def track_sequence(frames, cfg=None, mask=None, engine=None):
-    """track.track_sequence in chain mode (python/optflow_ref/track.py:260-315; rust/crates/optflow-core/src/track.rs:
-    1030-1245): yields (k, Result) with the displacement from frame 0 to frame k, k = 1, 2, ...; Result.timing adds
-    the reference index and the leg's mean confidence. The frames are tracked in one ofc_track_sequence call (all of
-    them are read first). seq_mode "hybrid" is not on the GPU engine (NotImplementedError)."""
-    cfg, c = _prep_cfg(cfg)
-    fr = [np.asarray(f) for f in frames]
+def _check_frames(fr, cfg, mask):
     if not fr:
         raise ValueError("no frames")
-    if cfg.seq_mode == "hybrid":
-        raise NotImplementedError("seq_mode 'hybrid' is not part of the GPU engine's sequence entry point")
     h, w = fr[0].shape
     for k, f in enumerate(fr):
         if f.shape != fr[0].shape:
@@ -308,6 +301,22 @@ def track_sequence(frames, cfg=None, mask=None, engine=None):
         raise ValueError("ROI mask is empty")
     if len(fr) > 1 and min(h, w) < cfg.poc_win:
         raise ValueError(f"image smaller than poc_win ({cfg.poc_win}): {fr[0].shape}")
+    return h, w
+
+
+def track_sequence(frames, cfg=None, mask=None, engine=None):
+    """track.track_sequence (python/optflow_ref/track.py:260-315; rust/crates/optflow-core/src/track.rs:1030-1245):
+    yields (k, Result) with the displacement from frame 0 to frame k, k = 1, 2, ...; Result.timing adds the reference
+    index and the leg's mean confidence. The frames are tracked in one ofc_track_sequence call (all of them are read
+    first); seq_mode "hybrid" goes to track_sequence_hybrid."""
+    cfg, c = _prep_cfg(cfg)
+    fr = [np.asarray(f) for f in frames]
+    if not fr:
+        raise ValueError("no frames")
+    if cfg.seq_mode == "hybrid":
+        yield from track_sequence_hybrid(fr, cfg, mask, engine=engine)
+        return
+    h, w = _check_frames(fr, cfg, mask)
     eng = engine or default_engine()
     f32 = [_f32(f) for f in fr]
     ptrs = (c_float_p * len(f32))(*[_ptr(f, c_float_p) for f in f32])
@@ -327,6 +336,90 @@ def track_sequence(frames, cfg=None, mask=None, engine=None):
         r = _result(outs[k - 1], arrs[k - 1])
         r.timing.update(reference=int(ref[k - 1]), mean_conf=float(mean[k - 1]))
         yield k, r
+
+
+def track_sequence_hybrid(frames, cfg=None, mask=None, ref_update_conf=None, legs=None, engine=None):
+    """track.track_sequence with seq_mode "hybrid" (python/optflow_ref/track.py:385-503; rust/crates/optflow-core/
+    src/track/hybrid.rs) over ofc_track_sequence_hybrid: yields (k, Result) with Result.fb (the fallback counters)
+    and the timing keys reference, mean_conf, n_fb_max, fallback_frac, fb_gate_rejected, reacquired.
+
+    ref_update_conf: one threshold per frame k = 1..n-1 (default cfg.ref_update_conf for all; the reference reads the
+    key anew at every frame). legs: a scripted leg source legs(i, j, init) -> (raw_ux, raw_uy, conf) that replaces
+    the engine's pair tracking of the leg frames[i] -> frames[j] (init: None or the (ux, uy) start), as the
+    reference's tests replace track_pair (python/tests/test_hybrid.py:38-52)."""
+    cfg, c = _prep_cfg(cfg)
+    fr = [np.asarray(f) for f in frames]
+    h, w = _check_frames(fr, cfg, mask)
+    nk = max(len(fr) - 1, 1)
+    ruc = np.full(nk, float(cfg.ref_update_conf)) if ref_update_conf is None else \
+        np.ascontiguousarray(ref_update_conf, dtype=np.float64)
+    if ruc.shape != (nk,):
+        raise ValueError(f"ref_update_conf needs one value per frame after the first ({nk})")
+    eng = engine or default_engine()
+    f32 = [_f32(f) for f in fr]
+    ptrs = (c_float_p * len(f32))(*[_ptr(f, c_float_p) for f in f32])
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    outs = (OfcPairOut * nk)()
+    arrs = []
+    for k in range(len(fr) - 1):
+        o, a = _pair_out(h, w)
+        outs[k] = o
+        arrs.append(a)
+    fb = np.zeros((nk, h, w), np.int32)
+    info = (_abi.OfcHybridFrame * nk)()
+    hy = _abi.OfcHybrid(int(cfg.fb_max), float(cfg.fb_radius), int(cfg.fb_min_support), float(cfg.fb_tol))
+    failure = []
+
+    def leg(_user, i, j, iu, iv, rx, ry, rc):
+        try:
+            init = None
+            if iu:
+                init = (np.ctypeslib.as_array(iu, (h, w)).copy(), np.ctypeslib.as_array(iv, (h, w)).copy())
+            out = legs(int(i), int(j), init)
+            for dst, src in zip((rx, ry, rc), out):
+                np.ctypeslib.as_array(dst, (h, w))[...] = np.broadcast_to(np.asarray(src, np.float32), (h, w))
+            return 0
+        except Exception as e:  # noqa: BLE001 -- handed back to the caller after the engine returns
+            failure.append(e)
+            return 1
+
+    fn = _abi.LEG_FN(leg) if legs is not None else _abi.LEG_FN()
+    try:
+        eng._call("ofc_track_sequence_hybrid", ptrs, len(fr), w, h, _ptr(m, c_u8_p), ctypes.byref(c),
+                  _ptr(ruc, c_double_p), ctypes.byref(hy), outs, _ptr(fb, _abi.c_i32_p), info, fn, None)
+    except ValueError:
+        if failure:
+            raise failure[0]
+        raise
+    for k in range(1, len(fr)):
+        r = _result(outs[k - 1], arrs[k - 1])
+        f = info[k - 1]
+        r.fb = fb[k - 1]
+        r.timing.update(reference=int(f.reference), mean_conf=float(f.mean_conf), n_fb_max=int(f.n_fb_max),
+                        fallback_frac=float(f.fallback_frac), fb_gate_rejected=float(f.fb_gate_rejected),
+                        reacquired=float(f.reacquired))
+        yield k, r
+
+
+def local_affine_agreement(ux, uy, support, tx, ty, radius, min_support, tol, engine=None):
+    """track._local_affine_agreement (python/optflow_ref/track.py:331-382) over ofc_local_affine_agreement: returns
+    (ok, n), ok = the robust local affine model of (ux, uy) on `support` predicts (tx, ty) within tol with at least
+    min_support pixels in the window, n = the number of them."""
+    eng = engine or default_engine()
+    a = np.ascontiguousarray(ux, dtype=np.float64)
+    if a.ndim != 2:
+        raise ValueError("2-D planes expected")
+    h, w = a.shape
+    planes = [np.ascontiguousarray(p, dtype=np.float64) for p in (uy, tx, ty)]
+    sup = np.ascontiguousarray(support, dtype=np.uint8)
+    if any(p.shape != (h, w) for p in planes) or sup.shape != (h, w):
+        raise ValueError("planes of different shapes")
+    ok = np.empty((h, w), np.uint8)
+    n = np.empty((h, w), np.int32)
+    eng._call("ofc_local_affine_agreement", w, h, _ptr(a, c_double_p), _ptr(planes[0], c_double_p),
+              _ptr(sup, c_u8_p), _ptr(planes[1], c_double_p), _ptr(planes[2], c_double_p), float(radius),
+              int(min_support), float(tol), _ptr(ok, c_u8_p), _ptr(n, _abi.c_i32_p))
+    return ok.astype(bool), n.astype(np.int64)
 
 
 def track_pair_device(I1, I2, cfg=None, mask=None, init=None, stream=None, engine=None):

@@ -66,6 +66,10 @@ class Config:
             return float(self.edge_guard_min_area)
         return 2.0 * (self.lam * max(self.scales)) ** 2
 
+    def fb_radius_px(self) -> float:
+        """Config.fb_radius_px (config.py:253-255): the hybrid gate's window half-size."""
+        return float(self.fb_radius) if self.fb_radius > 0 else 4.0 * self.sigma_w
+
     def n_filters(self) -> int:
         return self.n_orient * len(self.scales)
 
@@ -99,6 +103,12 @@ class Config:
             raise ValueError("n_orient, outer_iters and inner_iters must be >= 1")
         if not 0 <= self.conf_min <= 1 or not 0 <= self.poc_peak_min <= 1:
             raise ValueError("conf_min and poc_peak_min must lie in [0, 1]")
+        if self.fb_max < 0:
+            raise ValueError("fb_max must be >= 0")
+        if not _finite(self.fb_radius) or not _finite(self.fb_tol) or self.fb_tol <= 0 or self.fb_radius == 0:
+            raise ValueError("fb_radius must be finite and nonzero (negative: 4 sigma_w), fb_tol finite and positive")
+        if self.fb_min_support < 0 or self.tavg < 0 or self.tavg > 64:
+            raise ValueError("fb_min_support must be >= 0 and tavg in [0, 64]")
         if self.prewarp_freeze_at < 0:
             raise ValueError("prewarp_freeze_at must be >= 0")
         if (self.n_orient * len(self.scales) > 64 or self.sigma_w > 256 or self.sigma_s > 256

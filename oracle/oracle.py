@@ -360,3 +360,57 @@ def average_window(frames, centre, align=False, cfg=None, mask=None, keep_unalig
     for u in used[1:]:
         s += u
     return np.float32((c.astype(np.float64) + s) / (len(used) + 1))
+
+
+# ---------------------------------------------------------------- hybrid sequence gate
+def _window_sum(a, r):
+    """Sum over the (2r + 1)^2 window around every pixel, zero outside the image (hybrid.rs:69-108, the reference's
+    uniform_filter(mode="constant") * size^2), by a summed-area table."""
+    h, w = a.shape
+    s = np.zeros((h + 1, w + 1))
+    s[1:, 1:] = np.cumsum(np.cumsum(a, axis=0), axis=1)
+    y0 = np.clip(np.arange(h) - r, 0, h)
+    y1 = np.clip(np.arange(h) + r + 1, 0, h)
+    x0 = np.clip(np.arange(w) - r, 0, w)
+    x1 = np.clip(np.arange(w) + r + 1, 0, w)
+    return (s[y1][:, x1] - s[y0][:, x1] - s[y1][:, x0] + s[y0][:, x0])
+
+
+def local_affine_agreement(ux, uy, support, tx, ty, radius, min_support, tol):
+    """_local_affine_agreement (python/optflow_ref/track.py:331-382; rust/crates/optflow-core/src/track/hybrid.rs:
+    146-250): per pixel p the affine model u(q) = a + B (q - p), ridge 1e-3 r^2 on B, fitted by least squares to
+    (ux, uy) of the support pixels in the window of half-size r = max(1, round(radius)); two passes, the second
+    without the support pixels whose residual against their own first-pass model exceeds 3 tol. Returns (ok, n):
+    ok = n + 0.5 >= min_support, n >= 3 and |(tx, ty) - a| <= tol; n = the support of the last pass."""
+    h, w = ux.shape
+    r = max(1, int(round(radius)))
+    ridge = 1e-3 * r * r
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    support = np.asarray(support, bool)
+    u0, v0 = np.where(support, ux, 0.0), np.where(support, uy, 0.0)
+    sel = support.copy()
+    for it in range(2):
+        wt = sel.astype(np.float64)
+        S = [_window_sum(wt * f, r) for f in (np.ones_like(xx), xx, yy, xx * xx, xx * yy, yy * yy)]
+        s1, sx, sy, sxx, sxy, syy = S
+        m = np.empty((h, w, 3, 3))
+        m[..., 0, 0] = s1
+        m[..., 0, 1] = m[..., 1, 0] = sx - xx * s1
+        m[..., 0, 2] = m[..., 2, 0] = sy - yy * s1
+        m[..., 1, 1] = sxx - 2 * xx * sx + xx * xx * s1 + ridge * s1
+        m[..., 1, 2] = m[..., 2, 1] = sxy - xx * sy - yy * sx + xx * yy * s1
+        m[..., 2, 2] = syy - 2 * yy * sy + yy * yy * s1 + ridge * s1
+        fit = s1 >= 3
+        m[~fit] = np.eye(3)
+        a = []
+        for comp in (u0, v0):
+            su, sxu, syu = (_window_sum(wt * f * comp, r) for f in (np.ones_like(xx), xx, yy))
+            rhs = np.stack([su, sxu - xx * su, syu - yy * su], axis=-1)
+            rhs[~fit] = 0.0
+            a.append(np.where(fit, np.linalg.solve(m, rhs[..., None])[..., 0, 0], np.nan))
+        if it == 0:
+            with np.errstate(invalid="ignore"):
+                sel = support & (np.hypot(ux - a[0], uy - a[1]) <= 3 * tol)
+    with np.errstate(invalid="ignore"):
+        ok = (s1 + 0.5 >= min_support) & fit & (np.hypot(tx - a[0], ty - a[1]) <= tol)
+    return ok, np.rint(s1).astype(np.int64)

@@ -52,6 +52,4 @@ def test_track_sequence_arguments():
         next(track_sequence(fr, Config(), mask=np.zeros(fr[0].shape, bool)))
     with pytest.raises(ValueError, match="frame 2"):
         next(track_sequence(fr[:2] + [fr[2][:64]], Config()))
-    with pytest.raises(NotImplementedError):
-        next(track_sequence(fr, Config(seq_mode="hybrid")))
     assert list(track_sequence(fr[:1], Config())) == []

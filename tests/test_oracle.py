@@ -228,3 +228,20 @@ def test_ref_fixture_pair(oracle):
     assert rms(r["ux"], ux) < 1e-3 and rms(r["uy"], ref_fixture("pair_uy")) < 1e-3
     assert rms(r["conf"], ref_fixture("pair_conf")) < 1e-3
     assert rms(r["Exx"], ref_fixture("pair_Exx")) < 1e-5 and rms(r["gmax"], ref_fixture("pair_gmax")) < 1e-5
+
+
+def test_local_affine_agreement(oracle):
+    """The hybrid gate's restatement against the reference's _local_affine_agreement (tests/golden/hybrid.npz): the
+    plane with a hole at every radius, shift, support and tolerance of the golden cases, and the noisy field with a
+    displacement step at radius 6.5 (rounded to 6, ties to even): ok and n exactly."""
+    g = golden("hybrid")
+    ux, uy, sup = g["laa_plane_ux"], g["laa_plane_uy"], g["laa_plane_support"].astype(bool)
+    for c, (dx, radius, ms, tol) in enumerate(g["laa_plane_cases"]):
+        ok, n = oracle.local_affine_agreement(ux, uy, sup, g["laa_plane_px"] + dx, g["laa_plane_py"], radius, ms, tol)
+        np.testing.assert_array_equal(ok, g[f"laa_plane_ok{c}"].astype(bool), err_msg=f"case {c}")
+        np.testing.assert_array_equal(n, g[f"laa_plane_n{c}"], err_msg=f"case {c}")
+    sup = g["laa_step_support"].astype(bool)
+    ok, n = oracle.local_affine_agreement(np.where(sup, g["laa_step_ux"], np.nan), np.where(sup, g["laa_step_uy"], np.nan),
+                                          sup, g["laa_step_tx"], g["laa_step_ty"], 6.5, 20, 0.5)
+    np.testing.assert_array_equal(ok, g["laa_step_ok"].astype(bool))
+    np.testing.assert_array_equal(n, g["laa_step_n"])
