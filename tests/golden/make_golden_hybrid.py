@@ -11,6 +11,10 @@
    pattern under a growing uniform strain whose 28 x 30 px patch fades into a second pattern (the direct legs from
    frame 0 lose it, the adjacent legs keep it), an ROI; one run with the reference kept at frame 0, one with
    ref_update_conf 0.9 (the reference moves). Frames are rounded to float32 first (what the C ABI takes).
+4. The reference's committed hybrid fixtures (rust/crates/optflow-core/tests/fixtures/hyb_frames.npy, hybA_*.npy,
+   hybB_*.npy and meta.json's "hybrid" records, made by its python/bench/make_parity_fixtures.py:436-460 and checked
+   by its parity_track.rs:531-638), copied as they are: eight 112 x 112 frames of a translation with a foreign block,
+   tracked with ref_update_conf 0.8 and fb_max 10 (A) or 2 (B).
 
 Run in a checkout that has the reference: ``python tests/golden/make_golden_hybrid.py [/path/to/reference]``
 (default /root/reference).
@@ -125,11 +129,26 @@ def real_frames(out):
         print(f"real run {tag}: {time.time() - t:.1f} s")
 
 
+def ref_fixtures(out):
+    import json
+    fx = os.path.join(REF, "rust", "crates", "optflow-core", "tests", "fixtures")
+    load = lambda n: np.load(os.path.join(fx, n + ".npy"))
+    out["f_frames"] = np.float32(load("hyb_frames"))
+    out["f_A_ux"], out["f_A_conf"], out["f_B_ux"] = (np.float32(load(n)) for n in ("hybA_ux", "hybA_conf", "hybB_ux"))
+    out["f_A_fb"], out["f_B_fb"] = (load(n).astype(np.int16) for n in ("hybA_fb", "hybB_fb"))
+    with open(os.path.join(fx, "meta.json")) as fh:
+        meta = json.load(fh)["hybrid"]
+    for name in ("A", "B"):
+        out[f"f_{name}_timing"] = np.array([[t[q] for q in ("reference", "mean_conf", "n_fb_max", "fallback_frac",
+                                                             "fb_gate_rejected", "reacquired")] for t in meta[name]])
+
+
 def main():
     out = {}
     laa_cases(out)
     scripted(out)
     real_frames(out)
+    ref_fixtures(out)
     np.savez_compressed(os.path.join(HERE, "hybrid.npz"), **out)
     print("hybrid.npz written")
 

@@ -135,6 +135,31 @@ def test_real_frames_golden(g, tag):
     assert seen == len(fr) - 1
 
 
+@pytest.mark.parametrize("name,fb_max", [("A", 10), ("B", 2)])
+def test_reference_fixtures(g, name, fb_max):
+    """The reference's committed hybrid fixtures (a translation with a foreign block; the reference moves, pixels are
+    carried, the gate rejects some, the direct leg re-acquires others) with the bars of its own Rust parity test
+    (rust/crates/optflow-core/tests/parity_track.rs:550-629): reference and n_fb_max exactly, mean confidence within
+    1e-4, the shares within 2e-3, fb equal on 99.9 % of the pixels, NaN agreement 99.5 %, rms ux and (A) conf
+    below 1e-3."""
+    fr = list(g["f_frames"])
+    out = list(track_sequence(fr, Config(seq_mode="hybrid", ref_update_conf=0.8, fb_max=fb_max)))
+    assert len(out) == len(fr) - 1
+    for (k, r), t in zip(out, g[f"f_{name}_timing"]):
+        t = dict(zip(TIMING, t))
+        wx = g[f"f_{name}_ux"][k - 1]
+        assert r.timing["reference"] == int(t["reference"]), (name, k)
+        assert r.timing["n_fb_max"] == int(t["n_fb_max"]), (name, k)
+        assert abs(r.timing["mean_conf"] - t["mean_conf"]) < 1e-4, (name, k)
+        for q in ("fallback_frac", "fb_gate_rejected", "reacquired"):
+            assert abs(r.timing[q] - t[q]) < 2e-3, (name, k, q, r.timing[q], t[q])
+        assert (r.fb == g[f"f_{name}_fb"][k - 1]).mean() >= 0.999, (name, k)
+        assert (np.isfinite(r.ux) == np.isfinite(wx)).mean() >= 0.995, (name, k)
+        assert rms(r.ux, wx, np.isfinite(r.ux) & np.isfinite(wx)) < 1e-3, (name, k)
+        if name == "A":
+            assert rms(r.conf, g["f_A_conf"][k - 1]) < 1e-3, (name, k)
+
+
 def test_all_good_hybrid_equals_chain():
     """Where every pixel stays direct-good (fb == 0), the hybrid output is the chain's bit for bit (the reference's
     test_all_good_real_images_hybrid_is_bit_identical_to_chain, python/tests/test_hybrid.py:84-95)."""
