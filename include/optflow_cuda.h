@@ -218,6 +218,57 @@ OFC_API int ofc_track_sequence_hybrid(ofc_engine* eng, const float* const* frame
                               const ofc_hybrid* hy, ofc_pair_out* outs, int32_t* fb, ofc_hybrid_frame* info,
                               ofc_leg_fn leg, void* leg_user, char* err, size_t errlen);
 
+/* Pixel formats of frames handed to the engine (rows packed, channels interleaved): the grey levels of
+ * io.py:15-29 (to_gray) and io.rs:150-256 (gray_from), the rgb24 frames ffmpeg delivers for a video
+ * (video.rs:290-300, rgb_to_gray). */
+#define OFC_PIX_F32 0    /* grey float32, taken as it is */
+#define OFC_PIX_GRAY8 1  /* v / 255 */
+#define OFC_PIX_GRAY16 2 /* v / 65535 */
+#define OFC_PIX_RGB24 3  /* 0.299 R + 0.587 G + 0.114 B of v / 255, left to right */
+#define OFC_PIX_RGBA32 4 /* the same, alpha ignored */
+#define OFC_PIX_RGB48 5  /* the same of v / 65535 */
+
+/*
+ * to_gray + downscale + into_f32 (io.rs:44-52,258-281; io.py:15-51): the grey levels of a w x h image of `pixel`,
+ * box-averaged over scale x scale blocks (scale >= 1, the remainder cropped; the block's rows summed left to right,
+ * the row sums in order, / scale^2), in float64, rounded to float32. out: (w / scale) x (h / scale) values.
+ */
+OFC_API int ofc_to_gray(ofc_engine* eng, const void* px, int32_t pixel, size_t w, size_t h, int32_t scale,
+                float* out, char* err, size_t errlen);
+
+/* A frame source: writes frame k (w_in x h_in pixels of the stream's pixel format) to dst, page-locked memory
+ * of the engine, and returns 0; 1 when the sequence has no frame k; any other value stops the run with
+ * OFC_ERR_ARG. It is called for frame k + 1 while the GPU tracks frame k. */
+typedef int (*ofc_source_fn)(void* user, int64_t k, void* dst);
+/* A result sink: frame k's outputs (host views into page-locked memory, valid during the call; fb NULL in chain
+ * mode; info's hybrid shares 0 in chain mode), called while the GPU tracks frame k + 1. Non-zero stops the run
+ * with OFC_ERR_ARG. */
+typedef int (*ofc_sink_fn)(void* user, int64_t k, const ofc_pair_out* out, const int32_t* fb,
+                           const ofc_hybrid_frame* info);
+
+typedef struct ofc_stream {
+    int32_t pixel;          /* OFC_PIX_* of the source's frames */
+    size_t w_in, h_in;      /* their size; the tracked frames are (w_in / scale) x (h_in / scale) */
+    int32_t scale;          /* box downscale factor >= 1 (the CLI's --scale) */
+    int32_t hybrid;         /* 0: seq_mode "chain", 1: "hybrid" */
+    ofc_hybrid hy;          /* the hybrid keys (hybrid only) */
+    double ref_update_conf;
+    ofc_source_fn source;
+    void* source_user;
+    ofc_sink_fn sink;
+    void* sink_user;
+} ofc_stream;
+
+/*
+ * track::track_sequence over a frame source (the CLI's `optflow seq`, run.rs / track.rs:1276-1287): frames are
+ * pulled one ahead into page-locked buffers while the GPU works, converted to grey and downscaled on the GPU
+ * (ofc_to_gray), tracked in chain or hybrid mode (ofc_track_sequence, ofc_track_sequence_hybrid), and each
+ * frame's results go to the sink while the next frame is tracked (device staging, then a copy stream). roi
+ * (nullable): on the tracked grid. *n_out (nullable): the frames delivered to the sink.
+ */
+OFC_API int ofc_track_stream(ofc_engine* eng, const ofc_stream* s, const uint8_t* roi, const ofc_config* cfg,
+                     int64_t* n_out, char* err, size_t errlen);
+
 /*
  * _local_affine_agreement (python/optflow_ref/track.py:331-382; rust/crates/optflow-core/src/track/hybrid.rs:
  * 146-250): per pixel an affine model u(q) = a + B (q - p), ridge 1e-3 r^2 on B, fitted to (ux, uy) of the support

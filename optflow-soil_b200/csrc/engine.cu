@@ -9,6 +9,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -204,6 +205,15 @@ struct DevBuf {
   }
 };
 
+// page-locked host memory (the staging buffers of streamed frames and results)
+struct HostBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~HostBuf() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
 struct Lane {
   cudaStream_t stream = nullptr;
   std::mutex busy;
@@ -218,10 +228,12 @@ struct Lane {
   // the copy stream of batched calls and its ordering events (created on first use)
   cudaStream_t copy = nullptr;
   cudaEvent_t bev[8] = {};
+  cudaEvent_t sev[2] = {};  // timing events of a sequence frame's finish (the pair's ev[] time its legs)
   void ensure_copy_stream() {
     if (copy) return;
     OFC_CUDA(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
     for (auto& e : bev) OFC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& e : sev) OFC_CUDA(cudaEventCreate(&e));
   }
 
   template <class T>
@@ -239,6 +251,25 @@ struct Lane {
       b->p = nullptr;
       b->bytes = 0;
       OFC_CUDA(cudaMalloc(&b->p, bytes));
+      b->bytes = bytes;
+    }
+    return (T*)b->p;
+  }
+  std::unordered_map<std::string, std::unique_ptr<HostBuf>> hpool;
+  template <class T>
+  T* pinned(const std::string& name, size_t count) {
+    size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+    auto& b = hpool[name];
+    if (!b) b.reset(new HostBuf());
+    if (b->bytes < bytes) {
+      if (b->p) {
+        OFC_CUDA(cudaStreamSynchronize(stream));
+        if (copy) OFC_CUDA(cudaStreamSynchronize(copy));
+        OFC_CUDA(cudaFreeHost(b->p));
+      }
+      b->p = nullptr;
+      b->bytes = 0;
+      OFC_CUDA(cudaHostAlloc(&b->p, bytes, cudaHostAllocDefault));
       b->bytes = bytes;
     }
     return (T*)b->p;
@@ -303,6 +334,7 @@ struct Lane {
     graphs.clear();
     consts.clear();
     pool.clear();
+    hpool.clear();
     plans.clear();
   }
 };
@@ -1358,6 +1390,43 @@ __global__ void k_laa_solve(const double* __restrict__ rows, int W, int H, int r
   }
 }
 
+// ---------------------------------------------------------------- frame front-end (to_gray + downscale)
+// io.rs:44-52 (luminance, lut8), io.rs:258-281 (downscale), video.rs:290-300 (rgb_to_gray); every product and sum
+// rounded on its own (no contraction), as the CLI evaluates them
+
+__device__ __forceinline__ double luminance64(double r, double g, double b) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(0.299, r), __dmul_rn(0.587, g)), __dmul_rn(0.114, b));
+}
+
+template <int PIX>
+__device__ __forceinline__ double grey_at(const uint8_t* __restrict__ px, size_t i, const double* __restrict__ lut8) {
+  if (PIX == OFC_PIX_F32) return (double)reinterpret_cast<const float*>(px)[i];
+  if (PIX == OFC_PIX_GRAY8) return lut8[px[i]];
+  if (PIX == OFC_PIX_GRAY16) return __ddiv_rn((double)reinterpret_cast<const uint16_t*>(px)[i], 65535.0);
+  if (PIX == OFC_PIX_RGB24) return luminance64(lut8[px[3 * i]], lut8[px[3 * i + 1]], lut8[px[3 * i + 2]]);
+  if (PIX == OFC_PIX_RGBA32) return luminance64(lut8[px[4 * i]], lut8[px[4 * i + 1]], lut8[px[4 * i + 2]]);
+  const uint16_t* q = reinterpret_cast<const uint16_t*>(px) + 3 * i;  // OFC_PIX_RGB48
+  return luminance64(__ddiv_rn((double)q[0], 65535.0), __ddiv_rn((double)q[1], 65535.0),
+                     __ddiv_rn((double)q[2], 65535.0));
+}
+
+// one output pixel per thread: the scale x scale block's rows summed left to right, the row sums in order,
+// / scale^2, rounded to float32 (scale 1: the grey level itself)
+template <int PIX>
+__global__ void k_to_gray(const uint8_t* __restrict__ px, int w_in, int scale, int W, int H,
+                          const double* __restrict__ lut8, float* __restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= W) return;
+  double sum = 0.0;
+  for (int dy = 0; dy < scale; dy++) {
+    const size_t row = (size_t)(y * scale + dy) * w_in + (size_t)x * scale;
+    double rs = 0.0;
+    for (int dx = 0; dx < scale; dx++) rs = __dadd_rn(rs, grey_at<PIX>(px, row + dx, lut8));
+    sum = __dadd_rn(sum, rs);
+  }
+  out[(size_t)y * W + x] = (float)__ddiv_rn(sum, (double)scale * (double)scale);
+}
+
 // low = conf < conf_min (track.py:66) for ofc_finish
 __global__ void k_threshold_low(const double* c64, double cm, uint8_t* low, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -1380,6 +1449,45 @@ void hybrid_check(const ofc_hybrid* hy) {
   if (!std::isfinite(hy->fb_radius) || !std::isfinite(hy->fb_tol) || hy->fb_tol <= 0 || hy->fb_radius == 0)
     throw Error(OFC_ERR_ARG, "fb_radius must be finite and nonzero (negative: 4 sigma_w), fb_tol finite and positive");
   if (hy->fb_min_support < 0) throw Error(OFC_ERR_ARG, "fb_min_support must be >= 0 and tavg in [0, 64]");
+}
+
+// bytes per pixel of an OFC_PIX_* format; 0 for an unknown one
+size_t pixel_bytes(int32_t pixel) {
+  switch (pixel) {
+    case OFC_PIX_F32: return 4;
+    case OFC_PIX_GRAY8: return 1;
+    case OFC_PIX_GRAY16: return 2;
+    case OFC_PIX_RGB24: return 3;
+    case OFC_PIX_RGBA32: return 4;
+    case OFC_PIX_RGB48: return 6;
+    default: return 0;
+  }
+}
+
+// to_gray + downscale of a device image of w_in x (H * scale) or more rows into the W x H float32 plane out
+void to_gray_dev(Lane& L, const uint8_t* px, int32_t pixel, int w_in, int scale, int W, int H, float* out) {
+  static double lut[256];
+  for (int v = 0; v < 256; v++) lut[v] = v / 255.0;  // lut8 (io.rs:50-52)
+  const double* lut8 = L.cached("lut8", lut, 256);
+  const dim3 g(div_up(W, 128), H);
+  cudaStream_t st = L.stream;
+  switch (pixel) {
+    case OFC_PIX_F32: OFC_LAUNCH(k_to_gray<OFC_PIX_F32>, g, 128, 0, st, px, w_in, scale, W, H, lut8, out); break;
+    case OFC_PIX_GRAY8: OFC_LAUNCH(k_to_gray<OFC_PIX_GRAY8>, g, 128, 0, st, px, w_in, scale, W, H, lut8, out); break;
+    case OFC_PIX_GRAY16: OFC_LAUNCH(k_to_gray<OFC_PIX_GRAY16>, g, 128, 0, st, px, w_in, scale, W, H, lut8, out); break;
+    case OFC_PIX_RGB24: OFC_LAUNCH(k_to_gray<OFC_PIX_RGB24>, g, 128, 0, st, px, w_in, scale, W, H, lut8, out); break;
+    case OFC_PIX_RGBA32: OFC_LAUNCH(k_to_gray<OFC_PIX_RGBA32>, g, 128, 0, st, px, w_in, scale, W, H, lut8, out); break;
+    case OFC_PIX_RGB48: OFC_LAUNCH(k_to_gray<OFC_PIX_RGB48>, g, 128, 0, st, px, w_in, scale, W, H, lut8, out); break;
+    default: throw Error(OFC_ERR_ARG, "unknown pixel format " + std::to_string(pixel));
+  }
+}
+
+// the checks of a frame format: a known pixel, scale >= 1 (io.rs:260), a tracked size of at least one pixel
+void check_format(int32_t pixel, size_t w, size_t h, int32_t scale) {
+  if (pixel_bytes(pixel) == 0) throw Error(OFC_ERR_ARG, "unknown pixel format " + std::to_string(pixel));
+  if (scale < 1) throw Error(OFC_ERR_ARG, "scale must be >= 1, got " + std::to_string(scale));
+  check_sizes(w, h);
+  check_sizes(w / scale, h / scale);
 }
 
 // _local_affine_agreement on device planes (track.py:331-382): two passes of row sums and column sums + solve; the
@@ -1544,6 +1652,7 @@ void ofc_destroy(ofc_engine* e) {
     cudaStreamDestroy(l->side);
     if (l->copy) {
       for (auto& ev : l->bev) cudaEventDestroy(ev);
+      for (auto& ev : l->sev) cudaEventDestroy(ev);
       cudaStreamDestroy(l->copy);
     }
     cudaStreamDestroy(l->stream);
@@ -1905,282 +2014,276 @@ int ofc_track_pair(ofc_engine* e, const float* i1, const float* i2, size_t w, si
   });
 }
 
-int ofc_track_sequence(ofc_engine* e, const float* const* frames, size_t n, size_t w, size_t h, const uint8_t* roi,
-                       const ofc_config* c, double ref_update_conf, ofc_pair_out* outs, int32_t* reference,
-                       double* mean_conf, char* err, size_t errlen) {
-  return guarded(e, err, errlen, [&](Lane& L) {
-    cfg_check(c);
-    if (!frames || n == 0) throw Error(OFC_ERR_ARG, "no frames");
-    check_sizes(w, h);
-    for (size_t k = 0; k < n; k++)
-      if (!frames[k]) throw Error(OFC_ERR_ARG, "null frame " + std::to_string(k));
-    if (n > 1 && !outs) throw Error(OFC_ERR_ARG, "null outputs");
-    if (!std::isfinite(ref_update_conf)) throw Error(OFC_ERR_ARG, "ref_update_conf must be a finite number");
-    const size_t N = w * h;
-    if (roi) {
-      bool any = false;
-      for (size_t i = 0; i < N && !any; i++) any = roi[i] != 0;
-      if (!any) throw Error(OFC_ERR_ARG, "ROI mask is empty");
-    }
-    if (n == 1) return;
-    if ((int)std::min(w, h) < c->poc_win)
-      throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
-    check_fine_window(w, h, *c);
-    const int W = (int)w, H = (int)h;
-    cudaStream_t st = L.stream;
-    const dim3 g2(div_up(W, 128), H);
-    // the run's state on the device (track.rs:1030-1043)
-    float* ref = L.get<float>("seq_ref", N);
-    float* prev = L.get<float>("seq_prev", N);
-    float* fk = L.get<float>("seq_fk", N);
-    float* u0r = L.get<float>("seq_u0r", 2 * N);
-    float* u0n = L.get<float>("seq_u0n", 2 * N);
-    double* c0r = L.get<double>("seq_c0r", N);
-    double* conf0 = L.get<double>("seq_conf0", N);
-    float* praw = L.get<float>("seq_praw", 2 * N);
-    float* pconf = L.get<float>("seq_pconf", N);
-    float* cxy = L.get<float>("seq_cxy", 2 * N);
-    double* c64 = L.get<double>("seq_c64", 2 * N);
-    float* rep = L.get<float>("seq_rep", N);
-    double* rsum = L.get<double>("seq_rsum", (size_t)H);
-    long long* rcnt = L.get<long long>("seq_rcnt", (size_t)H);
-    double* dmean = L.get<double>("seq_mean", 1);
-    uint8_t* low = L.get<uint8_t>("seq_low", N);
-    const uint8_t* droi = roi ? L.upload("seq_roi", roi, N) : nullptr;
-    float* in1 = L.get<float>("in_i1", N);
-    float* in2 = L.get<float>("in_i2", N);
-    float* inu = L.get<float>("in_u", N);
-    float* inv = L.get<float>("in_v", N);
-    const ofc_pair_out d = device_pair_out(L, N);  // the leg's conf, raw_ux, raw_uy (planes 2, 8, 9)
-    const double B = guard_px(*c) > 0 ? 4.0 * c->sigma_w : 0.0;
-    OFC_CUDA(cudaMemcpyAsync(ref, frames[0], N * 4, cudaMemcpyHostToDevice, st));
-    OFC_CUDA(cudaMemcpyAsync(prev, ref, N * 4, cudaMemcpyDeviceToDevice, st));
-    OFC_CUDA(cudaMemsetAsync(u0r, 0, 2 * N * 4, st));
-    launch_fill_f64(c0r, 1.0, N, st);
-    bool have_prev = false;
-    int ref_idx = 0;
-    double t_coarse = 0, t_fine = 0;
-    // one leg reference -> frame k (pair_flow_on, track.rs:558-623): the coarse and fine stages on the lane's pair
-    // buffers, with the previous leg's raw field as the dense start when given
-    auto leg = [&](bool with_init) {
-      OFC_CUDA(cudaMemcpyAsync(in1, ref, N * 4, cudaMemcpyDeviceToDevice, st));
-      OFC_CUDA(cudaMemcpyAsync(in2, fk, N * 4, cudaMemcpyDeviceToDevice, st));
-      if (with_init) {
-        OFC_CUDA(cudaMemcpyAsync(inu, praw, N * 4, cudaMemcpyDeviceToDevice, st));
-        OFC_CUDA(cudaMemcpyAsync(inv, praw + N, N * 4, cudaMemcpyDeviceToDevice, st));
-      }
-      run_pair(L, W, H, false, with_init, *c, true, 2);
-      float ms0 = 0, ms1 = 0;
-      OFC_CUDA(cudaEventSynchronize(L.ev[3]));
-      OFC_CUDA(cudaEventElapsedTime(&ms0, L.ev[0], L.ev[1]));
-      OFC_CUDA(cudaEventElapsedTime(&ms1, L.ev[1], L.ev[3]));
-      t_coarse = ms0 * 1e-3;
-      t_fine = ms1 * 1e-3;
-    };
-    auto leg_mean = [&]() {
-      OFC_LAUNCH(k_reportable, g2, 128, 0, st, d.raw_ux, d.raw_uy, W, H, B, rep);
-      OFC_LAUNCH(k_mean_conf_rows, div_up(H, 128), 128, 0, st, d.conf, rep, u0r, u0r + N, droi, W, H, rsum, rcnt);
-      OFC_LAUNCH(k_mean_conf_fold, 1, 1, 0, st, rsum, rcnt, H, dmean);
-      double m = 0;
-      OFC_CUDA(cudaMemcpyAsync(&m, dmean, 8, cudaMemcpyDeviceToHost, st));
-      OFC_CUDA(cudaStreamSynchronize(st));
-      return m;
-    };
-    for (size_t k = 1; k < n; k++) {
-      OFC_CUDA(cudaMemcpyAsync(fk, frames[k], N * 4, cudaMemcpyHostToDevice, st));
-      leg(have_prev);
-      double cmean = leg_mean();
-      if (cmean < ref_update_conf && ref_idx != (int)k - 1) {
-        // the reference moves to frame k - 1: the previous leg extends the link of frame 0 (track.rs:1135-1155)
-        OFC_LAUNCH(k_link_conf, g2, 128, 0, st, c0r, pconf, u0r, u0r + N, W, H, c0r);
-        OFC_LAUNCH(k_compose, g2, 128, 0, st, u0r, u0r + N, praw, praw + N, W, H, u0n, u0n + N);
-        OFC_CUDA(cudaMemcpyAsync(u0r, u0n, 2 * N * 4, cudaMemcpyDeviceToDevice, st));
-        OFC_CUDA(cudaMemcpyAsync(ref, prev, N * 4, cudaMemcpyDeviceToDevice, st));
-        ref_idx = (int)k - 1;
-        leg(false);
-        cmean = leg_mean();
-      }
-      // frame 0 -> k and its link confidence, then the finish on the frame-0 grid (track.rs:1157-1200)
-      OFC_LAUNCH(k_compose, g2, 128, 0, st, u0r, u0r + N, d.raw_ux, d.raw_uy, W, H, cxy, cxy + N);
-      OFC_LAUNCH(k_link_conf, g2, 128, 0, st, c0r, d.conf, u0r, u0r + N, W, H, conf0);
-      OFC_CUDA(cudaMemcpyAsync(praw, d.raw_ux, N * 4, cudaMemcpyDeviceToDevice, st));
-      OFC_CUDA(cudaMemcpyAsync(praw + N, d.raw_uy, N * 4, cudaMemcpyDeviceToDevice, st));
-      OFC_CUDA(cudaMemcpyAsync(pconf, d.conf, N * 4, cudaMemcpyDeviceToDevice, st));
-      launch_f32_to_f64(cxy, c64, 2 * N, st);
-      ofc_threshold_low(conf0, c->conf_min, low, N, st);
-      OFC_CUDA(cudaEventRecord(L.ev[0], st));
-      finish_dev(L, low, droi, c64, c64 + N, conf0, W, H, *c, d, false);
-      OFC_CUDA(cudaEventRecord(L.ev[1], st));
-      download_pair(L, d, &outs[k - 1], N);
-      OFC_CUDA(cudaMemcpyAsync(prev, fk, N * 4, cudaMemcpyDeviceToDevice, st));
-      OFC_CUDA(cudaStreamSynchronize(st));
-      float ms = 0;
-      OFC_CUDA(cudaEventElapsedTime(&ms, L.ev[0], L.ev[1]));
-      outs[k - 1].timing[0] = t_coarse;
-      outs[k - 1].timing[1] = t_fine;
-      outs[k - 1].timing[2] = ms * 1e-3;
-      if (reference) reference[k - 1] = ref_idx;
-      if (mean_conf) mean_conf[k - 1] = cmean;
-      have_prev = true;
-    }
-  });
-}
+}  // extern "C"
 
-int ofc_track_sequence_hybrid(ofc_engine* e, const float* const* frames, size_t n, size_t w, size_t h,
-                              const uint8_t* roi, const ofc_config* c, const double* ruc, const ofc_hybrid* hy,
-                              ofc_pair_out* outs, int32_t* fb, ofc_hybrid_frame* info, ofc_leg_fn legfn,
-                              void* leg_user, char* err, size_t errlen) {
-  return guarded(e, err, errlen, [&](Lane& L) {
-    cfg_check(c);
-    hybrid_check(hy);
-    if (!frames || n == 0) throw Error(OFC_ERR_ARG, "no frames");
-    check_sizes(w, h);
-    for (size_t k = 0; k < n; k++)
-      if (!frames[k]) throw Error(OFC_ERR_ARG, "null frame " + std::to_string(k));
-    if (n > 1 && !outs) throw Error(OFC_ERR_ARG, "null outputs");
-    if (n > 1 && !ruc) throw Error(OFC_ERR_ARG, "null ref_update_conf");
-    for (size_t k = 0; k + 1 < n; k++)
-      if (!std::isfinite(ruc[k])) throw Error(OFC_ERR_ARG, "ref_update_conf must be a finite number");
-    const size_t N = w * h;
-    size_t n_roi = N;
-    if (roi) {
-      n_roi = 0;
-      for (size_t i = 0; i < N; i++) n_roi += roi[i] != 0;
-      if (n_roi == 0) throw Error(OFC_ERR_ARG, "ROI mask is empty");
+namespace {
+
+// ---------------------------------------------------------------- sequences: one driver for chain and hybrid
+// track.py:260-315 (chain) and 385-503 (hybrid); rust/crates/optflow-core/src/track.rs:1030-1245, track/hybrid.rs.
+// Frames come from `frame` (the caller's arrays, or a source filling page-locked slots one frame ahead while the
+// GPU works), go through ofc_to_gray's conversion when they are not float32 grey at full size, and each frame's
+// results go to `emit` from page-locked staging while the GPU tracks the next frame.
+struct SeqIO {
+  int W = 0, H = 0;           // the tracked grid
+  const uint8_t* roi = nullptr;  // host, W x H, nullable
+  const ofc_config* c = nullptr;
+  bool hybrid = false;
+  ofc_hybrid hy{};
+  int32_t pixel = OFC_PIX_F32;
+  int w_in = 0, h_in = 0, scale = 1;
+  // frame k's bytes: a host pointer (pageable or `slot`), or nullptr when the sequence has no frame k
+  std::function<const void*(int64_t k, void* slot)> frame;
+  std::function<double(int64_t k)> ruc;  // ref_update_conf at frame k
+  std::function<void(int64_t k, const ofc_pair_out& out, const int32_t* fb, const ofc_hybrid_frame& info)> emit;
+  ofc_leg_fn leg = nullptr;
+  void* leg_user = nullptr;
+};
+
+int64_t run_sequence(Lane& L, const SeqIO& io) {
+  const ofc_config& c = *io.c;
+  const int W = io.W, H = io.H;
+  const size_t N = (size_t)W * H;
+  cudaStream_t st = L.stream;
+  L.ensure_copy_stream();
+  const dim3 g2(div_up(W, 128), H);
+  const unsigned gN = std::min<unsigned>(div_up(N, 256), 148 * 8);
+  const double cm = c.conf_min, radius = io.hy.fb_radius > 0 ? io.hy.fb_radius : 4.0 * c.sigma_w;
+  const bool gate_on = io.hybrid && io.hy.fb_min_support > 0;
+  size_t n_roi = N;
+  if (io.roi) {
+    n_roi = 0;
+    for (size_t i = 0; i < N; i++) n_roi += io.roi[i] != 0;
+  }
+  // the run's state (track.py:423-431)
+  float* ref = L.get<float>("seq_ref", N);
+  float* prev = L.get<float>("seq_prev", N);
+  float* fk = L.get<float>("seq_fk", N);
+  float* u0r = L.get<float>("seq_u0r", 2 * N);
+  float* u0n = L.get<float>("seq_u0n", 2 * N);
+  double* c0r = L.get<double>("seq_c0r", N);
+  float* praw = L.get<float>("seq_praw", 2 * N);  // the last final direct leg: its raw field and conf
+  float* pconf = L.get<float>("seq_pconf", N);
+  float* cxy = L.get<float>("hy_cxy", 2 * N);
+  double* conf64 = L.get<double>("hy_conf", N);
+  double* u64 = L.get<double>("hy_u64", 2 * N);
+  float* rep = L.get<float>("seq_rep", N);
+  double* rsum = L.get<double>("seq_rsum", (size_t)H);
+  long long* rcnt = L.get<long long>("seq_rcnt", (size_t)H);
+  double* dmean = L.get<double>("seq_mean", 1);
+  uint8_t* low = L.get<uint8_t>("seq_low", N);
+  uint8_t *anch = nullptr, *goodp = nullptr, *support = nullptr, *gate0 = nullptr, *gate = nullptr;
+  int *nfb = nullptr, *dany = nullptr;
+  float *uprev = nullptr, *padj = nullptr, *axy = nullptr;
+  double *legc = nullptr, *link = nullptr, *ca = nullptr;
+  uint16_t* fl = nullptr;
+  unsigned long long* dcnt = nullptr;
+  if (io.hybrid) {
+    anch = L.get<uint8_t>("hy_anch", N);
+    goodp = L.get<uint8_t>("hy_goodp", N);
+    nfb = L.get<int>("hy_nfb", N);
+    uprev = L.get<float>("hy_uprev", 2 * N);
+    padj = L.get<float>("hy_padj", 2 * N);
+    axy = L.get<float>("hy_axy", 2 * N);
+    legc = L.get<double>("hy_legc", N);
+    link = L.get<double>("hy_link", N);
+    ca = L.get<double>("hy_ca", N);
+    fl = L.get<uint16_t>("hy_flags", N);
+    support = L.get<uint8_t>("hy_support", N);
+    gate0 = L.get<uint8_t>("hy_gate0", N);
+    gate = L.get<uint8_t>("hy_gate", N);
+    dany = L.get<int>("hy_any", 4);
+    dcnt = L.get<unsigned long long>("hy_cnt", 4);
+  }
+  const uint8_t* droi = io.roi ? L.upload("seq_roi", io.roi, N) : nullptr;
+  float* in1 = L.get<float>("in_i1", N);
+  float* in2 = L.get<float>("in_i2", N);
+  float* inu = L.get<float>("in_u", N);
+  float* inv = L.get<float>("in_v", N);
+  const ofc_pair_out d = device_pair_out(L, N);  // a leg's conf, raw_ux, raw_uy; the frame's outputs
+  const double B = guard_px(c) > 0 ? 4.0 * c.sigma_w : 0.0;
+  // frame input: two page-locked slots (a source fills one while the other's upload may be in flight), the raw
+  // frame on the device when it needs the conversion
+  const bool direct = io.pixel == OFC_PIX_F32 && io.scale == 1;
+  const size_t in_bytes = pixel_bytes(io.pixel) * (size_t)io.w_in * io.h_in;
+  void* slot[2] = {L.pinned<uint8_t>("seq_slot0", in_bytes), L.pinned<uint8_t>("seq_slot1", in_bytes)};
+  cudaEvent_t slot_free[2] = {L.bev[2], L.bev[3]};
+  bool slot_used[2] = {false, false};
+  uint8_t* rawin = direct ? nullptr : L.get<uint8_t>("seq_rawin", in_bytes);
+  auto load = [&](const void* p, int s, float* dst) {
+    if (direct) {
+      OFC_CUDA(cudaMemcpyAsync(dst, p, N * 4, cudaMemcpyHostToDevice, st));
+    } else {
+      OFC_CUDA(cudaMemcpyAsync(rawin, p, in_bytes, cudaMemcpyHostToDevice, st));
+      to_gray_dev(L, rawin, io.pixel, io.w_in, io.scale, W, H, dst);
     }
-    if (n == 1) return;
-    if ((int)std::min(w, h) < c->poc_win)
-      throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
-    if (!legfn) check_fine_window(w, h, *c);
-    const int W = (int)w, H = (int)h;
-    cudaStream_t st = L.stream;
-    const dim3 g2(div_up(W, 128), H);
-    const unsigned gN = std::min<unsigned>(div_up(N, 256), 148 * 8);
-    const double cm = c->conf_min, radius = hy->fb_radius > 0 ? hy->fb_radius : 4.0 * c->sigma_w;
-    const bool gate_on = hy->fb_min_support > 0;
-    // the chain's state (track.py:423-427) and the hybrid's (track.py:428-431)
-    float* ref = L.get<float>("seq_ref", N);
-    float* prev = L.get<float>("seq_prev", N);
-    float* fk = L.get<float>("seq_fk", N);
-    float* u0r = L.get<float>("seq_u0r", 2 * N);
-    double* c0r = L.get<double>("seq_c0r", N);
-    float* praw = L.get<float>("seq_praw", 2 * N);  // the direct leg of the last frame: its raw field and conf
-    float* pconf = L.get<float>("seq_pconf", N);
-    float* rep = L.get<float>("seq_rep", N);
-    double* rsum = L.get<double>("seq_rsum", (size_t)H);
-    long long* rcnt = L.get<long long>("seq_rcnt", (size_t)H);
-    double* dmean = L.get<double>("seq_mean", 1);
-    uint8_t* low = L.get<uint8_t>("seq_low", N);
-    uint8_t* anch = L.get<uint8_t>("hy_anch", N);
-    uint8_t* goodp = L.get<uint8_t>("hy_goodp", N);
-    int* nfb = L.get<int>("hy_nfb", N);
-    float* uprev = L.get<float>("hy_uprev", 2 * N);
-    float* padj = L.get<float>("hy_padj", 2 * N);
-    float* cxy = L.get<float>("hy_cxy", 2 * N);
-    float* axy = L.get<float>("hy_axy", 2 * N);
-    double* legc = L.get<double>("hy_legc", N);
-    double* link = L.get<double>("hy_link", N);
-    double* ca = L.get<double>("hy_ca", N);
-    double* conf64 = L.get<double>("hy_conf", N);
-    double* u64 = L.get<double>("hy_u64", 2 * N);
-    uint16_t* fl = L.get<uint16_t>("hy_flags", N);
-    uint8_t* support = L.get<uint8_t>("hy_support", N);
-    uint8_t* gate0 = L.get<uint8_t>("hy_gate0", N);
-    uint8_t* gate = L.get<uint8_t>("hy_gate", N);
-    int* dany = L.get<int>("hy_any", 4);
-    unsigned long long* dcnt = L.get<unsigned long long>("hy_cnt", 4);
-    const uint8_t* droi = roi ? L.upload("seq_roi", roi, N) : nullptr;
-    float* in1 = L.get<float>("in_i1", N);
-    float* in2 = L.get<float>("in_i2", N);
-    float* inu = L.get<float>("in_u", N);
-    float* inv = L.get<float>("in_v", N);
-    const ofc_pair_out d = device_pair_out(L, N);  // a leg's conf, raw_ux, raw_uy; the frame's outputs
-    const double B = guard_px(*c) > 0 ? 4.0 * c->sigma_w : 0.0;
-    OFC_CUDA(cudaMemcpyAsync(ref, frames[0], N * 4, cudaMemcpyHostToDevice, st));
-    OFC_CUDA(cudaMemcpyAsync(prev, ref, N * 4, cudaMemcpyDeviceToDevice, st));
-    OFC_CUDA(cudaMemsetAsync(u0r, 0, 2 * N * 4, st));
-    launch_fill_f64(c0r, 1.0, N, st);
+    if (p == slot[s]) {
+      OFC_CUDA(cudaEventRecord(slot_free[s], st));
+      slot_used[s] = true;
+    }
+  };
+  auto fetch = [&](int64_t k) -> const void* {
+    const int s = (int)(k & 1);
+    if (slot_used[s]) OFC_CUDA(cudaEventSynchronize(slot_free[s]));
+    slot_used[s] = false;
+    return io.frame(k, slot[s]);
+  };
+  // result output: the frame's planes copied on the device into staging (the next frame's legs overwrite them),
+  // then to page-locked memory on the copy stream; emitted during the next frame's first leg
+  float* dstage = L.get<float>("seq_stage", 10 * N);
+  uint8_t* dstage_v = L.get<uint8_t>("seq_stage_v", N);
+  int* dstage_fb = io.hybrid ? L.get<int>("seq_stage_fb", N) : nullptr;
+  float* hout = L.pinned<float>("seq_hout", 10 * N);
+  uint8_t* hvalid = L.pinned<uint8_t>("seq_hvalid", N);
+  int32_t* hfb = io.hybrid ? L.pinned<int32_t>("seq_hfb", N) : nullptr;
+  cudaEvent_t staged = L.bev[0], copied = L.bev[1];
+  bool copy_issued = false;
+  struct Pending {
+    bool active = false;
+    int64_t k = 0;
+    double coarse = 0, fine = 0;
+    ofc_hybrid_frame info{};
+  } pending;
+  const void* next = nullptr;
+  bool fetched = false;
+  int64_t k = 1, emitted = 0;
+  auto flush = [&]() {
+    if (!pending.active) return;
+    OFC_CUDA(cudaEventSynchronize(copied));
+    float ms = 0;
+    OFC_CUDA(cudaEventElapsedTime(&ms, L.sev[0], L.sev[1]));
+    ofc_pair_out o{};
+    float** f[10] = {&o.ux, &o.uy, &o.conf, &o.exx, &o.eyy, &o.exy, &o.gmax, &o.vol, &o.raw_ux, &o.raw_uy};
+    for (int i = 0; i < 10; i++) *f[i] = hout + i * N;
+    o.valid = hvalid;
+    o.timing[0] = pending.coarse;
+    o.timing[1] = pending.fine;
+    o.timing[2] = ms * 1e-3;
+    pending.active = false;
+    io.emit(pending.k, o, hfb, pending.info);
+    emitted++;
+  };
+  // while the GPU runs a frame's first leg: deliver the previous frame's results, fetch the next frame
+  auto service = [&]() {
+    flush();
+    if (!fetched) {
+      next = fetch(k + 1);
+      fetched = true;
+    }
+  };
+  // one leg frames[ia] -> frames[ib] (track.py:200-206) into d's conf / raw planes: the engine's coarse and fine
+  // stages with the dense start `init` (2 planes, nullable), or the caller's leg source; returns coarse, fine (s)
+  std::vector<float> hbuf;
+  auto leg = [&](const float* a, int64_t ia, const float* b, int64_t ib, const float* init,
+                 bool first) -> std::pair<double, double> {
+    if (io.leg) {
+      if (first) service();
+      hbuf.resize(5 * N);
+      float* hi = hbuf.data();
+      float* ho = hi + 2 * N;
+      if (init) OFC_CUDA(cudaMemcpyAsync(hi, init, 2 * N * 4, cudaMemcpyDeviceToHost, st));
+      OFC_CUDA(cudaStreamSynchronize(st));
+      if (io.leg(io.leg_user, (int32_t)ia, (int32_t)ib, init ? hi : nullptr, init ? hi + N : nullptr, ho, ho + N,
+                 ho + 2 * N) != 0)
+        throw Error(OFC_ERR_ARG, "the leg source failed on the leg " + std::to_string(ia) + " -> " + std::to_string(ib));
+      OFC_CUDA(cudaMemcpyAsync(d.raw_ux, ho, N * 4, cudaMemcpyHostToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(d.raw_uy, ho + N, N * 4, cudaMemcpyHostToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(d.conf, ho + 2 * N, N * 4, cudaMemcpyHostToDevice, st));
+      OFC_CUDA(cudaStreamSynchronize(st));
+      return {0.0, 0.0};
+    }
+    OFC_CUDA(cudaMemcpyAsync(in1, a, N * 4, cudaMemcpyDeviceToDevice, st));
+    OFC_CUDA(cudaMemcpyAsync(in2, b, N * 4, cudaMemcpyDeviceToDevice, st));
+    if (init) {
+      OFC_CUDA(cudaMemcpyAsync(inu, init, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(inv, init + N, N * 4, cudaMemcpyDeviceToDevice, st));
+    }
+    run_pair(L, W, H, false, init != nullptr, c, true, 2);
+    if (first) service();
+    float ms0 = 0, ms1 = 0;
+    OFC_CUDA(cudaEventSynchronize(L.ev[3]));
+    OFC_CUDA(cudaEventElapsedTime(&ms0, L.ev[0], L.ev[1]));
+    OFC_CUDA(cudaEventElapsedTime(&ms1, L.ev[1], L.ev[3]));
+    return {ms0 * 1e-3, ms1 * 1e-3};
+  };
+  auto leg_mean = [&]() {
+    OFC_LAUNCH(k_reportable, g2, 128, 0, st, d.raw_ux, d.raw_uy, W, H, B, rep);
+    OFC_LAUNCH(k_mean_conf_rows, div_up(H, 128), 128, 0, st, d.conf, rep, u0r, u0r + N, droi, W, H, rsum, rcnt);
+    OFC_LAUNCH(k_mean_conf_fold, 1, 1, 0, st, rsum, rcnt, H, dmean);
+    double m = 0;
+    OFC_CUDA(cudaMemcpyAsync(&m, dmean, 8, cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaStreamSynchronize(st));
+    return m;
+  };
+  int any[4];
+  auto read_any = [&]() {
+    OFC_CUDA(cudaMemcpyAsync(any, dany, sizeof(any), cudaMemcpyDeviceToHost, st));
+    OFC_CUDA(cudaStreamSynchronize(st));
+  };
+
+  const void* f0 = fetch(0);
+  if (!f0) throw Error(OFC_ERR_ARG, "no frames");
+  load(f0, 0, ref);
+  OFC_CUDA(cudaMemcpyAsync(prev, ref, N * 4, cudaMemcpyDeviceToDevice, st));
+  OFC_CUDA(cudaMemsetAsync(u0r, 0, 2 * N * 4, st));
+  launch_fill_f64(c0r, 1.0, N, st);
+  if (io.hybrid) {
     OFC_CUDA(cudaMemsetAsync(anch, 1, N, st));
     OFC_CUDA(cudaMemsetAsync(goodp, 1, N, st));
     OFC_CUDA(cudaMemsetAsync(nfb, 0, N * 4, st));
     OFC_CUDA(cudaMemsetAsync(uprev, 0, 2 * N * 4, st));
-    bool have_prev = false, have_padj = false;
-    int ref_idx = 0;
-    std::vector<float> hbuf;
-    // one leg frames[ia] -> frames[ib] (track.py:200-206) into d's conf / raw planes: the engine's coarse and fine
-    // stages with the dense start `init` (2 planes, nullable), or the caller's leg source; returns coarse, fine (s)
-    auto leg = [&](const float* a, int ia, const float* b, int ib, const float* init) -> std::pair<double, double> {
-      if (legfn) {
-        hbuf.resize(5 * N);
-        float* hi = hbuf.data();
-        float* ho = hi + 2 * N;
-        if (init) OFC_CUDA(cudaMemcpyAsync(hi, init, 2 * N * 4, cudaMemcpyDeviceToHost, st));
-        OFC_CUDA(cudaStreamSynchronize(st));
-        if (legfn(leg_user, ia, ib, init ? hi : nullptr, init ? hi + N : nullptr, ho, ho + N, ho + 2 * N) != 0)
-          throw Error(OFC_ERR_ARG, "the leg source failed on the leg " + std::to_string(ia) + " -> " + std::to_string(ib));
-        OFC_CUDA(cudaMemcpyAsync(d.raw_ux, ho, N * 4, cudaMemcpyHostToDevice, st));
-        OFC_CUDA(cudaMemcpyAsync(d.raw_uy, ho + N, N * 4, cudaMemcpyHostToDevice, st));
-        OFC_CUDA(cudaMemcpyAsync(d.conf, ho + 2 * N, N * 4, cudaMemcpyHostToDevice, st));
-        OFC_CUDA(cudaStreamSynchronize(st));
-        return {0.0, 0.0};
-      }
-      OFC_CUDA(cudaMemcpyAsync(in1, a, N * 4, cudaMemcpyDeviceToDevice, st));
-      OFC_CUDA(cudaMemcpyAsync(in2, b, N * 4, cudaMemcpyDeviceToDevice, st));
-      if (init) {
-        OFC_CUDA(cudaMemcpyAsync(inu, init, N * 4, cudaMemcpyDeviceToDevice, st));
-        OFC_CUDA(cudaMemcpyAsync(inv, init + N, N * 4, cudaMemcpyDeviceToDevice, st));
-      }
-      run_pair(L, W, H, false, init != nullptr, *c, true, 2);
-      float ms0 = 0, ms1 = 0;
-      OFC_CUDA(cudaEventSynchronize(L.ev[3]));
-      OFC_CUDA(cudaEventElapsedTime(&ms0, L.ev[0], L.ev[1]));
-      OFC_CUDA(cudaEventElapsedTime(&ms1, L.ev[1], L.ev[3]));
-      return {ms0 * 1e-3, ms1 * 1e-3};
-    };
-    auto leg_mean = [&]() {
-      OFC_LAUNCH(k_reportable, g2, 128, 0, st, d.raw_ux, d.raw_uy, W, H, B, rep);
-      OFC_LAUNCH(k_mean_conf_rows, div_up(H, 128), 128, 0, st, d.conf, rep, u0r, u0r + N, droi, W, H, rsum, rcnt);
-      OFC_LAUNCH(k_mean_conf_fold, 1, 1, 0, st, rsum, rcnt, H, dmean);
-      double m = 0;
-      OFC_CUDA(cudaMemcpyAsync(&m, dmean, 8, cudaMemcpyDeviceToHost, st));
-      OFC_CUDA(cudaStreamSynchronize(st));
-      return m;
-    };
-    int any[4];
-    auto read_any = [&]() {
-      OFC_CUDA(cudaMemcpyAsync(any, dany, sizeof(any), cudaMemcpyDeviceToHost, st));
-      OFC_CUDA(cudaStreamSynchronize(st));
-    };
-    for (size_t k = 1; k < n; k++) {
-      const int K = (int)k;
-      OFC_CUDA(cudaMemcpyAsync(fk, frames[k], N * 4, cudaMemcpyHostToDevice, st));
-      std::pair<double, double> t = leg(ref, ref_idx, fk, K, have_prev ? praw : nullptr);
-      double cmean = leg_mean();
-      if (cmean < ruc[k - 1] && ref_idx != K - 1) {
-        // the reference moves to k - 1 (track.py:433-440): c0K replaced, anchors = good_prev, u0K = u_{k-1}
+  }
+  bool have_prev = false, have_padj = false;
+  int64_t ref_idx = 0;
+  next = fetch(1);
+  while (next) {
+    load(next, (int)(k & 1), fk);
+    fetched = false;
+    next = nullptr;
+    const double ruc = io.ruc(k);
+    std::pair<double, double> t = leg(ref, ref_idx, fk, k, have_prev ? praw : nullptr, true);
+    double cmean = leg_mean();
+    if (cmean < ruc && ref_idx != k - 1) {
+      if (io.hybrid) {
+        // c0K replaced, anchors = good_prev, u0K = u_{k-1} (track.py:433-440)
         OFC_LAUNCH(k_hyb_move, g2, 128, 0, st, pconf, u0r, u0r + N, goodp, W, H, c0r, anch);
         OFC_CUDA(cudaMemcpyAsync(u0r, uprev, 2 * N * 4, cudaMemcpyDeviceToDevice, st));
-        OFC_CUDA(cudaMemcpyAsync(ref, prev, N * 4, cudaMemcpyDeviceToDevice, st));
-        ref_idx = K - 1;
-        t = leg(ref, ref_idx, fk, K, nullptr);
-        cmean = leg_mean();
+      } else {
+        // the previous leg extends the link of frame 0 (track.rs:1135-1155)
+        OFC_LAUNCH(k_link_conf, g2, 128, 0, st, c0r, pconf, u0r, u0r + N, W, H, c0r);
+        OFC_LAUNCH(k_compose, g2, 128, 0, st, u0r, u0r + N, praw, praw + N, W, H, u0n, u0n + N);
+        OFC_CUDA(cudaMemcpyAsync(u0r, u0n, 2 * N * 4, cudaMemcpyDeviceToDevice, st));
       }
-      OFC_CUDA(cudaMemcpyAsync(praw, d.raw_ux, N * 4, cudaMemcpyDeviceToDevice, st));
-      OFC_CUDA(cudaMemcpyAsync(praw + N, d.raw_uy, N * 4, cudaMemcpyDeviceToDevice, st));
-      OFC_CUDA(cudaMemcpyAsync(pconf, d.conf, N * 4, cudaMemcpyDeviceToDevice, st));
+      OFC_CUDA(cudaMemcpyAsync(ref, prev, N * 4, cudaMemcpyDeviceToDevice, st));
+      ref_idx = k - 1;
+      t = leg(ref, ref_idx, fk, k, nullptr, false);
+      cmean = leg_mean();
+    }
+    OFC_CUDA(cudaMemcpyAsync(praw, d.raw_ux, N * 4, cudaMemcpyDeviceToDevice, st));
+    OFC_CUDA(cudaMemcpyAsync(praw + N, d.raw_uy, N * 4, cudaMemcpyDeviceToDevice, st));
+    OFC_CUDA(cudaMemcpyAsync(pconf, d.conf, N * 4, cudaMemcpyDeviceToDevice, st));
+    ofc_hybrid_frame info{};
+    info.reference = (int32_t)ref_idx;
+    info.mean_conf = cmean;
+    if (!io.hybrid) {
+      // frame 0 -> k and its link confidence (track.rs:1157-1200)
+      OFC_LAUNCH(k_compose, g2, 128, 0, st, u0r, u0r + N, praw, praw + N, W, H, cxy, cxy + N);
+      OFC_LAUNCH(k_link_conf, g2, 128, 0, st, c0r, pconf, u0r, u0r + N, W, H, conf64);
+      launch_f32_to_f64(cxy, u64, 2 * N, st);
+      ofc_threshold_low(conf64, cm, low, N, st);
+    } else {
       OFC_CUDA(cudaMemsetAsync(dany, 0, 4 * sizeof(int), st));
       OFC_CUDA(cudaMemsetAsync(dcnt, 0, 4 * sizeof(unsigned long long), st));
       OFC_LAUNCH(k_hyb_classify, g2, 128, 0, st, praw, praw + N, pconf, u0r, u0r + N, c0r, anch, uprev, uprev + N,
-                 nfb, droi, W, H, cm, hy->fb_max, ref_idx + 1 < K ? 1 : 0, cxy, cxy + N, legc, link, fl, dany);
+                 nfb, droi, W, H, cm, io.hy.fb_max, ref_idx + 1 < k ? 1 : 0, cxy, cxy + N, legc, link, fl, dany);
       read_any();
       const float *arx = nullptr, *ary = nullptr, *acf = nullptr;
       if (any[0]) {
-        if (ref_idx == K - 1) {  // the direct leg is the adjacent leg
+        if (ref_idx == k - 1) {  // the direct leg is the adjacent leg
           arx = praw;
           ary = praw + N;
           acf = pconf;
         } else {
-          const std::pair<double, double> ta = leg(prev, K - 1, fk, K, have_padj ? padj : nullptr);
+          const std::pair<double, double> ta = leg(prev, k - 1, fk, k, have_padj ? padj : nullptr, false);
           t.first += ta.first;
           t.second += ta.second;
           arx = d.raw_ux;
@@ -2194,50 +2297,215 @@ int ofc_track_sequence_hybrid(ofc_engine* e, const float* const* frames, size_t 
         OFC_CUDA(cudaMemcpyAsync(padj + N, ary, N * 4, cudaMemcpyDeviceToDevice, st));
       }
       have_padj = any[0] != 0;
-      OFC_LAUNCH(k_hyb_pre, gN, 256, 0, st, fl, cxy, cxy + N, axy, axy + N, ca, droi, N, cm, hy->fb_tol, support,
+      OFC_LAUNCH(k_hyb_pre, gN, 256, 0, st, fl, cxy, cxy + N, axy, axy + N, ca, droi, N, cm, io.hy.fb_tol, support,
                  dany);
       read_any();
       const uint8_t* g0 = nullptr;
       if (gate_on && any[1]) {
-        laa_dev<float>(L, W, H, support, cxy, cxy + N, cxy, cxy + N, radius, hy->fb_min_support, hy->fb_tol, gate0,
-                       nullptr);
+        laa_dev<float>(L, W, H, support, cxy, cxy + N, cxy, cxy + N, radius, io.hy.fb_min_support, io.hy.fb_tol,
+                       gate0, nullptr);
         g0 = gate0;
       }
-      OFC_LAUNCH(k_hyb_re, gN, 256, 0, st, fl, g0, legc, c0r, anch, nfb, ca, droi, N, hy->fb_max, cm, support, dany);
+      OFC_LAUNCH(k_hyb_re, gN, 256, 0, st, fl, g0, legc, c0r, anch, nfb, ca, droi, N, io.hy.fb_max, cm, support,
+                 dany);
       read_any();
       const uint8_t* g1 = nullptr;
       if (gate_on && any[2]) {
-        laa_dev<float>(L, W, H, support, cxy, cxy + N, axy, axy + N, radius, hy->fb_min_support, hy->fb_tol, gate,
-                       nullptr);
+        laa_dev<float>(L, W, H, support, cxy, cxy + N, axy, axy + N, radius, io.hy.fb_min_support, io.hy.fb_tol,
+                       gate, nullptr);
         g1 = gate;
       }
-      OFC_LAUNCH(k_hyb_out, gN, 256, 0, st, fl, g1, cxy, cxy + N, axy, axy + N, link, ca, nfb, droi, N, hy->fb_max,
+      OFC_LAUNCH(k_hyb_out, gN, 256, 0, st, fl, g1, cxy, cxy + N, axy, axy + N, link, ca, nfb, droi, N, io.hy.fb_max,
                  uprev, uprev + N, u64, u64 + N, conf64, low, goodp, dcnt);
-      OFC_CUDA(cudaEventRecord(L.ev[0], st));
-      finish_dev(L, low, droi, u64, u64 + N, conf64, W, H, *c, d, false);
-      OFC_CUDA(cudaEventRecord(L.ev[1], st));
-      download_pair(L, d, &outs[k - 1], N);
-      if (fb) OFC_CUDA(cudaMemcpyAsync(fb + (k - 1) * N, nfb, N * 4, cudaMemcpyDeviceToHost, st));
       unsigned long long cnt[4];
       OFC_CUDA(cudaMemcpyAsync(cnt, dcnt, sizeof(cnt), cudaMemcpyDeviceToHost, st));
-      OFC_CUDA(cudaMemcpyAsync(prev, fk, N * 4, cudaMemcpyDeviceToDevice, st));
       OFC_CUDA(cudaStreamSynchronize(st));
-      float ms = 0;
-      OFC_CUDA(cudaEventElapsedTime(&ms, L.ev[0], L.ev[1]));
-      outs[k - 1].timing[0] = t.first;
-      outs[k - 1].timing[1] = t.second;
-      outs[k - 1].timing[2] = ms * 1e-3;
-      if (info) {
-        ofc_hybrid_frame& f = info[k - 1];
-        f.reference = ref_idx;
-        f.n_fb_max = (int32_t)cnt[3];
-        f.mean_conf = cmean;
-        f.fallback_frac = (double)cnt[0] / (double)n_roi;
-        f.fb_gate_rejected = (double)cnt[1] / (double)n_roi;
-        f.reacquired = (double)cnt[2] / (double)n_roi;
-      }
-      have_prev = true;
+      info.n_fb_max = (int32_t)cnt[3];
+      info.fallback_frac = (double)cnt[0] / (double)n_roi;
+      info.fb_gate_rejected = (double)cnt[1] / (double)n_roi;
+      info.reacquired = (double)cnt[2] / (double)n_roi;
     }
+    if (!fetched) service();  // a scripted run whose legs all came from the caller
+    OFC_CUDA(cudaEventRecord(L.sev[0], st));
+    finish_dev(L, low, droi, u64, u64 + N, conf64, W, H, c, d, false);
+    OFC_CUDA(cudaEventRecord(L.sev[1], st));
+    // stage the results (after the previous frame's copy has left the staging), copy them out on the copy stream
+    if (copy_issued) OFC_CUDA(cudaStreamWaitEvent(st, copied, 0));
+    OFC_CUDA(cudaMemcpyAsync(dstage, d.ux, 10 * N * 4, cudaMemcpyDeviceToDevice, st));
+    OFC_CUDA(cudaMemcpyAsync(dstage_v, d.valid, N, cudaMemcpyDeviceToDevice, st));
+    if (io.hybrid) OFC_CUDA(cudaMemcpyAsync(dstage_fb, nfb, N * 4, cudaMemcpyDeviceToDevice, st));
+    OFC_CUDA(cudaEventRecord(staged, st));
+    OFC_CUDA(cudaStreamWaitEvent(L.copy, staged, 0));
+    OFC_CUDA(cudaMemcpyAsync(hout, dstage, 10 * N * 4, cudaMemcpyDeviceToHost, L.copy));
+    OFC_CUDA(cudaMemcpyAsync(hvalid, dstage_v, N, cudaMemcpyDeviceToHost, L.copy));
+    if (io.hybrid) OFC_CUDA(cudaMemcpyAsync(hfb, dstage_fb, N * 4, cudaMemcpyDeviceToHost, L.copy));
+    OFC_CUDA(cudaEventRecord(copied, L.copy));
+    copy_issued = true;
+    pending.active = true;
+    pending.k = k;
+    pending.coarse = t.first;
+    pending.fine = t.second;
+    pending.info = info;
+    OFC_CUDA(cudaMemcpyAsync(prev, fk, N * 4, cudaMemcpyDeviceToDevice, st));
+    have_prev = true;
+    k++;
+  }
+  flush();
+  OFC_CUDA(cudaStreamSynchronize(st));
+  return emitted;
+}
+
+// the host planes of a staged frame into the caller's (each pointer nullable) and the timing
+void copy_pair_out(const ofc_pair_out& s, ofc_pair_out* d, size_t N) {
+  float* const* src[10] = {&s.ux, &s.uy, &s.conf, &s.exx, &s.eyy, &s.exy, &s.gmax, &s.vol, &s.raw_ux, &s.raw_uy};
+  float** dst[10] = {&d->ux, &d->uy, &d->conf, &d->exx, &d->eyy, &d->exy, &d->gmax, &d->vol, &d->raw_ux, &d->raw_uy};
+  for (int i = 0; i < 10; i++)
+    if (*dst[i]) std::memcpy(*dst[i], *src[i], N * 4);
+  if (d->valid) std::memcpy(d->valid, s.valid, N);
+  for (int i = 0; i < 3; i++) d->timing[i] = s.timing[i];
+}
+
+// the checks shared by the sequence entry points (track.py:274-279)
+void sequence_checks(const ofc_config* c, size_t w, size_t h, const uint8_t* roi) {
+  cfg_check(c);
+  check_sizes(w, h);
+  if (roi) {
+    bool any = false;
+    for (size_t i = 0, N = w * h; i < N && !any; i++) any = roi[i] != 0;
+    if (!any) throw Error(OFC_ERR_ARG, "ROI mask is empty");
+  }
+}
+
+void size_checks(size_t w, size_t h, const ofc_config* c, bool legs) {
+  if ((int)std::min(w, h) < c->poc_win)
+    throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
+  if (!legs) check_fine_window(w, h, *c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ofc_track_sequence(ofc_engine* e, const float* const* frames, size_t n, size_t w, size_t h, const uint8_t* roi,
+                       const ofc_config* c, double ref_update_conf, ofc_pair_out* outs, int32_t* reference,
+                       double* mean_conf, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    sequence_checks(c, w, h, roi);
+    if (!frames || n == 0) throw Error(OFC_ERR_ARG, "no frames");
+    for (size_t k = 0; k < n; k++)
+      if (!frames[k]) throw Error(OFC_ERR_ARG, "null frame " + std::to_string(k));
+    if (n > 1 && !outs) throw Error(OFC_ERR_ARG, "null outputs");
+    if (!std::isfinite(ref_update_conf)) throw Error(OFC_ERR_ARG, "ref_update_conf must be a finite number");
+    if (n == 1) return;
+    size_checks(w, h, c, false);
+    const size_t N = w * h;
+    SeqIO io;
+    io.W = (int)w;
+    io.H = (int)h;
+    io.roi = roi;
+    io.c = c;
+    io.w_in = (int)w;
+    io.h_in = (int)h;
+    io.frame = [&](int64_t k, void*) -> const void* { return k < (int64_t)n ? frames[k] : nullptr; };
+    io.ruc = [&](int64_t) { return ref_update_conf; };
+    io.emit = [&](int64_t k, const ofc_pair_out& o, const int32_t*, const ofc_hybrid_frame& info) {
+      copy_pair_out(o, &outs[k - 1], N);
+      if (reference) reference[k - 1] = info.reference;
+      if (mean_conf) mean_conf[k - 1] = info.mean_conf;
+    };
+    run_sequence(L, io);
+  });
+}
+
+int ofc_track_sequence_hybrid(ofc_engine* e, const float* const* frames, size_t n, size_t w, size_t h,
+                              const uint8_t* roi, const ofc_config* c, const double* ruc, const ofc_hybrid* hy,
+                              ofc_pair_out* outs, int32_t* fb, ofc_hybrid_frame* info, ofc_leg_fn legfn,
+                              void* leg_user, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    sequence_checks(c, w, h, roi);
+    hybrid_check(hy);
+    if (!frames || n == 0) throw Error(OFC_ERR_ARG, "no frames");
+    for (size_t k = 0; k < n; k++)
+      if (!frames[k]) throw Error(OFC_ERR_ARG, "null frame " + std::to_string(k));
+    if (n > 1 && !outs) throw Error(OFC_ERR_ARG, "null outputs");
+    if (n > 1 && !ruc) throw Error(OFC_ERR_ARG, "null ref_update_conf");
+    for (size_t k = 0; k + 1 < n; k++)
+      if (!std::isfinite(ruc[k])) throw Error(OFC_ERR_ARG, "ref_update_conf must be a finite number");
+    if (n == 1) return;
+    size_checks(w, h, c, legfn != nullptr);
+    const size_t N = w * h;
+    SeqIO io;
+    io.W = (int)w;
+    io.H = (int)h;
+    io.roi = roi;
+    io.c = c;
+    io.hybrid = true;
+    io.hy = *hy;
+    io.w_in = (int)w;
+    io.h_in = (int)h;
+    io.leg = legfn;
+    io.leg_user = leg_user;
+    io.frame = [&](int64_t k, void*) -> const void* { return k < (int64_t)n ? frames[k] : nullptr; };
+    io.ruc = [&](int64_t k) { return ruc[k - 1]; };
+    io.emit = [&](int64_t k, const ofc_pair_out& o, const int32_t* f, const ofc_hybrid_frame& fi) {
+      copy_pair_out(o, &outs[k - 1], N);
+      if (fb) std::memcpy(fb + (k - 1) * N, f, N * 4);
+      if (info) info[k - 1] = fi;
+    };
+    run_sequence(L, io);
+  });
+}
+
+int ofc_track_stream(ofc_engine* e, const ofc_stream* s, const uint8_t* roi, const ofc_config* c, int64_t* n_out,
+                     char* err, size_t errlen) {
+  if (n_out) *n_out = 0;
+  return guarded(e, err, errlen, [&](Lane& L) {
+    if (!s) throw Error(OFC_ERR_ARG, "null stream");
+    if (!s->source || !s->sink) throw Error(OFC_ERR_ARG, "the stream needs a source and a sink");
+    check_format(s->pixel, s->w_in, s->h_in, s->scale);
+    const size_t w = s->w_in / s->scale, h = s->h_in / s->scale;
+    sequence_checks(c, w, h, roi);
+    if (s->hybrid) hybrid_check(&s->hy);
+    if (!std::isfinite(s->ref_update_conf)) throw Error(OFC_ERR_ARG, "ref_update_conf must be a finite number");
+    size_checks(w, h, c, false);
+    SeqIO io;
+    io.W = (int)w;
+    io.H = (int)h;
+    io.roi = roi;
+    io.c = c;
+    io.hybrid = s->hybrid != 0;
+    io.hy = s->hy;
+    io.pixel = s->pixel;
+    io.w_in = (int)s->w_in;
+    io.h_in = (int)s->h_in;
+    io.scale = s->scale;
+    io.frame = [&](int64_t k, void* slot) -> const void* {
+      const int r = s->source(s->source_user, k, slot);
+      if (r == 1) return nullptr;
+      if (r != 0) throw Error(OFC_ERR_ARG, "the frame source failed on frame " + std::to_string(k));
+      return slot;
+    };
+    io.ruc = [&](int64_t) { return s->ref_update_conf; };
+    io.emit = [&](int64_t k, const ofc_pair_out& o, const int32_t* f, const ofc_hybrid_frame& fi) {
+      if (s->sink(s->sink_user, k, &o, f, &fi) != 0)
+        throw Error(OFC_ERR_ARG, "the result sink stopped the run at frame " + std::to_string(k));
+      if (n_out) *n_out = k;
+    };
+    run_sequence(L, io);
+  });
+}
+
+int ofc_to_gray(ofc_engine* e, const void* px, int32_t pixel, size_t w, size_t h, int32_t scale, float* out,
+                char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    if (!px || !out) throw Error(OFC_ERR_ARG, "null argument");
+    check_format(pixel, w, h, scale);
+    const size_t bytes = pixel_bytes(pixel) * w * h, W = w / scale, H = h / scale;
+    const uint8_t* d = L.upload("gray_in", (const uint8_t*)px, bytes);
+    float* o = L.get<float>("gray_out", W * H);
+    to_gray_dev(L, d, pixel, (int)w, scale, (int)W, (int)H, o);
+    OFC_CUDA(cudaMemcpyAsync(out, o, W * H * 4, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
   });
 }
 

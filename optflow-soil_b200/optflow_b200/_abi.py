@@ -112,6 +112,32 @@ class OfcHybridFrame(ctypes.Structure):
 LEG_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, c_float_p, c_float_p,
                           c_float_p, c_float_p, c_float_p)
 
+OFC_PIX = {"f32": 0, "gray8": 1, "gray16": 2, "rgb24": 3, "rgba32": 4, "rgb48": 5}
+
+# ofc_source_fn: (user, k, dst) -> 0 frame written, 1 no frame k, else error
+SOURCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p)
+# ofc_sink_fn: (user, k, out, fb, info) -> 0 to go on
+SINK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, c_i32_p,
+                           ctypes.POINTER(OfcHybridFrame))
+
+
+class OfcStream(ctypes.Structure):
+    """ofc_stream of include/optflow_cuda.h: a frame source, its format and a result sink."""
+    _fields_ = [
+        ("pixel", ctypes.c_int32),
+        ("w_in", ctypes.c_size_t),
+        ("h_in", ctypes.c_size_t),
+        ("scale", ctypes.c_int32),
+        ("hybrid", ctypes.c_int32),
+        ("hy", OfcHybrid),
+        ("ref_update_conf", ctypes.c_double),
+        ("source", SOURCE_FN),
+        ("source_user", ctypes.c_void_p),
+        ("sink", SINK_FN),
+        ("sink_user", ctypes.c_void_p),
+    ]
+
+
 PAIR_FIELDS = ("ux", "uy", "conf", "exx", "eyy", "exy", "gmax", "vol", "valid", "raw_ux", "raw_uy")
 
 # every symbol the header declares, with its ctypes signature (restype, argtypes)
@@ -143,6 +169,9 @@ SIGNATURES = {
     "ofc_local_affine_agreement": (ctypes.c_int, [_P, _S, _S, c_double_p, c_double_p, c_u8_p, c_double_p, c_double_p,
                                                   ctypes.c_double, ctypes.c_int64, ctypes.c_double, c_u8_p, c_i32_p,
                                                   _E, _S]),
+    "ofc_to_gray": (ctypes.c_int, [_P, ctypes.c_void_p, ctypes.c_int32, _S, _S, ctypes.c_int32, c_float_p, _E, _S]),
+    "ofc_track_stream": (ctypes.c_int, [_P, ctypes.POINTER(OfcStream), c_u8_p, ctypes.POINTER(OfcConfig),
+                                        ctypes.POINTER(ctypes.c_int64), _E, _S]),
     "ofc_align_to": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, c_u8_p, ctypes.c_int, ctypes.POINTER(OfcConfig),
                                     c_float_p, ctypes.POINTER(ctypes.c_int), _E, _S]),
     "ofc_average_window": (ctypes.c_int, [_P, ctypes.POINTER(c_float_p), _S, _S, _S, _S, ctypes.c_int, c_u8_p,

@@ -414,3 +414,31 @@ def local_affine_agreement(ux, uy, support, tx, ty, radius, min_support, tol):
     with np.errstate(invalid="ignore"):
         ok = (s1 + 0.5 >= min_support) & fit & (np.hypot(tx - a[0], ty - a[1]) <= tol)
     return ok, np.rint(s1).astype(np.int64)
+
+
+# ---------------------------------------------------------------- frame front-end
+_PIX_SCALE = {"gray8": 255.0, "rgb24": 255.0, "rgba32": 255.0, "gray16": 65535.0, "rgb48": 65535.0}
+
+
+def to_gray(px, pixel, scale=1):
+    """The CLI's grey levels of a frame, box-downscaled and rounded to float32 (rust/crates/optflow-cli/src/io.rs:
+    44-52 luminance and lut8, 150-256 gray_from, 258-281 downscale; video.rs:290-300 rgb_to_gray): v / 255 or
+    v / 65535, 0.299 R + 0.587 G + 0.114 B left to right, then per block the rows summed left to right and the
+    row sums in order, / scale^2. Returns (out float32, grey float64 before the downscale)."""
+    a = np.asarray(px)
+    if pixel == "f32":
+        g = a.astype(np.float32).astype(np.float64)
+    else:
+        f = a.astype(np.float64) / _PIX_SCALE[pixel]
+        g = f if f.ndim == 2 else 0.299 * f[..., 0] + 0.587 * f[..., 1] + 0.114 * f[..., 2]
+    if scale == 1:
+        return g.astype(np.float32), g
+    oh, ow = g.shape[0] // scale, g.shape[1] // scale
+    b = g[:oh * scale, :ow * scale].reshape(oh, scale, ow, scale)
+    total = np.zeros((oh, ow))
+    for dy in range(scale):
+        rs = np.zeros((oh, ow))
+        for dx in range(scale):
+            rs = rs + b[:, dy, :, dx]
+        total = total + rs
+    return (total / float(scale * scale)).astype(np.float32), g

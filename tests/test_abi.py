@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import numpy as np
+
 import pytest
 import torch
 from conftest import ROOT
@@ -92,3 +94,48 @@ def test_config_json_round_trip():
     assert d == c
     with pytest.raises(ValueError, match="unknown config keys"):
         Config.from_json('{"nope": 1}')
+
+
+@pytest.mark.parametrize("kw,msg", [
+    (dict(fb_max=-1), "fb_max must be >= 0"),
+    (dict(fb_tol=0.0), "fb_radius must be finite and nonzero (negative: 4 sigma_w), fb_tol finite and positive"),
+    (dict(fb_radius=0.0), "fb_radius must be finite and nonzero (negative: 4 sigma_w), fb_tol finite and positive"),
+    (dict(fb_min_support=-1), "fb_min_support must be >= 0 and tavg in [0, 64]"),
+    (dict(seq_mode="x"), "seq_mode must be 'chain' or 'hybrid', got 'x'"),
+])
+def test_hybrid_key_validation(kw, msg):
+    """The hybrid keys' rules and messages of config.py:195-200."""
+    with pytest.raises(ValueError) as e:
+        Config(**kw).validate()
+    assert str(e.value) == msg
+    assert Config().fb_radius_px() == 16.0 and Config(fb_radius=12.0).fb_radius_px() == 12.0
+
+
+def test_pixel_formats_and_save_result(tmp_path):
+    """The frame formats the stream takes, and save_result's file set (io.py:203-233): float32 planes, valid as
+    uint8 from ux, fb as int32 for hybrid results, timing.json."""
+    import json
+
+    from optflow_b200 import Result
+    from optflow_b200.stream import pixel_format, save_result
+    z = lambda *s, t=np.uint8: np.zeros(s, t)
+    assert [pixel_format(a) for a in (z(4, 5), z(4, 5, 3), z(4, 5, 4), z(4, 5, t=np.uint16), z(4, 5, 3, t=np.uint16),
+                                      z(4, 5, t=np.float64))] == ["gray8", "rgb24", "rgba32", "gray16", "rgb48", "f32"]
+    for bad in (z(4, 5, 2), z(4, 5, t=np.int32), z(4, 5, 4, t=np.uint16)):
+        with pytest.raises(ValueError, match="unsupported"):
+            pixel_format(bad)
+    rng = np.random.default_rng(2)
+    p = lambda: rng.random((6, 7))
+    ux = p()
+    ux[0, 0] = np.nan
+    st = {k: p() for k in ("Exx", "Eyy", "Exy", "gmax", "vol")}
+    r = Result(ux, p(), p(), st, p(), p(), {"coarse": 0.1, "reference": 2}, None, np.arange(42).reshape(6, 7))
+    save_result(str(tmp_path / "f1"), r, raw=True)
+    names = sorted(f.name for f in (tmp_path / "f1").iterdir())
+    assert names == sorted(["ux.npy", "uy.npy", "conf.npy", "Exx.npy", "Eyy.npy", "Exy.npy", "gmax.npy", "vol.npy",
+                            "raw_ux.npy", "raw_uy.npy", "valid.npy", "fb.npy", "timing.json"])
+    back = np.load(tmp_path / "f1" / "ux.npy")
+    assert back.dtype == np.dtype("<f4") and np.array_equal(back, ux.astype(np.float32), equal_nan=True)
+    assert np.load(tmp_path / "f1" / "valid.npy").tolist() == np.isfinite(ux).astype(np.uint8).tolist()
+    assert np.load(tmp_path / "f1" / "fb.npy").dtype == np.dtype("<i4")
+    assert json.load(open(tmp_path / "f1" / "timing.json")) == {"coarse": 0.1, "reference": 2}

@@ -245,3 +245,24 @@ def test_local_affine_agreement(oracle):
                                           sup, g["laa_step_tx"], g["laa_step_ty"], 6.5, 20, 0.5)
     np.testing.assert_array_equal(ok, g["laa_step_ok"].astype(bool))
     np.testing.assert_array_equal(n, g["laa_step_n"])
+
+
+def test_to_gray(oracle):
+    """The frame front-end's restatement against the reference's io.to_gray / io.downscale (tests/golden/frames.npz):
+    the grey levels exactly, the downscales within 1e-15 (numpy's mean sums in another order than the CLI), and the
+    CLI's own known answers (io.rs:675-698)."""
+    g = golden("frames")
+    for name in ("gray8", "rgb24", "rgba32", "gray16", "rgb48", "f32"):
+        out, grey = oracle.to_gray(g[f"{name}_in"], name)
+        np.testing.assert_array_equal(grey, g[f"{name}_gray"], err_msg=name)
+        np.testing.assert_array_equal(out, g[f"{name}_gray"].astype(np.float32), err_msg=name)
+        for s in (2, 3):
+            out, _ = oracle.to_gray(g[f"{name}_in"], name, s)
+            want = g[f"{name}_down{s}"]
+            assert out.shape == want.shape
+            assert np.abs(out.astype(np.float64) - want).max() <= 1e-7 * np.abs(want).max(), (name, s)
+    ramp = np.arange(16, dtype=np.float32).reshape(4, 4)
+    np.testing.assert_array_equal(oracle.to_gray(ramp, "f32", 2)[0], [[2.5, 4.5], [10.5, 12.5]])
+    blocks = np.array([[3 * y + x % 3 + 9 * (x // 3) for x in range(6)] for y in range(3)], np.float32)
+    np.testing.assert_array_equal(oracle.to_gray(blocks, "f32", 3)[0], [[4.0, 13.0]])
+    assert oracle.to_gray(np.ones((3, 5), np.float32), "f32", 2)[0].shape == (1, 2)
