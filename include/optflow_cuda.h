@@ -345,6 +345,25 @@ OFC_API int ofc_strain(ofc_engine* eng, const float* ux, const float* uy, size_t
 OFC_API int ofc_finish(ofc_engine* eng, const float* ux, const float* uy, const float* conf, const uint8_t* roi,
                size_t w, size_t h, const ofc_config* cfg, ofc_pair_out* out, char* err, size_t errlen);
 
+/* One pair of a batch (the arguments of ofc_track_pair). */
+typedef struct ofc_pair_in {
+    const float* i1;
+    const float* i2;
+    size_t w, h;
+    const uint8_t* roi;    /* nullable */
+    const float* init_ux;  /* nullable; both or neither */
+    const float* init_uy;
+} ofc_pair_in;
+
+/*
+ * Many independent pairs of any sizes (the CLI's pair runs, or the pairs of a sequence step) in one call: each
+ * result equals ofc_track_pair's bit for bit. The pairs run on up to four worker lanes of their own streams and
+ * buffers, the largest windows first; while one lane's pair computes, the host feeds the others, so small pairs
+ * overlap instead of leaving the GPU idle between their launches. outs[i] gets pairs[i]'s results.
+ */
+OFC_API int ofc_track_pairs(ofc_engine* eng, const ofc_pair_in* pairs, size_t n, const ofc_config* cfg,
+                    ofc_pair_out* outs, char* err, size_t errlen);
+
 /*
  * track::track_pair (python/optflow_ref/track.py:115-146; rust/crates/optflow-core/src/track.rs:
  * 567-623,765): coarse POC -> dense start -> fine stage -> finish, one pair, host buffers.

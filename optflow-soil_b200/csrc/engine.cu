@@ -330,7 +330,10 @@ struct Lane {
     slot.second = std::move(b);
     return slot.first;
   }
+  // the worker lanes of a batched call (ofc_track_pairs), created on first use and owned by this lane
+  std::vector<std::unique_ptr<Lane>> aux;
   void release() {
+    for (auto& a : aux) a->release();
     graphs.clear();
     consts.clear();
     pool.clear();
@@ -338,6 +341,43 @@ struct Lane {
     plans.clear();
   }
 };
+
+// a lane's streams and events (ofc_create), and their end (ofc_destroy): work in flight is waited for first
+void lane_init(Lane& l) {
+  OFC_CUDA(cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking));
+  OFC_CUDA(cudaStreamCreateWithFlags(&l.side, cudaStreamNonBlocking));
+  OFC_CUDA(cudaEventCreateWithFlags(&l.fork, cudaEventDisableTiming));
+  OFC_CUDA(cudaEventCreateWithFlags(&l.join, cudaEventDisableTiming));
+  OFC_CUDA(cudaEventCreateWithFlags(&l.masked, cudaEventDisableTiming));
+  for (auto& ev : l.ev) OFC_CUDA(cudaEventCreate(&ev));
+}
+
+void lane_sync(Lane& l) {
+  for (auto& a : l.aux) lane_sync(*a);
+  cudaStreamSynchronize(l.stream);
+  cudaStreamSynchronize(l.side);
+  if (l.copy) cudaStreamSynchronize(l.copy);
+}
+
+void lane_destroy(Lane& l) {
+  for (auto& a : l.aux) lane_destroy(*a);
+  l.aux.clear();
+  cudaStreamSynchronize(l.stream);
+  if (l.copy) cudaStreamSynchronize(l.copy);
+  cudaStreamSynchronize(l.side);
+  l.release();
+  for (auto& ev : l.ev) cudaEventDestroy(ev);
+  cudaEventDestroy(l.fork);
+  cudaEventDestroy(l.join);
+  cudaEventDestroy(l.masked);
+  cudaStreamDestroy(l.side);
+  if (l.copy) {
+    for (auto& ev : l.bev) cudaEventDestroy(ev);
+    for (auto& ev : l.sev) cudaEventDestroy(ev);
+    cudaStreamDestroy(l.copy);
+  }
+  cudaStreamDestroy(l.stream);
+}
 
 // a key of the configuration fields the pair path reads
 std::string cfg_key(const ofc_config& c) {
@@ -1621,12 +1661,7 @@ ofc_engine* ofc_create(int device, int lanes, char* err, size_t errlen) {
     eng->nlanes = lanes;
     for (int i = 0; i < lanes; i++) {
       std::unique_ptr<Lane> l(new Lane());
-      OFC_CUDA(cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking));
-      OFC_CUDA(cudaStreamCreateWithFlags(&l->side, cudaStreamNonBlocking));
-      OFC_CUDA(cudaEventCreateWithFlags(&l->fork, cudaEventDisableTiming));
-      OFC_CUDA(cudaEventCreateWithFlags(&l->join, cudaEventDisableTiming));
-      OFC_CUDA(cudaEventCreateWithFlags(&l->masked, cudaEventDisableTiming));
-      for (auto& ev : l->ev) OFC_CUDA(cudaEventCreate(&ev));
+      lane_init(*l);
       eng->lanes.push_back(std::move(l));
     }
     return eng.release();
@@ -1641,21 +1676,7 @@ void ofc_destroy(ofc_engine* e) {
   cudaSetDevice(e->device);
   for (auto& l : e->lanes) {
     std::lock_guard<std::mutex> lk(l->busy);
-    cudaStreamSynchronize(l->stream);
-    if (l->copy) cudaStreamSynchronize(l->copy);
-    cudaStreamSynchronize(l->side);
-    l->release();
-    for (auto& ev : l->ev) cudaEventDestroy(ev);
-    cudaEventDestroy(l->fork);
-    cudaEventDestroy(l->join);
-    cudaEventDestroy(l->masked);
-    cudaStreamDestroy(l->side);
-    if (l->copy) {
-      for (auto& ev : l->bev) cudaEventDestroy(ev);
-      for (auto& ev : l->sev) cudaEventDestroy(ev);
-      cudaStreamDestroy(l->copy);
-    }
-    cudaStreamDestroy(l->stream);
+    lane_destroy(*l);
   }
   delete e;
 }
@@ -1685,7 +1706,7 @@ void ofc_release_caches(ofc_engine* e) {
   cudaSetDevice(e->device);
   for (auto& l : e->lanes) {
     std::lock_guard<std::mutex> lk(l->busy);
-    cudaStreamSynchronize(l->stream);
+    lane_sync(*l);
     l->release();
   }
 }
@@ -1912,6 +1933,16 @@ int ofc_strain(ofc_engine* e, const float* ux, const float* uy, size_t w, size_t
   });
 }
 
+// the host planes of a staged frame into the caller's (each pointer nullable) and the timing
+static void copy_pair_out(const ofc_pair_out& s, ofc_pair_out* d, size_t N) {
+  float* const* src[10] = {&s.ux, &s.uy, &s.conf, &s.exx, &s.eyy, &s.exy, &s.gmax, &s.vol, &s.raw_ux, &s.raw_uy};
+  float** dst[10] = {&d->ux, &d->uy, &d->conf, &d->exx, &d->eyy, &d->exy, &d->gmax, &d->vol, &d->raw_ux, &d->raw_uy};
+  for (int i = 0; i < 10; i++)
+    if (*dst[i]) std::memcpy(*dst[i], *src[i], N * 4);
+  if (d->valid) std::memcpy(d->valid, s.valid, N);
+  for (int i = 0; i < 3; i++) d->timing[i] = s.timing[i];
+}
+
 static void download_pair(Lane& L, const ofc_pair_out& d, ofc_pair_out* h, size_t N) {
   cudaStream_t st = L.stream;
   float* const* dsrc[10] = {&d.ux, &d.uy, &d.conf, &d.exx, &d.eyy, &d.exy, &d.gmax, &d.vol, &d.raw_ux, &d.raw_uy};
@@ -1955,6 +1986,79 @@ int ofc_finish(ofc_engine* e, const float* ux, const float* uy, const float* con
     download_pair(L, d, out, N);
     OFC_CUDA(cudaStreamSynchronize(st));
     std::memset(out->timing, 0, sizeof(out->timing));
+  });
+}
+
+int ofc_track_pairs(ofc_engine* e, const ofc_pair_in* pairs, size_t n, const ofc_config* c, ofc_pair_out* outs,
+                    char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    if (n == 0) return;
+    if (!pairs || !outs) throw Error(OFC_ERR_ARG, "null argument");
+    for (size_t i = 0; i < n; i++) {
+      const ofc_pair_in& p = pairs[i];
+      const std::string at = "pair " + std::to_string(i) + ": ";
+      if (!p.i1 || !p.i2) throw Error(OFC_ERR_ARG, at + "null image");
+      if ((p.init_ux == nullptr) != (p.init_uy == nullptr))
+        throw Error(OFC_ERR_ARG, at + "init_ux and init_uy must both be given");
+      try {
+        check_fine_window(p.w, p.h, *c);
+      } catch (const Error& x) {
+        throw Error(x.status, at + x.what());
+      }
+      if ((int)std::min(p.w, p.h) < c->poc_win)
+        throw Error(OFC_ERR_ARG, at + "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
+    }
+    // the largest padded windows first, so that a worker's buffers are sized once
+    std::vector<size_t> order(n);
+    for (size_t i = 0; i < n; i++) order[i] = i;
+    auto padded = [&](size_t i) { return (pairs[i].w + 2 * PAD) * (pairs[i].h + 2 * PAD); };
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return padded(a) > padded(b); });
+    const int K = (int)std::min<size_t>(n, 4);
+    while ((int)L.aux.size() < K) {
+      std::unique_ptr<Lane> a(new Lane());
+      lane_init(*a);
+      L.aux.push_back(std::move(a));
+    }
+    std::vector<long long> busy(K, -1);
+    // a worker's finished pair: its planes from page-locked staging into the caller's buffers
+    auto drain = [&](int j) {
+      if (busy[j] < 0) return;
+      Lane& A = *L.aux[j];
+      const size_t i = (size_t)busy[j], N = pairs[i].w * pairs[i].h;
+      busy[j] = -1;
+      OFC_CUDA(cudaStreamSynchronize(A.stream));
+      float* hout = A.pinned<float>("batch_hout", 10 * N);
+      ofc_pair_out o{};
+      float** f[10] = {&o.ux, &o.uy, &o.conf, &o.exx, &o.eyy, &o.exy, &o.gmax, &o.vol, &o.raw_ux, &o.raw_uy};
+      for (int q = 0; q < 10; q++) *f[q] = hout + q * N;
+      o.valid = A.pinned<uint8_t>("batch_hvalid", N);
+      pair_timing(A, o.timing);
+      copy_pair_out(o, &outs[i], N);
+    };
+    for (size_t q = 0; q < n; q++) {
+      const size_t i = order[q];
+      const int j = (int)(q % K);
+      drain(j);
+      Lane& A = *L.aux[j];
+      const ofc_pair_in& p = pairs[i];
+      const size_t N = p.w * p.h;
+      A.upload("in_i1", p.i1, N);
+      A.upload("in_i2", p.i2, N);
+      if (p.roi) A.upload("in_roi", p.roi, N);
+      if (p.init_ux) {
+        A.upload("in_u", p.init_ux, N);
+        A.upload("in_v", p.init_uy, N);
+      }
+      run_pair(A, (int)p.w, (int)p.h, p.roi != nullptr, p.init_ux != nullptr, *c, true, 3);
+      const ofc_pair_out d = device_pair_out(A, N);
+      float* hout = A.pinned<float>("batch_hout", 10 * N);
+      uint8_t* hvalid = A.pinned<uint8_t>("batch_hvalid", N);
+      OFC_CUDA(cudaMemcpyAsync(hout, d.ux, 10 * N * 4, cudaMemcpyDeviceToHost, A.stream));
+      OFC_CUDA(cudaMemcpyAsync(hvalid, d.valid, N, cudaMemcpyDeviceToHost, A.stream));
+      busy[j] = (long long)i;
+    }
+    for (int j = 0; j < K; j++) drain(j);
   });
 }
 
@@ -2353,16 +2457,6 @@ int64_t run_sequence(Lane& L, const SeqIO& io) {
   flush();
   OFC_CUDA(cudaStreamSynchronize(st));
   return emitted;
-}
-
-// the host planes of a staged frame into the caller's (each pointer nullable) and the timing
-void copy_pair_out(const ofc_pair_out& s, ofc_pair_out* d, size_t N) {
-  float* const* src[10] = {&s.ux, &s.uy, &s.conf, &s.exx, &s.eyy, &s.exy, &s.gmax, &s.vol, &s.raw_ux, &s.raw_uy};
-  float** dst[10] = {&d->ux, &d->uy, &d->conf, &d->exx, &d->eyy, &d->exy, &d->gmax, &d->vol, &d->raw_ux, &d->raw_uy};
-  for (int i = 0; i < 10; i++)
-    if (*dst[i]) std::memcpy(*dst[i], *src[i], N * 4);
-  if (d->valid) std::memcpy(d->valid, s.valid, N);
-  for (int i = 0; i < 3; i++) d->timing[i] = s.timing[i];
 }
 
 // the checks shared by the sequence entry points (track.py:274-279)

@@ -86,6 +86,19 @@ class OfcWindow(ctypes.Structure):
     ]
 
 
+class OfcPairIn(ctypes.Structure):
+    """ofc_pair_in of include/optflow_cuda.h: one pair of a batch."""
+    _fields_ = [
+        ("i1", c_float_p),
+        ("i2", c_float_p),
+        ("w", ctypes.c_size_t),
+        ("h", ctypes.c_size_t),
+        ("roi", c_u8_p),
+        ("init_ux", c_float_p),
+        ("init_uy", c_float_p),
+    ]
+
+
 class OfcHybrid(ctypes.Structure):
     """ofc_hybrid of include/optflow_cuda.h: the hybrid keys of Config."""
     _fields_ = [
@@ -186,6 +199,8 @@ SIGNATURES = {
     "ofc_strain": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, ctypes.c_int32] + [c_float_p] * 9 + [_E, _S]),
     "ofc_finish": (ctypes.c_int, [_P, c_float_p, c_float_p, c_float_p, c_u8_p, _S, _S, ctypes.POINTER(OfcConfig),
                                   ctypes.POINTER(OfcPairOut), _E, _S]),
+    "ofc_track_pairs": (ctypes.c_int, [_P, ctypes.POINTER(OfcPairIn), _S, ctypes.POINTER(OfcConfig),
+                                       ctypes.POINTER(OfcPairOut), _E, _S]),
     "ofc_track_pair": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, c_u8_p, c_float_p, c_float_p,
                                       ctypes.POINTER(OfcConfig), ctypes.POINTER(OfcPairOut), _E, _S]),
     "ofc_track_pair_device": (ctypes.c_int, [_P, _P, _P, _S, _S, _P, _P, _P, ctypes.POINTER(OfcConfig),

@@ -248,6 +248,39 @@ def _result(o, arrs):
                   arrs["valid"].astype(bool))
 
 
+def track_pairs(items, cfg=None, engine=None):
+    """track_pair over many independent pairs of any sizes in one ofc_track_pairs call: items are (I1, I2),
+    (I1, I2, mask) or (I1, I2, mask, init) tuples; returns the list of Results, each equal to track_pair's. The
+    pairs overlap on the engine's worker lanes."""
+    cfg, c = _prep_cfg(cfg)
+    eng = engine or default_engine()
+    items = list(items)
+    ins = (_abi.OfcPairIn * max(len(items), 1))()
+    outs = (OfcPairOut * max(len(items), 1))()
+    keep, arrs = [], []
+    for i, it in enumerate(items):
+        I1, I2 = it[0], it[1]
+        mask = it[2] if len(it) > 2 else None
+        init = it[3] if len(it) > 3 else None
+        a = _f32(I1)
+        h, w = a.shape
+        b = _f32(I2, (h, w))
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+        if m is not None and m.shape != (h, w):
+            raise ValueError(f"pair {i}: ROI mask shape {m.shape} differs from the image shape {(h, w)}")
+        u = v = None
+        if init is not None:
+            u, v = _f32(init[0], (h, w)), _f32(init[1], (h, w))
+        ins[i] = _abi.OfcPairIn(_ptr(a, c_float_p), _ptr(b, c_float_p), w, h, _ptr(m, c_u8_p), _ptr(u, c_float_p),
+                                _ptr(v, c_float_p))
+        keep.append((a, b, m, u, v))
+        o, arr = _pair_out(h, w)
+        outs[i] = o
+        arrs.append(arr)
+    eng._call("ofc_track_pairs", ins, len(items), ctypes.byref(c), outs)
+    return [_result(outs[i], arrs[i]) for i in range(len(items))]
+
+
 def finish(ux, uy, conf, cfg=None, mask=None, engine=None) -> Result:
     """track._finish (python/optflow_ref/track.py:56-108) without the crack options."""
     eng = engine or default_engine()
