@@ -350,7 +350,7 @@ void launch_warp(const float* c2, int w2, int h2, const double* sx, const double
 // root of |r1|^2 |r2|^2, with |r1|^2 formed from the pack; the 16 tap offsets are computed once and reused by every
 // filter; the field spline is stored interleaved (one 16-byte load per tap for both components).
 constexpr int ACC_BX = 32, ACC_BY = 4;
-__global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict__ ref4, const float2* __restrict__ R,
+__global__ void __launch_bounds__(128, 8) k_accumulate(const float4* __restrict__ ref4, const float2* __restrict__ R,
                                                       int F, int ph, int pw, const double* __restrict__ ux,
                                                       const double* __restrict__ uy, const double* __restrict__ sx,
                                                       const double* __restrict__ sy, const double2* __restrict__ cs,
@@ -385,16 +385,14 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
   Taps t;
   const bool ok = make_taps(px + PAD, py + PAD, pw, ph, t);
   float fwx[4], fwy[4];
-  int o16[16];
+  int ro[4], xo[4];  // tap (j, q) at ro[j] + xo[q] in a filter's plane
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     fwx[k] = (float)t.wx[k];
     fwy[k] = (float)t.wy[k];
+    ro[k] = t.yi[k] * pw;
+    xo[k] = t.xi[k];
   }
-#pragma unroll
-  for (int j = 0; j < 4; j++)
-#pragma unroll
-    for (int q = 0; q < 4; q++) o16[j * 4 + q] = t.yi[j] * pw + t.xi[q];
   const size_t plane = (size_t)ph * pw;
   const float fnan = __int_as_float(0x7fc00000);
   __pipeline_wait_prior(0);
@@ -405,6 +403,11 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
     float br = fnan, bi = fnan;
     if (ok) {
       const float2* Rk = R + (size_t)k * plane;
+      // the next filter's tap rows into L1 while this filter's taps and arithmetic run
+      if (k + 1 < F) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) asm volatile("prefetch.global.L1 [%0];" ::"l"(Rk + plane + (ro[j] + xo[0])));
+      }
       br = 0.f;
       bi = 0.f;
 #pragma unroll
@@ -412,7 +415,7 @@ __global__ void __launch_bounds__(128, 6) k_accumulate(const float4* __restrict_
         float are = 0.f, aim = 0.f;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-          const float2 c = __ldg(Rk + o16[j * 4 + q]);
+          const float2 c = __ldg(Rk + (ro[j] + xo[q]));
           are = fmaf(fwx[q], c.x, are);
           aim = fmaf(fwx[q], c.y, aim);
         }

@@ -8,4 +8,4 @@ from .config import Config  # noqa: F401
 from .api import (Engine, Flow, Grid, Result, coarse_flow, displacement_gradient, finish, refine,  # noqa: F401
                   refine_raw, refine_batch, strain_fields, track_pair, track_pairs, track_pair_device,
                   track_sequence, track_sequence_hybrid, local_affine_agreement)
-from .stream import pixel_format, save_result, to_gray, track_stream  # noqa: F401,E402
+from .stream import iter_frames, pixel_format, save_result, to_gray, track_stream  # noqa: F401,E402

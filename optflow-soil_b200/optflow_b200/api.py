@@ -85,9 +85,11 @@ _lock = threading.Lock()
 
 
 def default_engine(device=0):
+    """The module's engine on `device`, created on first use with two lanes: a frame source (iter_frames) may then
+    call the engine while a streamed sequence (track_stream) holds the other lane."""
     with _lock:
         if device not in _default:
-            _default[device] = Engine(device)
+            _default[device] = Engine(device, lanes=2)
         return _default[device]
 
 

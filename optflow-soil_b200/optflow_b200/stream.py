@@ -189,3 +189,63 @@ def save_result(out_dir, res, raw=False):
         np.save(os.path.join(out_dir, "fb.npy"), np.ascontiguousarray(res.fb, dtype="<i4"))
     with open(os.path.join(out_dir, "timing.json"), "w") as f:
         json.dump(res.timing, f, indent=2)
+
+
+def iter_frames(frames, start=0, stop=None, step=1, scale=1, tavg=0, align=False, cfg=None, mask_fn=None,
+                engine=None):
+    """io.iter_frames (python/optflow_ref/io.py:100-153) over an iterable of decoded frames (every frame of the
+    video or image list, from index 0): frames start, start + step, ... < stop, each turned grey and downscaled on
+    the GPU (to_gray). tavg = m > 0: each is the mean of frames i - m .. i + m (clipped to the input) after the
+    downscale (tavg.average_window on the GPU); a window that is one-sided because the input ends has its
+    neighbours aligned with the dense model and keep_unaligned, unless `align` aligns every window (affine model of
+    cfg, mask_fn(shape) the ROI of the fit)."""
+    import dataclasses
+
+    from .config import Config
+    from .tavg import average_window
+    if step < 1:
+        raise ValueError(f"step must be >= 1, got {step}")
+    if start < 0:
+        raise ValueError(f"start must be >= 0, got {start}")
+    if tavg < 0:
+        raise ValueError(f"tavg must be >= 0, got {tavg}")
+    m = int(tavg)
+    lo_read = max(0, start - m)
+    hi_read = None if stop is None else stop + m
+    if not m:
+        for i, f in enumerate(frames):
+            if stop is not None and i >= stop:
+                break
+            if i >= start and (i - start) % step == 0:
+                yield to_gray(f, scale, engine=engine)
+        return
+    cfg = cfg or Config()
+    edge_cfg = dataclasses.replace(cfg, tavg_model="dense")
+    buf = {}
+    nxt, last = start, -1
+
+    def emit(s):
+        lo, hi = max(0, s - m), min(s + m, last)
+        fr = [buf[i] for i in range(lo, hi + 1)]
+        if not align and s - lo != hi - s and min(fr[0].shape) >= edge_cfg.poc_win:
+            return average_window(fr, s - lo, True, edge_cfg, None, keep_unaligned=True, engine=engine)
+        return average_window(fr, s - lo, align, cfg, mask_fn(fr[0].shape) if align and mask_fn else None,
+                              engine=engine)
+
+    def due(i_ready):
+        return (stop is None or nxt < stop) and nxt <= i_ready
+
+    for i, f in enumerate(frames):
+        if i < lo_read:
+            continue
+        if hi_read is not None and i >= hi_read:
+            break
+        buf[i], last = to_gray(f, scale, engine=engine), i
+        while due(i - m):
+            yield emit(nxt)
+            nxt += step
+            for j in [j for j in buf if j < nxt - m]:
+                del buf[j]
+    while due(last):
+        yield emit(nxt)
+        nxt += step

@@ -121,3 +121,32 @@ def test_stream_errors_and_early_stop():
     p = track_pair(fr[0], fr[1], Config(), mask=gs["roi"].astype(bool))
     assert np.isfinite(p.ux).any()
     assert list(track_stream(fr[:1], Config())) == []
+
+
+def test_iter_frames_matches_the_reference():
+    """iter_frames (GPU grey levels, downscale and window means) against the reference's io.iter_frames on the same
+    frames (tests/golden/iter.npz): without averaging within float32 rounding; with averaging, the plain and the
+    dense-aligned edge windows and the affine-aligned ones within 2e-3 away from the border (the reference warps with
+    scipy's map_coordinates, the CLI and the engine with the B-spline of interp::warp; test_gpu_tavg.py)."""
+    from optflow_b200.stream import iter_frames
+    g = golden("iter")
+    fr = list(g["frames"])
+    mask = g["mask"].astype(bool)
+    cfg = Config(max_disp=8.0)
+    inner = (slice(20, -20), slice(20, -20))
+    plain = list(iter_frames(iter(fr), start=2, stop=9, step=3, scale=2))
+    assert len(plain) == len(g["plain"])
+    for a, b in zip(plain, g["plain"]):
+        assert np.abs(a - b).max() < 1e-6
+    for name, kw in (("edge", dict(start=1, step=3, scale=2, tavg=2, cfg=cfg)),
+                     ("aligned", dict(start=0, stop=7, step=2, scale=2, tavg=1, align=True, cfg=cfg,
+                                      mask_fn=lambda shape: mask))):
+        got = list(iter_frames(iter(fr), **kw))
+        assert len(got) == len(g[name]), name
+        for k, (a, b) in enumerate(zip(got, g[name])):
+            assert np.abs(a[inner] - b[inner]).max() < 2e-3, (name, k, np.abs(a[inner] - b[inner]).max())
+    with pytest.raises(ValueError, match="step must be >= 1"):
+        next(iter_frames(iter(fr), step=0))
+    # the averaged frames feed the streamed tracking as any frames do
+    res = dict(track_stream(iter_frames(iter(fr), start=1, step=3, scale=2, tavg=2, cfg=cfg), Config()))
+    assert sorted(res) == [1, 2] and all(np.isfinite(r.ux).any() for r in res.values())
