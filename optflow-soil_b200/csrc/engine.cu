@@ -318,13 +318,23 @@ struct Lane {
     auto it = plans.find(L);
     if (it != plans.end()) return it->second.first;
     FftPlan pl = fft_make_plan(L);
-    std::vector<float2> tw = fft_twiddles(L);
+    // twiddles of the stages' length, then (Bluestein) the chirp and the filter
+    std::vector<float2> tw = fft_twiddles(fft_work_len(pl));
+    const size_t ntw = tw.size();
+    if (pl.M) {
+      std::vector<float2> bt = fft_bluestein_tables(L, pl.M);
+      tw.insert(tw.end(), bt.begin(), bt.end());
+    }
     std::unique_ptr<DevBuf> b(new DevBuf());
     size_t b32 = tw.size() * sizeof(float2);
     OFC_CUDA(cudaMalloc(&b->p, b32));
     b->bytes = b32;
     OFC_CUDA(cudaMemcpy(b->p, tw.data(), b32, cudaMemcpyHostToDevice));
     pl.tw = (const float2*)b->p;
+    if (pl.M) {
+      pl.chirp = pl.tw + ntw;
+      pl.filt = pl.chirp + L;
+    }
     auto& slot = plans[L];
     slot.first = pl;
     slot.second = std::move(b);
@@ -913,10 +923,10 @@ void check_sizes(size_t w, size_t h) {
 void check_fine_window(size_t w, size_t h, const ofc_config& c) {
   check_sizes(w, h);
   int pw = (int)w + 2 * PAD, ph = (int)h + 2 * PAD;
-  if (!fft_supported(pw) || !fft_supported(ph))
+  if (fft_work_length(pw) == 0 || fft_work_length(ph) == 0)
     throw Error(OFC_ERR_WINDOW, "window " + std::to_string(w) + "x" + std::to_string(h) +
-                                    ": padded FFT size " + std::to_string(pw) + "x" + std::to_string(ph) +
-                                    " has a prime factor above 31, which the CUDA engine does not transform");
+                                    ": no FFT plan for the padded size " + std::to_string(pw) + "x" +
+                                    std::to_string(ph));
   if (!fft_fits(ph, pw))
     throw Error(OFC_ERR_WINDOW, "window " + std::to_string(w) + "x" + std::to_string(h) +
                                     " exceeds the shared-memory FFT passes of the CUDA engine");
@@ -2738,7 +2748,7 @@ extern "C" {
 
 int ofc_test_fft_lines(ofc_engine* e, float* data, size_t lines, size_t L, int inverse, char* err, size_t errlen) {
   return guarded(e, err, errlen, [&](Lane& Ln) {
-    if (!fft_supported((int)L)) throw Error(OFC_ERR_ARG, "unsupported FFT length");
+    if (fft_work_length((int)L) == 0) throw Error(OFC_ERR_ARG, "unsupported FFT length");
     const FftPlan& pl = Ln.plan((int)L);
     float2* d = Ln.upload("t_fft", (const float2*)data, lines * L);
     launch_fft_lines(d, (int)lines, pl, inverse != 0, Ln.stream);

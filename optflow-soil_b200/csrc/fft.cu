@@ -32,19 +32,86 @@ bool fft_supported(int L) {
   return m == 1;
 }
 
+static int stage_count(int m) {
+  int n = 0;
+  while (m % 8 == 0) { n++; m /= 8; }
+  while (m % 4 == 0) { n++; m /= 4; }
+  while (m % 2 == 0) { n++; m /= 2; }
+  for (int p : {3, 5, 7, 11, 13, 17, 19, 23, 29, 31})
+    while (m % p == 0) { n++; m /= p; }
+  return n;
+}
+
+int fft_work_length(int L) {
+  if (L < 1) return 0;
+  if (fft_supported(L)) return stage_count(L) <= FFT_MAXST ? L : 0;
+  // Bluestein: the smallest 2^a 3^b 5^c 7^d >= 2L - 1
+  for (int M = 2 * L - 1; M <= 8 * L; M++) {
+    int m = M;
+    for (int p : {2, 3, 5, 7})
+      while (m % p == 0) m /= p;
+    if (m == 1) return stage_count(M) <= FFT_MAXST ? M : 0;
+  }
+  return 0;
+}
+
+std::vector<float2> fft_bluestein_tables(int L, int M) {
+  // chirp w[n] = exp(-i pi n^2 / L): the phase from n^2 mod 2L in integers, then float64
+  std::vector<double> wr(L), wi(L);
+  for (int n = 0; n < L; n++) {
+    const long long q = ((long long)n * n) % (2LL * L);
+    const double a = -PI * (double)q / (double)L;
+    wr[n] = std::cos(a);
+    wi[n] = std::sin(a);
+  }
+  // b = conj(w) wrapped to length M; filt = DFT_M(b) / M in float64 (a direct sum with an integer-indexed table)
+  std::vector<double> br(M, 0.0), bi(M, 0.0), cr(M), ci(M);
+  for (int n = 0; n < L; n++) {
+    br[n] = wr[n];
+    bi[n] = -wi[n];
+    if (n) {
+      br[M - n] = wr[n];
+      bi[M - n] = -wi[n];
+    }
+  }
+  for (int t = 0; t < M; t++) {
+    const double a = -2.0 * PI * (double)t / (double)M;
+    cr[t] = std::cos(a);
+    ci[t] = std::sin(a);
+  }
+  std::vector<float2> out((size_t)L + M);
+  for (int n = 0; n < L; n++) out[n] = make_float2((float)wr[n], (float)wi[n]);
+  for (int k = 0; k < M; k++) {
+    double sr = 0.0, si = 0.0;
+    long long idx = 0;
+    for (int n = 0; n < M; n++) {
+      if (br[n] != 0.0 || bi[n] != 0.0) {
+        sr += br[n] * cr[idx] - bi[n] * ci[idx];
+        si += br[n] * ci[idx] + bi[n] * cr[idx];
+      }
+      idx += k;
+      if (idx >= M) idx -= M;
+    }
+    out[(size_t)L + k] = make_float2((float)(sr / M), (float)(si / M));
+  }
+  return out;
+}
+
 FftPlan fft_make_plan(int L) {
-  if (!fft_supported(L))
-    throw Error(OFC_ERR_WINDOW, "FFT length " + std::to_string(L) + " has a prime factor above 31");
+  const int work = fft_work_length(L);
+  if (work == 0) throw Error(OFC_ERR_WINDOW, "no FFT plan for length " + std::to_string(L));
   FftPlan pl;
   pl.L = L;
-  int m = L;
+  pl.M = work == L ? 0 : work;
+  int m = work;
   std::vector<int> f;
   while (m % 8 == 0) { f.push_back(8); m /= 8; }
   while (m % 4 == 0) { f.push_back(4); m /= 4; }
   while (m % 2 == 0) { f.push_back(2); m /= 2; }
   for (int p : {3, 5, 7, 11, 13, 17, 19, 23, 29, 31})
     while (m % p == 0) { f.push_back(p); m /= p; }
-  if ((int)f.size() > FFT_MAXST) throw Error(OFC_ERR_WINDOW, "FFT length " + std::to_string(L) + " needs too many stages");
+  if ((int)f.size() > FFT_MAXST || m != 1)
+    throw Error(OFC_ERR_WINDOW, "FFT length " + std::to_string(L) + " needs too many stages");
   int s = 1;
   pl.nst = (int)f.size();
   for (int i = 0; i < pl.nst; i++) {
@@ -457,25 +524,67 @@ __device__ __forceinline__ void fft_stage(const C2* __restrict__ A, C2* __restri
 // runs the plan on buf (tmp: scratch of the same capacity, fft_buf_len(L, C)); buf holds the input unpadded
 // and the returned buffer the result unpadded. FIXL > 0: the length is FIXL and the plan is fixed at compile time
 // (kernels are instantiated per FIXL, so that a fixed-length kernel carries no runtime-plan code and its registers).
-template <int FIXL, int C, class C2>
-__device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
-  static_assert(C == 1 || C == 2 || C == 4, "C: a power of two up to 4");
-  static_assert(sizeof(C2) == sizeof(float2), "float32 transforms");
-  C2* a = buf;
-  C2* b = tmp;
-  const C2* tw = (const C2*)pl.tw;
+// the plan's stages on their length SL (L, or Bluestein's M): a holds the input unpadded, the returned buffer the
+// result unpadded
+template <int C, class C2>
+__device__ C2* fft_stages(C2* a, C2* b, const FftPlan& pl, int SL, bool inv) {
   constexpr int lc = C == 4 ? 2 : (C == 2 ? 1 : 0);
-  if constexpr (FIXL > 0) return fft_run_fixed<FIXL, C, 0, C2>(buf, tmp, tw, inv);
+  const C2* tw = (const C2*)pl.tw;
   int ish = 31;
   for (int st = 0; st < pl.nst; st++) {
     const int osh = (st + 1 < pl.nst && pl.s[st] * C < 32) ? FFT_PAD : 31;
-    fft_stage<C2>(a, b, lc, pl.L, pl.p[st], pl.s[st], pl.magic[st], tw, inv, ish, osh);
+    fft_stage<C2>(a, b, lc, SL, pl.p[st], pl.s[st], pl.magic[st], tw, inv, ish, osh);
     ish = osh;
     C2* t = a;
     a = b;
     b = t;
   }
   return a;
+}
+
+// Bluestein (the plan's M > 0): X_k = w_k sum_n (x_n w_n) conj(w_{k - n}), w_n = exp(-i pi n^2 / L), the convolution
+// cyclic over M >= 2L - 1 by two length-M transforms; the inverse transform as conj(forward(conj(x))). buf and tmp
+// hold fft_buf_len(M, C) values each.
+template <int C, class C2>
+__device__ __forceinline__ C2* fft_bluestein(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
+  constexpr int lc = C == 4 ? 2 : (C == 2 ? 1 : 0);
+  const int L = pl.L, M = pl.M;
+  const float2* w = pl.chirp;
+  const float2* f = pl.filt;
+  for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
+    const int i = idx >> lc;
+    float2 v = make_float2(0.f, 0.f);
+    if (i < L) {
+      v = buf[idx];
+      if (inv) v.y = -v.y;
+      v = cmul(v, __ldg(w + i));
+    }
+    buf[idx] = v;
+  }
+  __syncthreads();
+  C2* r = fft_stages<C, C2>(buf, tmp, pl, M, false);
+  for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) r[idx] = cmul(r[idx], __ldg(f + (idx >> lc)));
+  __syncthreads();
+  C2* q = fft_stages<C, C2>(r, r == buf ? tmp : buf, pl, M, true);
+  for (int idx = threadIdx.x; idx < L * C; idx += blockDim.x) {
+    float2 v = cmul(q[idx], __ldg(w + (idx >> lc)));
+    if (inv) v.y = -v.y;
+    q[idx] = v;
+  }
+  __syncthreads();
+  return q;
+}
+
+template <int FIXL, int C, class C2>
+__device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
+  static_assert(C == 1 || C == 2 || C == 4, "C: a power of two up to 4");
+  static_assert(std::is_same<C2, float2>::value, "float32 transforms");
+  if constexpr (FIXL > 0) {
+    return fft_run_fixed<FIXL, C, 0, C2>(buf, tmp, (const C2*)pl.tw, inv);
+  } else {
+    if (pl.M) return fft_bluestein<C, C2>(buf, tmp, pl, inv);
+    return fft_stages<C, C2>(buf, tmp, pl, pl.L, inv);
+  }
 }
 
 // z^e, 0 <= e < 64, of the B-spline pole z = sqrt(3) - 2 (interp.py:9): the product of its binary powers z^(2^b),
@@ -584,7 +693,7 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_fwd_real(const float* 
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* sm = (float2*)smraw;
   const int pw = FIXL ? FIXL : plw.L;
-  float2* t = sm + fft_buf_len(pw, 1);
+  float2* t = sm + fft_buf_len(FIXL ? FIXL : fft_work_len(plw), 1);
   const int yp = blockIdx.x;
   const int ys = reflect_near(yp - PAD, H);
   const float* row = img + (size_t)ys * W;
@@ -607,7 +716,7 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_fwd(const float2* Tin
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* A = (float2*)smraw;
   const int ph = FIXL ? FIXL : plh.L, n = ph * C;
-  float2* B = A + fft_buf_stride(ph, C);  // 16-byte aligned: the result may be either buffer
+  float2* B = A + fft_buf_stride(FIXL ? FIXL : fft_work_len(plh), C);  // 16-byte aligned: the result may be either buffer
   const int x0 = blockIdx.x * C;
   // C = 2 with an even row pitch: each row of the pair is 16 bytes on a 16-byte boundary, copied asynchronously
   const bool rows16 = C == 2 && pw % 2 == 0;
@@ -681,7 +790,7 @@ __global__ void __launch_bounds__(pair_threads<REFPACK>(FIXL), 2) k_fft_cols_pai
   const int ph = FIXL ? FIXL : plh.L, n = ph * C, tid = threadIdx.x, nt = blockDim.x;
   float2* raw = (float2*)smraw;
   float2* A = raw + n;
-  float2* B = A + fft_buf_stride(ph, C);
+  float2* B = A + fft_buf_stride(FIXL ? FIXL : fft_work_len(plh), C);
   const int x0 = blockIdx.x * C;
   const bool rows16 = x0 + 1 < pw && pw % 2 == 0;  // each row of the pair is 16 bytes on a 16-byte boundary
   if (rows16) {
@@ -756,7 +865,7 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const floa
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* A = (float2*)smraw;
   const int ph = plh.L, n = ph * C;
-  float2* B = A + fft_buf_len(ph, C);
+  float2* B = A + fft_buf_len(fft_work_len(plh), C);
   const int x0 = blockIdx.x * C;
   const int k = REFPACK ? k0 + blockIdx.y / 3 : blockIdx.y, var = REFPACK ? blockIdx.y % 3 : 0;
   const float* exkf = g.exf + (size_t)k * pw;
@@ -799,7 +908,7 @@ template <int FIXL>
 __global__ void __launch_bounds__(FIXL ? 288 : FFT_TMAX, FIXL ? 3 : 2)
     k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int nlines, float scale, float2* __restrict__ R) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int L = FIXL ? FIXL : plw.L, nb = fft_buf_stride(L, 1);
+  const int L = FIXL ? FIXL : plw.L, nb = fft_buf_stride(FIXL ? FIXL : fft_work_len(plw), 1);
   float2* in = (float2*)smraw;
   float2* tmp = in + nb;
   float2* pre = tmp + nb;
@@ -845,7 +954,7 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_ref(const float2* 
                                                                float* __restrict__ amp) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* sm = (float2*)smraw;
-  const int pw = FIXL ? FIXL : plw.L, nb = fft_buf_stride(pw, 1);
+  const int pw = FIXL ? FIXL : plw.L, nb = fft_buf_stride(FIXL ? FIXL : fft_work_len(plw), 1);
   float2* t = sm + 3 * nb;
   const int y = blockIdx.x, kk = blockIdx.y, k = k0 + kk;  // y: row of the W x H crop
   const size_t plane = (size_t)ph * pw;
@@ -896,7 +1005,7 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_lines(float2* data, FftPlan
   float2* row = data + (size_t)blockIdx.x * L;
   for (int x = threadIdx.x; x < L; x += blockDim.x) sm[x] = row[x];
   __syncthreads();
-  float2* r = fft_run<FIXL, 1>(sm, sm + fft_buf_len(L, 1), pl, inv != 0);
+  float2* r = fft_run<FIXL, 1>(sm, sm + fft_buf_len(FIXL ? FIXL : fft_work_len(pl), 1), pl, inv != 0);
   for (int x = threadIdx.x; x < L; x += blockDim.x) row[x] = r[x];
 }
 
@@ -915,8 +1024,11 @@ static size_t smem_prefilter(int L, int C, int T) {
   (void)T;
   return std::max<size_t>(2 * fbytes(L, C), fbytes(L, C) + 16 + (size_t)C * sizeof(float4));
 }
-// k_fft_cols_pair: the column pair and two buffers at the even stride
-static size_t smem_cols_pair(int L) { return ((size_t)2 * L + 2 * (size_t)fft_buf_stride(L, 2)) * sizeof(float2); }
+// k_fft_cols_pair: the column pair (2 L values) and two buffers of the work length (L, or Bluestein's M) at the even
+// stride
+static size_t smem_cols_pair(int L, int WL) {
+  return ((size_t)2 * L + 2 * (size_t)fft_buf_stride(WL, 2)) * sizeof(float2);
+}
 // k_fft_rows_inv_resp: three buffers at the even stride
 static size_t smem_rows_resp(int L) { return 3 * (size_t)fft_buf_stride(L, 1) * sizeof(float2); }
 
@@ -938,17 +1050,19 @@ static int persistent_blocks(const void* fn, int threads, size_t smem, int work)
 
 bool fft_fits(int ph, int pw) {
   try {
-    int Tc = std::min(fft_threads(ph, 2), COLS_TMAX);
-    if (smem_prefilter(ph, 2, Tc) > SMEM_MAX || 2 * (size_t)fft_buf_stride(ph, 2) * sizeof(float2) > SMEM_MAX) return false;
-    return 4 * (size_t)fft_buf_stride(pw, 1) * sizeof(float2) <= SMEM_MAX && smem_rows_resp(pw) <= SMEM_MAX;
+    const int wh = fft_work_length(ph), ww = fft_work_length(pw);
+    if (wh == 0 || ww == 0) return false;
+    int Tc = std::min(fft_threads(wh, 2), COLS_TMAX);
+    if (smem_prefilter(wh, 2, Tc) > SMEM_MAX || 2 * (size_t)fft_buf_stride(wh, 2) * sizeof(float2) > SMEM_MAX) return false;
+    return 4 * (size_t)fft_buf_stride(ww, 1) * sizeof(float2) <= SMEM_MAX && smem_rows_resp(ww) <= SMEM_MAX;
   } catch (const Error&) {
     return false;
   }
 }
 
 void launch_fft_rows_fwd_real(const float* img, int W, int H, const FftPlan& plw, int ph, float2* out, cudaStream_t st) {
-  int T = fft_threads(plw.L, 1);
-  size_t sm = 2 * fbytes(plw.L, 1);
+  int T = fft_threads(fft_work_len(plw), 1);
+  size_t sm = 2 * fbytes(fft_work_len(plw), 1);
   by_length(plw.L, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
     set_smem((const void*)k_fft_rows_fwd_real<FL>, sm);
@@ -958,9 +1072,9 @@ void launch_fft_rows_fwd_real(const float* img, int W, int H, const FftPlan& plw
 
 static void cols_fwd(float2* T, const FftPlan& plh, int pw, cudaStream_t st) {
   constexpr int C = 2;
-  const int ph = plh.L;
-  int nt = std::min(fft_threads(ph, C), COLS_TMAX);
-  size_t sm_f = 2 * (size_t)fft_buf_stride(ph, C) * sizeof(float2);
+  const int ph = plh.L, wh = fft_work_len(plh);
+  int nt = std::min(fft_threads(wh, C), COLS_TMAX);
+  size_t sm_f = 2 * (size_t)fft_buf_stride(wh, C) * sizeof(float2);
   // in place: a block reads its C columns whole before it writes their spectrum back
   by_length(ph, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
@@ -975,9 +1089,9 @@ template <bool REFPACK>
 static void cols_inverse(const float2* S, const FftPlan& plh, int pw, const GaborTables& g, int k0, int k1, float2* U,
                          cudaStream_t st) {
   constexpr int C = 2;
-  const int ph = plh.L;
-  int nt = std::min(fft_threads(ph, C), COLS_TMAX);
-  const size_t sm_p = smem_cols_pair(ph);
+  const int ph = plh.L, wh = fft_work_len(plh);
+  int nt = std::min(fft_threads(wh, C), COLS_TMAX);
+  const size_t sm_p = smem_cols_pair(ph, wh);
   if (sm_p <= SMEM_MAX) {
     if (ph == FFT_FIXED_L) nt = pair_threads<REFPACK>(ph);  // the block size the fixed-length kernel assumes
     dim3 grid(div_up(pw, C), REFPACK ? 3 : div_up(g.F, RESP_G));
@@ -989,7 +1103,7 @@ static void cols_inverse(const float2* S, const FftPlan& plh, int pw, const Gabo
     });
     return;
   }
-  size_t sm_i = REFPACK ? 2 * fbytes(ph, C) : smem_prefilter(ph, C, nt);
+  size_t sm_i = REFPACK ? 2 * fbytes(wh, C) : smem_prefilter(wh, C, nt);
   if (sm_i > SMEM_MAX) throw Error(OFC_ERR_WINDOW, "padded height " + std::to_string(ph) + " too large for the column pass");
   set_smem((const void*)k_fft_cols_inv_filter<C, REFPACK>, sm_i);
   dim3 grid(div_up(pw, C), REFPACK ? 3 * (k1 - k0) : g.F);
@@ -1003,8 +1117,8 @@ void launch_fft_cols_filters(float2* T, const FftPlan& plh, int pw, const GaborT
 }
 
 void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F, float2* R, cudaStream_t st) {
-  int T = fft_threads(plw.L, 1);
-  size_t sm = smem_rows_resp(plw.L);
+  int T = fft_threads(fft_work_len(plw), 1);
+  size_t sm = smem_rows_resp(fft_work_len(plw));
   float scale = (float)(36.0 / ((double)ph * (double)plw.L));
   const int nlines = F * ph;
   by_length(plw.L, [&](auto fl) {
@@ -1024,8 +1138,8 @@ void launch_fft_cols_ref_f32(const float2* S, const FftPlan& plh, int pw, const 
 
 void launch_fft_rows_inv_ref_f32(const float2* U, const FftPlan& plw, int ph, int k0, int k1, int W, int H,
                                  float4* ref4, float* amp, cudaStream_t st) {
-  int T = fft_threads(plw.L, 1);
-  size_t sm = 4 * (size_t)fft_buf_stride(plw.L, 1) * sizeof(float2);
+  int T = fft_threads(fft_work_len(plw), 1);
+  size_t sm = 4 * (size_t)fft_buf_stride(fft_work_len(plw), 1) * sizeof(float2);
   dim3 grid(H, k1 - k0);
   by_length(plw.L, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
@@ -1035,8 +1149,8 @@ void launch_fft_rows_inv_ref_f32(const float2* U, const FftPlan& plw, int ph, in
 }
 
 void launch_fft_lines(float2* data, int lines, const FftPlan& pl, bool inverse, cudaStream_t st) {
-  int T = fft_threads(pl.L, 1);
-  size_t sm = 2 * fbytes(pl.L, 1);
+  int T = fft_threads(fft_work_len(pl), 1);
+  size_t sm = 2 * fbytes(fft_work_len(pl), 1);
   by_length(pl.L, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
     set_smem((const void*)k_fft_lines<FL>, sm);

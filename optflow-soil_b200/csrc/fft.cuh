@@ -11,6 +11,10 @@ constexpr int FFT_TMAX = 512;  // threads per block at most
 
 // A 1-D plan of length L: mixed-radix Stockham stages (radix p[i], stride s[i] = product of the radices
 // before it) and the twiddle table W[t] = exp(-2 pi i t / L), t < L, rounded from float64.
+// A length with a prime factor above 31 is transformed by Bluestein's chirp z-transform (as the reference's Metal
+// FFT does, rust/crates/optflow-gpu/src/fft.rs:1-3): M > 0 is then the inner length (the smallest 2^a 3^b 5^c 7^d
+// >= 2L - 1), the stages and tw are those of length M, chirp[n] = exp(-i pi n^2 / L) for n < L, and filt is the
+// length-M transform of the conjugate chirp (wrapped: index m and M - m for m < L) times 1 / M.
 struct FftPlan {
   int L = 0;
   int nst = 0;
@@ -18,15 +22,25 @@ struct FftPlan {
   int s[FFT_MAXST] = {};
   unsigned magic[FFT_MAXST] = {};
   const float2* tw = nullptr;
+  int M = 0;
+  const float2* chirp = nullptr;
+  const float2* filt = nullptr;
 };
 
-// radices with a register-resident butterfly; a length with any other prime factor is refused
+// the length the stages of L's plan run on (and the shared-memory buffers are sized for): L, or Bluestein's M
+__host__ __device__ inline int fft_work_len(const FftPlan& p) { return p.M ? p.M : p.L; }
+
+// radices with a register-resident butterfly: the lengths transformed directly
 bool fft_supported(int L);
+// the stages' length of a plan of L (L itself, or Bluestein's inner length); 0 when no plan exists
+int fft_work_length(int L);
 // whether the column and row passes of a ph x pw padded window fit in shared memory
 bool fft_fits(int ph, int pw);
-// host: factor L and fill p/s; tw is set by the caller (device table of L values)
+// host: factor L (or Bluestein's M) and fill p/s; the caller sets tw (fft_twiddles(fft_work_length(L))) and, for
+// Bluestein, chirp and filt (fft_bluestein_tables: L chirp values, then M filter values)
 FftPlan fft_make_plan(int L);
 std::vector<float2> fft_twiddles(int L);
+std::vector<float2> fft_bluestein_tables(int L, int M);
 // threads of a block that transforms C interleaved lines of length L (multiple of C and of 32)
 int fft_threads(int L, int C);
 

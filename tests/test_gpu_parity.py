@@ -143,6 +143,19 @@ def test_track_pair_oracle(oracle, n, seed):
     compare_pair(r, want, f"oracle{n}")
 
 
+def test_track_pair_bluestein_sizes(oracle):
+    """A pair whose padded sizes have prime factors above 31 (127 x 100 -> 191 x 164 = 191 x 4 * 41: every transform
+    through Bluestein's chirp z-transform) against the oracle with the pair bars; a 960 x 540 frame (padded height
+    604 = 4 * 151, the CLI's 1920 x 1080 video at --scale 2) passes check_window."""
+    from optflow_b200.api import default_engine
+    a, b = _synthetic_pair(192, 21)
+    a, b = a[20:120, 30:157], b[20:120, 30:157]
+    want = oracle.track_pair(a, b, Config())
+    r = track_pair(a, b, Config())
+    compare_pair(r, want, "bluestein 127x100")
+    default_engine().check_window(960, 540, Config())
+
+
 def test_refine_raw_window_shift(oracle):
     """refine_raw on a window of a larger pair (FineEngine::refine_raw with a shift) equals refine on the crop
     when the second image's window covers the displaced positions."""
@@ -182,9 +195,10 @@ def test_refine_batch_equals_refine_raw():
     z = np.zeros((0, 0), np.float32)
     with pytest.raises(ValueError, match="window 1: empty"):
         refine_batch(wins[:1] + [(z, z, z, z, (0, 0))], Config())
-    p45 = np.zeros((45, 45), np.float32)  # padded 109: a prime above 31
+    # padded height 4099, a prime: Bluestein's inner length 8232 leaves no room for the column pass in shared memory
+    tall = np.zeros((4035, 45), np.float32)
     with pytest.raises(EngineError, match="window 2"):
-        refine_batch(wins[:2] + [(p45, p45, p45, p45, (0, 0))], Config())
+        refine_batch(wins[:2] + [(tall, tall, tall, tall, (0, 0))], Config())
 
 
 def test_track_pair_graph_replay_and_device_api():

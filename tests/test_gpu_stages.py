@@ -18,15 +18,23 @@ def T():
     return testing
 
 
-@pytest.mark.parametrize("L", [64, 128, 160, 192, 224, 320, 576, 832, 1088, 1152, 2112, 2*3*5*7*11, 3*17*19, 23*29, 31*8])
+# direct plans (radices up to 31), then lengths with a larger prime factor (Bluestein: 37, 41 * 4, 2 * 53, 151 * 4 =
+# the padded height of a 960 x 540 frame, the primes 191 and 1021, 1999 = the largest inner length here, 4000)
+BLUESTEIN = [37, 164, 106, 604, 191, 1021, 1999]
+
+
+@pytest.mark.parametrize("L", [64, 128, 160, 192, 224, 320, 576, 832, 1088, 1152, 2112, 2*3*5*7*11, 3*17*19, 23*29, 31*8]
+                         + BLUESTEIN)
 def test_fft_lines_match_numpy(T, L):
+    """Line transforms against numpy in float64: 2e-6 of the largest output for the direct plans, 1e-5 for
+    Bluestein's (a float32 chirp, two transforms of the inner length and a product between them)."""
     rng = np.random.default_rng(L)
     a = (rng.standard_normal((5, L)) + 1j * rng.standard_normal((5, L))).astype(np.complex64)
     for inv in (False, True):
         got = T.fft_lines(a, inverse=inv)
         ref = np.fft.ifft(a.astype(np.complex128), axis=1) * L if inv else np.fft.fft(a.astype(np.complex128), axis=1)
         err = np.abs(got - ref).max() / np.abs(ref).max()
-        assert err < 2e-6, (L, inv, err)
+        assert err < (1e-5 if L in BLUESTEIN else 2e-6), (L, inv, err)
 
 
 def test_reference_phase(T):
