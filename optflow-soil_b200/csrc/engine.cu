@@ -1516,9 +1516,14 @@ size_t pixel_bytes(int32_t pixel) {
 
 // to_gray + downscale of a device image of w_in x (H * scale) or more rows into the W x H float32 plane out
 void to_gray_dev(Lane& L, const uint8_t* px, int32_t pixel, int w_in, int scale, int W, int H, float* out) {
-  static double lut[256];
-  for (int v = 0; v < 256; v++) lut[v] = v / 255.0;  // lut8 (io.rs:50-52)
-  const double* lut8 = L.cached("lut8", lut, 256);
+  const double* lut8 = nullptr;
+  if (L.has_const("lut8")) {
+    lut8 = L.cached<double>("lut8", nullptr, 256);
+  } else {
+    double lut[256];
+    for (int v = 0; v < 256; v++) lut[v] = v / 255.0;  // lut8 (io.rs:50-52)
+    lut8 = L.cached("lut8", lut, 256);
+  }
   const dim3 g(div_up(W, 128), H);
   cudaStream_t st = L.stream;
   switch (pixel) {
