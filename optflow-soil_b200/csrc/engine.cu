@@ -2353,12 +2353,39 @@ int64_t run_sequence(Lane& L, const SeqIO& io) {
   }
   bool have_prev = false, have_padj = false;
   int64_t ref_idx = 0;
+  // hybrid: the adjacent leg k - 1 -> k runs on a worker lane beside the direct leg when the previous frame needed
+  // one (its inputs are known before the direct leg: prev, fk and the previous adjacent field as the start); it is
+  // used only where the reference's rule asks for it (track.py:452-457), so the results are those of the legs run
+  // one after the other
+  Lane* A = nullptr;
+  if (io.hybrid && !io.leg) {
+    if (L.aux.empty()) {
+      std::unique_ptr<Lane> a(new Lane());
+      lane_init(*a);
+      L.aux.push_back(std::move(a));
+    }
+    A = L.aux[0].get();
+  }
+  cudaEvent_t spec_ready = L.bev[4], spec_taken = L.bev[5], spec_done = L.bev[6];
   next = fetch(1);
   while (next) {
     load(next, (int)(k & 1), fk);
     fetched = false;
     next = nullptr;
     const double ruc = io.ruc(k);
+    bool spec = false;
+    if (A && ref_idx != k - 1 && have_padj) {
+      spec = true;
+      OFC_CUDA(cudaEventRecord(spec_ready, st));
+      OFC_CUDA(cudaStreamWaitEvent(A->stream, spec_ready, 0));
+      OFC_CUDA(cudaMemcpyAsync(A->get<float>("in_i1", N), prev, N * 4, cudaMemcpyDeviceToDevice, A->stream));
+      OFC_CUDA(cudaMemcpyAsync(A->get<float>("in_i2", N), fk, N * 4, cudaMemcpyDeviceToDevice, A->stream));
+      OFC_CUDA(cudaMemcpyAsync(A->get<float>("in_u", N), padj, N * 4, cudaMemcpyDeviceToDevice, A->stream));
+      OFC_CUDA(cudaMemcpyAsync(A->get<float>("in_v", N), padj + N, N * 4, cudaMemcpyDeviceToDevice, A->stream));
+      OFC_CUDA(cudaEventRecord(spec_taken, A->stream));
+      run_pair(*A, W, H, false, true, c, true, 2);
+      OFC_CUDA(cudaEventRecord(spec_done, A->stream));
+    }
     std::pair<double, double> t = leg(ref, ref_idx, fk, k, have_prev ? praw : nullptr, true);
     double cmean = leg_mean();
     if (cmean < ruc && ref_idx != k - 1) {
@@ -2396,11 +2423,24 @@ int64_t run_sequence(Lane& L, const SeqIO& io) {
                  nfb, droi, W, H, cm, io.hy.fb_max, ref_idx + 1 < k ? 1 : 0, cxy, cxy + N, legc, link, fl, dany);
       read_any();
       const float *arx = nullptr, *ary = nullptr, *acf = nullptr;
+      if (spec) OFC_CUDA(cudaStreamWaitEvent(st, spec_taken, 0));  // padj and prev may change from here on
       if (any[0]) {
         if (ref_idx == k - 1) {  // the direct leg is the adjacent leg
           arx = praw;
           ary = praw + N;
           acf = pconf;
+        } else if (spec) {  // the worker lane's leg (the same inputs as the leg below)
+          OFC_CUDA(cudaStreamWaitEvent(st, spec_done, 0));
+          const ofc_pair_out da = device_pair_out(*A, N);
+          float ms0 = 0, ms1 = 0;  // the two stages of the worker's leg (run_pair records ev[0], ev[1], ev[3])
+          OFC_CUDA(cudaEventSynchronize(A->ev[3]));
+          OFC_CUDA(cudaEventElapsedTime(&ms0, A->ev[0], A->ev[1]));
+          OFC_CUDA(cudaEventElapsedTime(&ms1, A->ev[1], A->ev[3]));
+          t.first += ms0 * 1e-3;
+          t.second += ms1 * 1e-3;
+          arx = da.raw_ux;
+          ary = da.raw_uy;
+          acf = da.conf;
         } else {
           const std::pair<double, double> ta = leg(prev, k - 1, fk, k, have_padj ? padj : nullptr, false);
           t.first += ta.first;
