@@ -1,0 +1,51 @@
+"""The CPU-runnable benchmark sequence (five uint8 256 x 256 frames, uniform strain exx = 0.005 k about the centre
+plus a 0.8 k px translation, noise 0.005, chain mode, defaults, no ROI) against the reference's own track_sequence
+(tests/golden/config1.npz, written by tests/golden/make_golden_config1.py): every frame within the pair bars
+(fields 1e-3 px on the pixels valid in both, validity flips only near conf_min or within the guard distance of such
+a pixel, strain 1e-5 on every second row and column), the reference index exactly, the mean confidence within 1e-3.
+The uint8 frames through the streamed driver (grey levels on the GPU) give the array entry's results bit for bit."""
+import numpy as np
+import pytest
+from conftest import golden, rms
+from scipy.ndimage import binary_dilation
+from test_gpu_parity import DISP_TOL, STRAIN_TOL
+
+from optflow_b200 import Config, track_sequence
+from optflow_b200.stream import track_stream
+
+pytestmark = pytest.mark.gpu
+
+
+def test_config1_sequence_against_the_reference():
+    g = golden("config1")
+    u8 = list(g["frames"])
+    grey = [np.float32(f.astype(np.float64) / 255.0) for f in u8]
+    cfg = Config()
+    res = dict(track_sequence(grey, cfg))
+    assert sorted(res) == [1, 2, 3, 4]
+    cmin, guard = cfg.conf_min, int(np.ceil(cfg.edge_guard_px())) + 1
+    for k, r in res.items():
+        p = f"f{k}_"
+        vg, vw = np.isfinite(r.ux), np.isfinite(g[p + "ux"])
+        diff = vg != vw
+        near = binary_dilation(np.abs(g[p + "conf"].astype(np.float64) - cmin) < 0.02, iterations=guard)
+        assert (diff & ~near).sum() == 0 and diff.mean() < 0.01, (k, diff.mean())
+        both = vg & vw
+        assert both.mean() > 0.5, k
+        assert rms(r.ux, g[p + "ux"], both) < DISP_TOL and rms(r.uy, g[p + "uy"], both) < DISP_TOL, k
+        assert rms(r.conf, g[p + "conf"]) < DISP_TOL, k
+        # the true field: exx = 0.005 k about x = 128 plus 0.8 k px
+        xx = np.arange(256)[None, :].repeat(256, 0)
+        true_ux = 0.8 * k + 0.005 * k * (xx - 128) / (1 + 0.005 * k)
+        assert rms(r.ux, true_ux, both) < 0.05, k
+        sub = both[::2, ::2]
+        for q in ("Exx", "Eyy", "Exy", "gmax", "vol"):
+            a, b = r.strain[q][::2, ::2], g[p + q]
+            m = sub & np.isfinite(a) & np.isfinite(b)
+            assert rms(a, b, m) < STRAIN_TOL, (k, q)
+        ref_idx, mean_conf = g[p + "meta"]
+        assert r.timing["reference"] == int(ref_idx) and abs(r.timing["mean_conf"] - mean_conf) < 1e-3, k
+    streamed = dict(track_stream(u8, cfg))
+    for k in res:
+        for q in ("ux", "uy", "conf", "raw_ux", "raw_uy"):
+            np.testing.assert_array_equal(getattr(streamed[k], q), getattr(res[k], q), err_msg=f"{k} {q}")
