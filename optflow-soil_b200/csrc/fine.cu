@@ -349,20 +349,20 @@ void launch_warp(const float* c2, int w2, int h2, const double* sx, const double
 // copied to shared memory asynchronously at the start (in flight during the fixed point); |r1| |r2| is one square
 // root of |r1|^2 |r2|^2, with |r1|^2 formed from the pack; the 16 tap offsets are computed once and reused by every
 // filter; the field spline is stored interleaved (one 16-byte load per tap for both components).
-constexpr int ACC_BX = 32, ACC_BY = 4;
-__global__ void __launch_bounds__(128, 8) k_accumulate(const float4* __restrict__ ref4, const float2* __restrict__ R,
+constexpr int ACC_BX = 32, ACC_BY = 8, ACC_T = ACC_BX * ACC_BY;
+__global__ void __launch_bounds__(ACC_T, 1024 / ACC_T) k_accumulate(const float4* __restrict__ ref4, const float2* __restrict__ R,
                                                       int F, int ph, int pw, const double* __restrict__ ux,
                                                       const double* __restrict__ uy, const double* __restrict__ sx,
                                                       const double* __restrict__ sy, const double2* __restrict__ cs,
                                                       int W, int H, double* __restrict__ sums) {
-  extern __shared__ float4 pk[];  // F x 128
+  extern __shared__ float4 pk[];  // F x ACC_T
   // a block covers ACC_BX x ACC_BY pixels: its warps' response taps share rows in L1
   const int x = blockIdx.x * ACC_BX + threadIdx.x, y = blockIdx.y * ACC_BY + threadIdx.y;
   const int tid = threadIdx.y * ACC_BX + threadIdx.x;
   if (x >= W || y >= H) return;
   const size_t N = (size_t)W * H;
   const size_t p = (size_t)y * W + x;
-  for (int k = 0; k < F; k++) __pipeline_memcpy_async(&pk[k * 128 + tid], ref4 + (size_t)k * N + p, 16);
+  for (int k = 0; k < F; k++) __pipeline_memcpy_async(&pk[k * ACC_T + tid], ref4 + (size_t)k * N + p, 16);
   __pipeline_commit();
   const double u = ux[p], v = uy[p];
   const double tx = x + u, ty = y + v;
@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(128, 8) k_accumulate(const float4* __restrict_
   const float fnan = __int_as_float(0x7fc00000);
   __pipeline_wait_prior(0);
   for (int k = 0; k < F; k++) {
-    const float4 r1 = pk[k * 128 + tid];
+    const float4 r1 = pk[k * ACC_T + tid];
     // |r1|^2 as the reference pack's amplitude squared (phaseflow.py:111), from the stored float32 response
     const float q1 = fmaf(r1.x, r1.x, fmaf(r1.y, r1.y, 1e-12f));
     float br = fnan, bi = fnan;
@@ -452,7 +452,7 @@ void launch_accumulate(const float4* ref4, const float2* R, int F, int ph, int p
                        const double* sx, const double* sy, const double2* cs, int W, int H, double* sums,
                        cudaStream_t st) {
   dim3 g(div_up(W, ACC_BX), div_up(H, ACC_BY));
-  const size_t sm = (size_t)F * 128 * sizeof(float4);
+  const size_t sm = (size_t)F * ACC_T * sizeof(float4);
   if (sm > 227 * 1024) throw Error(OFC_ERR_WINDOW, "too many Gabor filters (" + std::to_string(F) + ") for the CUDA engine");
   OFC_CUDA(cudaFuncSetAttribute((const void*)k_accumulate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   OFC_LAUNCH(k_accumulate, g, dim3(ACC_BX, ACC_BY), sm, st, ref4, R, F, ph, pw, ux, uy, sx, sy, cs, W, H, sums);
