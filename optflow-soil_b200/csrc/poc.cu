@@ -538,7 +538,7 @@ __device__ void poc_shift64(const double* __restrict__ b, int W, int x0, int y0,
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(POC_T, 2) k_poc_grid64(const double* __restrict__ a, const double* __restrict__ b,
+__global__ void __launch_bounds__(POC_T, 3) k_poc_grid64(const double* __restrict__ a, const double* __restrict__ b,
                                                           int W, int H, const int* __restrict__ xs,
                                                           const int* __restrict__ ys, int nx, const double* iux,
                                                           const double* iuy, const PocConst* __restrict__ pcg,
