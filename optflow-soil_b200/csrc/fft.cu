@@ -521,9 +521,10 @@ __device__ __forceinline__ void fft_stage(const C2* __restrict__ A, C2* __restri
   __syncthreads();
 }
 
-// runs the plan on buf (tmp: scratch of the same capacity, fft_buf_len(L, C)); buf holds the input unpadded
-// and the returned buffer the result unpadded. FIXL > 0: the length is FIXL and the plan is fixed at compile time
-// (kernels are instantiated per FIXL, so that a fixed-length kernel carries no runtime-plan code and its registers).
+// runs the plan on buf (tmp: scratch of the same capacity, fft_buf_len(fft_work_len(pl), C)); buf holds the input
+// unpadded and the returned buffer the result unpadded. FIXL > 0: the length is FIXL and the plan is fixed at
+// compile time; FIXL = 0: a runtime plan transformed directly; FIXL = -1: a runtime Bluestein plan (kernels are
+// instantiated per FIXL, so that each carries only its own path's code and registers).
 // the plan's stages on their length SL (L, or Bluestein's M): a holds the input unpadded, the returned buffer the
 // result unpadded
 template <int C, class C2>
@@ -581,8 +582,9 @@ __device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
   static_assert(std::is_same<C2, float2>::value, "float32 transforms");
   if constexpr (FIXL > 0) {
     return fft_run_fixed<FIXL, C, 0, C2>(buf, tmp, (const C2*)pl.tw, inv);
+  } else if constexpr (FIXL < 0) {  // the kernels' instantiation for Bluestein plans (pl.M > 0)
+    return fft_bluestein<C, C2>(buf, tmp, pl, inv);
   } else {
-    if (pl.M) return fft_bluestein<C, C2>(buf, tmp, pl, inv);
     return fft_stages<C, C2>(buf, tmp, pl, pl.L, inv);
   }
 }
@@ -692,8 +694,8 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_fwd_real(const float* 
                                                                   FftPlan plw, int ph, float2* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* sm = (float2*)smraw;
-  const int pw = FIXL ? FIXL : plw.L;
-  float2* t = sm + fft_buf_len(FIXL ? FIXL : fft_work_len(plw), 1);
+  const int pw = FIXL > 0 ? FIXL : plw.L;
+  float2* t = sm + fft_buf_len(FIXL > 0 ? FIXL : fft_work_len(plw), 1);
   const int yp = blockIdx.x;
   const int ys = reflect_near(yp - PAD, H);
   const float* row = img + (size_t)ys * W;
@@ -715,8 +717,8 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_fwd(const float2* Tin
   constexpr int LC = C == 4 ? 2 : (C == 2 ? 1 : 0);
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* A = (float2*)smraw;
-  const int ph = FIXL ? FIXL : plh.L, n = ph * C;
-  float2* B = A + fft_buf_stride(FIXL ? FIXL : fft_work_len(plh), C);  // 16-byte aligned: the result may be either buffer
+  const int ph = FIXL > 0 ? FIXL : plh.L, n = ph * C;
+  float2* B = A + fft_buf_stride(FIXL > 0 ? FIXL : fft_work_len(plh), C);  // 16-byte aligned: the result may be either buffer
   const int x0 = blockIdx.x * C;
   // C = 2 with an even row pitch: each row of the pair is 16 bytes on a 16-byte boundary, copied asynchronously
   const bool rows16 = C == 2 && pw % 2 == 0;
@@ -781,16 +783,16 @@ __device__ __forceinline__ void cols_multiply(int n, const T* __restrict__ tab, 
 // take more time per element, one per radix-8 butterfly of the two columns (2 x 2112 / 8)
 constexpr int PAIR_T_REF = 544;
 template <bool REFPACK>
-constexpr int pair_threads(int fixl) { return fixl && REFPACK ? PAIR_T_REF : COLS_TMAX; }
+constexpr int pair_threads(int fixl) { return fixl > 0 && REFPACK ? PAIR_T_REF : COLS_TMAX; }
 template <bool REFPACK, int FIXL>
 __global__ void __launch_bounds__(pair_threads<REFPACK>(FIXL), 2) k_fft_cols_pair(const float2* __restrict__ S, FftPlan plh, int pw,
                                                                 GaborTables g, int k0, int k1, float2* __restrict__ U) {
   constexpr int C = 2;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int ph = FIXL ? FIXL : plh.L, n = ph * C, tid = threadIdx.x, nt = blockDim.x;
+  const int ph = FIXL > 0 ? FIXL : plh.L, n = ph * C, tid = threadIdx.x, nt = blockDim.x;
   float2* raw = (float2*)smraw;
   float2* A = raw + n;
-  float2* B = A + fft_buf_stride(FIXL ? FIXL : fft_work_len(plh), C);
+  float2* B = A + fft_buf_stride(FIXL > 0 ? FIXL : fft_work_len(plh), C);
   const int x0 = blockIdx.x * C;
   const bool rows16 = x0 + 1 < pw && pw % 2 == 0;  // each row of the pair is 16 bytes on a 16-byte boundary
   if (rows16) {
@@ -858,7 +860,7 @@ __global__ void __launch_bounds__(pair_threads<REFPACK>(FIXL), 2) k_fft_cols_pai
 
 // The same inverse column pass with one block per (C columns, plane) and no staged spectrum: the form for padded
 // heights whose column pair does not fit in shared memory beside the two transform buffers.
-template <int C, bool REFPACK>
+template <int C, bool REFPACK, int FIXL>
 __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const float2* __restrict__ S, FftPlan plh, int pw,
                                                                       GaborTables g, int k0, float2* __restrict__ U) {
   constexpr int LC = C == 4 ? 2 : (C == 2 ? 1 : 0);
@@ -889,7 +891,7 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const floa
     }
   }
   __syncthreads();
-  float2* r = fft_run<0, C>(A, B, plh, true);
+  float2* r = fft_run<FIXL, C>(A, B, plh, true);
   if (!REFPACK) {
     float2* idle = r == A ? B : A;
     bspline_edges<C>(r, ph, (float4*)(((uintptr_t)idle + 15) & ~(uintptr_t)15));  // the prefilter's edge terms along y
@@ -905,10 +907,10 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const floa
 // (line = k ph + y of the F planes) and copies the next line into a third buffer (cp.async) while it transforms the
 // current one; then the prefilter's edge terms along x and the scale 36 / (ph pw).
 template <int FIXL>
-__global__ void __launch_bounds__(FIXL ? 288 : FFT_TMAX, FIXL ? 3 : 2)
+__global__ void __launch_bounds__(FIXL > 0 ? 288 : FFT_TMAX, FIXL > 0 ? 3 : 2)
     k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int nlines, float scale, float2* __restrict__ R) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int L = FIXL ? FIXL : plw.L, nb = fft_buf_stride(FIXL ? FIXL : fft_work_len(plw), 1);
+  const int L = FIXL > 0 ? FIXL : plw.L, nb = fft_buf_stride(FIXL > 0 ? FIXL : fft_work_len(plw), 1);
   float2* in = (float2*)smraw;
   float2* tmp = in + nb;
   float2* pre = tmp + nb;
@@ -954,7 +956,7 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_ref(const float2* 
                                                                float* __restrict__ amp) {
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* sm = (float2*)smraw;
-  const int pw = FIXL ? FIXL : plw.L, nb = fft_buf_stride(FIXL ? FIXL : fft_work_len(plw), 1);
+  const int pw = FIXL > 0 ? FIXL : plw.L, nb = fft_buf_stride(FIXL > 0 ? FIXL : fft_work_len(plw), 1);
   float2* t = sm + 3 * nb;
   const int y = blockIdx.x, kk = blockIdx.y, k = k0 + kk;  // y: row of the W x H crop
   const size_t plane = (size_t)ph * pw;
@@ -1001,11 +1003,11 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_rows_inv_ref(const float2* 
 template <int FIXL>
 __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_lines(float2* data, FftPlan pl, int inv) {
   extern __shared__ float2 sm[];
-  const int L = FIXL ? FIXL : pl.L;
+  const int L = FIXL > 0 ? FIXL : pl.L;
   float2* row = data + (size_t)blockIdx.x * L;
   for (int x = threadIdx.x; x < L; x += blockDim.x) sm[x] = row[x];
   __syncthreads();
-  float2* r = fft_run<FIXL, 1>(sm, sm + fft_buf_len(FIXL ? FIXL : fft_work_len(pl), 1), pl, inv != 0);
+  float2* r = fft_run<FIXL, 1>(sm, sm + fft_buf_len(FIXL > 0 ? FIXL : fft_work_len(pl), 1), pl, inv != 0);
   for (int x = threadIdx.x; x < L; x += blockDim.x) row[x] = r[x];
 }
 
@@ -1032,10 +1034,12 @@ static size_t smem_cols_pair(int L, int WL) {
 // k_fft_rows_inv_resp: three buffers at the even stride
 static size_t smem_rows_resp(int L) { return 3 * (size_t)fft_buf_stride(L, 1) * sizeof(float2); }
 
-// calls f with std::integral_constant<int, FIXL> for the kernels' instantiation of length L
+// calls f with std::integral_constant<int, FIXL> for the kernels' instantiation of a plan: the fixed length, the
+// runtime direct plan (0) or the runtime Bluestein plan (-1)
 template <class Fn>
-static void by_length(int L, Fn f) {
-  if (L == FFT_FIXED_L) f(std::integral_constant<int, FFT_FIXED_L>{});
+static void by_plan(const FftPlan& pl, Fn f) {
+  if (pl.L == FFT_FIXED_L && !pl.M) f(std::integral_constant<int, FFT_FIXED_L>{});
+  else if (pl.M) f(std::integral_constant<int, -1>{});
   else f(std::integral_constant<int, 0>{});
 }
 
@@ -1063,7 +1067,7 @@ bool fft_fits(int ph, int pw) {
 void launch_fft_rows_fwd_real(const float* img, int W, int H, const FftPlan& plw, int ph, float2* out, cudaStream_t st) {
   int T = fft_threads(fft_work_len(plw), 1);
   size_t sm = 2 * fbytes(fft_work_len(plw), 1);
-  by_length(plw.L, [&](auto fl) {
+  by_plan(plw, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
     set_smem((const void*)k_fft_rows_fwd_real<FL>, sm);
     OFC_LAUNCH(k_fft_rows_fwd_real<FL>, ph, T, sm, st, img, W, H, plw, ph, out);
@@ -1072,11 +1076,11 @@ void launch_fft_rows_fwd_real(const float* img, int W, int H, const FftPlan& plw
 
 static void cols_fwd(float2* T, const FftPlan& plh, int pw, cudaStream_t st) {
   constexpr int C = 2;
-  const int ph = plh.L, wh = fft_work_len(plh);
+  const int wh = fft_work_len(plh);
   int nt = std::min(fft_threads(wh, C), COLS_TMAX);
   size_t sm_f = 2 * (size_t)fft_buf_stride(wh, C) * sizeof(float2);
   // in place: a block reads its C columns whole before it writes their spectrum back
-  by_length(ph, [&](auto fl) {
+  by_plan(plh, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
     set_smem((const void*)k_fft_cols_fwd<C, FL>, sm_f);
     OFC_LAUNCH((k_fft_cols_fwd<C, FL>), div_up(pw, C), nt, sm_f, st, T, plh, pw, T);
@@ -1095,7 +1099,7 @@ static void cols_inverse(const float2* S, const FftPlan& plh, int pw, const Gabo
   if (sm_p <= SMEM_MAX) {
     if (ph == FFT_FIXED_L) nt = pair_threads<REFPACK>(ph);  // the block size the fixed-length kernel assumes
     dim3 grid(div_up(pw, C), REFPACK ? 3 : div_up(g.F, RESP_G));
-    by_length(ph, [&](auto fl) {
+    by_plan(plh, [&](auto fl) {
       constexpr int FL = decltype(fl)::value;
       set_smem((const void*)k_fft_cols_pair<REFPACK, FL>, sm_p);
       if constexpr (REFPACK) OFC_LAUNCH((k_fft_cols_pair<true, FL>), grid, nt, sm_p, st, S, plh, pw, g, k0, k1, U);
@@ -1105,10 +1109,14 @@ static void cols_inverse(const float2* S, const FftPlan& plh, int pw, const Gabo
   }
   size_t sm_i = REFPACK ? 2 * fbytes(wh, C) : smem_prefilter(wh, C, nt);
   if (sm_i > SMEM_MAX) throw Error(OFC_ERR_WINDOW, "padded height " + std::to_string(ph) + " too large for the column pass");
-  set_smem((const void*)k_fft_cols_inv_filter<C, REFPACK>, sm_i);
   dim3 grid(div_up(pw, C), REFPACK ? 3 * (k1 - k0) : g.F);
-  if constexpr (REFPACK) OFC_LAUNCH((k_fft_cols_inv_filter<C, true>), grid, nt, sm_i, st, S, plh, pw, g, k0, U);
-  else OFC_LAUNCH((k_fft_cols_inv_filter<C, false>), grid, nt, sm_i, st, S, plh, pw, g, k0, U);
+  auto launch = [&](auto fl) {
+    constexpr int FL = decltype(fl)::value;
+    set_smem((const void*)k_fft_cols_inv_filter<C, REFPACK, FL>, sm_i);
+    OFC_LAUNCH((k_fft_cols_inv_filter<C, REFPACK, FL>), grid, nt, sm_i, st, S, plh, pw, g, k0, U);
+  };
+  if (plh.M) launch(std::integral_constant<int, -1>{});
+  else launch(std::integral_constant<int, 0>{});
 }
 
 void launch_fft_cols_filters(float2* T, const FftPlan& plh, int pw, const GaborTables& g, float2* U, cudaStream_t st) {
@@ -1121,7 +1129,7 @@ void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F
   size_t sm = smem_rows_resp(fft_work_len(plw));
   float scale = (float)(36.0 / ((double)ph * (double)plw.L));
   const int nlines = F * ph;
-  by_length(plw.L, [&](auto fl) {
+  by_plan(plw, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
     const void* fn = (const void*)k_fft_rows_inv_resp<FL>;
     set_smem(fn, sm);
@@ -1141,7 +1149,7 @@ void launch_fft_rows_inv_ref_f32(const float2* U, const FftPlan& plw, int ph, in
   int T = fft_threads(fft_work_len(plw), 1);
   size_t sm = 4 * (size_t)fft_buf_stride(fft_work_len(plw), 1) * sizeof(float2);
   dim3 grid(H, k1 - k0);
-  by_length(plw.L, [&](auto fl) {
+  by_plan(plw, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
     set_smem((const void*)k_fft_rows_inv_ref<FL>, sm);
     OFC_LAUNCH(k_fft_rows_inv_ref<FL>, grid, T, sm, st, U, plw, ph, W, H, k0, ref4, amp);
@@ -1151,7 +1159,7 @@ void launch_fft_rows_inv_ref_f32(const float2* U, const FftPlan& plw, int ph, in
 void launch_fft_lines(float2* data, int lines, const FftPlan& pl, bool inverse, cudaStream_t st) {
   int T = fft_threads(fft_work_len(pl), 1);
   size_t sm = 2 * fbytes(fft_work_len(pl), 1);
-  by_length(pl.L, [&](auto fl) {
+  by_plan(pl, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
     set_smem((const void*)k_fft_lines<FL>, sm);
     OFC_LAUNCH(k_fft_lines<FL>, lines, T, sm, st, data, pl, inverse ? 1 : 0);

@@ -48,7 +48,7 @@ __global__ void k_corr_x(const double* __restrict__ in, double* __restrict__ out
 // Symmetric taps are paired (k(t) = k(-t)).
 constexpr int CORR_R = 16, CY_RY = 4, CX_RX = 3;
 
-__global__ void __launch_bounds__(128, 4) k_corr_y_rb(const double* __restrict__ in, double* __restrict__ out, int W,
+__global__ void __launch_bounds__(128, 6) k_corr_y_rb(const double* __restrict__ in, double* __restrict__ out, int W,
                                                      int H, const double* __restrict__ taps) {
   constexpr int R = CORR_R, RY = CY_RY, NV = RY + 2 * R;
   __shared__ double tk[R + 1];
@@ -319,7 +319,7 @@ void launch_bspline_f32(const float* in, float* out, double* tmp, int W, int H, 
 }
 
 // ---------------------------------------------------------------- warp
-__global__ void k_warp(const float* __restrict__ c2, int w2, int h2, const double* __restrict__ sx,
+__global__ void __launch_bounds__(128, 10) k_warp(const float* __restrict__ c2, int w2, int h2, const double* __restrict__ sx,
                        const double* __restrict__ sy, long shx, long shy, int W, int H, float* __restrict__ out) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int y = blockIdx.y;
