@@ -257,6 +257,16 @@ typedef struct ofc_stream {
     void* source_user;
     ofc_sink_fn sink;
     void* sink_user;
+    /* the sampled frames (io.py:100-123, iter_frames): the raw frames start, start + step, ... < stop (stop < 0: to
+     * the source's end) are the sequence's frames 0, 1, 2, ...; the source's k is the raw frame index. step >= 1. */
+    int64_t start, step, stop;
+    /* tavg > 0 (io.py:126-153): each sampled frame s is the mean of the downscaled raw frames s - tavg .. s + tavg,
+     * clipped to the source, kept on the device; with tavg_align every window is aligned to s with the affine model
+     * (tavg_mask, nullable: the fit's ROI on the tracked grid), else a window that the source's start or end makes
+     * one-sided is aligned with the dense model (a frame that fails enters unaligned). */
+    int32_t tavg;
+    int32_t tavg_align;
+    const uint8_t* tavg_mask;
 } ofc_stream;
 
 /*

@@ -1072,6 +1072,33 @@ __global__ void k_tavg_mean(const float* __restrict__ c, const double* __restric
     out[i] = (float)(((double)c[i] + acc[i]) / cnt);
 }
 
+// average_window_with on device frames (tavg.rs:163-210; tavg.py:61-74): the mean of frames[0..n) (each W x H)
+// around frames[centre] into out; align 0 plain, 1 affine (hmask the fit's ROI, host, nullable), 2 dense; a
+// neighbour whose alignment fails is left out, or with keep_unaligned enters unaligned. Returns the frames used.
+int window_mean_dev(Lane& L, const float* const* frames, size_t n, size_t centre, int W, int H, int align,
+                    const uint8_t* hmask, bool keep_unaligned, const ofc_config& c, float* out) {
+  cudaStream_t st = L.stream;
+  const size_t N = (size_t)W * H;
+  float* dal = L.get<float>("tavg_out", N);
+  double* acc = L.get<double>("tavg_acc", N);
+  const unsigned blocks = std::min(div_up(N, 256), 8192u);
+  const float* dc = frames[centre];
+  int used = 0;
+  for (size_t i = 0; i < n; i++) {
+    if (i == centre) continue;
+    const float* add = frames[i];
+    if (align) {
+      if (tavg_align_dev(L, dc, frames[i], W, H, align == 1 ? hmask : nullptr, align - 1, c, dal)) add = dal;
+      else if (!keep_unaligned) continue;
+    }
+    OFC_LAUNCH(k_tavg_add, blocks, 256, 0, st, add, N, acc, used == 0 ? 1 : 0);
+    used++;
+  }
+  if (used == 0) OFC_CUDA(cudaMemcpyAsync(out, dc, N * 4, cudaMemcpyDeviceToDevice, st));
+  else OFC_LAUNCH(k_tavg_mean, blocks, 256, 0, st, dc, acc, N, (double)(used + 1), out);
+  return used + 1;
+}
+
 // ---------------------------------------------------------------- sequence chain (track_sequence)
 // rust/crates/optflow-core/src/track.rs:863-1245 (python/optflow_ref/track.py:231-315)
 
@@ -2152,6 +2179,9 @@ struct SeqIO {
   int w_in = 0, h_in = 0, scale = 1;
   // frame k's bytes: a host pointer (pageable or `slot`), or nullptr when the sequence has no frame k
   std::function<const void*(int64_t k, void* slot)> frame;
+  // when set, frame k of the sequence is made on the device into dst (the stream's window means) instead of coming
+  // from `frame`; false: the sequence has no frame k
+  std::function<bool(int64_t k, float* dst)> produce;
   std::function<double(int64_t k)> ruc;  // ref_update_conf at frame k
   std::function<void(int64_t k, const ofc_pair_out& out, const int32_t* fb, const ofc_hybrid_frame& info)> emit;
   ofc_leg_fn leg = nullptr;
@@ -2282,10 +2312,15 @@ int64_t run_sequence(Lane& L, const SeqIO& io) {
     emitted++;
   };
   // while the GPU runs a frame's first leg: deliver the previous frame's results, fetch the next frame
+  // produced frames: the next frame's window is made into fk_next while this frame's first leg runs (its reads from
+  // the source overlap the leg; its kernels follow the leg's on the stream)
+  float* fk_next = io.produce ? L.get<float>("seq_fk_next", N) : nullptr;
+  bool have_next = false;
   auto service = [&]() {
     flush();
     if (!fetched) {
-      next = fetch(k + 1);
+      if (io.produce) have_next = io.produce(k + 1, fk_next);
+      else next = fetch(k + 1);
       fetched = true;
     }
   };
@@ -2339,9 +2374,13 @@ int64_t run_sequence(Lane& L, const SeqIO& io) {
     OFC_CUDA(cudaStreamSynchronize(st));
   };
 
-  const void* f0 = fetch(0);
-  if (!f0) throw Error(OFC_ERR_ARG, "no frames");
-  load(f0, 0, ref);
+  if (io.produce) {
+    if (!io.produce(0, ref)) throw Error(OFC_ERR_ARG, "no frames");
+  } else {
+    const void* f0 = fetch(0);
+    if (!f0) throw Error(OFC_ERR_ARG, "no frames");
+    load(f0, 0, ref);
+  }
   OFC_CUDA(cudaMemcpyAsync(prev, ref, N * 4, cudaMemcpyDeviceToDevice, st));
   OFC_CUDA(cudaMemsetAsync(u0r, 0, 2 * N * 4, st));
   launch_fill_f64(c0r, 1.0, N, st);
@@ -2367,9 +2406,10 @@ int64_t run_sequence(Lane& L, const SeqIO& io) {
     A = L.aux[0].get();
   }
   cudaEvent_t spec_ready = L.bev[4], spec_taken = L.bev[5], spec_done = L.bev[6];
-  next = fetch(1);
-  while (next) {
-    load(next, (int)(k & 1), fk);
+  if (io.produce) have_next = io.produce(1, fk);
+  else next = fetch(1);
+  while (io.produce ? have_next : next != nullptr) {
+    if (!io.produce) load(next, (int)(k & 1), fk);
     fetched = false;
     next = nullptr;
     const double ruc = io.ruc(k);
@@ -2508,6 +2548,7 @@ int64_t run_sequence(Lane& L, const SeqIO& io) {
     OFC_CUDA(cudaMemcpyAsync(prev, fk, N * 4, cudaMemcpyDeviceToDevice, st));
     have_prev = true;
     k++;
+    if (io.produce) std::swap(fk, fk_next);
   }
   flush();
   OFC_CUDA(cudaStreamSynchronize(st));
@@ -2628,12 +2669,85 @@ int ofc_track_stream(ofc_engine* e, const ofc_stream* s, const uint8_t* roi, con
     io.w_in = (int)s->w_in;
     io.h_in = (int)s->h_in;
     io.scale = s->scale;
-    io.frame = [&](int64_t k, void* slot) -> const void* {
-      const int r = s->source(s->source_user, k, slot);
-      if (r == 1) return nullptr;
-      if (r != 0) throw Error(OFC_ERR_ARG, "the frame source failed on frame " + std::to_string(k));
-      return slot;
+    if (s->step < 1) throw Error(OFC_ERR_ARG, "step must be >= 1, got " + std::to_string(s->step));
+    if (s->start < 0) throw Error(OFC_ERR_ARG, "start must be >= 0, got " + std::to_string(s->start));
+    if (s->tavg < 0) throw Error(OFC_ERR_ARG, "tavg must be >= 0, got " + std::to_string(s->tavg));
+    const int64_t start = s->start, step = s->step, stop = s->stop;
+    auto raw = [&](int64_t i, void* slot) -> bool {  // raw frame i of the source into slot; false at its end
+      const int r = s->source(s->source_user, i, slot);
+      if (r == 1) return false;
+      if (r != 0) throw Error(OFC_ERR_ARG, "the frame source failed on frame " + std::to_string(i));
+      return true;
     };
+    io.frame = [&](int64_t k, void* slot) -> const void* {
+      const int64_t i = start + k * step;
+      if (stop >= 0 && i >= stop) return nullptr;
+      return raw(i, slot) ? slot : nullptr;
+    };
+    // tavg (io.py:126-153): the downscaled raw frames stay on the device in a ring, from which each sampled frame's
+    // window mean is made (window_mean_dev) when the frames after it have been read
+    const int m = s->tavg;
+    const int W = (int)w, H = (int)h;
+    const size_t N = w * h, in_bytes = pixel_bytes(s->pixel) * s->w_in * s->h_in;
+    std::map<int64_t, float*> ring;
+    std::vector<float*> spare;
+    int nring = 0;
+    int64_t raw_next = 0, last = -1;
+    bool ended = false, slot_busy = false;
+    uint8_t* traw = nullptr;
+    void* tslot = nullptr;
+    if (m > 0) {
+      traw = L.get<uint8_t>("stream_tavg_raw", in_bytes);
+      tslot = L.pinned<uint8_t>("stream_tavg_slot", in_bytes);
+      L.ensure_copy_stream();
+      io.produce = [&](int64_t k, float* dst) -> bool {
+        cudaStream_t st = L.stream;
+        const int64_t sidx = start + k * step;
+        if (stop >= 0 && sidx >= stop) return false;
+        const int64_t lo = std::max<int64_t>(0, sidx - m);
+        for (auto it = ring.begin(); it != ring.end();) {  // frames below the window go back to the spares
+          if (it->first < lo) {
+            spare.push_back(it->second);
+            it = ring.erase(it);
+          } else {
+            ++it;
+          }
+        }
+        raw_next = std::max(raw_next, lo);
+        while (!ended && raw_next <= sidx + m && (stop < 0 || raw_next < stop + m)) {
+          if (slot_busy) OFC_CUDA(cudaEventSynchronize(L.bev[7]));  // the slot's last upload has left it
+          if (!raw(raw_next, tslot)) {
+            ended = true;
+            break;
+          }
+          float* d = nullptr;
+          if (!spare.empty()) {
+            d = spare.back();
+            spare.pop_back();
+          } else {
+            d = L.get<float>("stream_tavg_ring" + std::to_string(nring++), N);
+          }
+          OFC_CUDA(cudaMemcpyAsync(traw, tslot, in_bytes, cudaMemcpyHostToDevice, st));
+          OFC_CUDA(cudaEventRecord(L.bev[7], st));
+          slot_busy = true;
+          to_gray_dev(L, traw, s->pixel, (int)s->w_in, s->scale, W, H, d);
+          ring[raw_next] = d;
+          last = raw_next;
+          raw_next++;
+        }
+        if (!ring.count(sidx)) return false;  // the source ended before the sampled frame
+        const int64_t hi = std::min(sidx + m, last);
+        std::vector<const float*> fr;
+        for (int64_t i = lo; i <= hi; i++) fr.push_back(ring.at(i));
+        const size_t centre = (size_t)(sidx - lo);
+        if (!s->tavg_align && sidx - lo != hi - sidx && std::min(W, H) >= c->poc_win)
+          window_mean_dev(L, fr.data(), fr.size(), centre, W, H, 2, nullptr, true, *c, dst);
+        else
+          window_mean_dev(L, fr.data(), fr.size(), centre, W, H, s->tavg_align ? 1 : 0,
+                          s->tavg_align ? s->tavg_mask : nullptr, false, *c, dst);
+        return true;
+      };
+    }
     io.ruc = [&](int64_t) { return s->ref_update_conf; };
     io.emit = [&](int64_t k, const ofc_pair_out& o, const int32_t* f, const ofc_hybrid_frame& fi) {
       if (s->sink(s->sink_user, k, &o, f, &fi) != 0)
@@ -2715,32 +2829,18 @@ int ofc_average_window(ofc_engine* e, const float* const* frames, size_t n, size
       throw Error(OFC_ERR_ARG, "image smaller than poc_win (" + std::to_string(c->poc_win) + ")");
     const size_t N = w * h;
     cudaStream_t st = L.stream;
-    const float* dc = L.upload("tavg_c", frames[centre], N);
-    float* dframe = L.get<float>("tavg_o", N);
-    float* dal = L.get<float>("tavg_out", N);
-    double* acc = L.get<double>("tavg_acc", N);
-    const unsigned blocks = std::min(div_up(N, 256), 8192u);
-    int used = 0;
+    float* dwin = L.get<float>("tavg_win", n * N);
+    std::vector<const float*> dframes(n);
     for (size_t i = 0; i < n; i++) {
-      if (i == centre) continue;
-      OFC_CUDA(cudaMemcpyAsync(dframe, frames[i], N * 4, cudaMemcpyHostToDevice, st));
-      const float* add = dframe;
-      if (align) {
-        if (tavg_align_dev(L, dc, dframe, (int)w, (int)h, align == 1 ? mask : nullptr, align - 1, *c, dal)) add = dal;
-        else if (!keep_unaligned) continue;
-      }
-      OFC_LAUNCH(k_tavg_add, blocks, 256, 0, st, add, N, acc, used == 0 ? 1 : 0);
-      used++;
+      OFC_CUDA(cudaMemcpyAsync(dwin + i * N, frames[i], N * 4, cudaMemcpyHostToDevice, st));
+      dframes[i] = dwin + i * N;
     }
-    if (used == 0) {
-      OFC_CUDA(cudaMemcpyAsync(out, dc, N * 4, cudaMemcpyDeviceToHost, st));
-    } else {
-      float* dout = L.get<float>("tavg_mean", N);
-      OFC_LAUNCH(k_tavg_mean, blocks, 256, 0, st, dc, acc, N, (double)(used + 1), dout);
-      OFC_CUDA(cudaMemcpyAsync(out, dout, N * 4, cudaMemcpyDeviceToHost, st));
-    }
+    float* dout = L.get<float>("tavg_mean", N);
+    const int used = window_mean_dev(L, dframes.data(), n, centre, (int)w, (int)h, align, mask, keep_unaligned != 0,
+                                     *c, dout);
+    OFC_CUDA(cudaMemcpyAsync(out, dout, N * 4, cudaMemcpyDeviceToHost, st));
     OFC_CUDA(cudaStreamSynchronize(st));
-    if (used_count) *used_count = used + 1;
+    if (used_count) *used_count = used;
   });
 }
 

@@ -148,6 +148,12 @@ class OfcStream(ctypes.Structure):
         ("source_user", ctypes.c_void_p),
         ("sink", SINK_FN),
         ("sink_user", ctypes.c_void_p),
+        ("start", ctypes.c_int64),
+        ("step", ctypes.c_int64),
+        ("stop", ctypes.c_int64),
+        ("tavg", ctypes.c_int32),
+        ("tavg_align", ctypes.c_int32),
+        ("tavg_mask", c_u8_p),
     ]
 
 

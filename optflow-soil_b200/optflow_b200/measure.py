@@ -1,6 +1,6 @@
 """Device timings of the sequence-side components on synthetic inputs (one JSON line per workload).
 
-    PYTHONPATH=optflow-soil_b200 python -m optflow_b200.measure [frames] [tavg] [hybrid] [stream] [pairs]
+    PYTHONPATH=optflow-soil_b200 python -m optflow_b200.measure [frames] [tavg] [hybrid] [stream] [pairs] [pipeline]
 
 Every workload is rendered on the GPU (optflow_b200.synth, seeded) and timed after one warm-up run: wall times with
 host perf_counter around the call, device times with the engine's per-kernel CUDA events (ofc_set_profile /
@@ -14,6 +14,8 @@ ofc_profile_read) in a separate run, since the profile mode waits for every repl
   stream  the CLI's seq loop on 8 rgb24 1920 x 1080 frames at scale 2 (track_stream, chain): wall time per frame
           against the device time of the frame's kernels
   pairs   24 pairs of sides drawn from {256, ..., 2048} (seed 11): one track_pairs call against one track_pair call each
+  pipeline  23 rgb24 1920 x 1080 frames, scale 2, step 5, tavg 3, hybrid: the window means inside the streamed driver
+          against iter_frames feeding it
 """
 import ctypes
 import json
@@ -210,7 +212,28 @@ def pairs(eng):
             "track_pairs_s": round(t2, 3), "track_pairs_mpx_s": round(px / t2 / 1e6, 1)}
 
 
-WORKLOADS = {"frames": frames, "tavg": tavg, "hybrid": hybrid, "stream": stream, "pairs": pairs}
+def pipeline(eng):
+    """The CLI's recommended sequence settings on video frames: rgb24 1920 x 1080, scale 2, step 5, tavg 3, hybrid;
+    the window means made inside the streamed driver against iter_frames (grey frames back to the host, each window
+    uploaded again) feeding the same driver."""
+    from .stream import iter_frames
+    fr = _frames_rgb24(23, seed=13)
+    cfg = Config(seq_mode="hybrid")
+    kw = dict(step=5, tavg=3)
+    list(track_stream(fr[:12], cfg, scale=2, engine=eng, **kw))
+    t = time.perf_counter()
+    a = list(track_stream(fr, cfg, scale=2, engine=eng, **kw))
+    t_dev = time.perf_counter() - t
+    t = time.perf_counter()
+    b = list(track_stream(iter_frames(iter(fr), scale=2, cfg=cfg, engine=eng, **kw), cfg, engine=eng))
+    t_host = time.perf_counter() - t
+    same = all(np.array_equal(x.ux, y.ux, equal_nan=True) for (_, x), (_, y) in zip(a, b))
+    return {"workload": "pipeline: 23 rgb24 1920x1080 frames, scale 2, step 5, tavg 3, hybrid (5 tracked frames)",
+            "results": len(a), "wall_ms_per_result_device_windows": round(1e3 * t_dev / len(a), 2),
+            "wall_ms_per_result_iter_frames": round(1e3 * t_host / max(len(b), 1), 2), "identical": bool(same)}
+
+
+WORKLOADS = {"frames": frames, "tavg": tavg, "hybrid": hybrid, "stream": stream, "pairs": pairs, "pipeline": pipeline}
 
 
 def main(argv=None):

@@ -73,10 +73,20 @@ def _result(o, fb, info, shape):
     return r
 
 
-def track_stream(frames, cfg=None, mask=None, scale=1, engine=None):
-    """track.track_sequence over an iterable of frames (any format of pixel_format, all of one shape), each
-    downscaled by `scale` on the GPU (mask: on the downscaled grid; cfg.seq_mode chain or hybrid). Yields (k, Result)
-    as the engine delivers them, while it tracks the next frame; frames are read one ahead of the tracking."""
+def track_stream(frames, cfg=None, mask=None, scale=1, start=0, stop=None, step=1, tavg=0, align=False,
+                 align_mask=None, engine=None):
+    """track.track_sequence over io.iter_frames of an iterable of decoded frames (any format of pixel_format, all of
+    one shape; every frame of the video from index 0), all on the GPU: the frames start, start + step, ... < stop,
+    each downscaled by `scale`; tavg = m > 0: each the mean of the downscaled frames i - m .. i + m (align: aligned to
+    frame i with the affine model inside align_mask, on the downscaled grid; otherwise the windows the input's ends
+    make one-sided with the dense model), kept on the device. mask: the tracking ROI on the downscaled grid;
+    cfg.seq_mode chain or hybrid. Yields (k, Result) as the engine delivers them, while it tracks the next frame."""
+    if step < 1:
+        raise ValueError(f"step must be >= 1, got {step}")
+    if start < 0:
+        raise ValueError(f"start must be >= 0, got {start}")
+    if tavg < 0:
+        raise ValueError(f"tavg must be >= 0, got {tavg}")
     cfg, c = _prep_cfg(cfg)
     eng = engine or default_engine()
     it = iter(frames)
@@ -96,19 +106,28 @@ def track_stream(frames, cfg=None, mask=None, scale=1, engine=None):
         m = np.ascontiguousarray(mask, dtype=np.uint8)
         if not m.any():
             raise ValueError("ROI mask is empty")
+    am = None
+    if align_mask is not None:
+        if np.shape(align_mask) != shape:
+            raise ValueError(f"align mask shape {np.shape(align_mask)} differs from the frame shape {shape}")
+        am = np.ascontiguousarray(align_mask, dtype=np.uint8)
     nbytes = _packed(first, fmt).nbytes
     out_q = queue.Queue(maxsize=2)
-    stop = threading.Event()
-    state = {"first": first, "error": None}
+    halt = threading.Event()
+    state = {"first": first, "error": None, "pos": 0}  # pos: the index of the iterator's next frame
 
     def source(_user, k, dst):
         try:
-            if stop.is_set():
+            if halt.is_set():
                 return 2
-            if state["first"] is not None:
-                a, state["first"] = state["first"], None
-            else:
-                a = next(it)
+            while True:  # the engine asks for raw frame indices in increasing order; frames between are skipped
+                if state["first"] is not None:
+                    a, state["first"] = state["first"], None
+                else:
+                    a = next(it)
+                state["pos"] += 1
+                if state["pos"] - 1 == k:
+                    break
             p = _packed(a, fmt)
             if p.nbytes != nbytes or p.shape[:2] != (h_in, w_in):
                 raise ValueError(f"frame {k} has shape {np.shape(a)}, expected {first.shape}")
@@ -121,10 +140,10 @@ def track_stream(frames, cfg=None, mask=None, scale=1, engine=None):
             return 2
 
     def sink(_user, k, out, fb, info):
-        if stop.is_set():
+        if halt.is_set():
             return 1
         r = _result(ctypes.cast(out, ctypes.POINTER(OfcPairOut)).contents, fb, info.contents, shape)
-        while not stop.is_set():
+        while not halt.is_set():
             try:
                 out_q.put((int(k), r), timeout=0.1)
                 return 0
@@ -135,7 +154,8 @@ def track_stream(frames, cfg=None, mask=None, scale=1, engine=None):
     hy = _abi.OfcHybrid(int(cfg.fb_max), float(cfg.fb_radius), int(cfg.fb_min_support), float(cfg.fb_tol))
     src_fn, sink_fn = _abi.SOURCE_FN(source), _abi.SINK_FN(sink)
     s = _abi.OfcStream(_abi.OFC_PIX[fmt], w_in, h_in, int(scale), int(cfg.seq_mode == "hybrid"), hy,
-                       float(cfg.ref_update_conf), src_fn, None, sink_fn, None)
+                       float(cfg.ref_update_conf), src_fn, None, sink_fn, None, int(start), int(step),
+                       -1 if stop is None else int(stop), int(tavg), int(bool(align)), _ptr(am, c_u8_p))
     done = object()
 
     def work():
@@ -143,7 +163,7 @@ def track_stream(frames, cfg=None, mask=None, scale=1, engine=None):
             n = ctypes.c_int64(0)
             eng._call("ofc_track_stream", ctypes.byref(s), _ptr(m, c_u8_p), ctypes.byref(c), ctypes.byref(n))
         except Exception as e:  # noqa: BLE001
-            if state["error"] is None and not stop.is_set():
+            if state["error"] is None and not halt.is_set():
                 state["error"] = e
         finally:
             while True:
@@ -151,7 +171,7 @@ def track_stream(frames, cfg=None, mask=None, scale=1, engine=None):
                     out_q.put(done, timeout=0.1)
                     break
                 except queue.Full:
-                    if stop.is_set():
+                    if halt.is_set():
                         break
 
     th = threading.Thread(target=work, name="ofc_track_stream", daemon=True)
@@ -163,7 +183,7 @@ def track_stream(frames, cfg=None, mask=None, scale=1, engine=None):
                 break
             yield item
     finally:
-        stop.set()
+        halt.set()
         while th.is_alive():
             try:
                 out_q.get(timeout=0.1)

@@ -150,3 +150,26 @@ def test_iter_frames_matches_the_reference():
     # the averaged frames feed the streamed tracking as any frames do
     res = dict(track_stream(iter_frames(iter(fr), start=1, step=3, scale=2, tavg=2, cfg=cfg), Config()))
     assert sorted(res) == [1, 2] and all(np.isfinite(r.ux).any() for r in res.values())
+
+
+@pytest.mark.parametrize("kw", [dict(start=1, step=3, tavg=2), dict(start=0, stop=7, step=2, tavg=1, align=True),
+                                dict(start=2, stop=9, step=3)])
+def test_stream_sampling_and_tavg_equal_iter_frames(kw):
+    """The sampled and averaged frames made on the device inside the streamed driver (a ring of downscaled frames,
+    window means, the edge windows aligned with the dense model, or every window with the affine model inside a
+    mask) give the results of iter_frames' frames (pinned to the reference's io.iter_frames) through the array
+    entry, bit for bit."""
+    from optflow_b200.stream import iter_frames
+    g = golden("iter")
+    fr = list(g["frames"])
+    mask = g["mask"].astype(bool)
+    cfg = Config(max_disp=8.0)
+    mask_fn = (lambda shape: mask) if kw.get("align") else None
+    frames = list(iter_frames(iter(fr), scale=2, cfg=cfg, mask_fn=mask_fn, **kw))
+    want = dict(track_sequence(frames, cfg))
+    got = dict(track_stream(iter(fr), cfg, scale=2, align_mask=mask if kw.get("align") else None, **kw))
+    assert sorted(got) == sorted(want) == list(range(1, len(frames)))
+    for k in want:
+        same(got[k], want[k], f"{kw} frame {k}")
+    with pytest.raises(ValueError, match="step must be >= 1"):
+        next(track_stream(iter(fr), cfg, step=0))
