@@ -168,7 +168,7 @@ OFC_API int ofc_refine_batch(ofc_engine* eng, const ofc_window* wins, size_t n, 
  * frame k's result on the frame-0 grid (composed raw field, link confidence, guard and strain of the finish; timing
  * coarse / fine of the leg, strain of the finish); reference[k - 1] and mean_conf[k - 1] (nullable) the reference
  * index and the mean confidence. roi (nullable): the frame-0 ROI of the finish and of the mean. The hybrid mode is
- * not part of this entry point.
+ * ofc_track_sequence_hybrid; a frame source instead of arrays is ofc_track_stream.
  */
 OFC_API int ofc_track_sequence(ofc_engine* eng, const float* const* frames, size_t n, size_t w, size_t h,
                        const uint8_t* roi, const ofc_config* cfg, double ref_update_conf, ofc_pair_out* outs,
