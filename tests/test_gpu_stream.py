@@ -153,7 +153,7 @@ def test_iter_frames_matches_the_reference():
 
 
 @pytest.mark.parametrize("kw", [dict(start=1, step=3, tavg=2), dict(start=0, stop=7, step=2, tavg=1, align=True),
-                                dict(start=2, stop=9, step=3)])
+                                dict(start=2, stop=9, step=3), dict(start=0, step=2, tavg=1, hybrid=True)])
 def test_stream_sampling_and_tavg_equal_iter_frames(kw):
     """The sampled and averaged frames made on the device inside the streamed driver (a ring of downscaled frames,
     window means, the edge windows aligned with the dense model, or every window with the affine model inside a
@@ -163,7 +163,8 @@ def test_stream_sampling_and_tavg_equal_iter_frames(kw):
     g = golden("iter")
     fr = list(g["frames"])
     mask = g["mask"].astype(bool)
-    cfg = Config(max_disp=8.0)
+    kw = dict(kw)
+    cfg = Config(max_disp=8.0, seq_mode="hybrid" if kw.pop("hybrid", False) else "chain")
     mask_fn = (lambda shape: mask) if kw.get("align") else None
     frames = list(iter_frames(iter(fr), scale=2, cfg=cfg, mask_fn=mask_fn, **kw))
     want = dict(track_sequence(frames, cfg))
