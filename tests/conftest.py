@@ -9,8 +9,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "optflow-soil_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE = os.environ.get("OPTFLOW_REFERENCE", "/root/reference")
-REF_FIXTURES = os.path.join(REFERENCE, "rust", "crates", "optflow-core", "tests", "fixtures")
+# the reference's committed parity fixtures, packed by tests/golden/collect_ref_fixtures.py
+_REF_FIXTURES = None
 
 
 def pytest_configure(config):
@@ -23,10 +23,16 @@ def golden(name):
 
 
 def ref_fixture(name):
-    path = os.path.join(REF_FIXTURES, name + ".npy")
-    if not os.path.exists(path):
-        pytest.skip("the reference's fixtures are not present here")
-    return np.load(path)
+    global _REF_FIXTURES
+    if _REF_FIXTURES is None:
+        with np.load(os.path.join(GOLDEN, "ref_fixtures.npz")) as z:
+            _REF_FIXTURES = {k: z[k] for k in z.files}
+    return _REF_FIXTURES[name]
+
+
+def ref_meta():
+    import json
+    return json.loads(str(ref_fixture("meta.json")))
 
 
 def rms(a, b, mask=None):

@@ -1,7 +1,7 @@
 """Writes the golden vectors of tests/golden/*.npz by running the reference's own Python specification.
 
 Run in a checkout that has the reference (``python tests/golden/make_golden.py [/path/to/reference]``; the
-default path is /root/reference). The reference's ``python/optflow_ref`` package is imported and called on
+or the OPTFLOW_REFERENCE environment variable). The reference's ``python/optflow_ref`` package is imported and called on
 seeded synthetic inputs made with its own generator (``optflow_ref.synth``); inputs are rounded to float32
 first (what the C ABI takes, ``Image<f32>`` in the reference's Rust engine interface) and the reference is
 run on exactly those values, so inputs and expected outputs match bit for bit. Outputs are stored as float32
@@ -16,7 +16,9 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OPTFLOW_REFERENCE")
+if not REF:
+    sys.exit("usage: pass the reference checkout as the first argument (or set OPTFLOW_REFERENCE)")
 sys.path.insert(0, os.path.join(REF, "python"))
 
 from optflow_ref import interp, phaseflow, poc, strain, synth, track  # noqa: E402

@@ -8,7 +8,7 @@ Stored per frame: ux, uy and conf in full; Exx, Eyy, Exy, gmax and vol on every 
 fields are smooth; the subsample keeps the fixture small); the reference index and mean confidence.
 
 Run in a checkout that has the reference: ``python tests/golden/make_golden_config1.py [/path/to/reference]``
-(default /root/reference).
+(or the OPTFLOW_REFERENCE environment variable).
 """
 import os
 import sys
@@ -17,7 +17,9 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OPTFLOW_REFERENCE")
+if not REF:
+    sys.exit("usage: pass the reference checkout as the first argument (or set OPTFLOW_REFERENCE)")
 sys.path.insert(0, os.path.join(REF, "python"))
 
 from optflow_ref import synth, track  # noqa: E402

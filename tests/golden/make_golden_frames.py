@@ -3,7 +3,7 @@ to_gray and downscale): seeded 37 x 29 images of every pixel format the engine t
 grey and RGB; float32 grey), their grey levels (float64) and their box downscales by 2 and 3.
 
 Run in a checkout that has the reference: ``python tests/golden/make_golden_frames.py [/path/to/reference]``
-(default /root/reference).
+(or the OPTFLOW_REFERENCE environment variable).
 """
 import os
 import sys
@@ -11,7 +11,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OPTFLOW_REFERENCE")
+if not REF:
+    sys.exit("usage: pass the reference checkout as the first argument (or set OPTFLOW_REFERENCE)")
 sys.path.insert(0, os.path.join(REF, "python"))
 
 from optflow_ref import io  # noqa: E402

@@ -17,7 +17,7 @@
    tracked with ref_update_conf 0.8 and fb_max 10 (A) or 2 (B).
 
 Run in a checkout that has the reference: ``python tests/golden/make_golden_hybrid.py [/path/to/reference]``
-(default /root/reference).
+(or the OPTFLOW_REFERENCE environment variable).
 """
 import os
 import sys
@@ -26,7 +26,9 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OPTFLOW_REFERENCE")
+if not REF:
+    sys.exit("usage: pass the reference checkout as the first argument (or set OPTFLOW_REFERENCE)")
 sys.path.insert(0, os.path.join(REF, "python"))
 sys.path.insert(0, os.path.dirname(HERE))
 

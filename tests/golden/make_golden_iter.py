@@ -8,7 +8,7 @@ windows are one-sided and aligned with the dense model; (aligned) tavg 1, start 
 aligned with the affine model inside a mask.
 
 Run in a checkout that has the reference: ``python tests/golden/make_golden_iter.py [/path/to/reference]``
-(default /root/reference).
+(or the OPTFLOW_REFERENCE environment variable).
 """
 import os
 import sys
@@ -16,7 +16,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OPTFLOW_REFERENCE")
+if not REF:
+    sys.exit("usage: pass the reference checkout as the first argument (or set OPTFLOW_REFERENCE)")
 sys.path.insert(0, os.path.join(REF, "python"))
 
 from optflow_ref import io, synth  # noqa: E402

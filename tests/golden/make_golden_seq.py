@@ -1,8 +1,8 @@
 """Writes tests/golden/seq.npz by running the reference's own Python track_sequence (chain mode,
 python/optflow_ref/track.py:260-315) on seeded frames made with its generator (optflow_ref.synth).
 
-Run in a checkout that has the reference: ``python tests/golden/make_golden_seq.py [/path/to/reference]`` (default
-/root/reference). Frames are rounded to float32 first (what the C ABI takes) and the reference runs on those values.
+Run in a checkout that has the reference: ``python tests/golden/make_golden_seq.py [/path/to/reference]`` (or the
+OPTFLOW_REFERENCE environment variable). Frames are rounded to float32 first (what the C ABI takes) and the reference runs on those values.
 Two runs: the default ref_update_conf (the reference stays at frame 0) and ref_update_conf = 0.995 (the reference
 moves to k - 1 at every frame from k = 2 on), both with an ROI.
 """
@@ -13,7 +13,9 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OPTFLOW_REFERENCE")
+if not REF:
+    sys.exit("usage: pass the reference checkout as the first argument (or set OPTFLOW_REFERENCE)")
 sys.path.insert(0, os.path.join(REF, "python"))
 
 from optflow_ref import synth, track  # noqa: E402

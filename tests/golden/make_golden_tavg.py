@@ -1,8 +1,8 @@
 """Writes tests/golden/tavg.npz by running the reference's own Python temporal-averaging front-end
 (python/optflow_ref/tavg.py) on seeded frames made with its generator (optflow_ref.synth).
 
-Run in a checkout that has the reference: ``python tests/golden/make_golden_tavg.py [/path/to/reference]`` (default
-/root/reference). Frames are rounded to float32 first (what the C ABI takes) and the reference runs on those values.
+Run in a checkout that has the reference: ``python tests/golden/make_golden_tavg.py [/path/to/reference]`` (or the
+OPTFLOW_REFERENCE environment variable). Frames are rounded to float32 first (what the C ABI takes) and the reference runs on those values.
 The reference's warp is scipy's cubic map_coordinates (mode "nearest"); the reference CLI and this engine warp with
 the B-spline of interp::warp, so the two agree away from the image border, which is where the tests compare.
 """
@@ -12,7 +12,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OPTFLOW_REFERENCE")
+if not REF:
+    sys.exit("usage: pass the reference checkout as the first argument (or set OPTFLOW_REFERENCE)")
 sys.path.insert(0, os.path.join(REF, "python"))
 
 from optflow_ref import synth, tavg  # noqa: E402

@@ -5,12 +5,11 @@ tests/golden/make_golden.py), checked to float32 storage precision; and, where t
 present, the reference's own parity fixtures (rust/crates/optflow-core/tests/fixtures, written by
 python/bench/make_parity_fixtures.py) with the tolerances of the reference's Rust parity tests.
 """
-import json
 import os
 
 import numpy as np
 import pytest
-from conftest import REF_FIXTURES, golden, ref_fixture, rms
+from conftest import golden, ref_fixture, ref_meta, rms
 
 from optflow_b200.config import Config
 
@@ -134,11 +133,7 @@ def test_track_pair(oracle, name):
 
 # ---------------------------------------------------------------- the reference's own fixtures
 def _meta():
-    path = os.path.join(REF_FIXTURES, "meta.json")
-    if not os.path.exists(path):
-        pytest.skip("the reference's fixtures are not present here")
-    with open(path) as fh:
-        return json.load(fh)
+    return ref_meta()
 
 
 def test_tavg(oracle):
