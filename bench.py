@@ -3,15 +3,19 @@
 Workload (one step = one tracked pair: coarse POC pyramid -> dense start -> fine stage (8 outer x 2 inner
 iterations, 12 Gabor filters) -> confidence -> guard + strain; default configuration):
   * 2048 x 2048 uint8-quantised speckle pair: blobs of make_pattern(2048, 2048, seed=7, rmin=1.5, rmax=2.5) (mean
-    speckle diameter about 4 px), rendered with 4 x 4 supersampling;
+    speckle diameter about 4 px), rendered with 4 x 4 supersampling by the reference generator's arithmetic (the
+    frames equal the reference's synth.render/degrade output bit for bit: tests/test_gpu_config2.py);
   * deformation x = c + A (X - c) + 1.5 sin(2 pi X / 256) (1, 1), A = [[1.01, 0.003], [0.003, 0.996]] about the
     centre (exx 0.01, eyy -0.004, gxy 0.006), Gaussian noise 0.01, 8-bit quantisation;
   * polygon ROI covering the central 80 % ([204.8, 1843.2]^2).
 value: pixel-pairs/s with the inputs resident in device memory (ofc_track_pair_device), device time from CUDA
 events around each step, L2 flushed (256 MiB write) between steps; e2e: the same through the host C ABI
 (ofc_track_pair) with pinned host buffers, uploads and downloads of the nine CLI outputs included.
---impl reference: the CPU oracle (float64 C++/OpenMP restatement of the reference's pair path) on the host cores
-over a bounded sample of the same pair (its central 512^2 crop and ROI).
+--impl reference: the reference's CPU path (the float64 C++/OpenMP oracle, a restatement of it: the Rust CLI cannot
+be built here) on all host cores, over the same pair; a step is one window of the reference CLI's own 2 x 2 tiling
+of the pair (tile.rs:56,85: 1024 px tiles with a 64 px margin, windows of 1088^2), the four windows in turn, and
+the value is the tiles' core pixels per second. That process renders its inputs with the oracle's restatement of
+the generator and loads no part of the CUDA engine.
 
 Multi-GPU (torchrun): one independent replica per GPU (the pair path has no exchange step); value = all ranks'
 pixels / the slowest rank's time.
@@ -37,16 +41,29 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 
-def make_pair(n=N_PIX, engine=None):
+PAIR_FIELD = dict(A=((1.01, 0.003), (0.003, 0.996)), amp=1.5, wavelength=256.0, s=(1.0, 1.0))
+
+
+def make_pair(n=N_PIX, engine=None, renderer=None):
+    """The benchmark pair: (a, b, roi, field). renderer(pattern, h, w, field) -> float64 image; None: the engine's
+    GPU renderer (ofc_synth_render)."""
     from optflow_b200 import synth
     p = synth.make_pattern(n, n, seed=7, rmin=1.5, rmax=2.5)
     c = n / 2.0
-    field = synth.Field(A=((1.01, 0.003), (0.003, 0.996)), c=(c, c), amp=1.5, wavelength=256.0, s=(1.0, 1.0))
-    a = synth.degrade(synth.render(p, n, n, None, engine=engine), seed=1, noise=0.01, bits=8)
-    b = synth.degrade(synth.render(p, n, n, field, engine=engine), seed=2, noise=0.01, bits=8)
+    field = synth.Field(c=(c, c), **PAIR_FIELD)
+    render = renderer or (lambda pat, h, w, f: synth.render(pat, h, w, f, engine=engine))
+    a = synth.degrade(render(p, n, n, None), seed=1, noise=0.01, bits=8)
+    b = synth.degrade(render(p, n, n, field), seed=2, noise=0.01, bits=8)
     lo, hi = 0.1 * n, 0.9 * n
-    roi = synth.polygon_mask(n, n, [[lo, lo], [hi, lo], [hi, hi], [lo, hi]])
+    roi = synth.rect_roi(n, n, lo, lo, hi, hi)
     return a, b, roi, field
+
+
+def workload_config(n):
+    """The config object both arms print."""
+    return {"workload": f"{n}^2 speckle pair (seed 7, 4 px speckles), affine exx 0.01 eyy -0.004 gxy 0.006 + 1.5 px "
+                        f"sinusoid (256 px), noise 0.01, 8 bit, ROI 80 %",
+            "steps_are": "one tracked pair each", "l2": "flushed (256 MiB write) between steps"}
 
 
 class ClockSampler:
@@ -123,29 +140,40 @@ def accumulate_bytes(W, H, F=12):
 ACC_TRAFFIC_RATIO = 1670.0 / 1669.7
 
 
-def cpu_sample(a, b, roi, n=512):
-    c0 = (a.shape[0] - n) // 2
-    sl = (slice(c0, c0 + n), slice(c0, c0 + n))
-    return a[sl], b[sl], roi[sl]
+def tile_windows(n, tile=1024, margin=64):
+    """The reference CLI's tiling of an n x n image (rust/crates/optflow-core/src/tile.rs:56,85): (window slices,
+    core pixels) per tile, row-major."""
+    out = []
+    for y0 in range(0, n, tile):
+        for x0 in range(0, n, tile):
+            y1, x1 = min(y0 + tile, n), min(x0 + tile, n)
+            win = (slice(max(y0 - margin, 0), min(y1 + margin, n)), slice(max(x0 - margin, 0), min(x1 + margin, n)))
+            out.append((win, (y1 - y0) * (x1 - x0)))
+    return out
 
 
-def run_cpu(a, b, roi, steps, warmup, sample_n=512):
+def run_cpu(a, b, roi, steps, warmup):
+    """The oracle on all host threads, one tile window of the pair per step (the four in turn)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from optflow_b200 import Config
     threads = oracle.threads(0)
-    sa, sb, sr = cpu_sample(a, b, roi, sample_n)
-    times = []
+    wins = tile_windows(a.shape[0])
+    px, sec = 0, 0.0
     for i in range(warmup + steps):
+        win, core = wins[i % len(wins)]
         t = time.perf_counter()
-        oracle.track_pair(sa, sb, Config(), mask=sr)
+        oracle.track_pair(a[win], b[win], Config(), mask=roi[win])
+        dt = time.perf_counter() - t
         if i >= warmup:
-            times.append(time.perf_counter() - t)
-    sec = float(np.mean(times))
-    return {"value": sample_n * sample_n / sec, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"central {sample_n}x{sample_n} crop of the 2048^2 pair (with its ROI), float64 oracle "
-                      f"(C++/OpenMP restatement of the reference's pair path), {threads} threads, "
-                      f"{sec:.2f} s per pair"}
+            px += core
+            sec += dt
+    (wy, wx), core = wins[0][0], wins[0][1]
+    return {"value": px / sec, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} step(s), each one of the {len(wins)} windows of the reference CLI's tiling of the "
+                      f"{a.shape[0]}^2 pair ({wy.stop - wy.start}x{wx.stop - wx.start}, its {core} core pixels "
+                      f"credited), float64 oracle (C++/OpenMP restatement of the reference's pair path), {threads} "
+                      f"threads, {sec / steps:.2f} s per window"}
 
 
 def main():
@@ -167,17 +195,15 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        import torch
-        from optflow_b200 import Engine
-        eng = Engine(local) if torch.cuda.is_available() else None
-        a, b, roi, _ = make_pair(args.size, engine=eng)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        a, b, roi, _ = make_pair(args.size, renderer=oracle.render)
         base = run_cpu(a, b, roi, args.steps, args.warmup)
         line = {"metric": METRIC, "value": base["value"], "unit": UNIT, "impl": "reference", "n_gpus": 0,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic", "cpu_baseline": base,
                 "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                "config": {"workload": f"{args.size}^2 speckle pair, affine + 1.5 px sinusoid, noise 0.01, ROI 80 %; "
-                                       "CPU sample: central 512^2 crop"}}
+                "config": workload_config(args.size)}
         print(json.dumps(line), flush=True)
         return
 
@@ -326,10 +352,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_max * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "fp32 transforms + fp64 sums/solve", "data": "synthetic",
-                "config": {"workload": f"{n}^2 speckle pair (seed 7, 4 px speckles), affine exx 0.01 eyy -0.004 "
-                                       f"gxy 0.006 + 1.5 px sinusoid (256 px), noise 0.01, 8 bit, ROI 80 %",
-                           "steps_are": "one tracked pair each", "l2": "flushed (256 MiB write) between steps",
-                           "parallelism": f"replicas x{world}", "valid_fraction": valid_frac},
+                "config": dict(workload_config(n), parallelism=f"replicas x{world}"), "valid_fraction": valid_frac,
                 "e2e": {"value": world * n * n / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_sec * 1e3},
                 "gpu_launches": int(launches), "clocks": clk, "roofline": roof, "cpu_baseline": base}

@@ -23,10 +23,12 @@ typedef struct ofc_field {
     double sx, sy;             /* its direction */
 } ofc_field;
 
-/* Render a w x h image of n blobs (centres bx, by, radii br, amplitudes ba, as synth.make_pattern draws
- * them) deformed by `field` (NULL: the reference image) with ss x ss subsamples per pixel. */
+/* Render a w x h float64 image of n blobs (centres bx, by, radii br, amplitudes ba, as synth.make_pattern draws
+ * them) deformed by `field` (NULL: the reference image) with ss x ss subsamples per pixel: synth.render
+ * (synth.py:150-190), the same blob rectangles and float64 arithmetic, so its images equal the reference
+ * generator's to rounding. */
 OFC_API int ofc_synth_render(ofc_engine* eng, const double* bx, const double* by, const double* br, const double* ba,
-                             size_t n, size_t w, size_t h, int ss, const ofc_field* field, float* out, char* err,
+                             size_t n, size_t w, size_t h, int ss, const ofc_field* field, double* out, char* err,
                              size_t errlen);
 
 /* Per-kernel device time of this engine's launches since the last call (profile mode): up to `cap` entries

@@ -42,6 +42,14 @@ OFC_API int ofc_test_median(ofc_engine* eng, const double* v, size_t n, double* 
 OFC_API int ofc_test_large_components(ofc_engine* eng, const uint8_t* b, size_t w, size_t h, double min_area,
                                       uint8_t* out, char* err, size_t errlen);
 
+/* The integer peaks of the raw POC grid of pyramid level `level` (0 = full size) of coarse_flow
+ * (python/optflow_ref/poc.py:67-92, 216-239): per grid point (x, y) = the window offset round(d) plus the argmax
+ * of the last shifted correlation surface evaluated there (poc.py:50) minus the half window; INT_MIN where the
+ * first window already left the image. ipk holds cap ints (2 per grid point); nx, ny receive the level's grid. */
+OFC_API int ofc_test_poc_peaks(ofc_engine* eng, const float* a, const float* b, size_t w, size_t h,
+                               const ofc_config* cfg, int level, int32_t* ipk, size_t cap, int32_t* nx, int32_t* ny,
+                               char* err, size_t errlen);
+
 /* The trusted pre-warp fill of phaseflow.prewarp (phaseflow.py:344-354) before the blur: ux, uy (doubles),
  * slope (4 planes), low mask -> filled ux, uy. */
 OFC_API int ofc_test_prewarp_fill(ofc_engine* eng, const uint8_t* low, const double* ux, const double* uy,

@@ -182,4 +182,11 @@ __device__ inline float2 sample_c32(const float2* __restrict__ c, int w, const T
 // scalar bspline prefilter pole
 __host__ __device__ inline double bspline_z() { return sqrt(3.0) - 2.0; }  // interp.py:9
 
+// one blob of the synthetic speckle renderer (synth.cu): reference centre, radius, amplitude and the subsample
+// rectangle [i0, i1) x [j0, j1) it adds to
+struct SynthBlob {
+  double cx, cy, r, a;
+  int i0, i1, j0, j1;
+};
+
 }  // namespace ofc

@@ -658,6 +658,9 @@ struct CoarseOut {
   double* uy;
   double* peak;
   std::vector<int> hxs, hys;
+  // per pyramid level (level 0 first): the integer peaks of the raw POC grid (2 ints per point) and its shape
+  std::vector<int*> ipk;
+  std::vector<int> lnx, lny;
 };
 
 // coarse_flow (poc.py:216-239); a, b: float32 images W x H on the device; init: 2 planes or null
@@ -691,6 +694,8 @@ CoarseOut coarse_dev(Lane& L, const float* a, const float* b, int W, int H, cons
   std::vector<int> ys0 = arange(c.poc_win / 2, H - c.poc_win / 2 + 1, c.grid_step);
   CoarseOut prev{};
   bool have = false;
+  std::vector<int*> ipk(Lv + 1);
+  std::vector<int> lnx(Lv + 1), lny(Lv + 1);
   for (int lev = Lv; lev >= 0; lev--) {
     int w = pws[lev], h = phs[lev];
     int wy = c.poc_win, wx = c.poc_win;
@@ -725,12 +730,18 @@ CoarseOut coarse_dev(Lane& L, const float* a, const float* b, int W, int H, cons
     double* gv = L.get<double>("poc_v" + sfx, (size_t)nx * ny);
     double* gp = L.get<double>("poc_p" + sfx, (size_t)nx * ny);
     PocLevel lv{w, h, nx, ny, wy, wx};
-    launch_poc_grid(pa[lev], pb[lev], lv, dxs, dys, iu, iv, dconst, gu, gv, gp, st);
+    ipk[lev] = L.get<int>("poc_ipk" + sfx, (size_t)2 * nx * ny);
+    lnx[lev] = nx;
+    lny[lev] = ny;
+    launch_poc_grid(pa[lev], pb[lev], lv, dxs, dys, iu, iv, dconst, gu, gv, gp, ipk[lev], st);
     uint8_t* scr = L.get<uint8_t>("poc_flags", (size_t)3 * nx * ny);
     launch_poc_clean(gu, gv, gp, nx, ny, c.poc_peak_min, c.median_thresh, iu, iv, scr, st);
-    prev = CoarseOut{nx, ny, dxs, dys, gu, gv, gp, gx, gy};
+    prev = CoarseOut{nx, ny, dxs, dys, gu, gv, gp, gx, gy, {}, {}, {}};
     have = true;
   }
+  prev.ipk = ipk;
+  prev.lnx = lnx;
+  prev.lny = lny;
   return prev;
 }
 
@@ -1596,47 +1607,63 @@ void laa_dev(Lane& L, int W, int H, const uint8_t* support, const T* ux, const T
 
 // synth.cu
 namespace ofc {
-void synth_render_dev(const double* bx, const double* by, const double* br, const double* ba, const int* cell_start,
-                      int ncx, int ncy, double x0, double y0, double cell, int w, int h, int ss, const ofc_field* field,
-                      float* out, cudaStream_t st);
+void synth_render_dev(const SynthBlob* blobs, const int* cell_start, int ncx, int ncy, double cell, int w, int h,
+                      int ss, const ofc_field* field, double* out, cudaStream_t st);
 }
 
 namespace {
-// bins the blobs by cell of the reference frame (host) and renders on the device
+// the field's forward map (synth.cu field_fwd), for the blobs' mapped centres
+void field_fwd_host(const ofc_field& f, double X, double Y, double& x, double& y) {
+  double dx = X - f.cx, dy = Y - f.cy;
+  x = f.cx + f.a00 * dx + f.a01 * dy + f.tx;
+  y = f.cy + f.a10 * dx + f.a11 * dy + f.ty;
+  if (f.amp != 0.0) {
+    double s = f.amp * std::sin(2 * PI * X / f.wavelength);
+    x = x + s * f.sx;
+    y = y + s * f.sy;
+  }
+}
+
+// per blob the reference's subsample rectangle (synth.py:174-179: floor/ceil of (mapped centre -+ (5.2 r + 2) + 0.5)
+// * ss, clipped to the image); blobs with an empty rectangle are dropped, the rest binned by the cell of the mapped
+// centre (cells 1 px wider than the largest half size, the grid starting one cell before the image) and rendered
+// on the device
 void launch_synth_render(Lane& L, const double* bx, const double* by, const double* br, const double* ba, size_t n,
-                         int w, int h, int ss, const ofc_field* field, float* out) {
-  const double cell = 16.0;
-  double x0 = 0, y0 = 0, x1 = w, y1 = h;
-  for (size_t i = 0; i < n; i++) {
-    x0 = std::min(x0, bx[i]); y0 = std::min(y0, by[i]);
-    x1 = std::max(x1, bx[i]); y1 = std::max(y1, by[i]);
+                         int w, int h, int ss, const ofc_field* field, double* out) {
+  double rmax = 0;
+  for (size_t i = 0; i < n; i++) rmax = std::max(rmax, br[i]);
+  const double cell = std::ceil(5.2 * rmax + 2.0) + 2.0;
+  const long W = (long)w * ss, H = (long)h * ss;
+  const int ncx = (int)std::ceil((w + 2 * cell) / cell) + 1, ncy = (int)std::ceil((h + 2 * cell) / cell) + 1;
+  std::vector<SynthBlob> kept;
+  std::vector<int> cid;
+  for (size_t k = 0; k < n; k++) {
+    double px = bx[k], py = by[k];
+    if (field) field_fwd_host(*field, bx[k], by[k], px, py);
+    double rad = 5.2 * br[k] + 2.0;
+    long j0 = std::max((long)std::floor((px - rad + 0.5) * ss), 0L);
+    long j1 = std::min((long)std::ceil((px + rad + 0.5) * ss), W);
+    long i0 = std::max((long)std::floor((py - rad + 0.5) * ss), 0L);
+    long i1 = std::min((long)std::ceil((py + rad + 0.5) * ss), H);
+    if (j0 >= j1 || i0 >= i1) continue;
+    int cx = std::min(std::max((int)std::floor((px + cell) / cell), 0), ncx - 1);
+    int cy = std::min(std::max((int)std::floor((py + cell) / cell), 0), ncy - 1);
+    kept.push_back({bx[k], by[k], br[k], ba[k], (int)i0, (int)i1, (int)j0, (int)j1});
+    cid.push_back(cy * ncx + cx);
   }
-  x0 -= cell; y0 -= cell;
-  int ncx = (int)((x1 - x0) / cell) + 2, ncy = (int)((y1 - y0) / cell) + 2;
   std::vector<int> cnt((size_t)ncx * ncy + 1, 0);
-  std::vector<int> cid(n);
-  for (size_t i = 0; i < n; i++) {
-    int cx = (int)((bx[i] - x0) / cell), cy = (int)((by[i] - y0) / cell);
-    cid[i] = cy * ncx + cx;
-    cnt[cid[i] + 1]++;
-  }
+  for (int c : cid) cnt[c + 1]++;
   for (size_t c = 1; c < cnt.size(); c++) cnt[c] += cnt[c - 1];
-  std::vector<double> sx(n), sy(n), sr(n), sa(n);
+  std::vector<SynthBlob> sorted(kept.size());
   std::vector<int> fill(cnt.begin(), cnt.end() - 1);
-  for (size_t i = 0; i < n; i++) {
-    int d = fill[cid[i]]++;
-    sx[d] = bx[i]; sy[d] = by[i]; sr[d] = br[i]; sa[d] = ba[i];
-  }
-  double* dx = L.upload("syn_x", sx.data(), n);
-  double* dy = L.upload("syn_y", sy.data(), n);
-  double* dr = L.upload("syn_r", sr.data(), n);
-  double* da = L.upload("syn_a", sa.data(), n);
+  for (size_t i = 0; i < kept.size(); i++) sorted[fill[cid[i]]++] = kept[i];
+  SynthBlob* db = L.upload("syn_blobs", sorted.data(), std::max<size_t>(sorted.size(), 1));
   int* dc = L.upload("syn_cells", cnt.data(), cnt.size());
-  float* dout = L.get<float>("syn_out", (size_t)w * h);
+  double* dout = L.get<double>("syn_out", (size_t)w * h);
   ofc_field* df = nullptr;
   if (field) df = L.upload("syn_field", field, 1);
-  synth_render_dev(dx, dy, dr, da, dc, ncx, ncy, x0, y0, cell, w, h, ss, df, dout, L.stream);
-  OFC_CUDA(cudaMemcpyAsync(out, dout, (size_t)w * h * sizeof(float), cudaMemcpyDeviceToHost, L.stream));
+  synth_render_dev(db, dc, ncx, ncy, cell, w, h, ss, df, dout, L.stream);
+  OFC_CUDA(cudaMemcpyAsync(out, dout, (size_t)w * h * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
   OFC_CUDA(cudaStreamSynchronize(L.stream));
 }
 }  // namespace
@@ -3011,6 +3038,27 @@ int ofc_test_large_components(ofc_engine* e, const uint8_t* b, size_t w, size_t 
   });
 }
 
+int ofc_test_poc_peaks(ofc_engine* e, const float* a, const float* b, size_t w, size_t h, const ofc_config* c,
+                       int level, int32_t* ipk, size_t cap, int32_t* nx, int32_t* ny, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    cfg_check(c);
+    check_sizes(w, h);
+    if (!a || !b || !ipk || !nx || !ny) throw Error(OFC_ERR_ARG, "null argument");
+    const size_t N = w * h;
+    float* da = L.upload("in_i1", a, N);
+    float* db = L.upload("in_i2", b, N);
+    CoarseOut g = coarse_dev(L, da, db, (int)w, (int)h, nullptr, *c);
+    if (level < 0 || level >= (int)g.ipk.size())
+      throw Error(OFC_ERR_ARG, "pyramid level " + std::to_string(level) + " does not exist");
+    const size_t n = (size_t)g.lnx[level] * g.lny[level];
+    if (2 * n > cap) throw Error(OFC_ERR_ARG, "ipk holds fewer than 2 * nx * ny values");
+    OFC_CUDA(cudaMemcpyAsync(ipk, g.ipk[level], 2 * n * sizeof(int), cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+    *nx = g.lnx[level];
+    *ny = g.lny[level];
+  });
+}
+
 int ofc_test_prewarp_fill(ofc_engine* e, const uint8_t* low, const double* ux, const double* uy, const double* slope,
                           size_t w, size_t h, double radius, double* oux, double* ouy, char* err, size_t errlen) {
   return guarded(e, err, errlen, [&](Lane& L) {
@@ -3125,7 +3173,7 @@ int ofc_profile_read(ofc_engine* e, char* names, size_t stride, uint64_t* counts
 }
 
 int ofc_synth_render(ofc_engine* e, const double* bx, const double* by, const double* br, const double* ba, size_t n,
-                     size_t w, size_t h, int ss, const ofc_field* field, float* out, char* err, size_t errlen) {
+                     size_t w, size_t h, int ss, const ofc_field* field, double* out, char* err, size_t errlen) {
   return guarded(e, err, errlen, [&](Lane& L) {
     check_sizes(w, h);
     if (ss < 1 || ss > 16) throw Error(OFC_ERR_ARG, "ss must lie in [1, 16]");

@@ -42,14 +42,16 @@ __global__ void k_ccl_init(const uint8_t* __restrict__ b, int n, int* parent, in
   }
 }
 
+// rows strided by gridDim.y: a grid's y extent stops at 65,535, below the height of a tall image
 __global__ void k_ccl_merge(const uint8_t* __restrict__ b, int W, int H, int* parent) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y;
   if (x >= W) return;
-  int p = y * W + x;
-  if (!b[p]) return;
-  if (x + 1 < W && b[p + 1]) uf_union(parent, p, p + 1);
-  if (y + 1 < H && b[p + W]) uf_union(parent, p, p + W);
+  for (int y = blockIdx.y; y < H; y += gridDim.y) {
+    int p = y * W + x;
+    if (!b[p]) continue;
+    if (x + 1 < W && b[p + 1]) uf_union(parent, p, p + 1);
+    if (y + 1 < H && b[p + W]) uf_union(parent, p, p + W);
+  }
 }
 
 // after the merge: every pixel points to its root. The walk only reads (a splitting write could put an
@@ -88,7 +90,7 @@ void launch_large_components(const uint8_t* b, int W, int H, double min_area, in
   int n = W * H;
   unsigned g = std::min(div_up(n, 256), 8192u);
   OFC_LAUNCH(k_ccl_init, g, 256, 0, st, b, n, parent, size);
-  OFC_LAUNCH(k_ccl_merge, dim3(div_up(W, 128), H), 128, 0, st, b, W, H, parent);
+  OFC_LAUNCH(k_ccl_merge, dim3(div_up(W, 128), std::min(H, 65535)), 128, 0, st, b, W, H, parent);
   OFC_LAUNCH(k_ccl_flatten, g, 256, 0, st, b, n, parent);
   OFC_LAUNCH(k_ccl_count, g, 256, 0, st, b, n, parent, size);
   OFC_LAUNCH(k_ccl_mark, g, 256, 0, st, b, n, parent, size, min_area, out);

@@ -106,7 +106,7 @@ size_t poc_const_bytes();
 void poc_const_host(int wy, int wx, void* out);
 void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const int* xs, const int* ys,
                      const double* iux, const double* iuy, const void* dconst, double* ux, double* uy, double* peak,
-                     cudaStream_t st);
+                     int* ipk, cudaStream_t st);
 // clean (poc.py:95-140) in one thread block; fallback = init (nullable)
 void launch_poc_clean(double* ux, double* uy, double* peak, int nx, int ny, double peak_min, double thresh,
                       const double* fbx, const double* fby, uint8_t* scratch, cudaStream_t st);

@@ -64,6 +64,14 @@ extern "C" int ofc_large_components_noalloc(const uint8_t* d_mask, size_t w, siz
     }
     scratch = g_scratch_ptr[dev];
   }
+  // an error left pending by the caller's own earlier work would otherwise be reported as this call's failure
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    std::string m = std::string("ofc_large_components_noalloc: a CUDA error was pending before this call: ") +
+                    cudaGetErrorString(e);
+    set_msg(err, errlen, m.c_str());
+    return OFC_ERR_DEVICE;
+  }
   try {
     // k_ccl_init rewrites parent[] and zeroes size[] over the first w * h entries: no state of an earlier call
     // survives into this one

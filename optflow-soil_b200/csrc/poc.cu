@@ -2,6 +2,7 @@
 // windowed band-limited phase-only correlation on a grid, one thread block per grid point, with the
 // re-centring iterations, the outlier clean-up and the bilinear grid sampling.
 #include <cfloat>
+#include <climits>
 #include <cstring>
 
 #include "kernels.cuh"
@@ -317,15 +318,19 @@ __device__ void poc_shift_dev(const double* __restrict__ b, int W, int x0, int y
     res[0] = ix - wx / 2 + sxp;
     res[1] = iy - wy / 2 + syp;
     res[2] = c;
+    res[3] = (double)bi;  // the unclamped argmax of the shifted surface
   }
   __syncthreads();
 }
 
+// ipk (nullable): per grid point the integer peak of the last surface evaluated, round(d) + argmax - half window
+// (x, y), INT_MIN where the first window already left the image
 __global__ void __launch_bounds__(POC_T, 2) k_poc_grid(const double* __restrict__ a, const double* __restrict__ b,
                                                         int W, int H, int wy, int wx, const int* __restrict__ xs,
                                                         const int* __restrict__ ys, int nx, const double* iux,
                                                         const double* iuy, const PocConst* __restrict__ pcg,
-                                                        double lpm, double* oux, double* ouy, double* opeak) {
+                                                        double lpm, double* oux, double* ouy, double* opeak,
+                                                        int* ipk) {
   extern __shared__ double2 dsm[];
   double2* Z = dsm;
   const int qy = wy / 4, qx = wx / 4;
@@ -333,7 +338,7 @@ __global__ void __launch_bounds__(POC_T, 2) k_poc_grid(const double* __restrict_
   double2* alp = Z + wy * (wx + 1);
   __shared__ PocConst pc;
   __shared__ double red[POC_T / 32];
-  __shared__ double res[3];
+  __shared__ double res[4];
   for (int i = threadIdx.x; i < (int)(sizeof(PocConst) / sizeof(double)); i += POC_T)
     ((double*)&pc)[i] = ((const double*)pcg)[i];
   const int gi = blockIdx.x;
@@ -372,6 +377,7 @@ __global__ void __launch_bounds__(POC_T, 2) k_poc_grid(const double* __restrict_
   __syncthreads();
   double dx = iux ? iux[gi] : 0.0, dy = iuy ? iuy[gi] : 0.0;
   double pk = 0.0;
+  int px = INT_MIN, py = INT_MIN;
   for (int it = 0; it < 3; it++) {
     double ox = rint(dx), oy = rint(dy);  // Python round(): half to even
     long y0 = y - hy + (long)oy, x0 = x - hx + (long)ox;
@@ -379,6 +385,9 @@ __global__ void __launch_bounds__(POC_T, 2) k_poc_grid(const double* __restrict_
     poc_shift_dev(b, W, (int)x0, (int)y0, wy, wx, pc, alp, nlx, lpm, Z, red, res);
     double sx = res[0], sy = res[1];
     pk = res[2];
+    const int am = (int)res[3];
+    px = (int)ox + am % wx - hx;
+    py = (int)oy + am / wx - hy;
     dx = ox + sx;
     dy = oy + sy;
     if (fabs(sx) < 0.5 && fabs(sy) < 0.5) break;
@@ -387,6 +396,10 @@ __global__ void __launch_bounds__(POC_T, 2) k_poc_grid(const double* __restrict_
     oux[gi] = dx;
     ouy[gi] = dy;
     opeak[gi] = pk;
+    if (ipk) {
+      ipk[2 * gi] = px;
+      ipk[2 * gi + 1] = py;
+    }
   }
 }
 
@@ -534,6 +547,7 @@ __device__ void poc_shift64(const double* __restrict__ b, int W, int x0, int y0,
     res[0] = ix - 32 + sxp;
     res[1] = iy - 32 + syp;
     res[2] = c;
+    res[3] = (double)bi;  // the unclamped argmax of the shifted surface
   }
   __syncthreads();
 }
@@ -542,14 +556,15 @@ __global__ void __launch_bounds__(POC_T, 3) k_poc_grid64(const double* __restric
                                                           int W, int H, const int* __restrict__ xs,
                                                           const int* __restrict__ ys, int nx, const double* iux,
                                                           const double* iuy, const PocConst* __restrict__ pcg,
-                                                          double lpm, double* oux, double* ouy, double* opeak) {
+                                                          double lpm, double* oux, double* ouy, double* opeak,
+                                                          int* ipk) {
   extern __shared__ double2 dsm[];
   double2* Hz = dsm;                    // 64 x 17
   double2* alp = Hz + 64 * ZS;          // 33 x 17
   double* surf = (double*)(alp + 33 * ZS);  // 64 x 64
   __shared__ PocConst pc;
   __shared__ double red[POC_T / 32];
-  __shared__ double res[3];
+  __shared__ double res[4];
   for (int i = threadIdx.x; i < (int)(sizeof(PocConst) / sizeof(double)); i += POC_T)
     ((double*)&pc)[i] = ((const double*)pcg)[i];
   const int gi = blockIdx.x;
@@ -576,6 +591,7 @@ __global__ void __launch_bounds__(POC_T, 3) k_poc_grid64(const double* __restric
   __syncthreads();
   double dx = iux ? iux[gi] : 0.0, dy = iuy ? iuy[gi] : 0.0;
   double pk = 0.0;
+  int px = INT_MIN, py = INT_MIN;
   for (int it = 0; it < 3; it++) {
     double ox = rint(dx), oy = rint(dy);  // Python round(): half to even
     long y0 = y - 32 + (long)oy, x0 = x - 32 + (long)ox;
@@ -583,6 +599,9 @@ __global__ void __launch_bounds__(POC_T, 3) k_poc_grid64(const double* __restric
     poc_shift64(b, W, (int)x0, (int)y0, pc, tw, alp, lpm, Hz, surf, red, res);
     double sx = res[0], sy = res[1];
     pk = res[2];
+    const int am = (int)res[3];
+    px = (int)ox + (am & 63) - 32;
+    py = (int)oy + (am >> 6) - 32;
     dx = ox + sx;
     dy = oy + sy;
     if (fabs(sx) < 0.5 && fabs(sy) < 0.5) break;
@@ -591,6 +610,10 @@ __global__ void __launch_bounds__(POC_T, 3) k_poc_grid64(const double* __restric
     oux[gi] = dx;
     ouy[gi] = dy;
     opeak[gi] = pk;
+    if (ipk) {
+      ipk[2 * gi] = px;
+      ipk[2 * gi + 1] = py;
+    }
   }
 }
 
@@ -613,7 +636,7 @@ void poc_const_host(int wy, int wx, void* out) {
 
 void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const int* xs, const int* ys,
                      const double* iux, const double* iuy, const void* dconst, double* ux, double* uy, double* peak,
-                     cudaStream_t st) {
+                     int* ipk, cudaStream_t st) {
   auto ok_len = [](int n) { return n == 16 || n == 32 || n == 64; };
   if (!ok_len(lv.wy) || !ok_len(lv.wx))
     throw Error(OFC_ERR_ARG, "the CUDA engine's POC windows are 16, 32 or 64 px a side (poc_win <= 64)");
@@ -623,13 +646,13 @@ void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const
     const size_t sm64 = (size_t)(64 * ZS + 33 * ZS) * sizeof(double2) + 64 * 64 * sizeof(double);
     OFC_CUDA(cudaFuncSetAttribute((const void*)k_poc_grid64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64));
     OFC_LAUNCH(k_poc_grid64, lv.nx * lv.ny, POC_T, sm64, st, a, b, lv.W, lv.H, xs, ys, lv.nx, iux, iuy,
-               (const PocConst*)dconst, lpm, ux, uy, peak);
+               (const PocConst*)dconst, lpm, ux, uy, peak, ipk);
     return;
   }
   size_t smem = (size_t)(lv.wy * (lv.wx + 1) + (2 * (lv.wy / 4) + 1) * (2 * (lv.wx / 4) + 1)) * sizeof(double2);
   OFC_CUDA(cudaFuncSetAttribute((const void*)k_poc_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   OFC_LAUNCH(k_poc_grid, lv.nx * lv.ny, POC_T, smem, st, a, b, lv.W, lv.H, lv.wy, lv.wx, xs, ys, lv.nx, iux, iuy,
-             (const PocConst*)dconst, lpm, ux, uy, peak);
+             (const PocConst*)dconst, lpm, ux, uy, peak, ipk);
 }
 
 // ---------------------------------------------------------------- clean (poc.py:95-140)

@@ -230,6 +230,8 @@ TEST_SIGNATURES = {
                                            ctypes.POINTER(OfcConfig), c_double_p, _E, _S]),
     "ofc_test_prewarp_fill": (ctypes.c_int, [_P, c_u8_p, c_double_p, c_double_p, c_double_p, _S, _S, ctypes.c_double,
                                              c_double_p, c_double_p, _E, _S]),
+    "ofc_test_poc_peaks": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, ctypes.POINTER(OfcConfig), ctypes.c_int,
+                                          c_i32_p, _S, c_i32_p, c_i32_p, _E, _S]),
 }
 
 
@@ -242,7 +244,7 @@ class OfcField(ctypes.Structure):
 # include/optflow_cuda_synth.h
 SYNTH_SIGNATURES = {
     "ofc_synth_render": (ctypes.c_int, [_P, c_double_p, c_double_p, c_double_p, c_double_p, _S, _S, _S, ctypes.c_int,
-                                        ctypes.POINTER(OfcField), c_float_p, _E, _S]),
+                                        ctypes.POINTER(OfcField), c_double_p, _E, _S]),
     "ofc_set_profile": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "ofc_profile_read": (ctypes.c_int, [_P, ctypes.c_char_p, _S, ctypes.POINTER(ctypes.c_uint64), c_double_p, _S]),
 }

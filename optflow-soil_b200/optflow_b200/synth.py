@@ -3,14 +3,16 @@
 The blob draws follow the reference's generator call for call (python/optflow_ref/synth.py:20-29:
 numpy default_rng(seed), uniform centres over the image plus a margin, uniform radii and amplitudes with
 random sign), so a seed gives the reference's pattern; the rendering is the same analytic Gaussian-blob model
-(synth.py:150-190) evaluated by a CUDA kernel; degrade() is synth.py:192-205 (noise, clip, quantisation).
+(synth.py:150-190: the same per-blob subsample rectangles, float64 throughout) evaluated by a CUDA kernel, so
+render() returns the reference's float64 image to rounding; degrade() is synth.py:192-205 (noise, clip,
+quantisation).
 """
 import ctypes
 from dataclasses import dataclass
 
 import numpy as np
 
-from ._abi import OfcField, c_double_p, c_float_p
+from ._abi import OfcField, c_double_p
 from .api import _ptr, default_engine
 
 
@@ -68,10 +70,10 @@ def uniform_strain(exx, eyy, center, exy=0.0, t=(0.0, 0.0)) -> Field:
 def render(p: Pattern, h, w, field: Field = None, ss=4, engine=None) -> np.ndarray:
     eng = engine or default_engine()
     arrs = [np.ascontiguousarray(v, dtype=np.float64) for v in (p.cx, p.cy, p.r, p.a)]
-    out = np.empty((h, w), np.float32)
+    out = np.empty((h, w), np.float64)
     f = field.ofc() if field is not None else None
     eng._call("ofc_synth_render", *[_ptr(a, c_double_p) for a in arrs], len(p.cx), w, h, int(ss),
-              ctypes.byref(f) if f is not None else None, _ptr(out, c_float_p))
+              ctypes.byref(f) if f is not None else None, _ptr(out, c_double_p))
     return out
 
 
@@ -99,3 +101,14 @@ def polygon_mask(h, w, poly):
         xint = (x2 - x1) * (yy - y1) / np.where(y2 != y1, y2 - y1, 1.0) + x1
         inside ^= crosses & (xx < xint)
     return inside
+
+
+def rect_roi(h, w, x0, y0, x1, y1):
+    """The ROI mask the reference CLI draws for the axis-aligned rectangle polygon [[x0, y0], [x1, y0], [x1, y1],
+    [x0, y1]] (rust/crates/optflow-cli/src/polygon.rs:10-16, Pillow's scan-line filler, python/optflow_ref/io.py:155):
+    vertices truncated toward zero, then every row from the top to the bottom vertex filled from the left to the
+    right vertex, both ends inclusive."""
+    m = np.zeros((h, w), bool)
+    c0, r0, c1, r1 = int(x0), int(y0), int(x1), int(y1)
+    m[max(r0, 0):min(r1 + 1, h), max(c0, 0):min(c1 + 1, w)] = True
+    return m

@@ -3,7 +3,7 @@ import ctypes
 
 import numpy as np
 
-from ._abi import c_double_p, c_float_p, c_u8_p
+from ._abi import c_double_p, c_float_p, c_i32_p, c_u8_p
 from .api import _f32, _ptr, default_engine
 from .config import Config
 
@@ -75,6 +75,21 @@ def large_components(b, min_area, engine=None):
     out = np.empty_like(a)
     eng._call("ofc_test_large_components", _ptr(a, c_u8_p), w, h, ctypes.c_double(min_area), _ptr(out, c_u8_p))
     return out.astype(bool)
+
+
+def poc_peaks(I1, I2, cfg=None, level=0, engine=None):
+    """The integer POC peaks of pyramid level `level` of coarse_flow (ofc_test_poc_peaks): (ny, nx, 2) int32 of
+    (x, y), INT_MIN where no window was evaluated."""
+    eng = engine or default_engine()
+    a, b = _f32(I1), _f32(I2)
+    h, w = a.shape
+    c = (cfg or Config()).to_ofc()
+    cap = 2 * (h * w + 16)
+    buf = np.empty(cap, np.int32)
+    nx, ny = ctypes.c_int32(), ctypes.c_int32()
+    eng._call("ofc_test_poc_peaks", _ptr(a, c_float_p), _ptr(b, c_float_p), w, h, ctypes.byref(c), int(level),
+              _ptr(buf, c_i32_p), cap, ctypes.byref(nx), ctypes.byref(ny))
+    return buf[:2 * nx.value * ny.value].reshape(ny.value, nx.value, 2).copy()
 
 
 def prewarp_fill(low, ux, uy, slope, radius, engine=None):

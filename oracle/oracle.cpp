@@ -19,6 +19,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <climits>
 #include <limits>
 #include <stdexcept>
 #include <string>
@@ -27,6 +28,7 @@
 #include <omp.h>
 
 #include "../include/optflow_cuda.h"
+#include "../include/optflow_cuda_synth.h"
 
 namespace {
 
@@ -794,7 +796,13 @@ void refine_conf(const RawFlow& rf, const ofc_config& c, ImgD& conf) {
 }
 
 // ------------------------------------------------------------------ POC (poc.py)
-struct Grid { vector<int> xs, ys; ImgD ux, uy, peak; };
+struct Grid {
+  vector<int> xs, ys;
+  ImgD ux, uy, peak;
+  // the integer peak of the last correlation surface evaluated at each point: window offset (round(d)) plus the
+  // unclamped argmax of the shifted surface minus the half window (poc.py:50 np.argmax); INT_MIN if none was
+  vector<int> ipx, ipy;
+};
 
 double parabola(double m, double c, double p) {  // poc.py:34-36
   double den = m - 2.0 * c + p;
@@ -841,7 +849,8 @@ struct PocTables {
 };
 
 // poc_shift (poc.py:39-54): a, b are h x w windows (row-major)
-void poc_shift(const PocTables& T, const vector<double>& a, const vector<double>& b, double& dx, double& dy, double& pk) {
+void poc_shift(const PocTables& T, const vector<double>& a, const vector<double>& b, double& dx, double& dy, double& pk,
+               size_t* argmax = nullptr) {
   int h = T.h, w = T.w;
   size_t n = (size_t)h * w;
   double ma = mean_of(a), mb = mean_of(b);
@@ -867,6 +876,7 @@ void poc_shift(const PocTables& T, const vector<double>& a, const vector<double>
     if (std::isnan(r[i])) { best = i; break; }
     if (r[i] > r[best]) best = i;
   }
+  if (argmax) *argmax = best;
   int iy = (int)(best / w), ix = (int)(best % w);
   iy = std::min(std::max(iy, 1), h - 2);
   ix = std::min(std::max(ix, 1), w - 2);
@@ -893,6 +903,8 @@ Grid poc_grid(const ImgD& I1, const ImgD& I2, const vector<int>& xs, const vecto
   Grid g;
   g.xs = xs; g.ys = ys;
   g.ux = ImgD(nx, ny); g.uy = ImgD(nx, ny); g.peak = ImgD(nx, ny);
+  g.ipx.assign((size_t)nx * ny, INT_MIN);
+  g.ipy.assign((size_t)nx * ny, INT_MIN);
   PocTables T(wy, wx);
 #pragma omp parallel for schedule(dynamic, 4)
   for (int i = 0; i < ny; i++) {
@@ -910,7 +922,10 @@ Grid poc_grid(const ImgD& I1, const ImgD& I2, const vector<int>& xs, const vecto
         for (int r = 0; r < wy; r++)
           for (int q = 0; q < wx; q++) b[(size_t)r * wx + q] = I2((int)(x0 + q), (int)(y0 + r));
         double sx, sy;
-        poc_shift(T, a, b, sx, sy, pk);
+        size_t am = 0;
+        poc_shift(T, a, b, sx, sy, pk, &am);
+        g.ipx[(size_t)i * nx + j] = (int)(ox + (long)(am % wx) - wx / 2);
+        g.ipy[(size_t)i * nx + j] = (int)(oy + (long)(am / wx) - wy / 2);
         dx = ox + sx;
         dy = oy + sy;
         if (std::fabs(sx) < 0.5 && std::fabs(sy) < 0.5) break;
@@ -1035,7 +1050,9 @@ int n_levels(double max_disp, int win, int h, int w) {  // poc.py:190-195
 }
 
 // coarse_flow (poc.py:216-239)
-Grid coarse_flow(const ImgD& I1, const ImgD& I2, const ofc_config& c, const ImgD* idx, const ImgD* idy) {
+// raw (optional): the uncleaned POC grid of every level, level 0 first
+Grid coarse_flow(const ImgD& I1, const ImgD& I2, const ofc_config& c, const ImgD* idx, const ImgD* idy,
+                 vector<Grid>* raw_levels = nullptr) {
   int H = I1.h, W = I1.w;
   vector<int> xs, ys;
   grid_points(H, W, c.grid_step, c.poc_win, c.poc_win, xs, ys);
@@ -1043,6 +1060,7 @@ Grid coarse_flow(const ImgD& I1, const ImgD& I2, const ofc_config& c, const ImgD
   vector<std::pair<ImgD, ImgD>> pyr;
   pyr.push_back({I1, I2});
   for (int l = 0; l < L; l++) pyr.push_back({downsample(pyr.back().first), downsample(pyr.back().second)});
+  if (raw_levels) raw_levels->assign(L + 1, Grid());
   Grid g;
   bool have = false;
   for (int lev = L; lev >= 0; lev--) {
@@ -1079,6 +1097,7 @@ Grid coarse_flow(const ImgD& I1, const ImgD& I2, const ofc_config& c, const ImgD
       has_init = true;
     }
     Grid raw = poc_grid(a, b, gx, gy, wy, wx, has_init ? &ix : nullptr, has_init ? &iy : nullptr);
+    if (raw_levels) (*raw_levels)[lev] = raw;
     g = clean(raw, c.poc_peak_min, c.median_thresh, has_init ? &ix : nullptr, has_init ? &iy : nullptr);
     have = true;
   }
@@ -1224,6 +1243,97 @@ void finish(const ImgD& ux, const ImgD& uy, const ImgD& conf, const ImgB* mask, 
   st = strain_fields(a, b, cc, d);
 }
 
+// ------------------------------------------------------------------ synthetic speckle (synth.py:20-190)
+// The field x = c + A (X - c) + t + amp sin(2 pi X_x / wavelength) (sx, sy) of include/optflow_cuda_synth.h.
+void field_fwd(const ofc_field& f, double X, double Y, double& x, double& y) {  // synth.py:42-46
+  double dx = X - f.cx, dy = Y - f.cy;
+  x = f.cx + f.a00 * dx + f.a01 * dy + f.tx;
+  y = f.cy + f.a10 * dx + f.a11 * dy + f.ty;
+  if (f.amp != 0.0) {
+    double s = f.amp * std::sin(2 * PI * X / f.wavelength);
+    x = x + s * f.sx;
+    y = y + s * f.sy;
+  }
+}
+
+// the affine inverse (synth.py:48-51), then Newton steps on the sinusoid until the step is below 1e-13
+void field_inv(const ofc_field& f, double x, double y, double& X, double& Y) {
+  double det = f.a00 * f.a11 - f.a01 * f.a10;
+  double b00 = f.a11 / det, b01 = -f.a01 / det, b10 = -f.a10 / det, b11 = f.a00 / det;
+  double dx = x - f.cx - f.tx, dy = y - f.cy - f.ty;
+  X = f.cx + b00 * dx + b01 * dy;
+  Y = f.cy + b10 * dx + b11 * dy;
+  if (f.amp == 0.0) return;
+  for (int it = 0; it < 30; it++) {
+    double fx, fy;
+    field_fwd(f, X, Y, fx, fy);
+    fx -= x;
+    fy -= y;
+    double ds = f.amp * (2 * PI / f.wavelength) * std::cos(2 * PI * X / f.wavelength);
+    double j00 = f.a00 + ds * f.sx, j01 = f.a01, j10 = f.a10 + ds * f.sy, j11 = f.a11;
+    double d = j00 * j11 - j01 * j10;
+    double sx = (j11 * fx - j01 * fy) / d, sy = (-j10 * fx + j00 * fy) / d;
+    X -= sx;
+    Y -= sy;
+    if (std::fabs(sx) + std::fabs(sy) < 1e-13) break;
+  }
+}
+
+// synth.render (synth.py:150-190) without a gap: every blob k, in index order, adds a_k exp(-d^2 / (2 r_k^2)) to
+// the ss x ss subsamples of the rectangle of half size 5.2 r_k + 2 around its mapped centre, d measured between
+// the subsample's inverse-mapped position and the blob's reference centre; a pixel is 0.5 + 0.25 tanh(mean).
+// Rows of pixels run in parallel; each row adds its blobs in index order, so the sums are the reference's.
+void render(const double* bx, const double* by, const double* br, const double* ba, size_t n, int w, int h, int ss,
+            const ofc_field* f, double* out) {
+  const long W = (long)w * ss, H = (long)h * ss;
+  vector<long> i0(n), i1(n), j0(n), j1(n);
+  vector<vector<int>> rows(h);
+  for (size_t k = 0; k < n; k++) {
+    double px = bx[k], py = by[k];
+    if (f) field_fwd(*f, bx[k], by[k], px, py);
+    double rad = 5.2 * br[k] + 2.0;
+    j0[k] = std::max((long)std::floor((px - rad + 0.5) * ss), 0L);
+    j1[k] = std::min((long)std::ceil((px + rad + 0.5) * ss), W);
+    i0[k] = std::max((long)std::floor((py - rad + 0.5) * ss), 0L);
+    i1[k] = std::min((long)std::ceil((py + rad + 0.5) * ss), H);
+    if (j0[k] >= j1[k] || i0[k] >= i1[k]) continue;
+    for (long y = i0[k] / ss; y <= (i1[k] - 1) / ss; y++) rows[y].push_back((int)k);
+  }
+  vector<double> off(ss);
+  for (int s = 0; s < ss; s++) off[s] = (s + 0.5) / ss - 0.5;
+#pragma omp parallel
+  {
+    vector<double> X(ss * W), Y(ss * W), acc(ss * W);
+#pragma omp for schedule(dynamic, 4)
+    for (int y = 0; y < h; y++) {
+      for (int si = 0; si < ss; si++)
+        for (long j = 0; j < W; j++) {
+          double xs = (double)(j / ss) + off[j % ss], ys = (double)y + off[si];
+          size_t q = (size_t)si * W + j;
+          if (f) field_inv(*f, xs, ys, X[q], Y[q]);
+          else { X[q] = xs; Y[q] = ys; }
+          acc[q] = 0.0;
+        }
+      for (int k : rows[y]) {
+        long a0 = std::max(i0[k], (long)y * ss), a1 = std::min(i1[k], (long)(y + 1) * ss);
+        double r2 = 2 * (br[k] * br[k]);
+        for (long i = a0; i < a1; i++)
+          for (long j = j0[k]; j < j1[k]; j++) {
+            size_t q = (size_t)(i - (long)y * ss) * W + j;
+            double dx = X[q] - bx[k], dy = Y[q] - by[k];
+            acc[q] += ba[k] * std::exp(-(dx * dx + dy * dy) / r2);
+          }
+      }
+      for (int x = 0; x < w; x++) {
+        double s = 0;
+        for (int si = 0; si < ss; si++)
+          for (int sj = 0; sj < ss; sj++) s += acc[(size_t)si * W + (size_t)x * ss + sj];
+        out[(size_t)y * w + x] = 0.5 + 0.25 * std::tanh(s / (ss * ss));
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------------ glue
 ImgD from_ptr(const double* p, int w, int h) { ImgD a(w, h); std::memcpy(a.d.data(), p, sizeof(double) * a.n()); return a; }
 void to_ptr(const ImgD& a, double* p) { if (p) std::memcpy(p, a.d.data(), sizeof(double) * a.n()); }
@@ -1232,6 +1342,29 @@ void to_ptr(const ImgD& a, double* p) { if (p) std::memcpy(p, a.d.data(), sizeof
 
 // ------------------------------------------------------------------ C API (test infrastructure)
 extern "C" {
+
+void oro_render(const double* bx, const double* by, const double* br, const double* ba, size_t n, int w, int h, int ss,
+                const ofc_field* f, double* out) {
+  render(bx, by, br, ba, n, w, h, ss, f, out);
+}
+
+// the integer POC peaks (Grid::ipx, ipy) of pyramid level `level` of coarse_flow; returns the level's nx * ny, or
+// -1 when the level does not exist (cap: the room in ipk, 2 ints per grid point)
+int oro_coarse_peaks(const double* a, const double* b, int w, int h, const double* iux, const double* iuy,
+                     const ofc_config* c, int level, int* ipk, size_t cap, int* nx, int* ny) {
+  ImgD A = from_ptr(a, w, h), B = from_ptr(b, w, h), ix, iy;
+  if (iux) { ix = from_ptr(iux, w, h); iy = from_ptr(iuy, w, h); }
+  vector<Grid> raw;
+  coarse_flow(A, B, *c, iux ? &ix : nullptr, iux ? &iy : nullptr, &raw);
+  if (level < 0 || level >= (int)raw.size()) return -1;
+  const Grid& g = raw[level];
+  *nx = (int)g.xs.size();
+  *ny = (int)g.ys.size();
+  size_t n = g.ipx.size();
+  if (2 * n > cap) return -1;
+  for (size_t i = 0; i < n; i++) { ipk[2 * i] = g.ipx[i]; ipk[2 * i + 1] = g.ipy[i]; }
+  return (int)n;
+}
 
 void oro_set_f32_storage(int on) { g_f32_storage = on != 0; }
 

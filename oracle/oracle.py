@@ -442,3 +442,36 @@ def to_gray(px, pixel, scale=1):
             rs = rs + b[:, dy, :, dx]
         total = total + rs
     return (total / float(scale * scale)).astype(np.float32), g
+
+
+def render(p, h, w, field=None, ss=4):
+    """synth.render (python/optflow_ref/synth.py:150-190): the float64 speckle image of pattern p (cx, cy, r, a)
+    deformed by field (an object with .ofc(), the struct of include/optflow_cuda_synth.h; None: the reference
+    image), ss x ss subsamples per pixel."""
+    arrs = [_d(v) for v in (p.cx, p.cy, p.r, p.a)]
+    out = np.empty((h, w))
+    f = field.ofc() if field is not None else None
+    lib().oro_render(*[_p(a) for a in arrs], ctypes.c_size_t(arrs[0].size), int(w), int(h), int(ss),
+                     ctypes.byref(f) if f is not None else None, _p(out))
+    return out
+
+
+def coarse_peaks(I1, I2, cfg=None, level=0, init_dense=None):
+    """The integer POC peak of every grid point of pyramid level `level` of coarse_flow (level 0 = full size): the
+    window offset round(d) plus the argmax of the last shifted correlation surface evaluated there, minus the half
+    window (poc.py:50, 82-88), as an (ny, nx, 2) int array of (x, y); INT_MIN where no window was evaluated.
+    None when the level does not exist."""
+    a, b = _d(I1), _d(I2)
+    h, w = a.shape
+    pc, _ = _cfg(cfg)
+    iux = iuy = None
+    if init_dense is not None:
+        iux, iuy = _d(init_dense[0]), _d(init_dense[1])
+    cap = 2 * (h * w + 16)
+    buf = np.empty(cap, np.int32)
+    nx, ny = ctypes.c_int(), ctypes.c_int()
+    n = lib().oro_coarse_peaks(_p(a), _p(b), w, h, _p(iux), _p(iuy), pc, int(level), _p(buf), ctypes.c_size_t(cap),
+                               ctypes.byref(nx), ctypes.byref(ny))
+    if n < 0:
+        return None
+    return buf[:2 * n].reshape(ny.value, nx.value, 2).copy()

@@ -1,0 +1,114 @@
+"""The benchmark's 2048^2 pair (the headline configuration) through the C ABI, against the reference and the oracle.
+
+Inputs: the pair rendered on the GPU (ofc_synth_render) must be the reference generator's uint8 frames bit for bit
+(SHA-256 written by tests/golden/make_golden_config2.py from the reference's own synth.render/degrade), with the
+reference's io.polygon_mask ROI. Checks, in the words of the pair path's contract:
+  * POC integer peak indices identical at every grid point of both pyramid levels, against the reference's own
+    coarse_flow (golden) and the oracle; the cleaned coarse grid within 1e-3 px of the reference's;
+  * ux and uy within 1e-3 px (max) of the float64 oracle on the pixels valid in both;
+  * every strain component within 1e-5 (max) where the 15 x 15 strain window sees no validity difference;
+  * the low-confidence masks identical except at pixels whose oracle confidence lies within CONF_BAND of conf_min,
+    and the validity masks identical except within the guard distance of such a flip.
+The measured errors (max and RMS of ux, uy, conf and each strain, the flip band, the error against the known field)
+are printed on one line starting with CONFIG2 (run with -s to see it).
+"""
+import hashlib
+import json
+
+import numpy as np
+import pytest
+from conftest import golden
+
+from optflow_b200 import Config, coarse_flow, synth, testing, track_pair
+
+pytestmark = pytest.mark.gpu
+
+N = 2048
+DISP_MAX = 1e-3
+STRAIN_MAX = 1e-5
+CONF_BAND = 1e-3
+
+
+@pytest.fixture(scope="module")
+def pair():
+    p = synth.make_pattern(N, N, seed=7, rmin=1.5, rmax=2.5)
+    c = N / 2.0
+    field = synth.Field(A=((1.01, 0.003), (0.003, 0.996)), c=(c, c), amp=1.5, wavelength=256.0, s=(1.0, 1.0))
+    a = synth.degrade(synth.render(p, N, N, None), seed=1, noise=0.01, bits=8)
+    b = synth.degrade(synth.render(p, N, N, field), seed=2, noise=0.01, bits=8)
+    g = golden("config2")
+    roi = np.unpackbits(g["roi"])[:N * N].reshape(N, N).astype(bool)
+    # the benchmark's ROI is the reference's io.polygon_mask of the same polygon
+    np.testing.assert_array_equal(synth.rect_roi(N, N, 0.1 * N, 0.1 * N, 0.9 * N, 0.9 * N), roi)
+    return a, b, roi, field, g
+
+
+def _u8(img):
+    return np.round(img.astype(np.float64) * 255).astype(np.uint8)
+
+
+def test_config2_frames_are_the_reference_generators(pair):
+    a, b, _, _, g = pair
+    for img, k in ((a, "a"), (b, "b")):
+        q = _u8(img)
+        bad_rows = np.flatnonzero(q.sum(axis=1, dtype=np.int64) != g[f"rows_{k}"])
+        assert hashlib.sha256(q.tobytes()).hexdigest() == str(g[f"sha_{k}"]), f"frame {k}: rows differ {bad_rows[:10]}"
+
+
+def test_config2_poc_integer_peaks(pair, oracle):
+    a, b, _, _, g = pair
+    for lev in (0, 1):
+        got = testing.poc_peaks(a, b, Config(), level=lev)
+        np.testing.assert_array_equal(got, g[f"ipk_l{lev}"], err_msg=f"level {lev} vs the reference")
+    np.testing.assert_array_equal(oracle.coarse_peaks(a, b, Config(), level=0), g["ipk_l0"])
+    r = coarse_flow(a, b, Config())
+    np.testing.assert_array_equal(r.xs, g["xs"])
+    np.testing.assert_array_equal(r.ys, g["ys"])
+    for k in ("ux", "uy", "peak"):
+        assert np.abs(getattr(r, k) - g[k]).max() < DISP_MAX, k
+
+
+def test_config2_pair_against_the_oracle(pair, oracle):
+    from scipy.ndimage import binary_dilation, uniform_filter
+    a, b, roi, field, _ = pair
+    cfg = Config()
+    r = track_pair(a, b, cfg, mask=roi)
+    w = oracle.track_pair(a, b, cfg, mask=roi)
+    cmin = cfg.conf_min
+    rep = {}
+    conf_g, conf_w = r.conf.astype(np.float64), np.asarray(w["conf"], np.float64)
+    rep["conf_max"] = float(np.abs(conf_g - conf_w).max())
+    rep["conf_rms"] = float(np.sqrt(np.mean((conf_g - conf_w) ** 2)))
+    low_flip = (conf_g < cmin) != (conf_w < cmin)
+    rep["low_flips"] = int(low_flip.sum())
+    rep["flip_band"] = float(np.abs(conf_w[low_flip] - cmin).max()) if low_flip.any() else 0.0
+    valid_g, valid_w = np.isfinite(r.ux), np.isfinite(w["ux"])
+    vdiff = valid_g != valid_w
+    rep["valid_diffs"] = int(vdiff.sum())
+    zone = binary_dilation(low_flip, iterations=int(np.ceil(cfg.edge_guard_px())) + 1) if low_flip.any() else low_flip
+    rep["valid_diffs_outside_guard_zone"] = int((vdiff & ~zone).sum())
+    both = valid_g & valid_w
+    rep["valid_fraction"] = float(valid_w.mean())
+    for k in ("ux", "uy"):
+        d = getattr(r, k)[both].astype(np.float64) - w[k][both]
+        rep[f"{k}_max"] = float(np.abs(d).max())
+        rep[f"{k}_rms"] = float(np.sqrt(np.mean(d * d)))
+    # strain where the 15 x 15 window sees no validity difference
+    clean = uniform_filter(vdiff.astype(np.float64), size=cfg.strain_win, mode="constant") == 0
+    for k in ("Exx", "Eyy", "Exy", "gmax", "vol"):
+        m = clean & np.isfinite(r.strain[k]) & np.isfinite(w[k])
+        d = r.strain[k][m].astype(np.float64) - w[k][m]
+        rep[f"{k}_max"] = float(np.abs(d).max())
+        rep[f"{k}_rms"] = float(np.sqrt(np.mean(d * d)))
+    # error against the known field, on the pixels valid in both
+    tu, tv = field.displacement(N, N)
+    for name, ux, uy in (("engine", r.ux, r.uy), ("oracle", w["ux"], w["uy"])):
+        du, dv = ux[both] - tu[both], uy[both] - tv[both]
+        rep[f"truth_rms_{name}"] = float(np.sqrt(np.mean(du * du + dv * dv)))
+    print("CONFIG2 " + json.dumps(rep), flush=True)
+    assert rep["flip_band"] < CONF_BAND, rep
+    assert rep["valid_diffs_outside_guard_zone"] == 0, rep
+    assert rep["ux_max"] < DISP_MAX and rep["uy_max"] < DISP_MAX, rep
+    for k in ("Exx", "Eyy", "Exy", "gmax", "vol"):
+        assert rep[f"{k}_max"] < STRAIN_MAX, (k, rep)
+    np.testing.assert_array_equal(r.valid, valid_g)

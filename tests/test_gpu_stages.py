@@ -213,3 +213,17 @@ def test_prewarp_fill(T, oracle):
     ey = np.where(ok, uy, uy[iy, ix] + g[..., 1] * dx + g[..., 3] * dy)
     np.testing.assert_allclose(gx, ex, rtol=0, atol=1e-12)
     np.testing.assert_allclose(gy, ey, rtol=0, atol=1e-12)
+
+
+def test_render_matches_the_reference_generator(oracle):
+    """ofc_synth_render against the reference's own renders (tests/golden/synth.npz) and, at 384 x 320 with a
+    denser pattern, against the oracle's restatement: float64 images equal to 1e-12."""
+    from optflow_b200 import synth
+    from test_oracle import _synth_fields
+    g = golden("synth")
+    p = synth.make_pattern(64, 80, seed=3, rmin=1.5, rmax=2.5)
+    for name, f in _synth_fields().items():
+        assert np.abs(synth.render(p, 64, 80, f) - g[f"img_{name}"]).max() < 1e-12, name
+    p = synth.make_pattern(320, 384, seed=5, rmin=1.5, rmax=4.0)
+    for name, f in _synth_fields().items():
+        assert np.abs(synth.render(p, 320, 384, f) - oracle.render(p, 320, 384, f)).max() < 1e-12, name

@@ -261,3 +261,42 @@ def test_to_gray(oracle):
     blocks = np.array([[3 * y + x % 3 + 9 * (x // 3) for x in range(6)] for y in range(3)], np.float32)
     np.testing.assert_array_equal(oracle.to_gray(blocks, "f32", 3)[0], [[4.0, 13.0]])
     assert oracle.to_gray(np.ones((3, 5), np.float32), "f32", 2)[0].shape == (1, 2)
+
+
+# ---------------------------------------------------------------- synthetic speckle (the benchmark's inputs)
+def _synth_fields():
+    from optflow_b200 import synth
+    return {"none": None,
+            "strain": synth.uniform_strain(0.01, -0.004, (40.0, 32.0), exy=0.003, t=(1.3, -0.7)),
+            "sinaff": synth.Field(A=((1.01, 0.003), (0.003, 0.996)), c=(40.0, 32.0), t=(0.4, -0.25), amp=1.5,
+                                  wavelength=32.0, s=(1.0, 1.0))}
+
+
+def test_render_matches_the_reference_generator(oracle):
+    """The oracle's restatement of synth.render against the reference's own renders (tests/golden/synth.npz, by
+    make_golden_synth.py): the pattern draws exactly, the float64 images to 1e-12, the degraded 8-bit levels
+    exactly. The GPU renderer is pinned to this restatement in the GPU tests."""
+    from optflow_b200 import synth
+    g = golden("synth")
+    p = synth.make_pattern(64, 80, seed=3, rmin=1.5, rmax=2.5)
+    for k in ("cx", "cy", "r", "a"):
+        np.testing.assert_array_equal(getattr(p, k), g[k])
+    for i, (name, f) in enumerate(_synth_fields().items()):
+        img = oracle.render(p, 64, 80, f)
+        assert np.abs(img - g[f"img_{name}"]).max() < 1e-12, name
+        deg = synth.degrade(img, seed=10 + i, noise=0.01, bits=8)
+        np.testing.assert_array_equal(np.round(deg.astype(np.float64) * 255), np.round(g[f"deg_{name}"] * 255))
+
+
+def test_poc_integer_peaks_match_the_reference(oracle):
+    """The integer POC peaks of every grid point of every pyramid level (the window offset plus the argmax of the
+    last correlation surface) equal those of the reference's own coarse_flow on its POC fixtures
+    (tests/golden/poc_peaks.npz, read from its poc_shift by make_golden_config2.py)."""
+    g = golden("poc_peaks")
+    a, b = ref_fixture("poc_a").astype(np.float64), ref_fixture("poc_b").astype(np.float64)
+    sa, sb = ref_fixture("poc_strip_a").astype(np.float64), ref_fixture("poc_strip_b").astype(np.float64)
+    for name, (x, y, cfg) in {"grid": (a, b, Config()), "strip": (sa, sb, Config(max_disp=100))}.items():
+        levels = sorted(k for k in g if k.startswith(name + "_l"))
+        for lev, key in enumerate(levels):
+            np.testing.assert_array_equal(oracle.coarse_peaks(x, y, cfg, level=lev), g[key], err_msg=key)
+        assert oracle.coarse_peaks(x, y, cfg, level=len(levels)) is None

@@ -41,6 +41,22 @@ def test_noalloc_matches_the_allocating_entry_point_on_consecutive_calls():
             np.testing.assert_array_equal(got, want)
 
 
+def test_noalloc_tall_and_wide_images_at_the_size_limit():
+    """Images taller than a grid's 65,535-row y extent, and a single row, still give the exact mask."""
+    import oracle
+    import torch
+    from optflow_b200 import testing
+    lib = _abi.load()
+    stream = torch.cuda.Stream()
+    rng = np.random.default_rng(43)
+    for (h, w), p in [((65536, 16), 0.5), ((100000, 8), 0.6), ((1, 1 << 20), 0.7)]:
+        mask = rng.random((h, w)) < p
+        want = oracle.large_components(mask, 40.0)
+        np.testing.assert_array_equal(testing.large_components(mask, 40.0), want)
+        for _ in range(2):
+            np.testing.assert_array_equal(_noalloc(lib, mask, 40.0, stream), want)
+
+
 def test_noalloc_refuses_images_beyond_its_scratch():
     import torch
     lib = _abi.load()
