@@ -6,6 +6,7 @@
 // trusted pre-warp's "any low / not all trusted" cases) are decided on the device from counters that the
 // kernels read, so a whole pair can be captured and replayed as a CUDA graph.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -17,9 +18,12 @@
 #include <unordered_map>
 
 #include "fft.cuh"
+#include "synth_field.cuh"
 #include "kernels.cuh"
+#include "net.cuh"
 #include "../../include/optflow_cuda_testing.h"
 #include "../../include/optflow_cuda_synth.h"
+#include "../../include/optflow_cuda_net.h"
 
 namespace ofc {
 thread_local uint64_t* g_launch_counter = nullptr;
@@ -214,8 +218,23 @@ struct HostBuf {
   }
 };
 
+// the learned coarse proposal of an engine (ofc_set_coarse_net): the network's parameters on the device, the
+// per-tile fallback test, and its counters
+struct Proposal {
+  float* params = nullptr;  // float32 parameters (the biases are read from here)
+  uint16_t* w16 = nullptr;  // their bfloat16 copy, the tensor-core GEMMs' weights
+  int tile = 256;           // fallback tiles of tile x tile pixels
+  double max_low = 0.25;    // a tile fails when more than this share of its judged pixels has conf < conf_min
+  std::atomic<uint64_t> pairs{0}, tiles{0}, failed{0}, fallbacks{0};
+  ~Proposal() {
+    if (params) cudaFree(params);
+    if (w16) cudaFree(w16);
+  }
+};
+
 struct Lane {
   cudaStream_t stream = nullptr;
+  std::shared_ptr<Proposal> proposal;  // null: the POC coarse stage
   std::mutex busy;
   std::unordered_map<std::string, std::unique_ptr<DevBuf>> pool;
   std::map<int, std::pair<FftPlan, std::unique_ptr<DevBuf>>> plans;
@@ -299,8 +318,8 @@ struct Lane {
   // captured pair sequences, per (size, configuration, inputs present); events: the profile-mode event pairs
   // recorded inside the graph (kernel name, start, end)
   struct Graph {
-    cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
-    uint64_t launches[3] = {0, 0, 0};  // kernels per stage graph (the launch counter's share of a replay)
+    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint64_t launches[4] = {0, 0, 0, 0};  // kernels per stage graph (the launch counter's share of a replay)
     bool eager = false;                // the capture failed: this key runs eagerly
     std::vector<std::tuple<std::string, cudaEvent_t, cudaEvent_t>> events;
     ~Graph() {
@@ -830,6 +849,49 @@ void pair_stage(Lane& L, int stage, int W, int H, bool has_roi, bool has_init, c
                       conf64, low, nullptr, st);
     launch_f64_to_f32(u2, op + 8 * N, N, st);
     launch_f64_to_f32(u2 + N, op + 9 * N, N, st);
+  } else if (stage == 3) {
+    // the learned proposal in place of stage 0's POC: the network on the pair (padded to a multiple of 8 by edge
+    // replication), its 1/8-resolution flow interpolated to the dense start (kept in u2_learned for a fallback)
+    OFC_CUDA(cudaEventRecord(L.fork, st));
+    OFC_CUDA(cudaStreamWaitEvent(L.side, L.fork, 0));
+    fine_prep(L, i1, W, H, i2, W, H, c, L.side);
+    OFC_CUDA(cudaEventRecord(L.join, L.side));
+    const Proposal& P = *L.proposal;
+    const int W8 = (W + 7) / 8 * 8, H8 = (H + 7) / 8 * 8;
+    const float* a = i1;
+    const float* b = i2;
+    if (W8 != W || H8 != H) {
+      float* pa = L.get<float>("net_pad1", (size_t)W8 * H8);
+      float* pb = L.get<float>("net_pad2", (size_t)W8 * H8);
+      launch_pad8(i1, W, H, W8, H8, pa, st);
+      launch_pad8(i2, W, H, W8, H8, pb, st);
+      a = pa;
+      b = pb;
+    }
+    float* flow = L.get<float>("net_flow", (size_t)(W8 / 8) * (H8 / 8) * 2);
+    net::Workspace ws{[&L](const std::string& n, size_t bytes) { return (void*)L.get<uint8_t>(n, bytes); }, st};
+    net::forward(ws, P.params, P.w16, a, b, 1, H8, W8, flow);
+    launch_cells_to_dense(flow, W8 / 8, H8 / 8, W, H, u2, L.get<double>("u2_learned", 2 * N), st);
+    OFC_CUDA(cudaStreamWaitEvent(st, L.join, 0));
+  } else if (stage == 4) {
+    // the fallback's start: POC + dense start inside the failed tiles, the network's start elsewhere (the reference
+    // pack of i1 and the spline of i2 from stage 3 stay valid)
+    const Proposal& P = *L.proposal;
+    const int nt = ((W + P.tile - 1) / P.tile) * ((H + P.tile - 1) / P.tile);
+    CoarseOut g = coarse_dev(L, i1, i2, W, H, nullptr, c);
+    dense_start(L, g, W, H, nullptr, u2);
+    launch_blend_tiles(L.get<uint8_t>("tile_flags", nt), L.get<double>("u2_learned", 2 * N), W, H, P.tile, u2, st);
+  } else if (stage == 5) {
+    // the per-tile check of the refined result; the failed-tile count to page-locked memory for the host
+    const Proposal& P = *L.proposal;
+    const int nt = ((W + P.tile - 1) / P.tile) * ((H + P.tile - 1) / P.tile);
+    const uint8_t* roi = has_roi ? L.get<uint8_t>("in_roi", N) : nullptr;
+    int* nfail = L.get<int>("tile_nfail", 1);
+    // judged pixels: inside the ROI, beyond the border rule's band plus the network's reach (4 sigma_w + 40 px)
+    const int B = (int)std::ceil(4.0 * c.sigma_w) + 8 * net::CORR_R;
+    launch_tile_check(conf64, roi, W, H, P.tile, B, c.conf_min, P.max_low, L.get<uint8_t>("tile_flags", nt), nfail,
+                      st);
+    OFC_CUDA(cudaMemcpyAsync(L.pinned<int>("tile_nfail_h", 1), nfail, sizeof(int), cudaMemcpyDeviceToHost, st));
   } else {
     ofc_pair_out o{};
     float* p = L.get<float>("out_pair", 10 * N);
@@ -841,35 +903,32 @@ void pair_stage(Lane& L, int stage, int W, int H, bool has_roi, bool has_init, c
   }
 }
 
-// Runs the three stages on L.stream. The first call for a (size, configuration, inputs present, profile filter)
-// runs them eagerly, which allocates every buffer and uploads every constant, and then captures each stage as a
-// CUDA graph; later calls replay the graphs. timing: record the stage events L.ev[0..3] (the start of each stage
-// and the end), which pair_timing reads. nstages: 3 (the pair) or 2 (a sequence leg: coarse and fine, whose
-// conf, raw_ux and raw_uy planes of "out_pair" are its result).
-void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_config& c, bool timing, int nstages) {
+// Runs the stages `stages[0..n)` (pair_stage ids) on L.stream. The first call for a key (size, configuration, inputs
+// present, profile filter, stage list) runs them eagerly, which allocates every buffer and uploads every constant,
+// and then captures each stage as a CUDA graph; later calls replay the graphs. timing: record the stage events
+// L.ev[0..n) at the start of each stage and L.ev[3] at the end.
+void run_stage_list(Lane& L, const std::string& key, const int* stages, int n, int W, int H, bool has_roi,
+                    bool has_init, const ofc_config& c, bool timing) {
   cudaStream_t st = L.stream;
   Profiler* prof = g_profiler;
-  const std::string key = std::to_string(W) + "x" + std::to_string(H) + ":" + cfg_key(c) + ":" +
-                          (has_roi ? "r" : "-") + (has_init ? "i" : "-") + ":" + std::to_string(nstages) + ":" +
-                          (prof ? "P" + prof->filter : "");
   auto it = L.graphs.find(key);
   if (it == L.graphs.end() || it->second->eager) {
-    for (int sgi = 0; sgi < nstages; sgi++) {
+    for (int sgi = 0; sgi < n; sgi++) {
       if (timing) OFC_CUDA(cudaEventRecord(L.ev[sgi], st));
-      pair_stage(L, sgi, W, H, has_roi, has_init, c);
+      pair_stage(L, stages[sgi], W, H, has_roi, has_init, c);
     }
     if (timing) OFC_CUDA(cudaEventRecord(L.ev[3], st));
   }
   if (it == L.graphs.end()) {
     std::unique_ptr<Lane::Graph> g(new Lane::Graph());
     bool ok = true;
-    for (int sgi = 0; sgi < nstages && ok; sgi++) {
+    for (int sgi = 0; sgi < n && ok; sgi++) {
       cudaGraph_t graph = nullptr;
       const uint64_t before = g_launch_counter ? *g_launch_counter : 0;
       OFC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
       if (prof) prof->capture = &g->events;
       try {
-        pair_stage(L, sgi, W, H, has_roi, has_init, c);
+        pair_stage(L, stages[sgi], W, H, has_roi, has_init, c);
       } catch (...) {
         if (prof) prof->capture = nullptr;
         cudaStreamEndCapture(st, &graph);
@@ -897,7 +956,7 @@ void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_conf
     L.graphs[key] = std::move(g);
   } else if (!it->second->eager) {
     Lane::Graph& g = *it->second;
-    for (int sgi = 0; sgi < nstages; sgi++) {
+    for (int sgi = 0; sgi < n; sgi++) {
       if (timing) OFC_CUDA(cudaEventRecord(L.ev[sgi], st));
       OFC_CUDA(cudaGraphLaunch(g.exec[sgi], st));
       if (g_launch_counter) *g_launch_counter += g.launches[sgi];
@@ -916,6 +975,53 @@ void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_conf
       }
     }
   }
+}
+
+std::string pair_key(int W, int H, bool has_roi, bool has_init, const ofc_config& c, const std::string& tail) {
+  Profiler* prof = g_profiler;
+  return std::to_string(W) + "x" + std::to_string(H) + ":" + cfg_key(c) + ":" + (has_roi ? "r" : "-") +
+         (has_init ? "i" : "-") + ":" + tail + ":" + (prof ? "P" + prof->filter : "");
+}
+
+// A pair with the learned coarse proposal: the network's start (stage 3), the fine stage (1) and the per-tile check
+// (5); when a tile fails, the POC start inside the failed tiles (4) and the fine stage again (1); then the finish (2).
+// The host reads the failed-tile count between the two parts. Stage events as run_pair's: the coarse start, the
+// fine start, the finish start (after a fallback) and the end.
+void run_pair_learned(Lane& L, int W, int H, bool has_roi, const ofc_config& c, bool timing) {
+  Proposal& P = *L.proposal;
+  cudaStream_t st = L.stream;
+  const std::string tail = "learned" + std::to_string(P.tile) + "/" + std::to_string(P.max_low);
+  static const int first[3] = {3, 1, 5}, fallback[2] = {4, 1}, finish[1] = {2};
+  if (timing) OFC_CUDA(cudaEventRecord(L.ev[0], st));
+  run_stage_list(L, pair_key(W, H, has_roi, false, c, tail + "a"), first, 1, W, H, has_roi, false, c, false);
+  if (timing) OFC_CUDA(cudaEventRecord(L.ev[1], st));
+  run_stage_list(L, pair_key(W, H, has_roi, false, c, tail + "b"), first + 1, 2, W, H, has_roi, false, c, false);
+  OFC_CUDA(cudaStreamSynchronize(st));
+  const int nfail = *L.pinned<int>("tile_nfail_h", 1);
+  const int nt = ((W + P.tile - 1) / P.tile) * ((H + P.tile - 1) / P.tile);
+  P.pairs++;
+  P.tiles += nt;
+  P.failed += nfail;
+  if (nfail > 0) {
+    P.fallbacks++;
+    run_stage_list(L, pair_key(W, H, has_roi, false, c, tail + "f"), fallback, 2, W, H, has_roi, false, c, false);
+  }
+  if (timing) OFC_CUDA(cudaEventRecord(L.ev[2], st));
+  run_stage_list(L, pair_key(W, H, has_roi, false, c, tail + "e"), finish, 1, W, H, has_roi, false, c, false);
+  if (timing) OFC_CUDA(cudaEventRecord(L.ev[3], st));
+}
+
+// The pair's three stages (nstages 3), or a sequence leg's first two (nstages 2: coarse and fine, whose conf, raw_ux
+// and raw_uy planes of "out_pair" are its result). A lane with a learned proposal runs pairs without a start field
+// through run_pair_learned; sequence legs and pairs with a start keep the POC coarse stage.
+void run_pair(Lane& L, int W, int H, bool has_roi, bool has_init, const ofc_config& c, bool timing, int nstages) {
+  if (L.proposal && !has_init && nstages == 3) {
+    run_pair_learned(L, W, H, has_roi, c, timing);
+    return;
+  }
+  static const int stages[3] = {0, 1, 2};
+  run_stage_list(L, pair_key(W, H, has_roi, has_init, c, std::to_string(nstages)), stages, nstages, W, H, has_roi,
+                 has_init, c, timing);
 }
 
 // seconds per stage of the last run_pair that recorded its stage events (waits for its end)
@@ -1612,18 +1718,6 @@ void synth_render_dev(const SynthBlob* blobs, const int* cell_start, int ncx, in
 }
 
 namespace {
-// the field's forward map (synth.cu field_fwd), for the blobs' mapped centres
-void field_fwd_host(const ofc_field& f, double X, double Y, double& x, double& y) {
-  double dx = X - f.cx, dy = Y - f.cy;
-  x = f.cx + f.a00 * dx + f.a01 * dy + f.tx;
-  y = f.cy + f.a10 * dx + f.a11 * dy + f.ty;
-  if (f.amp != 0.0) {
-    double s = f.amp * std::sin(2 * PI * X / f.wavelength);
-    x = x + s * f.sx;
-    y = y + s * f.sy;
-  }
-}
-
 // per blob the reference's subsample rectangle (synth.py:174-179: floor/ceil of (mapped centre -+ (5.2 r + 2) + 0.5)
 // * ss, clipped to the image); blobs with an empty rectangle are dropped, the rest binned by the cell of the mapped
 // centre (cells 1 px wider than the largest half size, the grid starting one cell before the image) and rendered
@@ -1639,7 +1733,7 @@ void launch_synth_render(Lane& L, const double* bx, const double* by, const doub
   std::vector<int> cid;
   for (size_t k = 0; k < n; k++) {
     double px = bx[k], py = by[k];
-    if (field) field_fwd_host(*field, bx[k], by[k], px, py);
+    if (field) field_fwd(*field, bx[k], by[k], px, py);
     double rad = 5.2 * br[k] + 2.0;
     long j0 = std::max((long)std::floor((px - rad + 0.5) * ss), 0L);
     long j1 = std::min((long)std::ceil((px + rad + 0.5) * ss), W);
@@ -1661,7 +1755,15 @@ void launch_synth_render(Lane& L, const double* bx, const double* by, const doub
   int* dc = L.upload("syn_cells", cnt.data(), cnt.size());
   double* dout = L.get<double>("syn_out", (size_t)w * h);
   ofc_field* df = nullptr;
-  if (field) df = L.upload("syn_field", field, 1);
+  if (field) {
+    // the device copy of the field points at a device copy of its grid coefficients
+    ofc_field dev = *field;
+    if (field->grid && field->gnx > 0 && field->gny > 0)
+      dev.grid = L.upload("syn_grid", field->grid, (size_t)2 * field->gnx * field->gny);
+    else
+      dev.grid = nullptr;
+    df = L.upload("syn_field", &dev, 1);
+  }
   synth_render_dev(db, dc, ncx, ncy, cell, w, h, ss, df, dout, L.stream);
   OFC_CUDA(cudaMemcpyAsync(out, dout, (size_t)w * h * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
   OFC_CUDA(cudaStreamSynchronize(L.stream));
@@ -2089,6 +2191,7 @@ int ofc_track_pairs(ofc_engine* e, const ofc_pair_in* pairs, size_t n, const ofc
       lane_init(*a);
       L.aux.push_back(std::move(a));
     }
+    for (auto& a : L.aux) a->proposal = L.proposal;
     std::vector<long long> busy(K, -1);
     // a worker's finished pair: its planes from page-locked staging into the caller's buffers
     auto drain = [&](int j) {
@@ -3179,6 +3282,71 @@ int ofc_synth_render(ofc_engine* e, const double* bx, const double* by, const do
     if (ss < 1 || ss > 16) throw Error(OFC_ERR_ARG, "ss must lie in [1, 16]");
     launch_synth_render(L, bx, by, br, ba, n, (int)w, (int)h, ss, field, out);
   });
+}
+
+// ---------------------------------------------------------------- learned coarse proposal
+static void drop_graphs(Lane& l) {
+  for (auto& a : l.aux) drop_graphs(*a);
+  l.graphs.clear();
+}
+
+int ofc_set_coarse_net(ofc_engine* e, const float* params, size_t n, int tile, double max_low_share, char* err,
+                       size_t errlen) {
+  if (!e) {
+    set_err(err, errlen, "null engine");
+    return OFC_ERR_ARG;
+  }
+  // every lane: its graphs hold the old proposal's buffers
+  std::vector<std::unique_lock<std::mutex>> locks;
+  for (auto& l : e->lanes) {
+    std::unique_lock<std::mutex> t(l->busy, std::try_to_lock);
+    if (!t.owns_lock()) {
+      set_err(err, errlen, "the CUDA engine is busy: the proposal changes only between calls");
+      return OFC_ERR_BUSY;
+    }
+    locks.push_back(std::move(t));
+  }
+  try {
+    OFC_CUDA(cudaSetDevice(e->device));
+    std::shared_ptr<Proposal> P;
+    if (params) {
+      const size_t cnt = net::param_count();
+      if (n != cnt) throw Error(OFC_ERR_ARG, "the coarse network takes " + std::to_string(cnt) + " parameters");
+      if (tile < 32) throw Error(OFC_ERR_ARG, "fallback tiles must be at least 32 px");
+      if (!(max_low_share >= 0.0 && max_low_share <= 1.0)) throw Error(OFC_ERR_ARG, "max_low_share must lie in [0, 1]");
+      P = std::make_shared<Proposal>();
+      P->tile = tile;
+      P->max_low = max_low_share;
+      OFC_CUDA(cudaMalloc(&P->params, cnt * sizeof(float)));
+      OFC_CUDA(cudaMalloc(&P->w16, cnt * sizeof(uint16_t)));
+      OFC_CUDA(cudaMemcpy(P->params, params, cnt * sizeof(float), cudaMemcpyHostToDevice));
+      net::Workspace ws{[](const std::string&, size_t) -> void* { return nullptr; }, e->lanes[0]->stream};
+      net::to_bf16(ws, P->params, P->w16);
+      OFC_CUDA(cudaStreamSynchronize(e->lanes[0]->stream));
+    }
+    for (auto& l : e->lanes) {
+      lane_sync(*l);
+      drop_graphs(*l);
+      l->proposal = P;
+      for (auto& a : l->aux) a->proposal = P;
+    }
+    return OFC_OK;
+  } catch (const Error& x) {
+    set_err(err, errlen, x.what());
+    return x.status;
+  }
+}
+
+int ofc_coarse_net_stats(ofc_engine* e, uint64_t* out) {
+  if (!e || !out) return OFC_ERR_ARG;
+  out[0] = out[1] = out[2] = out[3] = 0;
+  const Proposal* P = e->lanes.empty() ? nullptr : e->lanes[0]->proposal.get();
+  if (!P) return OFC_OK;
+  out[0] = P->pairs;
+  out[1] = P->tiles;
+  out[2] = P->failed;
+  out[3] = P->fallbacks;
+  return OFC_OK;
 }
 
 }  // extern "C"

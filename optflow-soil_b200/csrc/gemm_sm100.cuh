@@ -1,0 +1,27 @@
+// gemm_sm100.cuh -- the tensor-core GEMMs of the learned coarse proposal (gemm_sm100.cu).
+#pragma once
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace ofc {
+
+enum class GemmKind { ForwardTN, WgradNT, DgradNN };
+
+// C[l] = A[l] * B[l] + beta C[l] for l < L; A is M x K, B is K x N, C is M x N row-major float. lda / ldb: the stride
+// of the operand's non-contiguous dimension (elements); batch_*: the stride between consecutive l.
+struct GemmArgs {
+  int M, N, K, L;
+  const void* A;  // bf16
+  int64_t lda, batch_a;
+  const void* B;  // bf16
+  int64_t ldb, batch_b;
+  float* C;
+  int64_t ldc, batch_c;
+  float beta;
+  const char* name;  // kernel name for the profile mode
+};
+
+void gemm_bf16(GemmKind kind, const GemmArgs& g, void* workspace, size_t workspace_bytes, cudaStream_t st);
+
+}  // namespace ofc

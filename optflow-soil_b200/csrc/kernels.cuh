@@ -139,4 +139,11 @@ void launch_pair_outputs(const double* mx, const double* my, const double* rux, 
                          const double* conf64, int n, float* ux, float* uy, float* conf, uint8_t* valid, float* raw_ux,
                          float* raw_uy, cudaStream_t st);
 
+// ---------------------------------------------------------------- learned coarse proposal (proposal.cu)
+void launch_pad8(const float* in, int W, int H, int W8, int H8, float* out, cudaStream_t st);
+void launch_cells_to_dense(const float* flow, int w8, int h8, int W, int H, double* u2, double* copy, cudaStream_t st);
+void launch_tile_check(const double* conf, const uint8_t* roi, int W, int H, int T, int B, double conf_min,
+                       double max_low, uint8_t* flags, int* nfail, cudaStream_t st);
+void launch_blend_tiles(const uint8_t* flags, const double* learned, int W, int H, int T, double* u2, cudaStream_t st);
+
 }  // namespace ofc

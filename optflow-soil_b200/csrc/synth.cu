@@ -1,44 +1,9 @@
 // synth.cu -- speckle rendering on the GPU (python/optflow_ref/synth.py:20-190 restated): Gaussian blobs
 // evaluated at the inverse-mapped coordinates of ss x ss subsamples per pixel, 0.5 + 0.25 tanh(mean), float64.
 #include "common.cuh"
-#include "../../include/optflow_cuda_synth.h"
+#include "synth_field.cuh"
 
 namespace ofc {
-
-// The field x = c + A (X - c) + t + amp sin(2 pi X_x / wavelength) (sx, sy), as synth.Affine (synth.py:33-51) plus a
-// sinusoid along X_x: forward, and the inverse by Newton steps from the affine inverse until the step is below 1e-13.
-__device__ void field_fwd(const ofc_field& f, double X, double Y, double& x, double& y) {
-  double dx = X - f.cx, dy = Y - f.cy;
-  x = f.cx + f.a00 * dx + f.a01 * dy + f.tx;
-  y = f.cy + f.a10 * dx + f.a11 * dy + f.ty;
-  if (f.amp != 0.0) {
-    double s = f.amp * sin(2 * PI * X / f.wavelength);
-    x = x + s * f.sx;
-    y = y + s * f.sy;
-  }
-}
-
-__device__ void field_inverse(const ofc_field& f, double x, double y, double& X, double& Y) {
-  double det = f.a00 * f.a11 - f.a01 * f.a10;
-  double b00 = f.a11 / det, b01 = -f.a01 / det, b10 = -f.a10 / det, b11 = f.a00 / det;
-  double dx = x - f.cx - f.tx, dy = y - f.cy - f.ty;
-  X = f.cx + b00 * dx + b01 * dy;
-  Y = f.cy + b10 * dx + b11 * dy;
-  if (f.amp == 0.0) return;
-  for (int it = 0; it < 30; it++) {
-    double fx, fy;
-    field_fwd(f, X, Y, fx, fy);
-    fx -= x;
-    fy -= y;
-    double ds = f.amp * (2 * PI / f.wavelength) * cos(2 * PI * X / f.wavelength);
-    double j00 = f.a00 + ds * f.sx, j01 = f.a01, j10 = f.a10 + ds * f.sy, j11 = f.a11;
-    double d = j00 * j11 - j01 * j10;
-    double sx = (j11 * fx - j01 * fy) / d, sy = (-j10 * fx + j00 * fy) / d;
-    X -= sx;
-    Y -= sy;
-    if (fabs(sx) + fabs(sy) < 1e-13) break;
-  }
-}
 
 // synth.render (synth.py:150-190) as a gather: blob k adds a_k exp(-d^2 / (2 r_k^2)) to exactly the subsamples
 // [i0, i1) x [j0, j1) that the reference's per-blob rectangle covers (half size 5.2 r_k + 2 around the mapped

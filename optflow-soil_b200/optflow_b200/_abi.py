@@ -235,10 +235,18 @@ TEST_SIGNATURES = {
 }
 
 
+class OfcBand(ctypes.Structure):
+    """struct ofc_band (include/optflow_cuda_synth.h)."""
+    _fields_ = [(n, ctypes.c_double) for n in ("ex", "ey", "tx", "ty", "delta", "width", "length", "bias")]
+
+
 class OfcField(ctypes.Structure):
     """struct ofc_field (include/optflow_cuda_synth.h)."""
-    _fields_ = [(n, ctypes.c_double) for n in ("a00", "a01", "a10", "a11", "cx", "cy", "tx", "ty", "amp",
-                                                "wavelength", "sx", "sy")]
+    _fields_ = ([(n, ctypes.c_double) for n in ("a00", "a01", "a10", "a11", "cx", "cy", "tx", "ty", "amp",
+                                                 "wavelength", "sx", "sy")]
+                + [("grid", c_double_p), ("gnx", ctypes.c_int), ("gny", ctypes.c_int)]
+                + [(n, ctypes.c_double) for n in ("gx0", "gy0", "gh", "fs", "fdecay", "fx0", "fx1", "fy")]
+                + [("n_bands", ctypes.c_int), ("bands", OfcBand * 4)])
 
 
 # include/optflow_cuda_synth.h
@@ -261,6 +269,22 @@ class EngineError(RuntimeError):
 _LIB = None
 
 
+# include/optflow_cuda_net.h
+NET_SIGNATURES = {
+    "ofc_net_param_count": (ctypes.c_size_t, []),
+    "ofc_net_create": (_P, [ctypes.c_int, _E, _S]),
+    "ofc_net_destroy": (None, [_P]),
+    "ofc_net_set_params": (ctypes.c_int, [_P, c_float_p, _S, _E, _S]),
+    "ofc_net_get_params": (ctypes.c_int, [_P, c_float_p, _S, _E, _S]),
+    "ofc_net_forward": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _E, _S]),
+    "ofc_net_gradients": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P,
+                                         c_double_p, _P, _E, _S]),
+    "ofc_net_adam": (ctypes.c_int, [_P, _P, ctypes.c_float, _P, _E, _S]),
+    "ofc_set_coarse_net": (ctypes.c_int, [_P, c_float_p, _S, ctypes.c_int, ctypes.c_double, _E, _S]),
+    "ofc_coarse_net_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64)]),
+}
+
+
 def load(path=None):
     """Load the engine library once and bind every declared symbol. Raises if it is missing."""
     global _LIB
@@ -271,7 +295,7 @@ def load(path=None):
         raise EngineError(2, f"CUDA engine library not built: {p} (run __graft_entry__.build() or "
                              f"python optflow-soil_b200/build.py)")
     lib = ctypes.CDLL(p)
-    for name, (res, args) in {**SIGNATURES, **TEST_SIGNATURES, **SYNTH_SIGNATURES}.items():
+    for name, (res, args) in {**SIGNATURES, **TEST_SIGNATURES, **SYNTH_SIGNATURES, **NET_SIGNATURES}.items():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args

@@ -69,6 +69,26 @@ class Engine:
     def lanes(self):
         return self.lib.ofc_lanes(self.handle)
 
+    def set_coarse_net(self, params=None, tile=256, max_low_share=0.25):
+        """Pair calls without a start field start from the learned coarse proposal (include/optflow_cuda_net.h):
+        params = the network's float32 parameters ("default": the trained set shipped with the package); None: back
+        to the POC coarse stage. Tiles of tile x tile px whose refined result has more than max_low_share
+        low-confidence pixels fall back to POC."""
+        if isinstance(params, str) and params == "default":
+            from .net import load_weights
+            params = load_weights()
+        if params is None:
+            self._call("ofc_set_coarse_net", None, 0, int(tile), ctypes.c_double(max_low_share))
+            return
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._call("ofc_set_coarse_net", p.ctypes.data_as(c_float_p), p.size, int(tile), ctypes.c_double(max_low_share))
+
+    def coarse_net_stats(self):
+        """Counters of the learned proposal: pairs, tiles judged, tiles failed, pairs that fell back to POC."""
+        out = (ctypes.c_uint64 * 4)()
+        self.lib.ofc_coarse_net_stats(self.handle, out)
+        return dict(pairs=out[0], tiles=out[1], failed_tiles=out[2], fallback_pairs=out[3])
+
     def kernel_launches(self):
         return int(self.lib.ofc_kernel_launches(self.handle))
 

@@ -1244,7 +1244,44 @@ void finish(const ImgD& ux, const ImgD& uy, const ImgD& conf, const ImgB* mask, 
 }
 
 // ------------------------------------------------------------------ synthetic speckle (synth.py:20-190)
-// The field x = c + A (X - c) + t + amp sin(2 pi X_x / wavelength) (sx, sy) of include/optflow_cuda_synth.h.
+// The field of include/optflow_cuda_synth.h: x = c + A (X - c) + t + amp sin(2 pi X_x / wavelength) (sx, sy), plus the
+// optional grid (cubic B-spline of coefficients), footing settlement and shear-band displacements of X.
+void field_extra_u(const ofc_field& f, double X, double Y, double& ux, double& uy) {
+  ux = uy = 0.0;
+  if (f.grid && f.gnx > 0 && f.gny > 0) {
+    auto basis = [](double t, double* w) {  // uniform cubic B-spline weights of taps i-1..i+2
+      w[0] = (1 - t) * (1 - t) * (1 - t) / 6;
+      w[1] = (3 * t * t * t - 6 * t * t + 4) / 6;
+      w[2] = (-3 * t * t * t + 3 * t * t + 3 * t + 1) / 6;
+      w[3] = t * t * t / 6;
+    };
+    double gx = (X - f.gx0) / f.gh, gy = (Y - f.gy0) / f.gh, wx[4], wy[4];
+    long ix = (long)std::floor(gx), iy = (long)std::floor(gy);
+    basis(gx - ix, wx);
+    basis(gy - iy, wy);
+    for (int a = 0; a < 4; a++)
+      for (int b = 0; b < 4; b++) {
+        long r = std::min(std::max(iy - 1 + a, 0L), (long)f.gny - 1), c = std::min(std::max(ix - 1 + b, 0L), (long)f.gnx - 1);
+        ux += wy[a] * wx[b] * f.grid[r * f.gnx + c];
+        uy += wy[a] * wx[b] * f.grid[(size_t)f.gnx * f.gny + r * f.gnx + c];
+      }
+  }
+  if (f.fs != 0.0) {
+    double px = std::min(std::max(X, f.fx0), f.fx1);
+    uy += f.fs * std::exp(-std::hypot(X - px, Y - f.fy) / f.fdecay);
+  }
+  for (int k = 0; k < f.n_bands; k++) {
+    const ofc_band& b = f.bands[k];
+    double s = -b.ty * (X - b.ex) + b.tx * (Y - b.ey), a = b.tx * (X - b.ex) + b.ty * (Y - b.ey);
+    double tp = b.length > 0 ? 0.25 * (1 + std::tanh(a / b.width)) * (1 + std::tanh((b.length - a) / b.width)) : 1.0;
+    double v = 0.5 * b.delta * (std::tanh(s / b.width) + b.bias) * tp;
+    ux += v * b.tx;
+    uy += v * b.ty;
+  }
+}
+
+bool field_has_extra(const ofc_field& f) { return f.grid || f.fs != 0.0 || f.n_bands > 0; }
+
 void field_fwd(const ofc_field& f, double X, double Y, double& x, double& y) {  // synth.py:42-46
   double dx = X - f.cx, dy = Y - f.cy;
   x = f.cx + f.a00 * dx + f.a01 * dy + f.tx;
@@ -1254,23 +1291,47 @@ void field_fwd(const ofc_field& f, double X, double Y, double& x, double& y) {  
     x = x + s * f.sx;
     y = y + s * f.sy;
   }
+  if (field_has_extra(f)) {
+    double ux, uy;
+    field_extra_u(f, X, Y, ux, uy);
+    x += ux;
+    y += uy;
+  }
 }
 
-// the affine inverse (synth.py:48-51), then Newton steps on the sinusoid until the step is below 1e-13
+// the affine inverse (synth.py:48-51), then Newton steps until the step is below 1e-13: the sinusoid's Jacobian in
+// closed form, the optional terms' by central differences (step 1e-5 px)
 void field_inv(const ofc_field& f, double x, double y, double& X, double& Y) {
   double det = f.a00 * f.a11 - f.a01 * f.a10;
   double b00 = f.a11 / det, b01 = -f.a01 / det, b10 = -f.a10 / det, b11 = f.a00 / det;
   double dx = x - f.cx - f.tx, dy = y - f.cy - f.ty;
   X = f.cx + b00 * dx + b01 * dy;
   Y = f.cy + b10 * dx + b11 * dy;
-  if (f.amp == 0.0) return;
+  const bool extra = field_has_extra(f);
+  if (f.amp == 0.0 && !extra) return;
   for (int it = 0; it < 30; it++) {
     double fx, fy;
     field_fwd(f, X, Y, fx, fy);
     fx -= x;
     fy -= y;
-    double ds = f.amp * (2 * PI / f.wavelength) * std::cos(2 * PI * X / f.wavelength);
-    double j00 = f.a00 + ds * f.sx, j01 = f.a01, j10 = f.a10 + ds * f.sy, j11 = f.a11;
+    double j00 = f.a00, j01 = f.a01, j10 = f.a10, j11 = f.a11;
+    if (f.amp != 0.0) {
+      double ds = f.amp * (2 * PI / f.wavelength) * std::cos(2 * PI * X / f.wavelength);
+      j00 += ds * f.sx;
+      j10 += ds * f.sy;
+    }
+    if (extra) {
+      const double e = 1e-5;
+      double ax, ay, bx, by, cx, cy, ex, ey;
+      field_extra_u(f, X + e, Y, ax, ay);
+      field_extra_u(f, X - e, Y, bx, by);
+      field_extra_u(f, X, Y + e, cx, cy);
+      field_extra_u(f, X, Y - e, ex, ey);
+      j00 += (ax - bx) / (2 * e);
+      j10 += (ay - by) / (2 * e);
+      j01 += (cx - ex) / (2 * e);
+      j11 += (cy - ey) / (2 * e);
+    }
     double d = j00 * j11 - j01 * j10;
     double sx = (j11 * fx - j01 * fy) / d, sy = (-j10 * fx + j00 * fy) / d;
     X -= sx;

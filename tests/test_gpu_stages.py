@@ -227,3 +227,18 @@ def test_render_matches_the_reference_generator(oracle):
     p = synth.make_pattern(320, 384, seed=5, rmin=1.5, rmax=4.0)
     for name, f in _synth_fields().items():
         assert np.abs(synth.render(p, 320, 384, f) - oracle.render(p, 320, 384, f)).max() < 1e-12, name
+
+
+def test_render_with_grid_footing_and_bands(oracle):
+    """The optional displacement terms of the renderer (a Gaussian-process grid, a footing settlement, finite shear
+    bands) against the oracle's restatement, whose Newton inverse takes those terms' Jacobian by central differences:
+    the two inverse maps meet at the same root, so the images agree to 1e-9."""
+    from optflow_b200 import synth
+    rng = np.random.default_rng(9)
+    h, w = 288, 352
+    grid, gx0, gy0 = synth.gp_grid(h, w, 96.0, 14.0, rng)
+    f = synth.Field(grid=grid, gx0=gx0, gy0=gy0, footing=(3.0, 150.0, 140.0, 220.0, 40.0),
+                    bands=[synth.Band((140.0, 40.0), (-0.7071067811865476, 0.7071067811865476), 6.0, 8.0, 180.0, 1.0),
+                           synth.Band((220.0, 40.0), (0.7071067811865476, 0.7071067811865476), 6.0, 8.0, 180.0, 1.0)])
+    p = synth.make_pattern(h, w, seed=4, rmin=1.5, rmax=2.5)
+    assert np.abs(synth.render(p, h, w, f) - oracle.render(p, h, w, f)).max() < 1e-9
