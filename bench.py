@@ -176,6 +176,56 @@ def run_cpu(a, b, roi, steps, warmup):
                       f"threads, {sec / steps:.2f} s per window"}
 
 
+def learned_leg(eng, d_a, d_b, roi, field, n, steps, flush, stream):
+    """The pair through the learned coarse proposal (device time per pair, CUDA events, L2 flushed between steps)
+    next to the POC path on the same pair: pixel-pairs/s of each, the RMS error of each path's valid pixels against
+    the known field, and the proposal's fallback counters."""
+    import torch
+    from optflow_b200 import Config, Engine, _abi
+    dev = d_a.device
+    en = Engine(dev.index or 0)
+    en.set_coarse_net("default")
+    c = Config().to_ofc()
+    d_roi = torch.from_numpy(roi.astype(np.uint8)).to(dev)
+    tu, tv = field.displacement(n, n)
+    res = {}
+    for name, e in (("poc", eng), ("learned", en)):
+        outs = {k: torch.empty((n, n), dtype=torch.uint8 if k == "valid" else torch.float32, device=dev)
+                for k in _abi.PAIR_FIELDS}
+        po = _abi.OfcPairOut()
+        for k, t in outs.items():
+            setattr(po, k, ctypes.cast(t.data_ptr(), _abi.c_u8_p if k == "valid" else _abi.c_float_p))
+        err = ctypes.create_string_buffer(1024)
+
+        def step():
+            st = e.lib.ofc_track_pair_device(e.handle, d_a.data_ptr(), d_b.data_ptr(), n, n, d_roi.data_ptr(), None,
+                                             None, ctypes.byref(c), ctypes.byref(po),
+                                             ctypes.c_void_p(stream.cuda_stream), err, 1024)
+            if st != 0:
+                raise RuntimeError(err.value.decode())
+
+        for _ in range(2):
+            step()
+        ms = []
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms.append(e0.elapsed_time(e1))
+        m = outs["valid"].cpu().numpy().astype(bool)
+        du = outs["ux"].cpu().numpy()[m] - tu[m]
+        dv = outs["uy"].cpu().numpy()[m] - tv[m]
+        res[name] = {"value": n * n / (float(np.mean(ms)) / 1e3), "unit": UNIT, "ms_per_step": float(np.mean(ms)),
+                     "truth_rms_px": float(np.sqrt(np.mean(du * du + dv * dv))), "valid_fraction": float(m.mean())}
+    res["learned"]["fallback"] = en.coarse_net_stats()
+    en.close()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -185,6 +235,7 @@ def main():
     ap.add_argument("--size", type=int, default=N_PIX)
     ap.add_argument("--profile-all", action="store_true", help="print every kernel's device time to stderr")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-proposal leg")
     args = ap.parse_args()
     assert args.warmup >= 0 and args.steps >= 1
 
@@ -217,7 +268,7 @@ def main():
     eng = Engine(local)
     lib = eng.lib
     n = args.size
-    a, b, roi, _ = make_pair(n, engine=eng)
+    a, b, roi, field = make_pair(n, engine=eng)
     cfg = Config()
     c = cfg.to_ofc()
 
@@ -331,6 +382,13 @@ def main():
         e2e_sec = float(tt.item())
     valid_frac = float(hout["valid"].numpy().mean())
 
+    # the same pair with the learned coarse proposal in place of POC (a second engine with the shipped weights):
+    # device time per pair and the error of both paths against the known field
+    learned = None
+    if not args.no_learned and os.path.exists(os.path.join(ROOT, "optflow-soil_b200", "optflow_b200", "weights",
+                                                           "coarse_net.npz")):
+        learned = learned_leg(eng, d_a, d_b, roi, field, n, args.steps, flush, stream)
+
     line = None
     if rank == 0:
         peak, peak_kind = hbm_peak()
@@ -355,7 +413,8 @@ def main():
                 "config": dict(workload_config(n), parallelism=f"replicas x{world}"), "valid_fraction": valid_frac,
                 "e2e": {"value": world * n * n / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_sec * 1e3},
-                "gpu_launches": int(launches), "clocks": clk, "roofline": roof, "cpu_baseline": base}
+                "gpu_launches": int(launches), "clocks": clk, "roofline": roof, "cpu_baseline": base,
+                "learned_vs_poc": learned}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -16,6 +16,9 @@ ofc_profile_read) in a separate run, since the profile mode waits for every repl
   pairs   24 pairs of sides drawn from {256, ..., 2048} (seed 11): one track_pairs call against one track_pair call each
   pipeline  23 rgb24 1920 x 1080 frames, scale 2, step 5, tavg 3, hybrid: the window means inside the streamed driver
           against iter_frames feeding it
+  learned[:n]  n (500) held-out 2048^2 pairs of the learned proposal's distribution: POC + refine against the learned
+          proposal + refine (device time, error against the known field, fallback counters)
+  footing[:n]  the footing-in-sand clip (n = 600 frames of 1920 x 1080) through the streamed hybrid driver
 """
 import ctypes
 import json
@@ -233,14 +236,142 @@ def pipeline(eng):
             "wall_ms_per_result_iter_frames": round(1e3 * t_host / max(len(b), 1), 2), "identical": bool(same)}
 
 
-WORKLOADS = {"frames": frames, "tavg": tavg, "hybrid": hybrid, "stream": stream, "pairs": pairs, "pipeline": pipeline}
+def _device_pair_ms(eng, d_a, d_b, n_w, n_h, reps=3, d_roi=None):
+    """Device time (CUDA events, median of reps after one untimed run) of one pair through ofc_track_pair_device on
+    device-resident inputs, and its outputs (host arrays)."""
+    import torch
+    from . import _abi
+    dev = d_a.device
+    outs = {k: torch.empty((n_h, n_w), dtype=torch.uint8 if k == "valid" else torch.float32, device=dev)
+            for k in _abi.PAIR_FIELDS}
+    po = _abi.OfcPairOut()
+    for k, t in outs.items():
+        setattr(po, k, ctypes.cast(t.data_ptr(), _abi.c_u8_p if k == "valid" else _abi.c_float_p))
+    c = Config().to_ofc()
+    stream = torch.cuda.Stream(dev)
+    err = ctypes.create_string_buffer(1024)
+
+    def run():
+        st = eng.lib.ofc_track_pair_device(eng.handle, d_a.data_ptr(), d_b.data_ptr(), n_w, n_h,
+                                           None if d_roi is None else d_roi.data_ptr(), None, None, ctypes.byref(c),
+                                           ctypes.byref(po), ctypes.c_void_p(stream.cuda_stream), err, 1024)
+        if st != 0:
+            raise RuntimeError(err.value.decode())
+
+    run()
+    ms = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    return float(np.median(ms)), {k: v.cpu().numpy() for k, v in outs.items()}
+
+
+def learned(eng, n_pairs=500, size=2048, seed=23):
+    """Held-out pairs of the learned proposal's distribution (a Gaussian-process field of length scale 64-512 px
+    plus a shear band; optflow_b200.net.random_field) at size^2: plain POC + refine (this engine) against the learned
+    proposal + refine (a second engine on the same GPU with the shipped weights), device time per pair (CUDA events,
+    inputs resident), RMS error of the valid pixels against the known field, and the proposal's fallback counters."""
+    import torch
+    from . import net
+    from .api import Engine
+    rng = np.random.default_rng(seed + 1000003)  # held out: the training set draws from default_rng(seed)
+    dev = torch.device("cuda", getattr(eng, "device", 0))
+    eng_net = Engine(getattr(eng, "device", 0))
+    eng_net.set_coarse_net("default")
+    t_poc, t_net, e_poc, e_net, v_poc, v_net = [], [], [], [], [], []
+    reps = 3
+    for _ in range(n_pairs):
+        a, b, field = net.training_pair(rng, size, size, engine=eng)
+        tu, tv = field.displacement(size, size)
+        d_a, d_b = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+        ms0, o0 = _device_pair_ms(eng, d_a, d_b, size, size, reps)
+        ms1, o1 = _device_pair_ms(eng_net, d_a, d_b, size, size, reps)
+        t_poc.append(ms0)
+        t_net.append(ms1)
+        for o, e, v in ((o0, e_poc, v_poc), (o1, e_net, v_net)):
+            m = o["valid"].astype(bool)
+            du, dv = o["ux"][m] - tu[m], o["uy"][m] - tv[m]
+            e.append(float(np.sqrt(np.mean(du * du + dv * dv))) if m.any() else float("nan"))
+            v.append(float(m.mean()))
+    st = eng_net.coarse_net_stats()
+    runs = reps + 1  # every pair runs once untimed and reps times timed, with the same outcome
+    fb = {k: int(v) // runs for k, v in st.items()}
+    px = size * size
+    e_poc, e_net = np.array(e_poc), np.array(e_net)
+    return {"workload": f"learned: {n_pairs} held-out {size}^2 pairs (GP field 64-512 px + shear band, seed {seed})",
+            "poc_ms_per_pair": round(float(np.mean(t_poc)), 3), "learned_ms_per_pair": round(float(np.mean(t_net)), 3),
+            "poc_pixel_pairs_s": px / (np.mean(t_poc) / 1e3), "learned_pixel_pairs_s": px / (np.mean(t_net) / 1e3),
+            "poc_rms_px": round(float(np.nanmean(e_poc)), 5), "learned_rms_px": round(float(np.nanmean(e_net)), 5),
+            "poc_rms_px_median": round(float(np.nanmedian(e_poc)), 5),
+            "learned_rms_px_median": round(float(np.nanmedian(e_net)), 5),
+            "pairs_within_0.02px": {"poc": int(np.sum(e_poc <= 0.02)), "learned": int(np.sum(e_net <= 0.02))},
+            "valid_fraction": {"poc": round(float(np.mean(v_poc)), 4), "learned": round(float(np.mean(v_net)), 4)},
+            "fallback": fb}
+
+
+def footing(eng, n_frames=600):
+    """The footing-in-sand clip (synth.footing_field): 1920 x 1080 uint8 frames (speckle seed 31, noise 0.008),
+    rendered on a second engine as the stream pulls them, tracked with the CLI's recommended video settings (scale 2,
+    step 5, seq_mode hybrid, tavg 3, prewarp_freeze_at 3) over the sand below the surface; wall time per result, the
+    RMS error of the valid pixels against the known field (on the downscaled grid), and the share of ROI pixels carried
+    by the adjacent leg."""
+    from .api import Engine
+    h, w, sc, step, tavg, surface = 1080, 1920, 2, 5, 3, 300.0
+    rend = Engine(getattr(eng, "device", 0))
+    p = synth.make_pattern(h, w, seed=31, rmin=1.5, rmax=2.5)
+
+    def frames():
+        for k in range(n_frames):
+            img = synth.degrade(synth.render(p, h, w, synth.footing_field(k, w, h, surface, frames=n_frames),
+                                             engine=rend), seed=1000 + k, noise=0.008, bits=8)
+            yield np.round(img * 255).astype(np.uint8)
+
+    hs, ws = h // sc, w // sc
+    roi = np.zeros((hs, ws), bool)
+    roi[int(np.ceil(surface / sc)) + 2:, :] = True
+    cfg = Config(seq_mode="hybrid", prewarp_freeze_at=3)
+    errs, fbs, valid, ks = [], [], [], []
+    # the downscaled grid's pixel centres in full-resolution coordinates (box downscale of sc x sc blocks)
+    yy, xx = np.mgrid[0:hs, 0:ws].astype(np.float64)
+    X, Y = sc * xx + (sc - 1) / 2.0, sc * yy + (sc - 1) / 2.0
+    t = time.perf_counter()
+    for k, r in track_stream(frames(), cfg, mask=roi, scale=sc, step=step, tavg=tavg, engine=eng):
+        raw = k * step
+        tu, tv = synth.footing_field(raw, w, h, surface, frames=n_frames).displacement_at(X, Y)
+        m = np.isfinite(r.ux)
+        du, dv = r.ux[m] - tu[m] / sc, r.uy[m] - tv[m] / sc
+        errs.append(float(np.sqrt(np.mean(du * du + dv * dv))) if m.any() else float("nan"))
+        valid.append(float(m[roi].mean()))
+        fbs.append(float((r.fb[roi] > 0).mean()) if r.fb is not None else 0.0)
+        ks.append(raw)
+    wall = time.perf_counter() - t
+    n = len(errs)
+    return {"workload": f"footing: {n_frames} 1920x1080 uint8 frames, scale 2, step 5, hybrid, tavg 3, "
+                        f"prewarp_freeze_at 3, sand ROI ({n} results)",
+            "results": n, "wall_ms_per_result_incl_rendering": round(1e3 * wall / max(n, 1), 2),
+            "rms_px_downscaled": {"mean": round(float(np.nanmean(errs)), 4), "max": round(float(np.nanmax(errs)), 4),
+                                  "last": round(errs[-1], 4)},
+            "valid_share_of_roi": {"mean": round(float(np.mean(valid)), 4), "min": round(float(np.min(valid)), 4)},
+            "adjacent_leg_share": {"mean": round(float(np.mean(fbs)), 4), "max": round(float(np.max(fbs)), 4)},
+            "settlement_px_last": round(0.05 * ks[-1], 2)}
+
+
+WORKLOADS = {"frames": frames, "tavg": tavg, "hybrid": hybrid, "stream": stream, "pairs": pairs, "pipeline": pipeline,
+             "learned": learned, "footing": footing}
 
 
 def main(argv=None):
-    names = (argv if argv is not None else sys.argv[1:]) or list(WORKLOADS)
+    """Workload names, optionally with a count (learned:64 runs 64 held-out pairs, footing:100 the first 100
+    frames); no name: every workload but learned and footing."""
+    names = (argv if argv is not None else sys.argv[1:]) or [k for k in WORKLOADS if k not in ("learned", "footing")]
     eng = default_engine()
     for n in names:
-        print(json.dumps(WORKLOADS[n](eng)), flush=True)
+        name, _, cnt = n.partition(":")
+        print(json.dumps(WORKLOADS[name](eng, int(cnt)) if cnt else WORKLOADS[name](eng)), flush=True)
 
 
 if __name__ == "__main__":

@@ -100,6 +100,18 @@ def test_config2_pair_against_the_oracle(pair, oracle):
         d = r.strain[k][m].astype(np.float64) - w[k][m]
         rep[f"{k}_max"] = float(np.abs(d).max())
         rep[f"{k}_rms"] = float(np.sqrt(np.mean(d * d)))
+    # where the largest field differences sit: distance to the nearest invalid pixel and the oracle's confidence
+    from scipy.ndimage import distance_transform_edt
+    dist = distance_transform_edt(valid_w)
+    dux = np.where(both, np.abs(r.ux.astype(np.float64) - w["ux"]), 0.0)
+    rep["ux_diff_over_1e-4"] = int((dux > 1e-4).sum())
+    top = np.argsort(dux.ravel())[-5:][::-1]
+    rep["ux_top"] = [[int(i // N), int(i % N), float(dux.ravel()[i]), float(conf_w.ravel()[i]),
+                      float(dist.ravel()[i])] for i in top]
+    for k in ("Exx", "Eyy", "Exy", "gmax", "vol"):
+        m = clean & np.isfinite(r.strain[k]) & np.isfinite(w[k])
+        d = np.abs(r.strain[k][m].astype(np.float64) - w[k][m])
+        rep[f"{k}_over_1e-5"] = int((d > 1e-5).sum())
     # error against the known field, on the pixels valid in both
     tu, tv = field.displacement(N, N)
     for name, ux, uy in (("engine", r.ux, r.uy), ("oracle", w["ux"], w["uy"])):
