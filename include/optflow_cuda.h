@@ -419,6 +419,19 @@ OFC_API int ofc_large_components_noalloc(const uint8_t* d_mask, size_t w, size_t
  * are all hand-written; no library kernel runs on the path). */
 OFC_API uint64_t ofc_kernel_launches(const ofc_engine* eng);
 
+/* FFT plan autotuner (no counterpart in the reference, whose Metal engine orders a length's factors by a fixed rule,
+ * rust/crates/optflow-gpu/src/fft.rs:190 factorise). A padded length's runtime plan can take one of
+ * ofc_fft_plan_variants() factor orders; the transform is the same, its speed and float32 rounding differ.
+ * ofc_fft_tune times every order of each length on `lines` lines on the engine's device (CUDA events, median of
+ * five) and returns the fastest order per length (best) and the times (ms: n x variants, INFINITY where an order
+ * does not exist). ofc_fft_set_plans installs a plan table for the process: plans that engines build afterwards take
+ * the table's order (a plan already built keeps its own), so results are reproducible for a given table. 2112 (the
+ * padded length of 2048-wide images) runs on a compile-time plan and is not tuned. */
+OFC_API int ofc_fft_plan_variants(void);
+OFC_API int ofc_fft_tune(ofc_engine* eng, const int32_t* lengths, size_t n, int lines, int32_t* best, float* ms,
+                         char* err, size_t errlen);
+OFC_API int ofc_fft_set_plans(const int32_t* lengths, const int32_t* variants, size_t n);
+
 #ifdef __cplusplus
 }
 #endif

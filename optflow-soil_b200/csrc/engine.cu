@@ -3349,4 +3349,79 @@ int ofc_coarse_net_stats(ofc_engine* e, uint64_t* out) {
   return OFC_OK;
 }
 
+// ---------------------------------------------------------------- FFT plan table (autotuner)
+int ofc_fft_tune(ofc_engine* e, const int32_t* lengths, size_t n, int lines, int32_t* best, float* ms, char* err,
+                 size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& Ln) {
+    if (!lengths || !best || lines < 1) throw Error(OFC_ERR_ARG, "null argument or no lines");
+    cudaEvent_t e0, e1;
+    OFC_CUDA(cudaEventCreate(&e0));
+    OFC_CUDA(cudaEventCreate(&e1));
+    for (size_t i = 0; i < n; i++) {
+      const int L = lengths[i];
+      best[i] = 0;
+      float bt = INFINITY;
+      for (int v = 0; v < FFT_PLAN_VARIANTS; v++) {
+        float t = INFINITY;
+        const int work = fft_work_length(L);
+        if (work > 0 && !(L == FFT_FIXED_L && work == L)) {
+          FftPlan pl;
+          bool ok = true;
+          try {
+            pl = fft_make_plan(L, v);
+          } catch (const Error&) {
+            ok = false;
+          }
+          if (ok) {
+            std::vector<float2> tw = fft_twiddles(fft_work_len(pl));
+            const size_t ntw = tw.size();
+            if (pl.M) {
+              std::vector<float2> bt2 = fft_bluestein_tables(L, pl.M);
+              tw.insert(tw.end(), bt2.begin(), bt2.end());
+            }
+            float2* dtw = Ln.upload("tune_tw", tw.data(), tw.size());
+            pl.tw = dtw;
+            if (pl.M) {
+              pl.chirp = pl.tw + ntw;
+              pl.filt = pl.chirp + L;
+            }
+            float2* d = Ln.get<float2>("tune_lines", (size_t)lines * L);
+            OFC_CUDA(cudaMemsetAsync(d, 0, (size_t)lines * L * sizeof(float2), Ln.stream));
+            launch_fft_lines(d, lines, pl, false, Ln.stream);
+            std::vector<float> rep;
+            for (int r = 0; r < 5; r++) {
+              OFC_CUDA(cudaEventRecord(e0, Ln.stream));
+              launch_fft_lines(d, lines, pl, false, Ln.stream);
+              OFC_CUDA(cudaEventRecord(e1, Ln.stream));
+              OFC_CUDA(cudaEventSynchronize(e1));
+              float m = 0;
+              OFC_CUDA(cudaEventElapsedTime(&m, e0, e1));
+              rep.push_back(m);
+            }
+            std::sort(rep.begin(), rep.end());
+            t = rep[rep.size() / 2];
+          }
+        }
+        if (ms) ms[i * FFT_PLAN_VARIANTS + v] = t;
+        if (t < bt) {
+          bt = t;
+          best[i] = v;
+        }
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  });
+}
+
+int ofc_fft_set_plans(const int32_t* lengths, const int32_t* variants, size_t n) {
+  if (n && (!lengths || !variants)) return OFC_ERR_ARG;
+  for (size_t i = 0; i < n; i++)
+    if (variants[i] < 0 || variants[i] >= FFT_PLAN_VARIANTS) return OFC_ERR_ARG;
+  for (size_t i = 0; i < n; i++) fft_set_plan_variant(lengths[i], variants[i]);
+  return OFC_OK;
+}
+
+int ofc_fft_plan_variants(void) { return FFT_PLAN_VARIANTS; }
+
 }  // extern "C"

@@ -16,7 +16,10 @@
 // transforms along the other, and the result is bspline_coeffs(ifft2(F2 * G)) of phaseflow.py:456 up to rounding.
 #include "fft.cuh"
 
+#include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <type_traits>
 
 #include <cuda_pipeline.h>
@@ -97,20 +100,64 @@ std::vector<float2> fft_bluestein_tables(int L, int M) {
   return out;
 }
 
-FftPlan fft_make_plan(int L) {
+namespace {
+std::mutex g_plan_mu;
+std::map<int, int> g_plan_table;  // padded length -> factor order (fft_set_plan_variant)
+}  // namespace
+
+void fft_set_plan_variant(int L, int variant) {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  if (variant <= 0) g_plan_table.erase(L);
+  else g_plan_table[L] = variant;
+}
+
+int fft_plan_variant(int L) {
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  auto it = g_plan_table.find(L);
+  return it == g_plan_table.end() ? 0 : it->second;
+}
+
+// The factor orders a plan of length n can take (the transform is the same; the stages, their strides and the
+// rounding differ): 0 radix 8 first, then 4, 2 and the odd radices ascending; 1 the odd radices first; 2 the power of
+// two in radix-4 stages (a radix 2 last when the power is odd); 3 the order of 0 reversed.
+static std::vector<int> factor_order(int n, int variant) {
+  std::vector<int> two, odd;
+  int m = n, e = 0;
+  while (m % 2 == 0) { m /= 2; e++; }
+  for (int p : {3, 5, 7, 11, 13, 17, 19, 23, 29, 31})
+    while (m % p == 0) { odd.push_back(p); m /= p; }
+  if (m != 1) return {};
+  if (variant == 2) {
+    for (; e >= 2; e -= 2) two.push_back(4);
+    if (e) two.push_back(2);
+  } else {
+    for (; e >= 3; e -= 3) two.push_back(8);
+    if (e == 2) two.push_back(4);
+    if (e == 1) two.push_back(2);
+  }
+  std::vector<int> f;
+  if (variant == 1) {
+    f = odd;
+    f.insert(f.end(), two.begin(), two.end());
+  } else {
+    f = two;
+    f.insert(f.end(), odd.begin(), odd.end());
+  }
+  if (variant == 3) std::reverse(f.begin(), f.end());
+  return f;
+}
+
+FftPlan fft_make_plan(int L) { return fft_make_plan(L, fft_plan_variant(L)); }
+
+FftPlan fft_make_plan(int L, int variant) {
   const int work = fft_work_length(L);
   if (work == 0) throw Error(OFC_ERR_WINDOW, "no FFT plan for length " + std::to_string(L));
+  if (variant < 0 || variant >= FFT_PLAN_VARIANTS) throw Error(OFC_ERR_ARG, "no FFT plan variant " + std::to_string(variant));
   FftPlan pl;
   pl.L = L;
   pl.M = work == L ? 0 : work;
-  int m = work;
-  std::vector<int> f;
-  while (m % 8 == 0) { f.push_back(8); m /= 8; }
-  while (m % 4 == 0) { f.push_back(4); m /= 4; }
-  while (m % 2 == 0) { f.push_back(2); m /= 2; }
-  for (int p : {3, 5, 7, 11, 13, 17, 19, 23, 29, 31})
-    while (m % p == 0) { f.push_back(p); m /= p; }
-  if ((int)f.size() > FFT_MAXST || m != 1)
+  std::vector<int> f = factor_order(work, variant);
+  if (f.empty() || (int)f.size() > FFT_MAXST)
     throw Error(OFC_ERR_WINDOW, "FFT length " + std::to_string(L) + " needs too many stages");
   int s = 1;
   pl.nst = (int)f.size();
@@ -684,7 +731,6 @@ __device__ __forceinline__ int reflect_near(int i, int n) {
 // prefilter's carries live in the buffer the transform left idle. The kernels are instantiated for FIXL = 0 (any
 // supported length, the plan read at run time) and FIXL = FFT_FIXED_L (2112 = 8 8 3 11, the padded length of
 // 2048-wide images, the plan fixed at compile time); the launchers pick by the plan's length.
-constexpr int FFT_FIXED_L = 2112;
 
 // buffer stride of the kernels that stage several lines: fft_buf_len rounded up to an even count (16-byte aligned)
 __host__ __device__ constexpr int fft_buf_stride(int L, int C) { return (fft_buf_len(L, C) + 1) & ~1; }

@@ -6,6 +6,8 @@
 namespace ofc {
 
 constexpr int FFT_MAXST = 16;
+// the padded length of 2048-wide images, whose transforms run on a plan fixed at compile time
+constexpr int FFT_FIXED_L = 2112;
 constexpr int FFT_E = 8;       // complex values per thread (sets the threads of a block)
 constexpr int FFT_TMAX = 512;  // threads per block at most
 
@@ -39,6 +41,13 @@ bool fft_fits(int ph, int pw);
 // host: factor L (or Bluestein's M) and fill p/s; the caller sets tw (fft_twiddles(fft_work_length(L))) and, for
 // Bluestein, chirp and filt (fft_bluestein_tables: L chirp values, then M filter values)
 FftPlan fft_make_plan(int L);
+// the plan with a given factor order (0 .. FFT_PLAN_VARIANTS - 1); fft_make_plan(L) takes the plan table's choice
+constexpr int FFT_PLAN_VARIANTS = 4;
+FftPlan fft_make_plan(int L, int variant);
+// the process-wide plan table: the factor order of the runtime plans of length L (0: the default order); plans an
+// engine has already built keep theirs
+void fft_set_plan_variant(int L, int variant);
+int fft_plan_variant(int L);
 std::vector<float2> fft_twiddles(int L);
 std::vector<float2> fft_bluestein_tables(int L, int M);
 // threads of a block that transforms C interleaved lines of length L (multiple of C and of 32)

@@ -284,6 +284,13 @@ NET_SIGNATURES = {
     "ofc_coarse_net_stats": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64)]),
 }
 
+# include/optflow_cuda.h: the FFT plan table
+PLAN_SIGNATURES = {
+    "ofc_fft_plan_variants": (ctypes.c_int, []),
+    "ofc_fft_tune": (ctypes.c_int, [_P, c_i32_p, _S, ctypes.c_int, c_i32_p, c_float_p, _E, _S]),
+    "ofc_fft_set_plans": (ctypes.c_int, [c_i32_p, c_i32_p, _S]),
+}
+
 
 def load(path=None):
     """Load the engine library once and bind every declared symbol. Raises if it is missing."""
@@ -295,7 +302,8 @@ def load(path=None):
         raise EngineError(2, f"CUDA engine library not built: {p} (run __graft_entry__.build() or "
                              f"python optflow-soil_b200/build.py)")
     lib = ctypes.CDLL(p)
-    for name, (res, args) in {**SIGNATURES, **TEST_SIGNATURES, **SYNTH_SIGNATURES, **NET_SIGNATURES}.items():
+    for name, (res, args) in {**SIGNATURES, **TEST_SIGNATURES, **SYNTH_SIGNATURES, **NET_SIGNATURES,
+                                **PLAN_SIGNATURES}.items():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args

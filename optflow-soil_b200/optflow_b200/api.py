@@ -37,6 +37,8 @@ class Engine:
 
     def __init__(self, device=0, lanes=1):
         self.lib = _abi.load()
+        from .fftplan import install
+        install()
         err = ctypes.create_string_buffer(_ERRLEN)
         h = self.lib.ofc_create(int(device), int(lanes), err, _ERRLEN)
         if not h:

@@ -31,7 +31,8 @@ def lib():
 def test_every_declared_symbol_is_exported(lib):
     names = declared_symbols()
     assert len(names) >= 20
-    bound = set(_abi.SIGNATURES) | set(_abi.TEST_SIGNATURES) | set(_abi.SYNTH_SIGNATURES) | set(_abi.NET_SIGNATURES)
+    bound = (set(_abi.SIGNATURES) | set(_abi.TEST_SIGNATURES) | set(_abi.SYNTH_SIGNATURES) | set(_abi.NET_SIGNATURES)
+             | set(_abi.PLAN_SIGNATURES))
     assert set(names) == bound, set(names) ^ bound
     for n in names:
         assert getattr(lib, n) is not None

@@ -242,3 +242,28 @@ def test_render_with_grid_footing_and_bands(oracle):
                            synth.Band((220.0, 40.0), (0.7071067811865476, 0.7071067811865476), 6.0, 8.0, 180.0, 1.0)])
     p = synth.make_pattern(h, w, seed=4, rmin=1.5, rmax=2.5)
     assert np.abs(synth.render(p, h, w, f) - oracle.render(p, h, w, f)).max() < 1e-9
+
+
+def test_fft_plan_orders_agree_and_tune():
+    """Every factor order of a runtime plan computes the same transform (against numpy, as the default order), and
+    the tuner returns an existing order per length."""
+    from optflow_b200 import _abi, fftplan, testing
+    lib = _abi.load()
+    rng = np.random.default_rng(3)
+    lengths = [320, 604, 1088]
+    res = fftplan.tune(lengths, lines=256)
+    for L in lengths:
+        b, times = res[L]
+        assert 0 <= b < lib.ofc_fft_plan_variants() and np.isfinite(times[b])
+    x = (rng.normal(size=(8, 1088)) + 1j * rng.normal(size=(8, 1088))).astype(np.complex64)
+    want = np.fft.fft(x.astype(np.complex128), axis=1)
+    for v in range(lib.ofc_fft_plan_variants()):
+        from optflow_b200 import Engine
+        L = np.array([1088], np.int32)
+        var = np.array([v], np.int32)
+        lib.ofc_fft_set_plans(L.ctypes.data_as(_abi.c_i32_p), var.ctypes.data_as(_abi.c_i32_p), 1)
+        got = testing.fft_lines(x, engine=Engine(0))  # a fresh engine builds its plan from the table
+        assert np.abs(got - want).max() < 1e-5 * np.abs(want).max(), v
+    zero = np.array([0], np.int32)
+    lib.ofc_fft_set_plans(L.ctypes.data_as(_abi.c_i32_p), zero.ctypes.data_as(_abi.c_i32_p), 1)
+    fftplan.install(force=True)  # the shipped table again
