@@ -19,6 +19,7 @@ ofc_profile_read) in a separate run, since the profile mode waits for every repl
   learned[:n]  n (500) held-out 2048^2 pairs of the learned proposal's distribution: POC + refine against the learned
           proposal + refine (device time, error against the known field, fallback counters)
   footing[:n]  the footing-in-sand clip (n = 600 frames of 1920 x 1080) through the streamed hybrid driver
+  batch64  the 64 uneven pairs of batch.batch_specs (seed 11): track_pairs against one track_pair call each
 """
 import ctypes
 import json
@@ -360,8 +361,33 @@ def footing(eng, n_frames=600):
             "settlement_px_last": round(0.05 * ks[-1], 2)}
 
 
+def batch64(eng, n=64):
+    """The uneven batch of independent pairs (batch.batch_specs: 64 pairs from seed 11, sides drawn from
+    {256, ..., 2048}, random affine strain |e| <= 0.02, translation <= 6 px, noise 0.003-0.02): one track_pairs call
+    (worker lanes with their own streams and graphs, the FFT plan table installed) against one track_pair call each,
+    wall time with the pairs on the host; every result equal between the two."""
+    from .batch import batch_specs, make_pair
+    specs = batch_specs(n, 11)
+    items = [make_pair(s, engine=eng)[:2] for s in specs]
+    px = sum(s.pixels for s in specs)
+    cfg = Config()
+    r_batch = track_pairs(items, cfg, engine=eng)  # warm-up: buffers, plans and graphs
+    r_one = [track_pair(x, y, cfg, engine=eng) for x, y in items]
+    t = time.perf_counter()
+    [track_pair(x, y, cfg, engine=eng) for x, y in items]
+    t1 = time.perf_counter() - t
+    t = time.perf_counter()
+    r_batch = track_pairs(items, cfg, engine=eng)
+    t2 = time.perf_counter() - t
+    same = all(np.array_equal(a.ux, b.ux, equal_nan=True) for a, b in zip(r_batch, r_one))
+    return {"workload": f"batch64: {n} pairs of uneven sides from {{256..2048}} (seed 11)",
+            "megapixels": round(px / 1e6, 2), "one_call_each_s": round(t1, 3),
+            "one_call_each_pixel_pairs_s": px / t1, "track_pairs_s": round(t2, 3), "track_pairs_pixel_pairs_s": px / t2,
+            "identical": bool(same)}
+
+
 WORKLOADS = {"frames": frames, "tavg": tavg, "hybrid": hybrid, "stream": stream, "pairs": pairs, "pipeline": pipeline,
-             "learned": learned, "footing": footing}
+             "learned": learned, "footing": footing, "batch64": batch64}
 
 
 def main(argv=None):

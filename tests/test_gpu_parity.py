@@ -85,6 +85,12 @@ def compare_pair(r, want, label, conf_band=0.02):
     assert both.sum() > 0.5 * valid_w.sum()
     assert rms(r.ux, want["ux"], both) < DISP_TOL, label
     assert rms(r.uy, want["uy"], both) < DISP_TOL, label
+    dmax = {k: float(np.abs(np.asarray(getattr(r, k), np.float64)[both] - want[k][both]).max()) for k in ("ux", "uy")}
+    smax = {}
+    for k in ("Exx", "Eyy", "Exy", "gmax", "vol"):
+        m = both & np.isfinite(r.strain[k]) & np.isfinite(want[k])
+        smax[k] = float(np.abs(np.asarray(r.strain[k], np.float64)[m] - want[k][m]).max()) if m.any() else 0.0
+    print(f"PAIRMAX {label} flips {int(diff.sum())} field_max {dmax} strain_max {smax}", flush=True)
     assert rms(r.conf, want["conf"]) < DISP_TOL, label
     # the unmasked field (the init of a sequence's next frame; not a CLI output) on the confident pixels
     trusted = np.asarray(want["conf"]) >= cmin
