@@ -219,13 +219,52 @@ def train(frames, targets, masks, steps, batch=16, lr=1e-3, seed=0, params=None,
     return net.get_params(), losses
 
 
+def time_net(size, batch, reps):
+    """Device time (CUDA events, median) of the forward pass on one size x size pair, and of one training step
+    (forward, backward, Adam) on `batch` pairs of 256^2; prints one JSON line."""
+    import json
+    import torch
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(5)
+    net = CoarseNet(0, init_params(1))
+    a, b, _ = training_pair(rng, size, size)
+    d_a, d_b = torch.from_numpy(a)[None].to(dev), torch.from_numpy(b)[None].to(dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        fn()
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    fwd = timed(lambda: net.forward(d_a, d_b, stream=stream))
+    fr = [training_pair(rng, 256, 256) for _ in range(batch)]
+    i1 = torch.from_numpy(np.stack([f[0] for f in fr])).to(dev)
+    i2 = torch.from_numpy(np.stack([f[1] for f in fr])).to(dev)
+    tg = torch.zeros((batch, 32, 32, 2), dtype=torch.float32, device=dev)
+    mk = torch.ones((batch, 32, 32), dtype=torch.uint8, device=dev)
+
+    def step():
+        net.gradients(i1, i2, tg, mk, stream=stream)
+        net.adam(1e-4, stream=stream)
+
+    trn = timed(step)
+    print(json.dumps({"forward_ms": fwd, "size": size, "train_step_ms": trn, "batch": batch, "train_size": 256}))
+
+
 def main(argv=None):
     """python -m optflow_b200.net train [--pairs N] [--size S] [--steps K] [--batch B] [--seed S] [--out PATH]:
     renders the training set on the GPU, trains on it with the network's kernels and writes the parameters."""
     import argparse
     import time
     ap = argparse.ArgumentParser(prog="python -m optflow_b200.net")
-    ap.add_argument("cmd", choices=["train"])
+    ap.add_argument("cmd", choices=["train", "time"])
     ap.add_argument("--pairs", type=int, default=20000)
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--steps", type=int, default=6000)
@@ -234,7 +273,11 @@ def main(argv=None):
     ap.add_argument("--plain-share", type=float, default=0.1)
     ap.add_argument("--seed", type=int, default=23)
     ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--reps", type=int, default=20)
     a = ap.parse_args(argv)
+    if a.cmd == "time":
+        time_net(a.size, a.batch, a.reps)
+        return
     from .api import Engine
     log = lambda m: print(f"[{time.strftime('%H:%M:%S')}] {m}", flush=True)
     eng = Engine(0)
