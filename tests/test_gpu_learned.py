@@ -2,7 +2,8 @@
 
 * Where the proposal starts the fine stage inside its capture range, the refined field equals the plain POC path's
   (the refinement is the same; only its start differs): on held-out pairs of the training distribution the learned
-  path's error against the known field stays within 2e-3 px (RMS) of the POC path's, and within 0.02 px.
+  path's error against the known field (RMS) stays within 2e-3 px of the POC path's, and its valid share within 2 %.
+  Both errors are the refinement's own (about 0.03-0.05 px on these fields, whose strains reach 15 %).
 * What the network gains over the method without it (its speed is measured by bench.py and optflow_b200.measure):
   it keeps working where the displacement leaves POC's capture range (a 28 px translation with max_disp = 8, where
   POC's single 64 px window cannot reach): there the learned path's error is far smaller.
@@ -41,7 +42,7 @@ def test_learned_path_matches_the_plain_path_on_held_out_pairs(engines):
         a, b, field = net.training_pair(rng, n, n, engine=plain)
         e0, v0 = _rms(track_pair(a, b, Config(), engine=plain), field, n)
         e1, v1 = _rms(track_pair(a, b, Config(), engine=learned), field, n)
-        assert e1 < 0.02 and e1 < e0 + 2e-3, (e0, e1)
+        assert abs(e1 - e0) < 2e-3 and e1 < 0.1, (e0, e1)
         assert v1 > v0 - 0.02, (v0, v1)
 
 
