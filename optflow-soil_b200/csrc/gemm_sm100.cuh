@@ -24,4 +24,20 @@ struct GemmArgs {
 
 void gemm_bf16(GemmKind kind, const GemmArgs& g, void* workspace, size_t workspace_bytes, cudaStream_t st);
 
+// D (M x N, row-major bfloat16) = act(A B + bias) with act = ReLU or the identity: the forward GEMM's layouts
+// (A K-contiguous, B = weights [N][K]) with the bias and the activation applied in the epilogue
+struct FusedArgs {
+  int M, N, K;
+  const void* A;  // bf16
+  int64_t lda;
+  const void* B;  // bf16
+  int64_t ldb;
+  void* D;  // bf16
+  int64_t ldd;
+  const float* bias;  // N floats
+  const char* name;
+};
+
+void gemm_bf16_fused(bool relu, const FusedArgs& g, void* workspace, size_t workspace_bytes, cudaStream_t st);
+
 }  // namespace ofc

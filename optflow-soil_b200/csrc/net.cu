@@ -401,18 +401,21 @@ void run(const Workspace& ws, const float* params, const uint16_t* w16, const fl
     col[l] = get<uint16_t>(ws, "net_col" + std::to_string(l), g.Mpad * kp);
     OFC_LAUNCH(k_im2col, grid_for(g.Mpad * kp / 8), 256, 0, st, in, g.Hi, g.Wi, S.cin, g.Ho, g.Wo, S.stride, S.dil, kp,
                g.M, g.Mpad, col[l]);
-    float* y32 = get<float>(ws, "net_y" + std::to_string(l), g.Mpad * S.cout);
-    GemmArgs a{(int)g.M, S.cout, kp, 1, col[l], kp, 0, w16 + param_offset(l), kp, 0, y32, S.cout, 0, 0.f,
-               "k_gemm_sm100_fprop"};
-    gemm_bf16(GemmKind::ForwardTN, a, gws, GEMM_WS, st);
     const float* bias = params + param_offset(l) + (size_t)S.cout * kp;
     if (l == NCONV - 1) {
+      // the last layer's float32 output: the flow's residual channels
+      float* y32 = get<float>(ws, "net_y" + std::to_string(l), g.Mpad * S.cout);
+      GemmArgs a{(int)g.M, S.cout, kp, 1, col[l], kp, 0, w16 + param_offset(l), kp, 0, y32, S.cout, 0, 0.f,
+                 "k_gemm_sm100_fprop"};
+      gemm_bf16(GemmKind::ForwardTN, a, gws, GEMM_WS, st);
       y4 = get<float>(ws, "net_y4", g.M * S.cout);
       OFC_LAUNCH(k_bias_act, grid_for(g.M * S.cout), 256, 0, st, y32, bias, S.cout, g.M, 0, (uint16_t*)nullptr, y4);
     } else {
+      // bias, ReLU and the bfloat16 store in the GEMM's epilogue
       act[l] = get<uint16_t>(ws, "net_act" + std::to_string(l), g.M * S.cout);
-      OFC_LAUNCH(k_bias_act, grid_for(g.M * S.cout), 256, 0, st, y32, bias, S.cout, g.M, S.relu, act[l],
-                 (float*)nullptr);
+      FusedArgs a{(int)g.M, S.cout, kp, col[l], kp, w16 + param_offset(l), kp, act[l], S.cout, bias,
+                  "k_gemm_sm100_fprop_fused"};
+      gemm_bf16_fused(S.relu != 0, a, gws, GEMM_WS, st);
     }
     if (l == 3) {
       const size_t np = (size_t)nb * h8 * w8;
