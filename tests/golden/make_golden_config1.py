@@ -4,8 +4,8 @@ synth.make_pattern(256, 256, seed=1), frame k under a uniform strain exx = 0.005
 translation (0.8 k, 0) px, rendered and degraded with Gaussian noise 0.005 (seed k) to 8 bits; default
 configuration, no ROI.
 
-Stored per frame: ux, uy and conf in full; Exx, Eyy, Exy, gmax and vol on every second row and column (the strain
-fields are smooth; the subsample keeps the fixture small); the reference index and mean confidence.
+Stored per frame: ux, uy, conf, Exx, Eyy, Exy, gmax and vol in full (float32); the reference index and mean
+confidence.
 
 Run in a checkout that has the reference: ``python tests/golden/make_golden_config1.py [/path/to/reference]``
 (or the OPTFLOW_REFERENCE environment variable).
@@ -39,7 +39,7 @@ def main():
     for k, r in track.track_sequence(grey, Config()):
         out[f"f{k}_ux"], out[f"f{k}_uy"], out[f"f{k}_conf"] = (np.float32(getattr(r, q)) for q in ("ux", "uy", "conf"))
         for q in ("Exx", "Eyy", "Exy", "gmax", "vol"):
-            out[f"f{k}_{q}"] = np.float32(r.strain[q][::2, ::2])
+            out[f"f{k}_{q}"] = np.float32(r.strain[q])
         out[f"f{k}_meta"] = np.array([r.timing["reference"], r.timing["mean_conf"]])
         print(k, f"{time.time() - t:.1f} s", flush=True)
     np.savez_compressed(os.path.join(HERE, "config1.npz"), **out)

@@ -90,7 +90,10 @@ def compare_pair(r, want, label, conf_band=0.02):
     for k in ("Exx", "Eyy", "Exy", "gmax", "vol"):
         m = both & np.isfinite(r.strain[k]) & np.isfinite(want[k])
         smax[k] = float(np.abs(np.asarray(r.strain[k], np.float64)[m] - want[k][m]).max()) if m.any() else 0.0
-    print(f"PAIRMAX {label} flips {int(diff.sum())} field_max {dmax} strain_max {smax}", flush=True)
+    low_flip = (np.asarray(r.conf, np.float64) < cmin) != (np.asarray(want["conf"], np.float64) < cmin)
+    band = float(np.abs(np.asarray(want["conf"], np.float64)[low_flip] - cmin).max()) if low_flip.any() else 0.0
+    print(f"PAIRMAX {label} validity diffs {int(diff.sum())} low flips {int(low_flip.sum())} band {band:.2e} "
+          f"field_max {dmax} strain_max {smax}", flush=True)
     assert rms(r.conf, want["conf"]) < DISP_TOL, label
     # the unmasked field (the init of a sequence's next frame; not a CLI output) on the confident pixels
     trusted = np.asarray(want["conf"]) >= cmin
