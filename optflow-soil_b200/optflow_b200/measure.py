@@ -316,7 +316,7 @@ def learned(eng, n_pairs=500, size=2048, seed=23):
 
 def footing(eng, n_frames=600):
     """The footing-in-sand clip (synth.footing_field): 1920 x 1080 uint8 frames (speckle seed 31, noise 0.008),
-    rendered on a second engine as the stream pulls them, tracked with the CLI's recommended video settings (scale 2,
+    rendered first on a second engine (timed apart), then tracked from host memory with the CLI's recommended video settings (scale 2,
     step 5, seq_mode hybrid, tavg 3, prewarp_freeze_at 3) over the sand below the surface; wall time per result, the
     RMS error of the valid pixels against the known field (on the downscaled grid), and the share of ROI pixels carried
     by the adjacent leg."""
@@ -325,11 +325,11 @@ def footing(eng, n_frames=600):
     rend = Engine(getattr(eng, "device", 0))
     p = synth.make_pattern(h, w, seed=31, rmin=1.5, rmax=2.5)
 
-    def frames():
-        for k in range(n_frames):
-            img = synth.degrade(synth.render(p, h, w, synth.footing_field(k, w, h, surface, frames=n_frames),
-                                             engine=rend), seed=1000 + k, noise=0.008, bits=8)
-            yield np.round(img * 255).astype(np.uint8)
+    t = time.perf_counter()
+    clip = [np.round(synth.degrade(synth.render(p, h, w, synth.footing_field(k, w, h, surface, frames=n_frames),
+                                                engine=rend), seed=1000 + k, noise=0.008, bits=8) * 255).astype(np.uint8)
+            for k in range(n_frames)]
+    t_render = time.perf_counter() - t
 
     hs, ws = h // sc, w // sc
     roi = np.zeros((hs, ws), bool)
@@ -340,20 +340,23 @@ def footing(eng, n_frames=600):
     yy, xx = np.mgrid[0:hs, 0:ws].astype(np.float64)
     X, Y = sc * xx + (sc - 1) / 2.0, sc * yy + (sc - 1) / 2.0
     t = time.perf_counter()
-    for k, r in track_stream(frames(), cfg, mask=roi, scale=sc, step=step, tavg=tavg, engine=eng):
+    got = [(k, r.ux, r.uy, r.fb) for k, r in track_stream(clip, cfg, mask=roi, scale=sc, step=step, tavg=tavg,
+                                                           engine=eng)]
+    wall = time.perf_counter() - t
+    for k, ux, uy, fb in got:
         raw = k * step
         tu, tv = synth.footing_field(raw, w, h, surface, frames=n_frames).displacement_at(X, Y)
-        m = np.isfinite(r.ux)
-        du, dv = r.ux[m] - tu[m] / sc, r.uy[m] - tv[m] / sc
+        m = np.isfinite(ux)
+        du, dv = ux[m] - tu[m] / sc, uy[m] - tv[m] / sc
         errs.append(float(np.sqrt(np.mean(du * du + dv * dv))) if m.any() else float("nan"))
         valid.append(float(m[roi].mean()))
-        fbs.append(float((r.fb[roi] > 0).mean()) if r.fb is not None else 0.0)
+        fbs.append(float((fb[roi] > 0).mean()) if fb is not None else 0.0)
         ks.append(raw)
-    wall = time.perf_counter() - t
     n = len(errs)
     return {"workload": f"footing: {n_frames} 1920x1080 uint8 frames, scale 2, step 5, hybrid, tavg 3, "
                         f"prewarp_freeze_at 3, sand ROI ({n} results)",
-            "results": n, "wall_ms_per_result_incl_rendering": round(1e3 * wall / max(n, 1), 2),
+            "results": n, "wall_ms_per_result": round(1e3 * wall / max(n, 1), 2),
+            "render_s_all_frames": round(t_render, 1),
             "rms_px_downscaled": {"mean": round(float(np.nanmean(errs)), 4), "max": round(float(np.nanmax(errs)), 4),
                                   "last": round(errs[-1], 4)},
             "valid_share_of_roi": {"mean": round(float(np.mean(valid)), 4), "min": round(float(np.min(valid)), 4)},

@@ -42,7 +42,7 @@ def test_learned_path_matches_the_plain_path_on_held_out_pairs(engines):
         a, b, field = net.training_pair(rng, n, n, engine=plain)
         e0, v0 = _rms(track_pair(a, b, Config(), engine=plain), field, n)
         e1, v1 = _rms(track_pair(a, b, Config(), engine=learned), field, n)
-        assert abs(e1 - e0) < 2e-3 and e1 < 0.1, (e0, e1)
+        assert abs(e1 - e0) < 2e-3 and e1 < 0.2, (e0, e1)
         assert v1 > v0 - 0.02, (v0, v1)
 
 
