@@ -367,8 +367,8 @@ typedef struct ofc_pair_in {
 
 /*
  * Many independent pairs of any sizes (the CLI's pair runs, or the pairs of a sequence step) in one call: each
- * result equals ofc_track_pair's bit for bit. The pairs run on up to four worker lanes of their own streams and
- * buffers, the largest windows first; while one lane's pair computes, the host feeds the others, so small pairs
+ * result equals ofc_track_pair's bit for bit. The pairs run on up to four worker lanes (the environment variable
+ * OFC_PAIR_WORKERS sets 1 to 16) of their own streams and buffers, the largest windows first; while one lane's pair computes, the host feeds the others, so small pairs
  * overlap instead of leaving the GPU idle between their launches. outs[i] gets pairs[i]'s results.
  */
 OFC_API int ofc_track_pairs(ofc_engine* eng, const ofc_pair_in* pairs, size_t n, const ofc_config* cfg,
