@@ -1,9 +1,9 @@
 """The CPU-runnable benchmark sequence (five uint8 256 x 256 frames, uniform strain exx = 0.005 k about the centre
 plus a 0.8 k px translation, noise 0.005, chain mode, defaults, no ROI) against the reference's own track_sequence
 (tests/golden/config1.npz, written by tests/golden/make_golden_config1.py): every frame within the pair bars
-(fields 1e-3 px on the pixels valid in both, validity flips only near conf_min or within the guard distance of such
-a pixel, strain RMS 1e-5 on every pixel valid in both), the reference index exactly, the mean confidence within
-1e-3; the largest differences are printed (CONFIG1 lines with -s).
+(fields within 1e-3 px and strains within 1e-5 at every pixel valid in both, validity flips only near conf_min or
+within the guard distance of such a pixel), the reference index exactly, the mean confidence within 1e-3; the
+largest differences are printed (CONFIG1 lines with -s).
 The uint8 frames through the streamed driver (grey levels on the GPU) give the array entry's results bit for bit."""
 import numpy as np
 import pytest
@@ -50,7 +50,8 @@ def test_config1_sequence_against_the_reference():
             smax[q] = float(np.abs(a[m].astype(np.float64) - b[m]).max())
         print(f"CONFIG1 frame {k}: validity diffs {int(diff.sum())}, low flips {int(low_flip.sum())} (band {band:.2e}), "
               f"field max {fmax:.2e}, strain max {smax}", flush=True)
-        assert fmax < 1e-2, (k, fmax)
+        # the contract's own bars at every pixel valid in both (measured: fields 3.9e-6 px, strains 4.8e-7 at most)
+        assert fmax < DISP_TOL and max(smax.values()) < STRAIN_TOL, (k, fmax, smax)
         ref_idx, mean_conf = g[p + "meta"]
         assert r.timing["reference"] == int(ref_idx) and abs(r.timing["mean_conf"] - mean_conf) < 1e-3, k
     streamed = dict(track_stream(u8, cfg))
