@@ -1,7 +1,8 @@
 // gemm_sm100.cu -- BF16 x BF16 -> FP32 GEMMs on the 5th-generation tensor cores, for the learned coarse proposal's
 // convolutions (forward, weight gradient, input gradient). Each is a CUTLASS sm100 collective: TMA loads of 128 x 64
-// and 64 x 64 operand tiles into shared memory (no cluster multicast: clusters of one CTA), tcgen05.mma issued by one
-// thread into a TMEM accumulator, and a TMEM -> register -> TMA-store epilogue. All three compute
+// and 64 x 64 operand tiles into shared memory (clusters of one CTA: each CTA loads only its own tiles),
+// tcgen05.mma issued by one thread into a TMEM accumulator, and a TMEM -> register -> TMA-store epilogue. All three
+// compute
 //   C[l] (M x N, row-major, float) = A[l] (M x K) * B[l] (K x N) + beta C[l],   l < batch,
 // and differ in which operand dimension is contiguous:
 //   GemmKind::ForwardTN   A K-contiguous (im2col rows), B K-contiguous (weights [N][K])      -> conv forward
