@@ -3166,6 +3166,28 @@ int ofc_test_poc_peaks(ofc_engine* e, const float* a, const float* b, size_t w, 
   });
 }
 
+int ofc_test_warp(ofc_engine* e, const float* c2, size_t w2, size_t h2, const double* sx, const double* sy, long shx,
+                  long shy, size_t w, size_t h, int mode, float* out, uint32_t* timeouts, char* err, size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    check_sizes(w2, h2);
+    check_sizes(w, h);
+    if (!c2 || !sx || !sy || !out) throw Error(OFC_ERR_ARG, "null argument");
+    const size_t N = w * h;
+    float* dc = L.upload("t_warp_c2", c2, w2 * h2);
+    double* dsx = L.upload("t_warp_sx", sx, N);
+    double* dsy = L.upload("t_warp_sy", sy, N);
+    float* o = L.get<float>("t_warp_out", N);
+    unsigned* tmo = L.get<unsigned>("t_warp_timeouts", 1);
+    OFC_CUDA(cudaMemsetAsync(tmo, 0, sizeof(unsigned), L.stream));
+    launch_warp_mode(mode, dc, (int)w2, (int)h2, dsx, dsy, shx, shy, (int)w, (int)h, o, tmo, L.stream);
+    OFC_CUDA(cudaMemcpyAsync(out, o, N * sizeof(float), cudaMemcpyDeviceToHost, L.stream));
+    unsigned th = 0;
+    OFC_CUDA(cudaMemcpyAsync(&th, tmo, sizeof(unsigned), cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+    if (timeouts) *timeouts = th;
+  });
+}
+
 int ofc_test_prewarp_fill(ofc_engine* e, const uint8_t* low, const double* ux, const double* uy, const double* slope,
                           size_t w, size_t h, double radius, double* oux, double* ouy, char* err, size_t errlen) {
   return guarded(e, err, errlen, [&](Lane& L) {

@@ -319,24 +319,27 @@ void launch_bspline_f32(const float* in, float* out, double* tmp, int W, int H, 
 }
 
 // ---------------------------------------------------------------- warp
-__global__ void __launch_bounds__(128, 10) k_warp(const float* __restrict__ c2, int w2, int h2, const double* __restrict__ sx,
+__global__ void __launch_bounds__(128, 8) k_warp(const float* __restrict__ c2, int w2, int h2, const double* __restrict__ sx,
                        const double* __restrict__ sy, long shx, long shy, int W, int H, float* __restrict__ out) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y;
   if (x >= W) return;
-  size_t p = (size_t)y * W + x;
-  Taps t;
-  double v;
-  if (make_taps(((double)x + (double)shx) + sx[p], ((double)y + (double)shy) + sy[p], w2, h2, t))
-    v = sample_real(c2, w2, t);
-  else
-    v = nan("");
-  out[p] = (float)v;
+  for (int y = blockIdx.y; y < H; y += gridDim.y) {  // rows beyond the grid's 65535 in steps of gridDim.y
+    size_t p = (size_t)y * W + x;
+    Taps t;
+    double v;
+    if (make_taps(((double)x + (double)shx) + sx[p], ((double)y + (double)shy) + sy[p], w2, h2, t))
+      v = sample_real(c2, w2, t);
+    else
+      v = nan("");
+    out[p] = (float)v;
+  }
 }
 
-void launch_warp(const float* c2, int w2, int h2, const double* sx, const double* sy, long shx, long shy, int W, int H,
-                 float* out, cudaStream_t st) {
-  dim3 g(div_up(W, 128), H);
+// the warp as a plain gather: the form for coefficient planes whose row pitch is not a multiple of 16 bytes (no
+// tensor map), and the reference the TMA-staged warp (warp_tma.cu) is checked against
+void launch_warp_gather(const float* c2, int w2, int h2, const double* sx, const double* sy, long shx, long shy, int W,
+                        int H, float* out, cudaStream_t st) {
+  dim3 g(div_up(W, 128), (unsigned)std::min(H, 65535));
   OFC_LAUNCH(k_warp, g, 128, 0, st, c2, w2, h2, sx, sy, shx, shy, W, H, out);
 }
 

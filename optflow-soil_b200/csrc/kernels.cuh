@@ -22,6 +22,13 @@ void launch_bspline_f64_pair(const double* in, double2* out, double* tmp, int W,
 // (x + shx + sx, y + shy + sy); spline2 is w2 x h2, out W x H
 void launch_warp(const float* c2, int w2, int h2, const double* sx, const double* sy, long shx, long shy, int W, int H,
                  float* out, cudaStream_t st);
+// the gather form of the warp (fine.cu); launch_warp (warp_tma.cu) stages each output tile's source region with a TMA
+// tile load and falls back to this where the coefficient plane has no tensor map
+void launch_warp_gather(const float* c2, int w2, int h2, const double* sx, const double* sy, long shx, long shy, int W,
+                        int H, float* out, cudaStream_t st);
+// the TMA-staged warp alone (mode 1) or the gather (mode 0), with the count of its timed-out tile waits
+void launch_warp_mode(int mode, const float* c2, int w2, int h2, const double* sx, const double* sy, long shx,
+                      long shy, int W, int H, float* out, unsigned* timeouts, cudaStream_t st);
 
 // the seven per-pixel sums of an inner iteration (phaseflow.py:468-483); ref4: F planes W x H of the reference
 // pack (r.re, r.im, gx, gy); R: F response planes (ph x pw); sums: 7 planes W x H

@@ -117,3 +117,19 @@ def first_sums(I1, I2, ux, uy, cfg=None, engine=None):
     eng._call("ofc_test_first_sums", _ptr(a, c_float_p), _ptr(b, c_float_p), w, h, _ptr(ux, c_double_p),
               _ptr(uy, c_double_p), ctypes.byref(c), _ptr(out, c_double_p))
     return out
+
+
+def warp(c2, sx, sy, shift=(0, 0), mode=1, engine=None):
+    """The B-spline warp of coefficient plane c2 (h2 x w2 float32) at (x + shift_x + sx, y + shift_y + sy) for fields
+    sx, sy (h x w float64), by the gather kernel (mode 0) or the TMA-staged kernel (mode 1): (out float32 h x w,
+    timed-out tile waits)."""
+    eng = engine or default_engine()
+    c = _f32(c2)
+    h2, w2 = c.shape
+    fx, fy = _d(sx), _d(sy)
+    h, w = fx.shape
+    out = np.empty((h, w), np.float32)
+    tmo = ctypes.c_uint32(0)
+    eng._call("ofc_test_warp", _ptr(c, c_float_p), w2, h2, _ptr(fx, c_double_p), _ptr(fy, c_double_p),
+              int(shift[0]), int(shift[1]), w, h, int(mode), _ptr(out, c_float_p), ctypes.byref(tmo))
+    return out, tmo.value
