@@ -609,7 +609,7 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
   double* sums = L.get<double>("sums", 7 * N);
   double* yplanes = L.get<double>("yplanes", (size_t)moment_yplanes(c.shape_order) * N);
   float* warped = L.get<float>("warped", N);
-  float2* R = L.get<float2>("resp", Np * F);
+  float2* R = L.get<float2>("resp", resp_values(F, Np));
   EnergyStats* stats = L.get<EnergyStats>("stats", 1);
   unsigned long long* hist = L.get<unsigned long long>("hist", MEDIAN_SCRATCH);
   uint8_t* low = L.get<uint8_t>("low", N);
@@ -3073,12 +3073,17 @@ int ofc_test_responses(ofc_engine* e, const float* img, size_t w, size_t h, cons
     float* d1 = L.upload("in_i1", img, N);
     float2* T = L.get<float2>("fft_T", Np);
     float2* U = L.get<float2>("fft_U", Np * F);
-    float2* R = L.get<float2>("resp", Np * F);
+    float2* R = L.get<float2>("resp", resp_values(F, Np));
     launch_fft_rows_fwd_real(d1, W, H, L.plan(pw), ph, T, L.stream);
     launch_fft_cols_filters(T, L.plan(ph), pw, g, U, L.stream);
     launch_fft_rows_inv_resp(U, L.plan(pw), ph, F, R, L.stream);
-    OFC_CUDA(cudaMemcpyAsync(resp, R, Np * F * sizeof(float2), cudaMemcpyDeviceToHost, L.stream));
+    // the pair layout back to F planes of ph x pw
+    std::vector<float2> h(resp_values(F, Np));
+    OFC_CUDA(cudaMemcpyAsync(h.data(), R, h.size() * sizeof(float2), cudaMemcpyDeviceToHost, L.stream));
     OFC_CUDA(cudaStreamSynchronize(L.stream));
+    float2* out = reinterpret_cast<float2*>(resp);
+    for (int k = 0; k < F; k++)
+      for (size_t i = 0; i < Np; i++) out[(size_t)k * Np + i] = h[((size_t)(k / 2) * Np + i) * 2 + (k & 1)];
   });
 }
 
@@ -3246,7 +3251,7 @@ int ofc_test_first_sums(ofc_engine* e, const float* i1, const float* i2, size_t 
     launch_corr_x(tmpb, s2, 2, W, H, d_ks, (int)ks.size() / 2, st);
     float* warped = L.get<float>("warped", N);
     launch_warp(c2, W, H, s2, s2 + N, 0, 0, W, H, warped, st);
-    float2* R = L.get<float2>("resp", Np * F);
+    float2* R = L.get<float2>("resp", resp_values(F, Np));
     launch_fft_rows_fwd_real(warped, W, H, L.plan(pw), ph, T, st);
     launch_fft_cols_filters(T, L.plan(ph), pw, g, U, st);
     launch_fft_rows_inv_resp(U, L.plan(pw), ph, F, R, st);

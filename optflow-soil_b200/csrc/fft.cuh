@@ -79,8 +79,11 @@ void launch_fft_rows_fwd_real(const float* img, int W, int H, const FftPlan& plw
 // column transforms of the responses: forward (in place in T, which then holds the 2-D spectrum), then per
 // filter multiply + inverse + B-spline prefilter along y -> U: F planes (ph x pw)
 void launch_fft_cols_filters(float2* T, const FftPlan& plh, int pw, const GaborTables& g, float2* U, cudaStream_t st);
-// inverse row transforms + B-spline prefilter along x + scale -> responses R (F planes of ph x pw)
+// inverse row transforms + B-spline prefilter along x + scale -> responses R in filter pairs, node-major: filter
+// 2j + c at node (y, x) at R[((j ph + y) pw + x) 2 + c] (pair j's second filter a copy of filter F - 1 when F is odd);
+// R holds resp_values(F, ph * pw) values
 void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F, float2* R, cudaStream_t st);
+inline size_t resp_values(int F, size_t Np) { return (size_t)2 * ((F + 1) / 2) * Np; }
 
 // the reference pack (reference_phase, phaseflow.py:92-112). launch_fft_cols_fwd: forward column transforms of the
 // row-transformed T, in place (T then holds the 2-D spectrum S); launch_fft_cols_ref_f32: for filters [k0, k1) the

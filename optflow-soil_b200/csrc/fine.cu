@@ -351,9 +351,14 @@ void launch_warp_gather(const float* c2, int w2, int h2, const double* sx, const
 // sum gcc - theta . b cancels. The kernel is latency-bound, so: the F reference-pack values of the pixel are
 // copied to shared memory asynchronously at the start (in flight during the fixed point); |r1| |r2| is one square
 // root of |r1|^2 |r2|^2, with |r1|^2 formed from the pack; the 16 tap offsets are computed once and reused by every
-// filter; the field spline is stored interleaved (one 16-byte load per tap for both components).
+// filter; the field spline is stored interleaved (one 16-byte load per tap for both components); the responses are
+// stored in filter pairs, node-major, so one 16-byte load per tap serves two filters (96 tap loads per pixel at F = 12
+// instead of 192).
 constexpr int ACC_BX = 32, ACC_BY = 8, ACC_T = ACC_BX * ACC_BY;
-__global__ void __launch_bounds__(ACC_T, 1024 / ACC_T) k_accumulate(const float4* __restrict__ ref4, const float2* __restrict__ R,
+#ifndef ACC_MINB
+#define ACC_MINB 4
+#endif
+__global__ void __launch_bounds__(ACC_T, ACC_MINB) k_accumulate(const float4* __restrict__ ref4, const float2* __restrict__ R,
                                                       int F, int ph, int pw, const double* __restrict__ ux,
                                                       const double* __restrict__ uy, const double* __restrict__ sx,
                                                       const double* __restrict__ sy, const double2* __restrict__ cs,
@@ -398,34 +403,11 @@ __global__ void __launch_bounds__(ACC_T, 1024 / ACC_T) k_accumulate(const float4
   }
   const size_t plane = (size_t)ph * pw;
   const float fnan = __int_as_float(0x7fc00000);
-  __pipeline_wait_prior(0);
-  for (int k = 0; k < F; k++) {
+  // filter k's contribution from its complex response sample b at X' (r2 of phaseflow.py:476-483)
+  auto add = [&](int k, float br, float bi) {
     const float4 r1 = pk[k * ACC_T + tid];
     // |r1|^2 as the reference pack's amplitude squared (phaseflow.py:111), from the stored float32 response
     const float q1 = fmaf(r1.x, r1.x, fmaf(r1.y, r1.y, 1e-12f));
-    float br = fnan, bi = fnan;
-    if (ok) {
-      const float2* Rk = R + (size_t)k * plane;
-      // the next filter's tap rows into L1 while this filter's taps and arithmetic run
-      if (k + 1 < F) {
-#pragma unroll
-        for (int j = 0; j < 4; j++) asm volatile("prefetch.global.L1 [%0];" ::"l"(Rk + plane + (ro[j] + xo[0])));
-      }
-      br = 0.f;
-      bi = 0.f;
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        float are = 0.f, aim = 0.f;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const float2 c = __ldg(Rk + (ro[j] + xo[q]));
-          are = fmaf(fwx[q], c.x, are);
-          aim = fmaf(fwx[q], c.y, aim);
-        }
-        br = fmaf(fwy[j], are, br);
-        bi = fmaf(fwy[j], aim, bi);
-      }
-    }
     // r1 conj(r2)
     const float re = fmaf(r1.x, br, r1.y * bi);
     const float im = fmaf(r1.y, br, -r1.x * bi);
@@ -441,6 +423,40 @@ __global__ void __launch_bounds__(ACC_T, 1024 / ACC_T) k_accumulate(const float4
     a4 = fma(wgy, c, a4);
     a5 = fma(wk * c, c, a5);
     a6 += wk;
+  };
+  // the responses in filter pairs, node-major: one 16-byte load per tap gives both filters of a pair
+  const float4* R4 = reinterpret_cast<const float4*>(R);
+  const int npairs = (F + 1) >> 1;
+  __pipeline_wait_prior(0);
+  for (int j = 0; j < npairs; j++) {
+    float b0r = fnan, b0i = fnan, b1r = fnan, b1i = fnan;
+    if (ok) {
+      const float4* Rj = R4 + (size_t)j * plane;
+      // the next pair's tap rows into L1 while this pair's taps and arithmetic run
+      if (j + 1 < npairs) {
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) asm volatile("prefetch.global.L1 [%0];" ::"l"(Rj + plane + (ro[jj] + xo[0])));
+      }
+      b0r = b0i = b1r = b1i = 0.f;
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) {
+        float a0r = 0.f, a0i = 0.f, a1r = 0.f, a1i = 0.f;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const float4 cv = __ldg(Rj + (ro[jj] + xo[q]));
+          a0r = fmaf(fwx[q], cv.x, a0r);
+          a0i = fmaf(fwx[q], cv.y, a0i);
+          a1r = fmaf(fwx[q], cv.z, a1r);
+          a1i = fmaf(fwx[q], cv.w, a1i);
+        }
+        b0r = fmaf(fwy[jj], a0r, b0r);
+        b0i = fmaf(fwy[jj], a0i, b0i);
+        b1r = fmaf(fwy[jj], a1r, b1r);
+        b1i = fmaf(fwy[jj], a1i, b1i);
+      }
+    }
+    add(2 * j, b0r, b0i);
+    if (2 * j + 1 < F) add(2 * j + 1, b1r, b1i);
   }
   sums[p] = a0;
   sums[N + p] = a1;
