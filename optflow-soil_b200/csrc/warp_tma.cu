@@ -74,7 +74,12 @@ __global__ void __launch_bounds__(WT_THREADS, 6) k_warp_tma(const __grid_constan
       }
     }
   }
-  if (lo_x <= hi_x) {
+  // the warp's extremes by warp reductions, then one shared atomic per warp and quantity
+  lo_x = __reduce_min_sync(0xffffffffu, lo_x);
+  hi_x = __reduce_max_sync(0xffffffffu, hi_x);
+  lo_y = __reduce_min_sync(0xffffffffu, lo_y);
+  hi_y = __reduce_max_sync(0xffffffffu, hi_y);
+  if (tx == 0 && lo_x <= hi_x) {
     atomicMin(&smin_x, lo_x);
     atomicMax(&smax_x, hi_x);
     atomicMin(&smin_y, lo_y);
