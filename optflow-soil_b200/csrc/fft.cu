@@ -949,91 +949,52 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const floa
   }
 }
 
-// Inverse row transforms of the filtered spectra into the responses R, persistent: a block walks the work items
-// blockIdx.x, + gridDim.x, ... and copies the next item's lines into a third buffer (cp.async) while it transforms the
-// current ones; then the prefilter's edge terms along x and the scale 36 / (ph pw).
+// Inverse row transforms of the filtered spectra into the responses R, persistent: a block walks the lines
+// blockIdx.x, + gridDim.x, ... and copies the next line into a third buffer (cp.async) while it transforms the
+// current one; then the prefilter's edge terms along x and the scale 36 / (ph pw).
 // R holds the filters in pairs, node-major: pair j = filters 2j and 2j + 1 (the second a copy of filter F - 1 when F
 // is odd), filter 2j + c at node (y, x) at R[((j ph + y) pw + x) 2 + c], so that one 16-byte load takes a tap of both
-// filters of a pair. C = 2: an item is row y of pair j, its two lines transformed interleaved (the transforms'
-// C-line layout is the pair layout) and stored as 16-byte runs. C = 1, for work lengths whose three interleaved
-// buffers do not fit in shared memory: an item is one line, stored at a 16-byte stride.
-struct RespItem {
-  int j, y, c;
-};
-template <int C>
-__device__ __forceinline__ RespItem resp_item(int item, int ph) {
-  RespItem r;
-  if constexpr (C == 2) {
-    r.j = item / ph;
-    r.y = item - r.j * ph;
-    r.c = 0;
-  } else {
-    r.j = item / (2 * ph);
-    const int q = item - r.j * 2 * ph;
-    r.y = q >> 1;
-    r.c = q & 1;
-  }
-  return r;
-}
-constexpr int rows_resp_threads(int fixl, int C) { return fixl > 0 ? (C == 2 ? 512 : 288) : FFT_TMAX; }
-
-template <int FIXL, int C>
-__global__ void __launch_bounds__(rows_resp_threads(FIXL, C), FIXL > 0 ? (C == 2 ? 2 : 3) : 2)
-    k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int ph, int F, int nitems, float scale,
+// filters of a pair. Work line l = (j ph + y) 2 + c: the two lines of a node row are consecutive, so neighbouring
+// blocks transform them at the same time and the two 8-byte halves of each 16-byte node meet in L2. (Transforming
+// both lines in one block, interleaved, waits longer at the Stockham barriers of its 512-thread blocks: 0.377
+// against 0.318 ms per launch at 2112.)
+template <int FIXL>
+__global__ void __launch_bounds__(FIXL > 0 ? 288 : FFT_TMAX, FIXL > 0 ? 3 : 2)
+    k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int ph, int F, int nlines, float scale,
                         float2* __restrict__ R) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int L = FIXL > 0 ? FIXL : plw.L, nb = fft_buf_stride(FIXL > 0 ? FIXL : fft_work_len(plw), C);
+  const int L = FIXL > 0 ? FIXL : plw.L, nb = fft_buf_stride(FIXL > 0 ? FIXL : fft_work_len(plw), 1);
   float2* in = (float2*)smraw;
   float2* tmp = in + nb;
   float2* pre = tmp + nb;
-  auto line_of = [&](const RespItem& it, int c) { return U + ((size_t)min(2 * it.j + c, F - 1) * ph + it.y) * L; };
-  auto prefetch = [&](int item, float2* dst) {
-    const RespItem it = resp_item<C>(item, ph);
-    if constexpr (C == 2) {  // the two lines interleaved: value i of line c at 2 i + c
-      const float2* s0 = line_of(it, 0);
-      const float2* s1 = line_of(it, 1);
-      for (int i = threadIdx.x; i < L; i += blockDim.x) {
-        __pipeline_memcpy_async(dst + 2 * i, s0 + i, 8);
-        __pipeline_memcpy_async(dst + 2 * i + 1, s1 + i, 8);
-      }
+  auto prefetch = [&](int line, float2* dst) {
+    const int row = line >> 1, j = row / ph, y = row - j * ph;
+    const float2* src = U + ((size_t)min(2 * j + (line & 1), F - 1) * ph + y) * L;
+    if (L % 2 == 0) {  // 16-byte chunks: the line starts on a 16-byte boundary
+      for (int i = threadIdx.x; i < L / 2; i += blockDim.x) __pipeline_memcpy_async(dst + 2 * i, src + 2 * i, 16);
     } else {
-      const float2* src = line_of(it, it.c);
-      if (L % 2 == 0) {  // 16-byte chunks: the line starts on a 16-byte boundary
-        for (int i = threadIdx.x; i < L / 2; i += blockDim.x) __pipeline_memcpy_async(dst + 2 * i, src + 2 * i, 16);
-      } else {
-        for (int i = threadIdx.x; i < L; i += blockDim.x) __pipeline_memcpy_async(dst + i, src + i, 8);
-      }
+      for (int i = threadIdx.x; i < L; i += blockDim.x) __pipeline_memcpy_async(dst + i, src + i, 8);
     }
     __pipeline_commit();
   };
-  int item = blockIdx.x;
-  if (item < nitems) prefetch(item, in);
-  for (; item < nitems; item += gridDim.x) {
-    const int nxt = item + gridDim.x;
-    if (nxt < nitems) {
+  int line = blockIdx.x;
+  if (line < nlines) prefetch(line, in);
+  for (; line < nlines; line += gridDim.x) {
+    const int nxt = line + gridDim.x;
+    if (nxt < nlines) {
       prefetch(nxt, pre);
       __pipeline_wait_prior(1);
     } else {
       __pipeline_wait_prior(0);
     }
     __syncthreads();
-    float2* r = fft_run<FIXL, C>(in, tmp, plw, true);
+    float2* r = fft_run<FIXL, 1>(in, tmp, plw, true);
     float2* idle = r == in ? tmp : in;
-    bspline_edges<C>(r, L, (float4*)idle);  // the prefilter's edge terms along x
-    const RespItem it = resp_item<C>(item, ph);
-    if constexpr (C == 2) {
-      float4* o = (float4*)R + ((size_t)it.j * ph + it.y) * L;
-      const float4* r4 = (const float4*)r;
-      for (int x = threadIdx.x; x < L; x += blockDim.x) {
-        const float4 v = r4[x];
-        o[x] = make_float4(v.x * scale, v.y * scale, v.z * scale, v.w * scale);
-      }
-    } else {
-      float2* o = R + ((size_t)it.j * ph + it.y) * L * 2 + it.c;
-      for (int x = threadIdx.x; x < L; x += blockDim.x) {
-        const float2 v = r[x];
-        o[2 * (size_t)x] = make_float2(v.x * scale, v.y * scale);
-      }
+    bspline_edges<1>(r, L, (float4*)idle);  // the prefilter's edge terms along x
+    float2* o = R + (size_t)(line >> 1) * L * 2 + (line & 1);  // node row (j ph + y), lane c of each node
+    for (int x = threadIdx.x; x < L; x += blockDim.x) {
+      const float2 v = r[x];
+      o[2 * x] = make_float2(v.x * scale, v.y * scale);
     }
     __syncthreads();
     float2* done = in;
@@ -1124,8 +1085,8 @@ static size_t smem_prefilter(int L, int C, int T) {
 static size_t smem_cols_pair(int L, int WL) {
   return ((size_t)2 * L + 2 * (size_t)fft_buf_stride(WL, 2)) * sizeof(float2);
 }
-// k_fft_rows_inv_resp: three buffers of C interleaved lines at the even stride
-static size_t smem_rows_resp(int L, int C = 1) { return 3 * (size_t)fft_buf_stride(L, C) * sizeof(float2); }
+// k_fft_rows_inv_resp: three buffers at the even stride
+static size_t smem_rows_resp(int L) { return 3 * (size_t)fft_buf_stride(L, 1) * sizeof(float2); }
 
 // calls f with std::integral_constant<int, FIXL> for the kernels' instantiation of a plan: the fixed length, the
 // runtime direct plan (0) or the runtime Bluestein plan (-1)
@@ -1218,22 +1179,16 @@ void launch_fft_cols_filters(float2* T, const FftPlan& plh, int pw, const GaborT
 }
 
 void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F, float2* R, cudaStream_t st) {
-  const int WL = fft_work_len(plw);
+  const int T = fft_threads(fft_work_len(plw), 1);
+  const size_t sm = smem_rows_resp(fft_work_len(plw));
   const float scale = (float)(36.0 / ((double)ph * (double)plw.L));
-  const int npairs = (F + 1) / 2;
-  auto go = [&](auto fl, auto cc) {
-    constexpr int FL = decltype(fl)::value, C = decltype(cc)::value;
-    const int T = FL > 0 ? rows_resp_threads(FL, C) : fft_threads(WL, C);
-    const size_t sm = smem_rows_resp(WL, C);
-    const int nitems = npairs * ph * (C == 2 ? 1 : 2);
-    const void* fn = (const void*)k_fft_rows_inv_resp<FL, C>;
-    set_smem(fn, sm);
-    OFC_LAUNCH((k_fft_rows_inv_resp<FL, C>), persistent_blocks(fn, T, sm, nitems), T, sm, st, U, plw, ph, F, nitems,
-               scale, R);
-  };
+  const int nlines = 2 * ((F + 1) / 2) * ph;
   by_plan(plw, [&](auto fl) {
-    if (smem_rows_resp(WL, 2) <= SMEM_MAX) go(fl, std::integral_constant<int, 2>{});
-    else go(fl, std::integral_constant<int, 1>{});
+    constexpr int FL = decltype(fl)::value;
+    const void* fn = (const void*)k_fft_rows_inv_resp<FL>;
+    set_smem(fn, sm);
+    OFC_LAUNCH(k_fft_rows_inv_resp<FL>, persistent_blocks(fn, T, sm, nlines), T, sm, st, U, plw, ph, F, nlines, scale,
+               R);
   });
 }
 
