@@ -949,59 +949,67 @@ __global__ void __launch_bounds__(COLS_TMAX, 3) k_fft_cols_inv_filter(const floa
   }
 }
 
-// Inverse row transforms of the filtered spectra into the responses R, persistent: a block walks the lines
-// blockIdx.x, + gridDim.x, ... and copies the next line into a third buffer (cp.async) while it transforms the
-// current one; then the prefilter's edge terms along x and the scale 36 / (ph pw).
+// Inverse row transforms of the filtered spectra into the responses R, persistent: a block walks the node rows
+// blockIdx.x, + gridDim.x, ...; per node row it transforms the row's two lines one after the other, each followed by
+// the prefilter's edge terms along x, and stores both at once with the scale 36 / (ph pw).
 // R holds the filters in pairs, node-major: pair j = filters 2j and 2j + 1 (the second a copy of filter F - 1 when F
 // is odd), filter 2j + c at node (y, x) at R[((j ph + y) pw + x) 2 + c], so that one 16-byte load takes a tap of both
-// filters of a pair. Work line l = (j ph + y) 2 + c: the two lines of a node row are consecutive, so neighbouring
-// blocks transform them at the same time and the two 8-byte halves of each 16-byte node meet in L2. (Transforming
-// both lines in one block, interleaved, waits longer at the Stockham barriers of its 512-thread blocks: 0.377
-// against 0.318 ms per launch at 2112.)
+// filters of a pair, and node row (j, y) is one run of pw 16-byte stores.
+// Four line buffers: the first line's result waits in one while the second line is transformed in two others, and the
+// fourth receives the next row's first line (cp.async) meanwhile; the next row's second line is copied while its
+// first line is transformed. (Both lines in one interleaved transform waits longer at the Stockham barriers of its
+// 512-thread blocks: 0.377 ms per launch at 2112; one line per block with 8-byte stores 16 bytes apart: 0.36 ms.)
 template <int FIXL>
 __global__ void __launch_bounds__(FIXL > 0 ? 288 : FFT_TMAX, FIXL > 0 ? 3 : 2)
-    k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int ph, int F, int nlines, float scale,
+    k_fft_rows_inv_resp(const float2* __restrict__ U, FftPlan plw, int ph, int F, int nrows, float scale,
                         float2* __restrict__ R) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int L = FIXL > 0 ? FIXL : plw.L, nb = fft_buf_stride(FIXL > 0 ? FIXL : fft_work_len(plw), 1);
-  float2* in = (float2*)smraw;
-  float2* tmp = in + nb;
-  float2* pre = tmp + nb;
-  auto prefetch = [&](int line, float2* dst) {
-    const int row = line >> 1, j = row / ph, y = row - j * ph;
-    const float2* src = U + ((size_t)min(2 * j + (line & 1), F - 1) * ph + y) * L;
-    if (L % 2 == 0) {  // 16-byte chunks: the line starts on a 16-byte boundary
-      for (int i = threadIdx.x; i < L / 2; i += blockDim.x) __pipeline_memcpy_async(dst + 2 * i, src + 2 * i, 16);
-    } else {
-      for (int i = threadIdx.x; i < L; i += blockDim.x) __pipeline_memcpy_async(dst + i, src + i, 8);
+  float2* b0 = (float2*)smraw;
+  float2 *x0 = b0, *x1 = b0 + nb, *fa = b0 + 2 * nb, *fb = b0 + 3 * nb;
+  // copies line c of node row `row` into dst as one group of asynchronous copies (an empty group past the end)
+  auto fetch = [&](int row, int c, float2* dst) {
+    if (row < nrows) {
+      const int j = row / ph, y = row - j * ph;
+      const float2* src = U + ((size_t)min(2 * j + c, F - 1) * ph + y) * L;
+      if (L % 2 == 0) {  // 16-byte chunks: the line starts on a 16-byte boundary
+        for (int i = threadIdx.x; i < L / 2; i += blockDim.x) __pipeline_memcpy_async(dst + 2 * i, src + 2 * i, 16);
+      } else {
+        for (int i = threadIdx.x; i < L; i += blockDim.x) __pipeline_memcpy_async(dst + i, src + i, 8);
+      }
     }
     __pipeline_commit();
   };
-  int line = blockIdx.x;
-  if (line < nlines) prefetch(line, in);
-  for (; line < nlines; line += gridDim.x) {
-    const int nxt = line + gridDim.x;
-    if (nxt < nlines) {
-      prefetch(nxt, pre);
-      __pipeline_wait_prior(1);
-    } else {
-      __pipeline_wait_prior(0);
-    }
+  int row = blockIdx.x;
+  fetch(row, 0, x0);
+  fetch(row, 1, x1);
+  for (; row < nrows; row += gridDim.x) {
+    const int nxt = row + gridDim.x;
+    __pipeline_wait_prior(1);  // line 0 has landed (line 1 may be in flight)
     __syncthreads();
-    float2* r = fft_run<FIXL, 1>(in, tmp, plw, true);
-    float2* idle = r == in ? tmp : in;
-    bspline_edges<1>(r, L, (float4*)idle);  // the prefilter's edge terms along x
-    float2* o = R + (size_t)(line >> 1) * L * 2 + (line & 1);  // node row (j ph + y), lane c of each node
+    float2* r0 = fft_run<FIXL, 1>(x0, fa, plw, true);
+    float2* s0 = r0 == x0 ? fa : x0;
+    bspline_edges<1>(r0, L, (float4*)s0);
+    fetch(nxt, 0, fb);         // the next row's line 0 during line 1's transform
+    __pipeline_wait_prior(1);  // line 1 has landed
+    __syncthreads();
+    float2* r1 = fft_run<FIXL, 1>(x1, s0, plw, true);
+    float2* s1 = r1 == x1 ? s0 : x1;
+    bspline_edges<1>(r1, L, (float4*)s1);
+    float4* o = (float4*)R + (size_t)row * L;
     for (int x = threadIdx.x; x < L; x += blockDim.x) {
-      const float2 v = r[x];
-      o[2 * x] = make_float2(v.x * scale, v.y * scale);
+      const float2 a = r0[x], b = r1[x];
+      o[x] = make_float4(a.x * scale, a.y * scale, b.x * scale, b.y * scale);
     }
     __syncthreads();
-    float2* done = in;
-    in = pre;
-    pre = tmp;
-    tmp = done;
+    // free now: r0, r1 and s1; the next row's line 0 is in fb
+    fetch(nxt, 1, s1);
+    x0 = fb;
+    x1 = s1;
+    fa = r0;
+    fb = r1;
   }
+  __pipeline_wait_prior(0);
 }
 
 template <int FIXL>
@@ -1085,8 +1093,8 @@ static size_t smem_prefilter(int L, int C, int T) {
 static size_t smem_cols_pair(int L, int WL) {
   return ((size_t)2 * L + 2 * (size_t)fft_buf_stride(WL, 2)) * sizeof(float2);
 }
-// k_fft_rows_inv_resp: three buffers at the even stride
-static size_t smem_rows_resp(int L) { return 3 * (size_t)fft_buf_stride(L, 1) * sizeof(float2); }
+// k_fft_rows_inv_resp: four line buffers at the even stride
+static size_t smem_rows_resp(int L) { return 4 * (size_t)fft_buf_stride(L, 1) * sizeof(float2); }
 
 // calls f with std::integral_constant<int, FIXL> for the kernels' instantiation of a plan: the fixed length, the
 // runtime direct plan (0) or the runtime Bluestein plan (-1)
@@ -1182,12 +1190,12 @@ void launch_fft_rows_inv_resp(const float2* U, const FftPlan& plw, int ph, int F
   const int T = fft_threads(fft_work_len(plw), 1);
   const size_t sm = smem_rows_resp(fft_work_len(plw));
   const float scale = (float)(36.0 / ((double)ph * (double)plw.L));
-  const int nlines = 2 * ((F + 1) / 2) * ph;
+  const int nrows = ((F + 1) / 2) * ph;
   by_plan(plw, [&](auto fl) {
     constexpr int FL = decltype(fl)::value;
     const void* fn = (const void*)k_fft_rows_inv_resp<FL>;
     set_smem(fn, sm);
-    OFC_LAUNCH(k_fft_rows_inv_resp<FL>, persistent_blocks(fn, T, sm, nlines), T, sm, st, U, plw, ph, F, nlines, scale,
+    OFC_LAUNCH(k_fft_rows_inv_resp<FL>, persistent_blocks(fn, T, sm, nrows), T, sm, st, U, plw, ph, F, nrows, scale,
                R);
   });
 }
