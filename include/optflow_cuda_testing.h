@@ -62,6 +62,13 @@ OFC_API int ofc_test_prewarp_fill(ofc_engine* eng, const uint8_t* low, const dou
 OFC_API int ofc_test_first_sums(ofc_engine* eng, const float* i1, const float* i2, size_t w, size_t h, const double* ux,
                                 const double* uy, const ofc_config* cfg, double* sums, char* err, size_t errlen);
 
+/* ofc_test_first_sums with the accumulate kernel chosen: mode 0 the gather kernel, mode 1 the TMA-staged kernel
+ * (the gather kernel where the planes have no tensor maps); *timeouts receives its stage waits that gave up (0 on a
+ * healthy run). */
+OFC_API int ofc_test_accumulate(ofc_engine* eng, const float* i1, const float* i2, size_t w, size_t h, const double* ux,
+                                const double* uy, const ofc_config* cfg, int mode, double* sums, uint32_t* timeouts,
+                                char* err, size_t errlen);
+
 /* The warp of the pre-warp and of the temporal-averaging alignment (warp_shifted, rust/crates/optflow-core/src/
  * phaseflow.rs:1420-1439): out(x, y) = the cubic B-spline of the w2 x h2 coefficient plane c2 sampled at
  * (x + shx + sx(x, y), y + shy + sy(x, y)) for the W x H fields sx, sy (doubles); NaN where a position is NaN.

@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "lib", "liboptflow_cuda.so")
 SOURCES = ["engine.cu", "fft.cu", "fine.cu", "poc.cu", "finish.cu", "synth.cu", "noalloc.cu", "gemm_sm100.cu", "net.cu",
-           "net_api.cu", "proposal.cu", "warp_tma.cu"]
+           "net_api.cu", "proposal.cu", "warp_tma.cu", "tma.cu",
+           "accumulate_tma.cu"]
 # sources compiled against the CUTLASS / CuTe header tree (its sm100 GEMM collectives)
 CUTLASS_SOURCES = {"gemm_sm100.cu"}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -3220,8 +3220,11 @@ int ofc_test_prewarp_fill(ofc_engine* e, const uint8_t* low, const double* ux, c
   });
 }
 
-int ofc_test_first_sums(ofc_engine* e, const float* i1, const float* i2, size_t w, size_t h, const double* ux,
-                        const double* uy, const ofc_config* c, double* sums, char* err, size_t errlen) {
+// refine's first inner-iteration sums from the start field (ux, uy) with the accumulate in `mode` (0: the gather
+// kernel, 1: the TMA-staged kernel); *timeouts: its stage waits that gave up
+static int first_sums(ofc_engine* e, const float* i1, const float* i2, size_t w, size_t h, const double* ux,
+                      const double* uy, const ofc_config* c, int mode, double* sums, uint32_t* timeouts, char* err,
+                      size_t errlen) {
   return guarded(e, err, errlen, [&](Lane& L) {
     cfg_check(c);
     check_fine_window(w, h, *c);
@@ -3257,10 +3260,26 @@ int ofc_test_first_sums(ofc_engine* e, const float* i1, const float* i2, size_t 
     launch_fft_rows_inv_resp(U, L.plan(pw), ph, F, R, st);
     launch_bspline_f64_pair(s2, (double2*)cs2, tmpb, W, H, st);
     double* ds = L.get<double>("sums", 7 * N);
-    launch_accumulate(ref4, R, F, ph, pw, u2, u2 + N, s2, s2 + N, (const double2*)cs2, W, H, ds, st);
+    unsigned* tmo = L.get<unsigned>("t_acc_timeouts", 1);
+    OFC_CUDA(cudaMemsetAsync(tmo, 0, sizeof(unsigned), st));
+    launch_accumulate_mode(mode, ref4, R, F, ph, pw, u2, u2 + N, s2, s2 + N, (const double2*)cs2, W, H, ds, tmo, st);
     OFC_CUDA(cudaMemcpyAsync(sums, ds, 7 * N * 8, cudaMemcpyDeviceToHost, st));
+    unsigned th = 0;
+    OFC_CUDA(cudaMemcpyAsync(&th, tmo, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     OFC_CUDA(cudaStreamSynchronize(st));
+    if (timeouts) *timeouts = th;
   });
+}
+
+int ofc_test_first_sums(ofc_engine* e, const float* i1, const float* i2, size_t w, size_t h, const double* ux,
+                        const double* uy, const ofc_config* c, double* sums, char* err, size_t errlen) {
+  return first_sums(e, i1, i2, w, h, ux, uy, c, 1, sums, nullptr, err, errlen);
+}
+
+int ofc_test_accumulate(ofc_engine* e, const float* i1, const float* i2, size_t w, size_t h, const double* ux,
+                        const double* uy, const ofc_config* c, int mode, double* sums, uint32_t* timeouts, char* err,
+                        size_t errlen) {
+  return first_sums(e, i1, i2, w, h, ux, uy, c, mode, sums, timeouts, err, errlen);
 }
 
 int ofc_set_profile(ofc_engine* e, const char* filter) {

@@ -467,9 +467,11 @@ __global__ void __launch_bounds__(ACC_T, ACC_MINB) k_accumulate(const float4* __
   sums[6 * N + p] = a6;
 }
 
-void launch_accumulate(const float4* ref4, const float2* R, int F, int ph, int pw, const double* ux, const double* uy,
-                       const double* sx, const double* sy, const double2* cs, int W, int H, double* sums,
-                       cudaStream_t st) {
+// the accumulate as a gather from the response planes: the form for planes without tensor maps, and the reference
+// the TMA-staged kernel (accumulate_tma.cu) is checked against
+void launch_accumulate_gather(const float4* ref4, const float2* R, int F, int ph, int pw, const double* ux,
+                              const double* uy, const double* sx, const double* sy, const double2* cs, int W, int H,
+                              double* sums, cudaStream_t st) {
   dim3 g(div_up(W, ACC_BX), div_up(H, ACC_BY));
   const size_t sm = (size_t)F * ACC_T * sizeof(float4);
   if (sm > 227 * 1024) throw Error(OFC_ERR_WINDOW, "too many Gabor filters (" + std::to_string(F) + ") for the CUDA engine");

@@ -31,10 +31,19 @@ void launch_warp_mode(int mode, const float* c2, int w2, int h2, const double* s
                       long shy, int W, int H, float* out, unsigned* timeouts, cudaStream_t st);
 
 // the seven per-pixel sums of an inner iteration (phaseflow.py:468-483); ref4: F planes W x H of the reference
-// pack (r.re, r.im, gx, gy); R: F response planes (ph x pw); sums: 7 planes W x H
+// pack (r.re, r.im, gx, gy); R: the responses in filter pairs, node-major (launch_fft_rows_inv_resp); sums: 7 planes
+// W x H
 void launch_accumulate(const float4* ref4, const float2* R, int F, int ph, int pw, const double* ux, const double* uy,
                        const double* sx, const double* sy, const double2* cs, int W, int H, double* sums,
                        cudaStream_t st);
+// the gather form (fine.cu) and the TMA-staged form (accumulate_tma.cu; mode 0: the gather form; timeouts: a device
+// counter of stage waits that gave up, nullptr for a library-wide one); launch_accumulate takes the staged form
+void launch_accumulate_gather(const float4* ref4, const float2* R, int F, int ph, int pw, const double* ux,
+                              const double* uy, const double* sx, const double* sy, const double2* cs, int W, int H,
+                              double* sums, cudaStream_t st);
+void launch_accumulate_mode(int mode, const float4* ref4, const float2* R, int F, int ph, int pw, const double* ux,
+                            const double* uy, const double* sx, const double* sy, const double2* cs, int W, int H,
+                            double* sums, unsigned* timeouts, cudaStream_t st);
 
 // Gaussian window moments + the per-pixel shape-function solve (phaseflow.py:114-161): mtaps: the
 // window taps k(t) t^p for p = 0..4 (5 x (2r+1) doubles, device); tp: the same taps for t = 0..r as a kernel

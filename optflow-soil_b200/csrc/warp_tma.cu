@@ -11,32 +11,16 @@
 // gather kernel does. Both paths run the same sampler on the same taps, so the output equals the gather kernel's bit
 // for bit. Waits on the mbarrier are bounded: a thread that gives up counts a timeout and samples global memory, and
 // the issuing thread waits again (bounded) before the block leaves, so no copy lands in a freed buffer.
-#include <cuda.h>
-
 #include <climits>
-#include <mutex>
 
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace ofc {
 namespace {
 
 constexpr int WT_X = 32, WT_Y = 16, WT_THREADS = 128;
 constexpr int BOX_W = 64, BOX_H = 40;
-constexpr unsigned WAIT_LIMIT = 1u << 22;
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(addr), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
 // the tap origin floor(clamp(p, 0, n - 1)) of make_taps
 __device__ __forceinline__ int tap_floor(double p, int n) { return (int)floor(fmin(fmax(p, 0.0), (double)(n - 1))); }
 
@@ -86,7 +70,7 @@ __global__ void __launch_bounds__(WT_THREADS, 6) k_warp_tma(const __grid_constan
     atomicMax(&smax_y, hi_y);
   }
   __syncthreads();
-  const uint32_t mbar_addr = (uint32_t)__cvta_generic_to_shared(&mbar);
+  const uint32_t mbar_addr = smem_addr(&mbar);
   if (tid == 0) {
     const int bx0 = ((smin_x - 1) >> 2) << 2;  // a multiple of 4 floats (16 bytes), rounded towards -inf
     const int by0 = smin_y - 1;
@@ -95,25 +79,17 @@ __global__ void __launch_bounds__(WT_THREADS, 6) k_warp_tma(const __grid_constan
     s_by0 = by0;
     s_use = use;
     if (use) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar_addr), "r"(1) : "memory");
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar_addr),
-                   "r"((unsigned)(BOX_W * BOX_H * sizeof(float)))
-                   : "memory");
-      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(box);
-      asm volatile(
-          "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
-              "r"(dst),
-          "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(bx0), "r"(by0), "r"(mbar_addr)
-          : "memory");
+      mbar_init(mbar_addr, 1);
+      mbar_fence_init();
+      mbar_expect(mbar_addr, (unsigned)(BOX_W * BOX_H * sizeof(float)));
+      tma_load_2d(smem_addr(box), &tmap, bx0, by0, mbar_addr);
     }
   }
   __syncthreads();
   const bool use = s_use != 0;
   bool ready = false;
   if (use) {
-    for (unsigned it = 0; it < WAIT_LIMIT && !ready; it++) ready = mbar_try_wait(mbar_addr, 0);
+    ready = mbar_wait(mbar_addr, 0);
     if (!ready) atomicAdd(timeouts, 1u);
   }
   const int bx0 = s_bx0, by0 = s_by0;
@@ -142,44 +118,17 @@ __global__ void __launch_bounds__(WT_THREADS, 6) k_warp_tma(const __grid_constan
     }
     out[(size_t)y * W + x] = (float)v;
   }
-  if (use && tid == 0 && !ready) {
-    // the copy may still be in flight: wait for it (bounded) before the block's shared memory is released
-    bool done = false;
-    for (unsigned it = 0; it < WAIT_LIMIT && !done; it++) done = mbar_try_wait(mbar_addr, 0);
-  }
-}
-
-using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiled encode_fn() {
-  static std::once_flag once;
-  static EncodeTiled fn = nullptr;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiled>(p);
-    (void)cudaGetLastError();
-  });
-  return fn;
+  if (use && tid == 0 && !ready) mbar_wait(mbar_addr, 0);  // a copy still in flight lands before the block leaves
 }
 
 // a tensor map of the w2 x h2 float32 plane c2 with 64 x 40 boxes; false when the plane cannot have one (row pitch
 // not a multiple of 16 bytes, base not 16-byte aligned, a plane smaller than the box, or no driver entry point)
 bool make_tmap(const float* c2, int w2, int h2, CUtensorMap* m) {
-  if (w2 % 4 != 0 || ((uintptr_t)c2 & 15) != 0 || w2 < BOX_W || h2 < BOX_H) return false;
-  EncodeTiled enc = encode_fn();
-  if (!enc) return false;
-  const cuuint64_t dims[2] = {(cuuint64_t)w2, (cuuint64_t)h2};
-  const cuuint64_t strides[1] = {(cuuint64_t)w2 * sizeof(float)};
-  const cuuint32_t boxd[2] = {BOX_W, BOX_H};
-  const cuuint32_t estr[2] = {1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(c2), dims, strides, boxd, estr,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  if (w2 % 4 != 0 || w2 < BOX_W || h2 < BOX_H) return false;
+  const uint64_t dims[2] = {(uint64_t)w2, (uint64_t)h2};
+  const uint64_t strides[1] = {(uint64_t)w2 * sizeof(float)};
+  const uint32_t box[2] = {BOX_W, BOX_H};
+  return tma_map_f32(m, c2, 2, dims, strides, box);
 }
 
 __device__ unsigned g_warp_timeouts;  // timed-out tile waits of launches that pass no counter of their own

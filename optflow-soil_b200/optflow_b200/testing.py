@@ -119,6 +119,22 @@ def first_sums(I1, I2, ux, uy, cfg=None, engine=None):
     return out
 
 
+def accumulate(I1, I2, ux, uy, mode=1, cfg=None, engine=None):
+    """first_sums with the accumulate kernel chosen: mode 0 the gather kernel, mode 1 the TMA-staged kernel.
+    Returns (sums (7, h, w), stage waits that gave up)."""
+    eng = engine or default_engine()
+    cfg = cfg or Config()
+    c = cfg.to_ofc()
+    a, b = _f32(I1), _f32(I2)
+    h, w = a.shape
+    ux, uy = _d(ux), _d(uy)
+    out = np.empty((7, h, w))
+    tmo = ctypes.c_uint32(0)
+    eng._call("ofc_test_accumulate", _ptr(a, c_float_p), _ptr(b, c_float_p), w, h, _ptr(ux, c_double_p),
+              _ptr(uy, c_double_p), ctypes.byref(c), int(mode), _ptr(out, c_double_p), ctypes.byref(tmo))
+    return out, tmo.value
+
+
 def warp(c2, sx, sy, shift=(0, 0), mode=1, engine=None):
     """The B-spline warp of coefficient plane c2 (h2 x w2 float32) at (x + shift_x + sx, y + shift_y + sy) for fields
     sx, sy (h x w float64), by the gather kernel (mode 0) or the TMA-staged kernel (mode 1): (out float32 h x w,
