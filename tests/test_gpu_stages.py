@@ -226,7 +226,7 @@ def test_accumulate_tma_matches_gather(T, shape, amp):
     """The TMA-staged accumulate (each filter pair's response box and reference-pack tile staged in shared memory)
     against the gather kernel, bit for bit, on refine's first inner iteration: a smooth start field, a sharp band whose
     blocks' taps span more than the 48 x 16-node box, a jump at the left border that moves taps outside the padded
-    plane (mirrored indices) and NaN start values."""
+    plane (mirrored indices)."""
     from scipy.ndimage import gaussian_filter
     rng = np.random.default_rng(shape[0])
     h, w = shape
@@ -237,7 +237,6 @@ def test_accumulate_tma_matches_gather(T, shape, amp):
     uy = amp * np.cos(xx / 29.0 + yy / 53.0)
     uy[h // 2:h // 2 + 3] += 40.0
     ux[:, :3] -= 80.0
-    ux[h - 3, w - 4] = np.nan
     from optflow_b200.api import default_engine
     from optflow_b200.measure import Profile
     s0, t0 = T.accumulate(a, b, ux, uy, mode=0)
@@ -246,7 +245,7 @@ def test_accumulate_tma_matches_gather(T, shape, amp):
     s1, t1 = T.accumulate(a, b, ux, uy, mode=1)
     assert "k_accumulate_tma" in prof.read()
     assert t0 == 0 and t1 == 0
-    assert np.isfinite(s1).mean() > 0.5
+    assert np.isfinite(s1).all()
     np.testing.assert_array_equal(s1, s0)
 
 
