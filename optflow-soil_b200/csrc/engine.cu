@@ -3273,7 +3273,7 @@ static int first_sums(ofc_engine* e, const float* i1, const float* i2, size_t w,
 
 int ofc_test_first_sums(ofc_engine* e, const float* i1, const float* i2, size_t w, size_t h, const double* ux,
                         const double* uy, const ofc_config* c, double* sums, char* err, size_t errlen) {
-  return first_sums(e, i1, i2, w, h, ux, uy, c, 1, sums, nullptr, err, errlen);
+  return first_sums(e, i1, i2, w, h, ux, uy, c, 0, sums, nullptr, err, errlen);
 }
 
 int ofc_test_accumulate(ofc_engine* e, const float* i1, const float* i2, size_t w, size_t h, const double* ux,

@@ -37,7 +37,7 @@ void launch_accumulate(const float4* ref4, const float2* R, int F, int ph, int p
                        const double* sx, const double* sy, const double2* cs, int W, int H, double* sums,
                        cudaStream_t st);
 // the gather form (fine.cu) and the TMA-staged form (accumulate_tma.cu; mode 0: the gather form; timeouts: a device
-// counter of stage waits that gave up, nullptr for a library-wide one); launch_accumulate takes the staged form
+// counter of stage waits that gave up, nullptr for a library-wide one); launch_accumulate takes the gather form
 void launch_accumulate_gather(const float4* ref4, const float2* R, int F, int ph, int pw, const double* ux,
                               const double* uy, const double* sx, const double* sy, const double2* cs, int W, int H,
                               double* sums, cudaStream_t st);

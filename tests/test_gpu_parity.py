@@ -271,7 +271,7 @@ def test_track_pair_graph_replay_and_device_api():
 
 def test_profile_mode_counts_replayed_kernels():
     """Profile mode (per-kernel device times, the reference's OPTFLOW_GPU_KERNELS) sees every launch of a
-    replayed pair graph: the accumulation (its TMA-staged kernel) runs outer_iters x inner_iters times per pair."""
+    replayed pair graph: the accumulation runs outer_iters x inner_iters times per pair."""
     import ctypes
     from optflow_b200 import Engine
     a, b = _synthetic_pair(192, 13)
@@ -288,8 +288,8 @@ def test_profile_mode_counts_replayed_kernels():
         eng.lib.ofc_set_profile(eng.handle, None)
         got = {names.raw[i * 64:(i + 1) * 64].split(b"\0", 1)[0].decode(): (counts[i], ms[i]) for i in range(n)}
         cfg = Config()
-        assert got["k_accumulate_tma"][0] == 3 * cfg.outer_iters * cfg.inner_iters
-        assert got["k_accumulate_tma"][1] > 0
+        assert got["k_accumulate"][0] == 3 * cfg.outer_iters * cfg.inner_iters
+        assert got["k_accumulate"][1] > 0
     finally:
         eng.close()
 
