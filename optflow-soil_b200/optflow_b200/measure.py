@@ -1,6 +1,6 @@
 """Device timings of the sequence-side components on synthetic inputs (one JSON line per workload).
 
-    PYTHONPATH=optflow-soil_b200 python -m optflow_b200.measure [frames] [tavg] [hybrid] [stream] [pairs] [pipeline]
+    PYTHONPATH=optflow-soil_b200 python -m optflow_b200.measure [frames] [tavg] [hybrid] [stream] [pairs] [pipeline] ...
 
 Every workload is rendered on the GPU (optflow_b200.synth, seeded) and timed after one warm-up run: wall times with
 host perf_counter around the call, device times with the engine's per-kernel CUDA events (ofc_set_profile /
@@ -20,6 +20,8 @@ ofc_profile_read) in a separate run, since the profile mode waits for every repl
           proposal + refine (device time, error against the known field, fallback counters)
   footing[:n]  the footing-in-sand clip (n = 600 frames of 1920 x 1080) through the streamed hybrid driver
   batch64  the 64 uneven pairs of batch.batch_specs (seed 11): track_pairs against one track_pair call each
+  warp    the warp of a 2048^2 plane: the gather kernel against the TMA-staged one
+  accumulate  refine's sums on a 2048^2 pair: the gather accumulate against the TMA-staged one
 """
 import ctypes
 import json
@@ -389,8 +391,71 @@ def batch64(eng, n=64):
             "identical": bool(same)}
 
 
+def _smooth_field(n, amp, seed=1):
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:n, 0:n].astype(np.float64)
+    ph = rng.uniform(0, 2 * np.pi, 2)
+    return (amp * np.sin(xx / 137.0 + ph[0]) * np.cos(yy / 153.0),
+            amp * np.cos(xx / 129.0 + yy / 161.0 + ph[1]))
+
+
+def _kernel_ms(eng, run, reps):
+    """Per-launch device time of every kernel `run` launches, over `reps` calls after one warm-up call."""
+    run()
+    prof = Profile(eng)
+    prof.start()
+    for _ in range(reps):
+        run()
+    return {k: round(t / c, 4) for k, (c, t) in prof.read().items() if c}
+
+
+def warp(eng, reps=20):
+    """The warp of a 2048^2 coefficient plane by a smooth 5 px field: the gather kernel (k_warp, the engine's) against
+    the TMA-staged one (k_warp_tma); per-launch device ms and whether the outputs are equal."""
+    from . import testing
+    n = 2048
+    c2 = np.random.default_rng(1).normal(size=(n, n)).astype(np.float32)
+    sx, sy = _smooth_field(n, 5.0)
+    out = {"workload": "warp: 2048^2 plane, smooth 5 px field", "ms_per_launch": {}}
+    res = {}
+    for mode in (0, 1):
+        res[mode] = testing.warp(c2, sx, sy, mode=mode, engine=eng)
+        ms = _kernel_ms(eng, lambda: testing.warp(c2, sx, sy, mode=mode, engine=eng), reps)
+        out["ms_per_launch"].update({k: v for k, v in ms.items() if k.startswith("k_warp")})
+    out["identical"] = bool(np.array_equal(res[0][0].view(np.uint32), res[1][0].view(np.uint32)))
+    out["timeouts"] = res[1][1]
+    return out
+
+
+def accumulate(eng, reps=5):
+    """refine's first inner-iteration sums of a 2048^2 speckle pair from a smooth 5 px start field: the gather
+    accumulate (k_accumulate, the engine's) against the TMA-staged one (k_accumulate_tma); per-launch device ms, the
+    achieved algorithmic bandwidth and whether the sums are equal."""
+    from . import testing
+    n = 2048
+    pat = synth.make_pattern(n, n, seed=7)
+    a = synth.render(pat, n, n, None, engine=eng).astype(np.float32)
+    b = synth.render(pat, n, n, synth.Field(t=(0.7, -0.4), c=(n / 2, n / 2)), engine=eng).astype(np.float32)
+    ux, uy = _smooth_field(n, 5.0)
+    cfg = Config()
+    F = cfg.n_filters()
+    byts = n * n * (16 * F + 104) + (n + 64) ** 2 * 8 * F
+    out = {"workload": "accumulate: 2048^2 pair, smooth 5 px start field", "ms_per_launch": {}, "GB_s": {}}
+    res = {}
+    for mode in (0, 1):
+        res[mode] = testing.accumulate(a, b, ux, uy, mode=mode, cfg=cfg, engine=eng)
+        ms = _kernel_ms(eng, lambda: testing.accumulate(a, b, ux, uy, mode=mode, cfg=cfg, engine=eng), reps)
+        for k, v in ms.items():
+            if k.startswith("k_accumulate"):
+                out["ms_per_launch"][k] = v
+                out["GB_s"][k] = round(byts / (v * 1e-3) / 1e9, 1)
+    out["identical"] = bool(np.array_equal(res[0][0], res[1][0], equal_nan=True))
+    out["timeouts"] = res[1][1]
+    return out
+
+
 WORKLOADS = {"frames": frames, "tavg": tavg, "hybrid": hybrid, "stream": stream, "pairs": pairs, "pipeline": pipeline,
-             "learned": learned, "footing": footing, "batch64": batch64}
+             "learned": learned, "footing": footing, "batch64": batch64, "warp": warp, "accumulate": accumulate}
 
 
 def main(argv=None):
