@@ -422,7 +422,7 @@ __device__ __forceinline__ void butterfly(In in, Emit emit, TwM tw_m, int RP, bo
     emit(6, csub(e[2], t2));
     emit(3, cadd(e[3], t3));
     emit(7, csub(e[3], t3));
-  } else if constexpr (P == 3 || P == 5 || P == 7 || P == 11 || P == 13) {
+  } else if constexpr (P == 3 || P == 5 || P == 7 || P == 11 || P == 13 || P == 17 || P == 19) {
     odd_butterfly<P, C2>(in, inv, emit);
   } else {
     for (int k = 0; k < RP; k++) {
@@ -485,7 +485,8 @@ __device__ __noinline__ void stage_loop(const C2* __restrict__ A, C2* __restrict
 template <int P, int S, int L, int C, int ISH, int OSH, class C2>
 __device__ __noinline__ void stage_fixed(const C2* __restrict__ A, C2* __restrict__ B, const C2* __restrict__ tw,
                                          bool inv) {
-  constexpr int PB = (P == 2 || P == 3 || P == 4 || P == 5 || P == 7 || P == 8 || P == 11 || P == 13) ? P : 0;
+  constexpr int PB =
+      (P == 2 || P == 3 || P == 4 || P == 5 || P == 7 || P == 8 || P == 11 || P == 13 || P == 17 || P == 19) ? P : 0;
   constexpr int M = L / (P * S), NB = (L / P) * C, ISTEP = S * M * C, OSTEP = S * C, LP = L / P;
   for (int b = threadIdx.x; b < NB; b += blockDim.x) {
     const int l = b % C, bi = b / C;
@@ -563,6 +564,8 @@ __device__ __forceinline__ void fft_stage(const C2* __restrict__ A, C2* __restri
     case 8: stage_loop<8, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
     case 11: stage_loop<11, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
     case 13: stage_loop<13, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
+    case 17: stage_loop<17, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
+    case 19: stage_loop<19, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
     default: stage_loop<0, C2>(A, B, lc, L, P, s, magic, tw, inv, ish, osh); break;
   }
   __syncthreads();
