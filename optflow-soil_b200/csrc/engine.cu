@@ -611,7 +611,7 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
   float* warped = L.get<float>("warped", N);
   float2* R = L.get<float2>("resp", resp_values(F, Np));
   EnergyStats* stats = L.get<EnergyStats>("stats", 1);
-  unsigned long long* hist = L.get<unsigned long long>("hist", MEDIAN_SCRATCH);
+  unsigned long long* hist = L.get<unsigned long long>("hist", median_scratch(N));
   uint8_t* low = L.get<uint8_t>("low", N);
   uint8_t* frozen = L.get<uint8_t>("frozen", N);
   uint8_t* okm = L.get<uint8_t>("okmask", N);
@@ -3107,7 +3107,7 @@ int ofc_test_local_solve(ofc_engine* e, const double* sums, const double* ux, co
     double* sl = L.get<double>("slope", 4 * N);
     double* yp = L.get<double>("yplanes", (size_t)moment_yplanes(c->shape_order) * N);
     EnergyStats* stats = L.get<EnergyStats>("stats", 1);
-    unsigned long long* hist = L.get<unsigned long long>("hist", MEDIAN_SCRATCH);
+    unsigned long long* hist = L.get<unsigned long long>("hist", median_scratch(N));
     OFC_CUDA(cudaMemsetAsync(hist, 0, 4096 * sizeof(unsigned long long), L.stream));
     launch_moments_solve(ds, u2, u2 + N, W, H, c->shape_order, d_mt, rw, mtp, yp, o2, o2 + N, en, rs, sl, L.stream);
     launch_energy_median(en, N, stats, false, hist, L.stream);
@@ -3126,7 +3126,7 @@ int ofc_test_median(ofc_engine* e, const double* v, size_t n, double* median, ch
     if (n == 0) throw Error(OFC_ERR_ARG, "empty");
     double* d = L.upload("t_med", v, n);
     EnergyStats* stats = L.get<EnergyStats>("stats", 1);
-    unsigned long long* hist = L.get<unsigned long long>("hist", MEDIAN_SCRATCH);
+    unsigned long long* hist = L.get<unsigned long long>("hist", median_scratch(n));
     OFC_CUDA(cudaMemsetAsync(hist, 0, 4096 * sizeof(unsigned long long), L.stream));
     launch_energy_median(d, n, stats, true, hist, L.stream);
     EnergyStats hs;

@@ -964,11 +964,12 @@ __device__ double atomic_max_d(double* a, double v) {
 // 1. k_stats_hist0: min / max / NaN (the reset rule, phaseflow.rs:846-854) and the histogram of the top 12 key bits
 //    in one scan; the last block decides whether the median is needed and picks the first digit.
 // 2. k_radix_hist pass 1: the next 12 bits among the elements of that bucket.
-// 3. k_radix_compact: the elements of the 24-bit bucket into a candidate list (at most CAND_CAP), and the largest
+// 3. k_radix_compact: the elements of the 24-bit bucket into a candidate list (room for all n), and the largest
 //    key below the bucket.
 // 4. k_radix_final (one block): the remaining 40 bits over the candidates, and the largest key below the median's.
-// A bucket above CAND_CAP (heavy ties) sets `fallback`: passes 2..5 and k_median_lo then run over all elements.
-constexpr int RBITS = 12, RBINS = 1 << RBITS, RPASSES = 6;
+// Six launches per median whatever the data; a bucket of many equal energies (heavy ties) only makes the one-block
+// final select longer.
+constexpr int RBITS = 12, RBINS = 1 << RBITS;
 constexpr int RH_T = 512;
 
 __global__ void k_stats_init(EnergyStats* s, size_t n) {
@@ -981,7 +982,6 @@ __global__ void k_stats_init(EnergyStats* s, size_t n) {
   s->ticket = 0;
   s->lo_val = 0;
   s->ncand = 0;
-  s->fallback = 0;
   s->below_max = 0;
 }
 
@@ -1107,11 +1107,10 @@ __global__ void __launch_bounds__(RH_T) k_stats_hist0(const double* __restrict__
 }
 
 // One pass over the elements that match the prefix: a block histogram of the digit, added to hist; the last block
-// picks. Passes >= 2 run only on the fallback.
+// picks.
 __global__ void __launch_bounds__(RH_T) k_radix_hist(const double* __restrict__ e, size_t n, EnergyStats* s, int pass,
                                                     unsigned long long* hist) {
   if (!s->need_median || s->nan) return;
-  if (pass >= 2 && !s->fallback) return;
   __shared__ unsigned int h[RBINS];
   __shared__ long long wsum[RH_T / 32];
   __shared__ bool last;
@@ -1154,7 +1153,7 @@ __global__ void k_radix_compact(const double* __restrict__ e, size_t n, EnergySt
       if (lane == __ffs(m) - 1) base = atomicAdd(&s->ncand, (unsigned)__popc(m));
       base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
       const unsigned slot = base + __popc(m & ((1u << lane) - 1));
-      if (in && slot < CAND_CAP) cand[slot] = k;
+      if (in) cand[slot] = k;  // slots < n: at most n elements match
     }
   }
   for (int o = 16; o; o >>= 1) {
@@ -1169,10 +1168,6 @@ __global__ void __launch_bounds__(1024) k_radix_final(EnergyStats* s, const unsi
   if (!s->need_median || s->nan) return;
   const unsigned nc = s->ncand;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  if (nc > (unsigned)CAND_CAP) {
-    if (tid == 0) s->fallback = 1;
-    return;
-  }
   __shared__ unsigned int h[1024];
   __shared__ unsigned int wtot[32];
   __shared__ unsigned long long sh_prefix, wmax[32];
@@ -1236,23 +1231,8 @@ __global__ void __launch_bounds__(1024) k_radix_final(EnergyStats* s, const unsi
   }
 }
 
-// after the passes: prefix = key of the element of rank n/2; for even n the one of rank n/2 - 1 is
-// the same value when `less` (elements below it) < n/2, else the largest element below it (fallback path)
-__global__ void k_median_lo(const double* __restrict__ e, size_t n, EnergyStats* s) {
-  if (!s->need_median || s->nan || !s->fallback || (n % 2) || s->less < (long long)(n / 2)) return;
-  const unsigned long long hk = s->prefix;
-  unsigned long long best = 0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    unsigned long long k = okey(e[i]);
-    if (k < hk && k > best) best = k;
-  }
-  for (int o = 16; o; o >>= 1) {
-    unsigned long long v = __shfl_xor_sync(0xffffffff, best, o);
-    best = v > best ? v : best;
-  }
-  if ((threadIdx.x & 31) == 0 && best) atomicMax((unsigned long long*)&s->lo_val, best);
-}
-
+// after the passes: prefix = key of the element of rank n/2; for even n the one of rank n/2 - 1 is the same value
+// when `less` (elements below it) < n/2, else the largest element below it (lo_val)
 __global__ void k_median_final(EnergyStats* s, size_t n) {
   if (!s->need_median) return;
   if (s->nan) { s->median = nan(""); return; }
@@ -1275,8 +1255,6 @@ void launch_energy_median(const double* energy, size_t n, EnergyStats* stats, bo
   OFC_LAUNCH(k_radix_hist, 296, RH_T, 0, st, energy, n, stats, 1, hist);
   OFC_LAUNCH(k_radix_compact, 296, 256, 0, st, energy, n, stats, cand);
   OFC_LAUNCH(k_radix_final, 1, 1024, 0, st, stats, cand);
-  for (int pass = 2; pass < RPASSES; pass++) OFC_LAUNCH(k_radix_hist, 296, RH_T, 0, st, energy, n, stats, pass, hist);
-  OFC_LAUNCH(k_median_lo, 296, 256, 0, st, energy, n, stats);
   OFC_LAUNCH(k_median_final, 1, 1, 0, st, stats, n);
 }
 

@@ -71,13 +71,12 @@ struct EnergyStats {
   double lo_val;
   unsigned int ticket;  // blocks of the current histogram pass that are done (the last one picks)
   unsigned int ncand;   // elements in the bucket of the first two digits (candidates of the final select)
-  int fallback;         // more than CAND_CAP candidates: the remaining digits take full passes
   unsigned long long below_max;  // the largest key below that bucket
 };
-constexpr int CAND_CAP = 1 << 16;
-constexpr size_t MEDIAN_SCRATCH = 4096 + (size_t)CAND_CAP;  // unsigned long long: the histogram, then the candidates
+// unsigned long long of the median's scratch for n energies: the histogram, then up to n candidates
+inline size_t median_scratch(size_t n) { return 4096 + n; }
 // stats->lo/hi/nan/skip_reset of energy, and its median into stats->median (np.median) when the reset needs it
-// or force_median; scratch: MEDIAN_SCRATCH unsigned long long whose first 4096 are zero (they are left zero)
+// or force_median; scratch: median_scratch(n) unsigned long long whose first 4096 are zero (they are left zero)
 void launch_energy_median(const double* energy, size_t n, EnergyStats* stats, bool force_median,
                           unsigned long long* scratch, cudaStream_t st);
 // reset below 1e-9 median + 1e-30 (phaseflow.py:149-151,158-161)
