@@ -732,8 +732,9 @@ __device__ __forceinline__ int reflect_near(int i, int n) {
 // ---------------------------------------------------------------- kernels
 // Every kernel stages its lines in buffers of fft_buf_len(L, C) values (the transforms' padded layouts); the
 // prefilter's carries live in the buffer the transform left idle. The kernels are instantiated for FIXL = 0 (any
-// supported length, the plan read at run time) and FIXL = FFT_FIXED_L (2112 = 8 8 3 11, the padded length of
-// 2048-wide images, the plan fixed at compile time); the launchers pick by the plan's length.
+// supported length, the plan read at run time), FIXL = -1 (Bluestein) and FIXL = each length of fft_fixed_length (the
+// padded lengths of 256-, 512-, 768-, 1024-, 1536- and 2048-wide images: 320, 576, 832, 1088, 1600, 2112 = 8 8 3 11;
+// the plan fixed at compile time); the launchers pick by the plan's length.
 
 // buffer stride of the kernels that stage several lines: fft_buf_len rounded up to an even count (16-byte aligned)
 __host__ __device__ constexpr int fft_buf_stride(int L, int C) { return (fft_buf_len(L, C) + 1) & ~1; }
@@ -1099,13 +1100,28 @@ static size_t smem_cols_pair(int L, int WL) {
 // k_fft_rows_inv_resp: four line buffers at the even stride
 static size_t smem_rows_resp(int L) { return 4 * (size_t)fft_buf_stride(L, 1) * sizeof(float2); }
 
-// calls f with std::integral_constant<int, FIXL> for the kernels' instantiation of a plan: the fixed length, the
-// runtime direct plan (0) or the runtime Bluestein plan (-1)
+// calls f with std::integral_constant<int, FIXL> for the kernels' instantiation of a plan: a length with a plan fixed
+// at compile time, the runtime direct plan (0) or the runtime Bluestein plan (-1)
 template <class Fn>
 static void by_plan(const FftPlan& pl, Fn f) {
-  if (pl.L == FFT_FIXED_L && !pl.M) f(std::integral_constant<int, FFT_FIXED_L>{});
-  else if (pl.M) f(std::integral_constant<int, -1>{});
-  else f(std::integral_constant<int, 0>{});
+  using std::integral_constant;
+  if (!pl.M) {
+    switch (pl.L) {
+      case 320: f(integral_constant<int, 320>{}); return;
+      case 576: f(integral_constant<int, 576>{}); return;
+      case 832: f(integral_constant<int, 832>{}); return;
+      case 1088: f(integral_constant<int, 1088>{}); return;
+      case 1600: f(integral_constant<int, 1600>{}); return;
+      case FFT_FIXED_L: f(integral_constant<int, FFT_FIXED_L>{}); return;
+      default: break;
+    }
+  }
+  if (pl.M) f(integral_constant<int, -1>{});
+  else f(integral_constant<int, 0>{});
+}
+
+bool fft_fixed_length(int L) {
+  return L == 320 || L == 576 || L == 832 || L == 1088 || L == 1600 || L == FFT_FIXED_L;
 }
 
 // blocks of a persistent launch: as many as are resident at once, at most one per unit of work
@@ -1162,7 +1178,7 @@ static void cols_inverse(const float2* S, const FftPlan& plh, int pw, const Gabo
   int nt = std::min(fft_threads(wh, C), COLS_TMAX);
   const size_t sm_p = smem_cols_pair(ph, wh);
   if (sm_p <= SMEM_MAX) {
-    if (ph == FFT_FIXED_L) nt = pair_threads<REFPACK>(ph);  // the block size the fixed-length kernel assumes
+    if (fft_fixed_length(ph)) nt = pair_threads<REFPACK>(ph);  // the block size the fixed-length kernel assumes
     dim3 grid(div_up(pw, C), REFPACK ? 3 : div_up(g.F, RESP_G));
     by_plan(plh, [&](auto fl) {
       constexpr int FL = decltype(fl)::value;
