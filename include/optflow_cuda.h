@@ -368,8 +368,10 @@ typedef struct ofc_pair_in {
 /*
  * Many independent pairs of any sizes (the CLI's pair runs, or the pairs of a sequence step) in one call: each
  * result equals ofc_track_pair's bit for bit. The pairs run on up to four worker lanes (the environment variable
- * OFC_PAIR_WORKERS sets 1 to 16) of their own streams and buffers, the largest windows first; while one lane's pair computes, the host feeds the others, so small pairs
- * overlap instead of leaving the GPU idle between their launches. outs[i] gets pairs[i]'s results.
+ * OFC_PAIR_WORKERS sets 1 to 16) of their own streams and buffers, the largest windows first, each lane fed by a
+ * host thread of its own (its uploads, launches and copies back run beside the other lanes'; in profile mode one
+ * host thread feeds them in turn), so small pairs overlap instead of leaving the GPU idle between their launches.
+ * outs[i] gets pairs[i]'s results; the call returns when every pair is done.
  */
 OFC_API int ofc_track_pairs(ofc_engine* eng, const ofc_pair_in* pairs, size_t n, const ofc_config* cfg,
                     ofc_pair_out* outs, char* err, size_t errlen);

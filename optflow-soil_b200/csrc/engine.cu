@@ -16,6 +16,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 
 #include "fft.cuh"
@@ -2196,6 +2197,75 @@ int ofc_track_pairs(ofc_engine* e, const ofc_pair_in* pairs, size_t n, const ofc
       L.aux.push_back(std::move(a));
     }
     for (auto& a : L.aux) a->proposal = L.proposal;
+    // one pair on worker lane j: inputs up, the pair, its planes down through page-locked staging into the caller's
+    // buffers
+    auto one_pair = [&](int j, size_t i) {
+      Lane& A = *L.aux[j];
+      const ofc_pair_in& p = pairs[i];
+      const size_t N = p.w * p.h;
+      A.upload("in_i1", p.i1, N);
+      A.upload("in_i2", p.i2, N);
+      if (p.roi) A.upload("in_roi", p.roi, N);
+      if (p.init_ux) {
+        A.upload("in_u", p.init_ux, N);
+        A.upload("in_v", p.init_uy, N);
+      }
+      run_pair(A, (int)p.w, (int)p.h, p.roi != nullptr, p.init_ux != nullptr, *c, true, 3);
+      const ofc_pair_out d = device_pair_out(A, N);
+      float* hout = A.pinned<float>("batch_hout", 10 * N);
+      uint8_t* hvalid = A.pinned<uint8_t>("batch_hvalid", N);
+      OFC_CUDA(cudaMemcpyAsync(hout, d.ux, 10 * N * 4, cudaMemcpyDeviceToHost, A.stream));
+      OFC_CUDA(cudaMemcpyAsync(hvalid, d.valid, N, cudaMemcpyDeviceToHost, A.stream));
+      OFC_CUDA(cudaStreamSynchronize(A.stream));
+      ofc_pair_out o{};
+      float** f[10] = {&o.ux, &o.uy, &o.conf, &o.exx, &o.eyy, &o.exy, &o.gmax, &o.vol, &o.raw_ux, &o.raw_uy};
+      for (int q = 0; q < 10; q++) *f[q] = hout + q * N;
+      o.valid = hvalid;
+      pair_timing(A, o.timing);
+      copy_pair_out(o, &outs[i], N);
+    };
+    // A host thread per worker lane, each taking the next pair (largest first) as soon as its lane is free: the
+    // uploads from the caller's memory and the copies back into it run side by side instead of in turn between the
+    // lanes' pairs. Profile mode (one list of event pairs, filled while a graph is captured) keeps one host thread.
+    if (K > 1 && !g_profiler) {
+      std::atomic<size_t> next{0};
+      std::atomic<bool> stop{false};
+      std::mutex emu;
+      int est = OFC_OK;
+      std::string emsg;
+      std::vector<uint64_t> launched(K, 0);
+      const int dev = e->device;
+      auto work = [&](int j) {
+        g_launch_counter = &launched[j];
+        g_profiler = nullptr;
+        try {
+          OFC_CUDA(cudaSetDevice(dev));
+          for (size_t q = next.fetch_add(1); q < n && !stop.load(); q = next.fetch_add(1)) one_pair(j, order[q]);
+        } catch (const Error& x) {
+          std::lock_guard<std::mutex> lk(emu);
+          if (est == OFC_OK) {
+            est = x.status;
+            emsg = x.what();
+          }
+          stop = true;
+        } catch (const std::exception& x) {
+          std::lock_guard<std::mutex> lk(emu);
+          if (est == OFC_OK) {
+            est = OFC_ERR_DEVICE;
+            emsg = x.what();
+          }
+          stop = true;
+        }
+        g_launch_counter = nullptr;
+      };
+      std::vector<std::thread> threads;
+      for (int j = 0; j < K; j++) threads.emplace_back(work, j);
+      for (auto& t : threads) t.join();
+      if (g_launch_counter)
+        for (uint64_t v : launched) *g_launch_counter += v;
+      if (est != OFC_OK) throw Error(est, emsg);
+      return;
+    }
     std::vector<long long> busy(K, -1);
     // a worker's finished pair: its planes from page-locked staging into the caller's buffers
     auto drain = [&](int j) {
