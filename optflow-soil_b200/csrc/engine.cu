@@ -2224,11 +2224,12 @@ int ofc_track_pairs(ofc_engine* e, const ofc_pair_in* pairs, size_t n, const ofc
       pair_timing(A, o.timing);
       copy_pair_out(o, &outs[i], N);
     };
-    // A host thread per worker lane, each taking the next pair (largest first) as soon as its lane is free: the
-    // uploads from the caller's memory and the copies back into it run side by side instead of in turn between the
-    // lanes' pairs. Profile mode (one list of event pairs, filled while a graph is captured) keeps one host thread.
+    // A host thread per worker lane, lane j taking pairs j, j + K, j + 2K, ... of the size order (the assignment of
+    // the one-thread form, so a lane meets the same sizes, and replays the same graphs, on every call with the same
+    // pairs): the uploads from the caller's memory and the copies back into it run side by side instead of in turn
+    // between the lanes' pairs. Profile mode (one list of event pairs, filled while a graph is captured) keeps one
+    // host thread.
     if (K > 1 && !g_profiler) {
-      std::atomic<size_t> next{0};
       std::atomic<bool> stop{false};
       std::mutex emu;
       int est = OFC_OK;
@@ -2240,7 +2241,7 @@ int ofc_track_pairs(ofc_engine* e, const ofc_pair_in* pairs, size_t n, const ofc
         g_profiler = nullptr;
         try {
           OFC_CUDA(cudaSetDevice(dev));
-          for (size_t q = next.fetch_add(1); q < n && !stop.load(); q = next.fetch_add(1)) one_pair(j, order[q]);
+          for (size_t q = (size_t)j; q < n && !stop.load(); q += (size_t)K) one_pair(j, order[q]);
         } catch (const Error& x) {
           std::lock_guard<std::mutex> lk(emu);
           if (est == OFC_OK) {
