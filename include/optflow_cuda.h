@@ -367,7 +367,7 @@ typedef struct ofc_pair_in {
 
 /*
  * Many independent pairs of any sizes (the CLI's pair runs, or the pairs of a sequence step) in one call: each
- * result equals ofc_track_pair's bit for bit. The pairs run on up to four worker lanes (the environment variable
+ * result equals ofc_track_pair's bit for bit. The pairs run on up to eight worker lanes (the environment variable
  * OFC_PAIR_WORKERS sets 1 to 16) of their own streams and buffers, the largest windows first, each lane fed by a
  * host thread of its own (its uploads, launches and copies back run beside the other lanes'; in profile mode one
  * host thread feeds them in turn), so small pairs overlap instead of leaving the GPU idle between their launches.
