@@ -45,17 +45,50 @@ static int stage_count(int m) {
   return n;
 }
 
+// The cost of a Bluestein inner length M: M times its Stockham stages of the radices with a butterfly of their own (8,
+// 4, 2 and the odd primes up to 19), a stage of radix 11 or 13 counted 1.2 and of 17 or 19 1.5 (their butterflies take
+// more registers); infinite for other factors. The transforms are bound by their stage barriers, not by arithmetic:
+// 604 = 4 151 (the padded height of 540-row frames) takes M = 1216 = 8 8 19 (3 stages) instead of the smallest
+// 2^a 3^b 5^c 7^d, 1215 = 3^5 5 (6 stages).
+static double bluestein_cost(int M) {
+  double c = 0;
+  int m = M;
+  while (m % 8 == 0) { c += 1; m /= 8; }
+  while (m % 4 == 0) { c += 1; m /= 4; }
+  while (m % 2 == 0) { c += 1; m /= 2; }
+  for (int p : {3, 5, 7, 11, 13, 17, 19}) {
+    const double w = p <= 7 ? 1.0 : (p <= 13 ? 1.2 : 1.5);
+    while (m % p == 0) { c += w; m /= p; }
+  }
+  return m == 1 ? c * M : 1e30;
+}
+
 int fft_work_length(int L) {
   if (L < 1) return 0;
   if (fft_supported(L)) return stage_count(L) <= FFT_MAXST ? L : 0;
-  // Bluestein: the smallest 2^a 3^b 5^c 7^d >= 2L - 1
-  for (int M = 2 * L - 1; M <= 8 * L; M++) {
+  // Bluestein: among the lengths M in [2L - 1, 1.25 (2L - 1)] the one of least stage cost (the smallest on ties),
+  // never above the smallest 2^a 3^b 5^c 7^d where that one fits the passes' shared memory and a larger one might not
+  // (about 6800: four line buffers of the row pass, two two-column buffers of the column pass)
+  const int lo = 2 * L - 1;
+  int smooth = 0;
+  for (int M = lo; M <= 8 * L && !smooth; M++) {
     int m = M;
     for (int p : {2, 3, 5, 7})
       while (m % p == 0) m /= p;
-    if (m == 1) return stage_count(M) <= FFT_MAXST ? M : 0;
+    if (m == 1) smooth = M;
   }
-  return 0;
+  constexpr int FIT = 6800;
+  const int hi = (smooth && smooth <= FIT) ? std::min(lo + lo / 4, std::max(smooth, FIT)) : lo + lo / 4;
+  int best = 0;
+  double bc = 1e29;  // below the cost of a length with an unsupported factor
+  for (int M = lo; M <= hi; M++) {
+    const double c = bluestein_cost(M);
+    if (c < bc) {
+      bc = c;
+      best = M;
+    }
+  }
+  return best && stage_count(best) <= FFT_MAXST ? best : 0;
 }
 
 std::vector<float2> fft_bluestein_tables(int L, int M) {

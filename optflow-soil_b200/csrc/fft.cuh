@@ -18,8 +18,8 @@ constexpr int FFT_TMAX = 512;  // threads per block at most
 // A 1-D plan of length L: mixed-radix Stockham stages (radix p[i], stride s[i] = product of the radices
 // before it) and the twiddle table W[t] = exp(-2 pi i t / L), t < L, rounded from float64.
 // A length with a prime factor above 31 is transformed by Bluestein's chirp z-transform (as the reference's Metal
-// FFT does, rust/crates/optflow-gpu/src/fft.rs:1-3): M > 0 is then the inner length (the smallest 2^a 3^b 5^c 7^d
-// >= 2L - 1), the stages and tw are those of length M, chirp[n] = exp(-i pi n^2 / L) for n < L, and filt is the
+// FFT does, rust/crates/optflow-gpu/src/fft.rs:1-3): M > 0 is then the inner length (a length >= 2L - 1 of
+// the radices with butterflies, of fewest stages: fft_work_length), the stages and tw are those of length M, chirp[n] = exp(-i pi n^2 / L) for n < L, and filt is the
 // length-M transform of the conjugate chirp (wrapped: index m and M - m for m < L) times 1 / M.
 struct FftPlan {
   int L = 0;
