@@ -1265,15 +1265,19 @@ __global__ void k_reportable(const float* __restrict__ rx, const float* __restri
   const double own = (double)min(min(x, y), min(W - 1 - x, H - 1 - y));
   rep[i] = (own >= B && tx >= B && ty >= B && (W - 1) - tx >= B && (H - 1) - ty >= B) ? 1.f : 0.f;
 }
-__global__ void k_mean_conf_rows(const float* __restrict__ conf, const float* __restrict__ rep,
-                                 const float* __restrict__ ux, const float* __restrict__ uy,
-                                 const uint8_t* __restrict__ mask, int W, int H, double* __restrict__ rsum,
-                                 long long* __restrict__ rcnt) {
-  const int y = blockIdx.x * blockDim.x + threadIdx.x;
-  if (y >= H) return;
+// one block of MC_T threads per row: each thread sums the pixels x = tid, tid + MC_T, ..., then a fixed-order tree
+// (warp shuffles, then the warps in order) gives the row's sum and count, the same on every run
+constexpr int MC_T = 128;
+__global__ void __launch_bounds__(MC_T) k_mean_conf_rows(const float* __restrict__ conf, const float* __restrict__ rep,
+                                                         const float* __restrict__ ux, const float* __restrict__ uy,
+                                                         const uint8_t* __restrict__ mask, int W, int H,
+                                                         double* __restrict__ rsum, long long* __restrict__ rcnt) {
+  __shared__ double wsum[MC_T / 32];
+  __shared__ long long wcnt[MC_T / 32];
+  const int y = blockIdx.x;
   double sum = 0.0;
   long long n = 0;
-  for (int x = 0; x < W; x++) {
+  for (int x = threadIdx.x; x < W; x += MC_T) {
     const size_t i = (size_t)y * W + x;
     const double px = x + (double)ux[i], py = y + (double)uy[i];
     const double c = bilinear64(conf, W, H, px, py);
@@ -1282,8 +1286,26 @@ __global__ void k_mean_conf_rows(const float* __restrict__ conf, const float* __
       n++;
     }
   }
-  rsum[y] = sum;
-  rcnt[y] = n;
+  for (int o = 16; o; o >>= 1) {
+    sum += __shfl_down_sync(0xffffffffu, sum, o);
+    n += __shfl_down_sync(0xffffffffu, n, o);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    wsum[wid] = sum;
+    wcnt[wid] = n;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    long long c = 0;
+    for (int k = 0; k < MC_T / 32; k++) {
+      s += wsum[k];
+      c += wcnt[k];
+    }
+    rsum[y] = s;
+    rcnt[y] = c;
+  }
 }
 __global__ void k_mean_conf_fold(const double* __restrict__ rsum, const long long* __restrict__ rcnt, int H,
                                  double* out) {
@@ -2567,7 +2589,7 @@ int64_t run_sequence(Lane& L, const SeqIO& io) {
   };
   auto leg_mean = [&]() {
     OFC_LAUNCH(k_reportable, g2, 128, 0, st, d.raw_ux, d.raw_uy, W, H, B, rep);
-    OFC_LAUNCH(k_mean_conf_rows, div_up(H, 128), 128, 0, st, d.conf, rep, u0r, u0r + N, droi, W, H, rsum, rcnt);
+    OFC_LAUNCH(k_mean_conf_rows, H, MC_T, 0, st, d.conf, rep, u0r, u0r + N, droi, W, H, rsum, rcnt);
     OFC_LAUNCH(k_mean_conf_fold, 1, 1, 0, st, rsum, rcnt, H, dmean);
     double m = 0;
     OFC_CUDA(cudaMemcpyAsync(&m, dmean, 8, cudaMemcpyDeviceToHost, st));
