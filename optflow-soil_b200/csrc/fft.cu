@@ -628,11 +628,16 @@ __device__ C2* fft_stages(C2* a, C2* b, const FftPlan& pl, int SL, bool inv) {
 
 // Bluestein (the plan's M > 0): X_k = w_k sum_n (x_n w_n) conj(w_{k - n}), w_n = exp(-i pi n^2 / L), the convolution
 // cyclic over M >= 2L - 1 by two length-M transforms; the inverse transform as conj(forward(conj(x))). buf and tmp
-// hold fft_buf_len(M, C) values each.
-template <int C, class C2>
+// hold fft_buf_len(M, C) values each. FM > 0: the inner length is FM, its two transforms on the plan fixed at compile
+// time (L still read at run time).
+template <int C, class C2, int FM = 0>
 __device__ __forceinline__ C2* fft_bluestein(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
   constexpr int lc = C == 4 ? 2 : (C == 2 ? 1 : 0);
-  const int L = pl.L, M = pl.M;
+  const int L = pl.L, M = FM > 0 ? FM : pl.M;
+  auto inner = [&](C2* a, C2* b, bool iv) {
+    if constexpr (FM > 0) return fft_run_fixed<FM, C, 0, C2>(a, b, (const C2*)pl.tw, iv);
+    else return fft_stages<C, C2>(a, b, pl, M, iv);
+  };
   const float2* w = pl.chirp;
   const float2* f = pl.filt;
   for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) {
@@ -646,10 +651,10 @@ __device__ __forceinline__ C2* fft_bluestein(C2* buf, C2* tmp, const FftPlan& pl
     buf[idx] = v;
   }
   __syncthreads();
-  C2* r = fft_stages<C, C2>(buf, tmp, pl, M, false);
+  C2* r = inner(buf, tmp, false);
   for (int idx = threadIdx.x; idx < M * C; idx += blockDim.x) r[idx] = cmul(r[idx], __ldg(f + (idx >> lc)));
   __syncthreads();
-  C2* q = fft_stages<C, C2>(r, r == buf ? tmp : buf, pl, M, true);
+  C2* q = inner(r, r == buf ? tmp : buf, true);
   for (int idx = threadIdx.x; idx < L * C; idx += blockDim.x) {
     float2 v = cmul(q[idx], __ldg(w + (idx >> lc)));
     if (inv) v.y = -v.y;
@@ -665,8 +670,10 @@ __device__ C2* fft_run(C2* buf, C2* tmp, const FftPlan& pl, bool inv) {
   static_assert(std::is_same<C2, float2>::value, "float32 transforms");
   if constexpr (FIXL > 0) {
     return fft_run_fixed<FIXL, C, 0, C2>(buf, tmp, (const C2*)pl.tw, inv);
-  } else if constexpr (FIXL < 0) {  // the kernels' instantiation for Bluestein plans (pl.M > 0)
+  } else if constexpr (FIXL == -1) {  // the kernels' instantiation for Bluestein plans (pl.M > 0)
     return fft_bluestein<C, C2>(buf, tmp, pl, inv);
+  } else if constexpr (FIXL < -1) {  // Bluestein with the inner length -FIXL fixed at compile time
+    return fft_bluestein<C, C2, -FIXL>(buf, tmp, pl, inv);
   } else {
     return fft_stages<C, C2>(buf, tmp, pl, pl.L, inv);
   }
@@ -1134,7 +1141,8 @@ static size_t smem_cols_pair(int L, int WL) {
 static size_t smem_rows_resp(int L) { return 4 * (size_t)fft_buf_stride(L, 1) * sizeof(float2); }
 
 // calls f with std::integral_constant<int, FIXL> for the kernels' instantiation of a plan: a length with a plan fixed
-// at compile time, the runtime direct plan (0) or the runtime Bluestein plan (-1)
+// at compile time, a Bluestein plan whose inner length -FIXL has one (FIXL < -1), the runtime direct plan (0) or the
+// runtime Bluestein plan (-1)
 template <class Fn>
 static void by_plan(const FftPlan& pl, Fn f) {
   using std::integral_constant;
@@ -1148,6 +1156,11 @@ static void by_plan(const FftPlan& pl, Fn f) {
       case FFT_FIXED_L: f(integral_constant<int, FFT_FIXED_L>{}); return;
       default: break;
     }
+  }
+  // the Bluestein inner length of 604 = 4 151 (the padded height of 540-row frames: the CLI's 1080p video at scale 2)
+  if (pl.M == FFT_FIXED_M) {
+    f(integral_constant<int, -FFT_FIXED_M>{});
+    return;
   }
   if (pl.M) f(integral_constant<int, -1>{});
   else f(integral_constant<int, 0>{});

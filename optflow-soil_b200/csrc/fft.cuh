@@ -12,6 +12,9 @@ constexpr int FFT_FIXED_L = 2112;
 // table's variants apply to the other lengths): the padded lengths (side + 64) of sides 256, 512, 768, 1024, 1536
 // and 2048
 bool fft_fixed_length(int L);
+// the Bluestein inner length whose two transforms run on a plan fixed at compile time: that of 604 = 4 151 (the
+// padded height of 540-row frames), 1216 = 8 8 19
+constexpr int FFT_FIXED_M = 1216;
 constexpr int FFT_E = 8;       // complex values per thread (sets the threads of a block)
 constexpr int FFT_TMAX = 512;  // threads per block at most
 
