@@ -773,8 +773,9 @@ __device__ __forceinline__ int reflect_near(int i, int n) {
 // Every kernel stages its lines in buffers of fft_buf_len(L, C) values (the transforms' padded layouts); the
 // prefilter's carries live in the buffer the transform left idle. The kernels are instantiated for FIXL = 0 (any
 // supported length, the plan read at run time), FIXL = -1 (Bluestein) and FIXL = each length of fft_fixed_length (the
-// padded lengths of 256-, 512-, 768-, 1024-, 1536- and 2048-wide images: 320, 576, 832, 1088, 1600, 2112 = 8 8 3 11;
-// the plan fixed at compile time); the launchers pick by the plan's length.
+// padded lengths of 256-, 512-, 768-, 960-, 1024-, 1536- and 2048-wide images: 320, 576, 832, 1024, 1088, 1600,
+// 2112 = 8 8 3 11; the plan fixed at compile time), and FIXL = -FFT_FIXED_M (Bluestein with that inner length fixed);
+// the launchers pick by the plan.
 
 // buffer stride of the kernels that stage several lines: fft_buf_len rounded up to an even count (16-byte aligned)
 __host__ __device__ constexpr int fft_buf_stride(int L, int C) { return (fft_buf_len(L, C) + 1) & ~1; }
@@ -1151,6 +1152,7 @@ static void by_plan(const FftPlan& pl, Fn f) {
       case 320: f(integral_constant<int, 320>{}); return;
       case 576: f(integral_constant<int, 576>{}); return;
       case 832: f(integral_constant<int, 832>{}); return;
+      case 1024: f(integral_constant<int, 1024>{}); return;
       case 1088: f(integral_constant<int, 1088>{}); return;
       case 1600: f(integral_constant<int, 1600>{}); return;
       case FFT_FIXED_L: f(integral_constant<int, FFT_FIXED_L>{}); return;
@@ -1167,7 +1169,7 @@ static void by_plan(const FftPlan& pl, Fn f) {
 }
 
 bool fft_fixed_length(int L) {
-  return L == 320 || L == 576 || L == 832 || L == 1088 || L == 1600 || L == FFT_FIXED_L;
+  return L == 320 || L == 576 || L == 832 || L == 1024 || L == 1088 || L == 1600 || L == FFT_FIXED_L;
 }
 
 // blocks of a persistent launch: as many as are resident at once, at most one per unit of work

@@ -9,8 +9,8 @@ constexpr int FFT_MAXST = 16;
 // the padded length of 2048-wide images, whose transforms run on a plan fixed at compile time
 constexpr int FFT_FIXED_L = 2112;
 // the lengths whose transforms run on plans fixed at compile time (their factor order is the default one: the plan
-// table's variants apply to the other lengths): the padded lengths (side + 64) of sides 256, 512, 768, 1024, 1536
-// and 2048
+// table's variants apply to the other lengths): the padded lengths (side + 64) of sides 256, 512, 768, 960, 1024,
+// 1536 and 2048
 bool fft_fixed_length(int L);
 // the Bluestein inner length whose two transforms run on a plan fixed at compile time: that of 604 = 4 151 (the
 // padded height of 540-row frames), 1216 = 8 8 19
