@@ -749,59 +749,62 @@ __global__ void __launch_bounds__(128, 4) k_moments_y_rb(const double* __restric
   }
 }
 
-// x pass + solve: a block of NT threads owns a row segment of SEG = NT RX pixels. For each y-plane it stages
-// the segment and its 2r halo in shared memory (double-buffered, the next plane's loads in flight meanwhile); a
-// thread takes the RX + 2r values around its RX consecutive pixels into registers (an odd RX keeps the warp's
-// reads on distinct banks) and writes their moments into a shared tile of nm x SEG (tap loop outermost, RX x
-// powers accumulators side by side); then each thread solves the pixels tid + NT i from the tile.
+// x pass + solve: a block owns a row segment of SEG = GT RX pixels and has two groups of GT threads. The groups
+// take the y-planes in pairs, group g plane Q + g of each pair: a group stages its plane's segment and 2r halo in
+// shared memory (double-buffered per group, its next plane's loads in flight meanwhile); a thread takes the RX + 2r
+// values around its RX consecutive pixels into registers (an odd RX keeps the warp's reads on distinct banks) and
+// writes their moments into a shared tile of nm x SEG (tap loop outermost, RX x powers accumulators side by side).
+// Then every thread of the block solves the pixels tid, tid + 2 GT, ... from the tile. Two groups give twice the warps
+// per SM of one group of GT threads at the same tile (the tile, 8 nm bytes per pixel, bounds the blocks per SM), and
+// each moment is formed by the same operations in the same order either way. Order 1 runs 4 blocks per SM (110
+// registers); order 2 runs 2 (its 12 x 12 solve in registers takes 218).
 template <int ORDER>
 struct MomX {
   static constexpr int RX = ORDER == 1 ? 3 : 1;
-  static constexpr int NT = 64, SEG = NT * RX, WIN = SEG + 2 * MOM_R;
-  static constexpr size_t smem() { return (size_t)(2 * WIN + build_table(ORDER).nm * SEG) * sizeof(double); }
+  static constexpr int GT = 64, NT = 2 * GT, SEG = GT * RX, WIN = SEG + 2 * MOM_R;
+  static constexpr size_t smem() { return (size_t)(4 * WIN + build_table(ORDER).nm * SEG) * sizeof(double); }
 };
 
-// the NPF values of a row segment (with its halo) that thread tid stages: i = tid + NT j
+// the NPF values of a row segment (with its halo) that thread lt of a group stages: i = lt + GT j
 template <int ORDER>
 struct MomPf {
-  static constexpr int NPF = (MomX<ORDER>::WIN + MomX<ORDER>::NT - 1) / MomX<ORDER>::NT;
+  static constexpr int NPF = (MomX<ORDER>::WIN + MomX<ORDER>::GT - 1) / MomX<ORDER>::GT;
   double v[NPF];
 };
 
 template <int ORDER>
-__device__ __forceinline__ void mom_x_fetch(const double* __restrict__ row, int x0, int W, MomPf<ORDER>& pf) {
-  constexpr int R = MOM_R, NT = MomX<ORDER>::NT, WIN = MomX<ORDER>::WIN;
+__device__ __forceinline__ void mom_x_fetch(const double* __restrict__ row, int x0, int W, int lt, MomPf<ORDER>& pf) {
+  constexpr int R = MOM_R, GT = MomX<ORDER>::GT, WIN = MomX<ORDER>::WIN;
 #pragma unroll
   for (int j = 0; j < MomPf<ORDER>::NPF; j++) {
-    const int i = threadIdx.x + NT * j;
+    const int i = lt + GT * j;
     if (i < WIN) pf.v[j] = row[min(max(x0 - R + i, 0), W - 1)];
   }
 }
 
 template <int ORDER>
-__device__ __forceinline__ void mom_x_stage(double* wb, const MomPf<ORDER>& pf) {
-  constexpr int NT = MomX<ORDER>::NT, WIN = MomX<ORDER>::WIN;
+__device__ __forceinline__ void mom_x_stage(double* wb, int lt, const MomPf<ORDER>& pf) {
+  constexpr int GT = MomX<ORDER>::GT, WIN = MomX<ORDER>::WIN;
 #pragma unroll
   for (int j = 0; j < MomPf<ORDER>::NPF; j++) {
-    const int i = threadIdx.x + NT * j;
+    const int i = lt + GT * j;
     if (i < WIN) wb[i] = pf.v[j];
   }
 }
 
-// plane Q: its segment is in shared buffer Q & 1; while it is processed, the loads of plane Q + 1 are in flight
-// (registers pf), which are then staged into the other buffer. The barrier at the end orders both buffers.
+// plane Q by one group: its segment is in the group's buffer `wb`; the loads of the group's next plane (Q + 2) are put
+// in flight first (registers pf) and staged into `wnext` at the end
 template <int ORDER, int Q>
-__device__ __forceinline__ void mom_x_planes(const double* __restrict__ yplanes, size_t N, int y, int x0, int W,
-                                             double* smd, double* mom, const MomTaps& tp, MomPf<ORDER>& pf) {
+__device__ __forceinline__ void mom_x_plane(const double* __restrict__ yplanes, size_t N, int y, int x0, int W, int lt,
+                                            const double* wb, double* wnext, double* mom, const MomTaps& tp,
+                                            MomPf<ORDER>& pf) {
   constexpr MomTable T = build_table(ORDER);
   if constexpr (Q < T.ny) {
-    constexpr int R = MOM_R, RX = MomX<ORDER>::RX, SEG = MomX<ORDER>::SEG, WIN = MomX<ORDER>::WIN, NV = RX + 2 * R;
-    const int tid = threadIdx.x;
-    if constexpr (Q + 1 < T.ny) mom_x_fetch<ORDER>(yplanes + (size_t)(Q + 1) * N + (size_t)y * W, x0, W, pf);
-    const double* wb = smd + (Q & 1) * WIN;
+    constexpr int R = MOM_R, RX = MomX<ORDER>::RX, SEG = MomX<ORDER>::SEG, NV = RX + 2 * R;
+    if constexpr (Q + 2 < T.ny) mom_x_fetch<ORDER>(yplanes + (size_t)(Q + 2) * N + (size_t)y * W, x0, W, lt, pf);
     double v[NV];
 #pragma unroll
-    for (int i = 0; i < NV; i++) v[i] = wb[tid * RX + i];
+    for (int i = 0; i < NV; i++) v[i] = wb[lt * RX + i];
     int mi[5] = {-1, -1, -1, -1, -1};  // moment index of (Q, px)
 #pragma unroll
     for (int m = 0; m < T.nm; m++)
@@ -824,15 +827,30 @@ __device__ __forceinline__ void mom_x_planes(const double* __restrict__ yplanes,
     for (int p = 0; p < 5; p++)
       if (mi[p] >= 0)
 #pragma unroll
-        for (int i = 0; i < RX; i++) mom[mi[p] * SEG + tid * RX + i] = acc[i][p];
-    if constexpr (Q + 1 < T.ny) mom_x_stage<ORDER>(smd + ((Q + 1) & 1) * WIN, pf);
+        for (int i = 0; i < RX; i++) mom[mi[p] * SEG + lt * RX + i] = acc[i][p];
+    if constexpr (Q + 2 < T.ny) mom_x_stage<ORDER>(wnext, lt, pf);
+  }
+}
+
+// the plane pair (K, K + 1): group g takes plane K + g from its buffer (K / 2) & 1; then a block barrier
+template <int ORDER, int K>
+__device__ __forceinline__ void mom_x_pairs(const double* __restrict__ yplanes, size_t N, int y, int x0, int W, int g,
+                                            int lt, double* smd, double* mom, const MomTaps& tp, MomPf<ORDER>& pf) {
+  constexpr MomTable T = build_table(ORDER);
+  if constexpr (K < T.ny) {
+    constexpr int WIN = MomX<ORDER>::WIN;
+    double* gb = smd + 2 * WIN * g;  // the group's two buffers
+    const double* wb = gb + ((K / 2) & 1) * WIN;
+    double* wnext = gb + (((K / 2) + 1) & 1) * WIN;
+    if (g == 0) mom_x_plane<ORDER, K>(yplanes, N, y, x0, W, lt, wb, wnext, mom, tp, pf);
+    else mom_x_plane<ORDER, K + 1>(yplanes, N, y, x0, W, lt, wb, wnext, mom, tp, pf);
     __syncthreads();
-    mom_x_planes<ORDER, Q + 1>(yplanes, N, y, x0, W, smd, mom, tp, pf);
+    mom_x_pairs<ORDER, K + 2>(yplanes, N, y, x0, W, g, lt, smd, mom, tp, pf);
   }
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(MomX<ORDER>::NT, 4) k_moments_x_solve_rb(const double* __restrict__ yplanes,
+__global__ void __launch_bounds__(MomX<ORDER>::NT, ORDER == 1 ? 4 : 2) k_moments_x_solve_rb(const double* __restrict__ yplanes,
                                                                const double* __restrict__ uxin,
                                                                const double* __restrict__ uyin, int W, int H,
                                                                MomTaps tp, double* __restrict__ oux,
@@ -840,19 +858,21 @@ __global__ void __launch_bounds__(MomX<ORDER>::NT, 4) k_moments_x_solve_rb(const
                                                                double* __restrict__ resid, double* __restrict__ slope) {
   constexpr MomTable T = build_table(ORDER);
   constexpr int n = ORDER == 1 ? 6 : 12;
-  constexpr int RX = MomX<ORDER>::RX, NT = MomX<ORDER>::NT, SEG = MomX<ORDER>::SEG, WIN = MomX<ORDER>::WIN;
+  constexpr int GT = MomX<ORDER>::GT, NT = MomX<ORDER>::NT, SEG = MomX<ORDER>::SEG, WIN = MomX<ORDER>::WIN;
   extern __shared__ double smd[];
-  double* mom = smd + 2 * WIN;
-  const int tid = threadIdx.x, y = blockIdx.y, x0 = blockIdx.x * SEG;
+  double* mom = smd + 4 * WIN;
+  const int tid = threadIdx.x, g = tid / GT, lt = tid - g * GT, y = blockIdx.y, x0 = blockIdx.x * SEG;
   const size_t N = (size_t)W * H;
   MomPf<ORDER> pf;
-  mom_x_fetch<ORDER>(yplanes + (size_t)y * W, x0, W, pf);
-  mom_x_stage<ORDER>(smd, pf);
+  if (g < T.ny) {  // group g's first plane into its buffer 0
+    mom_x_fetch<ORDER>(yplanes + (size_t)g * N + (size_t)y * W, x0, W, lt, pf);
+    mom_x_stage<ORDER>(smd + 2 * WIN * g, lt, pf);
+  }
   __syncthreads();
-  mom_x_planes<ORDER, 0>(yplanes, N, y, x0, W, smd, mom, tp, pf);
+  mom_x_pairs<ORDER, 0>(yplanes, N, y, x0, W, g, lt, smd, mom, tp, pf);
 #pragma unroll 1
-  for (int i = 0; i < RX; i++) {
-    const int s = tid + NT * i, x = x0 + s;
+  for (int s = tid; s < SEG; s += NT) {
+    const int x = x0 + s;
     if (x >= W) continue;
     double m[T.nm];
 #pragma unroll
