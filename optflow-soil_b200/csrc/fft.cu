@@ -704,10 +704,9 @@ __device__ __forceinline__ float zpow(int e) {
 // with x recovered locally as x[i] = c_per[i-1] + 4 c_per[i] + c_per[i+1] (circular) and the sums cut at
 // z^32 < 1e-18 (lines here are at least 65 long, so the terms of the two ends never meet). scratch: 2 C float4.
 template <int C>
-__device__ void bspline_edges(float2* buf, int n, float4* scratch) {
+__device__ void bspline_edge_consts(float2* buf, int n, float4* scratch) {
   const float z = (float)BZ1;
   const float g = (float)(BZ1 / (BZ2 - 1.0));
-  const float q = (float)(1.0 / (1.0 - BZ2));
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   auto c = [&](int i, int l) { return buf[(i < 0 ? i + n : (i >= n ? i - n : i)) * C + l]; };
   auto xr = [&](int i, int l) {
@@ -742,21 +741,31 @@ __device__ void bspline_edges(float2* buf, int n, float4* scratch) {
     }
   }
   __syncthreads();
-  for (int t = tid; t < 64 * C; t += blockDim.x) {
+}
+
+// value v of row j of a line of length n with the edge terms of its constants k added (the first and last 32 rows)
+__device__ __forceinline__ float2 bspline_edge_fix(float2 v, int j, int n, float4 k) {
+  const float q = (float)(1.0 / (1.0 - BZ2));
+  if (j < 32) {
+    const float zp = zpow(j + 1);  // z^(i+1), i = j
+    v.x = fmaf(-k.x * q, zp, v.x);
+    v.y = fmaf(-k.y * q, zp, v.y);
+  } else if (j >= n - 32) {
+    const float zp = zpow(n - 1 - j);
+    v.x = fmaf(k.z, zp, v.x);
+    v.y = fmaf(k.w, zp, v.y);
+  }
+  return v;
+}
+
+// the edge constants (bspline_edge_consts) and their terms applied in place
+template <int C>
+__device__ void bspline_edges(float2* buf, int n, float4* scratch) {
+  bspline_edge_consts<C>(buf, n, scratch);
+  for (int t = threadIdx.x; t < 64 * C; t += blockDim.x) {
     const int l = t % C, j = t / C;  // j < 32: the start of the line; j >= 32: its end
-    const float4 k = scratch[l];
-    if (j < 32) {
-      const float zp = zpow(j + 1);  // z^(i+1), i = j
-      float2& v = buf[j * C + l];
-      v.x = fmaf(-k.x * q, zp, v.x);
-      v.y = fmaf(-k.y * q, zp, v.y);
-    } else {
-      const int i = n - 64 + j;  // j = 32..63 -> i = n-32..n-1
-      const float zp = zpow(n - 1 - i);
-      float2& v = buf[i * C + l];
-      v.x = fmaf(k.z, zp, v.x);
-      v.y = fmaf(k.w, zp, v.y);
-    }
+    const int i = j < 32 ? j : n - 64 + j;
+    buf[i * C + l] = bspline_edge_fix(buf[i * C + l], i, n, scratch[l]);
   }
   __syncthreads();
 }
@@ -907,6 +916,21 @@ __global__ void __launch_bounds__(pair_threads<REFPACK>(FIXL), 2) k_fft_cols_pai
         if (x0 + (i & 1) < pw) dst[(size_t)(i >> 1) * pw + (i & 1)] = r[i];
     }
   };
+  // the same with the prefilter's edge terms along y (constants kc of the two columns) added as the rows are stored
+  auto store_edges = [&](const float2* r, const float4* kc, int plane) {
+    float2* dst = U + (size_t)plane * ph * pw + x0;
+    if (rows16) {
+      for (int y = tid; y < ph; y += nt) {
+        const float4 v = *(const float4*)(r + 2 * y);
+        const float2 a = bspline_edge_fix(make_float2(v.x, v.y), y, ph, kc[0]);
+        const float2 b = bspline_edge_fix(make_float2(v.z, v.w), y, ph, kc[1]);
+        *(float4*)(dst + (size_t)y * pw) = make_float4(a.x, a.y, b.x, b.y);
+      }
+    } else {
+      for (int i = tid; i < n; i += nt)
+        if (x0 + (i & 1) < pw) dst[(size_t)(i >> 1) * pw + (i & 1)] = bspline_edge_fix(r[i], i >> 1, ph, kc[i & 1]);
+    }
+  };
   if (!REFPACK) {
     const float hx = __ldg(g.hxf + x), omx = __ldg(g.omxf + x), bx = __ldg(g.bxf + x);
     const int kend = min(g.F, (int)(blockIdx.y + 1) * RESP_G);
@@ -921,8 +945,8 @@ __global__ void __launch_bounds__(pair_threads<REFPACK>(FIXL), 2) k_fft_cols_pai
       __syncthreads();
       float2* r = fft_run<FIXL, C>(A, B, plh, true);
       float2* idle = r == A ? B : A;
-      bspline_edges<C>(r, ph, (float4*)idle);  // the prefilter's edge terms along y
-      store(r, k);
+      bspline_edge_consts<C>(r, ph, (float4*)idle);  // the prefilter's edge terms along y, added by the store
+      store_edges(r, (const float4*)idle, k);
       __syncthreads();
     }
   } else {
@@ -1034,16 +1058,18 @@ __global__ void __launch_bounds__(FIXL > 0 ? 288 : FFT_TMAX, FIXL > 0 ? 3 : 2)
     __syncthreads();
     float2* r0 = fft_run<FIXL, 1>(x0, fa, plw, true);
     float2* s0 = r0 == x0 ? fa : x0;
-    bspline_edges<1>(r0, L, (float4*)s0);
+    bspline_edge_consts<1>(r0, L, (float4*)s0);  // the edge terms along x, added by the store
+    const float4 k0 = *(const float4*)s0;        // s0 is line 1's transform buffer next
     fetch(nxt, 0, fb);         // the next row's line 0 during line 1's transform
     __pipeline_wait_prior(1);  // line 1 has landed
     __syncthreads();
     float2* r1 = fft_run<FIXL, 1>(x1, s0, plw, true);
     float2* s1 = r1 == x1 ? s0 : x1;
-    bspline_edges<1>(r1, L, (float4*)s1);
+    bspline_edge_consts<1>(r1, L, (float4*)s1);
+    const float4 k1 = *(const float4*)s1;
     float4* o = (float4*)R + (size_t)row * L;
     for (int x = threadIdx.x; x < L; x += blockDim.x) {
-      const float2 a = r0[x], b = r1[x];
+      const float2 a = bspline_edge_fix(r0[x], x, L, k0), b = bspline_edge_fix(r1[x], x, L, k1);
       o[x] = make_float4(a.x * scale, a.y * scale, b.x * scale, b.y * scale);
     }
     __syncthreads();
