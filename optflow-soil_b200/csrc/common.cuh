@@ -92,10 +92,12 @@ __device__ inline bool make_taps(double x, double y, int w, int h, Taps& t) {
   int x0 = (int)fx, y0 = (int)fy;
   bspline_weights(x - fx, t.wx);
   bspline_weights(y - fy, t.wy);
+  // taps inside the plane (the usual case) need no mirroring: the same indices without the reflection tests
+  const bool ix = x0 >= 1 && x0 + 2 <= w - 1, iy = y0 >= 1 && y0 + 2 <= h - 1;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    t.xi[k] = mirror_near(x0 + k - 1, w);
-    t.yi[k] = mirror_near(y0 + k - 1, h);
+    t.xi[k] = ix ? x0 + k - 1 : mirror_near(x0 + k - 1, w);
+    t.yi[k] = iy ? y0 + k - 1 : mirror_near(y0 + k - 1, h);
   }
   return true;
 }
