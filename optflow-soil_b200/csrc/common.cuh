@@ -51,6 +51,11 @@ void prof_after(void* token, cudaStream_t st);
 
 inline unsigned div_up(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
 
+// raises kernel fn's dynamic shared-memory limit on the current device to at least `bytes` and never lowers it:
+// the limit belongs to the kernel, not to a launch, so host threads that launch it with different sizes at once
+// (the pair driver's lanes) must not shrink it under each other's launches
+void raise_smem_limit(const void* fn, size_t bytes);
+
 // ---------------------------------------------------------------- cubic B-spline (interp.py)
 __host__ __device__ inline long mirror_idx(long i, long n) {  // interp.py:38-43
   if (n == 1) return 0;

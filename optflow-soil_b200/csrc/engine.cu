@@ -74,6 +74,18 @@ struct Profiler {
   }
 };
 
+void raise_smem_limit(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> limit;
+  int dev = 0;
+  OFC_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = limit[{fn, dev}];
+  if (bytes <= cur) return;
+  OFC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
+}
+
 void prof_before(const char* name, cudaStream_t st, void** token) {
   Profiler* p = g_profiler;
   std::string n(name);

@@ -1148,7 +1148,7 @@ __global__ void __launch_bounds__(FFT_TMAX, 2) k_fft_lines(float2* data, FftPlan
 constexpr size_t SMEM_MAX = 227 * 1024;
 
 static void set_smem(const void* fn, size_t bytes) {
-  OFC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  raise_smem_limit(fn, bytes);
 }
 
 static size_t fbytes(int L, int C) { return (size_t)fft_buf_len(L, C) * sizeof(float2); }

@@ -298,7 +298,7 @@ static void bspline_axes(const Tin* in, Tout* out, double* tmp, double* tmp2, in
   OFC_LAUNCH((k_iir_anticausal<double>), gy, 128, 0, st, tmp, tmp2, H, W, (long)W, 1L, plane);
   // along x: both recursions in one pass through shared-memory tiles
   const size_t sm = (size_t)XR_ROWS * XR_TW * sizeof(double);
-  OFC_CUDA(cudaFuncSetAttribute((const void*)k_iir_x<Tout, ILV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  raise_smem_limit((const void*)k_iir_x<Tout, ILV>, sm);
   dim3 gx(div_up(W, XR_SEG), div_up(H, XR_ROWS), n_planes);
   OFC_LAUNCH((k_iir_x<Tout, ILV>), gx, XR_ROWS, sm, st, tmp2, out, W, H, plane);
 }
@@ -475,7 +475,7 @@ void launch_accumulate_gather(const float4* ref4, const float2* R, int F, int ph
   dim3 g(div_up(W, ACC_BX), div_up(H, ACC_BY));
   const size_t sm = (size_t)F * ACC_T * sizeof(float4);
   if (sm > 227 * 1024) throw Error(OFC_ERR_WINDOW, "too many Gabor filters (" + std::to_string(F) + ") for the CUDA engine");
-  OFC_CUDA(cudaFuncSetAttribute((const void*)k_accumulate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  raise_smem_limit((const void*)k_accumulate, sm);
   OFC_LAUNCH(k_accumulate, g, dim3(ACC_BX, ACC_BY), sm, st, ref4, R, F, ph, pw, ux, uy, sx, sy, cs, W, H, sums);
 }
 
@@ -924,8 +924,7 @@ static void launch_moments_rb(const double* sums, const double* ux, const double
   dim3 gy(div_up(W, 128), div_up(H, MOM_RY));
   OFC_LAUNCH(k_moments_y_rb<ORDER>, gy, 128, 0, st, sums, W, H, tp, yplanes);
   const size_t sm = MomX<ORDER>::smem();
-  OFC_CUDA(cudaFuncSetAttribute((const void*)k_moments_x_solve_rb<ORDER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sm));
+  raise_smem_limit((const void*)k_moments_x_solve_rb<ORDER>, sm);
   dim3 gx(div_up(W, MomX<ORDER>::SEG), H);
   OFC_LAUNCH(k_moments_x_solve_rb<ORDER>, gx, MomX<ORDER>::NT, sm, st, yplanes, ux, uy, W, H, tp, oux, ouy, energy, resid,
              slope);

@@ -644,13 +644,13 @@ void launch_poc_grid(const double* a, const double* b, const PocLevel& lv, const
   double lpm = (double)(2 * (lv.wy / 4) + 1) * (double)(2 * (lv.wx / 4) + 1) / ((double)lv.wy * lv.wx);
   if (lv.wy == 64 && lv.wx == 64) {
     const size_t sm64 = (size_t)(64 * ZS + 33 * ZS) * sizeof(double2) + 64 * 64 * sizeof(double);
-    OFC_CUDA(cudaFuncSetAttribute((const void*)k_poc_grid64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm64));
+    raise_smem_limit((const void*)k_poc_grid64, sm64);
     OFC_LAUNCH(k_poc_grid64, lv.nx * lv.ny, POC_T, sm64, st, a, b, lv.W, lv.H, xs, ys, lv.nx, iux, iuy,
                (const PocConst*)dconst, lpm, ux, uy, peak, ipk);
     return;
   }
   size_t smem = (size_t)(lv.wy * (lv.wx + 1) + (2 * (lv.wy / 4) + 1) * (2 * (lv.wx / 4) + 1)) * sizeof(double2);
-  OFC_CUDA(cudaFuncSetAttribute((const void*)k_poc_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit((const void*)k_poc_grid, smem);
   OFC_LAUNCH(k_poc_grid, lv.nx * lv.ny, POC_T, smem, st, a, b, lv.W, lv.H, lv.wy, lv.wx, xs, ys, lv.nx, iux, iuy,
              (const PocConst*)dconst, lpm, ux, uy, peak, ipk);
 }
