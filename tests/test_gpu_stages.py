@@ -18,12 +18,14 @@ def T():
     return testing
 
 
-# direct plans (radices up to 31), then lengths with a larger prime factor (Bluestein: 37, 41 * 4, 2 * 53, 151 * 4 =
-# the padded height of a 960 x 540 frame, the primes 191 and 1021, 1999 = the largest inner length here, 4000)
+# direct plans (radices up to 31; 320 ... 2112 on plans fixed at compile time), then lengths with a larger prime factor
+# (Bluestein: 37, 41 * 4, 2 * 53, 151 * 4 = the padded height of a 960 x 540 frame (inner length 1216, on a fixed
+# plan), the primes 191 and 1021, and 1999 = the largest inner length here, 4096)
 BLUESTEIN = [37, 164, 106, 604, 191, 1021, 1999]
 
 
-@pytest.mark.parametrize("L", [64, 128, 160, 192, 224, 320, 576, 832, 1088, 1152, 2112, 2*3*5*7*11, 3*17*19, 23*29, 31*8]
+@pytest.mark.parametrize("L", [64, 128, 160, 192, 224, 320, 576, 832, 1024, 1088, 1152, 1600, 2112, 2*3*5*7*11, 3*17*19,
+                               23*29, 31*8]
                          + BLUESTEIN)
 def test_fft_lines_match_numpy(T, L):
     """Line transforms against numpy in float64: 2e-6 of the largest output for the direct plans, 1e-5 for
