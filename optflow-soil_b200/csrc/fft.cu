@@ -955,16 +955,45 @@ __global__ void __launch_bounds__(pair_threads<REFPACK>(FIXL), 2) k_fft_cols_pai
     for (int k = k0; k < k1; k++) {
       const double ex = g.ex[(size_t)k * pw + x];
       const double* eyk = g.ey + (size_t)k * ph;
-      // the row factors omy[y] ey_k[y] (and fy[y]) gathered per element, their loads batched
-      cols_multiply<FIXL, PAIR_T_REF, 4>(n, g.omy, [&](int i, double omy) {
-        const int y = i >> 1;
+      // the row factors omy[y], ey_k[y] (and fy[y]) per element
+      auto mul = [&](int i, double omy, double eyv, double fyv) {
         const float2 sv = raw[i];
-        const double G = fma(hx, omy, omx) * ex * __ldg(eyk + y);
+        const double G = fma(hx, omy, omx) * ex * eyv;
         double re = sv.x * G, im = sv.y * G;
-        if (v == 1) { const double t = re; re = -im * fx; im = t * fx; }                 // x i fx
-        else if (v == 2) { const double f = __ldg(g.fy + y); const double t = re; re = -im * f; im = t * f; }  // x i fy
+        if (v == 1) { const double t = re; re = -im * fx; im = t * fx; }          // x i fx
+        else if (v == 2) { const double t = re; re = -im * fyv; im = t * fyv; }  // x i fy
         A[i] = make_float2((float)re, (float)im);
-      });
+      };
+      if constexpr (FIXL > 0) {
+        // the three row factors of UN elements loaded together before their multiplies, so that their latencies
+        // overlap (blockDim = PAIR_T_REF)
+        constexpr int NT = PAIR_T_REF, NI = (2 * FIXL + NT - 1) / NT, UN = 4;
+#pragma unroll
+        for (int m0 = 0; m0 < NI; m0 += UN) {
+          double oy[UN], ey[UN], fy[UN];
+#pragma unroll
+          for (int u = 0; u < UN; u++) {
+            const int i = threadIdx.x + NT * (m0 + u);
+            oy[u] = ey[u] = fy[u] = 0.0;
+            if (m0 + u < NI && i < 2 * FIXL) {
+              const int y = i >> 1;
+              oy[u] = __ldg(g.omy + y);
+              ey[u] = __ldg(eyk + y);
+              if (v == 2) fy[u] = __ldg(g.fy + y);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < UN; u++) {
+            const int i = threadIdx.x + NT * (m0 + u);
+            if (m0 + u < NI && i < 2 * FIXL) mul(i, oy[u], ey[u], fy[u]);
+          }
+        }
+      } else {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+          const int y = i >> 1;
+          mul(i, __ldg(g.omy + y), __ldg(eyk + y), v == 2 ? __ldg(g.fy + y) : 0.0);
+        }
+      }
       __syncthreads();
       float2* r = fft_run<FIXL, C>(A, B, plh, true);
       store(r, 3 * (k - k0) + v);
