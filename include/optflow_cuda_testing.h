@@ -69,6 +69,11 @@ OFC_API int ofc_test_accumulate(ofc_engine* eng, const float* i1, const float* i
                                 const double* uy, const ofc_config* cfg, int mode, double* sums, uint32_t* timeouts,
                                 char* err, size_t errlen);
 
+/* The float32 atan2 of the accumulate's phase differences (the phase of r1 conj(r2), phaseflow.py:476-483, np.angle)
+ * beside CUDA's atan2f on the same n arguments: mine[i] = atan2_phase(y[i], x[i]), cuda[i] = atan2f(y[i], x[i]). */
+OFC_API int ofc_test_atan2(ofc_engine* eng, const float* y, const float* x, size_t n, float* mine, float* cuda,
+                           char* err, size_t errlen);
+
 /* The warp of the pre-warp and of the temporal-averaging alignment (warp_shifted, rust/crates/optflow-core/src/
  * phaseflow.rs:1420-1439): out(x, y) = the cubic B-spline of the w2 x h2 coefficient plane c2 sampled at
  * (x + shx + sx(x, y), y + shy + sy(x, y)) for the W x H fields sx, sy (doubles); NaN where a position is NaN.

@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(AT_T, ACC_TMA_MINB)
     // r1 conj(r2)
     const float re = fmaf(r1.x, br, r1.y * bi);
     const float im = fmaf(r1.y, br, -r1.x * bi);
-    const double dphi = (double)atan2f(im, re);
+    const double dphi = (double)atan2_phase(im, re);
     const double wk = (double)sqrtf(q1 * fmaf(br, br, bi * bi));  // |r1| |r2|
     const double gx = r1.z, gy = r1.w;
     const double c = dphi + gx * u + gy * v;

@@ -56,6 +56,34 @@ inline unsigned div_up(size_t a, size_t b) { return (unsigned)((a + b - 1) / b);
 // (the pair driver's lanes) must not shrink it under each other's launches
 void raise_smem_limit(const void* fn, size_t bytes);
 
+// atan2(y, x) in float32 for finite or NaN arguments, from the mathematics: with a = min(|x|, |y|) / max(|x|, |y|)
+// in [0, 1], atan(a) = a P(a^2), P the 8-term fit of atan(a) / a made by atan_fit.py (a minimax fit of the relative
+// error by iteratively reweighted least squares; 1.6e-7 rad at most in a float32 Horner); then pi/2 - r where
+// |y| > |x|, pi - r where x is negative (its sign bit: -0 included) and the sign of y (+-0 as atan2 gives them).
+// At most 5e-7 rad (about 2 ulp of pi) from the exact angle of the float32 arguments with the quotient's rounding and
+// the reflections; NaN in gives NaN; atan2(+-0, +0) = +-0 and atan2(+-0, -0) = +-pi.
+__device__ __forceinline__ float atan2_phase(float y, float x) {
+  if (y != y || x != x) return y + x;
+  const float ax = fabsf(x), ay = fabsf(y);
+  const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+  float a;
+  if (mx > 1e-30f && mx < 1e30f) a = __fdividef(mn, mx);  // the reciprocal's range: a fast quotient
+  else a = mx > 0.f ? mn / mx : 0.f;
+  const float t = a * a;
+  float p = -4.693272372e-03f;
+  p = fmaf(p, t, 2.425239656e-02f);
+  p = fmaf(p, t, -5.948639446e-02f);
+  p = fmaf(p, t, 9.914293821e-02f);
+  p = fmaf(p, t, -1.401948170e-01f);
+  p = fmaf(p, t, 1.996972415e-01f);
+  p = fmaf(p, t, -3.333199078e-01f);
+  p = fmaf(p, t, 9.999999010e-01f);
+  float r = p * a;
+  if (ay > ax) r = 1.57079632679489662f - r;
+  if (signbit(x)) r = 3.14159265358979324f - r;
+  return copysignf(r, y);
+}
+
 // ---------------------------------------------------------------- cubic B-spline (interp.py)
 __host__ __device__ inline long mirror_idx(long i, long n) {  // interp.py:38-43
   if (n == 1) return 0;

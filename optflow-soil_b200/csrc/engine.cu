@@ -3277,6 +3277,34 @@ int ofc_test_poc_peaks(ofc_engine* e, const float* a, const float* b, size_t w, 
   });
 }
 
+}  // extern "C"
+namespace {
+__global__ void k_test_atan2(const float* __restrict__ y, const float* __restrict__ x, size_t n, float* mine,
+                             float* cuda) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    mine[i] = atan2_phase(y[i], x[i]);
+    cuda[i] = atan2f(y[i], x[i]);
+  }
+}
+}  // namespace
+extern "C" {
+
+int ofc_test_atan2(ofc_engine* e, const float* y, const float* x, size_t n, float* mine, float* cuda, char* err,
+                   size_t errlen) {
+  return guarded(e, err, errlen, [&](Lane& L) {
+    if (n == 0) return;
+    if (!y || !x || !mine || !cuda) throw Error(OFC_ERR_ARG, "null argument");
+    const float* dy = L.upload("t_at_y", y, n);
+    const float* dx = L.upload("t_at_x", x, n);
+    float* dm = L.get<float>("t_at_m", n);
+    float* dc = L.get<float>("t_at_c", n);
+    OFC_LAUNCH(k_test_atan2, 296, 256, 0, L.stream, dy, dx, n, dm, dc);
+    OFC_CUDA(cudaMemcpyAsync(mine, dm, n * 4, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaMemcpyAsync(cuda, dc, n * 4, cudaMemcpyDeviceToHost, L.stream));
+    OFC_CUDA(cudaStreamSynchronize(L.stream));
+  });
+}
+
 int ofc_test_warp(ofc_engine* e, const float* c2, size_t w2, size_t h2, const double* sx, const double* sy, long shx,
                   long shy, size_t w, size_t h, int mode, float* out, uint32_t* timeouts, char* err, size_t errlen) {
   return guarded(e, err, errlen, [&](Lane& L) {

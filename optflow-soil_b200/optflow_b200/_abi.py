@@ -235,6 +235,7 @@ TEST_SIGNATURES = {
     "ofc_test_accumulate": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, _S, c_double_p, c_double_p,
                                            ctypes.POINTER(OfcConfig), ctypes.c_int, c_double_p,
                                            ctypes.POINTER(ctypes.c_uint32), _E, _S]),
+    "ofc_test_atan2": (ctypes.c_int, [_P, c_float_p, c_float_p, _S, c_float_p, c_float_p, _E, _S]),
     "ofc_test_warp": (ctypes.c_int, [_P, c_float_p, _S, _S, c_double_p, c_double_p, ctypes.c_long, ctypes.c_long, _S,
                                      _S, ctypes.c_int, c_float_p, ctypes.POINTER(ctypes.c_uint32), _E, _S]),
 }

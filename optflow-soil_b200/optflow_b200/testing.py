@@ -149,3 +149,15 @@ def warp(c2, sx, sy, shift=(0, 0), mode=1, engine=None):
     eng._call("ofc_test_warp", _ptr(c, c_float_p), w2, h2, _ptr(fx, c_double_p), _ptr(fy, c_double_p),
               int(shift[0]), int(shift[1]), w, h, int(mode), _ptr(out, c_float_p), ctypes.byref(tmo))
     return out, tmo.value
+
+
+def atan2(y, x, engine=None):
+    """The accumulate's float32 atan2 and CUDA's atan2f on the device for float32 arrays y, x: (mine, cuda)."""
+    eng = engine or default_engine()
+    yy = np.ascontiguousarray(y, dtype=np.float32).ravel()
+    xx = np.ascontiguousarray(x, dtype=np.float32).ravel()
+    mine = np.empty_like(yy)
+    cuda = np.empty_like(yy)
+    eng._call("ofc_test_atan2", _ptr(yy, c_float_p), _ptr(xx, c_float_p), yy.size, _ptr(mine, c_float_p),
+              _ptr(cuda, c_float_p))
+    return mine.reshape(np.shape(y)), cuda.reshape(np.shape(y))
