@@ -571,81 +571,10 @@ constexpr CPlan cplan(int L) {
   return c;
 }
 
-// The first two stages of a fixed plan that starts with two radix-8 stages, fused: stage-1 butterfly (q, r) takes
-// output r of the stage-0 butterflies q + M2 j (j = 0..7, M2 = L / 64), so a group of 8 lanes of one warp computes
-// those 8 stage-0 butterflies (lane j: butterfly q + M2 j), exchanges the 64 values through the group's own 64
-// stage-1 output slots (elements 64 q .. 64 q + 63 of its line; a warp barrier instead of a block barrier) and computes
-// the 8 stage-1 butterflies (lane r: butterfly (q, r)) into those slots. The butterflies, twiddles and rounding are
-// those of the two stages run one after the other. Every lane of a warp takes the same loop trips (groups beyond the
-// last idle), so the warp barriers see the whole warp; blockDim is a multiple of 32.
-template <int L, int C, int OSH, class C2>
-__device__ __noinline__ void stage_fixed_64(const C2* __restrict__ A, C2* __restrict__ B, const C2* __restrict__ tw,
-                                            bool inv) {
-  constexpr int M2 = L / 64, NG = M2 * C;
-  const int lane = threadIdx.x & 31, sub = lane & 7, gw = lane >> 3;
-  const int nw = blockDim.x >> 5;
-  auto slot = [](int e, int l) {  // element e of line l in the stage-1 output layout
-    const int o = e * C + l;
-    if constexpr (OSH < 31) return o + (o >> OSH);
-    else return o;
-  };
-  for (int g0 = (threadIdx.x >> 5) * 4; g0 < NG; g0 += nw * 4) {
-    const int g = g0 + gw;
-    const bool act = g < NG;
-    const int l = act ? g % C : 0, q = act ? g / C : 0;
-    if (act) {
-      // stage 0, butterfly q0: inputs element q0 + (L / 8) j, outputs k twiddled by w^(k q0)
-      const int q0 = q + M2 * sub;
-      auto in = [&](int j) { return A[(q0 + (L / 8) * j) * C + l]; };
-      auto emit = [&](int k, C2 val) {
-        if (k > 0 && q0 > 0) {
-          C2 w = __ldg(tw + k * q0);
-          val = cmul(val, inv ? conjf2(w) : w);
-        }
-        B[slot(64 * q + 8 * k + sub, l)] = val;  // output k of butterfly q + M2 sub, for lane k of the group
-      };
-      auto tw_m = [&](int mm) {
-        C2 w = __ldg(tw + mm * (L / 8));
-        return inv ? conjf2(w) : w;
-      };
-      butterfly<8, C2>(in, emit, tw_m, 8, inv);
-    }
-    __syncwarp();
-    C2 z[8];
-    if (act) {
-#pragma unroll
-      for (int j = 0; j < 8; j++) z[j] = B[slot(64 * q + 8 * sub + j, l)];
-    }
-    __syncwarp();
-    if (act) {
-      // stage 1, butterfly (q, r = sub): outputs k to element r + 64 q + 8 k, twiddled by w^(8 k q)
-      auto in = [&](int j) { return z[j]; };
-      auto emit = [&](int k, C2 val) {
-        if (k > 0 && q > 0) {
-          C2 w = __ldg(tw + k * 8 * q);
-          val = cmul(val, inv ? conjf2(w) : w);
-        }
-        B[slot(sub + 64 * q + 8 * k, l)] = val;
-      };
-      auto tw_m = [&](int mm) {
-        C2 w = __ldg(tw + mm * (L / 8));
-        return inv ? conjf2(w) : w;
-      };
-      butterfly<8, C2>(in, emit, tw_m, 8, inv);
-    }
-    __syncwarp();
-  }
-}
-
 template <int L, int C, int ST, class C2>
 __device__ __forceinline__ C2* fft_run_fixed(C2* a, C2* b, const C2* tw, bool inv) {
   constexpr CPlan P = cplan(L);
-  if constexpr (ST == 0 && P.nst >= 3 && P.p[0] == 8 && P.p[1] == 8 && P.s[1] == 8) {
-    constexpr int OSH = P.s[1] * C < 32 ? FFT_PAD : 31;  // stage 1's output layout (a stage follows it)
-    stage_fixed_64<L, C, OSH, C2>(a, b, tw, inv);
-    __syncthreads();
-    return fft_run_fixed<L, C, 2, C2>(b, a, tw, inv);
-  } else if constexpr (ST == P.nst) {
+  if constexpr (ST == P.nst) {
     return a;
   } else {
     constexpr int OSH = (ST + 1 < P.nst && P.s[ST] * C < 32) ? FFT_PAD : 31;
