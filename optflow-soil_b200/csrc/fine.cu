@@ -792,61 +792,69 @@ __device__ __forceinline__ void mom_x_stage(double* wb, int lt, const MomPf<ORDE
   }
 }
 
-// plane Q by one group: its segment is in the group's buffer `wb`; the loads of the group's next plane (Q + 2) are put
-// in flight first (registers pf) and staged into `wnext` at the end
-template <int ORDER, int Q>
-__device__ __forceinline__ void mom_x_plane(const double* __restrict__ yplanes, size_t N, int y, int x0, int W, int lt,
-                                            const double* wb, double* wnext, double* mom, const MomTaps& tp,
-                                            MomPf<ORDER>& pf) {
-  constexpr MomTable T = build_table(ORDER);
-  if constexpr (Q < T.ny) {
-    constexpr int R = MOM_R, RX = MomX<ORDER>::RX, SEG = MomX<ORDER>::SEG, NV = RX + 2 * R;
-    if constexpr (Q + 2 < T.ny) mom_x_fetch<ORDER>(yplanes + (size_t)(Q + 2) * N + (size_t)y * W, x0, W, lt, pf);
-    double v[NV];
-#pragma unroll
-    for (int i = 0; i < NV; i++) v[i] = wb[lt * RX + i];
-    int mi[5] = {-1, -1, -1, -1, -1};  // moment index of (Q, px)
-#pragma unroll
+// Per y-plane of an order: the number of x powers it feeds (always a prefix 0 .. npow - 1 of the powers) and the
+// moment-tile row of each, so that one plane body per power count serves every plane
+struct PlaneRows {
+  int npow[32] = {};
+  int mi[32][5] = {};
+};
+__host__ __device__ constexpr PlaneRows build_plane_rows(int order) {
+  PlaneRows r{};
+  const MomTable T = build_table(order);
+  for (int q = 0; q < T.ny; q++) {
+    for (int p = 0; p < 5; p++) r.mi[q][p] = -1;
+    int np = 0;
     for (int m = 0; m < T.nm; m++)
-      if (T.mjob[m] == Q) mi[T.mpx[m]] = m;
-    double acc[RX][5];
-#pragma unroll
-    for (int i = 0; i < RX; i++)
-#pragma unroll
-      for (int p = 0; p < 5; p++) acc[i][p] = p == 0 ? tp.k[0][0] * v[i + R] : 0.0;
-#pragma unroll
-    for (int t = 1; t <= R; t++)
-#pragma unroll
-      for (int i = 0; i < RX; i++) {
-        const double sp = v[i + R + t] + v[i + R - t], dm = v[i + R + t] - v[i + R - t];
-#pragma unroll
-        for (int p = 0; p < 5; p++)
-          if (mi[p] >= 0) acc[i][p] = fma(tp.k[p][t], (p & 1) ? dm : sp, acc[i][p]);
+      if (T.mjob[m] == q) {
+        r.mi[q][T.mpx[m]] = m;
+        if (T.mpx[m] + 1 > np) np = T.mpx[m] + 1;
       }
-#pragma unroll
-    for (int p = 0; p < 5; p++)
-      if (mi[p] >= 0)
-#pragma unroll
-        for (int i = 0; i < RX; i++) mom[mi[p] * SEG + lt * RX + i] = acc[i][p];
-    if constexpr (Q + 2 < T.ny) mom_x_stage<ORDER>(wnext, lt, pf);
+    r.npow[q] = np;
   }
+  return r;
 }
+__host__ __device__ constexpr bool plane_rows_are_prefixes(int order) {
+  const PlaneRows r = build_plane_rows(order);
+  const MomTable T = build_table(order);
+  for (int q = 0; q < T.ny; q++)
+    for (int p = 0; p < r.npow[q]; p++)
+      if (r.mi[q][p] < 0) return false;
+  return true;
+}
+static_assert(plane_rows_are_prefixes(1) && plane_rows_are_prefixes(2), "a y-plane feeds a gap in the powers");
+__host__ __device__ constexpr int max_plane_powers(int order) {
+  const PlaneRows r = build_plane_rows(order);
+  int mx = 0;
+  for (int q = 0; q < build_table(order).ny; q++) mx = r.npow[q] > mx ? r.npow[q] : mx;
+  return mx;
+}
+static_assert(max_plane_powers(1) == 3 && max_plane_powers(2) == 5, "the bodies' power counts");
+__constant__ PlaneRows c_plane_rows[2] = {build_plane_rows(1), build_plane_rows(2)};
 
-// the plane pair (K, K + 1): group g takes plane K + g from its buffer (K / 2) & 1; then a block barrier
-template <int ORDER, int K>
-__device__ __forceinline__ void mom_x_pairs(const double* __restrict__ yplanes, size_t N, int y, int x0, int W, int g,
-                                            int lt, double* smd, double* mom, const MomTaps& tp, MomPf<ORDER>& pf) {
-  constexpr MomTable T = build_table(ORDER);
-  if constexpr (K < T.ny) {
-    constexpr int WIN = MomX<ORDER>::WIN;
-    double* gb = smd + 2 * WIN * g;  // the group's two buffers
-    const double* wb = gb + ((K / 2) & 1) * WIN;
-    double* wnext = gb + (((K / 2) + 1) & 1) * WIN;
-    if (g == 0) mom_x_plane<ORDER, K>(yplanes, N, y, x0, W, lt, wb, wnext, mom, tp, pf);
-    else mom_x_plane<ORDER, K + 1>(yplanes, N, y, x0, W, lt, wb, wnext, mom, tp, pf);
-    __syncthreads();
-    mom_x_pairs<ORDER, K + 2>(yplanes, N, y, x0, W, g, lt, smd, mom, tp, pf);
-  }
+// one plane's x moments of powers 0 .. NP - 1 for a thread's RX pixels, from the segment in `wb`, into the tile rows mi
+template <int ORDER, int NP>
+__device__ __forceinline__ void mom_x_plane_np(const double* wb, double* mom, const int* mi, int lt, const MomTaps& tp) {
+  constexpr int R = MOM_R, RX = MomX<ORDER>::RX, SEG = MomX<ORDER>::SEG, NV = RX + 2 * R;
+  double v[NV];
+#pragma unroll
+  for (int i = 0; i < NV; i++) v[i] = wb[lt * RX + i];
+  double acc[RX][NP];
+#pragma unroll
+  for (int i = 0; i < RX; i++)
+#pragma unroll
+    for (int p = 0; p < NP; p++) acc[i][p] = p == 0 ? tp.k[0][0] * v[i + R] : 0.0;
+#pragma unroll
+  for (int t = 1; t <= R; t++)
+#pragma unroll
+    for (int i = 0; i < RX; i++) {
+      const double sp = v[i + R + t] + v[i + R - t], dm = v[i + R + t] - v[i + R - t];
+#pragma unroll
+      for (int p = 0; p < NP; p++) acc[i][p] = fma(tp.k[p][t], (p & 1) ? dm : sp, acc[i][p]);
+    }
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+#pragma unroll
+    for (int i = 0; i < RX; i++) mom[mi[p] * SEG + lt * RX + i] = acc[i][p];
 }
 
 template <int ORDER>
@@ -869,7 +877,31 @@ __global__ void __launch_bounds__(MomX<ORDER>::NT, ORDER == 1 ? 4 : 2) k_moments
     mom_x_stage<ORDER>(smd + 2 * WIN * g, lt, pf);
   }
   __syncthreads();
-  mom_x_pairs<ORDER, 0>(yplanes, N, y, x0, W, g, lt, smd, mom, tp, pf);
+  // the plane pairs (K, K + 1): group g takes plane K + g from its buffer (K / 2) & 1, one body per power count
+  const PlaneRows& PR = c_plane_rows[ORDER - 1];
+  double* gb = smd + 2 * WIN * g;  // the group's two buffers
+#pragma unroll 1
+  for (int K = 0; K < T.ny; K += 2) {
+    const int Q = K + g;
+    const double* wb = gb + ((K / 2) & 1) * WIN;
+    double* wnext = gb + (((K / 2) + 1) & 1) * WIN;
+    if (Q + 2 < T.ny) mom_x_fetch<ORDER>(yplanes + (size_t)(Q + 2) * N + (size_t)y * W, x0, W, lt, pf);
+    if (Q < T.ny) {
+      int mi[5];
+#pragma unroll
+      for (int p = 0; p < 5; p++) mi[p] = PR.mi[Q][p];
+      const int np = PR.npow[Q];  // order 1: at most 3 (powers 0 .. 2); order 2: at most 5
+      if (np == 1) mom_x_plane_np<ORDER, 1>(wb, mom, mi, lt, tp);
+      else if (np == 2) mom_x_plane_np<ORDER, 2>(wb, mom, mi, lt, tp);
+      else if (ORDER == 1 || np == 3) mom_x_plane_np<ORDER, 3>(wb, mom, mi, lt, tp);
+      else if constexpr (ORDER > 1) {
+        if (np == 4) mom_x_plane_np<ORDER, 4>(wb, mom, mi, lt, tp);
+        else mom_x_plane_np<ORDER, 5>(wb, mom, mi, lt, tp);
+      }
+    }
+    if (Q + 2 < T.ny) mom_x_stage<ORDER>(wnext, lt, pf);
+    __syncthreads();
+  }
 #pragma unroll 1
   for (int s = tid; s < SEG; s += NT) {
     const int x = x0 + s;
