@@ -93,19 +93,23 @@ __host__ __device__ inline long mirror_idx(long i, long n) {  // interp.py:38-43
   return i >= n ? p - i : i;
 }
 
+// the reference's quotients by 6 as products with the nearest double to 1/6: a float64 division is a sequence of a
+// dozen dependent instructions on the GPU, and the product is within an ulp of the quotient
 __host__ __device__ inline void bspline_weights(double t, double w[4]) {  // interp.py:46-49
+  const double s = 1.0 / 6.0;
   double t2 = t * t, t3 = t2 * t;
   double u = 1 - t;
-  w[0] = u * u * u / 6;
-  w[1] = (3 * t3 - 6 * t2 + 4) / 6;
-  w[2] = (-3 * t3 + 3 * t2 + 3 * t + 1) / 6;
-  w[3] = t3 / 6;
+  w[0] = u * u * u * s;
+  w[1] = (3 * t3 - 6 * t2 + 4) * s;
+  w[2] = (-3 * t3 + 3 * t2 + 3 * t + 1) * s;
+  w[3] = t3 * s;
 }
 
 // taps of sample(): clamp to [0, n-1], floor, weights, mirrored indices (interp.py:52-69)
 struct Taps {
   int xi[4], yi[4];
   double wx[4], wy[4];
+  bool cx;  // xi[k] = xi[0] + k (no reflection in x): a row's four taps are adjacent
 };
 
 // mirror_idx for an index at most one reflection outside [0, n) (the taps of a clamped position lie in
@@ -127,6 +131,7 @@ __device__ inline bool make_taps(double x, double y, int w, int h, Taps& t) {
   bspline_weights(y - fy, t.wy);
   // taps inside the plane (the usual case) need no mirroring: the same indices without the reflection tests
   const bool ix = x0 >= 1 && x0 + 2 <= w - 1, iy = y0 >= 1 && y0 + 2 <= h - 1;
+  t.cx = ix;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     t.xi[k] = ix ? x0 + k - 1 : mirror_near(x0 + k - 1, w);
@@ -176,6 +181,23 @@ __device__ __forceinline__ void sample2_real(const T* __restrict__ c1, const T* 
 // two real splines stored interleaved (double2 per pixel), sampled at the same taps
 __device__ __forceinline__ double2 sample_pair(const double2* __restrict__ c, int w, const Taps& t) {
   double o1 = 0, o2 = 0;
+  if (t.cx) {  // adjacent taps: one address per row, the four loads at fixed offsets from it
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const double2* row = c + (size_t)t.yi[j] * w + t.xi[0];
+      const double2 c0 = __ldg(row);
+      double a1 = t.wx[0] * c0.x, a2 = t.wx[0] * c0.y;
+#pragma unroll
+      for (int k = 1; k < 4; k++) {
+        const double2 v = __ldg(row + k);
+        a1 += t.wx[k] * v.x;
+        a2 += t.wx[k] * v.y;
+      }
+      o1 += t.wy[j] * a1;
+      o2 += t.wy[j] * a2;
+    }
+    return make_double2(o1, o2);
+  }
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     const double2* row = c + (size_t)t.yi[j] * w;

@@ -393,13 +393,10 @@ __global__ void __launch_bounds__(ACC_T, ACC_MINB) k_accumulate(const float4* __
   Taps t;
   const bool ok = make_taps(px + PAD, py + PAD, pw, ph, t);
   float fwx[4], fwy[4];
-  int ro[4], xo[4];  // tap (j, q) at ro[j] + xo[q] in a filter's plane
 #pragma unroll
   for (int k = 0; k < 4; k++) {
     fwx[k] = (float)t.wx[k];
     fwy[k] = (float)t.wy[k];
-    ro[k] = t.yi[k] * pw;
-    xo[k] = t.xi[k];
   }
   const size_t plane = (size_t)ph * pw;
   const float fnan = __int_as_float(0x7fc00000);
@@ -424,39 +421,59 @@ __global__ void __launch_bounds__(ACC_T, ACC_MINB) k_accumulate(const float4* __
     a5 = fma(wk * c, c, a5);
     a6 += wk;
   };
-  // the responses in filter pairs, node-major: one 16-byte load per tap gives both filters of a pair
+  // the responses in filter pairs, node-major: one 16-byte load per tap gives both filters of a pair. A pair's
+  // sample from its plane Rj, tap (jj, q) at Rj + off(jj, q); the next pair's tap rows go into L1 meanwhile
   const float4* R4 = reinterpret_cast<const float4*>(R);
   const int npairs = (F + 1) >> 1;
-  __pipeline_wait_prior(0);
-  for (int j = 0; j < npairs; j++) {
-    float b0r = fnan, b0i = fnan, b1r = fnan, b1i = fnan;
-    if (ok) {
-      const float4* Rj = R4 + (size_t)j * plane;
-      // the next pair's tap rows into L1 while this pair's taps and arithmetic run
-      if (j + 1 < npairs) {
+  auto pair_sample = [&](const float4* Rj, bool next, auto off, float& b0r, float& b0i, float& b1r, float& b1i) {
+    if (next) {
 #pragma unroll
-        for (int jj = 0; jj < 4; jj++) asm volatile("prefetch.global.L1 [%0];" ::"l"(Rj + plane + (ro[jj] + xo[0])));
-      }
-      b0r = b0i = b1r = b1i = 0.f;
-#pragma unroll
-      for (int jj = 0; jj < 4; jj++) {
-        float a0r = 0.f, a0i = 0.f, a1r = 0.f, a1i = 0.f;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const float4 cv = __ldg(Rj + (ro[jj] + xo[q]));
-          a0r = fmaf(fwx[q], cv.x, a0r);
-          a0i = fmaf(fwx[q], cv.y, a0i);
-          a1r = fmaf(fwx[q], cv.z, a1r);
-          a1i = fmaf(fwx[q], cv.w, a1i);
-        }
-        b0r = fmaf(fwy[jj], a0r, b0r);
-        b0i = fmaf(fwy[jj], a0i, b0i);
-        b1r = fmaf(fwy[jj], a1r, b1r);
-        b1i = fmaf(fwy[jj], a1i, b1i);
-      }
+      for (int jj = 0; jj < 4; jj++) asm volatile("prefetch.global.L1 [%0];" ::"l"(Rj + plane + off(jj, 0)));
     }
-    add(2 * j, b0r, b0i);
-    if (2 * j + 1 < F) add(2 * j + 1, b1r, b1i);
+    b0r = b0i = b1r = b1i = 0.f;
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) {
+      float a0r = 0.f, a0i = 0.f, a1r = 0.f, a1i = 0.f;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float4 cv = __ldg(Rj + off(jj, q));
+        a0r = fmaf(fwx[q], cv.x, a0r);
+        a0i = fmaf(fwx[q], cv.y, a0i);
+        a1r = fmaf(fwx[q], cv.z, a1r);
+        a1i = fmaf(fwx[q], cv.w, a1i);
+      }
+      b0r = fmaf(fwy[jj], a0r, b0r);
+      b0i = fmaf(fwy[jj], a0i, b0i);
+      b1r = fmaf(fwy[jj], a1r, b1r);
+      b1i = fmaf(fwy[jj], a1i, b1i);
+    }
+  };
+  __pipeline_wait_prior(0);
+  if (ok && t.cx && t.yi[1] == t.yi[0] + 1 && t.yi[2] == t.yi[0] + 2 && t.yi[3] == t.yi[0] + 3) {
+    // no reflection in either direction (all but the positions within a node of the padded plane's edge): the 4 x 4
+    // taps are a block, one address per row and the four loads at fixed offsets from it
+    const float4* Rj = R4 + ((size_t)t.yi[0] * pw + t.xi[0]);
+    for (int j = 0; j < npairs; j++, Rj += plane) {
+      float b0r, b0i, b1r, b1i;
+      pair_sample(Rj, j + 1 < npairs, [&](int jj, int q) { return jj * pw + q; }, b0r, b0i, b1r, b1i);
+      add(2 * j, b0r, b0i);
+      if (2 * j + 1 < F) add(2 * j + 1, b1r, b1i);
+    }
+  } else {
+    int ro[4], xo[4];  // tap (j, q) at ro[j] + xo[q] in a filter's plane
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      ro[k] = ok ? t.yi[k] * pw : 0;
+      xo[k] = ok ? t.xi[k] : 0;
+    }
+    for (int j = 0; j < npairs; j++) {
+      float b0r = fnan, b0i = fnan, b1r = fnan, b1i = fnan;
+      if (ok)
+        pair_sample(R4 + (size_t)j * plane, j + 1 < npairs, [&](int jj, int q) { return ro[jj] + xo[q]; }, b0r, b0i,
+                    b1r, b1i);
+      add(2 * j, b0r, b0i);
+      if (2 * j + 1 < F) add(2 * j + 1, b1r, b1i);
+    }
   }
   sums[p] = a0;
   sums[N + p] = a1;
