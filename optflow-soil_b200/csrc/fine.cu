@@ -605,9 +605,9 @@ __device__ __forceinline__ bool cholesky_solve_dev(double (&M)[N * N], double (&
     for (int k = 0; k < N; k++)
       if (k < j) d -= M[j * N + k] * M[j * N + k];
     okp &= d > 0.0 && d <= DBL_MAX;  // a failed pivot goes on with meaningless values and reports false
-    const double l = sqrt(d);
-    il[j] = 1.0 / l;
-    M[j * N + j] = l;
+    // the substitutions below read the pivots only as 1 / l: one reciprocal square root instead of a square root and
+    // a division (each a sequence of dependent float64 instructions)
+    il[j] = rsqrt(d);
 #pragma unroll
     for (int i = 0; i < N; i++) {
       if (i <= j) continue;
@@ -686,7 +686,7 @@ __global__ void __launch_bounds__(128) k_moments_x_solve(const double* __restric
     double tr = 0;
 #pragma unroll
     for (int i = 0; i < n; i++) tr += M[i * n + i];
-    double ridge = 1e-12 * tr / n;
+    double ridge = (1e-12 / n) * tr;
 #pragma unroll
     for (int i = 0; i < n; i++) M[i * n + i] += ridge;
     ok = cholesky_solve_dev<n>(M, b);
@@ -941,7 +941,7 @@ __global__ void __launch_bounds__(MomX<ORDER>::NT, ORDER == 1 ? 4 : 2) k_moments
       double tr = 0;
 #pragma unroll
       for (int k = 0; k < n; k++) tr += M[k * n + k];
-      double ridge = 1e-12 * tr / n;
+      double ridge = (1e-12 / n) * tr;
 #pragma unroll
       for (int k = 0; k < n; k++) M[k * n + k] += ridge;
       ok = cholesky_solve_dev<n>(M, b);
