@@ -134,10 +134,10 @@ def accumulate_bytes(W, H, F=12):
 
 
 # DRAM traffic of one k_accumulate launch over its algorithmic bytes, from one ncu capture on the 2048^2 pair
-# (dram__bytes_read.sum + dram__bytes_write.sum = 1416.5 + 258.6 MB against 1669.7 MB algorithmic,
+# (dram__bytes_read.sum + dram__bytes_write.sum = 1415.0 + 231.8 MB against 1669.7 MB algorithmic,
 # profiles/k_accumulate_2048.txt); at another size the traffic is this ratio times its algorithmic bytes (both
 # grow with the pixel and padded-pixel counts)
-ACC_TRAFFIC_RATIO = 1675.1 / 1669.7
+ACC_TRAFFIC_RATIO = 1646.8 / 1669.7
 
 
 def tile_windows(n, tile=1024, margin=64):
