@@ -663,11 +663,17 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
     }
     launch_corr_y(blur_in, tmpb, 2, W, H, d_ks, rs, st);
     launch_corr_x(tmpb, s2, 2, W, H, d_ks, rs, st);
+    // the spline of the smoothed field needs only s2: it runs on the side stream beside the warp and the response
+    // transforms (which leave HBM mostly idle), joined before the inner iterations read it
+    OFC_CUDA(cudaEventRecord(L.fork, st));
+    OFC_CUDA(cudaStreamWaitEvent(L.side, L.fork, 0));
+    launch_bspline_f64_pair(s2, (double2*)cs2, tmpb, W, H, L.side);
+    OFC_CUDA(cudaEventRecord(L.join, L.side));
     launch_warp(c2, w2, h2, s2, s2 + N, shx, shy, W, H, warped, st);
     launch_fft_rows_fwd_real(warped, W, H, plw, ph, T, st);
     launch_fft_cols_filters(T, plh, pw, g, U, st);
     launch_fft_rows_inv_resp(U, plw, ph, F, R, st);
-    launch_bspline_f64_pair(s2, (double2*)cs2, tmpb, W, H, st);
+    OFC_CUDA(cudaStreamWaitEvent(st, L.join, 0));
     for (int in = 0; in < c.inner_iters; in++) {
       launch_accumulate(ref4, R, F, ph, pw, ucur, ucur + N, s2, s2 + N, (const double2*)cs2, W, H, sums, st);
       launch_moments_solve(sums, ucur, ucur + N, W, H, c.shape_order, d_mt, rw, mtp, yplanes, unext, unext + N, energy,
