@@ -1034,9 +1034,10 @@ __device__ double atomic_max_d(double* a, double v) {
 // 2. k_radix_hist pass 1: the next 12 bits among the elements of that bucket.
 // 3. k_radix_compact: the elements of the 24-bit bucket into a candidate list (room for all n), and the largest
 //    key below the bucket.
-// 4. k_radix_final (one block): the remaining 40 bits over the candidates, and the largest key below the median's.
-// Six launches per median whatever the data; a bucket of many equal energies (heavy ties) only makes the one-block
-// final select longer.
+// 4. k_radix_final (one block): the remaining 40 bits over the candidates, the largest key below the median's, and
+//    the median (the mean of the two middle values for even n).
+// Five launches per median whatever the data (k_stats_init first); a bucket of many equal energies (heavy ties) only
+// makes the one-block final select longer.
 constexpr int RBITS = 12, RBINS = 1 << RBITS;
 constexpr int RH_T = 512;
 
@@ -1232,8 +1233,30 @@ __global__ void k_radix_compact(const double* __restrict__ e, size_t n, EnergySt
 }
 
 // the remaining CBITS bits of the median's key over the candidates (10-bit digits), and the largest key below it
-__global__ void __launch_bounds__(1024) k_radix_final(EnergyStats* s, const unsigned long long* __restrict__ cand) {
-  if (!s->need_median || s->nan) return;
+// after the passes: prefix = key of the element of rank n/2; for even n the one of rank n/2 - 1 is the same value
+// when `less` (elements below it) < n/2, else the largest element below it (lo_val)
+__device__ void median_finish(EnergyStats* s, size_t n) {
+  const double hi = okey_inv(s->prefix);
+  if (n % 2) {
+    s->median = hi;
+    return;
+  }
+  double lo = hi;
+  if (s->less >= (long long)(n / 2)) {
+    unsigned long long k = *(unsigned long long*)&s->lo_val;
+    lo = okey_inv(k);
+  }
+  s->median = (lo + hi) / 2.0;
+}
+
+// the last bits of the select over the candidates, then the median itself (thread 0)
+__global__ void __launch_bounds__(1024) k_radix_final(EnergyStats* s, const unsigned long long* __restrict__ cand,
+                                                      size_t n) {
+  if (!s->need_median) return;
+  if (s->nan) {
+    if (threadIdx.x == 0) s->median = nan("");
+    return;
+  }
   const unsigned nc = s->ncand;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   __shared__ unsigned int h[1024];
@@ -1296,22 +1319,8 @@ __global__ void __launch_bounds__(1024) k_radix_final(EnergyStats* s, const unsi
     s->rank = rank;
     s->less = less;
     *(unsigned long long*)&s->lo_val = best;
+    median_finish(s, n);
   }
-}
-
-// after the passes: prefix = key of the element of rank n/2; for even n the one of rank n/2 - 1 is the same value
-// when `less` (elements below it) < n/2, else the largest element below it (lo_val)
-__global__ void k_median_final(EnergyStats* s, size_t n) {
-  if (!s->need_median) return;
-  if (s->nan) { s->median = nan(""); return; }
-  double hi = okey_inv(s->prefix);
-  if (n % 2) { s->median = hi; return; }
-  double lo = hi;
-  if (s->less >= (long long)(n / 2)) {
-    unsigned long long k = *(unsigned long long*)&s->lo_val;
-    lo = okey_inv(k);
-  }
-  s->median = (lo + hi) / 2.0;
 }
 
 void launch_energy_median(const double* energy, size_t n, EnergyStats* stats, bool force_median,
@@ -1322,8 +1331,7 @@ void launch_energy_median(const double* energy, size_t n, EnergyStats* stats, bo
   OFC_LAUNCH(k_stats_hist0, 296, RH_T, 0, st, energy, n, stats, force_median ? 1 : 0, hist);
   OFC_LAUNCH(k_radix_hist, 296, RH_T, 0, st, energy, n, stats, 1, hist);
   OFC_LAUNCH(k_radix_compact, 296, 256, 0, st, energy, n, stats, cand);
-  OFC_LAUNCH(k_radix_final, 1, 1024, 0, st, stats, cand);
-  OFC_LAUNCH(k_median_final, 1, 1, 0, st, stats, n);
+  OFC_LAUNCH(k_radix_final, 1, 1024, 0, st, stats, cand, n);
 }
 
 __global__ void k_reset(const double* __restrict__ energy, const double* __restrict__ uxin,
