@@ -143,6 +143,17 @@ __device__ inline bool make_taps(double x, double y, int w, int h, Taps& t) {
 template <class T>
 __device__ inline double sample_real(const T* c, int w, const Taps& t) {
   double out = 0;
+  if (t.cx) {  // adjacent taps: one address per row, the same operations in the same order
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const T* row = c + (size_t)t.yi[j] * w + t.xi[0];
+      double acc = t.wx[0] * (double)row[0];
+#pragma unroll
+      for (int k = 1; k < 4; k++) acc += t.wx[k] * (double)row[k];
+      out += t.wy[j] * acc;
+    }
+    return out;
+  }
 #pragma unroll
   for (int j = 0; j < 4; j++) {
     const T* row = c + (size_t)t.yi[j] * w;
