@@ -585,6 +585,61 @@ __device__ __forceinline__ C2* fft_run_fixed(C2* a, C2* b, const C2* tw, bool in
   }
 }
 
+// The first stage of a fixed-length inverse column transform of a column pair with the responses' factor folded into
+// its loads: element i is raw[i] G, G = (hx + omx omy) ex ey bx by with (omy, ey by) the row table's entry of row
+// i / 2 and hx, omx, exb = ex bx the factors of the thread's column, which stays fixed (blockDim and the stage's input
+// stride are even). The products are rounded as the separate multiply pass rounded them (no contraction into the
+// butterfly's additions), so the transform sees the same values without that pass's shared-memory round trip and
+// barrier.
+template <int P, int S, int L, int C, int OSH, class C2>
+__device__ __noinline__ void stage_fixed_mul(const C2* __restrict__ raw, C2* __restrict__ B, const C2* __restrict__ tw,
+                                             bool inv, const float2* __restrict__ yt, float hx, float omx, float exb) {
+  static_assert(C == 2 && S == 1, "the first stage of a column pair");
+  constexpr int PB =
+      (P == 2 || P == 3 || P == 4 || P == 5 || P == 7 || P == 8 || P == 11 || P == 13 || P == 17 || P == 19) ? P : 0;
+  constexpr int M = L / (P * S), NB = (L / P) * C, ISTEP = S * M * C, OSTEP = S * C, LP = L / P;
+  static_assert(ISTEP % 2 == 0, "an element's column is the thread's");
+  for (int b = threadIdx.x; b < NB; b += blockDim.x) {
+    const int l = b % C, bi = b / C;
+    const int q = bi / S, r = bi - q * S;
+    const int ob = (r + S * P * q) * C + l;
+    auto in = [&](int j) {
+      const int i = b + j * ISTEP;
+      const float2 t = __ldg(yt + (i >> 1));
+      const C2 sv = raw[i];
+      const float G = fmaf(hx, t.x, omx) * exb * t.y;
+      return mkc<C2>(__fmul_rn(sv.x, G), __fmul_rn(sv.y, G));
+    };
+    auto emit = [&](int k, C2 val) {
+      if (k > 0 && q > 0) {
+        C2 w = __ldg(tw + k * S * q);  // k q S < L
+        val = cmul(val, inv ? conjf2(w) : w);
+      }
+      const int o = ob + k * OSTEP;
+      if constexpr (OSH < 31) B[o + (o >> OSH)] = val;
+      else B[o] = val;
+    };
+    auto tw_m = [&](int mm) {  // w_P^mm
+      C2 w = __ldg(tw + mm * LP);
+      return inv ? conjf2(w) : w;
+    };
+    butterfly<PB, C2>(in, emit, tw_m, P, inv);
+  }
+}
+
+// the fixed-length transform of a column pair whose first stage reads the staged pair `raw` through the factor
+// (stage_fixed_mul into a), then the remaining stages between a and b; returns the buffer holding the result
+template <int L, int C, class C2>
+__device__ __forceinline__ C2* fft_run_fixed_mul(const C2* raw, C2* a, C2* b, const C2* tw, bool inv,
+                                                 const float2* yt, float hx, float omx, float exb) {
+  constexpr CPlan P = cplan(L);
+  static_assert(P.nst >= 2, "at least two stages");
+  constexpr int OSH = (1 < P.nst && P.s[0] * C < 32) ? FFT_PAD : 31;
+  stage_fixed_mul<P.p[0], P.s[0], L, C, OSH, C2>(raw, a, tw, inv, yt, hx, omx, exb);
+  __syncthreads();
+  return fft_run_fixed<L, C, 1, C2>(a, b, tw, inv);
+}
+
 template <class C2>
 __device__ __forceinline__ void fft_stage(const C2* __restrict__ A, C2* __restrict__ B, int lc, int L, int P, int s,
                                           unsigned magic, const C2* __restrict__ tw, bool inv, int ish, int osh) {
@@ -937,13 +992,19 @@ __global__ void __launch_bounds__(pair_threads<REFPACK>(FIXL), 2) k_fft_cols_pai
     for (int k = blockIdx.y * RESP_G; k < kend; k++) {
       // G = (hx + omx omy) ex ey (bx by): the x factors of the thread's column, (omy, ey by) from the row table
       const float exb = __ldg(g.exf + (size_t)k * pw + x) * bx;
-      cols_multiply<FIXL, COLS_TMAX, 14>(n, g.yt2 + (size_t)k * ph, [&](int i, float2 t) {
-        const float2 sv = raw[i];
-        const float G = fmaf(hx, t.x, omx) * exb * t.y;
-        A[i] = make_float2(sv.x * G, sv.y * G);
-      });
-      __syncthreads();
-      float2* r = fft_run<FIXL, C>(A, B, plh, true);
+      float2* r;
+      if constexpr (FIXL > 0) {
+        r = fft_run_fixed_mul<FIXL, C, float2>(raw, A, B, (const float2*)plh.tw, true, g.yt2 + (size_t)k * ph, hx,
+                                               omx, exb);
+      } else {
+        cols_multiply<FIXL, COLS_TMAX, 14>(n, g.yt2 + (size_t)k * ph, [&](int i, float2 t) {
+          const float2 sv = raw[i];
+          const float G = fmaf(hx, t.x, omx) * exb * t.y;
+          A[i] = make_float2(sv.x * G, sv.y * G);
+        });
+        __syncthreads();
+        r = fft_run<FIXL, C>(A, B, plh, true);
+      }
       float2* idle = r == A ? B : A;
       bspline_edge_consts<C>(r, ph, (float4*)idle);  // the prefilter's edge terms along y, added by the store
       store_edges(r, (const float4*)idle, k);
