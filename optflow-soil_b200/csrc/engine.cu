@@ -641,6 +641,7 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
   const int Kf = c.prewarp_freeze_at;
   double* ucur = u2;
   double* unext = u2b;
+  bool primed = false;  // the first median starts the select state itself; each reset primes the next one's
   for (int it = 0; it < c.outer_iters; it++) {
     const double* blur_in = ucur;
     if (it > 0) {
@@ -679,8 +680,9 @@ FineOut refine_dev(Lane& L, const float* i1, int W, int H, const float* i2, int 
       launch_moments_solve(sums, ucur, ucur + N, W, H, c.shape_order, d_mt, rw, mtp, yplanes, unext, unext + N, energy,
                            resid, slope, st);
       const bool last_inner = in == c.inner_iters - 1;
-      launch_energy_median(energy, N, stats, last_inner, hist, st);
-      launch_reset(energy, ucur, ucur + N, (int)N, stats, unext, unext + N, resid, slope, st);
+      launch_energy_median(energy, N, stats, last_inner, hist, st, primed);
+      launch_reset(energy, ucur, ucur + N, (int)N, stats, unext, unext + N, resid, slope, st, true);
+      primed = true;
       std::swap(ucur, unext);
     }
   }

@@ -1041,7 +1041,9 @@ __device__ double atomic_max_d(double* a, double v) {
 constexpr int RBITS = 12, RBINS = 1 << RBITS;
 constexpr int RH_T = 512;
 
-__global__ void k_stats_init(EnergyStats* s, size_t n) {
+// the select state a median starts from (median, need_median and skip_reset, which the median's readers use, are
+// left alone)
+__device__ __forceinline__ void stats_prime(EnergyStats* s, size_t n) {
   s->lo = DBL_MAX;
   s->hi = -DBL_MAX;
   s->nan = 0;
@@ -1053,6 +1055,8 @@ __global__ void k_stats_init(EnergyStats* s, size_t n) {
   s->ncand = 0;
   s->below_max = 0;
 }
+
+__global__ void k_stats_init(EnergyStats* s, size_t n) { stats_prime(s, n); }
 
 __device__ __forceinline__ void digit_of(int pass, int& shift, int& bits) {
   int hi = 64 - RBITS * pass;
@@ -1324,10 +1328,10 @@ __global__ void __launch_bounds__(1024) k_radix_final(EnergyStats* s, const unsi
 }
 
 void launch_energy_median(const double* energy, size_t n, EnergyStats* stats, bool force_median,
-                          unsigned long long* scratch, cudaStream_t st) {
+                          unsigned long long* scratch, cudaStream_t st, bool primed) {
   unsigned long long* hist = scratch;
   unsigned long long* cand = scratch + RBINS;
-  OFC_LAUNCH(k_stats_init, 1, 1, 0, st, stats, n);
+  if (!primed) OFC_LAUNCH(k_stats_init, 1, 1, 0, st, stats, n);
   OFC_LAUNCH(k_stats_hist0, 296, RH_T, 0, st, energy, n, stats, force_median ? 1 : 0, hist);
   OFC_LAUNCH(k_radix_hist, 296, RH_T, 0, st, energy, n, stats, 1, hist);
   OFC_LAUNCH(k_radix_compact, 296, 256, 0, st, energy, n, stats, cand);
@@ -1335,8 +1339,11 @@ void launch_energy_median(const double* energy, size_t n, EnergyStats* stats, bo
 }
 
 __global__ void k_reset(const double* __restrict__ energy, const double* __restrict__ uxin,
-                        const double* __restrict__ uyin, int n, const EnergyStats* s, double* ux, double* uy,
-                        double* resid, double* slope) {
+                        const double* __restrict__ uyin, int n, EnergyStats* s, double* ux, double* uy,
+                        double* resid, double* slope, int prime) {
+  // the next median's start state, in place of its own k_stats_init launch (this kernel is the last reader of the
+  // select state's result, and it reads only median and skip_reset)
+  if (prime && blockIdx.x == 0 && threadIdx.x == 0) stats_prime(s, (size_t)n);
   if (s->skip_reset) return;
   const double thr = 1e-9 * s->median + 1e-30;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
@@ -1349,9 +1356,10 @@ __global__ void k_reset(const double* __restrict__ energy, const double* __restr
   }
 }
 
-void launch_reset(const double* energy, const double* ux_in, const double* uy_in, int n, const EnergyStats* stats,
-                  double* ux, double* uy, double* resid, double* slope, cudaStream_t st) {
-  OFC_LAUNCH(k_reset, div_up(n, 256), 256, 0, st, energy, ux_in, uy_in, n, stats, ux, uy, resid, slope);
+void launch_reset(const double* energy, const double* ux_in, const double* uy_in, int n, EnergyStats* stats,
+                  double* ux, double* uy, double* resid, double* slope, cudaStream_t st, bool prime_next) {
+  OFC_LAUNCH(k_reset, div_up(n, 256), 256, 0, st, energy, ux_in, uy_in, n, stats, ux, uy, resid, slope,
+             prime_next ? 1 : 0);
 }
 
 // ---------------------------------------------------------------- confidence

@@ -77,11 +77,13 @@ struct EnergyStats {
 inline size_t median_scratch(size_t n) { return 4096 + n; }
 // stats->lo/hi/nan/skip_reset of energy, and its median into stats->median (np.median) when the reset needs it
 // or force_median; scratch: median_scratch(n) unsigned long long whose first 4096 are zero (they are left zero)
+// primed: stats already hold a median's start state (a launch_reset with prime_next since the last median)
 void launch_energy_median(const double* energy, size_t n, EnergyStats* stats, bool force_median,
-                          unsigned long long* scratch, cudaStream_t st);
-// reset below 1e-9 median + 1e-30 (phaseflow.py:149-151,158-161)
-void launch_reset(const double* energy, const double* ux_in, const double* uy_in, int n, const EnergyStats* stats,
-                  double* ux, double* uy, double* resid, double* slope, cudaStream_t st);
+                          unsigned long long* scratch, cudaStream_t st, bool primed = false);
+// reset below 1e-9 median + 1e-30 (phaseflow.py:149-151,158-161); prime_next: also put the next median's start state
+// into stats (its median and skip_reset stay as they are)
+void launch_reset(const double* energy, const double* ux_in, const double* uy_in, int n, EnergyStats* stats,
+                  double* ux, double* uy, double* resid, double* slope, cudaStream_t st, bool prime_next = false);
 
 // confidence before the border rule (phaseflow.py:320-323) and low = conf < conf_min; with border = true
 // also the border rule (phaseflow.py:297-317,508-510): conf_out (f32), low (u8), conf64 (nullable)
