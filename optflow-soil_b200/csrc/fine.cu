@@ -1036,8 +1036,8 @@ __device__ double atomic_max_d(double* a, double v) {
 //    key below the bucket.
 // 4. k_radix_final (one block): the remaining 40 bits over the candidates, the largest key below the median's, and
 //    the median (the mean of the two middle values for even n).
-// Five launches per median whatever the data (k_stats_init first); a bucket of many equal energies (heavy ties) only
-// makes the one-block final select longer.
+// Four or five launches per median whatever the data (k_stats_init first, unless the last k_reset primed the state);
+// a bucket of many equal energies (heavy ties) only makes the one-block final select longer.
 constexpr int RBITS = 12, RBINS = 1 << RBITS;
 constexpr int RH_T = 512;
 
