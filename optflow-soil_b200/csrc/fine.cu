@@ -45,8 +45,9 @@ __global__ void k_corr_x(const double* __restrict__ in, double* __restrict__ out
 // consecutive rows of a column and loads their 2r + CY_RY input rows once (instead of 2r + 1 loads per output,
 // most of them L2 traffic); x: a block stages a row segment and its halo in shared memory and a thread forms
 // CX_RX consecutive outputs from one register window (odd CX_RX: the warp's reads fall on distinct banks).
-// Symmetric taps are paired (k(t) = k(-t)).
-constexpr int CORR_R = 16, CY_RY = 4, CX_RX = 3;
+// Symmetric taps are paired (k(t) = k(-t)). Eight rows per thread in y (40 loads for 8 outputs, 80 registers, six
+// blocks per SM) took 0.040 ms per pass of the two field planes at 2048^2 against 0.052 ms with four.
+constexpr int CORR_R = 16, CY_RY = 8, CX_RX = 3;
 
 __global__ void __launch_bounds__(128, 6) k_corr_y_rb(const double* __restrict__ in, double* __restrict__ out, int W,
                                                      int H, const double* __restrict__ taps) {
